@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 statevector engine.
+
+Headline workload (one "step"): one application of a 28-qubit random brickwork circuit of
+depth 20 (Haar SU(2) on every qubit + alternating CZ layers), complex128, with the fusion
+width chosen by the autotuner.  Metric: gate GB/s = algorithmic HBM bytes of the fused-gate
+passes (2 x 2^n x 16 B per full-register pass) / device time.  The register (4 GiB) is larger
+than L2 (126 MB), so no L2 flush is needed between steps.
+
+Also reported on the same line:
+  * roofline of the dominant kernel (the fused dense-block pass) against measured HBM peak;
+  * e2e: the same metric through the public Register API with the command stream uploaded
+    and the final state read back into pinned host memory inside the timed region;
+  * adjoint: 24-qubit HEA (8 layers, 384 parameters) with TFIM + 500 random weight<=4
+    terms, gradients/s of the adjoint sweep vs the parameter-shift rule on the same GPU;
+  * cpu_baseline: the reference's own CPU simulator (oracle/_ref) on the host cores over a
+    bounded sample of the same workload.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QUBITS = 28
+DEPTH = 20
+SEED = 1234
+ADJ_N, ADJ_LAYERS, ADJ_TERMS = 24, 8, 500
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:  # noqa: BLE001
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for name, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- workload
+
+def brickwork_stream():
+    from openqarp_b200 import circuits, ir
+    cmds = circuits.brickwork(N_QUBITS, DEPTH, seed=SEED)
+    return cmds, ir.pack(cmds).buf
+
+
+def fused_passes(buf, n, k):
+    import ctypes
+    from openqarp_b200 import _lib
+    cnt = ctypes.c_int32()
+    hist = np.zeros(9, dtype=np.int32)
+    _lib.check(_lib.lib.qsv_fuse_count(_lib.u8ptr(buf), len(buf), n, k, 12, ctypes.byref(cnt),
+                                       _lib.i32ptr(hist)))
+    return cnt.value, hist
+
+
+class StreamTimer:
+    """CUDA events recorded on the engine register's own stream."""
+
+    def __init__(self, reg):
+        import torch
+        _, s = reg.device_pointer()
+        self.stream = torch.cuda.ExternalStream(s, device=torch.device("cuda", reg.device))
+        self.torch = torch
+
+    def event(self):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        return e
+
+
+def autotune(reg, buf, timer, candidates=(2, 3, 4, 5)):
+    """Pick the fusion width with the shortest device time for this circuit (one timed
+    application per candidate after one warm-up)."""
+    res = {}
+    for k in candidates:
+        reg.configure(k, 12)
+        reg.apply(buf)
+        reg.synchronize()
+        e0 = timer.event()
+        reg.apply(buf)
+        e1 = timer.event()
+        e1.synchronize()
+        res[k] = e0.elapsed_time(e1)
+    best = min(res, key=res.get)
+    return best, res
+
+
+def kernel_probe(reg, timer, k, reps=20):
+    """Average device time of one fused k-qubit dense pass (the dominant kernel), launched
+    back to back on the register's stream."""
+    from openqarp_b200 import ir
+    rng = np.random.default_rng(7)
+    z = rng.standard_normal((1 << k, 1 << k)) + 1j * rng.standard_normal((1 << k, 1 << k))
+    u, _ = np.linalg.qr(z)
+    qs = tuple(int(q) for q in rng.permutation(N_QUBITS)[:k])
+    one = ir.pack([ir.custom(qs, u)]).buf
+    buf = one * reps
+    reg.configure(0, 0)
+    reg.apply(one)
+    reg.synchronize()
+    e0 = timer.event()
+    reg.apply(buf)
+    e1 = timer.event()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return ms, qs
+
+
+def cpu_baseline_sample(buf_layer, n, threads=None):
+    """The reference CPU simulator (oracle/_ref, its own fused dispatch at k=3) on one
+    brickwork layer at the full register width: returns (GB/s, seconds, passes, cores)."""
+    from oracle.oracle import Reference, Restatement
+    cores = threads or os.cpu_count() or 1
+    try:
+        ref = Reference()
+        ref.set_threads(cores)
+        state = np.zeros(1 << n, dtype=np.complex128)
+        state[0] = 1
+        t0 = time.perf_counter()
+        passes = ref.apply_fused_inplace(state, n, buf_layer, 3, 12)
+        dt = time.perf_counter() - t0
+        kind = "reference"
+    except FileNotFoundError:
+        rs = Restatement()
+        state = np.zeros(1 << n, dtype=np.complex128)
+        state[0] = 1
+        t0 = time.perf_counter()
+        rs.apply(state, n, buf_layer)
+        dt = time.perf_counter() - t0
+        passes = fused_passes(buf_layer, n, 0)[0]
+        kind, cores = "port", 1
+    gbs = passes * 2 * (1 << n) * 16 / dt / 1e9
+    return gbs, dt, passes, cores, kind
+
+
+def adjoint_vs_param_shift(device, shift_sample=12):
+    """24-qubit adjoint gradient vs parameter shift on the same GPU (config-3 shape)."""
+    import torch
+    from openqarp_b200 import B200Simulator, circuits, ir, observable
+    from openqarp_b200.ir import Command, GateType as G
+    cmds, vals, names = circuits.hea(ADJ_N, ADJ_LAYERS, seed=SEED)
+    obs = circuits.tfim_chain(ADJ_N) + circuits.random_pauli_sum(ADJ_N, ADJ_TERMS, seed=SEED + 1,
+                                                                  max_weight=4, coeff_std=0.1)
+    sim = B200Simulator(device=device)
+    masks = observable.to_masks(obs, ADJ_N)
+    stream = ir.pack(cmds, vals, names)
+    reg = sim.register(ADJ_N)
+    reg.reset()
+    reg.adjoint(stream, len(names), masks)       # warm-up
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    reg.reset()
+    energy, grad = reg.adjoint(stream, len(names), masks)
+    t_adj = time.perf_counter() - t0
+    # parameter shift: 2 energy evaluations per parameter occurrence, timed on a sample
+    concrete = [Command(c.gate, c.qubits, tuple(p.evaluate(vals) for p in c.params)) for c in cmds]
+    param_idx = [i for i, c in enumerate(cmds) if c.is_parametric()]
+    sample = param_idx[:shift_sample]
+    shifted_bufs = []
+    for i in sample:
+        for s in (np.pi / 2, -np.pi / 2):
+            sh = list(concrete)
+            sh[i] = Command(sh[i].gate, sh[i].qubits, (sh[i].params[0] + s,))
+            shifted_bufs.append(ir.pack(sh).buf)
+    reg.reset()
+    reg.apply(shifted_bufs[0])
+    reg.expectation(masks)
+    t0 = time.perf_counter()
+    grads = []
+    for j in range(0, len(shifted_bufs), 2):
+        e = []
+        for b in shifted_bufs[j:j + 2]:
+            reg.reset()
+            reg.apply(b)
+            e.append(reg.expectation(masks).real)
+        grads.append(0.5 * (e[0] - e[1]))
+    t_ps_sample = time.perf_counter() - t0
+    t_ps = t_ps_sample * len(param_idx) / len(sample)
+    err = float(np.max(np.abs(np.array(grads) - grad[[names.index(cmds[i].params[0].free_symbols()[0])
+                                                       for i in sample]])))
+    sim.close()
+    return {"n_qubits": ADJ_N, "params": len(names), "terms": len(obs), "energy": energy,
+            "adjoint_s": t_adj, "adjoint_grads_per_s": 1.0 / t_adj,
+            "param_shift_s": t_ps, "param_shift_grads_per_s": 1.0 / t_ps,
+            "speedup_vs_param_shift": t_ps / t_adj,
+            "param_shift_sample": f"{len(sample)} of {len(param_idx)} parameter occurrences "
+                                  f"({2 * len(sample)} evaluations), time scaled by occurrences",
+            "max_abs_diff_adjoint_vs_shift": err}
+
+
+# ---------------------------------------------------------------- arms
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from openqarp_b200 import circuits, ir
+    layer = ir.pack(circuits.brickwork(N_QUBITS, 1, seed=SEED)).buf
+    for _ in range(args.warmup):
+        cpu_baseline_sample(layer, N_QUBITS)
+    times, rates = [], []
+    kind, cores, passes = "reference", os.cpu_count(), 0
+    for _ in range(args.steps):
+        gbs, dt, passes, cores, kind = cpu_baseline_sample(layer, N_QUBITS)
+        times.append(dt)
+        rates.append(gbs)
+    v = float(np.median(rates))
+    print(json.dumps({
+        "metric": "gate GB/s (%HBM peak) @28q", "value": v, "unit": "GB/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * float(np.median(times)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": f"brickwork n={N_QUBITS} depth=1 sample of depth {DEPTH}, fusion k=3",
+                   "l2": "register 4 GiB > L2"},
+        "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": kind,
+                         "sample": f"1 brickwork layer at {N_QUBITS} qubits per step ({passes} fused passes)"},
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def b200_arm(args, rank, world, local_rank):
+    import torch
+    from openqarp_b200 import Register, circuits, ir
+    device = local_rank
+    torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    cmds, buf = brickwork_stream()
+    reg = Register(N_QUBITS, "complex128", device)
+    timer = StreamTimer(reg)
+    best_k, sweep = autotune(reg, buf, timer)
+    reg.configure(best_k, 12)
+    passes, hist = fused_passes(buf, N_QUBITS, best_k)
+    pass_bytes = 2 * (1 << N_QUBITS) * 16
+    for _ in range(args.warmup):
+        reg.apply(buf)
+    reg.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    s0 = reg.stats()
+    with ClockSampler(device) as clocks:
+        e0 = timer.event()
+        for _ in range(args.steps):
+            reg.apply(buf)
+        e1 = timer.event()
+        e1.synchronize()
+    torch.cuda.synchronize(device)
+    s1 = reg.stats()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    bytes_per_step = (s1["hbm_bytes"] - s0["hbm_bytes"]) / args.steps
+    launches = int(s1["launches"] - s0["launches"])
+    ms_step = ms / args.steps
+    value = world * bytes_per_step / (ms_step * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+
+    # dominant kernel probe
+    probe_ms, probe_q = kernel_probe(reg, timer, best_k)
+    achieved = pass_bytes / (probe_ms * 1e-3) / 1e9
+    reg.configure(best_k, 12)
+
+    # end to end through the public API: upload commands, apply from |0>, read back
+    out = torch.empty(2 * (1 << N_QUBITS), dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+    reg.reset()
+    reg.apply(buf)
+    reg.get_state(out)
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        stream = ir.pack(cmds)
+        reg.reset()
+        reg.apply(stream)
+        reg.get_state(out)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e_times))
+    e2e_value = world * bytes_per_step / e2e_s / 1e9
+
+    result = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.skip_cpu:
+            layer = ir.pack(circuits.brickwork(N_QUBITS, 1, seed=SEED)).buf
+            gbs, dt, cpasses, cores, kind = cpu_baseline_sample(layer, N_QUBITS)
+            cpu = {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind,
+                   "sample": f"1 brickwork layer at {N_QUBITS} qubits ({cpasses} fused passes, k=3), "
+                             f"{dt:.1f} s"}
+        adj = None
+        if not args.skip_adjoint:
+            reg.close()
+            adj = adjoint_vs_param_shift(device)
+        result = {
+            "metric": "gate GB/s (%HBM peak) @28q", "value": value, "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": f"brickwork n={N_QUBITS} depth={DEPTH} Haar SU(2)+CZ, seed {SEED}",
+                       "fusion_k": best_k, "autotune_ms": sweep, "fused_passes": passes,
+                       "block_widths": {str(k): int(c) for k, c in enumerate(hist) if c},
+                       "executor": "stream (one HBM pass per fused block)",
+                       "l2": "register 4 GiB > L2 126 MB: no flush needed",
+                       "parallelism": f"replicas x{world}"},
+            "pct_hbm_peak": 100.0 * value / (world * peak),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": f"k_dense_reg<double,{best_k}> on qubits {list(probe_q)}",
+                         "peak_source": peak_kind},
+            "e2e": {"value": e2e_value, "unit": "GB/s",
+                    "h2d_bytes_per_step": len(buf), "d2h_bytes_per_step": (1 << N_QUBITS) * 16,
+                    "ms_per_step": 1e3 * e2e_s},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+            "adjoint": adj,
+        }
+    else:
+        reg.close()
+    return result
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-adjoint", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res = b200_arm(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+/*
+ * qsv.h — C-ABI of the B200 statevector engine (libqsv.so).
+ *
+ * The library replaces the CPU simulator object that the reference's QarpEngine holds
+ * as `self._sim` (reference: src/qarp/engines/_qarp_engine.py:195-202), i.e. the
+ * qarpx::QarpSimulator surface (src/qarpx/include/qarpx/simulator/qarp_simulator.h:31-284,
+ * bound to Python in src/qarpx/python/bindings.cpp:1336-1513).  Every entry point:
+ *   - takes plain pointers and sizes (host memory unless stated), no C++ types;
+ *   - returns a status code (QSV_OK = 0) and never throws across the ABI;
+ *   - on failure leaves a thread-local message readable with qsv_last_error().
+ * The status codes map one-to-one onto the reference's exception classes:
+ * std::invalid_argument -> QSV_EINVAL (ValueError), std::runtime_error -> QSV_ERUNTIME
+ * (RuntimeError), qarpx::capability_error -> QSV_ECAPABILITY (CapabilityError)
+ * (reference: src/qarpx/python/bindings.cpp:272-290).
+ *
+ * Amplitudes cross the ABI as interleaved complex128 (re, im doubles), LSB-first:
+ * bit q of the amplitude index is qubit q (reference: docs/contracts/qarp_conventions.md:42-49).
+ *
+ * Thread safety: one CUDA stream per handle; calls on different handles may run from
+ * different host threads.  Calls on the same handle must be serialised by the caller.
+ */
+#ifndef QSV_H
+#define QSV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define QSV_API __attribute__((visibility("default")))
+#else
+#define QSV_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define QSV_OK          0
+#define QSV_EINVAL      1   /* std::invalid_argument -> ValueError                  */
+#define QSV_ERUNTIME    2   /* std::runtime_error    -> RuntimeError                */
+#define QSV_ECAPABILITY 3   /* qarpx::capability_error -> qarp.errors.CapabilityError */
+#define QSV_ECUDA       4   /* CUDA runtime failure (message carries cudaGetErrorString) */
+#define QSV_ENOMEM      5   /* device allocation failed                              */
+
+/* ---- amplitude storage types ------------------------------------------------------- */
+#define QSV_C128 0          /* complex128 state (16 B / amplitude)                    */
+#define QSV_C64  1          /* complex64 bulk state (8 B / amplitude), FP64 reductions */
+
+/* ---- packed command stream --------------------------------------------------------- *
+ * A command buffer is a byte sequence of records, each 8-byte aligned:
+ *
+ *   qsv_cmd_header                      8 bytes
+ *   uint32_t qubits[n_qubits]           local bit b <-> qubits[b]
+ *   uint32_t cbits[n_cbits]             Measure's recorded classical bits
+ *   (zero padding to a multiple of 8)
+ *   double   params[n_params]           concrete angles, in the reference's order
+ *   double   matrix[2 * 4^n_qubits]     only for QSV_GATE_CUSTOM: row-major 2^k x 2^k,
+ *                                       interleaved (re, im); row index = local output bits
+ *
+ * It is the byte form of qarpx::Command (reference: src/qarpx/include/qarpx/core/command.h:29-110)
+ * restricted to concrete parameters: gate codes are qarpx::GateType's enumerator values
+ * (reference: src/qarpx/include/qarpx/core/gates.h:8-58), so a Python caller converts a
+ * qx.Command by copying gate/qubits/params/cbits and, for Custom, its unitary.
+ */
+typedef struct qsv_cmd_header {
+    uint16_t gate;      /* qarpx::GateType value                                  */
+    uint8_t  n_qubits;
+    uint8_t  n_params;
+    uint8_t  n_cbits;
+    uint8_t  flags;     /* bit 0: command carries a classical condition (rejected) */
+    uint16_t reserved;
+} qsv_cmd_header;
+
+/* qarpx::GateType enumerator values (reference: src/qarpx/include/qarpx/core/gates.h:8-58). */
+enum qsv_gate {
+    QSV_GATE_X = 0, QSV_GATE_Y, QSV_GATE_Z, QSV_GATE_H, QSV_GATE_S, QSV_GATE_SDG,
+    QSV_GATE_T, QSV_GATE_TDG, QSV_GATE_SX, QSV_GATE_SXDG, QSV_GATE_ID,
+    QSV_GATE_RX, QSV_GATE_RY, QSV_GATE_RZ, QSV_GATE_P,
+    QSV_GATE_U,
+    QSV_GATE_CX, QSV_GATE_CY, QSV_GATE_CZ, QSV_GATE_SWAP, QSV_GATE_ECR,
+    QSV_GATE_ISWAP, QSV_GATE_ISWAPDG,
+    QSV_GATE_CH, QSV_GATE_CS, QSV_GATE_CSDG, QSV_GATE_CSX, QSV_GATE_CSXDG,
+    QSV_GATE_CRX, QSV_GATE_CRY, QSV_GATE_CRZ, QSV_GATE_CP, QSV_GATE_RZZ,
+    QSV_GATE_RXX, QSV_GATE_RYY,
+    QSV_GATE_CU,
+    QSV_GATE_CCX, QSV_GATE_CSWAP,
+    QSV_GATE_MCZ,
+    QSV_GATE_GPHASE,
+    QSV_GATE_BARRIER, QSV_GATE_MEASURE, QSV_GATE_RESET,
+    QSV_GATE_BRANCH_BEGIN, QSV_GATE_BRANCH_ELSE, QSV_GATE_BRANCH_END,
+    QSV_GATE_CUSTOM,
+    QSV_GATE_COUNT
+};
+
+/* Widest Custom / fused block (reference: dense_kernel.h:13 kMaxDenseBlockQubits = 8). */
+#define QSV_MAX_BLOCK_QUBITS 8
+/* Widest register a handle accepts (device memory bound: 2^34 c128 = 256 GiB > HBM). */
+#define QSV_MAX_QUBITS 34
+
+/* ---- per-handle statistics (bytes moved, kernel time) ---------------------------- */
+typedef struct qsv_stats_t {
+    uint64_t launches;          /* kernels launched by this handle since creation      */
+    uint64_t passes;            /* full-state gate passes                              */
+    uint64_t hbm_bytes;         /* algorithmic HBM bytes of those passes               */
+    uint64_t fused_blocks;      /* dense blocks applied                                */
+    double   last_apply_ms;     /* device time of the last qsv_apply (CUDA events)     */
+} qsv_stats_t;
+
+/* ---- library ------------------------------------------------------------------------ */
+
+/* Message of the last failing call on this host thread ("" when none). */
+QSV_API const char* qsv_last_error(void);
+/* ABI version of this header (bumped on any signature change). */
+QSV_API int qsv_abi_version(void);
+
+/* ---- handles: one register + one stream --------------------------------------------- */
+
+/* Allocate a 2^n_qubits register on CUDA device `device` and set it to |0...0>.
+ * Replaces QarpSimulator construction + allocate_quantum_state / initialize_quantum_state
+ * (reference: qarp_simulator.cpp:66-70, :926-933).  n_qubits in [0, QSV_MAX_QUBITS]. */
+QSV_API int qsv_create(int n_qubits, int dtype, int device, void** out_handle);
+QSV_API int qsv_destroy(void* h);
+
+/* Fusion knobs: fusion_max_qubits 0..QSV_MAX_BLOCK_QUBITS (EINVAL above, as
+ * set_fusion_max_qubits, qarp_simulator.cpp:82-88) and fusion_min_qubits
+ * (qarp_simulator.h:73-74). */
+QSV_API int qsv_set_fusion(void* h, int max_qubits, int min_qubits);
+/* Executor: 0 = one HBM pass per fused block ("stream"), 1 = several blocks per pass
+ * staged in shared memory ("tiled"), -1 = the autotuned choice (default). */
+QSV_API int qsv_set_executor(void* h, int mode);
+
+/* Register <- |0...0>. */
+QSV_API int qsv_reset(void* h);
+/* Register <- caller amplitudes (interleaved c128, len = 2^n).  validate != 0 checks
+ * the norm within 1e-10 exactly as validate_initial_state (qarp_simulator.cpp:731-746). */
+QSV_API int qsv_set_state(void* h, const double* amps, uint64_t len, int validate);
+/* Caller buffer <- register (interleaved c128, len = 2^n). */
+QSV_API int qsv_get_state(void* h, double* amps, uint64_t len);
+/* Device pointer of the register (double2* for C128, float2* for C64) and its stream,
+ * for zero-copy interop; valid until qsv_destroy. */
+QSV_API int qsv_device_state(void* h, void** dptr, void** cuda_stream);
+/* Copy the register of `src` into `dst` (same width and dtype), on dst's stream. */
+QSV_API int qsv_copy_state(void* dst, const void* src);
+
+/* Host-only (no device work): length of the fused stream the handle-independent knobs
+ * produce, and a histogram of its dense-block widths (widths_hist[k] = Custom blocks on k
+ * qubits, k = 0..8; may be NULL).  Replaces fuse_for_dispatch / fuse_for_simulation
+ * (reference: qarp_simulator.cpp:120-129, fusion.cpp:120-268) for plan inspection. */
+QSV_API int qsv_fuse_count(const uint8_t* cmds, size_t nbytes, int n_qubits, int max_qubits,
+                           int min_qubits, int32_t* n_out, int32_t* widths_hist);
+
+/* Apply a packed command stream in place, after the simulation-fusion pass the handle's
+ * knobs select.  Replaces the `for cmd in fused: apply_command` loop of
+ * QarpSimulator::statevector (qarp_simulator.cpp:901-943) and apply_command itself
+ * (qarp_simulator.cpp:356-596).  Measure/Barrier are no-ops; Reset, classical
+ * conditions and branch markers are rejected with QSV_ERUNTIME as statevector() does. */
+QSV_API int qsv_apply(void* h, const uint8_t* cmds, size_t nbytes);
+/* Apply the same stream with no fusion (the adjoint's forward sweep, unitary oracle). */
+QSV_API int qsv_apply_unfused(void* h, const uint8_t* cmds, size_t nbytes);
+
+/* <bra|H|ket> for H = sum_t coeff_t P_t, P_t given as bit masks: xmask = X or Y positions,
+ * zmask = Z or Y positions (Y = both), coeff = interleaved complex (2*n_terms doubles).
+ * The i^{n_Y} factor of each Y is applied inside.  Replaces pauli_transition
+ * (reference: pauli_expectation.cpp:159-167) and QarpSimulator::transition
+ * (qarp_simulator.cpp:954-967).  bra may equal ket. */
+QSV_API int qsv_transition(void* bra, void* ket, const uint64_t* xmask, const uint64_t* zmask,
+                   const double* coeff, size_t n_terms, double out[2]);
+
+/* Terminal sampling with caller uniforms u in [0,1): out_idx[s] = lower_bound(cdf, u[s])
+ * over the normalised cumulative |amp|^2, the draw rule of the reference's
+ * std::discrete_distribution in sample_terminal (qarp_simulator.cpp:751-783). */
+QSV_API int qsv_sample(void* h, const double* u, size_t n_shots, uint64_t* out_idx);
+/* Same, drawing u from std::mt19937(seed) with std::generate_canonical<double,53>, the
+ * exact stream std::discrete_distribution consumes in sample_terminal. */
+QSV_API int qsv_sample_seeded(void* h, uint32_t seed, size_t n_shots, uint64_t* out_idx);
+/* The uniforms qsv_sample_seeded draws (host only; no device work). */
+QSV_API int qsv_uniforms(uint32_t seed, size_t n_shots, double* u_out);
+
+/* Adjoint gradient of <psi|H|psi>, psi = U(theta)|psi0>, psi0 = the handle's current
+ * register.  cmds is the concrete stream; for command i, its angle depends on params
+ * dep_param[dep_ptr[i] .. dep_ptr[i+1]) with coefficients dep_alpha (d angle / d param).
+ * grad has n_params entries; energy (may be NULL) receives <H>.  Replaces
+ * QarpSimulator::run_gradient / run_gradient_core (qarp_simulator.cpp:1519-1605).
+ * The register holds psi_final on return. */
+QSV_API int qsv_adjoint(void* h, const uint8_t* cmds, size_t nbytes,
+                const int32_t* dep_ptr, const int32_t* dep_param, const double* dep_alpha,
+                int n_params,
+                const uint64_t* xmask, const uint64_t* zmask, const double* coeff,
+                size_t n_terms, double* grad, double* energy);
+/* run_gradient_phi (qarp_simulator.cpp:1620-1639): the gradient of 2 Re<phi|U|psi0>
+ * with a caller |phi> (interleaved c128, 2^n). */
+QSV_API int qsv_adjoint_phi(void* h, const uint8_t* cmds, size_t nbytes,
+                    const int32_t* dep_ptr, const int32_t* dep_param, const double* dep_alpha,
+                    int n_params, const double* phi, double* grad);
+
+/* Sum of |amp|^2 in FP64 (norm check / complex64 renormalisation). */
+QSV_API int qsv_norm2(void* h, double* out);
+/* Multiply the register by a real scale (renormalisation). */
+QSV_API int qsv_scale(void* h, double scale);
+/* <a|b> in FP64 (fidelity against another handle of the same width; dtypes may differ). */
+QSV_API int qsv_inner(void* a, void* b, double out[2]);
+
+QSV_API int qsv_synchronize(void* h);
+QSV_API int qsv_stats(void* h, qsv_stats_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSV_H */

@@ -1,0 +1,344 @@
+// kern_gates.cu — one-pass gate kernels over the full register in HBM.
+//
+// Each kernel is a single coalesced pass: a thread owns one "group" of amplitudes (the
+// 2^k amplitudes a k-qubit operator mixes, or a single amplitude for diagonal operators),
+// loads them with 8/16-byte vector loads, applies the operator in registers and stores
+// them back.  Consecutive threads own groups whose indices differ in the lowest non-target
+// bits, so every warp-wide load instruction covers whole 32-byte sectors.  Operator
+// coefficients travel in the kernel parameter block (constant bank): every lane reads the
+// same coefficient at the same time, which the constant cache broadcasts.
+//
+// Reference counterparts: the csim per-gate kernels (src/qarpx/third_party/csim/update_ops_*.cpp)
+// and apply_dense_k (src/qarpx/src/simulator/dense_kernel.cpp:23-81).
+#include <algorithm>
+#include <stdexcept>
+#include <vector>
+
+#include "kernels.h"
+
+namespace qsv {
+
+namespace {
+
+template <typename T> __host__ cplx<T> to_c(c128 v) { return {static_cast<T>(v.real()), static_cast<T>(v.imag())}; }
+
+// sorted list of positions with the bit value to insert at each
+struct BitPlan {
+    uint8_t pos[40];
+    uint8_t val[40];
+    int k;
+};
+
+__device__ __forceinline__ uint64_t insert_bits(uint64_t g, const BitPlan& p) {
+    for (int b = 0; b < p.k; ++b) {
+        const uint64_t q = p.pos[b];
+        const uint64_t low = g & ((1ull << q) - 1ull);
+        g = ((g >> q) << (q + 1)) | (static_cast<uint64_t>(p.val[b]) << q) | low;
+    }
+    return g;
+}
+
+BitPlan plan_from_masks(uint64_t zeros, uint64_t ones) {
+    BitPlan p{};
+    p.k = 0;
+    for (int q = 0; q < 64; ++q) {
+        const bool z = (zeros >> q) & 1, o = (ones >> q) & 1;
+        if (z || o) {
+            if (p.k >= 40) throw std::invalid_argument("operator touches more than 40 qubits");
+            p.pos[p.k] = static_cast<uint8_t>(q);
+            p.val[p.k] = o ? 1 : 0;
+            ++p.k;
+        }
+    }
+    return p;
+}
+
+// ---------------------------------------------------------------- dense, k <= 4 in registers
+template <typename T, int K>
+struct DenseArgs {
+    uint64_t off[1 << K];        // index offset of local basis state l
+    uint8_t pos[8];              // ascending target positions
+    cplx<T> m[1 << (2 * K)];     // row-major 2^K x 2^K
+};
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kThreads) k_dense_reg(vec2_t<T>* __restrict__ s, uint64_t n_groups,
+                                                         const __grid_constant__ DenseArgs<T, K> a) {
+    constexpr int D = 1 << K;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_groups; g += stride) {
+        const uint64_t base = insert_zeros(g, a.pos, K);
+        vec2_t<T> in[D];
+#pragma unroll
+        for (int l = 0; l < D; ++l) in[l] = s[base | a.off[l]];
+#pragma unroll
+        for (int y = 0; y < D; ++y) {
+            vec2_t<T> acc = cmul<T>(a.m[y * D], in[0]);
+#pragma unroll
+            for (int x = 1; x < D; ++x) acc = cfma<T>(a.m[y * D + x], in[x], acc);
+            s[base | a.off[y]] = acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- dense, any k (matrix in global)
+// One thread per output amplitude; the group's inputs are re-read through L1/L2.  Used for
+// k >= 5 blocks, which only user Custom gates or fusion widths above 4 produce.
+struct DenseGenArgs {
+    uint64_t off[256];
+    uint8_t pos[8];
+    int k;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_dense_gen(const vec2_t<T>* __restrict__ src, vec2_t<T>* __restrict__ dst,
+                                                         uint64_t n_out, const cplx<T>* __restrict__ m,
+                                                         const __grid_constant__ DenseGenArgs a) {
+    const int D = 1 << a.k;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < n_out; t += stride) {
+        const uint64_t g = t >> a.k;
+        const int y = static_cast<int>(t & (D - 1));
+        const uint64_t base = insert_zeros(g, a.pos, a.k);
+        double re = 0, im = 0;
+        for (int x = 0; x < D; ++x) {
+            const vec2_t<T> v = src[base | a.off[x]];
+            const cplx<T> c = m[y * D + x];
+            re = fma(static_cast<double>(c.re), v.x, re);
+            re = fma(-static_cast<double>(c.im), v.y, re);
+            im = fma(static_cast<double>(c.re), v.y, im);
+            im = fma(static_cast<double>(c.im), v.x, im);
+        }
+        dst[base | a.off[y]] = mk<T>(static_cast<T>(re), static_cast<T>(im));
+    }
+}
+
+// ---------------------------------------------------------------- diagonal on k <= 8 qubits
+template <typename T>
+struct DiagArgs {
+    uint8_t q[8];
+    int k;
+    cplx<T> d[256];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_diag(vec2_t<T>* __restrict__ s, uint64_t dim,
+                                                   const __grid_constant__ DiagArgs<T> a) {
+    __shared__ cplx<T> d[256];
+    for (int l = threadIdx.x; l < (1 << a.k); l += blockDim.x) d[l] = a.d[l];
+    __syncthreads();
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
+        uint32_t l = 0;
+        for (int b = 0; b < a.k; ++b) l |= static_cast<uint32_t>((i >> a.q[b]) & 1ull) << b;
+        s[i] = cmul<T>(d[l], s[i]);
+    }
+}
+
+// ---------------------------------------------------------------- phase on a masked subspace
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_phase(vec2_t<T>* __restrict__ s, uint64_t n_idx,
+                                                    const __grid_constant__ BitPlan p, cplx<T> ph) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_idx; g += stride) {
+        const uint64_t i = insert_bits(g, p);
+        s[i] = cmul<T>(ph, s[i]);
+    }
+}
+
+// ---------------------------------------------------------------- controlled 2x2
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_ctrl1(vec2_t<T>* __restrict__ s, uint64_t n_pairs,
+                                                    const __grid_constant__ BitPlan p, uint64_t tbit,
+                                                    cplx<T> m0, cplx<T> m1, cplx<T> m2, cplx<T> m3) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_pairs; g += stride) {
+        const uint64_t i0 = insert_bits(g, p);
+        const vec2_t<T> a0 = s[i0], a1 = s[i0 | tbit];
+        s[i0] = cfma<T>(m1, a1, cmul<T>(m0, a0));
+        s[i0 | tbit] = cfma<T>(m3, a1, cmul<T>(m2, a0));
+    }
+}
+
+// ---------------------------------------------------------------- swap
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_swap(vec2_t<T>* __restrict__ s, uint64_t n_idx,
+                                                   const __grid_constant__ BitPlan p, uint64_t abit, uint64_t bbit) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_idx; g += stride) {
+        const uint64_t i = insert_bits(g, p);
+        const vec2_t<T> x = s[i | abit], y = s[i | bbit];
+        s[i | abit] = y;
+        s[i | bbit] = x;
+    }
+}
+
+// ---------------------------------------------------------------- exp(-i theta/2 P)
+// P|i> = i^{nY} (-1)^{popcount(i & z)} |i ^ x>
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_pauli_rot(vec2_t<T>* __restrict__ s, uint64_t n_pairs,
+                                                        const __grid_constant__ BitPlan p, uint64_t x,
+                                                        uint64_t z, int ny, T c, T sn) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_pairs; g += stride) {
+        const uint64_t i = insert_bits(g, p), j = i ^ x;
+        const vec2_t<T> ai = s[i], aj = s[j];
+        // phase(i) = i^{ny} * sign(i); -i * sn * phase * a
+        auto rot = [&](uint64_t idx, vec2_t<T> a) {
+            const int e = (ny + 2 * (__popcll(idx & z) & 1) + 3) & 3;  // (-i) * i^ny * sign
+            // multiply a by i^e
+            vec2_t<T> r;
+            switch (e) {
+                case 0: r = a; break;
+                case 1: r = mk<T>(-a.y, a.x); break;
+                case 2: r = mk<T>(-a.x, -a.y); break;
+                default: r = mk<T>(a.y, -a.x); break;
+            }
+            return r;
+        };
+        const vec2_t<T> pj = rot(j, aj), pi = rot(i, ai);
+        s[i] = mk<T>(c * ai.x + sn * pj.x, c * ai.y + sn * pj.y);
+        s[j] = mk<T>(c * aj.x + sn * pi.x, c * aj.y + sn * pi.y);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_scale(vec2_t<T>* __restrict__ s, uint64_t dim, cplx<T> f) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride)
+        s[i] = cmul<T>(f, s[i]);
+}
+
+template <typename T, int K>
+void launch_dense_reg(const Op& op, vec2_t<T>* s, int n, cudaStream_t st) {
+    DenseArgs<T, K> a{};
+    uint32_t sorted[8];
+    for (int b = 0; b < K; ++b) sorted[b] = op.qubits[b];
+    std::sort(sorted, sorted + K);
+    for (int b = 0; b < 8; ++b) a.pos[b] = b < K ? static_cast<uint8_t>(sorted[b]) : 0;
+    for (int l = 0; l < (1 << K); ++l) {
+        uint64_t o = 0;
+        for (int b = 0; b < K; ++b) if ((l >> b) & 1) o |= 1ull << op.qubits[b];
+        a.off[l] = o;
+    }
+    for (int e = 0; e < (1 << (2 * K)); ++e) a.m[e] = to_c<T>(op.m[e]);
+    const uint64_t groups = (1ull << n) >> K;
+    k_dense_reg<T, K><<<grid_for(groups, 1, 1u << 20), kThreads, 0, st>>>(s, groups, a);
+}
+
+}  // namespace
+
+template <typename T>
+void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws) {
+    const uint64_t dim = 1ull << n;
+    switch (op.kind) {
+        case OP_NOP: return;
+        case OP_DENSE: {
+            if (op.k > n) throw std::invalid_argument("block wider than the register");
+            switch (op.k) {
+                case 1: launch_dense_reg<T, 1>(op, s, n, st); return;
+                case 2: launch_dense_reg<T, 2>(op, s, n, st); return;
+                case 3: launch_dense_reg<T, 3>(op, s, n, st); return;
+                case 4: launch_dense_reg<T, 4>(op, s, n, st); return;
+                default: break;
+            }
+            // k >= 5: out of place through a workspace copy of the register
+            const int k = op.k;
+            const size_t D = size_t{1} << k;
+            DenseGenArgs a{};
+            uint32_t sorted[8];
+            for (int b = 0; b < k; ++b) sorted[b] = op.qubits[b];
+            std::sort(sorted, sorted + k);
+            for (int b = 0; b < 8; ++b) a.pos[b] = b < k ? static_cast<uint8_t>(sorted[b]) : 0;
+            for (size_t l = 0; l < D; ++l) {
+                uint64_t o = 0;
+                for (int b = 0; b < k; ++b) if ((l >> b) & 1) o |= 1ull << op.qubits[b];
+                a.off[l] = o;
+            }
+            a.k = k;
+            std::vector<cplx<T>> hm(D * D);
+            for (size_t e = 0; e < D * D; ++e) hm[e] = to_c<T>(op.m[e]);
+            cplx<T>* dm = static_cast<cplx<T>*>(ws.matrix(hm.size() * sizeof(cplx<T>)));
+            check_cuda(cudaMemcpyAsync(dm, hm.data(), hm.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice, st),
+                       "matrix upload");
+            vec2_t<T>* copy = static_cast<vec2_t<T>*>(ws.state_copy(dim * sizeof(vec2_t<T>)));
+            check_cuda(cudaMemcpyAsync(copy, s, dim * sizeof(vec2_t<T>), cudaMemcpyDeviceToDevice, st), "copy");
+            k_dense_gen<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(copy, s, dim, dm, a);
+            // the host matrix must outlive the async copy
+            check_cuda(cudaStreamSynchronize(st), "dense k>=5");
+            return;
+        }
+        case OP_DIAG: {
+            DiagArgs<T> a{};
+            a.k = op.k;
+            for (int b = 0; b < op.k; ++b) a.q[b] = static_cast<uint8_t>(op.qubits[b]);
+            for (int l = 0; l < (1 << op.k); ++l) a.d[l] = to_c<T>(op.m[l]);
+            k_diag<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(s, dim, a);
+            return;
+        }
+        case OP_PHASE: {
+            const BitPlan p = plan_from_masks(0, op.mask);
+            const uint64_t n_idx = dim >> p.k;
+            k_phase<T><<<grid_for(n_idx, 1, 1u << 20), kThreads, 0, st>>>(s, n_idx, p, to_c<T>(op.m[0]));
+            return;
+        }
+        case OP_CTRL1: {
+            const uint64_t tbit = 1ull << op.target;
+            const BitPlan p = plan_from_masks(tbit, op.mask);
+            const uint64_t n_pairs = dim >> p.k;
+            k_ctrl1<T><<<grid_for(n_pairs, 1, 1u << 20), kThreads, 0, st>>>(
+                s, n_pairs, p, tbit, to_c<T>(op.m[0]), to_c<T>(op.m[1]), to_c<T>(op.m[2]), to_c<T>(op.m[3]));
+            return;
+        }
+        case OP_SWAP: {
+            const uint64_t a = 1ull << op.qubits[0], b = 1ull << op.qubits[1];
+            const BitPlan p = plan_from_masks(a | b, 0);
+            const uint64_t n_idx = dim >> 2;
+            k_swap<T><<<grid_for(n_idx, 1, 1u << 20), kThreads, 0, st>>>(s, n_idx, p, a, b);
+            return;
+        }
+        case OP_PAULI_ROT: {
+            const uint64_t x = op.mask, z = op.zmask;
+            const T c = static_cast<T>(op.m[0].real()), sn = static_cast<T>(op.m[0].imag());
+            if (x == 0) {  // diagonal: handled as k-qubit diag over z's bits
+                Op d;
+                d.kind = OP_DIAG;
+                int k = 0;
+                for (int q = 0; q < 64; ++q) if ((z >> q) & 1) d.qubits[k++] = static_cast<uint32_t>(q);
+                d.k = k;
+                d.m.resize(size_t{1} << k);
+                for (size_t l = 0; l < d.m.size(); ++l)
+                    d.m[l] = (__builtin_popcountll(l) & 1) ? c128(c, sn) : c128(c, -sn);
+                launch_op<T>(d, s, n, st, ws);
+                return;
+            }
+            const uint64_t pivot = x & (~x + 1);
+            const BitPlan p = plan_from_masks(pivot, 0);
+            const uint64_t n_pairs = dim >> 1;
+            k_pauli_rot<T><<<grid_for(n_pairs, 1, 1u << 20), kThreads, 0, st>>>(
+                s, n_pairs, p, x, z, __builtin_popcountll(x & z), c, sn);
+            return;
+        }
+        case OP_SCALE:
+            k_scale<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(s, dim, to_c<T>(op.m[0]));
+            return;
+    }
+}
+
+template void launch_op<double>(const Op&, double2*, int, cudaStream_t, Workspace&);
+template void launch_op<float>(const Op&, float2*, int, cudaStream_t, Workspace&);
+
+// algorithmic HBM bytes of one op (read + write of every amplitude it touches)
+uint64_t op_bytes(const Op& op, int n, int amp_bytes) {
+    const uint64_t dim = 1ull << n;
+    uint64_t touched = dim;
+    switch (op.kind) {
+        case OP_NOP: touched = 0; break;
+        case OP_PHASE: touched = dim >> __builtin_popcountll(op.mask); break;
+        case OP_CTRL1: touched = dim >> __builtin_popcountll(op.mask); break;
+        default: break;
+    }
+    return 2ull * touched * static_cast<uint64_t>(amp_bytes);
+}
+
+}  // namespace qsv

@@ -1,0 +1,106 @@
+// kernels.h — host-callable launchers of the engine's CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "lower.h"
+#include "qsv_common.cuh"
+
+namespace qsv {
+
+struct cuda_error : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw cuda_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Device scratch owned by a handle; grows on demand, freed with the handle.
+class Workspace {
+public:
+    ~Workspace() { release(); }
+    void release();
+    void* matrix(size_t bytes) { return grow(mat_, mat_cap_, bytes); }
+    void* state_copy(size_t bytes) { return grow(copy_, copy_cap_, bytes); }
+    void* scratch(size_t bytes) { return grow(scr_, scr_cap_, bytes); }
+    void* shots(size_t bytes) { return grow(shot_, shot_cap_, bytes); }
+    // pinned host staging for small results
+    double* host_result(size_t n_doubles);
+
+private:
+    static void* grow(void*& p, size_t& cap, size_t bytes);
+    void* mat_ = nullptr; size_t mat_cap_ = 0;
+    void* copy_ = nullptr; size_t copy_cap_ = 0;
+    void* scr_ = nullptr; size_t scr_cap_ = 0;
+    void* shot_ = nullptr; size_t shot_cap_ = 0;
+    double* host_ = nullptr; size_t host_cap_ = 0;
+};
+
+// ---------------------------------------------------------------- gates (kern_gates.cu)
+template <typename T>
+void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
+uint64_t op_bytes(const Op& op, int n, int amp_bytes);
+
+// ---------------------------------------------------------------- reductions (kern_reduce.cu)
+
+// Pauli-sum terms prepared for the device: grouped by X mask, coefficients carrying i^{nY}.
+struct PauliTerms {
+    std::vector<uint64_t> gx;        // per group: X mask
+    std::vector<int32_t> gstart;     // per group: first term (size groups + 1)
+    std::vector<uint64_t> z;         // per term: Z mask
+    std::vector<double> c;           // per term: coefficient * i^{nY} (re, im)
+};
+PauliTerms prepare_terms(const uint64_t* xmask, const uint64_t* zmask, const double* coeff,
+                         size_t n_terms, int n_qubits);
+
+// <bra|H|ket> (FP64 accumulation); result written to out[2] (host), stream synchronised.
+template <typename T>
+void transition(const vec2_t<T>* bra, const vec2_t<T>* ket, int n, const PauliTerms& terms,
+                cudaStream_t st, Workspace& ws, double out[2]);
+
+// out = H psi (gather form, no atomics)
+template <typename T>
+void apply_observable(const vec2_t<T>* psi, vec2_t<T>* out, int n, const PauliTerms& terms,
+                      cudaStream_t st, Workspace& ws);
+
+// sum |a|^2 (FP64)
+template <typename T>
+double norm2(const vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
+// <a|b> (FP64); A and B may differ in precision
+template <typename TA, typename TB>
+void inner(const vec2_t<TA>* a, const vec2_t<TB>* b, int n, cudaStream_t st, Workspace& ws,
+           double out[2]);
+template <typename T>
+void scale_real(vec2_t<T>* s, int n, double f, cudaStream_t st);
+
+// terminal sampling: u sorted ascending (device), out_idx (device) in the same order
+template <typename T>
+void sample_sorted(const vec2_t<T>* s, int n, const double* d_u_sorted, size_t n_shots,
+                   uint64_t* d_out, cudaStream_t st, Workspace& ws);
+
+// ---------------------------------------------------------------- adjoint (kern_reduce.cu)
+// One reverse step of a parametric gate of width k (0..2): with psi, phi the states after
+// the gate, accumulate ip = <phi| G |psi> into slot `slot` of the partials table, then apply
+// the 2^k x 2^k matrix D (the gate's dagger) to both states.
+struct AdjStep {
+    int k;
+    uint32_t qubits[2];
+    std::vector<c128> G;   // generator matrix (2^k x 2^k)
+    std::vector<c128> D;   // dagger matrix
+};
+template <typename T>
+void adjoint_param_step(vec2_t<T>* psi, vec2_t<T>* phi, int n, const AdjStep& step,
+                        double* d_partials, unsigned n_blocks, cudaStream_t st);
+unsigned adjoint_blocks(int n);
+// sum the partials of every slot: d_partials[slot * n_blocks + b] (complex) -> host out
+void reduce_slots(const double* d_partials, int n_slots, unsigned n_blocks, cudaStream_t st,
+                  Workspace& ws, std::vector<double>& out);
+
+}  // namespace qsv

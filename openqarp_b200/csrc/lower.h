@@ -1,0 +1,98 @@
+// lower.h — host side of the engine: packed-command decoding, gate unitaries, the
+// simulation-fusion passes, and lowering of commands to device operations.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace qsv {
+
+using c128 = std::complex<double>;
+
+// qarpx::GateType enumerator values (reference: src/qarpx/include/qarpx/core/gates.h:8-58)
+enum Gate : int {
+    X = 0, Y, Z, H, S, SDG, T, TDG, SX, SXDG, ID,
+    RX, RY, RZ, P, U,
+    CX, CY, CZ, SWAP, ECR, ISWAP, ISWAPDG,
+    CH, CS, CSDG, CSX, CSXDG,
+    CRX, CRY, CRZ, CP, RZZ, RXX, RYY,
+    CU, CCX, CSWAP, MCZ, GPHASE,
+    BARRIER, MEASURE, RESET, BRANCH_BEGIN, BRANCH_ELSE, BRANCH_END, CUSTOM, GATE_COUNT
+};
+
+// Error classes mirrored from the reference (status codes of include/qsv.h).
+struct capability_error : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+// A decoded concrete command (the byte form of qarpx::Command, command.h:29-110).
+struct Cmd {
+    int gate = BARRIER;
+    std::vector<uint32_t> q;
+    std::vector<uint32_t> cbits;
+    std::vector<double> p;
+    std::vector<c128> u;     // Custom: 2^k x 2^k row-major, local bit b <-> q[b]
+    int flags = 0;           // bit 0: classical condition
+    int n_gates = 1;         // source gates folded into this command (fusion statistics)
+};
+
+std::vector<Cmd> decode(const uint8_t* buf, size_t nbytes);
+
+// True for the commands statevector() rejects (qarp_simulator.cpp:260-270 needs_trajectory).
+bool needs_trajectory(const Cmd& c);
+
+// Unitary of one concrete command over its own qubits, local bit b <-> q[b], row-major,
+// obtained by lowering the command and applying the ops to basis columns on the host
+// (the reference builds local_unitary the same way from apply_command,
+// qarp_simulator.cpp:90-118, so the fused matrices can never drift from the dispatch).
+std::vector<c128> local_unitary(const Cmd& c);
+
+// Command::dagger (reference: src/qarpx/src/core/command.cpp:19-59).
+Cmd dagger(const Cmd& c);
+
+// fuse_for_simulation (reference: src/qarpx/src/simulator/fusion.cpp:120-268).
+std::vector<Cmd> fuse_blocks(const std::vector<Cmd>& in, int max_qubits);
+// fuse_single_qubit_gates (reference: src/qarpx/src/transpiler/fusion.cpp:196-300).
+std::vector<Cmd> fuse_single_qubit(const std::vector<Cmd>& in);
+// fuse_for_dispatch (reference: qarp_simulator.cpp:120-129).
+std::vector<Cmd> fuse_for_dispatch(const std::vector<Cmd>& in, int n_qubits, int max_qubits,
+                                   int min_qubits);
+
+// ---------------------------------------------------------------- device operations
+enum OpKind : int {
+    OP_NOP = 0,
+    OP_DENSE,       // k-qubit dense matrix (k = 1..8) on qubits[0..k)
+    OP_DIAG,        // k-qubit diagonal, m[l] for local index l
+    OP_CTRL1,       // 2x2 on `target` where (i & mask) == mask
+    OP_PHASE,       // i -> m[0] * i where (i & mask) == mask
+    OP_SWAP,        // swap qubits[0], qubits[1]
+    OP_PAULI_ROT,   // exp(-i theta/2 P), P by (mask = X|Y bits, zmask = Z|Y bits); m[0] = (cos, sin)
+    OP_SCALE,       // every amplitude times m[0]
+};
+
+struct Op {
+    OpKind kind = OP_NOP;
+    int k = 0;
+    uint32_t qubits[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t mask = 0, zmask = 0;
+    int target = 0;
+    std::vector<c128> m;
+    int n_gates = 1;
+};
+
+// Lower one concrete command to device ops (empty for no-ops).
+std::vector<Op> lower(const Cmd& c, int n_qubits);
+
+// Apply an op to a host register (local_unitary's column builder; small registers only).
+void apply_op_host(const Op& op, c128* s, int n_qubits);
+
+// Generator of a parametric gate for the adjoint sweep (apply_generator,
+// qarp_simulator.cpp:1352-1418), as a local operator on the gate's qubits:
+// M = prefactor * G with G given as a 2^k x 2^k matrix (k = gate width).  Returns false
+// when the gate has no generator rule.
+bool generator(const Cmd& c, c128* prefactor, std::vector<c128>* G, int* k);
+
+}  // namespace qsv

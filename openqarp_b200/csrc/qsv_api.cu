@@ -1,0 +1,614 @@
+// qsv_api.cu — the extern "C" boundary declared in include/qsv.h.
+//
+// A handle owns one register in HBM, one CUDA stream and a workspace.  Every entry point
+// translates C++ exceptions into the status codes of qsv.h (the reference's exception
+// classes, src/qarpx/python/bindings.cpp:272-290) and never lets one cross the ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/qsv.h"
+#include "kernels.h"
+#include "lower.h"
+
+namespace qsv {
+namespace {
+
+thread_local std::string g_err;
+
+struct Handle {
+    int n = 0;
+    int dtype = QSV_C128;
+    int device = 0;
+    void* state = nullptr;
+    cudaStream_t stream = nullptr;
+    Workspace ws;
+    int fusion_max = 3;
+    int fusion_min = 12;
+    int executor = -1;
+    qsv_stats_t stats{};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    void* aux = nullptr;          // second register (adjoint's |phi>)
+    size_t aux_cap = 0;
+    uint64_t dim() const { return 1ull << n; }
+    size_t amp_bytes() const { return dtype == QSV_C128 ? 16 : 8; }
+};
+
+// QARP_FUSION_MAX_QUBITS, read once per process (qarp_simulator.cpp:47-63): a value that
+// does not parse or exceeds the maximum width is ignored.
+int default_fusion_max() {
+    static const int k = [] {
+        if (const char* env = std::getenv("QARP_FUSION_MAX_QUBITS")) {
+            char* end = nullptr;
+            const long v = std::strtol(env, &end, 10);
+            if (end != env && *end == '\0' && v >= 0 && v <= QSV_MAX_BLOCK_QUBITS)
+                return static_cast<int>(v);
+        }
+        return 3;
+    }();
+    return k;
+}
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        g_err.clear();
+        f();
+        return QSV_OK;
+    } catch (const capability_error& e) {
+        return fail(QSV_ECAPABILITY, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(QSV_EINVAL, e.what());
+    } catch (const cuda_error& e) {
+        return fail(QSV_ECUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(QSV_ENOMEM, "device or host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(QSV_ERUNTIME, e.what());
+    } catch (...) {
+        return fail(QSV_ERUNTIME, "unknown error");
+    }
+}
+
+Handle* H_(void* h) {
+    if (!h) throw std::invalid_argument("null handle");
+    Handle* p = static_cast<Handle*>(h);
+    check_cuda(cudaSetDevice(p->device), "cudaSetDevice");
+    return p;
+}
+
+double2* S128(Handle* h) { return static_cast<double2*>(h->state); }
+float2* S64(Handle* h) { return static_cast<float2*>(h->state); }
+
+void* aux_state(Handle* h) {
+    const size_t bytes = h->dim() * h->amp_bytes();
+    if (h->aux && h->aux_cap >= bytes) return h->aux;
+    if (h->aux) cudaFree(h->aux);
+    h->aux = nullptr;
+    h->aux_cap = 0;
+    if (cudaMalloc(&h->aux, bytes) != cudaSuccess) {
+        h->aux = nullptr;
+        throw std::bad_alloc();
+    }
+    h->aux_cap = bytes;
+    return h->aux;
+}
+
+void launch(Handle* h, const Op& op, void* target) {
+    if (h->dtype == QSV_C128)
+        launch_op<double>(op, static_cast<double2*>(target), h->n, h->stream, h->ws);
+    else
+        launch_op<float>(op, static_cast<float2*>(target), h->n, h->stream, h->ws);
+    check_cuda(cudaGetLastError(), "gate launch");
+    if (op.kind != OP_NOP) {
+        h->stats.launches++;
+        h->stats.passes++;
+        h->stats.hbm_bytes += op_bytes(op, h->n, static_cast<int>(h->amp_bytes()));
+        if (op.kind == OP_DENSE && op.k >= 2) h->stats.fused_blocks++;
+    }
+}
+
+void check_stream(const std::vector<Cmd>& cmds) {
+    for (const Cmd& c : cmds) {
+        if (c.gate == RESET || (c.flags & 1) || c.gate == BRANCH_BEGIN || c.gate == BRANCH_ELSE ||
+            c.gate == BRANCH_END)
+            throw std::runtime_error(
+                "circuit contains Reset, a classical condition or a branch marker: "
+                "no single statevector (use a trajectory simulator)");
+    }
+}
+
+void apply_stream(Handle* h, const uint8_t* buf, size_t nbytes, bool fuse) {
+    std::vector<Cmd> cmds = decode(buf, nbytes);
+    check_stream(cmds);
+    if (fuse) cmds = fuse_for_dispatch(cmds, h->n, h->fusion_max, h->fusion_min);
+    std::vector<Op> ops;
+    ops.reserve(cmds.size());
+    for (const Cmd& c : cmds)
+        for (Op& o : lower(c, h->n)) ops.push_back(std::move(o));
+    check_cuda(cudaEventRecord(h->e0, h->stream), "event");
+    for (const Op& o : ops) launch(h, o, h->state);
+    check_cuda(cudaEventRecord(h->e1, h->stream), "event");
+}
+
+PauliTerms terms_of(Handle* h, const uint64_t* xm, const uint64_t* zm, const double* coeff,
+                    size_t nt) {
+    if (nt && (!xm || !zm || !coeff)) throw std::invalid_argument("null observable arrays");
+    return prepare_terms(xm, zm, coeff, nt, h->n);
+}
+
+void to_device_c128(Handle* h, void* dst, const double* amps) {
+    const uint64_t dim = h->dim();
+    if (h->dtype == QSV_C128) {
+        check_cuda(cudaMemcpyAsync(dst, amps, dim * 16, cudaMemcpyHostToDevice, h->stream), "H2D");
+        check_cuda(cudaStreamSynchronize(h->stream), "H2D");
+        return;
+    }
+    // complex64 register: convert in host chunks
+    const size_t chunk = 1u << 20;
+    std::vector<float> tmp(2 * chunk);
+    for (uint64_t o = 0; o < dim; o += chunk) {
+        const uint64_t m = std::min<uint64_t>(chunk, dim - o);
+        for (uint64_t i = 0; i < 2 * m; ++i) tmp[i] = static_cast<float>(amps[2 * o + i]);
+        check_cuda(cudaMemcpyAsync(static_cast<float2*>(dst) + o, tmp.data(), m * 8,
+                                   cudaMemcpyHostToDevice, h->stream), "H2D");
+        check_cuda(cudaStreamSynchronize(h->stream), "H2D");
+    }
+}
+
+}  // namespace
+}  // namespace qsv
+
+using namespace qsv;
+
+extern "C" {
+
+const char* qsv_last_error(void) { return g_err.c_str(); }
+int qsv_abi_version(void) { return 1; }
+
+int qsv_create(int n_qubits, int dtype, int device, void** out) {
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("null output handle");
+        *out = nullptr;
+        if (n_qubits < 0 || n_qubits > QSV_MAX_QUBITS)
+            throw std::invalid_argument("n_qubits must be in [0, " + std::to_string(QSV_MAX_QUBITS) +
+                                        "], got " + std::to_string(n_qubits));
+        if (dtype != QSV_C128 && dtype != QSV_C64) throw std::invalid_argument("dtype must be QSV_C128 or QSV_C64");
+        int n_dev = 0;
+        check_cuda(cudaGetDeviceCount(&n_dev), "cudaGetDeviceCount");
+        if (device < 0 || device >= n_dev) throw std::invalid_argument("no such CUDA device");
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        auto* h = new Handle();
+        h->n = n_qubits;
+        h->dtype = dtype;
+        h->device = device;
+        h->fusion_max = default_fusion_max();
+        try {
+            check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+            check_cuda(cudaEventCreate(&h->e0), "event");
+            check_cuda(cudaEventCreate(&h->e1), "event");
+            if (cudaMalloc(&h->state, h->dim() * h->amp_bytes()) != cudaSuccess) {
+                h->state = nullptr;
+                cudaGetLastError();
+                throw std::bad_alloc();
+            }
+            check_cuda(cudaMemsetAsync(h->state, 0, h->dim() * h->amp_bytes(), h->stream), "memset");
+            const double one[2] = {1.0, 0.0};
+            const float onef[2] = {1.0f, 0.0f};
+            check_cuda(cudaMemcpyAsync(h->state, dtype == QSV_C128 ? static_cast<const void*>(one) : onef,
+                                       h->amp_bytes(), cudaMemcpyHostToDevice, h->stream), "init");
+            check_cuda(cudaStreamSynchronize(h->stream), "init");
+        } catch (...) {
+            if (h->state) cudaFree(h->state);
+            if (h->stream) cudaStreamDestroy(h->stream);
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int qsv_destroy(void* hp) {
+    return guarded([&] {
+        if (!hp) return;
+        Handle* h = static_cast<Handle*>(hp);
+        cudaSetDevice(h->device);
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        h->ws.release();
+        if (h->state) cudaFree(h->state);
+        if (h->aux) cudaFree(h->aux);
+        if (h->e0) cudaEventDestroy(h->e0);
+        if (h->e1) cudaEventDestroy(h->e1);
+        if (h->stream) cudaStreamDestroy(h->stream);
+        delete h;
+    });
+}
+
+int qsv_set_fusion(void* hp, int max_q, int min_q) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (max_q < 0 || max_q > QSV_MAX_BLOCK_QUBITS)
+            throw std::invalid_argument("QarpSimulator::set_fusion_max_qubits: " + std::to_string(max_q) +
+                                        " exceeds the maximum block width " +
+                                        std::to_string(QSV_MAX_BLOCK_QUBITS));
+        if (min_q < 0) throw std::invalid_argument("fusion_min_qubits must be >= 0");
+        h->fusion_max = max_q;
+        h->fusion_min = min_q;
+    });
+}
+
+int qsv_set_executor(void* hp, int mode) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (mode < -1 || mode > 1) throw std::invalid_argument("executor mode must be -1, 0 or 1");
+        h->executor = mode;
+    });
+}
+
+int qsv_reset(void* hp) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        check_cuda(cudaMemsetAsync(h->state, 0, h->dim() * h->amp_bytes(), h->stream), "memset");
+        const double one[2] = {1.0, 0.0};
+        const float onef[2] = {1.0f, 0.0f};
+        check_cuda(cudaMemcpyAsync(h->state, h->dtype == QSV_C128 ? static_cast<const void*>(one) : onef,
+                                   h->amp_bytes(), cudaMemcpyHostToDevice, h->stream), "init");
+        check_cuda(cudaStreamSynchronize(h->stream), "init");
+    });
+}
+
+int qsv_set_state(void* hp, const double* amps, uint64_t len, int validate) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!amps) throw std::invalid_argument("null amplitudes");
+        if (len != h->dim())
+            throw std::invalid_argument("initial_state length " + std::to_string(len) +
+                                        " != 2^n_qubits = " + std::to_string(h->dim()));
+        if (validate) {
+            double norm2 = 0;
+            for (uint64_t i = 0; i < 2 * len; ++i) norm2 += amps[i] * amps[i];
+            if (std::abs(std::sqrt(norm2) - 1.0) > 1e-10)
+                throw std::invalid_argument("initial_state is not normalised: |psi| = " +
+                                            std::to_string(std::sqrt(norm2)) +
+                                            " differs from 1 by more than 1e-10");
+        }
+        to_device_c128(h, h->state, amps);
+    });
+}
+
+int qsv_get_state(void* hp, double* amps, uint64_t len) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!amps) throw std::invalid_argument("null output buffer");
+        if (len != h->dim()) throw std::invalid_argument("output length != 2^n_qubits");
+        if (h->dtype == QSV_C128) {
+            check_cuda(cudaMemcpyAsync(amps, h->state, h->dim() * 16, cudaMemcpyDeviceToHost, h->stream), "D2H");
+            check_cuda(cudaStreamSynchronize(h->stream), "D2H");
+            return;
+        }
+        const size_t chunk = 1u << 20;
+        std::vector<float> tmp(2 * chunk);
+        for (uint64_t o = 0; o < h->dim(); o += chunk) {
+            const uint64_t m = std::min<uint64_t>(chunk, h->dim() - o);
+            check_cuda(cudaMemcpyAsync(tmp.data(), S64(h) + o, m * 8, cudaMemcpyDeviceToHost, h->stream), "D2H");
+            check_cuda(cudaStreamSynchronize(h->stream), "D2H");
+            for (uint64_t i = 0; i < 2 * m; ++i) amps[2 * o + i] = tmp[i];
+        }
+    });
+}
+
+int qsv_device_state(void* hp, void** dptr, void** stream) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (dptr) *dptr = h->state;
+        if (stream) *stream = h->stream;
+    });
+}
+
+int qsv_copy_state(void* dp, const void* sp) {
+    return guarded([&] {
+        Handle* d = H_(dp);
+        const Handle* s = static_cast<const Handle*>(sp);
+        if (!s) throw std::invalid_argument("null source handle");
+        if (s->n != d->n || s->dtype != d->dtype) throw std::invalid_argument("registers differ in width or dtype");
+        check_cuda(cudaStreamSynchronize(s->stream), "source sync");
+        check_cuda(cudaMemcpyAsync(d->state, s->state, d->dim() * d->amp_bytes(), cudaMemcpyDeviceToDevice,
+                                   d->stream), "D2D");
+    });
+}
+
+int qsv_fuse_count(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min_q, int32_t* n_out,
+                   int32_t* widths_hist) {
+    return guarded([&] {
+        if (!n_out) throw std::invalid_argument("null output");
+        if (max_q < 0 || max_q > QSV_MAX_BLOCK_QUBITS) throw std::invalid_argument("fusion width out of range");
+        const std::vector<Cmd> fused = fuse_for_dispatch(decode(cmds, nbytes), n, max_q, min_q);
+        *n_out = static_cast<int32_t>(fused.size());
+        if (widths_hist) {
+            for (int k = 0; k <= QSV_MAX_BLOCK_QUBITS; ++k) widths_hist[k] = 0;
+            for (const Cmd& c : fused)
+                if (c.gate == CUSTOM && c.q.size() <= QSV_MAX_BLOCK_QUBITS) widths_hist[c.q.size()]++;
+        }
+    });
+}
+
+int qsv_apply(void* hp, const uint8_t* cmds, size_t nbytes) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!cmds && nbytes) throw std::invalid_argument("null command buffer");
+        apply_stream(h, cmds, nbytes, true);
+    });
+}
+
+int qsv_apply_unfused(void* hp, const uint8_t* cmds, size_t nbytes) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!cmds && nbytes) throw std::invalid_argument("null command buffer");
+        apply_stream(h, cmds, nbytes, false);
+    });
+}
+
+int qsv_transition(void* bp, void* kp, const uint64_t* xm, const uint64_t* zm, const double* coeff,
+                   size_t nt, double out[2]) {
+    return guarded([&] {
+        Handle* b = H_(bp);
+        Handle* k = static_cast<Handle*>(kp);
+        if (!k || !out) throw std::invalid_argument("null argument");
+        if (b->n != k->n || b->dtype != k->dtype) throw std::invalid_argument("bra and ket registers differ");
+        const PauliTerms t = terms_of(k, xm, zm, coeff, nt);
+        if (b != k) check_cuda(cudaStreamSynchronize(b->stream), "bra sync");
+        if (k->dtype == QSV_C128) transition<double>(S128(b), S128(k), k->n, t, k->stream, k->ws, out);
+        else transition<float>(S64(b), S64(k), k->n, t, k->stream, k->ws, out);
+        k->stats.launches += 2;
+    });
+}
+
+int qsv_uniforms(uint32_t seed, size_t n_shots, double* u) {
+    return guarded([&] {
+        if (!u && n_shots) throw std::invalid_argument("null output");
+        std::mt19937 rng(seed);
+        for (size_t s = 0; s < n_shots; ++s)
+            u[s] = std::generate_canonical<double, std::numeric_limits<double>::digits>(rng);
+    });
+}
+
+int qsv_sample(void* hp, const double* u, size_t n_shots, uint64_t* out) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (n_shots == 0) return;
+        if (!u || !out) throw std::invalid_argument("null argument");
+        std::vector<size_t> perm(n_shots);
+        std::iota(perm.begin(), perm.end(), size_t{0});
+        std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) { return u[a] < u[b]; });
+        std::vector<double> us(n_shots);
+        for (size_t s = 0; s < n_shots; ++s) us[s] = u[perm[s]];
+        uint8_t* dev = static_cast<uint8_t*>(h->ws.shots(n_shots * 16));
+        double* d_u = reinterpret_cast<double*>(dev);
+        uint64_t* d_out = reinterpret_cast<uint64_t*>(dev + n_shots * 8);
+        check_cuda(cudaMemcpyAsync(d_u, us.data(), n_shots * 8, cudaMemcpyHostToDevice, h->stream), "shots H2D");
+        if (h->dtype == QSV_C128) sample_sorted<double>(S128(h), h->n, d_u, n_shots, d_out, h->stream, h->ws);
+        else sample_sorted<float>(S64(h), h->n, d_u, n_shots, d_out, h->stream, h->ws);
+        std::vector<uint64_t> idx(n_shots);
+        check_cuda(cudaMemcpyAsync(idx.data(), d_out, n_shots * 8, cudaMemcpyDeviceToHost, h->stream), "shots D2H");
+        check_cuda(cudaStreamSynchronize(h->stream), "sampling");
+        for (size_t s = 0; s < n_shots; ++s) out[perm[s]] = idx[s];
+        h->stats.launches += 5;
+    });
+}
+
+int qsv_sample_seeded(void* hp, uint32_t seed, size_t n_shots, uint64_t* out) {
+    std::vector<double> u(n_shots);
+    int rc = qsv_uniforms(seed, n_shots, u.data());
+    if (rc) return rc;
+    return qsv_sample(hp, u.data(), n_shots, out);
+}
+
+int qsv_norm2(void* hp, double* out) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!out) throw std::invalid_argument("null output");
+        *out = h->dtype == QSV_C128 ? norm2<double>(S128(h), h->n, h->stream, h->ws)
+                                    : norm2<float>(S64(h), h->n, h->stream, h->ws);
+    });
+}
+
+int qsv_scale(void* hp, double f) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (h->dtype == QSV_C128) scale_real<double>(S128(h), h->n, f, h->stream);
+        else scale_real<float>(S64(h), h->n, f, h->stream);
+    });
+}
+
+int qsv_inner(void* ap, void* bp, double out[2]) {
+    return guarded([&] {
+        Handle* a = H_(ap);
+        Handle* b = static_cast<Handle*>(bp);
+        if (!b || !out) throw std::invalid_argument("null argument");
+        if (a->n != b->n) throw std::invalid_argument("registers differ in width");
+        if (a->device != b->device) throw std::invalid_argument("registers live on different devices");
+        check_cuda(cudaStreamSynchronize(b->stream), "sync");
+        if (a->dtype == QSV_C128 && b->dtype == QSV_C128) inner<double, double>(S128(a), S128(b), a->n, a->stream, a->ws, out);
+        else if (a->dtype == QSV_C64 && b->dtype == QSV_C64) inner<float, float>(S64(a), S64(b), a->n, a->stream, a->ws, out);
+        else if (a->dtype == QSV_C64) inner<float, double>(S64(a), S128(b), a->n, a->stream, a->ws, out);
+        else inner<double, float>(S128(a), S64(b), a->n, a->stream, a->ws, out);
+    });
+}
+
+int qsv_synchronize(void* hp) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        check_cuda(cudaStreamSynchronize(h->stream), "synchronize");
+    });
+}
+
+int qsv_stats(void* hp, qsv_stats_t* out) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!out) throw std::invalid_argument("null output");
+        float ms = 0;
+        if (cudaEventQuery(h->e1) == cudaSuccess && cudaEventElapsedTime(&ms, h->e0, h->e1) == cudaSuccess)
+            h->stats.last_apply_ms = ms;
+        cudaGetLastError();
+        *out = h->stats;
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- adjoint
+
+namespace qsv {
+namespace {
+
+struct DepTable {
+    const int32_t* ptr;
+    const int32_t* param;
+    const double* alpha;
+    int n_params;
+};
+
+template <typename T>
+void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps, vec2_t<T>* psi,
+                   vec2_t<T>* phi, double* grad) {
+    const int n = h->n;
+    // count parametric steps, build them
+    struct Slot { size_t cmd; c128 pref; };
+    std::vector<Slot> slots;
+    const unsigned nb = adjoint_blocks(n);
+    size_t n_param_steps = 0;
+    for (size_t i = 0; i < cmds.size(); ++i)
+        if (deps.ptr[i + 1] > deps.ptr[i]) ++n_param_steps;
+    double* partials = static_cast<double*>(
+        h->ws.scratch((n_param_steps * nb + n_param_steps + 1) * 2 * sizeof(double)));
+    for (size_t idx = cmds.size(); idx-- > 0;) {
+        const Cmd& c = cmds[idx];
+        const Cmd d = dagger(c);
+        if (deps.ptr[idx + 1] > deps.ptr[idx]) {
+            AdjStep st;
+            c128 pref;
+            if (!generator(c, &pref, &st.G, &st.k))
+                throw capability_error(
+                    "run_gradient: gate '" + std::to_string(c.gate) +
+                    "' carries a symbolic parameter but has no adjoint generator rule "
+                    "(Rx/Ry/Rz/P/GPhase/CRx/CRy/CRz/CP/RXX/RYY/RZZ); rebase it to those gates "
+                    "before differentiating.");
+            st.qubits[0] = st.k > 0 ? c.q[0] : 0;
+            st.qubits[1] = st.k > 1 ? c.q[1] : 0;
+            for (int b = 0; b < st.k; ++b)
+                if (static_cast<int>(c.q[b]) >= n) throw std::invalid_argument("gate qubit outside the register");
+            if (st.k == 0) {
+                const double th = -c.p.at(0);
+                st.D = {c128(std::cos(th), std::sin(th))};
+            } else {
+                st.D = local_unitary(d);
+            }
+            adjoint_param_step<T>(psi, phi, n, st, partials + 2 * slots.size() * nb, nb, h->stream);
+            h->stats.launches++;
+            h->stats.passes++;
+            h->stats.hbm_bytes += 4ull * h->dim() * h->amp_bytes();
+            slots.push_back({idx, pref});
+        } else {
+            for (const Op& o : lower(d, n)) {
+                launch(h, o, psi);
+                launch(h, o, phi);
+            }
+        }
+    }
+    std::vector<double> ips;
+    reduce_slots(partials, static_cast<int>(slots.size()), nb, h->stream, h->ws, ips);
+    for (int p = 0; p < deps.n_params; ++p) grad[p] = 0.0;
+    for (size_t s = 0; s < slots.size(); ++s) {
+        const c128 ip(ips[2 * s], ips[2 * s + 1]);
+        const double base = 2.0 * std::real(slots[s].pref * ip);
+        const size_t i = slots[s].cmd;
+        for (int d = deps.ptr[i]; d < deps.ptr[i + 1]; ++d) grad[deps.param[d]] += deps.alpha[d] * base;
+    }
+}
+
+std::vector<Cmd> checked_adjoint_stream(const uint8_t* cmds, size_t nbytes, const int32_t* dep_ptr,
+                                        const int32_t* dep_param, int n_params, int n) {
+    std::vector<Cmd> cs = decode(cmds, nbytes);
+    for (const Cmd& c : cs)
+        if (needs_trajectory(c))
+            throw std::runtime_error(
+                "QarpSimulator::run_gradient: trajectory commands (Measure / Reset / classical "
+                "condition) are not differentiable.");
+    if (!dep_ptr) throw std::invalid_argument("null dependency table");
+    if (dep_ptr[0] != 0) throw std::invalid_argument("dep_ptr[0] must be 0");
+    for (size_t i = 0; i < cs.size(); ++i) {
+        if (dep_ptr[i + 1] < dep_ptr[i]) throw std::invalid_argument("dep_ptr must be non-decreasing");
+        for (int d = dep_ptr[i]; d < dep_ptr[i + 1]; ++d)
+            if (dep_param[d] < 0 || dep_param[d] >= n_params)
+                throw std::invalid_argument("dependency names a parameter outside [0, n_params)");
+        for (uint32_t q : cs[i].q)
+            if (static_cast<int>(q) >= n) throw std::invalid_argument("command acts on a qubit outside the register");
+    }
+    return cs;
+}
+
+}  // namespace
+}  // namespace qsv
+
+extern "C" {
+
+int qsv_adjoint(void* hp, const uint8_t* cmds, size_t nbytes, const int32_t* dep_ptr,
+                const int32_t* dep_param, const double* dep_alpha, int n_params, const uint64_t* xm,
+                const uint64_t* zm, const double* coeff, size_t nt, double* grad, double* energy) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (n_params < 0 || (n_params > 0 && !grad)) throw std::invalid_argument("bad gradient output");
+        const std::vector<Cmd> cs = checked_adjoint_stream(cmds, nbytes, dep_ptr, dep_param, n_params, h->n);
+        const PauliTerms t = terms_of(h, xm, zm, coeff, nt);
+        // forward sweep (fused: the reverse sweep below walks the unfused stream)
+        apply_stream(h, cmds, nbytes, true);
+        void* phi = aux_state(h);
+        DepTable deps{dep_ptr, dep_param, dep_alpha, n_params};
+        if (h->dtype == QSV_C128) {
+            apply_observable<double>(S128(h), static_cast<double2*>(phi), h->n, t, h->stream, h->ws);
+            if (energy) {
+                double e[2];
+                inner<double, double>(S128(h), static_cast<double2*>(phi), h->n, h->stream, h->ws, e);
+                *energy = e[0];
+            }
+            adjoint_sweep<double>(h, cs, deps, S128(h), static_cast<double2*>(phi), grad);
+        } else {
+            apply_observable<float>(S64(h), static_cast<float2*>(phi), h->n, t, h->stream, h->ws);
+            if (energy) {
+                double e[2];
+                inner<float, float>(S64(h), static_cast<float2*>(phi), h->n, h->stream, h->ws, e);
+                *energy = e[0];
+            }
+            adjoint_sweep<float>(h, cs, deps, S64(h), static_cast<float2*>(phi), grad);
+        }
+    });
+}
+
+int qsv_adjoint_phi(void* hp, const uint8_t* cmds, size_t nbytes, const int32_t* dep_ptr,
+                    const int32_t* dep_param, const double* dep_alpha, int n_params,
+                    const double* phi_host, double* grad) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!phi_host) throw std::invalid_argument("null phi");
+        if (n_params < 0 || (n_params > 0 && !grad)) throw std::invalid_argument("bad gradient output");
+        const std::vector<Cmd> cs = checked_adjoint_stream(cmds, nbytes, dep_ptr, dep_param, n_params, h->n);
+        apply_stream(h, cmds, nbytes, true);
+        void* phi = aux_state(h);
+        to_device_c128(h, phi, phi_host);
+        DepTable deps{dep_ptr, dep_param, dep_alpha, n_params};
+        if (h->dtype == QSV_C128) adjoint_sweep<double>(h, cs, deps, S128(h), static_cast<double2*>(phi), grad);
+        else adjoint_sweep<float>(h, cs, deps, S64(h), static_cast<float2*>(phi), grad);
+    });
+}
+
+}  // extern "C"

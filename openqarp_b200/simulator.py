@@ -1,0 +1,474 @@
+"""The B200 statevector simulator: the object a QarpEngine holds as ``self._sim``.
+
+``B200Simulator`` presents the duck-typed surface the reference's engines and primitives
+call on ``qx.QarpSimulator`` (reference: src/qarpx/python/bindings.cpp:1336-1513;
+src/qarpx/include/qarpx/simulator/qarp_simulator.h:31-284) — same method names, argument
+order, return types and exception classes — and runs every call on the GPU through
+libqsv.so.  ``Register`` is the lower-level handle: one device-resident register and one
+CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Mapping, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, i32ptr, lib, u64ptr, u8ptr
+from .errors import CapabilityError
+from .ir import (PackedStream, cbit_register_width, measurements_are_terminal, needs_trajectory,
+                 pack)
+from .observable import PauliMasks, to_masks
+
+MAX_QUBITS = 34
+MAX_BLOCK_QUBITS = 8
+_DTYPES = {"complex128": _lib.QSV_C128, "c128": _lib.QSV_C128,
+           "complex64": _lib.QSV_C64, "c64": _lib.QSV_C64}
+
+
+def _as_bytes(stream) -> bytes:
+    return stream.buf if isinstance(stream, PackedStream) else bytes(stream)
+
+
+class Register:
+    """One 2^n register in HBM with its own CUDA stream (a libqsv handle)."""
+
+    def __init__(self, n_qubits: int, dtype: str = "complex128", device: int = 0):
+        if dtype not in _DTYPES:
+            raise ValueError(f"dtype must be one of {sorted(_DTYPES)}")
+        self.n = int(n_qubits)
+        self.dtype = "complex128" if _DTYPES[dtype] == _lib.QSV_C128 else "complex64"
+        self.device = int(device)
+        h = ctypes.c_void_p()
+        check(lib.qsv_create(self.n, _DTYPES[dtype], self.device, ctypes.byref(h)))
+        self._h = h
+
+    # lifecycle -----------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.qsv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("register is closed")
+        return self._h
+
+    @property
+    def dim(self) -> int:
+        return 1 << self.n
+
+    # state ---------------------------------------------------------------------------
+    def reset(self):
+        check(lib.qsv_reset(self.handle))
+
+    def set_state(self, amps, validate: bool = True):
+        a = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128).reshape(-1))
+        check(lib.qsv_set_state(self.handle, dptr(a.view(np.float64)), a.shape[0], 1 if validate else 0))
+
+    def get_state(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Copy the register to host memory (into ``out`` when given, e.g. a pinned buffer)."""
+        if out is None:
+            out = np.empty(self.dim, dtype=np.complex128)
+        elif out.dtype != np.complex128 or out.shape != (self.dim,) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous complex128 array of length 2^n")
+        check(lib.qsv_get_state(self.handle, dptr(out.view(np.float64)), self.dim))
+        return out
+
+    def device_pointer(self) -> tuple[int, int]:
+        p, s = ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib.qsv_device_state(self.handle, ctypes.byref(p), ctypes.byref(s)))
+        return p.value or 0, s.value or 0
+
+    def copy_from(self, other: "Register"):
+        check(lib.qsv_copy_state(self.handle, other.handle))
+
+    def configure(self, fusion_max: int, fusion_min: int, executor: int = -1):
+        check(lib.qsv_set_fusion(self.handle, int(fusion_max), int(fusion_min)))
+        check(lib.qsv_set_executor(self.handle, int(executor)))
+
+    # gates ---------------------------------------------------------------------------
+    def apply(self, stream, fused: bool = True):
+        b = _as_bytes(stream)
+        fn = lib.qsv_apply if fused else lib.qsv_apply_unfused
+        check(fn(self.handle, u8ptr(b), len(b)))
+
+    # reductions ----------------------------------------------------------------------
+    def transition(self, ket: "Register", masks: PauliMasks) -> complex:
+        out = np.zeros(2)
+        check(lib.qsv_transition(self.handle, ket.handle, u64ptr(masks.x), u64ptr(masks.z),
+                                 dptr(masks.coeff), masks.n_terms, dptr(out)))
+        return complex(out[0], out[1])
+
+    def expectation(self, masks: PauliMasks) -> complex:
+        return self.transition(self, masks)
+
+    def norm2(self) -> float:
+        out = ctypes.c_double()
+        check(lib.qsv_norm2(self.handle, ctypes.byref(out)))
+        return out.value
+
+    def scale(self, f: float):
+        check(lib.qsv_scale(self.handle, float(f)))
+
+    def inner(self, other: "Register") -> complex:
+        out = np.zeros(2)
+        check(lib.qsv_inner(self.handle, other.handle, dptr(out)))
+        return complex(out[0], out[1])
+
+    def synchronize(self):
+        check(lib.qsv_synchronize(self.handle))
+
+    def stats(self) -> dict:
+        s = _lib.Stats()
+        check(lib.qsv_stats(self.handle, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _lib.Stats._fields_}
+
+    # sampling ------------------------------------------------------------------------
+    def sample(self, u: np.ndarray) -> np.ndarray:
+        u = np.ascontiguousarray(np.asarray(u, dtype=np.float64))
+        out = np.empty(u.shape[0], dtype=np.uint64)
+        check(lib.qsv_sample(self.handle, dptr(u), u.shape[0], u64ptr(out)))
+        return out
+
+    def sample_seeded(self, seed: int, n_shots: int) -> np.ndarray:
+        out = np.empty(int(n_shots), dtype=np.uint64)
+        check(lib.qsv_sample_seeded(self.handle, int(seed) & 0xFFFFFFFF, int(n_shots), u64ptr(out)))
+        return out
+
+    # adjoint -------------------------------------------------------------------------
+    def adjoint(self, stream: PackedStream, n_params: int, masks: PauliMasks):
+        grad = np.zeros(max(n_params, 1))
+        energy = ctypes.c_double()
+        b = stream.buf
+        check(lib.qsv_adjoint(self.handle, u8ptr(b), len(b), i32ptr(stream.dep_ptr),
+                              i32ptr(stream.dep_param), dptr(stream.dep_alpha), int(n_params),
+                              u64ptr(masks.x), u64ptr(masks.z), dptr(masks.coeff), masks.n_terms,
+                              dptr(grad), ctypes.byref(energy)))
+        return energy.value, grad[:n_params]
+
+    def adjoint_phi(self, stream: PackedStream, n_params: int, phi) -> np.ndarray:
+        grad = np.zeros(max(n_params, 1))
+        p = np.ascontiguousarray(np.asarray(phi, dtype=np.complex128).reshape(-1))
+        if p.shape[0] != self.dim:
+            raise RuntimeError("run_gradient: |phi> size mismatch (expected 2^n_qubits)")
+        b = stream.buf
+        check(lib.qsv_adjoint_phi(self.handle, u8ptr(b), len(b), i32ptr(stream.dep_ptr),
+                                  i32ptr(stream.dep_param), dptr(stream.dep_alpha), int(n_params),
+                                  dptr(p.view(np.float64)), dptr(grad)))
+        return grad[:n_params]
+
+
+def uniforms(seed: int, n_shots: int) -> np.ndarray:
+    """The uniforms the reference's sampler draws: std::generate_canonical<double, 53> over
+    std::mt19937(seed) (sample_terminal, qarp_simulator.cpp:751-783)."""
+    u = np.empty(int(n_shots), dtype=np.float64)
+    check(lib.qsv_uniforms(int(seed) & 0xFFFFFFFF, int(n_shots), dptr(u)))
+    return u
+
+
+class SamplingResult:
+    """Outcome counts of one execution (reference: src/qarpx/include/qarpx/simulator/
+    sampling_result.h:14-38).  Keys are LSB-first integers (bit 0 = qubit 0)."""
+
+    def __init__(self, n_qubits: int, n_shots: int):
+        self.n_qubits = n_qubits
+        self.n_shots = n_shots
+        self.counts: dict[int, int] = {}
+        self.n_cbits = 0
+        self.cbit_history: list[list[bool]] = []
+        self.statevector: list = []
+        self.outcomes: Optional[np.ndarray] = None   # per-shot sampled index (extension)
+
+    def probability(self, outcome: int) -> float:
+        return self.counts.get(int(outcome), 0) / self.n_shots if self.n_shots else 0.0
+
+    def __repr__(self):
+        return f"SamplingResult(n_qubits={self.n_qubits}, n_shots={self.n_shots}, counts={len(self.counts)} outcomes)"
+
+
+def _default_fusion_max() -> int:
+    env = os.environ.get("QARP_FUSION_MAX_QUBITS")
+    if env is not None:
+        try:
+            v = int(env)
+            if 0 <= v <= MAX_BLOCK_QUBITS:
+                return v
+        except ValueError:
+            pass
+    return 3
+
+
+class B200Simulator:
+    """GPU drop-in for ``qx.QarpSimulator``.
+
+    Args:
+        noise_model: accepted for signature parity; an enabled noise model needs the
+            trajectory path, which this engine does not provide (CapabilityError).
+        device: CUDA device index.
+        dtype: ``"complex128"`` (default; the reference's arithmetic) or ``"complex64"``
+            (bulk mode: complex64 storage, FP64 reductions).
+    """
+
+    kMaxCustomQubits = MAX_BLOCK_QUBITS
+    kMaxFusionQubits = MAX_BLOCK_QUBITS
+    kDefaultFusionQubits = 3
+    kDefaultFusionMinQubits = 12
+
+    def __init__(self, noise_model=None, *, device: int = 0, dtype: str = "complex128"):
+        if noise_model is not None and getattr(noise_model, "enabled", True):
+            raise CapabilityError("B200Simulator: active noise needs the per-shot trajectory path, "
+                                  "which the B200 engine does not implement")
+        if dtype not in _DTYPES:
+            raise ValueError(f"dtype must be one of {sorted(_DTYPES)}")
+        self._noise_model = noise_model
+        self.device = int(device)
+        self.dtype = dtype
+        self._fusion_max = _default_fusion_max()
+        self._fusion_min = self.kDefaultFusionMinQubits
+        self.executor = -1
+        self._regs: dict[tuple, Register] = {}
+
+    # knobs -------------------------------------------------------------------------------
+    @property
+    def noise_model(self):
+        return self._noise_model
+
+    @property
+    def fusion_max_qubits(self) -> int:
+        return self._fusion_max
+
+    @fusion_max_qubits.setter
+    def fusion_max_qubits(self, k: int):
+        k = int(k)
+        if k < 0 or k > self.kMaxFusionQubits:
+            raise ValueError(f"QarpSimulator::set_fusion_max_qubits: {k} exceeds the maximum block "
+                             f"width {self.kMaxFusionQubits}")
+        self._fusion_max = k
+
+    @property
+    def fusion_min_qubits(self) -> int:
+        return self._fusion_min
+
+    @fusion_min_qubits.setter
+    def fusion_min_qubits(self, n: int):
+        if int(n) < 0:
+            raise ValueError("fusion_min_qubits must be >= 0")
+        self._fusion_min = int(n)
+
+    def close(self):
+        for r in self._regs.values():
+            r.close()
+        self._regs.clear()
+
+    # registers ---------------------------------------------------------------------------
+    def register(self, n_qubits: int, slot: int = 0) -> Register:
+        n_qubits = int(n_qubits)
+        if n_qubits < 0 or n_qubits > MAX_QUBITS:
+            raise ValueError(f"n_qubits must be in [0, {MAX_QUBITS}], got {n_qubits}")
+        key = (n_qubits, slot, self.dtype)
+        r = self._regs.get(key)
+        if r is None:
+            # one register width at a time per slot keeps HBM use bounded
+            for k in [k for k in self._regs if k[1] == slot]:
+                self._regs.pop(k).close()
+            r = Register(n_qubits, self.dtype, self.device)
+            self._regs[key] = r
+        r.configure(self._fusion_max, self._fusion_min, self.executor)
+        return r
+
+    def _prepared(self, commands, n_qubits, initial_state, where, values=None) -> Register:
+        reg = self.register(n_qubits)
+        if initial_state is not None:
+            a = np.asarray(initial_state, dtype=np.complex128).reshape(-1)
+            if a.shape[0] != (1 << n_qubits):
+                raise ValueError(f"QarpSimulator::{where}: initial_state length {a.shape[0]} != "
+                                 f"2^n_qubits = {1 << n_qubits}")
+            reg.set_state(a, validate=True)
+        else:
+            reg.reset()
+        reg.apply(pack(commands, values))
+        return reg
+
+    # QarpSimulator surface ---------------------------------------------------------------
+    def statevector(self, commands, n_qubits: int, *, initial_state=None) -> np.ndarray:
+        """Final amplitudes of ``commands`` from |0...0> (or ``initial_state``)
+        (QarpSimulator::statevector, qarp_simulator.cpp:901-943)."""
+        commands = list(commands)
+        if any(needs_trajectory(c) for c in commands):
+            raise RuntimeError(
+                "QarpSimulator::statevector: circuit contains mid-circuit measurement, Reset, or "
+                "classical condition — statevector is not deterministic. Use run() for trajectory "
+                "simulation.")
+        return self._prepared(commands, n_qubits, initial_state, "statevector").get_state()
+
+    def run(self, commands, n_qubits: int, n_shots: int, seed: Optional[int] = None, *,
+            initial_state=None) -> SamplingResult:
+        """Sample ``n_shots`` terminal outcomes (QarpSimulator::run's sample-once path,
+        qarp_simulator.cpp:1016-1036).  Seeded draws reproduce the reference's uniforms."""
+        commands = list(commands)
+        if not measurements_are_terminal(commands):
+            raise CapabilityError(
+                "B200Simulator.run: mid-circuit measurement, Reset or classical conditions need "
+                "the per-shot trajectory path, which the B200 engine does not implement")
+        base_s = int(seed) if seed is not None else int.from_bytes(os.urandom(4), "little")
+        reg = self._prepared(commands, n_qubits, initial_state, "run")
+        return self._sample_result(reg, commands, n_qubits, n_shots, base_s)
+
+    def _sample_result(self, reg, commands, n_qubits, n_shots, base_s) -> SamplingResult:
+        res = SamplingResult(n_qubits, int(n_shots))
+        if n_shots <= 0:
+            res.n_cbits = cbit_register_width(commands)
+            return res
+        idx = reg.sample_seeded(base_s, n_shots)
+        res.outcomes = idx
+        keys, cnt = np.unique(idx, return_counts=True)
+        res.counts = {int(k): int(c) for k, c in zip(keys, cnt)}
+        res.n_cbits = cbit_register_width(commands)
+        recorded = [(int(c.qubits[0]), int(c.cbits[0])) for c in commands
+                    if int(getattr(c.gate, "value", c.gate)) == 41 and getattr(c, "cbits", ())]
+        if recorded:
+            hist = np.zeros((int(n_shots), res.n_cbits), dtype=bool)
+            for q, cb in recorded:
+                hist[:, cb] = ((idx >> np.uint64(q)) & np.uint64(1)).astype(bool)
+            res.cbit_history = [list(map(bool, row)) for row in hist]
+        return res
+
+    def batch_run(self, commands, n_qubits: int, n_shots: int, param_sets, seed=None):
+        commands = list(commands)
+        out = []
+        for i, values in enumerate(param_sets):
+            s = None if seed is None else (int(seed) + i) & 0xFFFFFFFF
+            if not measurements_are_terminal(commands):
+                raise CapabilityError("B200Simulator.batch_run: trajectory circuits are not supported")
+            base_s = s if s is not None else int.from_bytes(os.urandom(4), "little")
+            reg = self._prepared(commands, n_qubits, None, "run", values)
+            out.append(self._sample_result(reg, commands, n_qubits, n_shots, base_s))
+        return out
+
+    def program_statevector(self, program, n_qubits: int, *, initial_state=None) -> np.ndarray:
+        return self.statevector(_gates_of(program), n_qubits, initial_state=initial_state)
+
+    def program_run(self, program, n_qubits: int, n_shots: int, seed=None, *, initial_state=None):
+        return self.run(_gates_of(program), n_qubits, n_shots, seed, initial_state=initial_state)
+
+    def transition(self, bra, ket, n_qubits: int, observable) -> complex:
+        """<bra|H|ket> over caller host statevectors (QarpSimulator::transition,
+        qarp_simulator.cpp:954-967)."""
+        if n_qubits < 0 or n_qubits > 62:
+            raise ValueError(f"pauli_transition: n_qubits must be in [0, 62], got {n_qubits}")
+        dim = 1 << n_qubits
+        b = np.asarray(bra, dtype=np.complex128).reshape(-1)
+        k = np.asarray(ket, dtype=np.complex128).reshape(-1)
+        if b.shape[0] != dim or k.shape[0] != dim:
+            raise ValueError(f"QarpSimulator::transition: bra/ket lengths {b.shape[0]}/{k.shape[0]} "
+                             f"do not match 2^{n_qubits} = {dim}")
+        masks = to_masks(observable, n_qubits)
+        rk = self.register(n_qubits, slot=0)
+        rb = self.register(n_qubits, slot=1)
+        rk.set_state(k, validate=False)
+        rb.set_state(b, validate=False)
+        return rb.transition(rk, masks)
+
+    def expectation(self, commands, n_qubits: int, observable, *, initial_state=None) -> float:
+        """Re <psi|H|psi> with psi = circuit(initial or |0...0>), computed on the device
+        (QarpSimulator::expectation, qarp_simulator.cpp:945-952)."""
+        commands = list(commands)
+        if any(needs_trajectory(c) for c in commands):
+            raise RuntimeError("QarpSimulator::statevector: circuit contains mid-circuit measurement, "
+                               "Reset, or classical condition — statevector is not deterministic.")
+        masks = to_masks(observable, n_qubits)
+        reg = self._prepared(commands, n_qubits, initial_state, "statevector")
+        return reg.expectation(masks).real
+
+    def batch_expectation(self, commands, n_qubits: int, observable, param_sets) -> list:
+        commands = list(commands)
+        masks = to_masks(observable, n_qubits)
+        out = []
+        for values in param_sets:
+            reg = self._prepared(commands, n_qubits, None, "statevector", values)
+            out.append(reg.expectation(masks).real)
+        return out
+
+    def run_gradient(self, commands, n_qubits: int, observable, params: Mapping[str, float],
+                     param_order: Sequence[str], *, initial_state=None) -> list:
+        """d<H>/d theta_k for every name in ``param_order`` in one adjoint sweep
+        (QarpSimulator::run_gradient, qarp_simulator.cpp:1519-1618)."""
+        return list(self.energy_and_gradient(commands, n_qubits, observable, params, param_order,
+                                             initial_state=initial_state)[1])
+
+    def energy_and_gradient(self, commands, n_qubits, observable, params, param_order, *,
+                            initial_state=None):
+        commands = list(commands)
+        if any(needs_trajectory(c) for c in commands):
+            raise RuntimeError("QarpSimulator::run_gradient: trajectory commands (Measure / Reset / "
+                               "classical condition) are not differentiable.")
+        masks = to_masks(observable, n_qubits, where="run_gradient")
+        stream = pack(commands, dict(params), list(param_order))
+        reg = self.register(n_qubits)
+        self._seed(reg, n_qubits, initial_state, "run_gradient")
+        energy, grad = reg.adjoint(stream, len(param_order), masks)
+        return energy, grad
+
+    def run_gradient_phi(self, commands, n_qubits: int, phi, params, param_order, *,
+                         initial_state=None) -> list:
+        commands = list(commands)
+        if any(needs_trajectory(c) for c in commands):
+            raise RuntimeError("QarpSimulator::run_gradient: trajectory commands (Measure / Reset / "
+                               "classical condition) are not differentiable.")
+        stream = pack(commands, dict(params), list(param_order))
+        reg = self.register(n_qubits)
+        self._seed(reg, n_qubits, initial_state, "run_gradient")
+        return list(reg.adjoint_phi(stream, len(param_order), phi))
+
+    def _seed(self, reg, n_qubits, initial_state, where):
+        if initial_state is not None:
+            a = np.asarray(initial_state, dtype=np.complex128).reshape(-1)
+            if a.shape[0] != (1 << n_qubits):
+                raise ValueError(f"QarpSimulator::{where}: initial_state length {a.shape[0]} != "
+                                 f"2^n_qubits = {1 << n_qubits}")
+            reg.set_state(a, validate=True)
+        else:
+            reg.reset()
+
+    def unitary_matrix(self, commands, n_qubits: int) -> np.ndarray:
+        """Full 2^n x 2^n unitary, column by column, unfused (qarp_simulator.cpp:1271-1304)."""
+        commands = list(commands)
+        if any(needs_trajectory(c) for c in commands):
+            raise RuntimeError("QarpSimulator::unitary_matrix: circuit contains mid-circuit "
+                               "measurement, Reset, or classical condition — output is not unitary.")
+        dim = 1 << n_qubits
+        stream = pack(commands)
+        reg = self.register(n_qubits)
+        u = np.empty((dim, dim), dtype=np.complex128)
+        col = np.zeros(dim, dtype=np.complex128)
+        for j in range(dim):
+            col[:] = 0
+            col[j] = 1
+            reg.set_state(col, validate=False)
+            reg.apply(stream, fused=False)
+            u[:, j] = reg.get_state()
+        return u
+
+
+def _gates_of(program):
+    """Flatten a structured program whose kernels are all gate kernels; the typed
+    Permutation / Dense / ControlledPowers kernels are not on the B200 path yet."""
+    kernels = program.kernels() if callable(getattr(program, "kernels", None)) else program
+    out = []
+    for k in kernels:
+        cmds = getattr(k, "commands", None)
+        if cmds is None:
+            raise CapabilityError("B200Simulator: structured Permutation / Dense / ControlledPowers "
+                                  "kernels are not supported; run the gate path (structured=False)")
+        out.extend(cmds)
+    return out

@@ -1,0 +1,241 @@
+"""TEST INFRASTRUCTURE ONLY — Python access to the two CPU checkers of the statevector path.
+
+* ``Restatement`` — ``_build/liboracle.so``, the plain-C restatement (qsv_oracle.c).
+* ``Reference`` — ``_ref/libqarpref.so``, the reference's own simulator compiled from its
+  sources (ref_driver.cpp), present where the reference tree was available at build time.
+
+Only tests/, the smoke entry of __graft_entry__.py and bench.py's CPU legs load this module;
+the engine package never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_size_t, c_uint8, c_uint32, c_uint64
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT_SO = os.path.join(HERE, "_build", "liboracle.so")
+REFERENCE_SO = os.path.join(HERE, "_ref", "libqarpref.so")
+REF_ROOT = os.environ.get("QSV_REFERENCE_ROOT", "/root/reference")
+
+PD = POINTER(c_double)
+PU64 = POINTER(c_uint64)
+PI32 = POINTER(c_int32)
+P8 = POINTER(c_uint8)
+
+
+def build(reference: bool = True) -> None:
+    """Compile the restatement, and the reference library when its sources are present."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if reference and os.path.isdir(os.path.join(REF_ROOT, "src", "qarpx")):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"], check=True)
+
+
+def _d(a):
+    return a.ctypes.data_as(PD)
+
+
+def _u64(a):
+    return a.ctypes.data_as(PU64)
+
+
+def _i32(a):
+    return a.ctypes.data_as(PI32)
+
+
+def _u8(b: bytes):
+    return ctypes.cast(ctypes.c_char_p(b), P8)
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+class Restatement:
+    def __init__(self):
+        if not os.path.exists(RESTATEMENT_SO):
+            build(reference=False)
+        lib = ctypes.CDLL(RESTATEMENT_SO)
+        lib.or_last_error.restype = c_char_p
+        lib.or_apply.argtypes = [PD, c_int, P8, c_size_t]
+        lib.or_transition.argtypes = [PD, PD, c_int, PU64, PU64, PD, c_size_t, PD]
+        lib.or_apply_observable.argtypes = [PD, PD, c_int, PU64, PU64, PD, c_size_t]
+        lib.or_uniforms.argtypes = [c_uint32, c_size_t, PD]
+        lib.or_uniforms.restype = None
+        lib.or_sample.argtypes = [PD, c_int, PD, c_size_t, PU64, PD]
+        lib.or_adjoint.argtypes = [PD, c_int, P8, c_size_t, PI32, PI32, PD, c_int, PU64, PU64, PD,
+                                   c_size_t, PD, PD]
+        lib.or_adjoint_phi.argtypes = [PD, c_int, P8, c_size_t, PI32, PI32, PD, c_int, PD, PD]
+        self.lib = lib
+
+    def _check(self, rc):
+        if rc:
+            raise OracleError(f"[{rc}] " + self.lib.or_last_error().decode())
+
+    def statevector(self, buf: bytes, n: int, initial=None) -> np.ndarray:
+        s = np.zeros(1 << n, dtype=np.complex128)
+        if initial is None:
+            s[0] = 1
+        else:
+            s[:] = initial
+        self._check(self.lib.or_apply(_d(s.view(np.float64)), n, _u8(buf), len(buf)))
+        return s
+
+    def apply(self, state: np.ndarray, n: int, buf: bytes) -> np.ndarray:
+        s = np.ascontiguousarray(state, dtype=np.complex128).copy()
+        self._check(self.lib.or_apply(_d(s.view(np.float64)), n, _u8(buf), len(buf)))
+        return s
+
+    def transition(self, bra, ket, n, masks) -> complex:
+        out = np.zeros(2)
+        b = np.ascontiguousarray(bra, dtype=np.complex128)
+        k = np.ascontiguousarray(ket, dtype=np.complex128)
+        self._check(self.lib.or_transition(_d(b.view(np.float64)), _d(k.view(np.float64)), n,
+                                           _u64(masks.x), _u64(masks.z), _d(masks.coeff),
+                                           masks.n_terms, _d(out)))
+        return complex(out[0], out[1])
+
+    def apply_observable(self, psi, n, masks) -> np.ndarray:
+        p = np.ascontiguousarray(psi, dtype=np.complex128)
+        out = np.zeros_like(p)
+        self._check(self.lib.or_apply_observable(_d(p.view(np.float64)), _d(out.view(np.float64)), n,
+                                                 _u64(masks.x), _u64(masks.z), _d(masks.coeff),
+                                                 masks.n_terms))
+        return out
+
+    def uniforms(self, seed: int, shots: int) -> np.ndarray:
+        u = np.zeros(shots)
+        self.lib.or_uniforms(seed & 0xFFFFFFFF, shots, _d(u))
+        return u
+
+    def sample(self, state, n, u, with_cdf: bool = False):
+        s = np.ascontiguousarray(state, dtype=np.complex128)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.zeros(u.shape[0], dtype=np.uint64)
+        cp = np.zeros(1 << n) if with_cdf else None
+        self._check(self.lib.or_sample(_d(s.view(np.float64)), n, _d(u), u.shape[0], _u64(out),
+                                       _d(cp) if cp is not None else None))
+        return (out, cp) if with_cdf else out
+
+    def adjoint(self, stream, n, n_params, masks, psi0=None):
+        grad = np.zeros(max(n_params, 1))
+        energy = c_double()
+        p0 = None if psi0 is None else np.ascontiguousarray(psi0, dtype=np.complex128)
+        self._check(self.lib.or_adjoint(
+            _d(p0.view(np.float64)) if p0 is not None else None, n, _u8(stream.buf), len(stream.buf),
+            _i32(stream.dep_ptr), _i32(stream.dep_param), _d(stream.dep_alpha), n_params,
+            _u64(masks.x), _u64(masks.z), _d(masks.coeff), masks.n_terms, _d(grad),
+            ctypes.byref(energy)))
+        return energy.value, grad[:n_params]
+
+    def adjoint_phi(self, stream, n, n_params, phi, psi0=None):
+        grad = np.zeros(max(n_params, 1))
+        ph = np.ascontiguousarray(phi, dtype=np.complex128)
+        p0 = None if psi0 is None else np.ascontiguousarray(psi0, dtype=np.complex128)
+        self._check(self.lib.or_adjoint_phi(
+            _d(p0.view(np.float64)) if p0 is not None else None, n, _u8(stream.buf), len(stream.buf),
+            _i32(stream.dep_ptr), _i32(stream.dep_param), _d(stream.dep_alpha), n_params,
+            _d(ph.view(np.float64)), _d(grad)))
+        return grad[:n_params]
+
+
+class Reference:
+    """The reference's own QarpSimulator (built from its sources into oracle/_ref)."""
+
+    def __init__(self):
+        if not os.path.exists(REFERENCE_SO):
+            raise FileNotFoundError(REFERENCE_SO)
+        lib = ctypes.CDLL(REFERENCE_SO)
+        lib.qref_last_error.restype = c_char_p
+        lib.qref_set_threads.argtypes = [c_int]
+        lib.qref_statevector.argtypes = [P8, c_size_t, c_int, c_int, c_int, PD, PD]
+        lib.qref_apply_inplace.argtypes = [P8, c_size_t, c_int, PD]
+        lib.qref_apply_fused_inplace.argtypes = [P8, c_size_t, c_int, c_int, c_int, PD, PI32]
+        lib.qref_fuse_count.argtypes = [P8, c_size_t, c_int, c_int, c_int, PI32, PI32]
+        lib.qref_transition.argtypes = [PD, PD, c_int, PU64, PU64, PD, c_size_t, PD]
+        lib.qref_expectation.argtypes = [P8, c_size_t, c_int, c_int, c_int, PU64, PU64, PD, c_size_t, PD]
+        lib.qref_run.argtypes = [P8, c_size_t, c_int, c_int, c_uint32, c_int, c_int, PU64, PI32, c_size_t,
+                                 POINTER(c_size_t)]
+        lib.qref_uniforms.argtypes = [c_uint32, c_size_t, PD]
+        lib.qref_run_gradient.argtypes = [P8, c_size_t, c_int, PI32, PI32, PD, c_int, PD, PU64, PU64, PD,
+                                          c_size_t, PD, PD]
+        self.lib = lib
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REFERENCE_SO)
+
+    def _check(self, rc):
+        if rc:
+            raise OracleError(f"[{rc}] " + self.lib.qref_last_error().decode())
+
+    def set_threads(self, n: int) -> int:
+        return self.lib.qref_set_threads(int(n))
+
+    def statevector(self, buf, n, fusion_max=-1, fusion_min=-1, initial=None):
+        out = np.zeros(1 << n, dtype=np.complex128)
+        init = None if initial is None else np.ascontiguousarray(initial, dtype=np.complex128)
+        self._check(self.lib.qref_statevector(_u8(buf), len(buf), n, fusion_max, fusion_min,
+                                              _d(init.view(np.float64)) if init is not None else None,
+                                              _d(out.view(np.float64))))
+        return out
+
+    def apply_inplace(self, state, n, buf):
+        self._check(self.lib.qref_apply_inplace(_u8(buf), len(buf), n, _d(state.view(np.float64))))
+        return state
+
+    def apply_fused_inplace(self, state, n, buf, fusion_max=3, fusion_min=12) -> int:
+        cnt = c_int32()
+        self._check(self.lib.qref_apply_fused_inplace(_u8(buf), len(buf), n, fusion_max, fusion_min,
+                                                      _d(state.view(np.float64)), ctypes.byref(cnt)))
+        return cnt.value
+
+    def fuse_count(self, buf, n, fusion_max, fusion_min=-1):
+        cnt = c_int32()
+        hist = np.zeros(9, dtype=np.int32)
+        self._check(self.lib.qref_fuse_count(_u8(buf), len(buf), n, fusion_max, fusion_min,
+                                             ctypes.byref(cnt), _i32(hist)))
+        return cnt.value, hist
+
+    def transition(self, bra, ket, n, masks) -> complex:
+        out = np.zeros(2)
+        b = np.ascontiguousarray(bra, dtype=np.complex128)
+        k = np.ascontiguousarray(ket, dtype=np.complex128)
+        self._check(self.lib.qref_transition(_d(b.view(np.float64)), _d(k.view(np.float64)), n,
+                                             _u64(masks.x), _u64(masks.z), _d(masks.coeff),
+                                             masks.n_terms, _d(out)))
+        return complex(out[0], out[1])
+
+    def expectation(self, buf, n, masks, fusion_max=-1, fusion_min=-1) -> float:
+        out = c_double()
+        self._check(self.lib.qref_expectation(_u8(buf), len(buf), n, fusion_max, fusion_min,
+                                              _u64(masks.x), _u64(masks.z), _d(masks.coeff),
+                                              masks.n_terms, ctypes.byref(out)))
+        return out.value
+
+    def run(self, buf, n, shots, seed, fusion_max=-1, fusion_min=-1) -> dict:
+        cap = max(1, min(shots, 1 << n))
+        keys = np.zeros(cap, dtype=np.uint64)
+        cnts = np.zeros(cap, dtype=np.int32)
+        got = c_size_t()
+        self._check(self.lib.qref_run(_u8(buf), len(buf), n, shots, seed & 0xFFFFFFFF, fusion_max,
+                                      fusion_min, _u64(keys), _i32(cnts), cap, ctypes.byref(got)))
+        return {int(keys[i]): int(cnts[i]) for i in range(got.value)}
+
+    def uniforms(self, seed, shots):
+        u = np.zeros(shots)
+        self._check(self.lib.qref_uniforms(seed & 0xFFFFFFFF, shots, _d(u)))
+        return u
+
+    def run_gradient(self, stream, n, n_params, param_values, masks, initial=None):
+        grad = np.zeros(max(n_params, 1))
+        vals = np.ascontiguousarray(param_values, dtype=np.float64)
+        init = None if initial is None else np.ascontiguousarray(initial, dtype=np.complex128)
+        self._check(self.lib.qref_run_gradient(
+            _u8(stream.buf), len(stream.buf), n, _i32(stream.dep_ptr), _i32(stream.dep_param),
+            _d(stream.dep_alpha), n_params, _d(vals), _u64(masks.x), _u64(masks.z), _d(masks.coeff),
+            masks.n_terms, _d(init.view(np.float64)) if init is not None else None, _d(grad)))
+        return grad[:n_params]

@@ -1,0 +1,340 @@
+// ref_driver.cpp — TEST INFRASTRUCTURE ONLY.
+//
+// A C-ABI shim over the reference's own CPU simulator (qarpx::QarpSimulator, compiled
+// from the reference sources by oracle/Makefile into oracle/_ref/).  It decodes the
+// engine's packed command stream (include/qsv.h) into qarpx::Command records and calls
+// the reference's public methods unchanged:
+//
+//   qref_statevector   -> QarpSimulator::statevector        (qarp_simulator.cpp:901-943)
+//   qref_apply_inplace -> QarpSimulator::apply_command loop  (qarp_simulator.h:168-170; the
+//                         caller-owned-buffer path for registers too wide to copy)
+//   qref_transition    -> QarpSimulator::transition         (qarp_simulator.cpp:954-967)
+//   qref_expectation   -> QarpSimulator::expectation        (qarp_simulator.cpp:945-952)
+//   qref_run           -> QarpSimulator::run                (qarp_simulator.cpp:988-1244)
+//   qref_run_gradient  -> QarpSimulator::run_gradient       (qarp_simulator.cpp:1607-1618)
+//   qref_fuse_count    -> fuse_for_simulation               (fusion.cpp:120-268), block count
+//
+// Used by tests/ (parity pins, golden fixture generation) and by bench.py's reference arm
+// (the reference's own CPU implementation timed on the host cores).
+#include "../include/qsv.h"
+
+#include "qarpx/simulator/qarp_simulator.h"
+#include "qarpx/simulator/fusion.h"
+#include "qarpx/transpiler/fusion.h"
+#include "qarpx/core/param.h"
+#include "qarpx/core/errors.h"
+
+#include <complex>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <random>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+thread_local std::string g_err;
+
+using qarpx::Command;
+using qarpx::GateType;
+using qarpx::Param;
+using cd = std::complex<double>;
+
+struct Rec {
+    uint16_t gate;
+    int nq, np, ncb, flags;
+    const uint32_t* q;
+    const double* p;
+    const double* m;
+};
+
+std::vector<Rec> decode_all(const uint8_t* buf, size_t nbytes) {
+    std::vector<Rec> out;
+    size_t off = 0;
+    while (off < nbytes) {
+        if (off + 8 > nbytes) throw std::invalid_argument("command buffer truncated");
+        qsv_cmd_header h;
+        std::memcpy(&h, buf + off, sizeof h);
+        Rec r{h.gate, h.n_qubits, h.n_params, h.n_cbits, h.flags, nullptr, nullptr, nullptr};
+        size_t o = off + 8;
+        r.q = reinterpret_cast<const uint32_t*>(buf + o);
+        o += 4u * static_cast<size_t>(r.nq + r.ncb);
+        o = (o + 7u) & ~size_t{7};
+        r.p = reinterpret_cast<const double*>(buf + o);
+        o += 8u * static_cast<size_t>(r.np);
+        if (r.gate == QSV_GATE_CUSTOM) {
+            r.m = reinterpret_cast<const double*>(buf + o);
+            o += 16u * (size_t{1} << (2 * r.nq));
+        }
+        if (o > nbytes) throw std::invalid_argument("command buffer truncated");
+        out.push_back(r);
+        off = o;
+    }
+    return out;
+}
+
+Command to_command(const Rec& r) {
+    Command c;
+    c.gate = static_cast<GateType>(r.gate);
+    for (int b = 0; b < r.nq; ++b) c.qubits.push_back(r.q[b]);
+    for (int b = 0; b < r.ncb; ++b) c.cbits.push_back(r.q[r.nq + b]);
+    for (int b = 0; b < r.np; ++b) c.params.push_back(Param(r.p[b]));
+    if (r.m) {
+        const int D = 1 << r.nq;
+        Eigen::MatrixXcd U(D, D);
+        for (int y = 0; y < D; ++y)
+            for (int x = 0; x < D; ++x)
+                U(y, x) = cd(r.m[2 * (y * D + x)], r.m[2 * (y * D + x) + 1]);
+        c.unitary = std::make_shared<const Eigen::MatrixXcd>(std::move(U));
+    }
+    return c;
+}
+
+std::vector<Command> to_commands(const uint8_t* buf, size_t nbytes) {
+    std::vector<Command> out;
+    for (const Rec& r : decode_all(buf, nbytes)) out.push_back(to_command(r));
+    return out;
+}
+
+qarpx::PauliObservable to_observable(const uint64_t* xm, const uint64_t* zm,
+                                     const double* coeff, size_t nt) {
+    qarpx::PauliObservable obs;
+    for (size_t t = 0; t < nt; ++t) {
+        std::vector<std::pair<uint32_t, char>> ps;
+        const uint64_t any = xm[t] | zm[t];
+        for (uint32_t q = 0; q < 64; ++q) {
+            if (!((any >> q) & 1)) continue;
+            const bool x = (xm[t] >> q) & 1, z = (zm[t] >> q) & 1;
+            ps.emplace_back(q, x && z ? 'Y' : x ? 'X' : 'Z');
+        }
+        obs.emplace_back(std::move(ps), cd(coeff[2 * t], coeff[2 * t + 1]));
+    }
+    return obs;
+}
+
+int translate(const std::exception_ptr& e) {
+    try {
+        std::rethrow_exception(e);
+    } catch (const qarpx::capability_error& ex) {
+        g_err = ex.what();
+        return QSV_ECAPABILITY;
+    } catch (const std::invalid_argument& ex) {
+        g_err = ex.what();
+        return QSV_EINVAL;
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
+        return QSV_ERUNTIME;
+    }
+}
+
+qarpx::QarpSimulator make_sim(int fusion_max, int fusion_min) {
+    qarpx::QarpSimulator sim;
+    if (fusion_max >= 0) sim.set_fusion_max_qubits(static_cast<std::size_t>(fusion_max));
+    if (fusion_min >= 0) sim.set_fusion_min_qubits(static_cast<std::size_t>(fusion_min));
+    return sim;
+}
+
+std::optional<std::vector<cd>> initial(const double* init, int n) {
+    if (!init) return std::nullopt;
+    const size_t dim = size_t{1} << n;
+    const cd* p = reinterpret_cast<const cd*>(init);
+    return std::vector<cd>(p, p + dim);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* qref_last_error() { return g_err.c_str(); }
+
+int qref_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+int qref_statevector(const uint8_t* cmds, size_t nbytes, int n, int fusion_max,
+                     int fusion_min, const double* init, double* out) {
+    try {
+        auto sim = make_sim(fusion_max, fusion_min);
+        auto sv = sim.statevector(to_commands(cmds, nbytes), n, initial(init, n));
+        std::memcpy(out, sv.data(), sv.size() * sizeof(cd));
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_apply_inplace(const uint8_t* cmds, size_t nbytes, int n, double* state) {
+    try {
+        qarpx::QarpSimulator sim;
+        const uint64_t dim = uint64_t{1} << n;
+        for (const Command& c : to_commands(cmds, nbytes))
+            sim.apply_command(c, reinterpret_cast<cd*>(state), dim);
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+// statevector()'s inner loop on a caller-owned register: the reference's fusion pass at
+// width fusion_max (from fusion_min qubits), then apply_command per fused command
+// (qarp_simulator.cpp:921-935) — without statevector()'s allocate + copy-out, so a 28-qubit
+// register needs one 4 GiB buffer instead of three.  Returns the fused stream length.
+int qref_apply_fused_inplace(const uint8_t* cmds, size_t nbytes, int n, int fusion_max,
+                             int fusion_min, double* state, int32_t* n_fused) {
+    try {
+        auto sim = make_sim(fusion_max, fusion_min);
+        auto in = to_commands(cmds, nbytes);
+        std::vector<Command> fused;
+        if (fusion_max == 0) fused = in;
+        else if (fusion_max == 1 || static_cast<std::size_t>(std::max(n, 0)) < sim.fusion_min_qubits())
+            fused = qarpx::fuse_single_qubit_gates(in);
+        else fused = qarpx::fuse_for_simulation(
+            in, static_cast<std::size_t>(fusion_max),
+            [&sim](const Command& c) { return sim.local_unitary(c); });
+        const uint64_t dim = uint64_t{1} << n;
+        for (const Command& c : fused) sim.apply_command(c, reinterpret_cast<cd*>(state), dim);
+        if (n_fused) *n_fused = static_cast<int32_t>(fused.size());
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+// The fused stream's length for the given knobs (fusion plan parity).
+int qref_fuse_count(const uint8_t* cmds, size_t nbytes, int n, int fusion_max,
+                    int fusion_min, int32_t* n_out, int32_t* widths_hist /* [9] */) {
+    try {
+        // the selection fuse_for_dispatch makes (qarp_simulator.cpp:120-129)
+        auto sim = make_sim(fusion_max, fusion_min);
+        auto in = to_commands(cmds, nbytes);
+        std::vector<Command> fused;
+        if (fusion_max == 0) fused = in;
+        else if (fusion_max == 1 || static_cast<std::size_t>(std::max(n, 0)) < sim.fusion_min_qubits())
+            fused = qarpx::fuse_single_qubit_gates(in);
+        else fused = qarpx::fuse_for_simulation(
+            in, static_cast<std::size_t>(fusion_max),
+            [&sim](const Command& c) { return sim.local_unitary(c); });
+        *n_out = static_cast<int32_t>(fused.size());
+        if (widths_hist) {
+            for (int k = 0; k <= 8; ++k) widths_hist[k] = 0;
+            for (const Command& c : fused)
+                if (c.gate == GateType::Custom && c.qubits.size() <= 8)
+                    widths_hist[c.qubits.size()]++;
+        }
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_transition(const double* bra, const double* ket, int n, const uint64_t* xm,
+                    const uint64_t* zm, const double* coeff, size_t nt, double out[2]) {
+    try {
+        qarpx::QarpSimulator sim;
+        const size_t dim = size_t{1} << n;
+        std::vector<cd> b(reinterpret_cast<const cd*>(bra), reinterpret_cast<const cd*>(bra) + dim);
+        std::vector<cd> k(reinterpret_cast<const cd*>(ket), reinterpret_cast<const cd*>(ket) + dim);
+        const cd r = sim.transition(b, k, n, to_observable(xm, zm, coeff, nt));
+        out[0] = r.real();
+        out[1] = r.imag();
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_expectation(const uint8_t* cmds, size_t nbytes, int n, int fusion_max,
+                     int fusion_min, const uint64_t* xm, const uint64_t* zm,
+                     const double* coeff, size_t nt, double* out) {
+    try {
+        auto sim = make_sim(fusion_max, fusion_min);
+        *out = sim.expectation(to_commands(cmds, nbytes), n, to_observable(xm, zm, coeff, nt));
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_run(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed,
+             int fusion_max, int fusion_min, uint64_t* keys, int32_t* counts, size_t cap,
+             size_t* n_out) {
+    try {
+        auto sim = make_sim(fusion_max, fusion_min);
+        auto res = sim.run(to_commands(cmds, nbytes), n, shots, seed);
+        size_t i = 0;
+        for (const auto& [k, v] : res.counts) {
+            if (i >= cap) throw std::invalid_argument("qref_run: output capacity too small");
+            keys[i] = k;
+            counts[i] = v;
+            ++i;
+        }
+        *n_out = i;
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+// The uniforms sample_terminal's std::discrete_distribution consumes, drawn by the
+// toolchain's own std::generate_canonical (pins the oracle's MT19937 restatement).
+int qref_uniforms(uint32_t seed, size_t shots, double* u) {
+    std::mt19937 rng(seed);
+    for (size_t s = 0; s < shots; ++s)
+        u[s] = std::generate_canonical<double, std::numeric_limits<double>::digits>(rng);
+    return QSV_OK;
+}
+
+// run_gradient with symbolic parameters rebuilt from the dependency table: command i's
+// first parameter becomes sum_d alpha_d * p<param_d> + offset, offset chosen so that it
+// evaluates to the concrete value in the stream at `param_values`.
+int qref_run_gradient(const uint8_t* cmds, size_t nbytes, int n, const int32_t* dep_ptr,
+                      const int32_t* dep_param, const double* dep_alpha, int n_params,
+                      const double* param_values, const uint64_t* xm, const uint64_t* zm,
+                      const double* coeff, size_t nt, const double* init, double* grad) {
+    try {
+        qarpx::QarpSimulator sim;
+        auto recs = decode_all(cmds, nbytes);
+        std::vector<Command> cs;
+        cs.reserve(recs.size());
+        for (size_t i = 0; i < recs.size(); ++i) {
+            Command c = to_command(recs[i]);
+            if (dep_ptr[i + 1] > dep_ptr[i] && !c.params.empty()) {
+                double offset = recs[i].p[0];
+                for (int d = dep_ptr[i]; d < dep_ptr[i + 1]; ++d)
+                    offset -= dep_alpha[d] * param_values[dep_param[d]];
+                Param p = Param::linear(dep_alpha[dep_ptr[i]],
+                                        "p" + std::to_string(dep_param[dep_ptr[i]]), offset);
+                for (int d = dep_ptr[i] + 1; d < dep_ptr[i + 1]; ++d)
+                    p = p + Param::linear(dep_alpha[d], "p" + std::to_string(dep_param[d]), 0.0);
+                c.params[0] = p;
+            }
+            cs.push_back(std::move(c));
+        }
+        std::unordered_map<std::string, double> values;
+        std::vector<std::string> order;
+        for (int p = 0; p < n_params; ++p) {
+            values["p" + std::to_string(p)] = param_values[p];
+            order.push_back("p" + std::to_string(p));
+        }
+        auto g = sim.run_gradient(cs, n, to_observable(xm, zm, coeff, nt), values, order,
+                                  initial(init, n));
+        for (int p = 0; p < n_params; ++p) grad[p] = g[static_cast<size_t>(p)];
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,129 @@
+"""CPU: the C-ABI library loads and exports every declared symbol; host logic (packing,
+observable validation, fusion plans, affine probe, seeding) matches the reference."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from openqarp_b200 import _lib, circuits, ir, observable
+from openqarp_b200.errors import CapabilityError
+from openqarp_b200.ir import Command, GateType as G, Param
+
+
+def declared_symbols():
+    with open(os.path.join(ROOT, "include", "qsv.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"QSV_API\s+[\w\s\*]*?\b(qsv_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(_lib.lib, name), name
+    assert set(names) == set(_lib.DECLARED)
+    assert _lib.lib.qsv_abi_version() == 1
+
+
+def test_gate_codes_follow_reference_enum():
+    # src/qarpx/include/qarpx/core/gates.h:8-58 enumerator order
+    with open(os.path.join(ROOT, "include", "qsv.h")) as f:
+        text = f.read()
+    body = text[text.index("enum qsv_gate {"):text.index("QSV_GATE_COUNT")]
+    codes = re.findall(r"QSV_GATE_(\w+)", body)
+    assert len(codes) == len(G)
+    assert [g.name.upper() for g in G] == [c.replace("_", "") for c in codes]
+
+
+def test_pack_layout_and_affine_dependencies():
+    cmds = [Command(G.Rx, (3,), (Param.linear(2.0, "a", 0.5),)),
+            Command(G.CX, (0, 1)),
+            Command(G.RZZ, (1, 2), (Param.linear(-1.0, "b") + Param.linear(3.0, "a"),))]
+    st = ir.pack(cmds, {"a": 0.25, "b": 1.0}, ["a", "b"])
+    assert st.n_cmds == 3
+    np.testing.assert_array_equal(st.dep_ptr, [0, 1, 1, 3])
+    assert sorted(zip(st.dep_param[1:], st.dep_alpha[1:])) == [(0, 3.0), (1, -1.0)]
+    # header of the first record: gate, n_qubits, n_params
+    assert st.buf[0] == int(G.Rx) and st.buf[2] == 1 and st.buf[3] == 1
+    (angle,) = np.frombuffer(st.buf[16:24], dtype=np.float64)
+    assert angle == 2.0 * 0.25 + 0.5
+
+
+def test_affine_probe_rejects_non_affine():
+    class Sq:
+        def is_symbolic(self):
+            return True
+
+        def free_symbols(self):
+            return ["x"]
+
+        def evaluate(self, v):
+            return v["x"] ** 2
+
+    with pytest.raises(CapabilityError):
+        ir.affine_coefficients(Sq())
+
+
+def test_observable_validation_messages():
+    with pytest.raises(ValueError, match="out of range"):
+        observable.to_masks([([(5, "X")], 1.0)], 3)
+    with pytest.raises(ValueError, match="repeated"):
+        observable.to_masks([([(1, "X"), (1, "Z")], 1.0)], 3)
+    with pytest.raises(ValueError, match="invalid Pauli"):
+        observable.to_masks([([(1, "Q")], 1.0)], 3)
+    m = observable.to_masks([([(0, "Y"), (2, "X")], 0.5 + 0.25j)], 3)
+    assert int(m.x[0]) == 0b101 and int(m.z[0]) == 0b001
+    np.testing.assert_array_equal(m.coeff, [0.5, 0.25])
+
+
+def test_uniforms_are_the_reference_draws(golden):
+    from openqarp_b200 import uniforms
+    np.testing.assert_array_equal(uniforms(7, 257), golden["uniforms_seed7"])
+
+
+def fuse_count(buf, n, k, kmin):
+    import ctypes
+    cnt = ctypes.c_int32()
+    hist = np.zeros(9, dtype=np.int32)
+    _lib.check(_lib.lib.qsv_fuse_count(_lib.u8ptr(buf), len(buf), n, k, kmin, ctypes.byref(cnt),
+                                       _lib.i32ptr(hist)))
+    return cnt.value, hist
+
+
+def test_fusion_plan_matches_reference_golden(golden):
+    n = int(golden["brick_n"])
+    cnt, hist = fuse_count(golden["brick_buf"].tobytes(), n, 3, 0)
+    assert cnt == int(golden["brick_fused3_len"])
+    np.testing.assert_array_equal(hist, golden["brick_fused3_hist"])
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3, 4, 5, 6])
+def test_fusion_plan_matches_reference_live(reference, k):
+    for n, cmds in ((12, circuits.brickwork(12, 6, seed=4)),
+                    (9, circuits.hea(9, 3, seed=2)[0]),
+                    (8, circuits.heisenberg_trotter(8, 2, 0.05, np.linspace(-1, 1, 8)))):
+        vals = circuits.hea(9, 3, seed=2)[1]
+        buf = ir.pack(cmds, vals).buf
+        mine = fuse_count(buf, n, k, 0)
+        theirs = reference.fuse_count(buf, n, k, 0)
+        assert mine[0] == theirs[0]
+        np.testing.assert_array_equal(mine[1], theirs[1])
+
+
+def test_fusion_knob_bounds():
+    with pytest.raises(ValueError):
+        fuse_count(b"", 4, 9, 0)
+
+
+def test_random_regular_graph_is_regular():
+    for n in (10, 12, 20):
+        edges = circuits.random_regular_graph(3, n, seed=n)
+        deg = np.zeros(n, dtype=int)
+        for u, v in edges:
+            assert u != v
+            deg[u] += 1
+            deg[v] += 1
+        assert (deg == 3).all()
+        assert len(set(edges)) == len(edges)
