@@ -132,7 +132,7 @@ class StreamTimer:
         return e
 
 
-def autotune(reg, buf, timer, candidates=(2, 3, 4, 5)):
+def autotune(reg, buf, timer, candidates=(2, 3, 4)):
     """Pick the fusion width with the shortest device time for this circuit (one timed
     application per candidate after one warm-up)."""
     res = {}
