@@ -1,0 +1,65 @@
+"""Small, self-contained cases of each hot kernel for profiling under ncu.
+
+    python -m openqarp_b200.profile_cases dense --n 26 --k 3 --reps 5
+    python -m openqarp_b200.profile_cases brickwork --n 26 --depth 4 --k 3
+    python -m openqarp_b200.profile_cases transition --n 24 --terms 547
+    python -m openqarp_b200.profile_cases adjoint --n 22 --layers 2
+    python -m openqarp_b200.profile_cases sample --n 26 --shots 100000
+
+Registers of 2^26 complex128 amplitudes (1 GiB) exceed L2 (126 MB), so DRAM counters are
+meaningful, and stay small enough for a full-set capture to end within minutes.
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+from . import Register, circuits, ir, observable
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["dense", "brickwork", "transition", "adjoint", "sample"])
+    ap.add_argument("--n", type=int, default=26)
+    ap.add_argument("--k", type=int, default=3)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--depth", type=int, default=4)
+    ap.add_argument("--terms", type=int, default=547)
+    ap.add_argument("--layers", type=int, default=2)
+    ap.add_argument("--shots", type=int, default=100000)
+    ap.add_argument("--dtype", default="complex128")
+    ap.add_argument("--executor", type=int, default=-1)
+    a = ap.parse_args(argv)
+    rng = np.random.default_rng(7)
+    reg = Register(a.n, a.dtype)
+    reg.configure(a.k, 12, a.executor)
+    if a.case == "dense":
+        z = rng.standard_normal((1 << a.k, 1 << a.k)) + 1j * rng.standard_normal((1 << a.k, 1 << a.k))
+        u, _ = np.linalg.qr(z)
+        qs = tuple(int(q) for q in rng.permutation(a.n)[:a.k])
+        reg.configure(0, 0, a.executor)
+        reg.apply(ir.pack([ir.custom(qs, u)] * a.reps).buf)
+    elif a.case == "brickwork":
+        reg.apply(ir.pack(circuits.brickwork(a.n, a.depth, seed=1)).buf)
+    elif a.case == "transition":
+        obs = circuits.tfim_chain(a.n) + circuits.random_pauli_sum(a.n, a.terms - (2 * a.n - 1), seed=2,
+                                                                    max_weight=4, coeff_std=0.1)
+        reg.apply(ir.pack(circuits.brickwork(a.n, 1, seed=1)).buf)
+        m = observable.to_masks(obs, a.n)
+        for _ in range(a.reps):
+            reg.expectation(m)
+    elif a.case == "adjoint":
+        cmds, vals, names = circuits.hea(a.n, a.layers, seed=3)
+        obs = circuits.tfim_chain(a.n)
+        reg.adjoint(ir.pack(cmds, vals, names), len(names), observable.to_masks(obs, a.n))
+    elif a.case == "sample":
+        reg.apply(ir.pack(circuits.brickwork(a.n, 1, seed=1)).buf)
+        reg.sample(np.sort(rng.random(a.shots)))
+    reg.synchronize()
+    reg.close()
+    print("ok", a.case)
+
+
+if __name__ == "__main__":
+    main()
