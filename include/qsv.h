@@ -201,6 +201,25 @@ QSV_API int qsv_scale(void* h, double scale);
 /* <a|b> in FP64 (fidelity against another handle of the same width; dtypes may differ). */
 QSV_API int qsv_inner(void* a, void* b, double out[2]);
 
+/* ---- allocation-free variant ------------------------------------------------------- *
+ * No counterpart in the reference: it exists for callers that cannot call cudaMalloc —
+ * a process whose device memory is owned by its own pool allocator (PyTorch's caching
+ * allocator, an inference server's arena), or a latency-critical path that cannot take the
+ * device-wide synchronisation cudaMalloc/cudaFree imply.  Same value as qsv_transition,
+ * <bra|H|ket>, for caller-owned DEVICE registers d_bra/d_ket (double2* for QSV_C128, float2*
+ * for QSV_C64, 2^n_qubits amplitudes on the same device), host observable arrays and a host
+ * out[2], on the caller's stream (NULL = legacy default stream); returns after the result
+ * is in out.  It allocates nothing: its scratch (term tables + partial sums) is one
+ * file-scope device array of 256 KiB that every GPU loading the library holds until exit.
+ * Limits and rules: at most QSV_STATIC_MAX_TERMS terms (more -> QSV_EINVAL); every call on a
+ * device shares that array and leaves its contents behind, so calls that overlap on the GPU
+ * race and must be serialised by the caller; the first call on a device looks up the
+ * array's address with that device current and should come before any stream capture. */
+#define QSV_STATIC_MAX_TERMS 4096
+QSV_API int qsv_transition_static(const void* d_bra, const void* d_ket, int n_qubits, int dtype,
+                                  const uint64_t* xmask, const uint64_t* zmask, const double* coeff,
+                                  size_t n_terms, void* cuda_stream, double out[2]);
+
 QSV_API int qsv_synchronize(void* h);
 QSV_API int qsv_stats(void* h, qsv_stats_t* out);
 

@@ -63,6 +63,8 @@ def _load():
         "qsv_inner": (c_int, [c_void_p, c_void_p, PD]),
         "qsv_synchronize": (c_int, [c_void_p]),
         "qsv_stats": (c_int, [c_void_p, POINTER(Stats)]),
+        "qsv_transition_static": (c_int, [c_void_p, c_void_p, c_int, c_int, PU64, PU64, PD, c_size_t,
+                                          c_void_p, PD]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -78,8 +80,9 @@ DECLARED = (
     "qsv_set_executor", "qsv_reset", "qsv_set_state", "qsv_get_state", "qsv_device_state",
     "qsv_copy_state", "qsv_fuse_count", "qsv_apply", "qsv_apply_unfused", "qsv_transition", "qsv_sample",
     "qsv_sample_seeded", "qsv_uniforms", "qsv_adjoint", "qsv_adjoint_phi", "qsv_norm2",
-    "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats",
+    "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_transition_static",
 )
+STATIC_MAX_TERMS = 4096
 
 
 def check(rc: int) -> None:

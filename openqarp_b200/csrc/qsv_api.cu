@@ -167,6 +167,10 @@ void to_device_c128(Handle* h, void* dst, const double* amps) {
 }
 
 }  // namespace
+
+// lets entry points defined in other translation units report through qsv_last_error
+void set_last_error(const std::string& msg) { g_err = msg; }
+
 }  // namespace qsv
 
 using namespace qsv;
