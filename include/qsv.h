@@ -129,6 +129,10 @@ QSV_API int qsv_set_fusion(void* h, int max_qubits, int min_qubits);
 /* Executor: 0 = one HBM pass per fused block ("stream"), 1 = several blocks per pass
  * staged in shared memory ("tiled"), -1 = the autotuned choice (default). */
 QSV_API int qsv_set_executor(void* h, int mode);
+/* Tile width of the tiled executor: qubits held in shared memory per tile, 8..13
+ * (0 = the default: 12 for complex128, 13 for complex64).  No reference counterpart: the
+ * reference applies one fused block per pass (qarp_simulator.cpp:934-935). */
+QSV_API int qsv_set_tile_qubits(void* h, int m);
 
 /* Register <- |0...0>. */
 QSV_API int qsv_reset(void* h);

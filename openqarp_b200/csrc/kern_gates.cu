@@ -61,23 +61,27 @@ struct DenseArgs {
     cplx<T> m[1 << (2 * K)];     // row-major 2^K x 2^K
 };
 
+// One group per thread and no loop: the matrix stays in the parameter bank (used as a
+// constant operand) instead of being hoisted into registers, which keeps the register count
+// low enough for 4 (K <= 3) or 2 (K = 4) resident blocks per SM — the memory-level
+// parallelism an HBM-streaming pass needs.  Loads and stores are evict-first (__ldcs /
+// __stcs): the register is touched once per pass.
 template <typename T, int K>
-__global__ void __launch_bounds__(kThreads) k_dense_reg(vec2_t<T>* __restrict__ s, uint64_t n_groups,
-                                                         const __grid_constant__ DenseArgs<T, K> a) {
+__global__ void __launch_bounds__(kThreads, (K <= 3 ? 4 : 2))
+    k_dense_reg(vec2_t<T>* __restrict__ s, uint64_t n_groups, const __grid_constant__ DenseArgs<T, K> a) {
     constexpr int D = 1 << K;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_groups; g += stride) {
-        const uint64_t base = insert_zeros(g, a.pos, K);
-        vec2_t<T> in[D];
+    const uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n_groups) return;
+    const uint64_t base = insert_zeros(g, a.pos, K);
+    vec2_t<T> in[D];
 #pragma unroll
-        for (int l = 0; l < D; ++l) in[l] = s[base | a.off[l]];
+    for (int l = 0; l < D; ++l) in[l] = __ldcs(s + (base | a.off[l]));
 #pragma unroll
-        for (int y = 0; y < D; ++y) {
-            vec2_t<T> acc = cmul<T>(a.m[y * D], in[0]);
+    for (int y = 0; y < D; ++y) {
+        vec2_t<T> acc = cmul<T>(a.m[y * D], in[0]);
 #pragma unroll
-            for (int x = 1; x < D; ++x) acc = cfma<T>(a.m[y * D + x], in[x], acc);
-            s[base | a.off[y]] = acc;
-        }
+        for (int x = 1; x < D; ++x) acc = cfma<T>(a.m[y * D + x], in[x], acc);
+        __stcs(s + (base | a.off[y]), acc);
     }
 }
 
@@ -223,7 +227,8 @@ void launch_dense_reg(const Op& op, vec2_t<T>* s, int n, cudaStream_t st) {
     }
     for (int e = 0; e < (1 << (2 * K)); ++e) a.m[e] = to_c<T>(op.m[e]);
     const uint64_t groups = (1ull << n) >> K;
-    k_dense_reg<T, K><<<grid_for(groups, 1, 1u << 20), kThreads, 0, st>>>(s, groups, a);
+    const uint64_t blocks = (groups + kThreads - 1) / kThreads;
+    k_dense_reg<T, K><<<static_cast<unsigned>(blocks), kThreads, 0, st>>>(s, groups, a);
 }
 
 }  // namespace

@@ -1,0 +1,399 @@
+// kern_tile.cu — the tiled executor's pass kernel (see tile.h).
+//
+// One launch per pass.  Each CTA loops over tiles: it loads the tile's 2^m amplitudes
+// (contiguous runs of 2^c, coalesced, evict-first) into shared memory, applies every op of
+// the pass there with a __syncthreads() between ops, and stores the tile back.  Several
+// CTAs per SM overlap one CTA's loads with another's arithmetic.  Diagonal factors on
+// qubits outside the tile, and controls outside it, are constants of the tile's base index.
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "tile.h"
+
+namespace qsv {
+
+namespace {
+
+constexpr int kTileThreads = 256;
+constexpr int kTileCoefMax = 256;   // widest op: a 4-qubit dense block or an 8-qubit diagonal
+
+enum : uint8_t { T_DENSE = 1, T_DIAG, T_PHASE, T_CTRL1, T_SWAP, T_PAULI, T_SCALE };
+
+struct TileOpDev {
+    uint8_t kind, k, nlz, pad0;
+    uint32_t coef;          // offset into the coefficient array
+    uint32_t ncoef;         // coefficients of this op (staged in shared memory before use)
+    uint32_t pad1;
+    uint8_t lpos[8];        // local bit of op-local bit b (0xff: outside the tile)
+    uint8_t gq[8];          // global qubit of op-local bit b (DIAG)
+    uint64_t lmask;         // PHASE/CTRL1 local controls; PAULI local x mask
+    uint64_t gmask;         // PHASE/CTRL1 controls outside the tile (global bits)
+    uint64_t lz;            // PAULI local z mask
+    uint64_t gz;            // PAULI z bits outside the tile (global)
+};
+
+struct TilePassDev {
+    uint32_t op_begin, op_end;
+    int32_t m;
+    uint8_t tq[16];         // global qubit of local bit j, ascending
+};
+
+__device__ __forceinline__ uint32_t ins_zero32(uint32_t g, uint32_t p) {
+    const uint32_t low = g & ((1u << p) - 1u);
+    return ((g >> p) << (p + 1)) | low;
+}
+
+template <typename T>
+__device__ __forceinline__ vec2_t<T> ldc(const cplx<T>* p) {
+    const cplx<T> c = *p;
+    return mk<T>(c.re, c.im);
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void tile_dense(vec2_t<T>* tile, int m, const TileOpDev& op, const cplx<T>* coef) {
+    constexpr int D = 1 << K;
+    uint32_t loff[D];
+    uint8_t sp[K];
+#pragma unroll
+    for (int x = 0; x < D; ++x) {
+        uint32_t o = 0;
+#pragma unroll
+        for (int b = 0; b < K; ++b) if ((x >> b) & 1) o |= 1u << op.lpos[b];
+        loff[x] = o;
+    }
+#pragma unroll
+    for (int b = 0; b < K; ++b) sp[b] = op.lpos[b];
+    // ascending positions for zero insertion
+#pragma unroll
+    for (int a = 0; a < K; ++a)
+#pragma unroll
+        for (int b = a + 1; b < K; ++b)
+            if (sp[b] < sp[a]) { const uint8_t t = sp[a]; sp[a] = sp[b]; sp[b] = t; }
+    const cplx<T>* mat = coef;
+    const uint32_t groups = 1u << (m - K);
+    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
+        uint32_t b0 = g;
+#pragma unroll
+        for (int b = 0; b < K; ++b) b0 = ins_zero32(b0, sp[b]);
+        vec2_t<T> in[D];
+#pragma unroll
+        for (int x = 0; x < D; ++x) in[x] = tile[b0 | loff[x]];
+#pragma unroll
+        for (int y = 0; y < D; ++y) {
+            vec2_t<T> acc = cmul<T>(mat[y * D], in[0]);
+#pragma unroll
+            for (int x = 1; x < D; ++x) acc = cfma<T>(mat[y * D + x], in[x], acc);
+            tile[b0 | loff[y]] = acc;
+        }
+    }
+}
+
+template <typename T>
+__device__ void tile_op(vec2_t<T>* tile, int m, uint64_t base, const TileOpDev& op, const cplx<T>* coef) {
+    const uint32_t M = 1u << m;
+    switch (op.kind) {
+        case T_DENSE:
+            switch (op.k) {
+                case 1: tile_dense<T, 1>(tile, m, op, coef); break;
+                case 2: tile_dense<T, 2>(tile, m, op, coef); break;
+                case 3: tile_dense<T, 3>(tile, m, op, coef); break;
+                default: tile_dense<T, 4>(tile, m, op, coef); break;
+            }
+            return;
+        case T_DIAG: {
+            uint32_t idx_out = 0;
+            for (int b = 0; b < op.k; ++b)
+                if (op.lpos[b] == 0xff) idx_out |= static_cast<uint32_t>((base >> op.gq[b]) & 1ull) << b;
+            const cplx<T>* d = coef;
+            for (uint32_t l = threadIdx.x; l < M; l += blockDim.x) {
+                uint32_t idx = idx_out;
+                for (int b = 0; b < op.k; ++b)
+                    if (op.lpos[b] != 0xff) idx |= ((l >> op.lpos[b]) & 1u) << b;
+                tile[l] = cmul<T>(d[idx], tile[l]);
+            }
+            return;
+        }
+        case T_PHASE: {
+            if ((base & op.gmask) != op.gmask) return;
+            const cplx<T> ph = coef[0];
+            const int nb = __popcll(op.lmask);
+            const uint32_t cnt = M >> nb;
+            for (uint32_t g = threadIdx.x; g < cnt; g += blockDim.x) {
+                uint32_t l = g;
+                uint64_t msk = op.lmask;
+                while (msk) {
+                    const uint32_t p = __ffsll(static_cast<long long>(msk)) - 1;
+                    msk &= msk - 1;
+                    l = ins_zero32(l, p) | (1u << p);
+                }
+                tile[l] = cmul<T>(ph, tile[l]);
+            }
+            return;
+        }
+        case T_CTRL1: {
+            if ((base & op.gmask) != op.gmask) return;
+            const cplx<T> m0 = coef[0], m1 = coef[1], m2 = coef[2], m3 = coef[3];
+            const uint32_t tb = 1u << op.lpos[0];
+            const uint64_t all = op.lmask | tb;
+            const int nb = __popcll(all);
+            const uint32_t cnt = M >> nb;
+            for (uint32_t g = threadIdx.x; g < cnt; g += blockDim.x) {
+                uint32_t l = g;
+                uint64_t msk = all;
+                while (msk) {
+                    const uint32_t p = __ffsll(static_cast<long long>(msk)) - 1;
+                    msk &= msk - 1;
+                    l = ins_zero32(l, p) | (((op.lmask >> p) & 1ull) ? (1u << p) : 0u);
+                }
+                const vec2_t<T> a0 = tile[l], a1 = tile[l | tb];
+                tile[l] = cfma<T>(m1, a1, cmul<T>(m0, a0));
+                tile[l | tb] = cfma<T>(m3, a1, cmul<T>(m2, a0));
+            }
+            return;
+        }
+        case T_SWAP: {
+            const uint32_t pa = op.lpos[0], pb = op.lpos[1];
+            const uint32_t lo = min(pa, pb), hi = max(pa, pb);
+            const uint32_t cnt = M >> 2;
+            for (uint32_t g = threadIdx.x; g < cnt; g += blockDim.x) {
+                const uint32_t l = ins_zero32(ins_zero32(g, lo), hi);
+                const vec2_t<T> x = tile[l | (1u << pa)], y = tile[l | (1u << pb)];
+                tile[l | (1u << pa)] = y;
+                tile[l | (1u << pb)] = x;
+            }
+            return;
+        }
+        case T_PAULI: {
+            const cplx<T> cs = coef[0];    // (cos, sin)
+            const int ny = op.nlz;               // number of Y factors
+            const int gpar = __popcll(base & op.gz) & 1;
+            const uint32_t x = static_cast<uint32_t>(op.lmask), z = static_cast<uint32_t>(op.lz);
+            const uint32_t pivot = __ffs(x) - 1;
+            const uint32_t cnt = M >> 1;
+            for (uint32_t g = threadIdx.x; g < cnt; g += blockDim.x) {
+                const uint32_t i = ins_zero32(g, pivot), j = i ^ x;
+                const vec2_t<T> ai = tile[i], aj = tile[j];
+                auto rot = [&](uint32_t idx, vec2_t<T> a) {
+                    const int e = (ny + 2 * ((__popc(idx & z) + gpar) & 1) + 3) & 3;
+                    switch (e) {
+                        case 0: return a;
+                        case 1: return mk<T>(-a.y, a.x);
+                        case 2: return mk<T>(-a.x, -a.y);
+                        default: return mk<T>(a.y, -a.x);
+                    }
+                };
+                const vec2_t<T> pj = rot(j, aj), pi = rot(i, ai);
+                tile[i] = mk<T>(cs.re * ai.x + cs.im * pj.x, cs.re * ai.y + cs.im * pj.y);
+                tile[j] = mk<T>(cs.re * aj.x + cs.im * pi.x, cs.re * aj.y + cs.im * pi.y);
+            }
+            return;
+        }
+        case T_SCALE: {
+            const cplx<T> f = coef[0];
+            for (uint32_t l = threadIdx.x; l < M; l += blockDim.x) tile[l] = cmul<T>(f, tile[l]);
+            return;
+        }
+        default:
+            return;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTileThreads) k_tile_pass(vec2_t<T>* __restrict__ s, int n,
+                                                            const TilePassDev* __restrict__ passes, int pass_idx,
+                                                            const TileOpDev* __restrict__ ops,
+                                                            const cplx<T>* __restrict__ coef) {
+    extern __shared__ unsigned char smem_raw[];
+    vec2_t<T>* tile = reinterpret_cast<vec2_t<T>*>(smem_raw);
+    const TilePassDev P = passes[pass_idx];
+    const int m = P.m;
+    const uint32_t M = 1u << m;
+    cplx<T>* scoef = reinterpret_cast<cplx<T>*>(smem_raw + M * sizeof(vec2_t<T>));
+    const uint64_t n_tiles = 1ull << (n - m);
+    // deposit of the thread's low local bits (tid covers local bits 0..7)
+    uint64_t dep_lo = 0;
+    for (int j = 0; j < 8 && j < m; ++j)
+        if ((threadIdx.x >> j) & 1u) dep_lo |= 1ull << P.tq[j];
+    const uint32_t reps = M / kTileThreads;
+    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        // base: insert a zero at every tile qubit position (ascending)
+        uint64_t base = t;
+        for (int j = 0; j < m; ++j) {
+            const uint64_t p = P.tq[j];
+            base = ((base >> p) << (p + 1)) | (base & ((1ull << p) - 1ull));
+        }
+        for (uint32_t r = 0; r < reps; ++r) {
+            uint64_t dep = dep_lo;
+            for (int j = 8; j < m; ++j)
+                if ((r >> (j - 8)) & 1u) dep |= 1ull << P.tq[j];
+            tile[threadIdx.x + r * kTileThreads] = __ldcs(s + (base | dep));
+        }
+        __syncthreads();
+        for (uint32_t o = P.op_begin; o < P.op_end; ++o) {
+            const TileOpDev& op = ops[o];
+            // stage the op's coefficients next to the tile: reads inside the group loops then
+            // cannot be hoisted past the tile stores (same address space), so the matrix is
+            // not pinned in registers
+            for (uint32_t e = threadIdx.x; e < op.ncoef; e += blockDim.x) scoef[e] = coef[op.coef + e];
+            __syncthreads();
+            tile_op<T>(tile, m, base, op, scoef);
+            __syncthreads();
+        }
+        for (uint32_t r = 0; r < reps; ++r) {
+            uint64_t dep = dep_lo;
+            for (int j = 8; j < m; ++j)
+                if ((r >> (j - 8)) & 1u) dep |= 1ull << P.tq[j];
+            __stcs(s + (base | dep), tile[threadIdx.x + r * kTileThreads]);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+int tile_blocks_per_sm(int m) {
+    const size_t bytes = (size_t{1} << m) * sizeof(vec2_t<T>) + kTileCoefMax * sizeof(cplx<T>);
+    const size_t per_sm = 227 * 1024;
+    int b = static_cast<int>(per_sm / (bytes + 1024));
+    return std::max(1, std::min(b, 8));
+}
+
+}  // namespace
+
+// Encode the passes for the device and launch them in order on `st`.
+template <typename T>
+void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
+               const std::function<void(const Op&)>& stream_op) {
+    std::vector<TilePassDev> pdev;
+    std::vector<TileOpDev> odev;
+    std::vector<cplx<T>> cdev;
+    for (const TilePass& p : passes) {
+        if (p.tile_qubits.empty()) continue;
+        TilePassDev pd{};
+        pd.m = static_cast<int32_t>(p.tile_qubits.size());
+        for (size_t j = 0; j < p.tile_qubits.size(); ++j) pd.tq[j] = static_cast<uint8_t>(p.tile_qubits[j]);
+        int local_of[64];
+        for (int q = 0; q < 64; ++q) local_of[q] = -1;
+        for (size_t j = 0; j < p.tile_qubits.size(); ++j) local_of[p.tile_qubits[j]] = static_cast<int>(j);
+        auto lmask_of = [&](uint64_t gm, uint64_t* outside) {
+            uint64_t lm = 0, out = 0;
+            for (int q = 0; q < 64; ++q)
+                if ((gm >> q) & 1) {
+                    if (local_of[q] >= 0) lm |= 1ull << local_of[q];
+                    else out |= 1ull << q;
+                }
+            if (outside) *outside = out;
+            return lm;
+        };
+        pd.op_begin = static_cast<uint32_t>(odev.size());
+        for (const Op& o : p.ops) {
+            // every qubit the kernel addresses as a local bit must be a tile qubit: a planner
+            // mistake becomes a host error here, never an out-of-range shared-memory index
+            const uint64_t mix = op_mixing_mask(o);
+            for (int q = 0; q < 64; ++q)
+                if (((mix >> q) & 1) && (q >= n || local_of[q] < 0))
+                    throw std::logic_error("tile planner placed an op whose qubit " + std::to_string(q) +
+                                           " is outside its tile");
+            if (o.kind == OP_DENSE && o.k > 4) throw std::logic_error("dense block too wide for a tile");
+            if (o.kind == OP_DIAG && o.k > 8) throw std::logic_error("diagonal too wide for a tile");
+            TileOpDev d{};
+            std::memset(d.lpos, 0xff, sizeof d.lpos);
+            d.coef = static_cast<uint32_t>(cdev.size());
+            d.k = static_cast<uint8_t>(o.k);
+            auto push = [&](c128 v) { cdev.push_back(cplx<T>{static_cast<T>(v.real()), static_cast<T>(v.imag())}); };
+            switch (o.kind) {
+                case OP_DENSE:
+                    d.kind = T_DENSE;
+                    for (int b = 0; b < o.k; ++b) d.lpos[b] = static_cast<uint8_t>(local_of[o.qubits[b]]);
+                    for (const c128& v : o.m) push(v);
+                    break;
+                case OP_DIAG:
+                    d.kind = T_DIAG;
+                    for (int b = 0; b < o.k; ++b) {
+                        d.gq[b] = static_cast<uint8_t>(o.qubits[b]);
+                        d.lpos[b] = local_of[o.qubits[b]] >= 0 ? static_cast<uint8_t>(local_of[o.qubits[b]]) : 0xff;
+                    }
+                    for (const c128& v : o.m) push(v);
+                    break;
+                case OP_PHASE:
+                    d.kind = T_PHASE;
+                    d.lmask = lmask_of(o.mask, &d.gmask);
+                    push(o.m[0]);
+                    break;
+                case OP_CTRL1:
+                    d.kind = T_CTRL1;
+                    d.lmask = lmask_of(o.mask, &d.gmask);
+                    d.lpos[0] = static_cast<uint8_t>(local_of[o.target]);
+                    for (int e = 0; e < 4; ++e) push(o.m[e]);
+                    break;
+                case OP_SWAP:
+                    d.kind = T_SWAP;
+                    d.lpos[0] = static_cast<uint8_t>(local_of[o.qubits[0]]);
+                    d.lpos[1] = static_cast<uint8_t>(local_of[o.qubits[1]]);
+                    break;
+                case OP_PAULI_ROT:
+                    d.kind = T_PAULI;
+                    d.lmask = lmask_of(o.mask, nullptr);
+                    d.lz = lmask_of(o.zmask, &d.gz);
+                    d.nlz = static_cast<uint8_t>(__builtin_popcountll(o.mask & o.zmask) & 3);
+                    push(o.m[0]);
+                    break;
+                case OP_SCALE:
+                    d.kind = T_SCALE;
+                    push(o.m[0]);
+                    break;
+                default:
+                    continue;
+            }
+            d.ncoef = static_cast<uint32_t>(cdev.size()) - d.coef;
+            odev.push_back(d);
+        }
+        pd.op_end = static_cast<uint32_t>(odev.size());
+        pdev.push_back(pd);
+    }
+    // one upload of every descriptor and coefficient of this apply call
+    const size_t a_p = 0;
+    const size_t a_o = (pdev.size() * sizeof(TilePassDev) + 255) & ~size_t{255};
+    const size_t a_c = a_o + ((odev.size() * sizeof(TileOpDev) + 255) & ~size_t{255});
+    const size_t total = a_c + cdev.size() * sizeof(cplx<T>) + 256;
+    std::vector<uint8_t> host(total, 0);
+    if (!pdev.empty()) std::memcpy(host.data() + a_p, pdev.data(), pdev.size() * sizeof(TilePassDev));
+    if (!odev.empty()) std::memcpy(host.data() + a_o, odev.data(), odev.size() * sizeof(TileOpDev));
+    if (!cdev.empty()) std::memcpy(host.data() + a_c, cdev.data(), cdev.size() * sizeof(cplx<T>));
+    check_cuda(cudaStreamSynchronize(st), "tile descriptor reuse");
+    uint8_t* dev = static_cast<uint8_t*>(ws.tiles(total));
+    check_cuda(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, st), "tile descriptors");
+    const TilePassDev* d_p = reinterpret_cast<const TilePassDev*>(dev + a_p);
+    const TileOpDev* d_o = reinterpret_cast<const TileOpDev*>(dev + a_o);
+    const cplx<T>* d_c = reinterpret_cast<const cplx<T>*>(dev + a_c);
+    int sms = 0, device = 0;
+    check_cuda(cudaGetDevice(&device), "device");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
+    int pi = 0;
+    for (const TilePass& p : passes) {
+        if (p.tile_qubits.empty()) {
+            for (const Op& o : p.ops) stream_op(o);
+            continue;
+        }
+        const int m = static_cast<int>(p.tile_qubits.size());
+        const size_t smem = (size_t{1} << m) * sizeof(vec2_t<T>) + kTileCoefMax * sizeof(cplx<T>);
+        check_cuda(cudaFuncSetAttribute(k_tile_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)), "tile smem");
+        const uint64_t n_tiles = 1ull << (n - m);
+        const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sms) * tile_blocks_per_sm<T>(m));
+        k_tile_pass<T><<<static_cast<unsigned>(grid), kTileThreads, smem, st>>>(s, n, d_p, pi, d_o, d_c);
+        check_cuda(cudaGetLastError(), "tile pass launch");
+        ++pi;
+    }
+    // `host` is pageable: cudaMemcpyAsync returned only after staging it, so it may go now
+}
+
+template void run_tiled<double>(const std::vector<TilePass>&, double2*, int, cudaStream_t, Workspace&,
+                                const std::function<void(const Op&)>&);
+template void run_tiled<float>(const std::vector<TilePass>&, float2*, int, cudaStream_t, Workspace&,
+                               const std::function<void(const Op&)>&);
+
+}  // namespace qsv

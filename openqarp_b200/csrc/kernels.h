@@ -4,12 +4,14 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "lower.h"
 #include "qsv_common.cuh"
+#include "tile.h"
 
 namespace qsv {
 
@@ -31,6 +33,7 @@ public:
     void* state_copy(size_t bytes) { return grow(copy_, copy_cap_, bytes); }
     void* scratch(size_t bytes) { return grow(scr_, scr_cap_, bytes); }
     void* shots(size_t bytes) { return grow(shot_, shot_cap_, bytes); }
+    void* tiles(size_t bytes) { return grow(tile_, tile_cap_, bytes); }
     // pinned host staging for small results
     double* host_result(size_t n_doubles);
 
@@ -40,6 +43,7 @@ private:
     void* copy_ = nullptr; size_t copy_cap_ = 0;
     void* scr_ = nullptr; size_t scr_cap_ = 0;
     void* shot_ = nullptr; size_t shot_cap_ = 0;
+    void* tile_ = nullptr; size_t tile_cap_ = 0;
     double* host_ = nullptr; size_t host_cap_ = 0;
 };
 
@@ -47,6 +51,12 @@ private:
 template <typename T>
 void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
 uint64_t op_bytes(const Op& op, int n, int amp_bytes);
+
+// ---------------------------------------------------------------- tiled executor (kern_tile.cu)
+// Launch the planned passes; one-op stream passes (empty tile_qubits) go to `stream_op`.
+template <typename T>
+void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
+               const std::function<void(const Op&)>& stream_op);
 
 // ---------------------------------------------------------------- reductions (kern_reduce.cu)
 

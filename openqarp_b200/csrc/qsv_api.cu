@@ -31,6 +31,7 @@ struct Handle {
     int fusion_max = 3;
     int fusion_min = 12;
     int executor = -1;
+    int tile_qubits = 0;          // 0: default_tile_qubits
     qsv_stats_t stats{};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     void* aux = nullptr;          // second register (adjoint's |phi>)
@@ -128,6 +129,15 @@ void check_stream(const std::vector<Cmd>& cmds) {
     }
 }
 
+// Executor choice: 1 = tiled, 0 = stream, -1 = tiled from 16 qubits (registers beyond L2,
+// where HBM passes dominate).  Tiles need at least kTileMinQubits qubits.
+bool use_tiled(const Handle* h) {
+    if (h->n < kTileMinQubits) return false;
+    if (h->executor == 1) return true;
+    if (h->executor == 0) return false;
+    return h->n >= 16;
+}
+
 void apply_stream(Handle* h, const uint8_t* buf, size_t nbytes, bool fuse) {
     std::vector<Cmd> cmds = decode(buf, nbytes);
     check_stream(cmds);
@@ -137,7 +147,24 @@ void apply_stream(Handle* h, const uint8_t* buf, size_t nbytes, bool fuse) {
     for (const Cmd& c : cmds)
         for (Op& o : lower(c, h->n)) ops.push_back(std::move(o));
     check_cuda(cudaEventRecord(h->e0, h->stream), "event");
-    for (const Op& o : ops) launch(h, o, h->state);
+    if (fuse && use_tiled(h)) {
+        const int m = h->tile_qubits > 0 ? std::min(h->tile_qubits, h->n)
+                                         : default_tile_qubits(h->n, static_cast<int>(h->amp_bytes()));
+        const std::vector<TilePass> passes = plan_tiles(ops, h->n, m);
+        auto stream_op = [h](const Op& o) { launch(h, o, h->state); };
+        if (h->dtype == QSV_C128) run_tiled<double>(passes, S128(h), h->n, h->stream, h->ws, stream_op);
+        else run_tiled<float>(passes, S64(h), h->n, h->stream, h->ws, stream_op);
+        for (const TilePass& p : passes) {
+            if (p.tile_qubits.empty()) continue;   // counted by launch()
+            h->stats.launches++;
+            h->stats.passes++;
+            h->stats.hbm_bytes += 2ull * h->dim() * h->amp_bytes();
+            for (const Op& o : p.ops)
+                if (o.kind == OP_DENSE && o.k >= 2) h->stats.fused_blocks++;
+        }
+    } else {
+        for (const Op& o : ops) launch(h, o, h->state);
+    }
     check_cuda(cudaEventRecord(h->e1, h->stream), "event");
 }
 
@@ -256,6 +283,18 @@ int qsv_set_executor(void* hp, int mode) {
         Handle* h = H_(hp);
         if (mode < -1 || mode > 1) throw std::invalid_argument("executor mode must be -1, 0 or 1");
         h->executor = mode;
+    });
+}
+
+int qsv_set_tile_qubits(void* hp, int m) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (m != 0 && (m < kTileMinQubits || m > kTileMaxQubits))
+            throw std::invalid_argument("tile qubits must be 0 (default) or in [" + std::to_string(kTileMinQubits) +
+                                        ", " + std::to_string(kTileMaxQubits) + "]");
+        if (m > 12 && h->dtype == QSV_C128)
+            throw std::invalid_argument("complex128 tiles hold at most 12 qubits");
+        h->tile_qubits = m;
     });
 }
 

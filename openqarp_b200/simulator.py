@@ -92,9 +92,12 @@ class Register:
     def copy_from(self, other: "Register"):
         check(lib.qsv_copy_state(self.handle, other.handle))
 
-    def configure(self, fusion_max: int, fusion_min: int, executor: int = -1):
+    def configure(self, fusion_max: int, fusion_min: int, executor: int = -1, tile_qubits: int = 0):
+        """Fusion knobs (fusion_max_qubits / fusion_min_qubits), executor (0 = one HBM pass per
+        fused block, 1 = tiled passes in shared memory, -1 = tiled from 16 qubits) and tile width."""
         check(lib.qsv_set_fusion(self.handle, int(fusion_max), int(fusion_min)))
         check(lib.qsv_set_executor(self.handle, int(executor)))
+        check(lib.qsv_set_tile_qubits(self.handle, int(tile_qubits)))
 
     # gates ---------------------------------------------------------------------------
     def apply(self, stream, fused: bool = True):

@@ -143,6 +143,74 @@ def test_deterministic_bitwise():
     assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
 
 
+# ---------------------------------------------------------------- tiled executor
+
+def mixed_circuits(n):
+    """Every gate kind (controls and diagonals inside and outside tiles), brickwork, HEA,
+    Heisenberg Trotter, QAOA."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from gen_golden import all_gates_circuit
+    rng = np.random.default_rng(n)
+    hea_c, hea_v, _ = circuits.hea(n, 3, seed=2)
+    hea_c = [Command(c.gate, c.qubits, tuple(p.evaluate(hea_v) for p in c.params)) for c in hea_c]
+    edges = circuits.random_regular_graph(3, n, seed=1)
+    q_c, q_names, _ = circuits.qaoa_maxcut(n, edges, 2)
+    q_v = dict(zip(q_names, rng.uniform(0, np.pi, len(q_names))))
+    q_c = [Command(c.gate, c.qubits, tuple(p.evaluate(q_v) if hasattr(p, "evaluate") else p
+                                           for p in c.params)) for c in q_c]
+    big = [custom(tuple(int(q) for q in rng.permutation(n)[:6]), random_unitary(6, rng))]
+    return {
+        "allgates": all_gates_circuit(n, 5) + all_gates_circuit(n, 6),
+        "brickwork": circuits.brickwork(n, 6, seed=3),
+        "hea": hea_c,
+        "heisenberg": circuits.heisenberg_trotter(n, 2, 0.1, rng.uniform(-1, 1, n)),
+        "qaoa": q_c,
+        "wide_block_inside": circuits.brickwork(n, 2, seed=4) + big + circuits.brickwork(n, 2, seed=5),
+    }
+
+
+@pytest.mark.parametrize("m", [8, 10, 12])
+def test_tiled_executor_matches_oracle(m, restatement):
+    n = 14
+    for name, cmds in mixed_circuits(n).items():
+        buf = ir.pack(cmds).buf
+        want = restatement.statevector(buf, n)
+        for k in (1, 2, 3, 4):
+            reg = Register(n)
+            reg.configure(k, 0, 1, m)
+            reg.apply(buf)
+            got = reg.get_state()
+            reg.close()
+            np.testing.assert_allclose(got, want, atol=AMP_TOL, rtol=0, err_msg=f"{name} k={k} m={m}")
+
+
+def test_tiled_executor_complex64(restatement):
+    n = 16
+    for name, cmds in mixed_circuits(n).items():
+        buf = ir.pack(cmds).buf
+        want = restatement.statevector(buf, n)
+        reg = Register(n, "complex64")
+        reg.configure(3, 0, 1, 13)
+        reg.apply(buf)
+        got = reg.get_state()
+        reg.close()
+        assert np.max(np.abs(got - want)) < 2e-5, name
+
+
+def test_tiled_and_stream_agree_at_24q():
+    n = 24
+    buf = ir.pack(circuits.brickwork(n, 10, seed=8)).buf
+    out = []
+    for executor in (0, 1):
+        reg = Register(n)
+        reg.configure(3, 12, executor)
+        reg.apply(buf)
+        out.append(reg.get_state())
+        reg.close()
+    assert np.max(np.abs(out[0] - out[1])) < AMP_TOL
+
+
 # ---------------------------------------------------------------- <H>
 
 def test_config1_hea_expectation_and_transition(golden, restatement, sim):
