@@ -291,6 +291,54 @@ def adjoint_vs_param_shift(device, shift_sample=12):
             "max_abs_diff_adjoint_vs_shift": err}
 
 
+def qaoa_batched(rank, world, device, dist, steps=3, sample=16):
+    """Config 4: 2048 QAOA MaxCut instances (n in 10..20 even, p in 1..4, 3-regular graphs),
+    <C> and adjoint gradients for all of them in one persistent graph-captured launch per GPU;
+    instances are LPT-sharded over ranks.  Compared with running the same instances one at a
+    time through the engine's generic per-circuit adjoint (a timed sample, scaled)."""
+    import torch
+    from openqarp_b200 import B200Simulator, circuits
+    from openqarp_b200.batch import QaoaBatch, config4_instances, partition_lpt
+    inst, params = config4_instances(2048, seed=SEED)
+    mine = partition_lpt([i.cost for i in inst], world)[rank]
+    batch = QaoaBatch([inst[i] for i in mine], device)
+    prm = [params[i] for i in mine]
+    batch.run(prm)
+    times = [batch.run(prm)[2] for _ in range(steps)]
+    energies, grads, _ = batch.run(prm)
+    batch.close()
+    ms = float(np.median(times))
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    out = {"instances": len(inst), "widths": "10..20 even", "depths": "1..4",
+           "ms_per_batch": ms, "instances_per_s": len(inst) / (ms * 1e-3),
+           "gradients": "adjoint, all 2p parameters of every instance",
+           "graph": "one CUDA graph: params H2D, queue reset, persistent kernel, results D2H"}
+    if rank == 0:
+        sim = B200Simulator(device=device)
+        rng = np.random.default_rng(SEED)
+        pick = rng.choice(len(mine), size=min(sample, len(mine)), replace=False)
+        t0 = time.perf_counter()
+        err = 0.0
+        for j in pick:
+            k = mine[int(j)]
+            cmds, names, cost = circuits.qaoa_maxcut(inst[k].n, inst[k].edges, inst[k].p)
+            e, g = sim.energy_and_gradient(cmds, inst[k].n, cost, dict(zip(names, params[k])), names)
+            err = max(err, abs(e - energies[int(j)]), float(np.max(np.abs(np.asarray(g) - grads[int(j)]))))
+        dt = (time.perf_counter() - t0) / len(pick)
+        sim.close()
+        est_ms = dt * 1e3 * len(inst) * (sum(i.cost for i in inst) / len(inst)) / \
+            (sum(inst[mine[int(j)]].cost for j in pick) / len(pick))
+        out.update({"per_circuit_engine_ms_est": est_ms,
+                    "speedup_vs_per_circuit": est_ms / (ms * world),
+                    "per_circuit_sample": f"{len(pick)} instances timed through B200Simulator.energy_and_gradient, "
+                                          "scaled by total cost",
+                    "max_abs_diff_vs_per_circuit": err})
+    return out
+
+
 # ---------------------------------------------------------------- arms
 
 def reference_arm(args, rank, world):
@@ -401,6 +449,10 @@ def b200_arm(args, rank, world, local_rank):
     e2e_s = float(np.median(e2e_times))
     e2e_value = world * work_bytes / e2e_s / 1e9
 
+    qaoa = None
+    if not args.skip_qaoa:
+        qaoa = qaoa_batched(rank, world, device, dist)
+
     result = None
     if rank == 0:
         cpu = None
@@ -414,6 +466,11 @@ def b200_arm(args, rank, world, local_rank):
         if not args.skip_adjoint:
             reg.close()
             adj = adjoint_vs_param_shift(device)
+        heis = None
+        if not args.skip_heisenberg:
+            reg.close()
+            from openqarp_b200.workloads import heisenberg_bulk
+            heis = heisenberg_bulk(n=31, steps=50, dt=0.05, seed=SEED, device=device)
         fp64_achieved = flops / (ms_step * 1e-3) / 1e12
         result = {
             "metric": "gate GB/s (%HBM peak) @28q", "value": value, "unit": "GB/s",
@@ -444,6 +501,8 @@ def b200_arm(args, rank, world, local_rank):
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "adjoint": adj,
+            "heisenberg31_c64_bulk": heis,
+            "qaoa_batched": qaoa,
         }
     else:
         reg.close()
@@ -458,6 +517,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--skip-heisenberg", action="store_true")
+    ap.add_argument("--skip-qaoa", action="store_true")
     ap.add_argument("--executor", type=int, default=None, choices=[0, 1],
                     help="pin the executor (0 stream, 1 tiled) instead of autotuning; needs --k")
     ap.add_argument("--k", type=int, default=None, help="pin the fusion width; needs --executor")

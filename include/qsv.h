@@ -205,6 +205,24 @@ QSV_API int qsv_scale(void* h, double scale);
 /* <a|b> in FP64 (fidelity against another handle of the same width; dtypes may differ). */
 QSV_API int qsv_inner(void* a, void* b, double out[2]);
 
+/* ---- batched QAOA MaxCut ----------------------------------------------------------- *
+ * Many instances of uneven width in one persistent, CUDA-graph-captured launch.  Replaces the
+ * serial per-circuit sweep the reference runs for a batch of parameter sets / circuits
+ * (QarpEngine._sweep, src/qarp/engines/_qarp_engine.py:450-503; QarpSimulator::
+ * batch_expectation / run_gradient per instance, qarp_simulator.cpp:971-984, 1519-1605).
+ * Instance i has n_qubits[i] qubits (2..24), depth[i] rounds, and the edges
+ * edges[2e], edges[2e+1] for e in [edge_ptr[i], edge_ptr[i+1]).  Its circuit is H on every
+ * qubit then, per round r, RZZ(2 gamma_r) on every edge and RX(2 beta_r) on every qubit;
+ * its cost is the cut size sum_e (1 - Z_u Z_v)/2.  Parameters and gradients are packed per
+ * instance in order (gamma_0, beta_0, gamma_1, beta_1, ...), instances back to back. */
+QSV_API int qsv_qaoa_create(int device, int n_instances, const int32_t* n_qubits, const int32_t* depth,
+                            const int32_t* edge_ptr, const int32_t* edges, void** out);
+/* energies[n_instances] <- <C>; with_gradient: grads (same layout as params) <- dE/dparams;
+ * device_ms (may be NULL) <- device time of the graph launch. */
+QSV_API int qsv_qaoa_run(void* q, const double* params, int with_gradient, double* energies,
+                         double* grads, double* device_ms);
+QSV_API int qsv_qaoa_destroy(void* q);
+
 /* ---- allocation-free variant ------------------------------------------------------- *
  * No counterpart in the reference: it exists for callers that cannot call cudaMalloc —
  * a process whose device memory is owned by its own pool allocator (PyTorch's caching

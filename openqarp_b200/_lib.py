@@ -64,6 +64,9 @@ def _load():
         "qsv_inner": (c_int, [c_void_p, c_void_p, PD]),
         "qsv_synchronize": (c_int, [c_void_p]),
         "qsv_stats": (c_int, [c_void_p, POINTER(Stats)]),
+        "qsv_qaoa_create": (c_int, [c_int, c_int, PI32, PI32, PI32, PI32, POINTER(c_void_p)]),
+        "qsv_qaoa_run": (c_int, [c_void_p, PD, c_int, PD, PD, PD]),
+        "qsv_qaoa_destroy": (c_int, [c_void_p]),
         "qsv_transition_static": (c_int, [c_void_p, c_void_p, c_int, c_int, PU64, PU64, PD, c_size_t,
                                           c_void_p, PD]),
     }
@@ -82,6 +85,7 @@ DECLARED = (
     "qsv_copy_state", "qsv_fuse_count", "qsv_apply", "qsv_apply_unfused", "qsv_transition", "qsv_sample",
     "qsv_sample_seeded", "qsv_uniforms", "qsv_adjoint", "qsv_adjoint_phi", "qsv_norm2",
     "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_transition_static",
+    "qsv_qaoa_create", "qsv_qaoa_run", "qsv_qaoa_destroy",
 )
 STATIC_MAX_TERMS = 4096
 

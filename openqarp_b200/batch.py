@@ -1,0 +1,141 @@
+"""Batched QAOA MaxCut: many instances of uneven width, one persistent graph-captured launch.
+
+``QaoaBatch`` wraps qsv_qaoa_create / qsv_qaoa_run (include/qsv.h).  Each instance is the
+circuit ``circuits.qaoa_maxcut`` emits — H on every qubit, then per round RZZ(2 gamma) on every
+edge and RX(2 beta) on every qubit — with cost sum_e (1 - Z_u Z_v)/2; ``run`` returns <C> for
+every instance and, optionally, the adjoint gradient of every gamma and beta.
+
+For several GPUs the instances are partitioned by cost (2^n x rounds, longest first onto the
+least-loaded rank) with no data-path collective; ranks gather their results at the end.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib, circuits
+from ._lib import check, dptr, i32ptr, lib
+
+
+@dataclass
+class QaoaInstance:
+    n: int
+    p: int
+    edges: list
+
+    @property
+    def cost(self) -> float:
+        return float(2 ** self.n) * (4 * self.p + 1)
+
+
+def config4_instances(count: int = 2048, seed: int = 1234, widths=(10, 12, 14, 16, 18, 20),
+                      depths=(1, 2, 3, 4)):
+    """Seeded instances of the batched-QAOA configuration: width uniform over the even
+    counts 10..20, depth uniform 1..4, a random 3-regular graph each, and gamma, beta uniform
+    on [0, pi).  Returns (instances, params) with params[i] = [g0, b0, g1, b1, ...]."""
+    rng = np.random.default_rng(seed)
+    inst, params = [], []
+    for i in range(count):
+        n = int(rng.choice(widths))
+        p = int(rng.choice(depths))
+        edges = circuits.random_regular_graph(3, n, seed=int(rng.integers(1 << 31)))
+        inst.append(QaoaInstance(n, p, edges))
+        params.append(rng.uniform(0.0, np.pi, 2 * p))
+    return inst, params
+
+
+class QaoaBatch:
+    def __init__(self, instances: Sequence[QaoaInstance], device: int = 0):
+        self.instances = list(instances)
+        self.device = int(device)
+        n = np.asarray([i.n for i in self.instances], dtype=np.int32)
+        p = np.asarray([i.p for i in self.instances], dtype=np.int32)
+        ptr = np.zeros(len(self.instances) + 1, dtype=np.int32)
+        flat = []
+        for k, inst in enumerate(self.instances):
+            ptr[k + 1] = ptr[k] + len(inst.edges)
+            for u, v in inst.edges:
+                flat += [int(u), int(v)]
+        edges = np.asarray(flat if flat else [0, 0], dtype=np.int32)
+        self._offsets = np.concatenate([[0], np.cumsum(2 * p)]).astype(np.int64)
+        h = ctypes.c_void_p()
+        check(lib.qsv_qaoa_create(self.device, len(self.instances), i32ptr(n), i32ptr(p), i32ptr(ptr),
+                                  i32ptr(edges), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.qsv_qaoa_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def run(self, params: Sequence[np.ndarray], with_gradient: bool = True):
+        """Returns (energies [n_instances], grads [list of arrays] or None, device ms)."""
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float64) for x in params]))
+        if flat.shape[0] != self._offsets[-1]:
+            raise ValueError(f"expected {int(self._offsets[-1])} parameters, got {flat.shape[0]}")
+        energies = np.zeros(len(self.instances))
+        grads = np.zeros(max(flat.shape[0], 1))
+        ms = ctypes.c_double()
+        check(lib.qsv_qaoa_run(self._h, dptr(flat), 1 if with_gradient else 0, dptr(energies), dptr(grads),
+                               ctypes.byref(ms)))
+        g = None
+        if with_gradient:
+            g = [grads[self._offsets[k]:self._offsets[k + 1]].copy() for k in range(len(self.instances))]
+        return energies, g, ms.value
+
+
+def partition_lpt(costs: Sequence[float], world: int) -> list:
+    """Longest-processing-time partition: instances in descending cost, each to the rank with
+    the least load so far.  Returns one index list per rank (each in ascending order)."""
+    loads = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: -costs[k]):
+        r = min(range(world), key=lambda k: (loads[k], k))
+        parts[r].append(i)
+        loads[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def run_sharded(instances, params, rank: int, world: int, device: int, runner=None, dist=None,
+                with_gradient: bool = True):
+    """Run this rank's share of the batch and gather every instance's result on every rank.
+
+    ``runner(instances, params) -> (energies, grads, ms)`` defaults to a QaoaBatch on
+    ``device``; ``dist`` is torch.distributed (any backend; None for a single process).
+    Returns (energies, grads, max device ms over ranks, this rank's indices)."""
+    parts = partition_lpt([i.cost for i in instances], world)
+    mine = parts[rank]
+    if runner is None:
+        def runner(inst, prm):
+            b = QaoaBatch(inst, device)
+            try:
+                return b.run(prm, with_gradient)
+            finally:
+                b.close()
+    if mine:
+        e, g, ms = runner([instances[i] for i in mine], [params[i] for i in mine])
+    else:
+        e, g, ms = np.zeros(0), [], 0.0
+    local = {"idx": mine, "e": list(map(float, e)), "g": [list(map(float, x)) for x in (g or [])], "ms": ms}
+    if dist is None or world == 1:
+        gathered = [local]
+    else:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, local)
+    energies = np.zeros(len(instances))
+    grads: list = [None] * len(instances)
+    for part in gathered:
+        for j, i in enumerate(part["idx"]):
+            energies[i] = part["e"][j]
+            if part["g"]:
+                grads[i] = np.asarray(part["g"][j])
+    return energies, grads, max(p["ms"] for p in gathered), mine

@@ -18,7 +18,7 @@ namespace qsv {
 
 namespace {
 
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = 512;
 constexpr int kTileCoefMax = 256;   // widest op: a 4-qubit dense block or an 8-qubit diagonal
 
 enum : uint8_t { T_DENSE = 1, T_DIAG, T_PHASE, T_CTRL1, T_SWAP, T_PAULI, T_SCALE };
@@ -75,6 +75,9 @@ __device__ __forceinline__ void tile_dense(vec2_t<T>* tile, int m, const TileOpD
             if (sp[b] < sp[a]) { const uint8_t t = sp[a]; sp[a] = sp[b]; sp[b] = t; }
     const cplx<T>* mat = coef;
     const uint32_t groups = 1u << (m - K);
+    // outputs are accumulated YB at a time with the input index outermost, so consecutive
+    // FMAs belong to independent accumulators (2*YB chains) instead of one serial chain
+    constexpr int YB = D < 8 ? D : 8;
     for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
         uint32_t b0 = g;
 #pragma unroll
@@ -83,11 +86,16 @@ __device__ __forceinline__ void tile_dense(vec2_t<T>* tile, int m, const TileOpD
 #pragma unroll
         for (int x = 0; x < D; ++x) in[x] = tile[b0 | loff[x]];
 #pragma unroll
-        for (int y = 0; y < D; ++y) {
-            vec2_t<T> acc = cmul<T>(mat[y * D], in[0]);
+        for (int yb = 0; yb < D; yb += YB) {
+            vec2_t<T> acc[YB];
 #pragma unroll
-            for (int x = 1; x < D; ++x) acc = cfma<T>(mat[y * D + x], in[x], acc);
-            tile[b0 | loff[y]] = acc;
+            for (int y = 0; y < YB; ++y) acc[y] = cmul<T>(mat[(yb + y) * D], in[0]);
+#pragma unroll
+            for (int x = 1; x < D; ++x)
+#pragma unroll
+                for (int y = 0; y < YB; ++y) acc[y] = cfma<T>(mat[(yb + y) * D + x], in[x], acc[y]);
+#pragma unroll
+            for (int y = 0; y < YB; ++y) tile[b0 | loff[yb + y]] = acc[y];
         }
     }
 }
@@ -202,37 +210,69 @@ __device__ void tile_op(vec2_t<T>* tile, int m, uint64_t base, const TileOpDev& 
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// One persistent CTA per SM with two tile buffers: while the ops of tile t run on one buffer,
+// the 16-byte cp.async copies of tile t+G (G = grid size) land in the other, so HBM and the
+// FP64 pipes work at the same time.  A thread copies 16-byte chunks: one complex128
+// amplitude or two adjacent complex64 amplitudes (qubit 0 is always tile bit 0).
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads) k_tile_pass(vec2_t<T>* __restrict__ s, int n,
-                                                            const TilePassDev* __restrict__ passes, int pass_idx,
-                                                            const TileOpDev* __restrict__ ops,
-                                                            const cplx<T>* __restrict__ coef) {
-    extern __shared__ unsigned char smem_raw[];
-    vec2_t<T>* tile = reinterpret_cast<vec2_t<T>*>(smem_raw);
+__global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __restrict__ s, int n,
+                                                               const TilePassDev* __restrict__ passes, int pass_idx,
+                                                               const TileOpDev* __restrict__ ops,
+                                                               const cplx<T>* __restrict__ coef) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const TilePassDev P = passes[pass_idx];
     const int m = P.m;
     const uint32_t M = 1u << m;
-    cplx<T>* scoef = reinterpret_cast<cplx<T>*>(smem_raw + M * sizeof(vec2_t<T>));
-    const uint64_t n_tiles = 1ull << (n - m);
-    // deposit of the thread's low local bits (tid covers local bits 0..7)
+    vec2_t<T>* buf0 = reinterpret_cast<vec2_t<T>*>(smem_raw);
+    vec2_t<T>* buf1 = buf0 + M;
+    cplx<T>* scoef = reinterpret_cast<cplx<T>*>(buf1 + M);
+    constexpr int kAmpsPerChunk = 16 / sizeof(vec2_t<T>);
+    constexpr int acl = kAmpsPerChunk == 2 ? 1 : 0;
+    constexpr int hi_shift = 9 + acl;                 // log2(kTileThreads) + acl
+    const uint32_t R = M >> hi_shift;                  // chunks per thread per tile
+    const uint32_t lt = threadIdx.x << acl;            // this thread's local index within a row of chunks
     uint64_t dep_lo = 0;
-    for (int j = 0; j < 8 && j < m; ++j)
-        if ((threadIdx.x >> j) & 1u) dep_lo |= 1ull << P.tq[j];
-    const uint32_t reps = M / kTileThreads;
-    for (uint64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        // base: insert a zero at every tile qubit position (ascending)
-        uint64_t base = t;
+    for (int j = 0; j < hi_shift && j < m; ++j)
+        if ((lt >> j) & 1u) dep_lo |= 1ull << P.tq[j];
+    auto dep_hi = [&](uint32_t r) {
+        uint64_t d = 0;
+        for (int j = hi_shift; j < m; ++j)
+            if ((r >> (j - hi_shift)) & 1u) d |= 1ull << P.tq[j];
+        return d;
+    };
+    auto tile_base = [&](uint64_t t) {
+        uint64_t base = t;   // insert a zero at every tile qubit position (ascending)
         for (int j = 0; j < m; ++j) {
             const uint64_t p = P.tq[j];
             base = ((base >> p) << (p + 1)) | (base & ((1ull << p) - 1ull));
         }
-        for (uint32_t r = 0; r < reps; ++r) {
-            uint64_t dep = dep_lo;
-            for (int j = 8; j < m; ++j)
-                if ((r >> (j - 8)) & 1u) dep |= 1ull << P.tq[j];
-            tile[threadIdx.x + r * kTileThreads] = __ldcs(s + (base | dep));
-        }
-        __syncthreads();
+        return base;
+    };
+    auto issue = [&](vec2_t<T>* dst, uint64_t base) {
+        for (uint32_t r = 0; r < R; ++r)
+            cp_async16(dst + (lt + (r << hi_shift)), s + (base | dep_lo | dep_hi(r)));
+    };
+    const uint64_t n_tiles = 1ull << (n - m);
+    const uint64_t G = gridDim.x;
+    uint64_t t = blockIdx.x;
+    if (t < n_tiles) issue(buf0, tile_base(t));
+    cp_async_commit();
+    for (uint32_t i = 0; t < n_tiles; t += G, ++i) {
+        vec2_t<T>* cur = (i & 1u) ? buf1 : buf0;
+        vec2_t<T>* nxt = (i & 1u) ? buf0 : buf1;
+        if (t + G < n_tiles) issue(nxt, tile_base(t + G));
+        cp_async_commit();
+        cp_async_wait1();     // this thread's copies of tile t have landed
+        __syncthreads();      // ... and everybody else's
+        const uint64_t base = tile_base(t);
         for (uint32_t o = P.op_begin; o < P.op_end; ++o) {
             const TileOpDev& op = ops[o];
             // stage the op's coefficients next to the tile: reads inside the group loops then
@@ -240,25 +280,17 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_pass(vec2_t<T>* __restric
             // not pinned in registers
             for (uint32_t e = threadIdx.x; e < op.ncoef; e += blockDim.x) scoef[e] = coef[op.coef + e];
             __syncthreads();
-            tile_op<T>(tile, m, base, op, scoef);
+            tile_op<T>(cur, m, base, op, scoef);
             __syncthreads();
         }
-        for (uint32_t r = 0; r < reps; ++r) {
-            uint64_t dep = dep_lo;
-            for (int j = 8; j < m; ++j)
-                if ((r >> (j - 8)) & 1u) dep |= 1ull << P.tq[j];
-            __stcs(s + (base | dep), tile[threadIdx.x + r * kTileThreads]);
+        for (uint32_t r = 0; r < R; ++r) {
+            const uint32_t l = lt + (r << hi_shift);
+            const float4 v = *reinterpret_cast<const float4*>(cur + l);
+            __stcs(reinterpret_cast<float4*>(s + (base | dep_lo | dep_hi(r))), v);
         }
-        __syncthreads();
+        __syncthreads();      // the buffer is refilled two iterations from now
     }
-}
-
-template <typename T>
-int tile_blocks_per_sm(int m) {
-    const size_t bytes = (size_t{1} << m) * sizeof(vec2_t<T>) + kTileCoefMax * sizeof(cplx<T>);
-    const size_t per_sm = 227 * 1024;
-    int b = static_cast<int>(per_sm / (bytes + 1024));
-    return std::max(1, std::min(b, 8));
+    cp_async_wait0();
 }
 
 }  // namespace
@@ -379,11 +411,12 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
             continue;
         }
         const int m = static_cast<int>(p.tile_qubits.size());
-        const size_t smem = (size_t{1} << m) * sizeof(vec2_t<T>) + kTileCoefMax * sizeof(cplx<T>);
+        if (m < kTileMinQubits) throw std::logic_error("tile narrower than one chunk row per thread");
+        const size_t smem = 2 * (size_t{1} << m) * sizeof(vec2_t<T>) + kTileCoefMax * sizeof(cplx<T>);
         check_cuda(cudaFuncSetAttribute(k_tile_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem)), "tile smem");
         const uint64_t n_tiles = 1ull << (n - m);
-        const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sms) * tile_blocks_per_sm<T>(m));
+        const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sms));
         k_tile_pass<T><<<static_cast<unsigned>(grid), kTileThreads, smem, st>>>(s, n, d_p, pi, d_o, d_c);
         check_cuda(cudaGetLastError(), "tile pass launch");
         ++pi;

@@ -58,6 +58,12 @@ template <typename T>
 void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
                const std::function<void(const Op&)>& stream_op);
 
+// ---------------------------------------------------------------- batched QAOA (kern_qaoa.cu)
+void* qaoa_create(int device, int n_inst, const int32_t* n_qubits, const int32_t* depth, const int32_t* edge_ptr,
+                  const int32_t* edges);
+void qaoa_run(void* q, const double* params, int with_grad, double* energies, double* grads, double* ms);
+void qaoa_destroy(void* q);
+
 // ---------------------------------------------------------------- reductions (kern_reduce.cu)
 
 // Pauli-sum terms prepared for the device: grouped by X mask, coefficients carrying i^{nY}.

@@ -129,13 +129,13 @@ void check_stream(const std::vector<Cmd>& cmds) {
     }
 }
 
-// Executor choice: 1 = tiled, 0 = stream, -1 = tiled from 16 qubits (registers beyond L2,
-// where HBM passes dominate).  Tiles need at least kTileMinQubits qubits.
+// Executor choice: 1 = tiled, 0 = stream, -1 = the measured default.  On the B200 the
+// stream executor's 4-qubit blocks run at the HBM roofline and beat the tiled passes on the
+// benchmark circuits (bench.py autotunes both), so the default is stream.  Tiles need at
+// least kTileMinQubits qubits.
 bool use_tiled(const Handle* h) {
     if (h->n < kTileMinQubits) return false;
-    if (h->executor == 1) return true;
-    if (h->executor == 0) return false;
-    return h->n >= 16;
+    return h->executor == 1;
 }
 
 void apply_stream(Handle* h, const uint8_t* buf, size_t nbytes, bool fuse) {
@@ -486,6 +486,27 @@ int qsv_inner(void* ap, void* bp, double out[2]) {
         else if (a->dtype == QSV_C64) inner<float, double>(S64(a), S128(b), a->n, a->stream, a->ws, out);
         else inner<double, float>(S128(a), S64(b), a->n, a->stream, a->ws, out);
     });
+}
+
+int qsv_qaoa_create(int device, int n_instances, const int32_t* n_qubits, const int32_t* depth,
+                    const int32_t* edge_ptr, const int32_t* edges, void** out) {
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("null output handle");
+        *out = nullptr;
+        int n_dev = 0;
+        check_cuda(cudaGetDeviceCount(&n_dev), "cudaGetDeviceCount");
+        if (device < 0 || device >= n_dev) throw std::invalid_argument("no such CUDA device");
+        *out = qaoa_create(device, n_instances, n_qubits, depth, edge_ptr, edges);
+    });
+}
+
+int qsv_qaoa_run(void* q, const double* params, int with_gradient, double* energies, double* grads,
+                 double* device_ms) {
+    return guarded([&] { qaoa_run(q, params, with_gradient, energies, grads, device_ms); });
+}
+
+int qsv_qaoa_destroy(void* q) {
+    return guarded([&] { qaoa_destroy(q); });
 }
 
 int qsv_synchronize(void* hp) {

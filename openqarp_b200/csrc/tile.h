@@ -19,7 +19,7 @@ namespace qsv {
 constexpr int kTileMaxQubits = 13;   // 2^13 c128 amplitudes = 128 KiB of shared memory
 constexpr int kTileLowQubits = 5;    // contiguous low qubits in every tile
 constexpr int kTileMaxDense = 4;     // widest dense block applied inside a tile
-constexpr int kTileMinQubits = 8;    // a tile holds at least one amplitude per thread
+constexpr int kTileMinQubits = 10;   // a tile holds at least one 16-byte chunk per thread (512 threads)
 
 struct TilePlanOp {
     Op op;

@@ -170,7 +170,7 @@ def mixed_circuits(n):
     }
 
 
-@pytest.mark.parametrize("m", [8, 10, 12])
+@pytest.mark.parametrize("m", [10, 11, 12])
 def test_tiled_executor_matches_oracle(m, restatement):
     n = 14
     for name, cmds in mixed_circuits(n).items():
@@ -449,6 +449,24 @@ def test_complex64_bulk_mode_error_bounds(restatement, sim64):
     m = observable.to_masks(obs, n)
     want = restatement.transition(ref, ref, n, m).real
     assert abs(sim64.expectation(cmds, n, obs) - want) < 1e-5
+
+
+def test_heisenberg_bulk_complex64_against_oracle(restatement):
+    """Config-5 shape at 16 qubits: complex64 bulk evolution with FP64 renormalisation per
+    Trotter step against the complex128 CPU oracle."""
+    from openqarp_b200.workloads import heisenberg_bulk
+    n, steps, dt = 16, 12, 0.05
+    res = heisenberg_bulk(n=n, steps=steps, dt=dt, seed=3)
+    fields = np.random.default_rng(3).uniform(-1.0, 1.0, n)
+    cmds = [Command(G.X, (q,)) for q in range(1, n, 2)] + \
+        circuits.heisenberg_trotter(n, steps, dt, fields, neel=False)
+    ref = restatement.statevector(ir.pack(cmds).buf, n)
+    h = observable.to_masks(circuits.heisenberg_observable(n, fields), n)
+    e_ref = restatement.transition(ref, ref, n, h).real
+    assert abs(res["c128_energy"] - e_ref) < EV_TOL
+    assert abs(res["c64_energy"] - e_ref) < 1e-4
+    assert res["fidelity"] > 1 - 1e-8
+    assert abs(res["c64_norm2"] - 1.0) < 1e-6
 
 
 def test_complex64_adjoint_error_bound(sim, sim64):
