@@ -247,7 +247,14 @@ void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws
                 case 4: launch_dense_reg<T, 4>(op, s, n, st); return;
                 default: break;
             }
-            // k >= 5: out of place through a workspace copy of the register
+            // k = 5, 6 in complex128: a batched complex GEMM on the FP64 tensor pipe
+            if constexpr (sizeof(T) == sizeof(double)) {
+                if (launch_dense_tensor(op, reinterpret_cast<double2*>(s), n, st, ws)) return;
+            } else {
+                // k = 5 in complex64: tcgen05 3xTF32 GEMM with TMEM accumulators
+                if (launch_dense_umma(op, reinterpret_cast<float2*>(s), n, st, ws)) return;
+            }
+            // other wide blocks: out of place through a workspace copy of the register
             const int k = op.k;
             const size_t D = size_t{1} << k;
             DenseGenArgs a{};

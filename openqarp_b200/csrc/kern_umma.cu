@@ -1,0 +1,266 @@
+// kern_umma.cu — 5-qubit fused blocks in complex64 on the 5th-generation tensor cores
+// (tcgen05, kind::tf32, accumulators in TMEM), with 3xTF32 split products.
+//
+// For a tile of 128 groups (2^5 amplitudes each) the block is the real GEMM
+//     D[g][r] = sum_k X[g][k] W[r][k]      g < 128 groups, r, k < 64
+// where row g of X is group g's amplitudes as [Re(a_0..a_31), Im(a_0..a_31)] and
+// W = [[Ur, -Ui], [Ui, Ur]], so D[g] = [Re(y_0..y_31), Im(y_0..y_31)] for y = U a.  The group
+// tile is the M = 128 operand: TMEM lane g holds group g's 64 outputs, which thread g of the
+// CTA reads back with one tcgen05.ld and scatters to HBM.  Both operands sit in shared memory
+// in the K-major "interleaved" canonical layout (8-row x 16-byte core matrices, no swizzle).
+// Each operand is split hi + lo with hi = tf32(x) and lo = tf32(x - hi); D accumulates
+// A_hi B_hi + A_hi B_lo + A_lo B_hi, which keeps single-precision accuracy.
+//
+// One thread issues the MMAs and commits them to an mbarrier; every wait on that barrier is
+// bounded: on timeout the kernel records an error flag, releases its TMEM and returns.
+#include <algorithm>
+#include <stdexcept>
+#include <vector>
+
+#include "kernels.h"
+
+namespace qsv {
+
+namespace {
+
+constexpr int kUThreads = 128;                 // 4 warps: TMEM lane quadrants 0..3
+constexpr int kUK = 5;
+constexpr int kUD = 1 << kUK;                  // 32 complex amplitudes per group
+constexpr int kUR = 2 * kUD;                   // 64 real rows / depth
+constexpr int kUM = 128;                       // groups per tile (MMA M)
+constexpr uint32_t kUCols = 64;                // TMEM columns (MMA N, fp32)
+constexpr int kUChunks = kUR / 4;              // 16-byte K chunks per row (16)
+constexpr int kUOperandA = kUM * kUR * 4;      // bytes of one A plane (32 KiB)
+constexpr int kUOperandB = kUR * kUR * 4;      // bytes of one B plane (16 KiB)
+constexpr size_t kUSmem = 2 * kUOperandA + 2 * kUOperandB + 1024;
+constexpr long long kUWaitLimit = 1ll << 26;   // mbarrier polls before giving up
+
+struct UmmaArgs {
+    uint64_t off[kUD];
+    uint8_t pos[8];
+};
+
+// byte offset of element (row, k) in the K-major interleaved layout (row-groups of 8, K
+// chunks of 4 elements = 16 bytes): LBO = 128 B between K chunks, SBO = 16 * 128 B between
+// 8-row groups
+__device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {
+    return static_cast<uint32_t>(((row >> 3) * kUChunks + (k >> 2)) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+    const uint64_t lbo = 128 >> 4, sbo = (kUChunks * 128) >> 4;
+    return static_cast<uint64_t>((saddr >> 4) & 0x3fff) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t tf32_round(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void split_store(unsigned char* hi, unsigned char* lo, uint32_t off, float4 v) {
+    uint4 h, l;
+    h.x = tf32_round(v.x); l.x = tf32_round(v.x - __uint_as_float(h.x));
+    h.y = tf32_round(v.y); l.y = tf32_round(v.y - __uint_as_float(h.y));
+    h.z = tf32_round(v.z); l.z = tf32_round(v.z - __uint_as_float(h.z));
+    h.w = tf32_round(v.w); l.w = tf32_round(v.w - __uint_as_float(h.w));
+    *reinterpret_cast<uint4*>(hi + off) = h;
+    *reinterpret_cast<uint4*>(lo + off) = l;
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kUWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ s, uint64_t n_groups,
+                                                           const float* __restrict__ W,
+                                                           const __grid_constant__ UmmaArgs a,
+                                                           int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char usm[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(usm) + 1023) & ~uintptr_t{1023});
+    unsigned char* a_hi = base;
+    unsigned char* a_lo = a_hi + kUOperandA;
+    unsigned char* b_hi = a_lo + kUOperandA;
+    unsigned char* b_lo = b_hi + kUOperandB;
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    // W (N = 64 rows x K = 64) in the K-major layout, split hi/lo
+    for (int e = tid; e < kUR * kUChunks; e += blockDim.x) {
+        const int r = e / kUChunks, kc = e % kUChunks;
+        const float4 v = make_float4(W[r * kUR + 4 * kc], W[r * kUR + 4 * kc + 1], W[r * kUR + 4 * kc + 2],
+                                     W[r * kUR + 4 * kc + 3]);
+        split_store(b_hi, b_lo, kmajor_offset(r, 4 * kc), v);
+    }
+    if (tid == 0) {
+        s_fail = 0;
+        const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&s_bar));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&s_tmem));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kUCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&s_bar));
+    // M = 128, N = 64, A/B TF32 K-major, D F32
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((kUCols >> 3) << 17) | ((kUM >> 4) << 24);
+    const uint32_t sa_hi = static_cast<uint32_t>(__cvta_generic_to_shared(a_hi));
+    const uint32_t sa_lo = static_cast<uint32_t>(__cvta_generic_to_shared(a_lo));
+    const uint32_t sb_hi = static_cast<uint32_t>(__cvta_generic_to_shared(b_hi));
+    const uint32_t sb_lo = static_cast<uint32_t>(__cvta_generic_to_shared(b_lo));
+    uint32_t phase = 0;
+    for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kUM; t0 < n_groups; t0 += static_cast<uint64_t>(gridDim.x) * kUM) {
+        // gather: thread `tid` owns group t0 + tid (row tid of A)
+        const uint64_t g = t0 + tid;
+        const bool live = g < n_groups;
+        const uint64_t gb = live ? insert_zeros(g, a.pos, kUK) : 0;
+        float re[kUD], im[kUD];
+#pragma unroll
+        for (int x = 0; x < kUD; ++x) {
+            const float2 v = live ? __ldcs(s + (gb | a.off[x])) : make_float2(0.f, 0.f);
+            re[x] = v.x;
+            im[x] = v.y;
+        }
+#pragma unroll
+        for (int kc = 0; kc < kUD / 4; ++kc) {
+            split_store(a_hi, a_lo, kmajor_offset(tid, 4 * kc),
+                        make_float4(re[4 * kc], re[4 * kc + 1], re[4 * kc + 2], re[4 * kc + 3]));
+            split_store(a_hi, a_lo, kmajor_offset(tid, kUD + 4 * kc),
+                        make_float4(im[4 * kc], im[4 * kc + 1], im[4 * kc + 2], im[4 * kc + 3]));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+#pragma unroll
+            for (int ks = 0; ks < kUR / 8; ++ks) {
+                const uint32_t koff = ks * 256;   // two 16-byte chunks (K = 8) per step
+                umma_tf32(tmem, smem_desc(sa_hi + koff), smem_desc(sb_hi + koff), idesc, ks > 0 ? 1u : 0u);
+                umma_tf32(tmem, smem_desc(sa_hi + koff), smem_desc(sb_lo + koff), idesc, 1u);
+                umma_tf32(tmem, smem_desc(sa_lo + koff), smem_desc(sb_hi + koff), idesc, 1u);
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        const bool ok = mbar_wait(bar, phase);
+        phase ^= 1u;
+        if (!ok) s_fail = 1;
+        __syncthreads();
+        if (s_fail) {
+            if (tid == 0) atomicExch(err, 1);
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // TMEM lane (32 * warp + lane) = group t0 + tid: its 64 fp32 outputs
+        uint32_t d[kUCols];
+        const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+            "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+            "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+            : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+              "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+              "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+              "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31]),
+              "=r"(d[32]), "=r"(d[33]), "=r"(d[34]), "=r"(d[35]), "=r"(d[36]), "=r"(d[37]), "=r"(d[38]), "=r"(d[39]),
+              "=r"(d[40]), "=r"(d[41]), "=r"(d[42]), "=r"(d[43]), "=r"(d[44]), "=r"(d[45]), "=r"(d[46]), "=r"(d[47]),
+              "=r"(d[48]), "=r"(d[49]), "=r"(d[50]), "=r"(d[51]), "=r"(d[52]), "=r"(d[53]), "=r"(d[54]), "=r"(d[55]),
+              "=r"(d[56]), "=r"(d[57]), "=r"(d[58]), "=r"(d[59]), "=r"(d[60]), "=r"(d[61]), "=r"(d[62]), "=r"(d[63])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (live) {
+#pragma unroll
+            for (int x = 0; x < kUD; ++x)
+                __stcs(s + (gb | a.off[x]), make_float2(__uint_as_float(d[x]), __uint_as_float(d[kUD + x])));
+        }
+        // every warp has read its TMEM lanes before the next tile's first MMA overwrites them
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kUCols));
+}
+
+}  // namespace
+
+bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws) {
+    if (op.kind != OP_DENSE || op.k != kUK || n < kUK) return false;
+    UmmaArgs a{};
+    uint32_t sorted[8];
+    for (int b = 0; b < kUK; ++b) sorted[b] = op.qubits[b];
+    std::sort(sorted, sorted + kUK);
+    for (int b = 0; b < 8; ++b) a.pos[b] = b < kUK ? static_cast<uint8_t>(sorted[b]) : 0;
+    for (int l = 0; l < kUD; ++l) {
+        uint64_t o = 0;
+        for (int b = 0; b < kUK; ++b) if ((l >> b) & 1) o |= 1ull << op.qubits[b];
+        a.off[l] = o;
+    }
+    // W = [[Ur, -Ui], [Ui, Ur]] (row r = output, column k = input), single precision
+    std::vector<float> W(static_cast<size_t>(kUR) * kUR);
+    for (int y = 0; y < kUD; ++y)
+        for (int x = 0; x < kUD; ++x) {
+            const c128 u = op.m[static_cast<size_t>(y) * kUD + x];
+            W[static_cast<size_t>(y) * kUR + x] = static_cast<float>(u.real());
+            W[static_cast<size_t>(y) * kUR + kUD + x] = static_cast<float>(-u.imag());
+            W[static_cast<size_t>(y + kUD) * kUR + x] = static_cast<float>(u.imag());
+            W[static_cast<size_t>(y + kUD) * kUR + kUD + x] = static_cast<float>(u.real());
+        }
+    uint8_t* buf = static_cast<uint8_t*>(ws.matrix(W.size() * sizeof(float) + 256));
+    float* dW = reinterpret_cast<float*>(buf);
+    int* d_err = reinterpret_cast<int*>(buf + W.size() * sizeof(float));
+    check_cuda(cudaStreamSynchronize(st), "matrix buffer reuse");
+    check_cuda(cudaMemcpyAsync(dW, W.data(), W.size() * sizeof(float), cudaMemcpyHostToDevice, st), "W upload");
+    check_cuda(cudaMemsetAsync(d_err, 0, sizeof(int), st), "error flag");
+    check_cuda(cudaFuncSetAttribute(k_dense5_umma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kUSmem)), "umma smem");
+    int device = 0, sms = 0, per_sm = 0;
+    check_cuda(cudaGetDevice(&device), "device");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense5_umma, kUThreads, kUSmem), "occupancy");
+    const uint64_t groups = (1ull << n) >> kUK;
+    const uint64_t tiles = (groups + kUM - 1) / kUM;
+    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(sms) * std::max(per_sm, 1)));
+    k_dense5_umma<<<static_cast<unsigned>(grid), kUThreads, kUSmem, st>>>(s, groups, dW, a, d_err);
+    check_cuda(cudaGetLastError(), "umma launch");
+    int h_err = 0;
+    check_cuda(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error flag");
+    check_cuda(cudaStreamSynchronize(st), "umma pass");
+    if (h_err) throw std::runtime_error("tensor-core pass timed out waiting for its MMA commit");
+    return true;
+}
+
+}  // namespace qsv

@@ -51,6 +51,11 @@ private:
 template <typename T>
 void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
 uint64_t op_bytes(const Op& op, int n, int amp_bytes);
+// Dense k = 5, 6 blocks in complex128 on the FP64 tensor pipe (kern_mma.cu); false when the
+// op is not such a block.
+bool launch_dense_tensor(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws);
+// Dense k = 5 blocks in complex64 on tcgen05 (kern_umma.cu); false when not such a block.
+bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws);
 
 // ---------------------------------------------------------------- tiled executor (kern_tile.cu)
 // Launch the planned passes; one-op stream passes (empty tile_qubits) go to `stream_op`.
