@@ -291,6 +291,43 @@ def adjoint_vs_param_shift(device, shift_sample=12):
             "max_abs_diff_adjoint_vs_shift": err}
 
 
+def k_sweep(device, buf):
+    """Config 2's fusion-width sweep at 28 qubits in complex128 and complex64 (stream
+    executor): circuit time per k, and for the tensor-core widths (k = 5, 6) a probe of one
+    dense pass (FP64 DMMA in complex128; tcgen05 3xTF32 at k = 5 in complex64)."""
+    from openqarp_b200 import Register
+    out = {}
+    pass_amps = 1 << N_QUBITS
+    for dtype, amp in (("complex128", 16), ("complex64", 8)):
+        reg = Register(N_QUBITS, dtype, device)
+        timer = StreamTimer(reg)
+        rows = {}
+        for k in (2, 3, 4, 5, 6):
+            reg.configure(k, 12, 0)
+            reg.apply(buf)
+            reg.synchronize()
+            s0 = reg.stats()
+            e0 = timer.event()
+            reg.apply(buf)
+            e1 = timer.event()
+            e1.synchronize()
+            s1 = reg.stats()
+            ms = e0.elapsed_time(e1)
+            rows[f"k{k}"] = {"ms": round(ms, 3), "passes": int(s1["passes"] - s0["passes"]),
+                             "physical_gbs": round((s1["hbm_bytes"] - s0["hbm_bytes"]) / (ms * 1e-3) / 1e9, 1)}
+        for k in (5, 6):
+            probe_ms, qs = kernel_probe(reg, timer, k, reps=5)
+            rows[f"k{k}"]["dense_pass_ms"] = round(probe_ms, 3)
+            rows[f"k{k}"]["dense_pass_gbs"] = round(2 * pass_amps * amp / (probe_ms * 1e-3) / 1e9, 1)
+            rows[f"k{k}"]["dense_pass_tflops"] = round(8 * (1 << k) * pass_amps / (probe_ms * 1e-3) / 1e12, 2)
+            rows[f"k{k}"]["kernel"] = ("k_dense_dmma (FP64 mma.sync)" if dtype == "complex128" else
+                                      ("k_dense5_umma (tcgen05 kind::tf32, 3 products)" if k == 5
+                                       else "k_dense_gen (no tensor path)"))
+        reg.close()
+        out[dtype] = rows
+    return out
+
+
 def qaoa_batched(rank, world, device, dist, steps=3, sample=16):
     """Config 4: 2048 QAOA MaxCut instances (n in 10..20 even, p in 1..4, 3-regular graphs),
     <C> and adjoint gradients for all of them in one persistent graph-captured launch per GPU;
@@ -466,6 +503,10 @@ def b200_arm(args, rank, world, local_rank):
         if not args.skip_adjoint:
             reg.close()
             adj = adjoint_vs_param_shift(device)
+        sweep_k = None
+        if not args.skip_ksweep:
+            reg.close()
+            sweep_k = k_sweep(device, buf)
         heis = None
         if not args.skip_heisenberg:
             reg.close()
@@ -501,6 +542,7 @@ def b200_arm(args, rank, world, local_rank):
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "adjoint": adj,
+            "k_sweep_28q": sweep_k,
             "heisenberg31_c64_bulk": heis,
             "qaoa_batched": qaoa,
         }
@@ -519,6 +561,7 @@ def main():
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-heisenberg", action="store_true")
     ap.add_argument("--skip-qaoa", action="store_true")
+    ap.add_argument("--skip-ksweep", action="store_true")
     ap.add_argument("--executor", type=int, default=None, choices=[0, 1],
                     help="pin the executor (0 stream, 1 tiled) instead of autotuning; needs --k")
     ap.add_argument("--k", type=int, default=None, help="pin the fusion width; needs --executor")
