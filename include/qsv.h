@@ -93,6 +93,24 @@ enum qsv_gate {
     QSV_GATE_COUNT
 };
 
+/* Engine extension record: a permutation |x> -> |table[x]> on its qubits (local bit b <->
+ * qubits[b]), the PermutationKernel of a structured program (reference:
+ * src/qarpx/include/qarpx/simulator/program.h:18-21, apply_permutation program.cpp:610-643).
+ * Payload after the (zero) params: uint64_t table[2^n_qubits], a bijection.  The register
+ * keeps its device address (the kernel scatters from a workspace copy). */
+#define QSV_GATE_PERMUTATION 200
+/* reference: program.cpp:35 kMaxTableQubits = 26 */
+#define QSV_MAX_PERMUTATION_QUBITS 26
+
+/* Engine extension record: a 2^m x 2^m unitary on qubits[0..m) applied where qubits[m] is
+ * |1> (m = n_qubits - 1).  One record is one (control, power) pair of a ControlledPowersKernel
+ * (reference: program.h:33-39, apply_controlled_powers program.cpp:648-711), the power already
+ * multiplied out by the caller.  Payload after the (zero) params: the complex128 matrix,
+ * row-major, local bit b <-> qubits[b]; only amplitudes with the control set are read. */
+#define QSV_GATE_CONTROLLED_UNITARY 201
+/* reference: _program.py K_POWERS = 12 (widest controlled-powers unitary) */
+#define QSV_MAX_CONTROLLED_TARGETS 12
+
 /* Widest Custom / fused block (reference: dense_kernel.h:13 kMaxDenseBlockQubits = 8). */
 #define QSV_MAX_BLOCK_QUBITS 8
 /* Widest register a handle accepts (device memory bound: 2^34 c128 = 256 GiB > HBM). */
@@ -180,6 +198,22 @@ QSV_API int qsv_sample(void* h, const double* u, size_t n_shots, uint64_t* out_i
 QSV_API int qsv_sample_seeded(void* h, uint32_t seed, size_t n_shots, uint64_t* out_idx);
 /* The uniforms qsv_sample_seeded draws (host only; no device work). */
 QSV_API int qsv_uniforms(uint32_t seed, size_t n_shots, double* u_out);
+
+/* PauliAveraging's parity post-processor on the device (PauliAveraging.run,
+ * src/qarp/algorithms/_primitives/pauli_averaging.py:174-205): draws n_shots terminal samples
+ * exactly as qsv_sample_seeded does, keeps the outcomes on the device, and for every Z mask
+ * writes odd[t] = the number of outcomes with odd popcount(outcome & zmasks[t]).  The
+ * estimator E[t] = sign_t * (n_shots - 2 odd[t]) / n_shots then equals the reference's
+ * weights @ (1 - 2 parity) / n_shots bit for bit. */
+QSV_API int qsv_sample_parities(void* h, uint32_t seed, size_t n_shots, const uint64_t* zmasks,
+                                size_t n_masks, uint64_t* odd);
+
+/* Exact Born readout (_exact_result, src/qarp/engines/_engine.py:79-99): the indices i with
+ * |a_i|^2 > threshold, ascending, and their |a_i|^2 (FP64).  *n_out receives the count; the
+ * host buffers keys/probs (cap entries each) are written only when the count fits, so a
+ * caller may query with cap = 0 and NULL buffers first. */
+QSV_API int qsv_exact_probs(void* h, double threshold, uint64_t* keys, double* probs, uint64_t cap,
+                            uint64_t* n_out);
 
 /* Adjoint gradient of <psi|H|psi>, psi = U(theta)|psi0>, psi0 = the handle's current
  * register.  cmds is the concrete stream; for command i, its angle depends on params

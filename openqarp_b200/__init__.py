@@ -8,11 +8,12 @@ loudly when it is missing: there is no CPU fallback.
 from .errors import CapabilityError, CudaError
 from .ir import Command, GateType, Param, custom, gate, pack
 from .observable import PauliMasks, from_strings, to_masks
+from .program import Program
 from .simulator import B200Simulator, Register, SamplingResult, uniforms
 
 __all__ = [
     "B200Simulator", "Register", "SamplingResult", "uniforms",
     "Command", "GateType", "Param", "custom", "gate", "pack",
-    "PauliMasks", "from_strings", "to_masks",
+    "PauliMasks", "from_strings", "to_masks", "Program",
     "CapabilityError", "CudaError",
 ]

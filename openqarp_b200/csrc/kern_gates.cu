@@ -14,6 +14,7 @@
 #include <stdexcept>
 #include <vector>
 
+#include "../../include/qsv.h"
 #include "kernels.h"
 
 namespace qsv {
@@ -57,7 +58,8 @@ BitPlan plan_from_masks(uint64_t zeros, uint64_t ones) {
 template <typename T, int K>
 struct DenseArgs {
     uint64_t off[1 << K];        // index offset of local basis state l
-    uint8_t pos[8];              // ascending target positions
+    uint8_t pos[8];              // ascending target (and control) positions
+    uint64_t ctrl;               // control bits, all set in every group
     cplx<T> m[1 << (2 * K)];     // row-major 2^K x 2^K
 };
 
@@ -65,14 +67,16 @@ struct DenseArgs {
 // constant operand) instead of being hoisted into registers, which keeps the register count
 // low enough for 4 (K <= 3) or 2 (K = 4) resident blocks per SM — the memory-level
 // parallelism an HBM-streaming pass needs.  Loads and stores are evict-first (__ldcs /
-// __stcs): the register is touched once per pass.
-template <typename T, int K>
+// __stcs): the register is touched once per pass.  C = 1: one control qubit, whose groups
+// with the control clear are neither read nor written.
+template <typename T, int K, int C>
 __global__ void __launch_bounds__(kThreads, (K <= 3 ? 4 : 2))
     k_dense_reg(vec2_t<T>* __restrict__ s, uint64_t n_groups, const __grid_constant__ DenseArgs<T, K> a) {
     constexpr int D = 1 << K;
     const uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= n_groups) return;
-    const uint64_t base = insert_zeros(g, a.pos, K);
+    uint64_t base = insert_zeros(g, a.pos, K + C);
+    if constexpr (C != 0) base |= a.ctrl;
     vec2_t<T> in[D];
 #pragma unroll
     for (int l = 0; l < D; ++l) in[l] = __ldcs(s + (base | a.off[l]));
@@ -87,33 +91,40 @@ __global__ void __launch_bounds__(kThreads, (K <= 3 ? 4 : 2))
 
 // ---------------------------------------------------------------- dense, any k (matrix in global)
 // One thread per output amplitude; the group's inputs are re-read through L1/L2.  Used for
-// k >= 5 blocks, which only user Custom gates or fusion widths above 4 produce.
+// blocks the register and tensor-core kernels do not take: k >= 5 blocks (user Custom gates,
+// fusion widths above 4) and controlled unitaries on up to 12 targets.
 struct DenseGenArgs {
-    uint64_t off[256];
-    uint8_t pos[8];
+    uint8_t pos[kMaxOpQubits + 1];   // ascending target and control positions
+    int npos;
     int k;
+    uint64_t ctrl;
 };
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_dense_gen(const vec2_t<T>* __restrict__ src, vec2_t<T>* __restrict__ dst,
                                                          uint64_t n_out, const cplx<T>* __restrict__ m,
+                                                         const uint64_t* __restrict__ off,
                                                          const __grid_constant__ DenseGenArgs a) {
     const int D = 1 << a.k;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < n_out; t += stride) {
-        const uint64_t g = t >> a.k;
+        uint64_t base = t >> a.k;
         const int y = static_cast<int>(t & (D - 1));
-        const uint64_t base = insert_zeros(g, a.pos, a.k);
+        for (int b = 0; b < a.npos; ++b) {
+            const uint64_t p = a.pos[b];
+            base = ((base >> p) << (p + 1)) | (base & ((1ull << p) - 1ull));
+        }
+        base |= a.ctrl;
         double re = 0, im = 0;
         for (int x = 0; x < D; ++x) {
-            const vec2_t<T> v = src[base | a.off[x]];
+            const vec2_t<T> v = src[base | __ldg(off + x)];
             const cplx<T> c = m[y * D + x];
             re = fma(static_cast<double>(c.re), v.x, re);
             re = fma(-static_cast<double>(c.im), v.y, re);
             im = fma(static_cast<double>(c.re), v.y, im);
             im = fma(static_cast<double>(c.im), v.x, im);
         }
-        dst[base | a.off[y]] = mk<T>(static_cast<T>(re), static_cast<T>(im));
+        dst[base | __ldg(off + y)] = mk<T>(static_cast<T>(re), static_cast<T>(im));
     }
 }
 
@@ -206,6 +217,28 @@ __global__ void __launch_bounds__(kThreads) k_pauli_rot(vec2_t<T>* __restrict__ 
     }
 }
 
+// |x> -> |table[x]> on the op's qubits, out of place (apply_permutation, program.cpp:610-643)
+struct PermArgs {
+    uint8_t q[QSV_MAX_PERMUTATION_QUBITS];
+    int k;
+    uint64_t keep;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_perm(const vec2_t<T>* __restrict__ src, vec2_t<T>* __restrict__ dst,
+                                                   uint64_t dim, const uint64_t* __restrict__ table,
+                                                   const __grid_constant__ PermArgs a) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
+        uint64_t x = 0;
+        for (int b = 0; b < a.k; ++b) x |= ((i >> a.q[b]) & 1ull) << b;
+        const uint64_t y = __ldg(table + x);
+        uint64_t j = i & a.keep;
+        for (int b = 0; b < a.k; ++b) j |= ((y >> b) & 1ull) << a.q[b];
+        dst[j] = src[i];
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_scale(vec2_t<T>* __restrict__ s, uint64_t dim, cplx<T> f) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -216,19 +249,25 @@ __global__ void __launch_bounds__(kThreads) k_scale(vec2_t<T>* __restrict__ s, u
 template <typename T, int K>
 void launch_dense_reg(const Op& op, vec2_t<T>* s, int n, cudaStream_t st) {
     DenseArgs<T, K> a{};
+    const int nc = __builtin_popcountll(op.ctrl);
+    if (nc > 1) throw std::logic_error("dense op with more than one control");
     uint32_t sorted[8];
-    for (int b = 0; b < K; ++b) sorted[b] = op.qubits[b];
-    std::sort(sorted, sorted + K);
-    for (int b = 0; b < 8; ++b) a.pos[b] = b < K ? static_cast<uint8_t>(sorted[b]) : 0;
+    int np = 0;
+    for (int b = 0; b < K; ++b) sorted[np++] = op.qubits[b];
+    if (nc) sorted[np++] = static_cast<uint32_t>(__builtin_ctzll(op.ctrl));
+    std::sort(sorted, sorted + np);
+    for (int b = 0; b < 8; ++b) a.pos[b] = b < np ? static_cast<uint8_t>(sorted[b]) : 0;
+    a.ctrl = op.ctrl;
     for (int l = 0; l < (1 << K); ++l) {
         uint64_t o = 0;
         for (int b = 0; b < K; ++b) if ((l >> b) & 1) o |= 1ull << op.qubits[b];
         a.off[l] = o;
     }
     for (int e = 0; e < (1 << (2 * K)); ++e) a.m[e] = to_c<T>(op.m[e]);
-    const uint64_t groups = (1ull << n) >> K;
+    const uint64_t groups = (1ull << n) >> np;
     const uint64_t blocks = (groups + kThreads - 1) / kThreads;
-    k_dense_reg<T, K><<<static_cast<unsigned>(blocks), kThreads, 0, st>>>(s, groups, a);
+    if (nc) k_dense_reg<T, K, 1><<<static_cast<unsigned>(blocks), kThreads, 0, st>>>(s, groups, a);
+    else k_dense_reg<T, K, 0><<<static_cast<unsigned>(blocks), kThreads, 0, st>>>(s, groups, a);
 }
 
 }  // namespace
@@ -247,35 +286,53 @@ void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws
                 case 4: launch_dense_reg<T, 4>(op, s, n, st); return;
                 default: break;
             }
-            // k = 5, 6 in complex128: a batched complex GEMM on the FP64 tensor pipe
-            if constexpr (sizeof(T) == sizeof(double)) {
-                if (launch_dense_tensor(op, reinterpret_cast<double2*>(s), n, st, ws)) return;
-            } else {
-                // k = 5 in complex64: tcgen05 3xTF32 GEMM with TMEM accumulators
-                if (launch_dense_umma(op, reinterpret_cast<float2*>(s), n, st, ws)) return;
+            if (op.ctrl == 0) {
+                // k = 5, 6 in complex128: a batched complex GEMM on the FP64 tensor pipe
+                if constexpr (sizeof(T) == sizeof(double)) {
+                    if (launch_dense_tensor(op, reinterpret_cast<double2*>(s), n, st, ws)) return;
+                } else {
+                    // k = 5 in complex64: tcgen05 3xTF32 GEMM with TMEM accumulators
+                    if (launch_dense_umma(op, reinterpret_cast<float2*>(s), n, st, ws)) return;
+                }
             }
             // other wide blocks: out of place through a workspace copy of the register
             const int k = op.k;
+            if (k < 1 || k > kMaxOpQubits) throw std::logic_error("dense op width outside 1..12");
             const size_t D = size_t{1} << k;
             DenseGenArgs a{};
-            uint32_t sorted[8];
-            for (int b = 0; b < k; ++b) sorted[b] = op.qubits[b];
-            std::sort(sorted, sorted + k);
-            for (int b = 0; b < 8; ++b) a.pos[b] = b < k ? static_cast<uint8_t>(sorted[b]) : 0;
+            uint32_t sorted[kMaxOpQubits + 1];
+            int np = 0;
+            for (int b = 0; b < k; ++b) sorted[np++] = op.qubits[b];
+            for (int q = 0; q < 64; ++q)
+                if ((op.ctrl >> q) & 1) {
+                    if (np > kMaxOpQubits) throw std::logic_error("dense op with too many controls");
+                    sorted[np++] = static_cast<uint32_t>(q);
+                }
+            if (np > n) throw std::invalid_argument("block wider than the register");
+            std::sort(sorted, sorted + np);
+            for (int b = 0; b < np; ++b) a.pos[b] = static_cast<uint8_t>(sorted[b]);
+            a.npos = np;
+            a.k = k;
+            a.ctrl = op.ctrl;
+            // matrix then the offset table, in one upload (the table 16-byte aligned)
+            const size_t mat_bytes = D * D * sizeof(cplx<T>);
+            std::vector<unsigned char> blob(mat_bytes + D * sizeof(uint64_t));
+            cplx<T>* hm = reinterpret_cast<cplx<T>*>(blob.data());
+            for (size_t e = 0; e < D * D; ++e) hm[e] = to_c<T>(op.m[e]);
+            uint64_t* hoff = reinterpret_cast<uint64_t*>(blob.data() + mat_bytes);
             for (size_t l = 0; l < D; ++l) {
                 uint64_t o = 0;
                 for (int b = 0; b < k; ++b) if ((l >> b) & 1) o |= 1ull << op.qubits[b];
-                a.off[l] = o;
+                hoff[l] = o;
             }
-            a.k = k;
-            std::vector<cplx<T>> hm(D * D);
-            for (size_t e = 0; e < D * D; ++e) hm[e] = to_c<T>(op.m[e]);
-            cplx<T>* dm = static_cast<cplx<T>*>(ws.matrix(hm.size() * sizeof(cplx<T>)));
-            check_cuda(cudaMemcpyAsync(dm, hm.data(), hm.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice, st),
-                       "matrix upload");
+            unsigned char* dblob = static_cast<unsigned char*>(ws.matrix(blob.size()));
+            check_cuda(cudaMemcpyAsync(dblob, blob.data(), blob.size(), cudaMemcpyHostToDevice, st), "matrix upload");
+            const cplx<T>* dm = reinterpret_cast<const cplx<T>*>(dblob);
+            const uint64_t* doff = reinterpret_cast<const uint64_t*>(dblob + mat_bytes);
             vec2_t<T>* copy = static_cast<vec2_t<T>*>(ws.state_copy(dim * sizeof(vec2_t<T>)));
             check_cuda(cudaMemcpyAsync(copy, s, dim * sizeof(vec2_t<T>), cudaMemcpyDeviceToDevice, st), "copy");
-            k_dense_gen<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(copy, s, dim, dm, a);
+            const uint64_t n_out = (dim >> np) << k;
+            k_dense_gen<T><<<grid_for(n_out, 1, 1u << 20), kThreads, 0, st>>>(copy, s, n_out, dm, doff, a);
             // the host matrix must outlive the async copy
             check_cuda(cudaStreamSynchronize(st), "dense k>=5");
             return;
@@ -334,7 +391,36 @@ void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws
         case OP_SCALE:
             k_scale<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(s, dim, to_c<T>(op.m[0]));
             return;
+        case OP_PERM:
+            launch_perm<T>(op, s, n, st, ws);
+            return;
     }
+}
+
+// The register keeps its address (a zero-copy caller may hold it): copy it aside, then
+// scatter the copy back through the table.
+template <typename T>
+void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws) {
+    if (op.k < 1 || op.k > QSV_MAX_PERMUTATION_QUBITS || op.table.size() != (size_t{1} << op.k))
+        throw std::logic_error("malformed permutation op");
+    PermArgs a{};
+    a.k = op.k;
+    a.keep = ~0ull;
+    for (int b = 0; b < op.k; ++b) {
+        if (static_cast<int>(op.pq[b]) >= n) throw std::invalid_argument("permutation qubit outside the register");
+        a.q[b] = static_cast<uint8_t>(op.pq[b]);
+        a.keep &= ~(1ull << op.pq[b]);
+    }
+    uint64_t* dt = static_cast<uint64_t*>(ws.matrix(op.table.size() * sizeof(uint64_t)));
+    // the matrix buffer's previous user must be done; the pageable copy returns once staged
+    check_cuda(cudaStreamSynchronize(st), "matrix buffer reuse");
+    check_cuda(cudaMemcpyAsync(dt, op.table.data(), op.table.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st),
+               "permutation table");
+    const uint64_t dim = 1ull << n;
+    vec2_t<T>* copy = static_cast<vec2_t<T>*>(ws.state_copy(dim * sizeof(vec2_t<T>)));
+    check_cuda(cudaMemcpyAsync(copy, s, dim * sizeof(vec2_t<T>), cudaMemcpyDeviceToDevice, st), "copy");
+    k_perm<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(copy, s, dim, dt, a);
+    check_cuda(cudaGetLastError(), "permutation launch");
 }
 
 template void launch_op<double>(const Op&, double2*, int, cudaStream_t, Workspace&);
@@ -346,6 +432,8 @@ uint64_t op_bytes(const Op& op, int n, int amp_bytes) {
     uint64_t touched = dim;
     switch (op.kind) {
         case OP_NOP: touched = 0; break;
+        case OP_PERM: touched = 2 * dim; break;   // copy aside, then scatter back
+        case OP_DENSE: touched = dim >> __builtin_popcountll(op.ctrl); break;
         case OP_PHASE: touched = dim >> __builtin_popcountll(op.mask); break;
         case OP_CTRL1: touched = dim >> __builtin_popcountll(op.mask); break;
         default: break;

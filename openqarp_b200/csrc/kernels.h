@@ -51,6 +51,9 @@ private:
 template <typename T>
 void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
 uint64_t op_bytes(const Op& op, int n, int amp_bytes);
+// Permutation op (kern_gates.cu): through the workspace copy, register address unchanged.
+template <typename T>
+void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
 // Dense k = 5, 6 blocks in complex128 on the FP64 tensor pipe (kern_mma.cu); false when the
 // op is not such a block.
 bool launch_dense_tensor(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws);
@@ -105,6 +108,16 @@ void scale_real(vec2_t<T>* s, int n, double f, cudaStream_t st);
 template <typename T>
 void sample_sorted(const vec2_t<T>* s, int n, const double* d_u_sorted, size_t n_shots,
                    uint64_t* d_out, cudaStream_t st, Workspace& ws);
+
+// ---------------------------------------------------------------- readouts (kern_readout.cu)
+// Exact Born readout: counts the indices with |a|^2 > thr (returned); when d_keys is non-null
+// and the count fits `cap`, writes them in ascending order with their probabilities.
+template <typename T>
+uint64_t exact_readout(const vec2_t<T>* s, int n, double thr, uint64_t* d_keys, double* d_probs, uint64_t cap,
+                       cudaStream_t st, Workspace& ws);
+// d_odd[t] = #{s : popcount(d_outcome[s] & d_masks[t]) odd}
+void parity_counts(const uint64_t* d_outcome, size_t n_shots, const uint64_t* d_masks, size_t n_masks,
+                   unsigned long long* d_odd, cudaStream_t st);
 
 // ---------------------------------------------------------------- adjoint (kern_reduce.cu)
 // One reverse step of a parametric gate of width k (0..2): with psi, phi the states after

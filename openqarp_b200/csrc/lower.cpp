@@ -110,7 +110,7 @@ std::vector<Cmd> decode(const uint8_t* buf, size_t nbytes) {
             throw std::invalid_argument("command buffer truncated in a header");
         qsv_cmd_header h;
         std::memcpy(&h, buf + off, sizeof h);
-        if (h.gate >= GATE_COUNT)
+        if (h.gate >= GATE_COUNT && h.gate != PERMUTATION && h.gate != CONTROLLED_UNITARY)
             throw std::invalid_argument("unknown gate code " + std::to_string(h.gate));
         Cmd c;
         c.gate = h.gate;
@@ -136,6 +136,34 @@ std::vector<Cmd> decode(const uint8_t* buf, size_t nbytes) {
             c.u.resize(d * d);
             std::memcpy(c.u.data(), buf + o, 16 * d * d);
             o += 16 * d * d;
+        }
+        if (c.gate == CONTROLLED_UNITARY) {
+            // add_controlled_powers' checks (program.cpp:527-543): targets, a control, distinct
+            if (nq < 2 || nq - 1 > QSV_MAX_CONTROLLED_TARGETS)
+                throw std::invalid_argument("controlled unitary must act on 1.." +
+                                            std::to_string(QSV_MAX_CONTROLLED_TARGETS) +
+                                            " targets and one control");
+            const size_t d = size_t{1} << (nq - 1);
+            if (o + 16 * d * d > nbytes) throw std::invalid_argument("command buffer truncated");
+            c.u.resize(d * d);
+            std::memcpy(c.u.data(), buf + o, 16 * d * d);
+            o += 16 * d * d;
+        }
+        if (c.gate == PERMUTATION) {
+            // add_permutation's checks (program.h): distinct qubits, a bijection of [0, 2^k)
+            if (nq == 0 || nq > QSV_MAX_PERMUTATION_QUBITS)
+                throw std::invalid_argument("permutation kernel must act on 1.." +
+                                            std::to_string(QSV_MAX_PERMUTATION_QUBITS) + " qubits");
+            const size_t d = size_t{1} << nq;
+            if (o + 8 * d > nbytes) throw std::invalid_argument("command buffer truncated");
+            c.table.resize(d);
+            std::memcpy(c.table.data(), buf + o, 8 * d);
+            o += 8 * d;
+            std::vector<char> seen(d, 0);
+            for (uint64_t v : c.table) {
+                if (v >= d || seen[v]) throw std::invalid_argument("permutation table is not a bijection of [0, 2^k)");
+                seen[v] = 1;
+            }
         }
         out.push_back(std::move(c));
         off = o;
@@ -165,7 +193,7 @@ std::vector<Op> lower(const Cmd& c, int n) {
             if (c.q[a] == c.q[b])
                 throw std::invalid_argument("command repeats qubit " + std::to_string(c.q[b]));
     }
-    if (g != CUSTOM && g != MCZ && g != BARRIER && g != MEASURE && g != RESET &&
+    if (g != CUSTOM && g != MCZ && g != BARRIER && g != MEASURE && g != RESET && g != CONTROLLED_UNITARY &&
         static_cast<int>(c.q.size()) < expected_qubits(g))
         throw std::runtime_error("gate " + std::to_string(g) + " requires " +
                                  std::to_string(expected_qubits(g)) + " qubits");
@@ -265,6 +293,40 @@ std::vector<Op> lower(const Cmd& c, int n) {
             }
             return {o};
         }
+        case CONTROLLED_UNITARY: {
+            const int k = static_cast<int>(c.q.size()) - 1;
+            const size_t d = size_t{1} << k;
+            if (k < 1 || k > kMaxOpQubits || c.u.size() != d * d)
+                throw std::runtime_error("controlled unitary size does not match its qubits");
+            bool diag = true;
+            for (size_t y = 0; y < d && diag; ++y)
+                for (size_t x = 0; x < d; ++x)
+                    if (x != y && c.u[y * d + x] != I0) { diag = false; break; }
+            Op o; o.n_gates = c.n_gates;
+            if (diag && k + 1 <= QSV_MAX_BLOCK_QUBITS) {
+                // a diagonal power: one diagonal pass over targets + control, 1 where control is 0
+                o.kind = OP_DIAG;
+                o.k = k + 1;
+                for (int b = 0; b <= k; ++b) o.qubits[b] = c.q[b];
+                o.m.assign(2 * d, I1);
+                for (size_t l = 0; l < d; ++l) o.m[d + l] = c.u[l * d + l];
+            } else {
+                o.kind = OP_DENSE;
+                o.k = k;
+                for (int b = 0; b < k; ++b) o.qubits[b] = c.q[b];
+                o.ctrl = bit(c.q[k]);
+                o.m = c.u;
+            }
+            return {o};
+        }
+        case PERMUTATION: {
+            Op o;
+            o.kind = OP_PERM;
+            o.k = static_cast<int>(c.q.size());
+            o.pq = c.q;
+            o.table = c.table;
+            return {o};
+        }
         case RESET:
             throw std::runtime_error("Reset is not deterministic: it has no statevector");
         default:
@@ -323,6 +385,20 @@ void apply_op_host(const Op& op, c128* s, int n) {
             }
             return;
         }
+        case OP_PERM: {
+            std::vector<c128> out(dim);
+            uint64_t keep = ~0ull;
+            for (uint32_t q : op.pq) keep &= ~bit(q);
+            for (uint64_t i = 0; i < dim; ++i) {
+                uint64_t x = 0, j = i & keep;
+                for (size_t b = 0; b < op.pq.size(); ++b) x |= ((i >> op.pq[b]) & 1ull) << b;
+                const uint64_t y = op.table[x];
+                for (size_t b = 0; b < op.pq.size(); ++b) j |= ((y >> b) & 1ull) << op.pq[b];
+                out[j] = s[i];
+            }
+            std::copy(out.begin(), out.end(), s);
+            return;
+        }
         case OP_DENSE: {
             const int k = op.k;
             const uint64_t d = 1ull << k;
@@ -336,7 +412,7 @@ void apply_op_host(const Op& op, c128* s, int n) {
                 off[l] = o;
             }
             for (uint64_t i = 0; i < dim; ++i) {
-                if (i & tmask) continue;
+                if ((i & tmask) || (i & op.ctrl) != op.ctrl) continue;
                 for (uint64_t l = 0; l < d; ++l) in[l] = s[i | off[l]];
                 for (uint64_t y = 0; y < d; ++y) {
                     c128 acc(0, 0);
@@ -399,6 +475,15 @@ Cmd dagger(const Cmd& c) {
                 for (size_t x = 0; x < d; ++x) r.u[y * d + x] = std::conj(c.u[x * d + y]);
             return r;
         }
+        case CONTROLLED_UNITARY: {
+            const size_t d = size_t{1} << (c.q.size() - 1);
+            for (size_t y = 0; y < d; ++y)
+                for (size_t x = 0; x < d; ++x) r.u[y * d + x] = std::conj(c.u[x * d + y]);
+            return r;
+        }
+        case PERMUTATION:
+            for (size_t x = 0; x < c.table.size(); ++x) r.table[c.table[x]] = x;
+            return r;
         default:
             for (double& v : r.p) v = -v;
             return r;
@@ -467,6 +552,7 @@ bool contains(const std::vector<uint32_t>& v, uint32_t x) {
 }
 
 bool fusible(const Cmd& c, int k) {
+    if (c.gate == PERMUTATION || c.gate == CONTROLLED_UNITARY) return false;
     if (c.q.empty() || static_cast<int>(c.q.size()) > k) return false;
     if (is_marker(c.gate) || c.gate == GPHASE) return false;
     if (c.flags & 1) return false;

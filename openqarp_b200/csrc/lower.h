@@ -20,7 +20,9 @@ enum Gate : int {
     CH, CS, CSDG, CSX, CSXDG,
     CRX, CRY, CRZ, CP, RZZ, RXX, RYY,
     CU, CCX, CSWAP, MCZ, GPHASE,
-    BARRIER, MEASURE, RESET, BRANCH_BEGIN, BRANCH_ELSE, BRANCH_END, CUSTOM, GATE_COUNT
+    BARRIER, MEASURE, RESET, BRANCH_BEGIN, BRANCH_ELSE, BRANCH_END, CUSTOM, GATE_COUNT,
+    PERMUTATION = 200,        // engine extension: structured-program permutation kernel
+    CONTROLLED_UNITARY = 201  // engine extension: a unitary on q[0..k-1) where q[k-1] is |1>
 };
 
 // Error classes mirrored from the reference (status codes of include/qsv.h).
@@ -35,6 +37,8 @@ struct Cmd {
     std::vector<uint32_t> cbits;
     std::vector<double> p;
     std::vector<c128> u;     // Custom: 2^k x 2^k row-major, local bit b <-> q[b]
+                             // ControlledUnitary: 2^(k-1) square on q[0..k-1)
+    std::vector<uint64_t> table;   // Permutation: |x> -> |table[x]>
     int flags = 0;           // bit 0: classical condition
     int n_gates = 1;         // source gates folded into this command (fusion statistics)
 };
@@ -62,24 +66,30 @@ std::vector<Cmd> fuse_for_dispatch(const std::vector<Cmd>& in, int n_qubits, int
                                    int min_qubits);
 
 // ---------------------------------------------------------------- device operations
+// widest dense op: a controlled-powers unitary on up to 12 targets
+constexpr int kMaxOpQubits = 12;
 enum OpKind : int {
     OP_NOP = 0,
-    OP_DENSE,       // k-qubit dense matrix (k = 1..8) on qubits[0..k)
+    OP_DENSE,       // k-qubit dense matrix (k = 1..12) on qubits[0..k), where (i & ctrl) == ctrl
     OP_DIAG,        // k-qubit diagonal, m[l] for local index l
     OP_CTRL1,       // 2x2 on `target` where (i & mask) == mask
     OP_PHASE,       // i -> m[0] * i where (i & mask) == mask
     OP_SWAP,        // swap qubits[0], qubits[1]
     OP_PAULI_ROT,   // exp(-i theta/2 P), P by (mask = X|Y bits, zmask = Z|Y bits); m[0] = (cos, sin)
     OP_SCALE,       // every amplitude times m[0]
+    OP_PERM,        // out-of-place permutation of basis states on qubits[0..k) (table)
 };
 
 struct Op {
     OpKind kind = OP_NOP;
     int k = 0;
-    uint32_t qubits[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t qubits[kMaxOpQubits] = {};
     uint64_t mask = 0, zmask = 0;
+    uint64_t ctrl = 0;             // OP_DENSE: control bits (all must be 1)
     int target = 0;
     std::vector<c128> m;
+    std::vector<uint64_t> table;   // OP_PERM
+    std::vector<uint32_t> pq;      // OP_PERM qubits (may exceed 8)
     int n_gates = 1;
 };
 

@@ -456,6 +456,64 @@ int qsv_sample_seeded(void* hp, uint32_t seed, size_t n_shots, uint64_t* out) {
     return qsv_sample(hp, u.data(), n_shots, out);
 }
 
+int qsv_sample_parities(void* hp, uint32_t seed, size_t n_shots, const uint64_t* zmasks, size_t n_masks,
+                        uint64_t* odd) {
+    std::vector<double> u(n_shots);
+    int rc = qsv_uniforms(seed, n_shots, u.data());
+    if (rc) return rc;
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (n_masks && (!zmasks || !odd)) throw std::invalid_argument("null argument");
+        for (size_t t = 0; t < n_masks; ++t)
+            if (h->n < 64 && (zmasks[t] >> h->n) != 0)
+                throw std::invalid_argument("Z mask names a qubit outside the register");
+        if (n_masks == 0) return;
+        // outcomes stay on the device in sorted-uniform order: parities do not depend on it
+        std::sort(u.begin(), u.end());
+        uint8_t* dev = static_cast<uint8_t*>(h->ws.shots(n_shots * 16));
+        double* d_u = reinterpret_cast<double*>(dev);
+        uint64_t* d_out = reinterpret_cast<uint64_t*>(dev + n_shots * 8);
+        uint64_t* d_masks = static_cast<uint64_t*>(h->ws.matrix(n_masks * 16));
+        auto* d_odd = reinterpret_cast<unsigned long long*>(d_masks + n_masks);
+        check_cuda(cudaMemcpyAsync(d_masks, zmasks, n_masks * 8, cudaMemcpyHostToDevice, h->stream), "masks H2D");
+        if (n_shots) {
+            check_cuda(cudaMemcpyAsync(d_u, u.data(), n_shots * 8, cudaMemcpyHostToDevice, h->stream), "shots H2D");
+            if (h->dtype == QSV_C128) sample_sorted<double>(S128(h), h->n, d_u, n_shots, d_out, h->stream, h->ws);
+            else sample_sorted<float>(S64(h), h->n, d_u, n_shots, d_out, h->stream, h->ws);
+        }
+        parity_counts(d_out, n_shots, d_masks, n_masks, d_odd, h->stream);
+        check_cuda(cudaMemcpyAsync(odd, d_odd, n_masks * 8, cudaMemcpyDeviceToHost, h->stream), "parities D2H");
+        check_cuda(cudaStreamSynchronize(h->stream), "parities");
+        h->stats.launches += 6;
+    });
+}
+
+int qsv_exact_probs(void* hp, double threshold, uint64_t* keys, double* probs, uint64_t cap, uint64_t* n_out) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!n_out) throw std::invalid_argument("null output");
+        if (cap && (!keys || !probs)) throw std::invalid_argument("null key/probability buffers");
+        if (!(threshold >= 0.0)) throw std::invalid_argument("threshold must be >= 0");
+        // first pass counts; the device buffers are sized by the count before the write pass
+        uint64_t total = h->dtype == QSV_C128
+                             ? exact_readout<double>(S128(h), h->n, threshold, nullptr, nullptr, 0, h->stream, h->ws)
+                             : exact_readout<float>(S64(h), h->n, threshold, nullptr, nullptr, 0, h->stream, h->ws);
+        *n_out = total;
+        h->stats.launches += 2;
+        if (total == 0 || total > cap) return;
+        uint8_t* dev = static_cast<uint8_t*>(h->ws.shots(total * 16));
+        uint64_t* d_keys = reinterpret_cast<uint64_t*>(dev);
+        double* d_probs = reinterpret_cast<double*>(dev + total * 8);
+        total = h->dtype == QSV_C128
+                    ? exact_readout<double>(S128(h), h->n, threshold, d_keys, d_probs, total, h->stream, h->ws)
+                    : exact_readout<float>(S64(h), h->n, threshold, d_keys, d_probs, total, h->stream, h->ws);
+        check_cuda(cudaMemcpyAsync(keys, d_keys, total * 8, cudaMemcpyDeviceToHost, h->stream), "keys D2H");
+        check_cuda(cudaMemcpyAsync(probs, d_probs, total * 8, cudaMemcpyDeviceToHost, h->stream), "probs D2H");
+        check_cuda(cudaStreamSynchronize(h->stream), "exact readout");
+        h->stats.launches += 3;
+    });
+}
+
 int qsv_norm2(void* hp, double* out) {
     return guarded([&] {
         Handle* h = H_(hp);

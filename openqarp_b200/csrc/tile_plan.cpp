@@ -23,6 +23,9 @@ uint64_t op_mixing_mask(const Op& op) {
             return bit(static_cast<uint32_t>(op.target));
         case OP_SWAP: return bit(op.qubits[0]) | bit(op.qubits[1]);
         case OP_PAULI_ROT: return op.mask;
+        case OP_PERM:
+            for (uint32_t q : op.pq) m |= bit(q);
+            return m;
         default: return 0;
     }
 }
@@ -32,10 +35,13 @@ uint64_t op_support_mask(const Op& op) {
     switch (op.kind) {
         case OP_DENSE: case OP_DIAG: case OP_SWAP:
             for (int b = 0; b < op.k; ++b) m |= bit(op.qubits[b]);
-            return m;
+            return m | op.ctrl;
         case OP_PHASE: return op.mask;
         case OP_CTRL1: return op.mask | bit(static_cast<uint32_t>(op.target));
         case OP_PAULI_ROT: return op.mask | op.zmask;
+        case OP_PERM:
+            for (uint32_t q : op.pq) m |= bit(q);
+            return m;
         default: return 0;
     }
 }
@@ -52,6 +58,8 @@ std::vector<TilePass> plan_tiles(const std::vector<Op>& ops_in, int n, int m, in
     // an op fits a tile when it is a kind the tile kernel applies and its mixing qubits fit
     auto fits = [&](const Op& o) {
         if (o.kind == OP_DENSE && o.k > kTileMaxDense) return false;
+        if (o.kind == OP_PERM) return false;   // out of place: always a stream pass
+        if (o.ctrl != 0) return false;         // controlled dense: a stream pass
         return __builtin_popcountll(op_mixing_mask(o) & ~low) + c <= m;
     };
     while (!remaining.empty()) {

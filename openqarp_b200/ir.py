@@ -262,6 +262,56 @@ def custom(qubits: Sequence[int], u: np.ndarray) -> Command:
     return Command(GateType.Custom, tuple(qubits), (), np.asarray(u, dtype=np.complex128))
 
 
+# ---------------------------------------------------------------- structured records
+# Engine extension records (include/qsv.h QSV_GATE_PERMUTATION / QSV_GATE_CONTROLLED_UNITARY):
+# the typed kernels of a structured program travel in the same packed stream as gates.
+PERMUTATION_CODE = 200
+CONTROLLED_UNITARY_CODE = 201
+MAX_PERMUTATION_QUBITS = 26     # program.cpp:35 kMaxTableQubits
+MAX_CONTROLLED_TARGETS = 12     # _program.py K_POWERS
+
+
+@dataclass(frozen=True)
+class PermutationRecord:
+    """|x> -> |table[x]> on ``qubits`` (local bit b <-> qubits[b])."""
+
+    qubits: tuple
+    table: np.ndarray
+
+
+@dataclass(frozen=True)
+class ControlledUnitaryRecord:
+    """``matrix`` on ``targets`` wherever ``control`` is |1>."""
+
+    targets: tuple
+    control: int
+    matrix: np.ndarray
+
+
+def _pack_record(out: bytearray, rec) -> None:
+    if isinstance(rec, PermutationRecord):
+        qubits = [int(q) for q in rec.qubits]
+        table = np.ascontiguousarray(np.asarray(rec.table, dtype=np.uint64).reshape(-1))
+        if not 1 <= len(qubits) <= MAX_PERMUTATION_QUBITS or table.shape[0] != (1 << len(qubits)):
+            raise ValueError("permutation record: table length does not match its qubits")
+        code, payload = PERMUTATION_CODE, table.tobytes()
+    else:
+        qubits = [int(q) for q in rec.targets] + [int(rec.control)]
+        m = np.ascontiguousarray(np.asarray(rec.matrix, dtype=np.complex128))
+        k = len(qubits) - 1
+        if not 1 <= k <= MAX_CONTROLLED_TARGETS:
+            raise CapabilityError(f"controlled unitary on {k} targets: the engine applies 1.."
+                                  f"{MAX_CONTROLLED_TARGETS}")
+        if m.shape != (1 << k, 1 << k):
+            raise ValueError("controlled unitary record: matrix is not 2^|targets| square")
+        code, payload = CONTROLLED_UNITARY_CODE, m.tobytes()
+    out += _HDR.pack(code, len(qubits), 0, 0, 0, 0)
+    out += struct.pack(f"<{len(qubits)}I", *qubits)
+    if len(out) % 8:
+        out += b"\0" * (8 - len(out) % 8)
+    out += payload
+
+
 # ---------------------------------------------------------------- packing
 
 _HDR = struct.Struct("<HBBBBH")
@@ -311,6 +361,12 @@ def pack(commands: Iterable, values: Optional[Mapping[str, float]] = None,
     dep_alpha: list[float] = []
     n = 0
     for cmd in commands:
+        if isinstance(cmd, (PermutationRecord, ControlledUnitaryRecord)):
+            _pack_record(out, cmd)
+            if index is not None:
+                dep_ptr.append(len(dep_param))
+            n += 1
+            continue
         g, qubits, params, cbits, cond, unitary = _cmd_fields(cmd)
         vals = [_param_value(p, values) for p in params]
         if len(qubits) > 255 or len(params) > 255 or len(cbits) > 255:

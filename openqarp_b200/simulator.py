@@ -21,6 +21,7 @@ from .errors import CapabilityError
 from .ir import (PackedStream, cbit_register_width, measurements_are_terminal, needs_trajectory,
                  pack)
 from .observable import PauliMasks, to_masks
+from .program import GatesKernel, as_program
 
 MAX_QUBITS = 34
 MAX_BLOCK_QUBITS = 8
@@ -147,6 +148,30 @@ class Register:
         out = np.empty(int(n_shots), dtype=np.uint64)
         check(lib.qsv_sample_seeded(self.handle, int(seed) & 0xFFFFFFFF, int(n_shots), u64ptr(out)))
         return out
+
+    def sample_parities(self, seed: int, n_shots: int, z_masks) -> np.ndarray:
+        """Seeded terminal samples (the draws of sample_seeded) reduced on the device: for every
+        Z mask, how many outcomes have odd popcount(outcome & mask)."""
+        m = np.ascontiguousarray(np.asarray(z_masks, dtype=np.uint64).reshape(-1))
+        odd = np.zeros(m.shape[0], dtype=np.uint64)
+        check(lib.qsv_sample_parities(self.handle, int(seed) & 0xFFFFFFFF, int(n_shots), u64ptr(m),
+                                      m.shape[0], u64ptr(odd)))
+        return odd.astype(np.int64)
+
+    def exact_probs(self, threshold: float = 1e-12) -> tuple[np.ndarray, np.ndarray]:
+        """(keys, probs): the indices with |a|^2 > threshold, ascending, and |a|^2, compacted on
+        the device."""
+        n = ctypes.c_uint64()
+        check(lib.qsv_exact_probs(self.handle, float(threshold), None, None, 0, ctypes.byref(n)))
+        keys = np.empty(n.value, dtype=np.uint64)
+        probs = np.empty(n.value, dtype=np.float64)
+        if n.value:
+            got = ctypes.c_uint64()
+            check(lib.qsv_exact_probs(self.handle, float(threshold), u64ptr(keys), dptr(probs), n.value,
+                                      ctypes.byref(got)))
+            if got.value != n.value:
+                raise RuntimeError("exact readout count changed between passes")
+        return keys.astype(np.int64), probs
 
     # adjoint -------------------------------------------------------------------------
     def adjoint(self, stream: PackedStream, n_params: int, masks: PauliMasks):
@@ -302,6 +327,27 @@ class B200Simulator:
         reg.apply(pack(commands, values))
         return reg
 
+    def prepared_register(self, commands, n_qubits, initial_state=None, where="statevector") -> Register:
+        """The register after ``commands`` (concrete) from |0...0> or ``initial_state``; it stays
+        on the device for further readouts."""
+        return self._prepared(list(commands), n_qubits, initial_state, where)
+
+    def prepared_program_register(self, program, n_qubits, initial_state=None,
+                                  where="program_statevector") -> Register:
+        prog = as_program(program)
+        _check_program_width(prog, n_qubits, where)
+        return self._prepared(prog.to_stream(), n_qubits, initial_state, where)
+
+    def exact_result(self, commands, n_qubits: int, initial_state=None):
+        """Exact Born distribution (the engine's _exact_result, _engine.py:79-99), compacted on
+        the device."""
+        from .readout import exact_result
+        return exact_result(self, commands, n_qubits, initial_state)
+
+    def exact_program_result(self, program, n_qubits: int, initial_state=None):
+        from .readout import exact_program_result
+        return exact_program_result(self, program, n_qubits, initial_state)
+
     # QarpSimulator surface ---------------------------------------------------------------
     def statevector(self, commands, n_qubits: int, *, initial_state=None) -> np.ndarray:
         """Final amplitudes of ``commands`` from |0...0> (or ``initial_state``)
@@ -359,10 +405,41 @@ class B200Simulator:
         return out
 
     def program_statevector(self, program, n_qubits: int, *, initial_state=None) -> np.ndarray:
-        return self.statevector(_gates_of(program), n_qubits, initial_state=initial_state)
+        """statevector() for a structured program (QarpSimulator::program_statevector,
+        qarp_simulator.cpp:821-849): permutation, dense and controlled-powers kernels run as
+        device records between the fused gate slices."""
+        prog = as_program(program)
+        _check_program_width(prog, n_qubits, "program_statevector")
+        for k in prog.kernels():
+            if isinstance(k, GatesKernel) and any(needs_trajectory(c) for c in k.commands):
+                raise RuntimeError(
+                    "QarpSimulator::program_statevector: program contains mid-circuit "
+                    "measurement, Reset, or classical condition — statevector is not "
+                    "deterministic.")
+        return self._prepared(prog.to_stream(), n_qubits, initial_state,
+                              "program_statevector").get_state()
 
     def program_run(self, program, n_qubits: int, n_shots: int, seed=None, *, initial_state=None):
-        return self.run(_gates_of(program), n_qubits, n_shots, seed, initial_state=initial_state)
+        """run()'s terminal sample-once path for a structured program
+        (QarpSimulator::program_run, qarp_simulator.cpp:851-897)."""
+        prog = as_program(program)
+        _check_program_width(prog, n_qubits, "program_run")
+        kernels = prog.kernels()
+        last = None
+        for i, k in enumerate(kernels):
+            if not isinstance(k, GatesKernel):
+                continue
+            if i + 1 == len(kernels):
+                last = list(k.commands)
+            elif any(needs_trajectory(c) for c in k.commands):
+                raise ValueError("QarpSimulator::program_run: a measurement or classical condition "
+                                 "outside the program's last gates kernel")
+        if last is not None and not measurements_are_terminal(last):
+            raise ValueError("QarpSimulator::program_run: the last gates kernel's measurements are "
+                             "not terminal")
+        base_s = int(seed) if seed is not None else int.from_bytes(os.urandom(4), "little")
+        reg = self._prepared(prog.to_stream(), n_qubits, initial_state, "program_run")
+        return self._sample_result(reg, last or [], n_qubits, n_shots, base_s)
 
     def transition(self, bra, ket, n_qubits: int, observable) -> complex:
         """<bra|H|ket> over caller host statevectors (QarpSimulator::transition,
@@ -463,15 +540,9 @@ class B200Simulator:
         return u
 
 
-def _gates_of(program):
-    """Flatten a structured program whose kernels are all gate kernels; the typed
-    Permutation / Dense / ControlledPowers kernels are not on the B200 path yet."""
-    kernels = program.kernels() if callable(getattr(program, "kernels", None)) else program
-    out = []
-    for k in kernels:
-        cmds = getattr(k, "commands", None)
-        if cmds is None:
-            raise CapabilityError("B200Simulator: structured Permutation / Dense / ControlledPowers "
-                                  "kernels are not supported; run the gate path (structured=False)")
-        out.extend(cmds)
-    return out
+def _check_program_width(program, n_qubits: int, where: str) -> None:
+    """check_program_width (qarp_simulator.cpp:812-819)."""
+    width = program.min_register_width
+    if n_qubits < 0 or width > n_qubits:
+        raise ValueError(f"QarpSimulator::{where}: a kernel acts on qubit {width - 1} of a "
+                         f"{n_qubits}-qubit register")

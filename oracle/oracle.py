@@ -25,6 +25,7 @@ PD = POINTER(c_double)
 PU64 = POINTER(c_uint64)
 PI32 = POINTER(c_int32)
 P8 = POINTER(c_uint8)
+PU32 = POINTER(c_uint32)
 
 
 def build(reference: bool = True) -> None:
@@ -44,6 +45,10 @@ def _u64(a):
 
 def _i32(a):
     return a.ctypes.data_as(PI32)
+
+
+def _u32(a):
+    return a.ctypes.data_as(PU32)
 
 
 def _u8(b: bytes):
@@ -162,6 +167,17 @@ class Reference:
         lib.qref_uniforms.argtypes = [c_uint32, c_size_t, PD]
         lib.qref_run_gradient.argtypes = [P8, c_size_t, c_int, PI32, PI32, PD, c_int, PD, PU64, PU64, PD,
                                           c_size_t, PD, PD]
+        lib.qref_program_new.restype = ctypes.c_void_p
+        lib.qref_program_free.argtypes = [ctypes.c_void_p]
+        lib.qref_program_add_gates.argtypes = [ctypes.c_void_p, P8, c_size_t]
+        lib.qref_program_add_permutation.argtypes = [ctypes.c_void_p, PU32, c_int, PU64, c_size_t]
+        lib.qref_program_add_dense.argtypes = [ctypes.c_void_p, PU32, c_int, PD, c_int]
+        lib.qref_program_add_controlled_powers.argtypes = [ctypes.c_void_p, PU32, PU64, c_int, PU32, c_int,
+                                                           PD, c_int]
+        lib.qref_program_kinds.argtypes = [ctypes.c_void_p, PI32, c_size_t, POINTER(c_size_t)]
+        lib.qref_program_statevector.argtypes = [ctypes.c_void_p, c_int, c_int, c_int, PD, PD]
+        lib.qref_program_run.argtypes = [ctypes.c_void_p, c_int, c_int, c_uint32, PU64, PI32, c_size_t,
+                                         POINTER(c_size_t)]
         self.lib = lib
 
     @staticmethod
@@ -229,6 +245,74 @@ class Reference:
         u = np.zeros(shots)
         self._check(self.lib.qref_uniforms(seed & 0xFFFFFFFF, shots, _d(u)))
         return u
+
+    # structured programs ------------------------------------------------------------------
+    # A program is given as a list of kernel specs:
+    #   ("gates", packed_buf) | ("permutation", qubits, table) | ("dense", qubits, matrix) |
+    #   ("controlled_powers", controls, exponents, targets, matrix)
+    def _program(self, specs):
+        h = self.lib.qref_program_new()
+        try:
+            for sp in specs:
+                kind = sp[0]
+                if kind == "gates":
+                    self._check(self.lib.qref_program_add_gates(h, _u8(sp[1]), len(sp[1])))
+                elif kind == "permutation":
+                    q = np.ascontiguousarray(sp[1], dtype=np.uint32)
+                    t = np.ascontiguousarray(sp[2], dtype=np.uint64)
+                    self._check(self.lib.qref_program_add_permutation(h, _u32(q), len(q), _u64(t), t.size))
+                elif kind == "dense":
+                    q = np.ascontiguousarray(sp[1], dtype=np.uint32)
+                    m = np.ascontiguousarray(sp[2], dtype=np.complex128)
+                    self._check(self.lib.qref_program_add_dense(h, _u32(q), len(q), _d(m.view(np.float64)),
+                                                                m.shape[0]))
+                else:
+                    c = np.ascontiguousarray(sp[1], dtype=np.uint32)
+                    e = np.ascontiguousarray(sp[2], dtype=np.uint64)
+                    t = np.ascontiguousarray(sp[3], dtype=np.uint32)
+                    m = np.ascontiguousarray(sp[4], dtype=np.complex128)
+                    self._check(self.lib.qref_program_add_controlled_powers(
+                        h, _u32(c), _u64(e), len(c), _u32(t), len(t), _d(m.view(np.float64)), m.shape[0]))
+        except Exception:
+            self.lib.qref_program_free(h)
+            raise
+        return h
+
+    def program_kinds(self, specs) -> list:
+        h = self._program(specs)
+        try:
+            out = np.zeros(len(specs) + 1, dtype=np.int32)
+            got = c_size_t()
+            self._check(self.lib.qref_program_kinds(h, _i32(out), out.size, ctypes.byref(got)))
+            names = ["permutation", "dense", "controlled_powers", "gates"]
+            return [names[int(v)] for v in out[:got.value]]
+        finally:
+            self.lib.qref_program_free(h)
+
+    def program_statevector(self, specs, n, initial=None, fusion_max=-1, fusion_min=-1):
+        h = self._program(specs)
+        try:
+            out = np.zeros(1 << n, dtype=np.complex128)
+            init = None if initial is None else np.ascontiguousarray(initial, dtype=np.complex128)
+            self._check(self.lib.qref_program_statevector(
+                h, n, fusion_max, fusion_min, _d(init.view(np.float64)) if init is not None else None,
+                _d(out.view(np.float64))))
+            return out
+        finally:
+            self.lib.qref_program_free(h)
+
+    def program_run(self, specs, n, shots, seed) -> dict:
+        h = self._program(specs)
+        try:
+            cap = max(1, min(shots, 1 << n))
+            keys = np.zeros(cap, dtype=np.uint64)
+            cnts = np.zeros(cap, dtype=np.int32)
+            got = c_size_t()
+            self._check(self.lib.qref_program_run(h, n, shots, seed & 0xFFFFFFFF, _u64(keys), _i32(cnts), cap,
+                                                  ctypes.byref(got)))
+            return {int(keys[i]): int(cnts[i]) for i in range(got.value)}
+        finally:
+            self.lib.qref_program_free(h)
 
     def run_gradient(self, stream, n, n_params, param_values, masks, initial=None):
         grad = np.zeros(max(n_params, 1))

@@ -45,7 +45,9 @@ enum {
     G_CH, G_CS, G_CSDG, G_CSX, G_CSXDG,
     G_CRX, G_CRY, G_CRZ, G_CP, G_RZZ, G_RXX, G_RYY,
     G_CU, G_CCX, G_CSWAP, G_MCZ, G_GPHASE,
-    G_BARRIER, G_MEASURE, G_RESET, G_BBEGIN, G_BELSE, G_BEND, G_CUSTOM
+    G_BARRIER, G_MEASURE, G_RESET, G_BBEGIN, G_BELSE, G_BEND, G_CUSTOM,
+    /* structured-program records of include/qsv.h */
+    G_PERMUTATION = 200, G_CTRL_UNITARY = 201
 };
 
 /* ---------------------------------------------------------------- command decoding */
@@ -54,7 +56,8 @@ typedef struct {
     int gate, nq, np, ncb, flags;
     const uint32_t* q;
     const double* p;
-    const double* m;   /* Custom matrix (interleaved) or NULL */
+    const double* m;   /* Custom / controlled-unitary matrix (interleaved) or NULL */
+    const uint64_t* t; /* permutation table or NULL */
     size_t size;       /* bytes of the record */
 } rec_t;
 
@@ -70,10 +73,19 @@ static int decode(const uint8_t* buf, size_t nbytes, size_t off, rec_t* r) {
     r->p = (const double*)(buf + o);
     o += 8u * (size_t)r->np;
     r->m = NULL;
+    r->t = NULL;
     if (r->gate == G_CUSTOM) {
         if (r->nq < 1 || r->nq > 8) return fail(2, "Custom gate must carry 1..8 qubit targets");
         r->m = (const double*)(buf + o);
         o += 16u * ((size_t)1 << (2 * r->nq));
+    } else if (r->gate == G_PERMUTATION) {
+        if (r->nq < 1 || r->nq > 26) return fail(1, "permutation must act on 1..26 qubits");
+        r->t = (const uint64_t*)(buf + o);
+        o += 8u * ((size_t)1 << r->nq);
+    } else if (r->gate == G_CTRL_UNITARY) {
+        if (r->nq < 2 || r->nq > 13) return fail(1, "controlled unitary must act on 1..12 targets + 1 control");
+        r->m = (const double*)(buf + o);
+        o += 16u * ((size_t)1 << (2 * (r->nq - 1)));
     }
     if (o > nbytes) return fail(1, "command buffer truncated (payload)");
     r->size = o - off;
@@ -175,6 +187,67 @@ static void k_dense(cplx* s, int n, int k, const uint32_t* qubits, const double*
             s[base | masks[y]] = acc;
         }
     }
+}
+
+/* |x> -> |table[x]> on qubits[0..k), out of place then copied back
+ * (apply_permutation, src/qarpx/src/simulator/program.cpp:610-643) */
+static int k_permutation(cplx* s, int n, int k, const uint32_t* qubits, const uint64_t* table) {
+    const uint64_t dim = 1ull << n;
+    uint64_t keep = ~0ull;
+    for (int b = 0; b < k; ++b) keep &= ~(1ull << qubits[b]);
+    cplx* out = (cplx*)malloc(dim * sizeof(cplx));
+    if (!out) return fail(2, "out of memory");
+    for (uint64_t i = 0; i < dim; ++i) {
+        uint64_t x = 0, j = i & keep;
+        for (int b = 0; b < k; ++b) x |= ((i >> qubits[b]) & 1ull) << b;
+        const uint64_t y = table[x];
+        for (int b = 0; b < k; ++b) j |= ((y >> b) & 1ull) << qubits[b];
+        out[j] = s[i];
+    }
+    memcpy(s, out, dim * sizeof(cplx));
+    free(out);
+    return 0;
+}
+
+/* one (control, power) step of apply_controlled_powers (program.cpp:680-708): the m-target
+ * matrix on every group whose control bit is set */
+static int k_controlled_dense(cplx* s, int n, int m, const uint32_t* targets, uint32_t control,
+                              const double* mat) {
+    const uint64_t d = 1ull << m, cbit = 1ull << control;
+    uint32_t sorted[16];
+    for (int b = 0; b < m; ++b) sorted[b] = targets[b];
+    for (int a = 0; a < m; ++a)
+        for (int b = a + 1; b < m; ++b)
+            if (sorted[b] < sorted[a]) { uint32_t t = sorted[a]; sorted[a] = sorted[b]; sorted[b] = t; }
+    uint64_t* off = (uint64_t*)malloc(d * sizeof(uint64_t));
+    cplx* col = (cplx*)malloc(d * sizeof(cplx));
+    if (!off || !col) { free(off); free(col); return fail(2, "out of memory"); }
+    for (uint64_t l = 0; l < d; ++l) {
+        uint64_t o = 0;
+        for (int b = 0; b < m; ++b) if ((l >> b) & 1) o |= 1ull << targets[b];
+        off[l] = o;
+    }
+    const uint64_t outer = (1ull << n) >> m;
+    for (uint64_t o = 0; o < outer; ++o) {
+        uint64_t base = o;
+        for (int b = 0; b < m; ++b) {
+            const uint64_t p = sorted[b];
+            base = ((base >> p) << (p + 1)) | (base & ((1ull << p) - 1));
+        }
+        if (!(base & cbit)) continue;
+        for (uint64_t l = 0; l < d; ++l) col[l] = s[base | off[l]];
+        for (uint64_t y = 0; y < d; ++y) {
+            cplx acc = 0.0;
+            for (uint64_t x = 0; x < d; ++x) {
+                const double* e = mat + 2 * (y * d + x);
+                acc += (e[0] + I * e[1]) * col[x];
+            }
+            s[base | off[y]] = acc;
+        }
+    }
+    free(off);
+    free(col);
+    return 0;
 }
 
 /* ---------------------------------------------------------------- gate matrices */
@@ -361,6 +434,10 @@ static int apply_rec(cplx* s, int n, const rec_t* r) {
                 k_dense(s, n, r->nq, r->q, r->m);
             }
             return 0;
+        case G_PERMUTATION:
+            return k_permutation(s, n, r->nq, r->q, r->t);
+        case G_CTRL_UNITARY:
+            return k_controlled_dense(s, n, r->nq - 1, r->q, r->q[r->nq - 1], r->m);
         default:
             return fail(2, "unsupported gate");
     }

@@ -13,12 +13,15 @@
 //   qref_run           -> QarpSimulator::run                (qarp_simulator.cpp:988-1244)
 //   qref_run_gradient  -> QarpSimulator::run_gradient       (qarp_simulator.cpp:1607-1618)
 //   qref_fuse_count    -> fuse_for_simulation               (fusion.cpp:120-268), block count
+//   qref_program_*     -> qarpx::Program + QarpSimulator::program_statevector / program_run
+//                         (program.h:51-86, qarp_simulator.cpp:821-897)
 //
 // Used by tests/ (parity pins, golden fixture generation) and by bench.py's reference arm
 // (the reference's own CPU implementation timed on the host cores).
 #include "../include/qsv.h"
 
 #include "qarpx/simulator/qarp_simulator.h"
+#include "qarpx/simulator/program.h"
 #include "qarpx/simulator/fusion.h"
 #include "qarpx/transpiler/fusion.h"
 #include "qarpx/core/param.h"
@@ -145,6 +148,13 @@ std::optional<std::vector<cd>> initial(const double* init, int n) {
     const size_t dim = size_t{1} << n;
     const cd* p = reinterpret_cast<const cd*>(init);
     return std::vector<cd>(p, p + dim);
+}
+
+Eigen::MatrixXcd to_matrix(const double* m, int D) {
+    Eigen::MatrixXcd U(D, D);
+    for (int y = 0; y < D; ++y)
+        for (int x = 0; x < D; ++x) U(y, x) = cd(m[2 * (y * D + x)], m[2 * (y * D + x) + 1]);
+    return U;
 }
 
 }  // namespace
@@ -331,6 +341,95 @@ int qref_run_gradient(const uint8_t* cmds, size_t nbytes, int n, const int32_t* 
         auto g = sim.run_gradient(cs, n, to_observable(xm, zm, coeff, nt), values, order,
                                   initial(init, n));
         for (int p = 0; p < n_params; ++p) grad[p] = g[static_cast<size_t>(p)];
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+// ---- structured programs: the reference's own Program, kernel by kernel
+void* qref_program_new() { return new qarpx::Program(); }
+void qref_program_free(void* p) { delete static_cast<qarpx::Program*>(p); }
+
+int qref_program_add_gates(void* p, const uint8_t* cmds, size_t nbytes) {
+    try {
+        static_cast<qarpx::Program*>(p)->add_gates(to_commands(cmds, nbytes));
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_program_add_permutation(void* p, const uint32_t* qubits, int k, const uint64_t* table,
+                                 size_t table_len) {
+    try {
+        static_cast<qarpx::Program*>(p)->add_permutation(
+            std::vector<uint32_t>(qubits, qubits + k), std::vector<uint64_t>(table, table + table_len));
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_program_add_dense(void* p, const uint32_t* qubits, int k, const double* m, int dim) {
+    try {
+        static_cast<qarpx::Program*>(p)->add_dense(std::vector<uint32_t>(qubits, qubits + k),
+                                                   to_matrix(m, dim));
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_program_add_controlled_powers(void* p, const uint32_t* controls, const uint64_t* exps, int nc,
+                                       const uint32_t* targets, int nt, const double* m, int dim) {
+    try {
+        static_cast<qarpx::Program*>(p)->add_controlled_powers(
+            std::vector<uint32_t>(controls, controls + nc), std::vector<uint64_t>(exps, exps + nc),
+            std::vector<uint32_t>(targets, targets + nt), to_matrix(m, dim));
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+// kinds as codes: 0 permutation, 1 dense, 2 controlled_powers, 3 gates
+int qref_program_kinds(void* p, int32_t* out, size_t cap, size_t* n_out) {
+    const auto kinds = static_cast<qarpx::Program*>(p)->kinds();
+    size_t i = 0;
+    for (const auto& k : kinds) {
+        if (i >= cap) break;
+        out[i++] = k == "permutation" ? 0 : k == "dense" ? 1 : k == "controlled_powers" ? 2 : 3;
+    }
+    *n_out = kinds.size();
+    return QSV_OK;
+}
+
+int qref_program_statevector(void* p, int n, int fusion_max, int fusion_min, const double* init,
+                             double* out) {
+    try {
+        auto sim = make_sim(fusion_max, fusion_min);
+        auto sv = sim.program_statevector(*static_cast<qarpx::Program*>(p), n, initial(init, n));
+        std::memcpy(out, sv.data(), sv.size() * sizeof(cd));
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+int qref_program_run(void* p, int n, int shots, uint32_t seed, uint64_t* keys, int32_t* counts,
+                     size_t cap, size_t* n_out) {
+    try {
+        auto sim = make_sim(-1, -1);
+        auto res = sim.program_run(*static_cast<qarpx::Program*>(p), n, shots, seed);
+        size_t i = 0;
+        for (const auto& [k, v] : res.counts) {
+            if (i >= cap) throw std::invalid_argument("qref_program_run: output capacity too small");
+            keys[i] = k;
+            counts[i] = v;
+            ++i;
+        }
+        *n_out = i;
         return QSV_OK;
     } catch (...) {
         return translate(std::current_exception());
