@@ -14,7 +14,10 @@ Also reported on the same line:
   * adjoint: 24-qubit HEA (8 layers, 384 parameters) with TFIM + 500 random weight<=4
     terms, gradients/s of the adjoint sweep vs the parameter-shift rule on the same GPU;
   * cpu_baseline: the reference's own CPU simulator (oracle/_ref) on the host cores over a
-    bounded sample of the same workload.
+    bounded sample of the same workload;
+  * structured_and_readouts: a phase-estimation-shaped structured program (controlled powers
+    + inverse QFT) at 28 and 22 qubits with the reference's CPU program_statevector at 22, the
+    exact Born readout and the PauliAveraging parity counts on the device.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 """
@@ -507,6 +510,11 @@ def b200_arm(args, rank, world, local_rank):
         if not args.skip_ksweep:
             reg.close()
             sweep_k = k_sweep(device, buf)
+        structured = None
+        if not args.skip_structured:
+            reg.close()
+            from openqarp_b200.workloads import structured_rows
+            structured = structured_rows(device=device)
         heis = None
         if not args.skip_heisenberg:
             reg.close()
@@ -545,6 +553,7 @@ def b200_arm(args, rank, world, local_rank):
             "k_sweep_28q": sweep_k,
             "heisenberg31_c64_bulk": heis,
             "qaoa_batched": qaoa,
+            "structured_and_readouts": structured,
         }
     else:
         reg.close()
@@ -562,6 +571,7 @@ def main():
     ap.add_argument("--skip-heisenberg", action="store_true")
     ap.add_argument("--skip-qaoa", action="store_true")
     ap.add_argument("--skip-ksweep", action="store_true")
+    ap.add_argument("--skip-structured", action="store_true")
     ap.add_argument("--executor", type=int, default=None, choices=[0, 1],
                     help="pin the executor (0 stream, 1 tiled) instead of autotuning; needs --k")
     ap.add_argument("--k", type=int, default=None, help="pin the fusion width; needs --executor")

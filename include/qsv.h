@@ -171,6 +171,13 @@ QSV_API int qsv_copy_state(void* dst, const void* src);
  * (reference: qarp_simulator.cpp:120-129, fusion.cpp:120-268) for plan inspection. */
 QSV_API int qsv_fuse_count(const uint8_t* cmds, size_t nbytes, int n_qubits, int max_qubits,
                            int min_qubits, int32_t* n_out, int32_t* widths_hist);
+/* Host-only (no device work): the tiled executor's plan for a stream — how many
+ * shared-memory tile passes and how many single-op HBM passes (ops a tile cannot hold) it
+ * launches for the given fusion knobs and tile width (0 = the default for complex128).  An
+ * engine extension with no reference counterpart: plan inspection for tuning. */
+QSV_API int qsv_tile_plan_count(const uint8_t* cmds, size_t nbytes, int n_qubits, int max_qubits,
+                                int min_qubits, int tile_qubits, int32_t* tile_passes,
+                                int32_t* stream_passes);
 
 /* Apply a packed command stream in place, after the simulation-fusion pass the handle's
  * knobs select.  Replaces the `for cmd in fused: apply_command` loop of

@@ -385,6 +385,24 @@ int qsv_fuse_count(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min
     });
 }
 
+int qsv_tile_plan_count(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min_q, int tile_qubits,
+                        int32_t* tile_passes, int32_t* stream_passes) {
+    return guarded([&] {
+        if (!tile_passes || !stream_passes) throw std::invalid_argument("null output");
+        if (max_q < 0 || max_q > QSV_MAX_BLOCK_QUBITS) throw std::invalid_argument("fusion width out of range");
+        if (n < kTileMinQubits || n > QSV_MAX_QUBITS) throw std::invalid_argument("register too narrow for tiles");
+        const int m = tile_qubits > 0 ? std::min(tile_qubits, n) : default_tile_qubits(n, 16);
+        if (m < kTileMinQubits || m > kTileMaxQubits) throw std::invalid_argument("tile width out of range");
+        std::vector<Op> ops;
+        for (const Cmd& c : fuse_for_dispatch(decode(cmds, nbytes), n, max_q, min_q))
+            for (Op& o : lower(c, n)) ops.push_back(std::move(o));
+        int32_t t = 0, st = 0;
+        for (const TilePass& p : plan_tiles(ops, n, m)) (p.tile_qubits.empty() ? st : t)++;
+        *tile_passes = t;
+        *stream_passes = st;
+    });
+}
+
 int qsv_apply(void* hp, const uint8_t* cmds, size_t nbytes) {
     return guarded([&] {
         Handle* h = H_(hp);

@@ -59,3 +59,119 @@ def heisenberg_bulk(n: int = 31, steps: int = 50, dt: float = 0.05, seed: int = 
         r128.close()
     r64.close()
     return out
+
+
+# ---------------------------------------------------------------- structured programs / readouts
+
+def qpe_program(n_count: int, n_target: int, seed: int = 1234):
+    """Phase-estimation shape as a structured program: Hadamards on the counting qubits
+    0..n_count-1, one controlled-powers kernel U^(2^j) under counting qubit j on the target
+    register (U a seeded Haar unitary on n_target qubits), then the inverse QFT on the counting
+    register as a gates kernel (H, controlled phases, reversing swaps)."""
+    from .program import Program
+    G = ir.GateType
+    rng = np.random.default_rng(seed)
+    d = 1 << n_target
+    z = (rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))) / np.sqrt(2)
+    q, r = np.linalg.qr(z)
+    u = q * (np.diag(r) / np.abs(np.diag(r)))
+    cnt = list(range(n_count))
+    tgt = list(range(n_count, n_count + n_target))
+    p = Program()
+    p.add_gates([ir.Command(G.H, (c,)) for c in cnt])
+    p.add_controlled_powers(cnt, [1 << j for j in range(n_count)], tgt, u)
+    iqft = []
+    for a in range(n_count // 2):
+        iqft.append(ir.Command(G.SWAP, (a, n_count - 1 - a)))
+    for j in range(n_count):
+        for k in range(j):
+            iqft.append(ir.Command(G.CP, (k, j), (-np.pi / (1 << (j - k)),)))
+        iqft.append(ir.Command(G.H, (j,)))
+    p.add_gates(iqft)
+    return p
+
+
+def structured_rows(device: int = 0, n_big: int = 28, n_small: int = 22, shots: int = 1 << 20,
+                    n_masks: int = 512, seed: int = 1234) -> dict:
+    """Measurements of the structured-program and readout paths:
+
+    * qpe: program_statevector-equivalent device time of ``qpe_program`` at n_big and n_small
+      qubits (4 target qubits), and the reference CPU simulator's own program_statevector at
+      n_small on the host cores (oracle/_ref), so the ratio is taken on the same workload;
+    * exact readout: device time of the ordered |a|^2 > 1e-12 compaction of an n_big brickwork
+      register (count pass, and count + write pass with the survivors copied to host);
+    * parities: seeded sampling of ``shots`` outcomes plus the odd-parity counts of ``n_masks``
+      Z masks on the device, against the same counts by numpy on the host outcomes."""
+    from . import Register
+    from .ir import pack
+    out = {}
+    for n in (n_big, n_small):
+        prog = qpe_program(n - 4, 4, seed)
+        buf = pack(prog.to_stream()).buf
+        reg = Register(n, "complex128", device)
+        reg.configure(3, 12, 0)
+        reg.apply(buf)
+        reg.synchronize()
+        times = []
+        for _ in range(3):
+            reg.reset()
+            reg.synchronize()
+            t0 = time.perf_counter()
+            reg.apply(buf)
+            reg.synchronize()
+            times.append(time.perf_counter() - t0)
+        out[f"qpe_{n}q_ms"] = 1e3 * float(np.median(times))
+        reg.close()
+    try:
+        import os
+        from oracle.oracle import Reference
+        ref = Reference()
+        cores = ref.set_threads(os.cpu_count() or 1)
+        prog = qpe_program(n_small - 4, 4, seed)
+        specs = []
+        for k in prog.kernels():
+            if hasattr(k, "commands"):
+                specs.append(("gates", pack(k.commands).buf))
+            elif hasattr(k, "controls"):
+                specs.append(("controlled_powers", k.controls, k.exponents, k.targets, k.matrix))
+        t0 = time.perf_counter()
+        ref.program_statevector(specs, n_small)
+        out[f"qpe_{n_small}q_reference_cpu_ms"] = 1e3 * (time.perf_counter() - t0)
+        out["reference_cpu_cores"] = cores
+        out[f"qpe_{n_small}q_speedup"] = out[f"qpe_{n_small}q_reference_cpu_ms"] / out[f"qpe_{n_small}q_ms"]
+    except (FileNotFoundError, ImportError, OSError):
+        out["reference_cpu"] = "oracle/_ref not built on this machine"
+
+    reg = Register(n_big, "complex128", device)
+    reg.configure(4, 12, 0)
+    reg.apply(pack(circuits.brickwork(n_big, 4, seed=seed)).buf)
+    reg.synchronize()
+    import ctypes
+    from ._lib import lib, check
+    cnt = ctypes.c_uint64()
+    t0 = time.perf_counter()
+    check(lib.qsv_exact_probs(reg.handle, 1e-12, None, None, 0, ctypes.byref(cnt)))
+    out["exact_count_pass_ms"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    keys, probs = reg.exact_probs(1e-12)
+    out["exact_readout_ms"] = 1e3 * (time.perf_counter() - t0)
+    out["exact_survivors"] = int(keys.shape[0])
+    del keys, probs
+    rng = np.random.default_rng(seed)
+    masks = rng.integers(0, 1 << n_big, size=n_masks).astype(np.uint64)
+    reg.sample_parities(7, shots, masks)
+    t0 = time.perf_counter()
+    odd = reg.sample_parities(7, shots, masks)
+    out["parities_ms"] = 1e3 * (time.perf_counter() - t0)
+    idx = reg.sample_seeded(7, shots)
+    t0 = time.perf_counter()
+    keys_h, cnt_h = np.unique(idx.astype(np.int64), return_counts=True)
+    x = keys_h[:, None] & masks.astype(np.int64)[None, :]
+    for sh in (32, 16, 8, 4, 2, 1):
+        x = x ^ (x >> sh)
+    host_odd = cnt_h.astype(np.float64) @ (x & 1).astype(np.float64)
+    out["parities_numpy_ms"] = 1e3 * (time.perf_counter() - t0)
+    out["parities_match"] = bool(np.array_equal(host_odd.astype(np.int64), odd))
+    out["parities_config"] = f"{shots} shots, {n_masks} Z masks, {n_big}-qubit brickwork depth 4"
+    reg.close()
+    return out
