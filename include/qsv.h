@@ -144,8 +144,10 @@ QSV_API int qsv_destroy(void* h);
  * set_fusion_max_qubits, qarp_simulator.cpp:82-88) and fusion_min_qubits
  * (qarp_simulator.h:73-74). */
 QSV_API int qsv_set_fusion(void* h, int max_qubits, int min_qubits);
-/* Executor: 0 = one HBM pass per fused block ("stream"), 1 = several blocks per pass
- * staged in shared memory ("tiled"), -1 = the autotuned choice (default). */
+/* Executor: 0 = one HBM pass per fused block ("stream"), 1 = several ops per pass on
+ * 2^12-amplitude tiles held in registers, with shared-memory transposes between layouts
+ * ("tiled"; passes it cannot hold fall back to 2), 2 = several ops per pass applied to tiles
+ * staged in shared memory, -1 = the default (stream). */
 QSV_API int qsv_set_executor(void* h, int mode);
 /* Tile width of the tiled executor: qubits held in shared memory per tile, 8..13
  * (0 = the default: 12 for complex128, 13 for complex64).  No reference counterpart: the

@@ -18,7 +18,7 @@ namespace {
 
 constexpr int kRoLog = 12;                       // amplitudes per chunk = 4096
 constexpr int kRoThreads = 256;
-constexpr int kRoPer = (1 << kRoLog) / kRoThreads;   // 16 consecutive amplitudes per thread
+constexpr int kRoPer = (1 << kRoLog) / kRoThreads;   // 16 rounds of 256 amplitudes per chunk
 constexpr int kScanThreads = 1024;
 
 template <typename T>
@@ -54,17 +54,19 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
     return warp_tot[warp] + incl - v;
 }
 
+// Chunk c covers amplitudes [c * 4096, (c + 1) * 4096).  Round j of a chunk is the 256
+// consecutive amplitudes start + 256 j + threadIdx.x: every load instruction is coalesced.
 template <typename T>
 __global__ void __launch_bounds__(kRoThreads) k_exact_count(const vec2_t<T>* __restrict__ s, uint64_t dim,
                                                             double thr, uint32_t* __restrict__ counts) {
     __shared__ uint32_t warp_tot[32];
     __shared__ uint32_t total;
-    const uint64_t start = (static_cast<uint64_t>(blockIdx.x) << kRoLog) + static_cast<uint64_t>(threadIdx.x) * kRoPer;
+    const uint64_t start = static_cast<uint64_t>(blockIdx.x) << kRoLog;
     uint32_t c = 0;
 #pragma unroll
     for (int r = 0; r < kRoPer; ++r) {
-        const uint64_t i = start + r;
-        if (i < dim && born<T>(s[i]) > thr) ++c;
+        const uint64_t i = start + static_cast<uint64_t>(r) * kRoThreads + threadIdx.x;
+        if (i < dim && born<T>(__ldcs(s + i)) > thr) ++c;
     }
     block_exclusive_scan(c, warp_tot, &total);
     if (threadIdx.x == 0) counts[blockIdx.x] = total;
@@ -97,30 +99,44 @@ __global__ void __launch_bounds__(kScanThreads) k_exact_offsets(const uint32_t* 
     }
 }
 
+// Survivors of a chunk in index order: per round a warp ballot ranks the survivors of each
+// warp, a shared-memory prefix over the 8 warps places the warps, and the round total advances
+// the chunk's running offset.
 template <typename T>
 __global__ void __launch_bounds__(kRoThreads) k_exact_write(const vec2_t<T>* __restrict__ s, uint64_t dim, double thr,
                                                             const uint64_t* __restrict__ off,
                                                             uint64_t* __restrict__ keys, double* __restrict__ probs) {
-    __shared__ uint32_t warp_tot[32];
-    __shared__ uint32_t total;
-    const uint64_t start = (static_cast<uint64_t>(blockIdx.x) << kRoLog) + static_cast<uint64_t>(threadIdx.x) * kRoPer;
+    constexpr int kWarps = kRoThreads / 32;
+    __shared__ uint32_t wcount[kRoPer][kWarps];
+    const uint64_t start = static_cast<uint64_t>(blockIdx.x) << kRoLog;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
     double p[kRoPer];
-    uint32_t c = 0;
+    uint32_t ball[kRoPer];
 #pragma unroll
     for (int r = 0; r < kRoPer; ++r) {
-        const uint64_t i = start + r;
-        p[r] = i < dim ? born<T>(s[i]) : 0.0;
-        if (i < dim && p[r] > thr) ++c;
+        const uint64_t i = start + static_cast<uint64_t>(r) * kRoThreads + threadIdx.x;
+        p[r] = i < dim ? born<T>(__ldcs(s + i)) : 0.0;
+        ball[r] = __ballot_sync(0xffffffffu, i < dim && p[r] > thr);
+        if (lane == 0) wcount[r][warp] = __popc(ball[r]);
     }
-    uint64_t o = off[blockIdx.x] + block_exclusive_scan(c, warp_tot, &total);
+    __syncthreads();
+    uint64_t o = off[blockIdx.x];
 #pragma unroll
     for (int r = 0; r < kRoPer; ++r) {
-        const uint64_t i = start + r;
-        if (i < dim && p[r] > thr) {
-            keys[o] = i;
-            probs[o] = p[r];
-            ++o;
+        uint32_t before = 0, round = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = wcount[r][w];
+            before += w < warp ? c : 0u;
+            round += c;
         }
+        if ((ball[r] >> lane) & 1u) {
+            const uint64_t dst = o + before + __popc(ball[r] & lt);
+            keys[dst] = start + static_cast<uint64_t>(r) * kRoThreads + threadIdx.x;
+            probs[dst] = p[r];
+        }
+        o += round;
     }
 }
 

@@ -52,10 +52,11 @@ void Workspace::release() {
     if (scr_) cudaFree(scr_);
     if (shot_) cudaFree(shot_);
     if (tile_) cudaFree(tile_);
+    if (rtile_) cudaFree(rtile_);
     if (host_) cudaFreeHost(host_);
-    mat_ = copy_ = scr_ = shot_ = tile_ = nullptr;
+    mat_ = copy_ = scr_ = shot_ = tile_ = rtile_ = nullptr;
     host_ = nullptr;
-    mat_cap_ = copy_cap_ = scr_cap_ = shot_cap_ = tile_cap_ = host_cap_ = 0;
+    mat_cap_ = copy_cap_ = scr_cap_ = shot_cap_ = tile_cap_ = rtile_cap_ = host_cap_ = 0;
 }
 
 namespace {

@@ -298,12 +298,25 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
 // Encode the passes for the device and launch them in order on `st`.
 template <typename T>
 void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
-               const std::function<void(const Op&)>& stream_op) {
+               const std::function<void(const Op&)>& stream_op, bool register_tiles) {
+    // passes the register-tile kernel can run go there; the rest use shared-memory ops
+    std::vector<int> rt_idx(passes.size(), -1);
+    std::vector<const TilePass*> rt_passes;
+    if (register_tiles) {
+        RtPlan probe;
+        for (size_t i = 0; i < passes.size(); ++i)
+            if (!passes[i].tile_qubits.empty() && plan_rt(passes[i], &probe)) {
+                rt_idx[i] = static_cast<int>(rt_passes.size());
+                rt_passes.push_back(&passes[i]);
+            }
+    }
+    const RtUpload rt = encode_rt<T>(rt_passes, st, ws);
     std::vector<TilePassDev> pdev;
     std::vector<TileOpDev> odev;
     std::vector<cplx<T>> cdev;
-    for (const TilePass& p : passes) {
-        if (p.tile_qubits.empty()) continue;
+    for (size_t i = 0; i < passes.size(); ++i) {
+        const TilePass& p = passes[i];
+        if (p.tile_qubits.empty() || rt_idx[i] >= 0) continue;
         TilePassDev pd{};
         pd.m = static_cast<int32_t>(p.tile_qubits.size());
         for (size_t j = 0; j < p.tile_qubits.size(); ++j) pd.tq[j] = static_cast<uint8_t>(p.tile_qubits[j]);
@@ -405,9 +418,14 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
     check_cuda(cudaGetDevice(&device), "device");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
     int pi = 0;
-    for (const TilePass& p : passes) {
+    for (size_t i = 0; i < passes.size(); ++i) {
+        const TilePass& p = passes[i];
         if (p.tile_qubits.empty()) {
             for (const Op& o : p.ops) stream_op(o);
+            continue;
+        }
+        if (rt_idx[i] >= 0) {
+            launch_rt<T>(rt, rt_idx[i], s, n, st);
             continue;
         }
         const int m = static_cast<int>(p.tile_qubits.size());
@@ -425,8 +443,8 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
 }
 
 template void run_tiled<double>(const std::vector<TilePass>&, double2*, int, cudaStream_t, Workspace&,
-                                const std::function<void(const Op&)>&);
+                                const std::function<void(const Op&)>&, bool);
 template void run_tiled<float>(const std::vector<TilePass>&, float2*, int, cudaStream_t, Workspace&,
-                               const std::function<void(const Op&)>&);
+                               const std::function<void(const Op&)>&, bool);
 
 }  // namespace qsv

@@ -34,6 +34,7 @@ public:
     void* scratch(size_t bytes) { return grow(scr_, scr_cap_, bytes); }
     void* shots(size_t bytes) { return grow(shot_, shot_cap_, bytes); }
     void* tiles(size_t bytes) { return grow(tile_, tile_cap_, bytes); }
+    void* rt_tiles(size_t bytes) { return grow(rtile_, rtile_cap_, bytes); }
     // pinned host staging for small results
     double* host_result(size_t n_doubles);
 
@@ -44,6 +45,7 @@ private:
     void* scr_ = nullptr; size_t scr_cap_ = 0;
     void* shot_ = nullptr; size_t shot_cap_ = 0;
     void* tile_ = nullptr; size_t tile_cap_ = 0;
+    void* rtile_ = nullptr; size_t rtile_cap_ = 0;
     double* host_ = nullptr; size_t host_cap_ = 0;
 };
 
@@ -62,9 +64,24 @@ bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspac
 
 // ---------------------------------------------------------------- tiled executor (kern_tile.cu)
 // Launch the planned passes; one-op stream passes (empty tile_qubits) go to `stream_op`.
+// With register_tiles, passes plan_rt accepts run on the register-tile kernel.
 template <typename T>
 void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
-               const std::function<void(const Op&)>& stream_op);
+               const std::function<void(const Op&)>& stream_op, bool register_tiles);
+
+// ---------------------------------------------------------------- register tiles (kern_tile_rt.cu)
+struct RtUpload {
+    const void* passes = nullptr;
+    const void* steps = nullptr;
+    const void* coef = nullptr;
+    std::vector<size_t> extra_smem;   // per pass: shared memory for its steps and coefficients
+};
+// Plan (plan_rt) and upload the given register-tile-capable passes, in order.
+template <typename T>
+RtUpload encode_rt(const std::vector<const TilePass*>& passes, cudaStream_t st, Workspace& ws);
+// Launch the idx-th uploaded pass.
+template <typename T>
+void launch_rt(const RtUpload& u, int idx, vec2_t<T>* s, int n, cudaStream_t st);
 
 // ---------------------------------------------------------------- batched QAOA (kern_qaoa.cu)
 void* qaoa_create(int device, int n_inst, const int32_t* n_qubits, const int32_t* depth, const int32_t* edge_ptr,

@@ -135,7 +135,7 @@ void check_stream(const std::vector<Cmd>& cmds) {
 // least kTileMinQubits qubits.
 bool use_tiled(const Handle* h) {
     if (h->n < kTileMinQubits) return false;
-    return h->executor == 1;
+    return h->executor == 1 || h->executor == 2;
 }
 
 void apply_stream(Handle* h, const uint8_t* buf, size_t nbytes, bool fuse) {
@@ -152,8 +152,9 @@ void apply_stream(Handle* h, const uint8_t* buf, size_t nbytes, bool fuse) {
                                          : default_tile_qubits(h->n, static_cast<int>(h->amp_bytes()));
         const std::vector<TilePass> passes = plan_tiles(ops, h->n, m);
         auto stream_op = [h](const Op& o) { launch(h, o, h->state); };
-        if (h->dtype == QSV_C128) run_tiled<double>(passes, S128(h), h->n, h->stream, h->ws, stream_op);
-        else run_tiled<float>(passes, S64(h), h->n, h->stream, h->ws, stream_op);
+        const bool rt = h->executor == 1;
+        if (h->dtype == QSV_C128) run_tiled<double>(passes, S128(h), h->n, h->stream, h->ws, stream_op, rt);
+        else run_tiled<float>(passes, S64(h), h->n, h->stream, h->ws, stream_op, rt);
         for (const TilePass& p : passes) {
             if (p.tile_qubits.empty()) continue;   // counted by launch()
             h->stats.launches++;
@@ -191,6 +192,52 @@ void to_device_c128(Handle* h, void* dst, const double* amps) {
                                    cudaMemcpyHostToDevice, h->stream), "H2D");
         check_cuda(cudaStreamSynchronize(h->stream), "H2D");
     }
+}
+
+// Device -> host copy of `bytes` into caller memory.  Page-locked destinations take one
+// cudaMemcpyAsync; pageable ones go through two 32 MiB pinned staging buffers, the host copy of
+// chunk i overlapping the DMA of chunk i + 1 (a pageable cudaMemcpy stages through the driver's
+// small bounce buffer one piece at a time).
+void d2h(Handle* h, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return;
+    cudaPointerAttributes attr{};
+    const bool pinned = cudaPointerGetAttributes(&attr, dst) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+    (void)cudaGetLastError();
+    constexpr size_t kStage = size_t{32} << 20;
+    if (pinned || bytes <= kStage / 8) {
+        check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H");
+        check_cuda(cudaStreamSynchronize(h->stream), "D2H");
+        return;
+    }
+    uint8_t* stage = reinterpret_cast<uint8_t*>(h->ws.host_result(2 * kStage / sizeof(double)));
+    cudaEvent_t ev[2];
+    check_cuda(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), "event");
+    check_cuda(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), "event");
+    const uint8_t* s8 = static_cast<const uint8_t*>(src);
+    uint8_t* d8 = static_cast<uint8_t*>(dst);
+    const size_t n_chunks = (bytes + kStage - 1) / kStage;
+    auto drain = [&](size_t c) {
+        const size_t len = std::min(kStage, bytes - c * kStage);
+        check_cuda(cudaEventSynchronize(ev[c & 1]), "D2H");
+        std::memcpy(d8 + c * kStage, stage + (c & 1) * kStage, len);
+    };
+    try {
+        for (size_t c = 0; c < n_chunks; ++c) {
+            const size_t len = std::min(kStage, bytes - c * kStage);
+            check_cuda(cudaMemcpyAsync(stage + (c & 1) * kStage, s8 + c * kStage, len, cudaMemcpyDeviceToHost,
+                                       h->stream), "D2H");
+            check_cuda(cudaEventRecord(ev[c & 1], h->stream), "event");
+            if (c > 0) drain(c - 1);
+        }
+        drain(n_chunks - 1);
+    } catch (...) {
+        cudaStreamSynchronize(h->stream);
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        throw;
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
 }
 
 }  // namespace
@@ -281,7 +328,7 @@ int qsv_set_fusion(void* hp, int max_q, int min_q) {
 int qsv_set_executor(void* hp, int mode) {
     return guarded([&] {
         Handle* h = H_(hp);
-        if (mode < -1 || mode > 1) throw std::invalid_argument("executor mode must be -1, 0 or 1");
+        if (mode < -1 || mode > 2) throw std::invalid_argument("executor mode must be -1, 0, 1 or 2");
         h->executor = mode;
     });
 }
@@ -335,8 +382,7 @@ int qsv_get_state(void* hp, double* amps, uint64_t len) {
         if (!amps) throw std::invalid_argument("null output buffer");
         if (len != h->dim()) throw std::invalid_argument("output length != 2^n_qubits");
         if (h->dtype == QSV_C128) {
-            check_cuda(cudaMemcpyAsync(amps, h->state, h->dim() * 16, cudaMemcpyDeviceToHost, h->stream), "D2H");
-            check_cuda(cudaStreamSynchronize(h->stream), "D2H");
+            d2h(h, amps, h->state, h->dim() * 16);
             return;
         }
         const size_t chunk = 1u << 20;
@@ -525,9 +571,8 @@ int qsv_exact_probs(void* hp, double threshold, uint64_t* keys, double* probs, u
         total = h->dtype == QSV_C128
                     ? exact_readout<double>(S128(h), h->n, threshold, d_keys, d_probs, total, h->stream, h->ws)
                     : exact_readout<float>(S64(h), h->n, threshold, d_keys, d_probs, total, h->stream, h->ws);
-        check_cuda(cudaMemcpyAsync(keys, d_keys, total * 8, cudaMemcpyDeviceToHost, h->stream), "keys D2H");
-        check_cuda(cudaMemcpyAsync(probs, d_probs, total * 8, cudaMemcpyDeviceToHost, h->stream), "probs D2H");
-        check_cuda(cudaStreamSynchronize(h->stream), "exact readout");
+        d2h(h, keys, d_keys, total * 8);
+        d2h(h, probs, d_probs, total * 8);
         h->stats.launches += 3;
     });
 }

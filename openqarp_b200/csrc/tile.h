@@ -37,6 +37,48 @@ uint64_t op_support_mask(const Op& op);
 
 std::vector<TilePass> plan_tiles(const std::vector<Op>& ops, int n, int m, int c = kTileLowQubits);
 
+// ---------------------------------------------------------------- register-resident tiles
+// The register-tile kernel (kern_tile_rt.cu) holds a 2^12-amplitude tile in the registers of
+// 256 threads, 16 amplitudes each.  A layout assigns the tile's 12 local bits to the 4
+// register-slot bits, 5 lane bits and 3 warp bits of the amplitude's holder.  Ops whose mixing
+// qubits are all register slots run without data movement; a transpose through shared memory
+// changes the layout between them; a SWAP only relabels the layout.
+#ifndef QSV_RT_REG_BITS
+#define QSV_RT_REG_BITS 4
+#endif
+constexpr int kRtQubits = 12;
+constexpr int kRtRegBits = QSV_RT_REG_BITS;                  // amplitudes per thread = 2^kRtRegBits
+constexpr int kRtLaneBits = 5;
+constexpr int kRtWarpBits = kRtQubits - kRtRegBits - kRtLaneBits;
+constexpr int kRtMaxDense = 3;        // widest dense block applied in registers
+
+struct RtLayout {
+    uint8_t reg[kRtRegBits];    // local bit held by register-slot bit p
+    uint8_t lane[kRtLaneBits];  // local bit of lane-id bit k
+    uint8_t warp[kRtWarpBits];  // local bit of warp-id bit k
+};
+static_assert(sizeof(RtLayout) == kRtQubits, "a layout names every local bit once");
+
+enum RtKind : uint8_t { RT_XPOSE = 1, RT_RELABEL, RT_DENSE, RT_DIAG, RT_PHASE, RT_CTRL1, RT_PAULI, RT_SCALE };
+
+struct RtStep {
+    RtKind kind = RT_SCALE;
+    RtLayout layout{};          // the layout after the step
+    uint8_t slots = 0;          // DENSE: slot mask of the op bits; CTRL1: target slot bit; PAULI: x slots
+    std::vector<int> slot_of;   // DENSE: slot of op-local bit b (the matrix is re-indexed to slot order)
+    const Op* op = nullptr;     // the op itself (coefficients, masks); null for transposes
+};
+
+struct RtPlan {
+    RtLayout load{};            // the layout the tile is read into from the staging buffer
+    std::vector<RtStep> steps;  // ends in a layout whose lanes are local bits 0..4 (store)
+    int transposes = 0;
+};
+
+// Plan one tile pass for the register-tile kernel; false when the pass has an op the kernel
+// cannot apply in registers (then the shared-memory tile kernel runs it).
+bool plan_rt(const TilePass& pass, RtPlan* out);
+
 // Tiles per register width and storage: 2^12 complex128 or 2^13 complex64 (64 KiB).
 inline int default_tile_qubits(int n, int amp_bytes) {
     const int m = amp_bytes == 16 ? 12 : 13;

@@ -95,7 +95,8 @@ class Register:
 
     def configure(self, fusion_max: int, fusion_min: int, executor: int = -1, tile_qubits: int = 0):
         """Fusion knobs (fusion_max_qubits / fusion_min_qubits), executor (0 = one HBM pass per
-        fused block, 1 = tiled passes in shared memory, -1 = tiled from 16 qubits) and tile width."""
+        fused block, 1 = tiled passes with 2^12-amplitude tiles in registers, 2 = tiled passes in
+        shared memory, -1 = the default, stream) and tile width (0 = default)."""
         check(lib.qsv_set_fusion(self.handle, int(fusion_max), int(fusion_min)))
         check(lib.qsv_set_executor(self.handle, int(executor)))
         check(lib.qsv_set_tile_qubits(self.handle, int(tile_qubits)))

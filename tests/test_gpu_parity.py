@@ -170,45 +170,53 @@ def mixed_circuits(n):
     }
 
 
-@pytest.mark.parametrize("m", [10, 11, 12])
-def test_tiled_executor_matches_oracle(m, restatement):
+@pytest.mark.parametrize("m,executor", [(10, 2), (11, 2), (12, 2), (12, 1)])
+def test_tiled_executor_matches_oracle(m, executor, restatement):
+    """executor 1: passes on 12-qubit tiles run in registers (k <= 3 blocks), the rest in
+    shared memory; executor 2: every pass in shared memory."""
     n = 14
     for name, cmds in mixed_circuits(n).items():
         buf = ir.pack(cmds).buf
         want = restatement.statevector(buf, n)
         for k in (1, 2, 3, 4):
             reg = Register(n)
-            reg.configure(k, 0, 1, m)
+            reg.configure(k, 0, executor, m)
             reg.apply(buf)
             got = reg.get_state()
             reg.close()
             np.testing.assert_allclose(got, want, atol=AMP_TOL, rtol=0, err_msg=f"{name} k={k} m={m}")
 
 
-def test_tiled_executor_complex64(restatement):
+@pytest.mark.parametrize("m,executor", [(13, 2), (12, 1)])
+def test_tiled_executor_complex64(m, executor, restatement):
     n = 16
     for name, cmds in mixed_circuits(n).items():
         buf = ir.pack(cmds).buf
         want = restatement.statevector(buf, n)
-        reg = Register(n, "complex64")
-        reg.configure(3, 0, 1, 13)
-        reg.apply(buf)
-        got = reg.get_state()
-        reg.close()
-        assert np.max(np.abs(got - want)) < 2e-5, name
+        for k in (1, 3):
+            reg = Register(n, "complex64")
+            reg.configure(k, 0, executor, m)
+            reg.apply(buf)
+            got = reg.get_state()
+            reg.close()
+            assert np.max(np.abs(got - want)) < 2e-5, f"{name} k={k}"
 
 
-def test_tiled_and_stream_agree_at_24q():
+@pytest.mark.parametrize("dtype,tol", [("complex128", AMP_TOL), ("complex64", 2e-5)])
+def test_tiled_and_stream_agree_at_24q(dtype, tol):
+    """4096 tiles: every CTA of the persistent tile kernels walks many tiles (prefetch path)."""
     n = 24
-    buf = ir.pack(circuits.brickwork(n, 10, seed=8)).buf
+    cmds = circuits.brickwork(n, 10, seed=8) + mixed_circuits(n)["allgates"]
+    buf = ir.pack(cmds).buf
     out = []
-    for executor in (0, 1):
-        reg = Register(n)
-        reg.configure(3, 12, executor)
+    for executor, k, m in ((0, 3, 0), (1, 1, 12), (1, 3, 12), (2, 3, 12)):
+        reg = Register(n, dtype)
+        reg.configure(k, 12, executor, m)
         reg.apply(buf)
         out.append(reg.get_state())
         reg.close()
-    assert np.max(np.abs(out[0] - out[1])) < AMP_TOL
+    for o in out[1:]:
+        assert np.max(np.abs(out[0] - o)) < tol
 
 
 # ---------------------------------------------------------------- <H>
