@@ -153,6 +153,14 @@ QSV_API int qsv_set_executor(void* h, int mode);
  * (0 = the default: 12 for complex128, 13 for complex64).  No reference counterpart: the
  * reference applies one fused block per pass (qarp_simulator.cpp:934-935). */
 QSV_API int qsv_set_tile_qubits(void* h, int m);
+/* Adjoint sweeps (qsv_adjoint, qsv_adjoint_phi): keep a copy of |psi> every k commands of the
+ * forward sweep and restart the reverse sweep's |psi> from it, so uncomputing through inverse
+ * gates drifts over at most k gates.  -1 = default (none in complex128; in complex64 at most
+ * 16 copies, at least 16 commands apart), 0 = none.  The copies are device allocations of one
+ * register each, skipped when they would take more than half of the free memory.  The
+ * reference uncomputes through inverse gates only (run_gradient_core,
+ * qarp_simulator.cpp:1562-1601); in complex128 that is exact enough. */
+QSV_API int qsv_set_checkpoint_interval(void* h, int k);
 
 /* Register <- |0...0>. */
 QSV_API int qsv_reset(void* h);

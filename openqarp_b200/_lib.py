@@ -44,6 +44,7 @@ def _load():
         "qsv_set_fusion": (c_int, [c_void_p, c_int, c_int]),
         "qsv_set_executor": (c_int, [c_void_p, c_int]),
         "qsv_set_tile_qubits": (c_int, [c_void_p, c_int]),
+        "qsv_set_checkpoint_interval": (c_int, [c_void_p, c_int]),
         "qsv_reset": (c_int, [c_void_p]),
         "qsv_set_state": (c_int, [c_void_p, PD, c_uint64, c_int]),
         "qsv_get_state": (c_int, [c_void_p, PD, c_uint64]),
@@ -84,7 +85,7 @@ lib = _load()
 
 DECLARED = (
     "qsv_last_error", "qsv_abi_version", "qsv_create", "qsv_destroy", "qsv_set_fusion",
-    "qsv_set_executor", "qsv_set_tile_qubits", "qsv_reset", "qsv_set_state", "qsv_get_state", "qsv_device_state",
+    "qsv_set_executor", "qsv_set_tile_qubits", "qsv_set_checkpoint_interval", "qsv_reset", "qsv_set_state", "qsv_get_state", "qsv_device_state",
     "qsv_copy_state", "qsv_fuse_count", "qsv_tile_plan_count", "qsv_apply", "qsv_apply_unfused", "qsv_transition", "qsv_sample",
     "qsv_sample_seeded", "qsv_uniforms", "qsv_sample_parities", "qsv_exact_probs", "qsv_adjoint", "qsv_adjoint_phi", "qsv_norm2",
     "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_transition_static",

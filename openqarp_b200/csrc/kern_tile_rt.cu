@@ -102,6 +102,29 @@ __device__ __forceinline__ vec2_t<T> cfmav(vec2_t<T> a, vec2_t<T> b, vec2_t<T> a
     return acc;
 }
 
+// -a when neg, else a, by the sign bits alone (integer ops, no FP64 pipe, no branch)
+template <typename T>
+__device__ __forceinline__ vec2_t<T> flip_sign(vec2_t<T> a, bool neg) {
+    if constexpr (sizeof(T) == 8) {
+        const int m = neg ? static_cast<int>(0x80000000u) : 0;
+        a.x = __hiloint2double(__double2hiint(a.x) ^ m, __double2loint(a.x));
+        a.y = __hiloint2double(__double2hiint(a.y) ^ m, __double2loint(a.y));
+    } else {
+        const unsigned m = neg ? 0x80000000u : 0u;
+        a.x = __uint_as_float(__float_as_uint(a.x) ^ m);
+        a.y = __uint_as_float(__float_as_uint(a.y) ^ m);
+    }
+    return a;
+}
+
+// registers r whose slot bits include all of rm: bit r of the result
+__device__ __forceinline__ uint32_t pattern_of(uint32_t rm) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int r = 0; r < kRtAmps; ++r) m |= ((static_cast<uint32_t>(r) & rm) == rm ? 1u : 0u) << r;
+    return m;
+}
+
 // Per-thread view of the current layout.
 struct Lay {
     uint32_t lfix;            // local index bits fixed by lane and warp id
@@ -259,6 +282,35 @@ __device__ __forceinline__ void rt_pauli(vec2_t<T> (&v)[kRtAmps], const Lay& L, 
     }
 }
 
+// one-qubit gates on every slot of MASK, ascending, four coefficients each: straight-line code
+// with a single join for the whole layer
+template <typename T, int MASK>
+__device__ __forceinline__ void rt_layer(vec2_t<T> (&v)[kRtAmps], const cplx<T>* __restrict__ c) {
+    int idx = 0;
+#pragma unroll
+    for (int p = 0; p < kRtRegBits; ++p)
+        if ((MASK >> p) & 1) {
+            switch (p) {
+                case 0: rt_dense<T, 1>(v, c + 4 * idx); break;
+                case 1: rt_dense<T, 2>(v, c + 4 * idx); break;
+                case 2: rt_dense<T, 4>(v, c + 4 * idx); break;
+                default: if constexpr (kRtRegBits > 3) rt_dense<T, 8>(v, c + 4 * idx); break;
+            }
+            ++idx;
+        }
+}
+
+template <typename T, int M = 1>
+__device__ __forceinline__ void rt_layer_dispatch(vec2_t<T> (&v)[kRtAmps], int slots, const cplx<T>* __restrict__ c) {
+    if constexpr (M < (1 << kRtRegBits)) {
+        if (slots == M) {
+            rt_layer<T, M>(v, c);
+            return;
+        }
+        rt_layer_dispatch<T, M + 1>(v, slots, c);
+    }
+}
+
 // slot-mask dispatch: one uniform compare per candidate mask, the matching body inlined
 template <typename T, int M = 1>
 __device__ __forceinline__ void rt_dense_dispatch(vec2_t<T> (&v)[kRtAmps], int slots, const cplx<T>* __restrict__ c) {
@@ -309,7 +361,7 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 // staging buffer straight into the pass's first layout.  Shared memory: the transpose buffer
 // and the staging buffer (2^12 16-byte slots each, both indexed through swz()), then the pass's
 // steps and coefficients when they fit.
-template <typename T>
+template <typename T, bool SMEM>
 __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict__ s, int n,
                                                           const RtPassDev* __restrict__ passes, int pass_idx,
                                                           const RtStepDev* __restrict__ steps,
@@ -327,7 +379,7 @@ __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict
     // every tile reads the pass's steps and coefficients: keep them on chip when they fit
     const RtStepDev* stp = steps + P->step_begin;
     const cplx<T>* cf = coef + P->coef_begin;
-    if (P->in_smem) {
+    if constexpr (SMEM) {
         RtStepDev* ss = reinterpret_cast<RtStepDev*>(stage + (1 << kRtQubits));
         cplx<T>* sc = reinterpret_cast<cplx<T>*>(ss + ((n_steps + 1) & ~1u));
         for (uint32_t i = threadIdx.x; i < n_steps; i += blockDim.x) ss[i] = stp[i];
@@ -398,7 +450,31 @@ __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict
             const RtStepDev& st = stp[si];
             const uint8_t kind = st.kind;
             const cplx<T>* coef_st = cf + st.coef;
-            if (kind == RT_XPOSE) {
+            if (kind == RT_SIGNS) {
+                // st.k conditions follow; each flips the sign of the registers it selects
+                uint32_t neg = 0;
+                for (uint32_t i = 1; i <= st.k; ++i) {
+                    const RtStepDev& it = stp[si + i];
+                    if ((base & it.gmask) != it.gmask) continue;
+                    bool tok;
+                    const uint32_t rm = L.slot_pattern(static_cast<uint32_t>(it.lmask), &tok);
+                    if (tok) neg ^= pattern_of(rm);
+                }
+                si += st.k;
+#pragma unroll
+                for (int r = 0; r < kRtAmps; ++r) v[r] = flip_sign<T>(v[r], (neg >> r) & 1u);
+            } else if (kind == RT_SIGN_ITEM) {
+                // consumed by its RT_SIGNS head
+            } else if (kind == RT_GL) {
+                rt_layer_dispatch<T>(v, st.slots, coef_st);
+            } else if (kind == RT_G1) {
+                switch (st.slots) {
+                    case 1: rt_dense<T, 1>(v, coef_st); break;
+                    case 2: rt_dense<T, 2>(v, coef_st); break;
+                    case 4: rt_dense<T, 4>(v, coef_st); break;
+                    default: if constexpr (kRtRegBits > 3) rt_dense<T, 8>(v, coef_st); break;
+                }
+            } else if (kind == RT_XPOSE) {
                 __syncthreads();   // the previous transpose's reads are done
 #pragma unroll
                 for (int r = 0; r < kRtAmps; ++r) *reinterpret_cast<vec2_t<T>*>(xb + L.sw(r)) = v[r];
@@ -417,13 +493,14 @@ __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict
                 if (!tok) continue;
                 const vec2_t<T> ph = ldcoef<T>(coef_st);
                 if (ph.x == T(-1) && ph.y == T(0)) {
+                    // a sign flip: XOR of the sign bits, every register written unconditionally
 #pragma unroll
-                    for (int r = 0; r < kRtAmps; ++r)
-                        if ((static_cast<uint32_t>(r) & rm) == rm) v[r] = mk<T>(-v[r].x, -v[r].y);
+                    for (int r = 0; r < kRtAmps; ++r) v[r] = flip_sign<T>(v[r], (static_cast<uint32_t>(r) & rm) == rm);
                 } else {
+                    const vec2_t<T> one = mk<T>(T(1), T(0));
 #pragma unroll
                     for (int r = 0; r < kRtAmps; ++r)
-                        if ((static_cast<uint32_t>(r) & rm) == rm) v[r] = cmulv<T>(ph, v[r]);
+                        v[r] = cmulv<T>((static_cast<uint32_t>(r) & rm) == rm ? ph : one, v[r]);
                 }
             } else if (kind == RT_DIAG) {
                 const int k = st.k;
@@ -508,6 +585,8 @@ RtUpload encode_rt(const std::vector<const TilePass*>& passes, cudaStream_t st, 
         for (int j = 0; j < kRtQubits; ++j) pd.tq[j] = static_cast<uint8_t>(p.tile_qubits[j]);
         put_layout(pd.load, plan.load);
         auto push = [&](c128 v) { cdev.push_back(cplx<T>{static_cast<T>(v.real()), static_cast<T>(v.imag())}); };
+        size_t signs_head = 0;
+        bool signs_open = false;
         for (const RtStep& stp : plan.steps) {
             RtStepDev d{};
             d.kind = stp.kind;
@@ -526,6 +605,7 @@ RtUpload encode_rt(const std::vector<const TilePass*>& passes, cudaStream_t st, 
                             m[to_slot_order(y, stp.slot_of) * D + to_slot_order(x, stp.slot_of)] = o->m[y * D + x];
                     for (const c128& v : m) push(v);
                     d.k = static_cast<uint8_t>(o->k);
+                    if (o->k == 1) d.kind = RT_G1;
                     break;
                 }
                 case RT_DIAG:
@@ -556,6 +636,52 @@ RtUpload encode_rt(const std::vector<const TilePass*>& passes, cudaStream_t st, 
                 default:   // RT_SCALE
                     push(o->m[0]);
                     break;
+            }
+            // a sign-flip phase joins a directly preceding run of them (diagonal ops commute)
+            if (d.kind == RT_PHASE && o->m[0] == c128(-1.0, 0.0)) {
+                cdev.pop_back();   // the phase itself is implied
+                d.kind = RT_SIGN_ITEM;
+                d.coef = 0;
+                if (sdev.size() > pd.step_begin && sdev[signs_head].kind == RT_SIGNS && signs_open &&
+                    sdev[signs_head].k < 255) {
+                    sdev[signs_head].k++;
+                    sdev.push_back(d);
+                    continue;
+                }
+                RtStepDev head{};
+                head.kind = RT_SIGNS;
+                head.k = 1;
+                std::memset(head.lpos, 0xff, sizeof head.lpos);
+                put_layout(head.layout, stp.layout);
+                signs_head = sdev.size();
+                sdev.push_back(head);
+                sdev.push_back(d);
+                signs_open = true;
+                continue;
+            }
+            signs_open = false;
+            // a one-qubit gate on a slot the previous one-qubit step leaves alone joins it: gates
+            // on distinct qubits commute, and the layer's coefficients are kept in slot order
+            if (d.kind == RT_G1 && sdev.size() > pd.step_begin &&
+                (sdev.back().kind == RT_G1 || sdev.back().kind == RT_GL) && !(sdev.back().slots & d.slots)) {
+                RtStepDev& prev = sdev.back();
+                const size_t first = pd.coef_begin + prev.coef;
+                std::vector<std::pair<int, std::vector<cplx<T>>>> by_slot;
+                int idx = 0;
+                for (int p = 0; p < kRtRegBits; ++p)
+                    if ((prev.slots >> p) & 1) {
+                        by_slot.push_back({p, std::vector<cplx<T>>(cdev.begin() + first + 4 * idx,
+                                                                   cdev.begin() + first + 4 * idx + 4)});
+                        ++idx;
+                    }
+                by_slot.push_back({__builtin_ctz(d.slots), std::vector<cplx<T>>(cdev.end() - 4, cdev.end())});
+                std::sort(by_slot.begin(), by_slot.end(),
+                          [](const auto& a, const auto& b) { return a.first < b.first; });
+                cdev.resize(first);
+                for (const auto& e : by_slot) cdev.insert(cdev.end(), e.second.begin(), e.second.end());
+                prev.kind = RT_GL;
+                prev.slots = static_cast<uint8_t>(prev.slots | d.slots);
+                continue;
             }
             sdev.push_back(d);
         }
@@ -595,14 +721,20 @@ void launch_rt(const RtUpload& u, int idx, vec2_t<T>* s, int n, cudaStream_t st)
     int sms = 0, device = 0;
     check_cuda(cudaGetDevice(&device), "device");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
-    check_cuda(cudaFuncSetAttribute(k_tile_rt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(kRtTileSmem + kRtExtraSmemMax)), "register-tile smem");
-    const size_t smem = kRtTileSmem + u.extra_smem.at(idx);
+    const size_t extra = u.extra_smem.at(idx);
+    const size_t smem = kRtTileSmem + extra;
     const uint64_t n_tiles = 1ull << (n - kRtQubits);
     const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sms));
-    k_tile_rt<T><<<static_cast<unsigned>(grid), kRtThreads, smem, st>>>(
-        s, n, static_cast<const RtPassDev*>(u.passes), idx, static_cast<const RtStepDev*>(u.steps),
-        static_cast<const cplx<T>*>(u.coef));
+    auto go = [&](auto kernel) {
+        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kRtTileSmem + kRtExtraSmemMax)), "register-tile smem");
+        kernel<<<static_cast<unsigned>(grid), kRtThreads, smem, st>>>(
+            s, n, static_cast<const RtPassDev*>(u.passes), idx, static_cast<const RtStepDev*>(u.steps),
+            static_cast<const cplx<T>*>(u.coef));
+    };
+    // extra > 0: the pass's steps and coefficients are copied into shared memory
+    if (extra > 0) go(k_tile_rt<T, true>);
+    else go(k_tile_rt<T, false>);
     check_cuda(cudaGetLastError(), "register-tile launch");
 }
 

@@ -36,6 +36,7 @@ struct Handle {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     void* aux = nullptr;          // second register (adjoint's |phi>)
     size_t aux_cap = 0;
+    int checkpoint_interval = -1; // adjoint: commands between psi checkpoints (-1 auto, 0 none)
     uint64_t dim() const { return 1ull << n; }
     size_t amp_bytes() const { return dtype == QSV_C128 ? 16 : 8; }
 };
@@ -138,8 +139,13 @@ bool use_tiled(const Handle* h) {
     return h->executor == 1 || h->executor == 2;
 }
 
+void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse);
+
 void apply_stream(Handle* h, const uint8_t* buf, size_t nbytes, bool fuse) {
-    std::vector<Cmd> cmds = decode(buf, nbytes);
+    apply_cmds(h, decode(buf, nbytes), fuse);
+}
+
+void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
     check_stream(cmds);
     if (fuse) cmds = fuse_for_dispatch(cmds, h->n, h->fusion_max, h->fusion_min);
     std::vector<Op> ops;
@@ -330,6 +336,14 @@ int qsv_set_executor(void* hp, int mode) {
         Handle* h = H_(hp);
         if (mode < -1 || mode > 2) throw std::invalid_argument("executor mode must be -1, 0, 1 or 2");
         h->executor = mode;
+    });
+}
+
+int qsv_set_checkpoint_interval(void* hp, int k) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (k < -1) throw std::invalid_argument("checkpoint interval must be -1 (default), 0 (none) or > 0");
+        h->checkpoint_interval = k;
     });
 }
 
@@ -663,9 +677,61 @@ struct DepTable {
     int n_params;
 };
 
+// |psi> checkpoints of the adjoint sweep: bufs[s - 1] holds the state before command s * K.
+// The reverse sweep uncomputes psi through the inverse gates of one segment at most and then
+// restarts from the stored state, so the rounding drift of uncomputation (which complex64
+// accumulates over a long circuit) stays bounded by K gates.
+struct Checkpoints {
+    size_t K = 0;                 // 0: no checkpoints
+    std::vector<void*> bufs;
+    Checkpoints() = default;
+    Checkpoints(const Checkpoints&) = delete;
+    Checkpoints& operator=(const Checkpoints&) = delete;
+    ~Checkpoints() {
+        for (void* b : bufs) cudaFree(b);
+    }
+};
+
+size_t checkpoint_interval(const Handle* h, size_t n_cmds) {
+    if (h->checkpoint_interval >= 0) return static_cast<size_t>(h->checkpoint_interval);
+    // default: none in complex128; in complex64 at most 16 checkpoints, at least 16 commands apart
+    if (h->dtype != QSV_C64) return 0;
+    return std::max<size_t>(16, (n_cmds + 15) / 16);
+}
+
+// The adjoint's forward sweep: fused, segment by segment when checkpoints are kept (a segment's
+// commands fuse among themselves only).  Falls back to no checkpoints when they would take
+// more than half of the free device memory.
+void adjoint_forward(Handle* h, const std::vector<Cmd>& cs, Checkpoints& ck) {
+    const size_t K = checkpoint_interval(h, cs.size());
+    const size_t bytes = h->dim() * h->amp_bytes();
+    const size_t S = K ? (cs.size() + K - 1) / K : 1;
+    size_t free_b = 0, total_b = 0;
+    if (S > 1) check_cuda(cudaMemGetInfo(&free_b, &total_b), "memory info");
+    if (S <= 1 || (S - 1) * bytes > free_b / 2) {
+        ck.K = 0;
+        apply_cmds(h, cs, true);
+        return;
+    }
+    ck.K = K;
+    for (size_t s = 0; s < S; ++s) {
+        if (s > 0) {
+            void* b = nullptr;
+            if (cudaMalloc(&b, bytes) != cudaSuccess) {
+                (void)cudaGetLastError();
+                throw std::bad_alloc();
+            }
+            ck.bufs.push_back(b);
+            check_cuda(cudaMemcpyAsync(b, h->state, bytes, cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
+        }
+        const size_t lo = s * K, hi = std::min(cs.size(), lo + K);
+        apply_cmds(h, std::vector<Cmd>(cs.begin() + lo, cs.begin() + hi), true);
+    }
+}
+
 template <typename T>
 void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps, vec2_t<T>* psi,
-                   vec2_t<T>* phi, double* grad) {
+                   vec2_t<T>* phi, double* grad, const Checkpoints& ck) {
     const int n = h->n;
     // count parametric steps, build them
     struct Slot { size_t cmd; c128 pref; };
@@ -709,6 +775,10 @@ void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps
                 launch(h, o, phi);
             }
         }
+        // psi is now the state before command idx: restart it from the checkpoint there
+        if (ck.K && idx > 0 && idx % ck.K == 0)
+            check_cuda(cudaMemcpyAsync(psi, ck.bufs.at(idx / ck.K - 1), h->dim() * h->amp_bytes(),
+                                       cudaMemcpyDeviceToDevice, h->stream), "checkpoint restore");
     }
     std::vector<double> ips;
     reduce_slots(partials, static_cast<int>(slots.size()), nb, h->stream, h->ws, ips);
@@ -756,7 +826,8 @@ int qsv_adjoint(void* hp, const uint8_t* cmds, size_t nbytes, const int32_t* dep
         const std::vector<Cmd> cs = checked_adjoint_stream(cmds, nbytes, dep_ptr, dep_param, n_params, h->n);
         const PauliTerms t = terms_of(h, xm, zm, coeff, nt);
         // forward sweep (fused: the reverse sweep below walks the unfused stream)
-        apply_stream(h, cmds, nbytes, true);
+        Checkpoints ck;
+        adjoint_forward(h, cs, ck);
         void* phi = aux_state(h);
         DepTable deps{dep_ptr, dep_param, dep_alpha, n_params};
         if (h->dtype == QSV_C128) {
@@ -766,7 +837,7 @@ int qsv_adjoint(void* hp, const uint8_t* cmds, size_t nbytes, const int32_t* dep
                 inner<double, double>(S128(h), static_cast<double2*>(phi), h->n, h->stream, h->ws, e);
                 *energy = e[0];
             }
-            adjoint_sweep<double>(h, cs, deps, S128(h), static_cast<double2*>(phi), grad);
+            adjoint_sweep<double>(h, cs, deps, S128(h), static_cast<double2*>(phi), grad, ck);
         } else {
             apply_observable<float>(S64(h), static_cast<float2*>(phi), h->n, t, h->stream, h->ws);
             if (energy) {
@@ -774,7 +845,7 @@ int qsv_adjoint(void* hp, const uint8_t* cmds, size_t nbytes, const int32_t* dep
                 inner<float, float>(S64(h), static_cast<float2*>(phi), h->n, h->stream, h->ws, e);
                 *energy = e[0];
             }
-            adjoint_sweep<float>(h, cs, deps, S64(h), static_cast<float2*>(phi), grad);
+            adjoint_sweep<float>(h, cs, deps, S64(h), static_cast<float2*>(phi), grad, ck);
         }
     });
 }
@@ -787,12 +858,13 @@ int qsv_adjoint_phi(void* hp, const uint8_t* cmds, size_t nbytes, const int32_t*
         if (!phi_host) throw std::invalid_argument("null phi");
         if (n_params < 0 || (n_params > 0 && !grad)) throw std::invalid_argument("bad gradient output");
         const std::vector<Cmd> cs = checked_adjoint_stream(cmds, nbytes, dep_ptr, dep_param, n_params, h->n);
-        apply_stream(h, cmds, nbytes, true);
+        Checkpoints ck;
+        adjoint_forward(h, cs, ck);
         void* phi = aux_state(h);
         to_device_c128(h, phi, phi_host);
         DepTable deps{dep_ptr, dep_param, dep_alpha, n_params};
-        if (h->dtype == QSV_C128) adjoint_sweep<double>(h, cs, deps, S128(h), static_cast<double2*>(phi), grad);
-        else adjoint_sweep<float>(h, cs, deps, S64(h), static_cast<float2*>(phi), grad);
+        if (h->dtype == QSV_C128) adjoint_sweep<double>(h, cs, deps, S128(h), static_cast<double2*>(phi), grad, ck);
+        else adjoint_sweep<float>(h, cs, deps, S64(h), static_cast<float2*>(phi), grad, ck);
     });
 }
 

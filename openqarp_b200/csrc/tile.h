@@ -59,7 +59,12 @@ struct RtLayout {
 };
 static_assert(sizeof(RtLayout) == kRtQubits, "a layout names every local bit once");
 
-enum RtKind : uint8_t { RT_XPOSE = 1, RT_RELABEL, RT_DENSE, RT_DIAG, RT_PHASE, RT_CTRL1, RT_PAULI, RT_SCALE };
+// The encoder's compact forms: RT_G1 / RT_GL, one-qubit RT_DENSE steps (one gate, or a layer of
+// gates on distinct register slots applied in one step); RT_SIGNS, a run of sign-flip phases
+// (CZ-like, phase -1) whose conditions follow as RT_SIGN_ITEM records and whose flips are
+// applied in one pass over the registers.
+enum RtKind : uint8_t { RT_XPOSE = 1, RT_RELABEL, RT_DENSE, RT_DIAG, RT_PHASE, RT_CTRL1, RT_PAULI, RT_SCALE,
+                        RT_G1, RT_GL, RT_SIGNS, RT_SIGN_ITEM };
 
 struct RtStep {
     RtKind kind = RT_SCALE;

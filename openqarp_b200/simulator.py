@@ -93,6 +93,10 @@ class Register:
     def copy_from(self, other: "Register"):
         check(lib.qsv_copy_state(self.handle, other.handle))
 
+    def set_checkpoint_interval(self, k: int):
+        """Adjoint sweeps keep |psi> every k commands (-1 default: complex64 only, 0 none)."""
+        check(lib.qsv_set_checkpoint_interval(self.handle, int(k)))
+
     def configure(self, fusion_max: int, fusion_min: int, executor: int = -1, tile_qubits: int = 0):
         """Fusion knobs (fusion_max_qubits / fusion_min_qubits), executor (0 = one HBM pass per
         fused block, 1 = tiled passes with 2^12-amplitude tiles in registers, 2 = tiled passes in

@@ -486,6 +486,47 @@ def test_complex64_adjoint_error_bound(sim, sim64):
     assert np.max(np.abs(g64 - g128)) < 1e-4
 
 
+def test_complex64_adjoint_checkpoints_bound_the_drift(sim):
+    """A deep circuit (1900 commands): complex64 gradients restart |psi> from a checkpoint every
+    few dozen commands instead of uncomputing through the whole circuit; both agree with
+    complex128 within the complex64 bound, and the checkpoints are really used."""
+    from openqarp_b200 import Register, ir, observable
+    n = 10
+    cmds, vals, names = circuits.hea(n, 64, seed=4)
+    obs = observable.to_masks(circuits.tfim_chain(n), n)
+    stream = ir.pack(cmds, vals, names)
+    g128 = np.array(sim.run_gradient(cmds, n, circuits.tfim_chain(n), vals, names))
+    out = {}
+    for k in (-1, 0, 24):
+        reg = Register(n, "complex64")
+        reg.set_checkpoint_interval(k)
+        reg.reset()
+        _, g = reg.adjoint(stream, len(names), obs)
+        reg.close()
+        out[k] = np.asarray(g)
+    for k, g in out.items():
+        assert np.max(np.abs(g - g128)) < 1e-4, k
+    assert not np.array_equal(out[-1], out[0])
+
+
+def test_complex128_adjoint_with_checkpoints_matches(sim):
+    from openqarp_b200 import Register, ir, observable
+    n = 9
+    cmds, vals, names = circuits.hea(n, 6, seed=5)
+    obs = observable.to_masks(circuits.tfim_chain(n), n)
+    stream = ir.pack(cmds, vals, names)
+    res = []
+    for k in (0, 7):
+        reg = Register(n)
+        reg.set_checkpoint_interval(k)
+        reg.reset()
+        e, g = reg.adjoint(stream, len(names), obs)
+        reg.close()
+        res.append((e, np.asarray(g)))
+    assert abs(res[0][0] - res[1][0]) < 1e-12
+    assert np.max(np.abs(res[0][1] - res[1][1])) < 1e-10
+
+
 # ---------------------------------------------------------------- error paths
 
 def test_error_paths(sim):
