@@ -202,12 +202,39 @@ __device__ __forceinline__ void rt_dense(vec2_t<T> (&v)[kRtAmps], const cplx<T>*
     constexpr int D = 1 << K;
     if constexpr (K == 1) {
         const vec2_t<T> m0 = ldcoef<T>(c), m1 = ldcoef<T>(c + 1), m2 = ldcoef<T>(c + 2), m3 = ldcoef<T>(c + 3);
+        // four rounds over all pairs, so every round's FMAs are independent of each other:
+        // the FP64 pipe then never waits on one accumulator chain
+        constexpr int NP = kRtAmps / 2;
+        vec2_t<T> o0[NP], o1[NP];
 #pragma unroll
-        for (int g = 0; g < kRtAmps; ++g) {
+        for (int g = 0, j = 0; g < kRtAmps; ++g) {
             if (g & MASK) continue;
-            const vec2_t<T> a0 = v[g], a1 = v[g | MASK];
-            v[g] = cfmav<T>(m1, a1, cmulv<T>(m0, a0));
-            v[g | MASK] = cfmav<T>(m3, a1, cmulv<T>(m2, a0));
+            o0[j] = mk<T>(m0.x * v[g].x, m0.x * v[g].y);
+            o1[j] = mk<T>(m2.x * v[g].x, m2.x * v[g].y);
+            ++j;
+        }
+#pragma unroll
+        for (int g = 0, j = 0; g < kRtAmps; ++g) {
+            if (g & MASK) continue;
+            o0[j] = mk<T>(fma(-m0.y, v[g].y, o0[j].x), fma(m0.y, v[g].x, o0[j].y));
+            o1[j] = mk<T>(fma(-m2.y, v[g].y, o1[j].x), fma(m2.y, v[g].x, o1[j].y));
+            ++j;
+        }
+#pragma unroll
+        for (int g = 0, j = 0; g < kRtAmps; ++g) {
+            if (g & MASK) continue;
+            const vec2_t<T> a1 = v[g | MASK];
+            o0[j] = mk<T>(fma(m1.x, a1.x, o0[j].x), fma(m1.x, a1.y, o0[j].y));
+            o1[j] = mk<T>(fma(m3.x, a1.x, o1[j].x), fma(m3.x, a1.y, o1[j].y));
+            ++j;
+        }
+#pragma unroll
+        for (int g = 0, j = 0; g < kRtAmps; ++g) {
+            if (g & MASK) continue;
+            const vec2_t<T> a1 = v[g | MASK];
+            v[g] = mk<T>(fma(-m1.y, a1.y, o0[j].x), fma(m1.y, a1.x, o0[j].y));
+            v[g | MASK] = mk<T>(fma(-m3.y, a1.y, o1[j].x), fma(m3.y, a1.x, o1[j].y));
+            ++j;
         }
     } else {
 #pragma unroll

@@ -183,11 +183,6 @@ int slot_of_bit(const RtLayout& l, int b) {
     return -1;
 }
 
-uint32_t reg_mask(const RtLayout& l) {
-    uint32_t m = 0;
-    for (int p = 0; p < kRtRegBits; ++p) m |= 1u << l.reg[p];
-    return m;
-}
 
 }  // namespace
 
@@ -200,101 +195,182 @@ bool plan_rt(const TilePass& pass, RtPlan* out) {
     for (int j = 0; j < kRtQubits; ++j) local_of[pass.tile_qubits[j]] = j;
     const size_t n_ops = pass.ops.size();
     std::vector<uint32_t> mix(n_ops);
+    std::vector<uint64_t> sup(n_ops);
     for (size_t i = 0; i < n_ops; ++i) {
         mix[i] = local_set(op_mixing_mask(pass.ops[i]), local_of);
         if (!rt_capable(pass.ops[i], mix[i])) return false;
+        sup[i] = op_support_mask(pass.ops[i]) | op_mixing_mask(pass.ops[i]);
     }
-    // register bits wanted next: `first`, then the mixing bits of ops i, i+1, ... in order
-    auto wanted = [&](size_t i, uint32_t first, uint32_t exclude, std::vector<int>& bits, uint32_t& have) {
-        auto take = [&](uint32_t m) {
-            for (int b = 0; b < kRtQubits && static_cast<int>(bits.size()) < kRtRegBits; ++b)
-                if (((m >> b) & 1) && !((have >> b) & 1) && !((exclude >> b) & 1)) {
-                    bits.push_back(b);
-                    have |= 1u << b;
-                }
-        };
-        take(first);
-        for (size_t j = i; j < n_ops && static_cast<int>(bits.size()) < kRtRegBits; ++j)
-            if (pass.ops[j].kind != OP_SWAP) take(mix[j]);
+    // Ops sharing a qubit keep their order; ops on disjoint qubits commute.  Per qubit, the
+    // indices of the ops touching it in order; an op is ready when it heads every one of its
+    // qubits' lists.
+    std::vector<std::vector<uint32_t>> chain(64);
+    for (size_t i = 0; i < n_ops; ++i)
+        for (uint64_t m = sup[i]; m; m &= m - 1) chain[__builtin_ctzll(m)].push_back(static_cast<uint32_t>(i));
+    std::vector<uint32_t> head(64, 0);
+    std::vector<char> done(n_ops, 0);
+    auto is_ready = [&](size_t i, const std::vector<uint32_t>& hd) {
+        for (uint64_t m = sup[i]; m; m &= m - 1) {
+            const int q = __builtin_ctzll(m);
+            if (chain[q][hd[q]] != i) return false;
+        }
+        return true;
     };
-    auto pad = [&](std::vector<int>& bits, uint32_t& have, const RtLayout* keep) {
-        if (keep)
-            for (int p = 0; p < kRtRegBits && static_cast<int>(bits.size()) < kRtRegBits; ++p)
-                if (!((have >> keep->reg[p]) & 1)) {
-                    bits.push_back(keep->reg[p]);
-                    have |= 1u << keep->reg[p];
-                }
-        for (int b = kRtQubits - 1; b >= 0 && static_cast<int>(bits.size()) < kRtRegBits; --b)
-            if (!((have >> b) & 1)) {
-                bits.push_back(b);
-                have |= 1u << b;
+    auto advance = [&](size_t i, std::vector<uint32_t>& hd) {
+        for (uint64_t m = sup[i]; m; m &= m - 1) ++hd[__builtin_ctzll(m)];
+    };
+    auto swap_bits = [](uint32_t regs, int a, int b) {
+        const uint32_t ba = (regs >> a) & 1u, bb = (regs >> b) & 1u;
+        regs &= ~((1u << a) | (1u << b));
+        return regs | (ba << b) | (bb << a);
+    };
+    // ops a register set lets run before a transpose is needed (one scan in order: an op's
+    // predecessors come before it), weighted by their arithmetic
+    auto simulate = [&](uint32_t regs) {
+        std::vector<uint32_t> hd(head);
+        int gain = 0;
+        for (size_t i = 0; i < n_ops; ++i) {
+            if (done[i] || !is_ready(i, hd)) continue;
+            const Op& o = pass.ops[i];
+            if (o.kind == OP_SWAP) {
+                regs = swap_bits(regs, local_of[o.qubits[0]], local_of[o.qubits[1]]);
+            } else if (mix[i] & ~regs) {
+                continue;
+            } else if (mix[i]) {
+                gain += 4;
+            } else {
+                gain += 1;
             }
+            advance(i, hd);
+        }
+        return gain;
+    };
+    // candidate register sets: the bits of one waiting ready op, completed with the bits of
+    // other ops (whole ops only) taken in order from the ready ones or from all waiting ones,
+    // then with the current register bits
+    auto choose = [&](uint32_t current) {
+        std::vector<size_t> waiting, ready_waiting;
+        for (size_t i = 0; i < n_ops; ++i)
+            if (!done[i] && mix[i] && pass.ops[i].kind != OP_SWAP) {
+                waiting.push_back(i);
+                if (is_ready(i, head)) ready_waiting.push_back(i);
+            }
+        auto complete = [&](uint32_t regs, const std::vector<size_t>& from) {
+            for (size_t j : from) {
+                const uint32_t m = regs | mix[j];
+                if (__builtin_popcount(m) <= kRtRegBits) regs = m;
+            }
+            for (int b = 0; b < kRtQubits && __builtin_popcount(regs) < kRtRegBits; ++b)
+                if ((current >> b) & 1) regs |= 1u << b;
+            for (int b = kRtQubits - 1; b >= 0 && __builtin_popcount(regs) < kRtRegBits; --b) regs |= 1u << b;
+            return regs;
+        };
+        uint32_t best = 0;
+        int best_gain = -1;
+        for (size_t r : ready_waiting)
+            for (int variant = 0; variant < 2; ++variant) {
+                const uint32_t cand = complete(mix[r], variant ? waiting : ready_waiting);
+                const int g = simulate(cand);
+                // ties: keep more of the current register bits (cheaper to reason about)
+                if (g > best_gain || (g == best_gain && __builtin_popcount(cand & current) >
+                                                          __builtin_popcount(best & current))) {
+                    best_gain = g;
+                    best = cand;
+                }
+            }
+        if (best == 0) best = complete(0, waiting);
+        std::vector<int> bits;
+        // keep bits already in register slots in place where possible (order is free here)
+        for (int b = 0; b < kRtQubits; ++b)
+            if ((best >> b) & 1) bits.push_back(b);
+        return bits;
+    };
+    auto reg_set = [](const RtLayout& l) {
+        uint32_t m = 0;
+        for (int p = 0; p < kRtRegBits; ++p) m |= 1u << l.reg[p];
+        return m;
     };
     out->steps.clear();
     out->transposes = 0;
-    // the tile is read from the staging buffer straight into the first layout the ops want
-    std::vector<int> bits;
-    uint32_t have = 0;
-    wanted(0, 0, 0, bits, have);
-    pad(bits, have, nullptr);
-    RtLayout L = make_layout(bits, false);
+    // the tile is read from the staging buffer straight into the first layout chosen
+    RtLayout L = make_layout(choose(0), false);
     out->load = L;
+    size_t remaining = 0;
     for (size_t i = 0; i < n_ops; ++i) {
-        const Op& o = pass.ops[i];
-        if (o.kind == OP_NOP) continue;
-        if (o.kind == OP_SWAP) {
-            // exchange the roles of the two local bits: the data stays where it is
-            const int a = local_of[o.qubits[0]], b = local_of[o.qubits[1]];
-            uint8_t* where[kRtQubits] = {};
-            for (int p = 0; p < kRtRegBits; ++p) where[L.reg[p]] = &L.reg[p];
-            for (int k = 0; k < kRtLaneBits; ++k) where[L.lane[k]] = &L.lane[k];
-            for (int k = 0; k < kRtWarpBits; ++k) where[L.warp[k]] = &L.warp[k];
-            std::swap(*where[a], *where[b]);
-            RtStep st;
-            st.kind = RT_RELABEL;
-            st.layout = L;
-            st.op = &o;
-            out->steps.push_back(st);
-            continue;
+        if (pass.ops[i].kind == OP_NOP) {
+            done[i] = 1;
+            advance(i, head);
+        } else {
+            ++remaining;
         }
-        if (mix[i] & ~reg_mask(L)) {
-            std::vector<int> nb;
-            uint32_t got = 0;
-            wanted(i, mix[i], 0, nb, got);
-            pad(nb, got, &L);
-            L = make_layout(nb, false);
-            RtStep st;
-            st.kind = RT_XPOSE;
-            st.layout = L;
-            out->steps.push_back(st);
-            ++out->transposes;
-        }
-        RtStep st;
-        st.op = &o;
-        switch (o.kind) {
-            case OP_DENSE:
-                st.kind = RT_DENSE;
-                st.slot_of.resize(o.k);
-                for (int b = 0; b < o.k; ++b) {
-                    st.slot_of[b] = slot_of_bit(L, local_of[o.qubits[b]]);
-                    st.slots |= static_cast<uint8_t>(1u << st.slot_of[b]);
+    }
+    while (remaining) {
+        bool progress = false;
+        for (size_t i = 0; i < n_ops; ++i) {
+            if (done[i] || !is_ready(i, head)) continue;
+            const Op& o = pass.ops[i];
+            if (o.kind == OP_SWAP) {
+                // exchange the roles of the two local bits: the data stays where it is
+                const int a = local_of[o.qubits[0]], b = local_of[o.qubits[1]];
+                uint8_t* where[kRtQubits] = {};
+                for (int p = 0; p < kRtRegBits; ++p) where[L.reg[p]] = &L.reg[p];
+                for (int k = 0; k < kRtLaneBits; ++k) where[L.lane[k]] = &L.lane[k];
+                for (int k = 0; k < kRtWarpBits; ++k) where[L.warp[k]] = &L.warp[k];
+                std::swap(*where[a], *where[b]);
+                RtStep st;
+                st.kind = RT_RELABEL;
+                st.layout = L;
+                st.op = &o;
+                out->steps.push_back(st);
+            } else {
+                if (mix[i] & ~reg_set(L)) continue;
+                RtStep st;
+                st.op = &o;
+                switch (o.kind) {
+                    case OP_DENSE:
+                        st.kind = RT_DENSE;
+                        st.slot_of.resize(o.k);
+                        for (int b = 0; b < o.k; ++b) {
+                            st.slot_of[b] = slot_of_bit(L, local_of[o.qubits[b]]);
+                            st.slots |= static_cast<uint8_t>(1u << st.slot_of[b]);
+                        }
+                        break;
+                    case OP_CTRL1:
+                        st.kind = RT_CTRL1;
+                        st.slots = static_cast<uint8_t>(1u << slot_of_bit(L, local_of[o.target]));
+                        break;
+                    case OP_PAULI_ROT:
+                        st.kind = RT_PAULI;
+                        for (int b = 0; b < kRtQubits; ++b)
+                            if ((mix[i] >> b) & 1) st.slots |= static_cast<uint8_t>(1u << slot_of_bit(L, b));
+                        break;
+                    case OP_DIAG: st.kind = RT_DIAG; break;
+                    case OP_PHASE: st.kind = RT_PHASE; break;
+                    default: st.kind = RT_SCALE; break;
                 }
-                break;
-            case OP_CTRL1:
-                st.kind = RT_CTRL1;
-                st.slots = static_cast<uint8_t>(1u << slot_of_bit(L, local_of[o.target]));
-                break;
-            case OP_PAULI_ROT:
-                st.kind = RT_PAULI;
-                for (int b = 0; b < kRtQubits; ++b)
-                    if ((mix[i] >> b) & 1) st.slots |= static_cast<uint8_t>(1u << slot_of_bit(L, b));
-                break;
-            case OP_DIAG: st.kind = RT_DIAG; break;
-            case OP_PHASE: st.kind = RT_PHASE; break;
-            default: st.kind = RT_SCALE; break;
+                st.layout = L;
+                out->steps.push_back(st);
+            }
+            done[i] = 1;
+            advance(i, head);
+            --remaining;
+            progress = true;
         }
+        if (!remaining) break;
+        // one scan in order runs everything this register set allows (an op's predecessors
+        // come before it): transpose to the best next set
+        const uint32_t before = reg_set(L);
+        std::vector<int> bits = choose(before);
+        uint32_t m = 0;
+        for (int b : bits) m |= 1u << b;
+        if (m == before && !progress) throw std::logic_error("register-tile planner made no progress");
+        if (m == before) continue;
+        L = make_layout(bits, false);
+        RtStep st;
+        st.kind = RT_XPOSE;
         st.layout = L;
         out->steps.push_back(st);
+        ++out->transposes;
     }
     // the store wants lanes = local bits 0..4 in order (32 consecutive amplitudes per warp)
     bool store_ok = true;
