@@ -17,6 +17,10 @@
 #include "../../include/qsv.h"
 #include "kernels.h"
 
+#ifndef QSV_DENSE4_F32_BLOCKS
+#define QSV_DENSE4_F32_BLOCKS 4
+#endif
+
 namespace qsv {
 
 namespace {
@@ -69,8 +73,15 @@ struct DenseArgs {
 // parallelism an HBM-streaming pass needs.  Loads and stores are evict-first (__ldcs /
 // __stcs): the register is touched once per pass.  C = 1: one control qubit, whose groups
 // with the control clear are neither read nor written.
+// resident blocks per SM the register budget is sized for: complex64 groups take half the
+// registers, so their 4-qubit blocks can keep more loads in flight
+template <typename T, int K>
+constexpr int dense_min_blocks() {
+    return K <= 3 ? 4 : (sizeof(T) == 8 ? 2 : QSV_DENSE4_F32_BLOCKS);
+}
+
 template <typename T, int K, int C>
-__global__ void __launch_bounds__(kThreads, (K <= 3 ? 4 : 2))
+__global__ void __launch_bounds__(kThreads, (dense_min_blocks<T, K>()))
     k_dense_reg(vec2_t<T>* __restrict__ s, uint64_t n_groups, const __grid_constant__ DenseArgs<T, K> a) {
     constexpr int D = 1 << K;
     const uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -291,8 +302,9 @@ void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws
                 if constexpr (sizeof(T) == sizeof(double)) {
                     if (launch_dense_tensor(op, reinterpret_cast<double2*>(s), n, st, ws)) return;
                 } else {
-                    // k = 5 in complex64: tcgen05 3xTF32 GEMM with TMEM accumulators
+                    // k = 5 in complex64: tcgen05 3xTF32 GEMM with TMEM accumulators; k = 6: DMMA
                     if (launch_dense_umma(op, reinterpret_cast<float2*>(s), n, st, ws)) return;
+                    if (launch_dense_tensor_f32(op, reinterpret_cast<float2*>(s), n, st, ws)) return;
                 }
             }
             // other wide blocks: out of place through a workspace copy of the register

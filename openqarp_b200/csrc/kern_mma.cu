@@ -10,7 +10,10 @@
 // qubits are not the lowest ones), split them into real/imaginary planes, run the MMAs, write
 // the result planes back and scatter them to HBM.  Row strides are padded by 4 doubles so
 // the fragment loads are bank-conflict free.  Arithmetic intensity is 2^(k-2) flop/byte
-// (8 at k = 5), above the FP64 ridge: these blocks are tensor-bound, not HBM-bound.
+// (8 at k = 5), above the FP64 ridge: these blocks are tensor-bound, not HBM-bound.  A
+// complex64 register goes through the same kernel (amplitudes widened to FP64 in the planes):
+// its k = 6 blocks have no 3xTF32 path, because shared memory cannot hold both split operands
+// of their 128 x 128 real GEMM tile next to the group tile.
 #include <algorithm>
 #include <stdexcept>
 #include <vector>
@@ -47,8 +50,8 @@ struct MmaShape {
     static constexpr size_t smem = sizeof(double) * (static_cast<size_t>(R) * WS + 2 * static_cast<size_t>(D) * S);
 };
 
-template <int K>
-__global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(double2* __restrict__ s, uint64_t n_groups,
+template <typename T, int K>
+__global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(vec2_t<T>* __restrict__ s, uint64_t n_groups,
                                                             const double* __restrict__ W,
                                                             const __grid_constant__ MmaArgs a) {
     using Sh = MmaShape<K>;
@@ -68,10 +71,10 @@ __global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(double2* __restrict_
         for (int e = threadIdx.x; e < EL; e += blockDim.x) {
             const int j = e % Sh::NG, x = e / Sh::NG;
             const uint64_t g = t0 + j;
-            double2 v = make_double2(0.0, 0.0);
+            vec2_t<T> v = mk<T>(T(0), T(0));
             if (g < n_groups) v = __ldcs(s + (insert_zeros(g, a.pos, K) | a.off[x]));
-            xr[x * Sh::S + j] = v.x;
-            xi[x * Sh::S + j] = v.y;
+            xr[x * Sh::S + j] = static_cast<double>(v.x);
+            xi[x * Sh::S + j] = static_cast<double>(v.y);
         }
         __syncthreads();
         double acc[Sh::MPW][2];
@@ -100,13 +103,14 @@ __global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(double2* __restrict_
             const int j = e % Sh::NG, x = e / Sh::NG;
             const uint64_t g = t0 + j;
             if (g < n_groups)
-                __stcs(s + (insert_zeros(g, a.pos, K) | a.off[x]), make_double2(xr[x * Sh::S + j], xi[x * Sh::S + j]));
+                __stcs(s + (insert_zeros(g, a.pos, K) | a.off[x]),
+                       mk<T>(static_cast<T>(xr[x * Sh::S + j]), static_cast<T>(xi[x * Sh::S + j])));
         }
     }
 }
 
-template <int K>
-void launch_dmma(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws) {
+template <typename T, int K>
+void launch_dmma(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws) {
     using Sh = MmaShape<K>;
     MmaArgs a{};
     uint32_t sorted[8];
@@ -133,17 +137,17 @@ void launch_dmma(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws
     // source makes cudaMemcpyAsync return only after W has been staged, so W may go out of scope
     check_cuda(cudaStreamSynchronize(st), "matrix buffer reuse");
     check_cuda(cudaMemcpyAsync(dW, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, st), "W upload");
-    check_cuda(cudaFuncSetAttribute(k_dense_dmma<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    check_cuda(cudaFuncSetAttribute(k_dense_dmma<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(Sh::smem)), "dmma smem");
     int device = 0, sms = 0, per_sm = 0;
     check_cuda(cudaGetDevice(&device), "device");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_dmma<K>, kMmaThreads, Sh::smem),
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_dmma<T, K>, kMmaThreads, Sh::smem),
                "occupancy");
     const uint64_t groups = (1ull << n) >> K;
     const uint64_t tiles = (groups + Sh::NG - 1) / Sh::NG;
     const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(sms) * std::max(per_sm, 1)));
-    k_dense_dmma<K><<<static_cast<unsigned>(grid), kMmaThreads, Sh::smem, st>>>(s, groups, dW, a);
+    k_dense_dmma<T, K><<<static_cast<unsigned>(grid), kMmaThreads, Sh::smem, st>>>(s, groups, dW, a);
     check_cuda(cudaGetLastError(), "dmma launch");
 }
 
@@ -151,8 +155,15 @@ void launch_dmma(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws
 
 bool launch_dense_tensor(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws) {
     if (op.kind != OP_DENSE || op.k < 5 || op.k > 6 || n < op.k) return false;
-    if (op.k == 5) launch_dmma<5>(op, s, n, st, ws);
-    else launch_dmma<6>(op, s, n, st, ws);
+    if (op.k == 5) launch_dmma<double, 5>(op, s, n, st, ws);
+    else launch_dmma<double, 6>(op, s, n, st, ws);
+    return true;
+}
+
+bool launch_dense_tensor_f32(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws) {
+    if (op.kind != OP_DENSE || op.k < 5 || op.k > 6 || n < op.k) return false;
+    if (op.k == 5) launch_dmma<float, 5>(op, s, n, st, ws);
+    else launch_dmma<float, 6>(op, s, n, st, ws);
     return true;
 }
 

@@ -61,6 +61,9 @@ void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& 
 bool launch_dense_tensor(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws);
 // Dense k = 5 blocks in complex64 on tcgen05 (kern_umma.cu); false when not such a block.
 bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws);
+// Dense k = 5, 6 blocks of a complex64 register on the FP64 tensor pipe (kern_mma.cu): the k = 6
+// path, and k = 5 where the tcgen05 kernel declines.
+bool launch_dense_tensor_f32(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws);
 
 // ---------------------------------------------------------------- tiled executor (kern_tile.cu)
 // Launch the planned passes; one-op stream passes (empty tile_qubits) go to `stream_op`.

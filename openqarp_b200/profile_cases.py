@@ -5,6 +5,9 @@
     python -m openqarp_b200.profile_cases transition --n 24 --terms 547
     python -m openqarp_b200.profile_cases adjoint --n 22 --layers 2
     python -m openqarp_b200.profile_cases sample --n 26 --shots 100000
+    python -m openqarp_b200.profile_cases exact --n 26
+    python -m openqarp_b200.profile_cases parity --n 26 --shots 1048576 --terms 512
+    python -m openqarp_b200.profile_cases perm --n 26
 
 Registers of 2^26 complex128 amplitudes (1 GiB) exceed L2 (126 MB), so DRAM counters are
 meaningful, and stay small enough for a full-set capture to end within minutes.
@@ -20,7 +23,8 @@ from . import Register, circuits, ir, observable
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense", "brickwork", "transition", "adjoint", "sample"])
+    ap.add_argument("case", choices=["dense", "brickwork", "transition", "adjoint", "sample", "exact", "parity",
+                                     "perm"])
     ap.add_argument("--n", type=int, default=26)
     ap.add_argument("--k", type=int, default=3)
     ap.add_argument("--reps", type=int, default=5)
@@ -56,6 +60,22 @@ def main(argv=None):
     elif a.case == "sample":
         reg.apply(ir.pack(circuits.brickwork(a.n, 1, seed=1)).buf)
         reg.sample(np.sort(rng.random(a.shots)))
+    elif a.case == "exact":
+        reg.apply(ir.pack(circuits.brickwork(a.n, 1, seed=1)).buf)
+        for _ in range(a.reps):
+            reg.exact_probs(1e-12)
+    elif a.case == "parity":
+        reg.apply(ir.pack(circuits.brickwork(a.n, 1, seed=1)).buf)
+        masks = rng.integers(0, 1 << a.n, size=a.terms).astype(np.uint64)
+        for _ in range(a.reps):
+            reg.sample_parities(7, a.shots, masks)
+    elif a.case == "perm":
+        from .ir import PermutationRecord
+        qs = tuple(int(q) for q in rng.permutation(a.n)[:16])
+        rec = PermutationRecord(qs, rng.permutation(1 << 16).astype(np.uint64))
+        reg.configure(0, 0, 0)
+        for _ in range(a.reps):
+            reg.apply(ir.pack([rec]).buf)
     reg.synchronize()
     reg.close()
     print("ok", a.case)

@@ -64,7 +64,8 @@ def test_tcgen05_wide_block_complex64(n, restatement):
         assert np.max(np.abs(got - want)) < 50 * np.finfo(np.float32).eps
 
 
-def test_complex64_k6_fallback(restatement):
+def test_complex64_k6_on_the_fp64_tensor_pipe(restatement):
+    """complex64 k = 6 blocks go through the DMMA kernel with the planes widened to FP64."""
     n, k = 12, 6
     rng = np.random.default_rng(4)
     psi = random_state(n, 5)
