@@ -285,7 +285,21 @@ def adjoint_vs_param_shift(device, shift_sample=12):
     err = float(np.max(np.abs(np.array(grads) - grad[[names.index(cmds[i].params[0].free_symbols()[0])
                                                        for i in sample]])))
     sim.close()
+    # the same adjoint in complex64 bulk mode (FP64 accumulations, checkpointed psi)
+    from openqarp_b200 import Register
+    r64 = Register(ADJ_N, "complex64", device)
+    r64.reset()
+    r64.adjoint(stream, len(names), masks)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    r64.reset()
+    e64, g64 = r64.adjoint(stream, len(names), masks)
+    t_adj64 = time.perf_counter() - t0
+    r64.close()
     return {"n_qubits": ADJ_N, "params": len(names), "terms": len(obs), "energy": energy,
+            "complex64": {"adjoint_s": t_adj64, "adjoint_grads_per_s": 1.0 / t_adj64,
+                          "max_abs_grad_diff_vs_complex128": float(np.max(np.abs(np.asarray(g64) - grad))),
+                          "energy_diff_vs_complex128": abs(e64 - energy)},
             "adjoint_s": t_adj, "adjoint_grads_per_s": 1.0 / t_adj,
             "param_shift_s": t_ps, "param_shift_grads_per_s": 1.0 / t_ps,
             "speedup_vs_param_shift": t_ps / t_adj,

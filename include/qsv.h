@@ -97,7 +97,7 @@ enum qsv_gate {
  * qubits[b]), the PermutationKernel of a structured program (reference:
  * src/qarpx/include/qarpx/simulator/program.h:18-21, apply_permutation program.cpp:610-643).
  * Payload after the (zero) params: uint64_t table[2^n_qubits], a bijection.  The register
- * keeps its device address (the kernel scatters from a workspace copy). */
+ * keeps its device address (the kernel gathers from a workspace copy). */
 #define QSV_GATE_PERMUTATION 200
 /* reference: program.cpp:35 kMaxTableQubits = 26 */
 #define QSV_MAX_PERMUTATION_QUBITS 26

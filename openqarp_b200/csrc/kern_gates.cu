@@ -241,12 +241,14 @@ __global__ void __launch_bounds__(kThreads) k_perm(const vec2_t<T>* __restrict__
                                                    const __grid_constant__ PermArgs a) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
-        uint64_t x = 0;
-        for (int b = 0; b < a.k; ++b) x |= ((i >> a.q[b]) & 1ull) << b;
-        const uint64_t y = __ldg(table + x);
+        // gather form: output j takes input inverse[j], so the writes are coalesced and only
+        // the reads are scattered (a scattered 16-byte write costs a sector read-modify-write)
+        uint64_t y = 0;
+        for (int b = 0; b < a.k; ++b) y |= ((i >> a.q[b]) & 1ull) << b;
+        const uint64_t x = __ldg(table + y);
         uint64_t j = i & a.keep;
-        for (int b = 0; b < a.k; ++b) j |= ((y >> b) & 1ull) << a.q[b];
-        dst[j] = src[i];
+        for (int b = 0; b < a.k; ++b) j |= ((x >> b) & 1ull) << a.q[b];
+        dst[i] = src[j];
     }
 }
 
@@ -409,8 +411,8 @@ void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws
     }
 }
 
-// The register keeps its address (a zero-copy caller may hold it): copy it aside, then
-// scatter the copy back through the table.
+// The register keeps its address (a zero-copy caller may hold it): copy it aside, then gather
+// it back through the inverse table.
 template <typename T>
 void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws) {
     if (op.k < 1 || op.k > QSV_MAX_PERMUTATION_QUBITS || op.table.size() != (size_t{1} << op.k))
@@ -423,10 +425,12 @@ void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& 
         a.q[b] = static_cast<uint8_t>(op.pq[b]);
         a.keep &= ~(1ull << op.pq[b]);
     }
-    uint64_t* dt = static_cast<uint64_t*>(ws.matrix(op.table.size() * sizeof(uint64_t)));
+    std::vector<uint64_t> inverse(op.table.size());
+    for (size_t x = 0; x < op.table.size(); ++x) inverse[op.table[x]] = x;
+    uint64_t* dt = static_cast<uint64_t*>(ws.matrix(inverse.size() * sizeof(uint64_t)));
     // the matrix buffer's previous user must be done; the pageable copy returns once staged
     check_cuda(cudaStreamSynchronize(st), "matrix buffer reuse");
-    check_cuda(cudaMemcpyAsync(dt, op.table.data(), op.table.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st),
+    check_cuda(cudaMemcpyAsync(dt, inverse.data(), inverse.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st),
                "permutation table");
     const uint64_t dim = 1ull << n;
     vec2_t<T>* copy = static_cast<vec2_t<T>*>(ws.state_copy(dim * sizeof(vec2_t<T>)));
