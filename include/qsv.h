@@ -53,6 +53,8 @@ extern "C" {
  *   qsv_cmd_header                      8 bytes
  *   uint32_t qubits[n_qubits]           local bit b <-> qubits[b]
  *   uint32_t cbits[n_cbits]             Measure's recorded classical bits
+ *   uint32_t cond_bits[n_cond]          classical condition: the command (or a BranchBegin's
+ *   uint32_t cond_values[n_cond]        branch) applies when every cbit equals its value
  *   (zero padding to a multiple of 8)
  *   double   params[n_params]           concrete angles, in the reference's order
  *   double   matrix[2 * 4^n_qubits]     only for QSV_GATE_CUSTOM: row-major 2^k x 2^k,
@@ -68,8 +70,9 @@ typedef struct qsv_cmd_header {
     uint8_t  n_qubits;
     uint8_t  n_params;
     uint8_t  n_cbits;
-    uint8_t  flags;     /* bit 0: command carries a classical condition (rejected) */
-    uint16_t reserved;
+    uint8_t  flags;     /* bit 0: command carries a classical condition            */
+    uint8_t  n_cond;    /* condition entries (qarpx::Command condition_bits/values) */
+    uint8_t  reserved;
 } qsv_cmd_header;
 
 /* qarpx::GateType enumerator values (reference: src/qarpx/include/qarpx/core/gates.h:8-58). */

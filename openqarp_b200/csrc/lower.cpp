@@ -116,13 +116,20 @@ std::vector<Cmd> decode(const uint8_t* buf, size_t nbytes) {
         c.gate = h.gate;
         c.flags = h.flags;
         size_t o = off + sizeof h;
-        const size_t nq = h.n_qubits, nc = h.n_cbits, np = h.n_params;
-        if (o + 4 * (nq + nc) > nbytes) throw std::invalid_argument("command buffer truncated");
+        const size_t nq = h.n_qubits, nc = h.n_cbits, np = h.n_params, ncd = h.n_cond;
+        if (o + 4 * (nq + nc + 2 * ncd) > nbytes) throw std::invalid_argument("command buffer truncated");
         c.q.resize(nq);
         c.cbits.resize(nc);
+        c.cond_bits.resize(ncd);
+        c.cond_values.resize(ncd);
         if (nq) std::memcpy(c.q.data(), buf + o, 4 * nq);
         if (nc) std::memcpy(c.cbits.data(), buf + o + 4 * nq, 4 * nc);
-        o += 4 * (nq + nc);
+        if (ncd) {
+            std::memcpy(c.cond_bits.data(), buf + o + 4 * (nq + nc), 4 * ncd);
+            std::memcpy(c.cond_values.data(), buf + o + 4 * (nq + nc + ncd), 4 * ncd);
+            c.flags |= 1;
+        }
+        o += 4 * (nq + nc + 2 * ncd);
         o = (o + 7) & ~size_t{7};
         if (o + 8 * np > nbytes) throw std::invalid_argument("command buffer truncated");
         c.p.resize(np);

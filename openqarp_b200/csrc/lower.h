@@ -35,6 +35,8 @@ struct Cmd {
     int gate = BARRIER;
     std::vector<uint32_t> q;
     std::vector<uint32_t> cbits;
+    std::vector<uint32_t> cond_bits;     // classical condition: every cond_bits[i] == cond_values[i]
+    std::vector<uint32_t> cond_values;
     std::vector<double> p;
     std::vector<c128> u;     // Custom: 2^k x 2^k row-major, local bit b <-> q[b]
                              // ControlledUnitary: 2^(k-1) square on q[0..k-1)

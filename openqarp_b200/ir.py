@@ -305,7 +305,7 @@ def _pack_record(out: bytearray, rec) -> None:
         if m.shape != (1 << k, 1 << k):
             raise ValueError("controlled unitary record: matrix is not 2^|targets| square")
         code, payload = CONTROLLED_UNITARY_CODE, m.tobytes()
-    out += _HDR.pack(code, len(qubits), 0, 0, 0, 0)
+    out += _HDR.pack(code, len(qubits), 0, 0, 0, 0, 0)
     out += struct.pack(f"<{len(qubits)}I", *qubits)
     if len(out) % 8:
         out += b"\0" * (8 - len(out) % 8)
@@ -314,7 +314,7 @@ def _pack_record(out: bytearray, rec) -> None:
 
 # ---------------------------------------------------------------- packing
 
-_HDR = struct.Struct("<HBBBBH")
+_HDR = struct.Struct("<HBBBBBB")
 
 
 def _gate_code(g) -> int:
@@ -371,9 +371,15 @@ def pack(commands: Iterable, values: Optional[Mapping[str, float]] = None,
         vals = [_param_value(p, values) for p in params]
         if len(qubits) > 255 or len(params) > 255 or len(cbits) > 255:
             raise ValueError("command too wide to pack")
+        cond_vals = [1 if v else 0 for v in (getattr(cmd, "condition_values", ()) or ())]
+        if len(cond_vals) != len(cond):
+            raise ValueError("condition_bits and condition_values differ in length")
+        if len(cond) > 255:
+            raise ValueError("command too wide to pack")
         flags = 1 if cond else 0
-        out += _HDR.pack(g, len(qubits), len(vals), len(cbits), flags, 0)
-        out += struct.pack(f"<{len(qubits) + len(cbits)}I", *qubits, *cbits)
+        out += _HDR.pack(g, len(qubits), len(vals), len(cbits), flags, len(cond), 0)
+        out += struct.pack(f"<{len(qubits) + len(cbits) + 2 * len(cond)}I", *qubits, *cbits,
+                           *[int(b) for b in cond], *cond_vals)
         if len(out) % 8:
             out += b"\0" * (8 - len(out) % 8)
         out += struct.pack(f"<{len(vals)}d", *vals)

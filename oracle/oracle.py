@@ -165,6 +165,8 @@ class Reference:
         lib.qref_run.argtypes = [P8, c_size_t, c_int, c_int, c_uint32, c_int, c_int, PU64, PI32, c_size_t,
                                  POINTER(c_size_t)]
         lib.qref_uniforms.argtypes = [c_uint32, c_size_t, PD]
+        lib.qref_run_history.argtypes = [P8, c_size_t, c_int, c_int, c_uint32, c_int, c_int, PU64, PI32, c_size_t,
+                                         POINTER(c_size_t), PU64, POINTER(c_int)]
         lib.qref_run_gradient.argtypes = [P8, c_size_t, c_int, PI32, PI32, PD, c_int, PD, PU64, PU64, PD,
                                           c_size_t, PD, PD]
         lib.qref_program_new.restype = ctypes.c_void_p
@@ -240,6 +242,19 @@ class Reference:
         self._check(self.lib.qref_run(_u8(buf), len(buf), n, shots, seed & 0xFFFFFFFF, fusion_max,
                                       fusion_min, _u64(keys), _i32(cnts), cap, ctypes.byref(got)))
         return {int(keys[i]): int(cnts[i]) for i in range(got.value)}
+
+    def run_history(self, buf, n, shots, seed, fusion_max=-1, fusion_min=-1):
+        """run() with the per-shot classical register (bitmasks) and its width."""
+        cap = max(1, min(shots, 1 << n))
+        keys = np.zeros(cap, dtype=np.uint64)
+        cnts = np.zeros(cap, dtype=np.int32)
+        hist = np.zeros(max(shots, 1), dtype=np.uint64)
+        got = c_size_t()
+        ncb = c_int()
+        self._check(self.lib.qref_run_history(_u8(buf), len(buf), n, shots, seed & 0xFFFFFFFF, fusion_max,
+                                              fusion_min, _u64(keys), _i32(cnts), cap, ctypes.byref(got),
+                                              _u64(hist), ctypes.byref(ncb)))
+        return {int(keys[i]): int(cnts[i]) for i in range(got.value)}, hist[:shots], ncb.value
 
     def uniforms(self, seed, shots):
         u = np.zeros(shots)

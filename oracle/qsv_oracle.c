@@ -66,9 +66,11 @@ static int decode(const uint8_t* buf, size_t nbytes, size_t off, rec_t* r) {
     uint16_t gate; memcpy(&gate, buf + off, 2);
     r->gate = gate;
     r->nq = buf[off + 2]; r->np = buf[off + 3]; r->ncb = buf[off + 4]; r->flags = buf[off + 5];
+    const int ncond = buf[off + 6];   /* condition entries: bits then values, after the cbits */
     size_t o = off + 8;
     r->q = (const uint32_t*)(buf + o);
-    o += 4u * (size_t)(r->nq + r->ncb);
+    o += 4u * (size_t)(r->nq + r->ncb + 2 * ncond);
+    if (ncond) r->flags |= 1;
     o = (o + 7u) & ~(size_t)7u;
     r->p = (const double*)(buf + o);
     o += 8u * (size_t)r->np;

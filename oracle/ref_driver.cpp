@@ -55,6 +55,7 @@ struct Rec {
     const uint32_t* q;
     const double* p;
     const double* m;
+    int ncond = 0;   // condition bits then values follow the cbits in q[]
 };
 
 std::vector<Rec> decode_all(const uint8_t* buf, size_t nbytes) {
@@ -64,10 +65,10 @@ std::vector<Rec> decode_all(const uint8_t* buf, size_t nbytes) {
         if (off + 8 > nbytes) throw std::invalid_argument("command buffer truncated");
         qsv_cmd_header h;
         std::memcpy(&h, buf + off, sizeof h);
-        Rec r{h.gate, h.n_qubits, h.n_params, h.n_cbits, h.flags, nullptr, nullptr, nullptr};
+        Rec r{h.gate, h.n_qubits, h.n_params, h.n_cbits, h.flags, nullptr, nullptr, nullptr, h.n_cond};
         size_t o = off + 8;
         r.q = reinterpret_cast<const uint32_t*>(buf + o);
-        o += 4u * static_cast<size_t>(r.nq + r.ncb);
+        o += 4u * static_cast<size_t>(r.nq + r.ncb + 2 * r.ncond);
         o = (o + 7u) & ~size_t{7};
         r.p = reinterpret_cast<const double*>(buf + o);
         o += 8u * static_cast<size_t>(r.np);
@@ -88,6 +89,10 @@ Command to_command(const Rec& r) {
     for (int b = 0; b < r.nq; ++b) c.qubits.push_back(r.q[b]);
     for (int b = 0; b < r.ncb; ++b) c.cbits.push_back(r.q[r.nq + b]);
     for (int b = 0; b < r.np; ++b) c.params.push_back(Param(r.p[b]));
+    for (int b = 0; b < r.ncond; ++b) {
+        c.condition_bits.push_back(r.q[r.nq + r.ncb + b]);
+        c.condition_values.push_back(r.q[r.nq + r.ncb + r.ncond + b] != 0);
+    }
     if (r.m) {
         const int D = 1 << r.nq;
         Eigen::MatrixXcd U(D, D);
@@ -277,12 +282,35 @@ int qref_expectation(const uint8_t* cmds, size_t nbytes, int n, int fusion_max,
     }
 }
 
+int qref_run_history(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed,
+                     int fusion_max, int fusion_min, uint64_t* keys, int32_t* counts, size_t cap,
+                     size_t* n_out, uint64_t* history, int* n_cbits);
+
 int qref_run(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed,
              int fusion_max, int fusion_min, uint64_t* keys, int32_t* counts, size_t cap,
              size_t* n_out) {
+    return qref_run_history(cmds, nbytes, n, shots, seed, fusion_max, fusion_min, keys, counts, cap, n_out,
+                            nullptr, 0);
+}
+
+// run() with the per-shot classical register: history[s] holds shot s's cbits as a bitmask
+// (cbit c -> bit c), for registers of at most 64 cbits.
+int qref_run_history(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed,
+                     int fusion_max, int fusion_min, uint64_t* keys, int32_t* counts, size_t cap,
+                     size_t* n_out, uint64_t* history, int* n_cbits) {
     try {
         auto sim = make_sim(fusion_max, fusion_min);
         auto res = sim.run(to_commands(cmds, nbytes), n, shots, seed);
+        if (history) {
+            if (res.n_cbits > 64) throw std::invalid_argument("qref_run_history: more than 64 cbits");
+            for (size_t s = 0; s < res.cbit_history.size(); ++s) {
+                uint64_t m = 0;
+                for (size_t c = 0; c < res.cbit_history[s].size(); ++c)
+                    if (res.cbit_history[s][c]) m |= 1ull << c;
+                history[s] = m;
+            }
+            if (n_cbits) *n_cbits = static_cast<int>(res.n_cbits);
+        }
         size_t i = 0;
         for (const auto& [k, v] : res.counts) {
             if (i >= cap) throw std::invalid_argument("qref_run: output capacity too small");
