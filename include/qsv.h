@@ -235,6 +235,25 @@ QSV_API int qsv_sample_parities(void* h, uint32_t seed, size_t n_shots, const ui
 QSV_API int qsv_exact_probs(void* h, double threshold, uint64_t* keys, double* probs, uint64_t cap,
                             uint64_t* n_out);
 
+/* Shot trajectories: QarpSimulator::run's per-shot path for streams with mid-circuit Measure,
+ * Reset, classical conditions and BranchBegin / BranchElse / BranchEnd (reference:
+ * qarp_simulator.cpp:1040-1243; per-command rules apply_command_trajectory :600-695).  The
+ * unitary prefix (commands before the first Reset, recorded Measure, conditioned command or
+ * BranchBegin) runs once on the handle's register, which keeps that state on return; the rest
+ * runs per shot, batched on the device.  Shot s draws from std::mt19937(seed + s) with
+ * uniform_real_distribution<double>(0, 1): one draw per Measure / Reset it executes, then one
+ * for its final sample (threshold = u * total, first index whose running sum reaches it).
+ * out_idx[s] = shot s's sampled basis index; out_cbits[s] = its classical register as a bit
+ * mask (bit c = cbit c); *n_cbits = the register width (cbit_register_width,
+ * command.cpp:259-271; at most 64).  This entry always takes the trajectory path: the caller
+ * picks run()'s sample-once path for streams whose measurements are terminal. */
+/* Shots per device batch of qsv_run_trajectories (rounded down to a power of two; 0, the
+ * default: as many as half the free device memory holds, at most 2^20).  Results do not depend
+ * on it. */
+QSV_API int qsv_set_trajectory_batch(void* h, uint64_t max_shots);
+QSV_API int qsv_run_trajectories(void* h, const uint8_t* cmds, size_t nbytes, uint32_t seed, size_t n_shots,
+                                 uint64_t* out_idx, uint64_t* out_cbits, int32_t* n_cbits);
+
 /* Adjoint gradient of <psi|H|psi>, psi = U(theta)|psi0>, psi0 = the handle's current
  * register.  cmds is the concrete stream; for command i, its angle depends on params
  * dep_param[dep_ptr[i] .. dep_ptr[i+1]) with coefficients dep_alpha (d angle / d param).

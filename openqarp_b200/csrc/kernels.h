@@ -139,6 +139,21 @@ uint64_t exact_readout(const vec2_t<T>* s, int n, double thr, uint64_t* d_keys, 
 void parity_counts(const uint64_t* d_outcome, size_t n_shots, const uint64_t* d_masks, size_t n_masks,
                    unsigned long long* d_odd, cudaStream_t st);
 
+// ---------------------------------------------------------------- trajectories (kern_traj.cu)
+struct TrajOptions {
+    int fusion_max = 3;           // fusion of the gates every shot applies
+    int fusion_min = 12;
+    uint64_t max_batch_shots = 0; // shots per device batch (0: as many as half the free memory holds)
+};
+// Run n_shots trajectories of `suffix` from the n-qubit device state d_prefix (left unchanged):
+// out_idx[s] = shot s's final sampled index, out_cbits[s] = its classical register (bit c =
+// cbit c).  Shot s draws from std::mt19937(seed + s).  The suffix is validated (branch
+// structure, condition and cbit ranges) even when n_shots is 0.
+template <typename T>
+void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const vec2_t<T>* d_prefix, uint32_t seed,
+                      size_t n_shots, const TrajOptions& opt, uint64_t* out_idx, uint64_t* out_cbits,
+                      cudaStream_t st, Workspace& ws, uint64_t* launches);
+
 // ---------------------------------------------------------------- adjoint (kern_reduce.cu)
 // One reverse step of a parametric gate of width k (0..2): with psi, phi the states after
 // the gate, accumulate ip = <phi| G |psi> into slot `slot` of the partials table, then apply

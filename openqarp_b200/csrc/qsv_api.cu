@@ -37,6 +37,7 @@ struct Handle {
     void* aux = nullptr;          // second register (adjoint's |phi>)
     size_t aux_cap = 0;
     int checkpoint_interval = -1; // adjoint: commands between psi checkpoints (-1 auto, 0 none)
+    uint64_t traj_batch = 0;      // trajectories: shots per device batch (0: memory-bound default)
     uint64_t dim() const { return 1ull << n; }
     size_t amp_bytes() const { return dtype == QSV_C128 ? 16 : 8; }
 };
@@ -347,6 +348,10 @@ int qsv_set_checkpoint_interval(void* hp, int k) {
     });
 }
 
+int qsv_set_trajectory_batch(void* hp, uint64_t max_shots) {
+    return guarded([&] { H_(hp)->traj_batch = max_shots; });
+}
+
 int qsv_set_tile_qubits(void* hp, int m) {
     return guarded([&] {
         Handle* h = H_(hp);
@@ -588,6 +593,40 @@ int qsv_exact_probs(void* hp, double threshold, uint64_t* keys, double* probs, u
         d2h(h, keys, d_keys, total * 8);
         d2h(h, probs, d_probs, total * 8);
         h->stats.launches += 3;
+    });
+}
+
+int qsv_run_trajectories(void* hp, const uint8_t* cmds, size_t nbytes, uint32_t seed, size_t n_shots,
+                         uint64_t* out_idx, uint64_t* out_cbits, int32_t* n_cbits) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!cmds && nbytes) throw std::invalid_argument("null command buffer");
+        const std::vector<Cmd> cs = decode(cmds, nbytes);
+        // classical register width (cbit_register_width, command.cpp:259-271)
+        int width = 0;
+        for (const Cmd& c : cs) {
+            if (c.gate == MEASURE)
+                for (uint32_t b : c.cbits) width = std::max(width, static_cast<int>(b) + 1);
+            for (uint32_t b : c.cond_bits) width = std::max(width, static_cast<int>(b) + 1);
+        }
+        if (n_cbits) *n_cbits = width;
+        // unitary prefix once, on the handle's register (first_trajectory_index,
+        // qarp_simulator.cpp:273-278)
+        size_t split = 0;
+        while (split < cs.size() && !needs_trajectory(cs[split])) ++split;
+        const std::vector<Cmd> prefix(cs.begin(), cs.begin() + static_cast<std::ptrdiff_t>(split));
+        const std::vector<Cmd> suffix(cs.begin() + static_cast<std::ptrdiff_t>(split), cs.end());
+        TrajOptions opt;
+        opt.fusion_max = h->fusion_max;
+        opt.fusion_min = h->fusion_min;
+        opt.max_batch_shots = h->traj_batch;
+        if (!prefix.empty()) apply_cmds(h, prefix, true);
+        if (h->dtype == QSV_C128)
+            run_trajectories<double>(suffix, h->n, width, S128(h), seed, n_shots, opt, out_idx, out_cbits, h->stream,
+                                     h->ws, &h->stats.launches);
+        else
+            run_trajectories<float>(suffix, h->n, width, S64(h), seed, n_shots, opt, out_idx, out_cbits, h->stream,
+                                    h->ws, &h->stats.launches);
     });
 }
 

@@ -178,6 +178,22 @@ class Register:
                 raise RuntimeError("exact readout count changed between passes")
         return keys.astype(np.int64), probs
 
+    def set_trajectory_batch(self, max_shots: int):
+        """Shots per device batch of run_trajectories (0: memory-bound default)."""
+        check(lib.qsv_set_trajectory_batch(self.handle, int(max_shots)))
+
+    def run_trajectories(self, stream, seed: int, n_shots: int) -> tuple[np.ndarray, np.ndarray, int]:
+        """Per-shot trajectories of a stream with mid-circuit Measure / Reset / conditions /
+        branches (qsv_run_trajectories): (outcomes, classical registers as bit masks, width).
+        The register keeps the state after the stream's unitary prefix."""
+        b = _as_bytes(stream)
+        out = np.empty(max(int(n_shots), 1), dtype=np.uint64)
+        regs = np.empty(max(int(n_shots), 1), dtype=np.uint64)
+        width = ctypes.c_int32()
+        check(lib.qsv_run_trajectories(self.handle, u8ptr(b), len(b), int(seed) & 0xFFFFFFFF, int(n_shots),
+                                       u64ptr(out), u64ptr(regs), ctypes.byref(width)))
+        return out[:int(n_shots)], regs[:int(n_shots)], width.value
+
     # adjoint -------------------------------------------------------------------------
     def adjoint(self, stream: PackedStream, n_params: int, masks: PauliMasks):
         grad = np.zeros(max(n_params, 1))
@@ -367,16 +383,36 @@ class B200Simulator:
 
     def run(self, commands, n_qubits: int, n_shots: int, seed: Optional[int] = None, *,
             initial_state=None) -> SamplingResult:
-        """Sample ``n_shots`` terminal outcomes (QarpSimulator::run's sample-once path,
-        qarp_simulator.cpp:1016-1036).  Seeded draws reproduce the reference's uniforms."""
+        """Sample ``n_shots`` outcomes (QarpSimulator::run, qarp_simulator.cpp:987-1243): the
+        sample-once path when every measurement is terminal (qarp_simulator.cpp:1016-1036), else
+        the per-shot trajectory path, batched on the device.  Seeded runs reproduce the
+        reference's draws."""
         commands = list(commands)
-        if not measurements_are_terminal(commands):
-            raise CapabilityError(
-                "B200Simulator.run: mid-circuit measurement, Reset or classical conditions need "
-                "the per-shot trajectory path, which the B200 engine does not implement")
         base_s = int(seed) if seed is not None else int.from_bytes(os.urandom(4), "little")
+        if not measurements_are_terminal(commands):
+            return self._trajectory_result(commands, n_qubits, n_shots, base_s, initial_state)
         reg = self._prepared(commands, n_qubits, initial_state, "run")
         return self._sample_result(reg, commands, n_qubits, n_shots, base_s)
+
+    def _trajectory_result(self, commands, n_qubits, n_shots, base_s, initial_state) -> SamplingResult:
+        """run()'s per-shot trajectory path (qarp_simulator.cpp:1040-1243), batched on the
+        device: counts of each shot's final sampled index and its classical register."""
+        reg = self.register(n_qubits)
+        self._seed(reg, n_qubits, initial_state, "run")
+        idx, regs, width = reg.run_trajectories(pack(commands), base_s, int(n_shots))
+        return self._counts_result(n_qubits, n_shots, idx, regs, width)
+
+    @staticmethod
+    def _counts_result(n_qubits, n_shots, idx, regs, width) -> SamplingResult:
+        res = SamplingResult(n_qubits, int(n_shots))
+        res.n_cbits = width
+        res.outcomes = idx
+        if idx.shape[0]:
+            keys, cnt = np.unique(idx, return_counts=True)
+            res.counts = {int(k): int(c) for k, c in zip(keys, cnt)}
+        bits = ((regs[:, None] >> np.arange(width, dtype=np.uint64)[None, :]) & np.uint64(1)).astype(bool)
+        res.cbit_history = [list(map(bool, row)) for row in bits]
+        return res
 
     def _sample_result(self, reg, commands, n_qubits, n_shots, base_s) -> SamplingResult:
         res = SamplingResult(n_qubits, int(n_shots))
@@ -402,9 +438,13 @@ class B200Simulator:
         out = []
         for i, values in enumerate(param_sets):
             s = None if seed is None else (int(seed) + i) & 0xFFFFFFFF
-            if not measurements_are_terminal(commands):
-                raise CapabilityError("B200Simulator.batch_run: trajectory circuits are not supported")
             base_s = s if s is not None else int.from_bytes(os.urandom(4), "little")
+            if not measurements_are_terminal(commands):
+                reg = self.register(n_qubits)
+                reg.reset()
+                idx, regs, width = reg.run_trajectories(pack(commands, values), base_s, int(n_shots))
+                out.append(self._counts_result(n_qubits, n_shots, idx, regs, width))
+                continue
             reg = self._prepared(commands, n_qubits, None, "run", values)
             out.append(self._sample_result(reg, commands, n_qubits, n_shots, base_s))
         return out
