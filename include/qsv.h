@@ -241,12 +241,24 @@ QSV_API int qsv_exact_probs(void* h, double threshold, uint64_t* keys, double* p
  * unitary prefix (commands before the first Reset, recorded Measure, conditioned command or
  * BranchBegin) runs once on the handle's register, which keeps that state on return; the rest
  * runs per shot, batched on the device.  Shot s draws from std::mt19937(seed + s) with
- * uniform_real_distribution<double>(0, 1): one draw per Measure / Reset it executes, then one
- * for its final sample (threshold = u * total, first index whose running sum reaches it).
+ * uniform_real_distribution<double>(0, 1): one draw per Measure / Reset it executes, the noise
+ * channels' draws (qsv_set_noise), then one for its final sample (threshold = u * total, first
+ * index whose running sum reaches it).
  * out_idx[s] = shot s's sampled basis index; out_cbits[s] = its classical register as a bit
  * mask (bit c = cbit c); *n_cbits = the register width (cbit_register_width,
  * command.cpp:259-271; at most 64).  This entry always takes the trajectory path: the caller
  * picks run()'s sample-once path for streams whose measurements are terminal. */
+/* Noise channels of qsv_run_trajectories, one per gate type g < n_gate_types (a
+ * qarpx::NoiseModel built from its named channels, noise_model.h:18-142): kind[g] 0 none,
+ * 1 Pauli (p_x, p_y, p_z), 2 two-qubit Pauli (15 weights, index (p0 | p1 << 2) - 1 with
+ * I, X, Y, Z = 0..3), 3 one-qubit Kraus (8 doubles per operator: K00, K01, K10, K11 as re, im),
+ * 4 depolarizing over the command's k qubits (p_total); its parameters are
+ * params[offset[g] .. offset[g + 1]).  After every command a shot executes, the channel of the
+ * command's gate type draws (apply_post_gate_noise, qarp_simulator.cpp:699-725), and the stream
+ * runs per shot from its first command, as the reference's noisy path does.  n_gate_types = 0
+ * (or no channel) switches noise off.  Only qsv_run_trajectories reads it. */
+QSV_API int qsv_set_noise(void* h, int n_gate_types, const int32_t* kind, const int32_t* offset,
+                          const double* params);
 /* Shots per device batch of qsv_run_trajectories (rounded down to a power of two; 0, the
  * default: as many as half the free device memory holds, at most 2^20).  Results do not depend
  * on it. */

@@ -7,6 +7,8 @@ loudly when it is missing: there is no CPU fallback.
 """
 from .errors import CapabilityError, CudaError
 from .ir import Command, GateType, Param, custom, gate, pack
+from .noise import (NoiseModel, make_amplitude_damping, make_bit_flip, make_depolarizing,
+                    make_pauli)
 from .observable import PauliMasks, from_strings, to_masks
 from .program import Program
 from .simulator import B200Simulator, Register, SamplingResult, uniforms
@@ -16,4 +18,5 @@ __all__ = [
     "Command", "GateType", "Param", "custom", "gate", "pack",
     "PauliMasks", "from_strings", "to_masks", "Program",
     "CapabilityError", "CudaError",
+    "NoiseModel", "make_depolarizing", "make_pauli", "make_bit_flip", "make_amplitude_damping",
 ]

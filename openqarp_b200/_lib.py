@@ -60,6 +60,7 @@ def _load():
         "qsv_uniforms": (c_int, [c_uint32, c_size_t, PD]),
         "qsv_sample_parities": (c_int, [c_void_p, c_uint32, c_size_t, PU64, c_size_t, PU64]),
         "qsv_exact_probs": (c_int, [c_void_p, c_double, PU64, PD, c_uint64, PU64]),
+        "qsv_set_noise": (c_int, [c_void_p, c_int, PI32, PI32, PD]),
         "qsv_set_trajectory_batch": (c_int, [c_void_p, c_uint64]),
         "qsv_run_trajectories": (c_int, [c_void_p, P8, c_size_t, c_uint32, c_size_t, PU64, PU64, PI32]),
         "qsv_adjoint": (c_int, [c_void_p, P8, c_size_t, PI32, PI32, PD, c_int, PU64, PU64, PD,
@@ -89,7 +90,7 @@ DECLARED = (
     "qsv_last_error", "qsv_abi_version", "qsv_create", "qsv_destroy", "qsv_set_fusion",
     "qsv_set_executor", "qsv_set_tile_qubits", "qsv_set_checkpoint_interval", "qsv_reset", "qsv_set_state", "qsv_get_state", "qsv_device_state",
     "qsv_copy_state", "qsv_fuse_count", "qsv_tile_plan_count", "qsv_apply", "qsv_apply_unfused", "qsv_transition", "qsv_sample",
-    "qsv_sample_seeded", "qsv_uniforms", "qsv_sample_parities", "qsv_exact_probs", "qsv_set_trajectory_batch", "qsv_run_trajectories", "qsv_adjoint", "qsv_adjoint_phi", "qsv_norm2",
+    "qsv_sample_seeded", "qsv_uniforms", "qsv_sample_parities", "qsv_exact_probs", "qsv_set_noise", "qsv_set_trajectory_batch", "qsv_run_trajectories", "qsv_adjoint", "qsv_adjoint_phi", "qsv_norm2",
     "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_transition_static",
     "qsv_qaoa_create", "qsv_qaoa_run", "qsv_qaoa_destroy",
 )

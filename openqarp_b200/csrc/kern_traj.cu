@@ -11,10 +11,17 @@
 // the position in the shot's uniform stream and the outcome of the current measurement.
 //
 // Randomness.  Shot s draws from std::mt19937(seed + s) through
-// std::uniform_real_distribution<double>(0, 1), one draw per Measure / Reset it executes and one
-// for its final sample — the reference's consumption order.  The host fills each shot's stream
-// (as many uniforms as the suffix has Measure / Reset commands, plus one) before the batch runs;
-// the device keeps a per-shot read position.
+// std::uniform_real_distribution<double>(0, 1): one draw per Measure / Reset it executes, one per
+// noise channel that fires a choice, and one for its final sample — the reference's consumption
+// order.  Every shot's engine lives on the device (traj_rng.cuh) and is advanced by the kernel
+// that needs the draw, so shots that skip a command skip its draws.
+//
+// Noise (apply_post_gate_noise, qarp_simulator.cpp:699-725; channels noise_model.cpp:60-190):
+// after every command a shot executes, the channel attached to its gate type draws.  Pauli
+// channels choose a Pauli string per shot from the draw alone; the shots where one fired are
+// listed on the device and only their amplitudes move.  A one-qubit Kraus channel needs the
+// shot's reduced density matrix on its qubit: per-chunk sums, then per shot the firing
+// probabilities tr(K rho K^dag), the draw, and the chosen operator scaled by 1/sqrt(p).
 //
 // Guarded gates (a classical condition, or inside a branch) run as masked dense blocks of at
 // most four qubits: a per-shot pass flag is computed first, and the block kernel skips the
@@ -24,10 +31,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <random>
-#include <thread>
 
 #include "kernels.h"
+#include "traj_rng.cuh"
 
 namespace qsv {
 
@@ -36,6 +42,7 @@ namespace {
 constexpr int kTrThreads = 256;
 constexpr int kTrChunkLog = 12;            // amplitudes per partial sum: 4096
 constexpr int kTrMaskedMaxQubits = 4;      // widest masked dense block
+constexpr int kMaxKrausOps = 8;
 
 struct TrDenseArgs {
     uint64_t off[16];   // index offset of local basis state l (local bit b <-> qubit q[b])
@@ -156,31 +163,258 @@ __global__ void k_tr_shot_sums(const double* __restrict__ chunk_sums, uint64_t n
     sum[s] = t;
 }
 
+// The shot-minor MT19937 states of a batch: word i of shot s at w[i * stride + s].
+struct MtState {
+    uint32_t* w;
+    uint32_t* idx;
+    uint64_t stride;
+    __device__ __forceinline__ MtView of(int s) const { return MtView{w + s, stride, idx + s}; }
+};
+
+// every shot's engine: std::mt19937(seed + first_shot + s)
+__global__ void k_tr_seed(MtState mt, int n_shots, uint32_t seed) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_shots) return;
+    mt.of(s).seed(seed + static_cast<uint32_t>(s));
+}
+
 // Measure / Reset decision per shot (qarp_simulator.cpp:636-690): r = the shot's next uniform,
 // outcome 1 when r >= p0; renormalisation factor sqrt(1 / p) with p = max(p_outcome, 0)
 // (csim normalize, update_ops_named_state.cpp:21-35); Measure records the outcome in its cbit.
-__global__ void k_tr_decide(const uint8_t* __restrict__ pass, const double* __restrict__ p0,
-                            const double* __restrict__ u, int u_stride, uint32_t* __restrict__ upos,
+__global__ void k_tr_decide(const uint8_t* __restrict__ pass, const double* __restrict__ p0, MtState mt,
                             uint64_t* __restrict__ cbits, int n_shots, int cbit, int8_t* __restrict__ outcome,
-                            double* __restrict__ scale, uint32_t* __restrict__ overrun) {
+                            double* __restrict__ scale) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots) return;
     if (!pass[s]) {
         outcome[s] = -1;
         return;
     }
-    const uint32_t k = upos[s]++;
-    if (k >= static_cast<uint32_t>(u_stride)) {   // the host sizes every stream for the worst path
-        atomicAdd(overrun, 1u);
-        outcome[s] = -1;
-        return;
-    }
-    const double r = u[static_cast<uint64_t>(s) * u_stride + k];
+    const double r = mt.of(s).canonical();
     const bool one = r >= p0[s];
     const double p = one ? fmax(1.0 - p0[s], 0.0) : fmax(p0[s], 0.0);
     outcome[s] = one ? 1 : 0;
     scale[s] = sqrt(1.0 / p);
     if (cbit >= 0) cbits[s] = one ? (cbits[s] | (1ull << cbit)) : (cbits[s] & ~(1ull << cbit));
+}
+
+// ---------------------------------------------------------------- noise channels
+
+enum NoiseKind : int { NOISE_NONE = 0, NOISE_PAULI = 1, NOISE_PAULI2 = 2, NOISE_KRAUS = 3, NOISE_PAULIK = 4 };
+
+struct TrQubits {
+    uint8_t q[32];
+    int k;
+};
+
+__device__ __forceinline__ void add_pauli(int axis, int q, uint64_t& x, uint64_t& z, uint32_t& ny) {
+    const uint64_t bit = 1ull << q;
+    if (axis == 1) x |= bit;
+    else if (axis == 2) { x |= bit; z |= bit; ++ny; }
+    else if (axis == 3) z |= bit;
+}
+
+// Pauli channels (apply_pauli_channel_1q / _2q / _kq, noise_model.cpp:60-124): each passing shot
+// draws, the cumulative weights pick a Pauli string, and the shots where a non-identity string
+// fired are appended to `active` with their X mask, Z mask and Y count.
+__global__ void k_tr_noise_pauli(const uint8_t* __restrict__ pass, MtState mt, int n_shots, int kind,
+                                 const double* __restrict__ prm, const __grid_constant__ TrQubits tq,
+                                 uint64_t* __restrict__ ax, uint64_t* __restrict__ az, uint32_t* __restrict__ any,
+                                 uint32_t* __restrict__ active, uint32_t* __restrict__ n_active) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_shots || !pass[s]) return;
+    const MtView g = mt.of(s);
+    uint64_t x = 0, z = 0;
+    uint32_t ny = 0;
+    if (kind == NOISE_PAULI) {
+        const double r = g.canonical();
+        double acc = prm[0];
+        if (r < acc) add_pauli(1, tq.q[0], x, z, ny);
+        else if (r < (acc += prm[1])) add_pauli(2, tq.q[0], x, z, ny);
+        else if (r < (acc += prm[2])) add_pauli(3, tq.q[0], x, z, ny);
+    } else if (kind == NOISE_PAULI2) {
+        const double r = g.canonical();
+        double acc = 0.0;
+        for (int id = 0; id < 15; ++id) {
+            acc += prm[id];
+            if (r < acc) {
+                const int packed = id + 1;
+                add_pauli(packed & 3, tq.q[0], x, z, ny);
+                add_pauli((packed >> 2) & 3, tq.q[1], x, z, ny);
+                break;
+            }
+        }
+    } else {   // NOISE_PAULIK: k in [1, 31] (the host drops the others, which draw nothing)
+        if (g.canonical() < prm[0]) {
+            const uint64_t code = g.uniform(1, (1ull << (2 * tq.k)) - 1);
+            for (int i = 0; i < tq.k; ++i) add_pauli(static_cast<int>((code >> (2 * i)) & 3u), tq.q[i], x, z, ny);
+        }
+    }
+    if (x | z) {
+        ax[s] = x;
+        az[s] = z;
+        any[s] = ny;
+        active[atomicAdd(n_active, 1u)] = static_cast<uint32_t>(s);
+    }
+}
+
+// c * a for c = i^ny * (-1)^neg; exact
+template <typename T>
+__device__ __forceinline__ vec2_t<T> pauli_phase(vec2_t<T> a, uint32_t ny, bool neg) {
+    vec2_t<T> r;
+    switch (ny & 3u) {
+        case 0: r = a; break;
+        case 1: r = mk<T>(-a.y, a.x); break;
+        case 2: r = mk<T>(-a.x, -a.y); break;
+        default: r = mk<T>(a.y, -a.x); break;
+    }
+    if (neg) r = mk<T>(-r.x, -r.y);
+    return r;
+}
+
+// P = i^nY X^x Z^z on every listed shot: |j> -> i^nY (-1)^popcount(j & z) |j ^ x>.  Work items are
+// (listed shot, pair) with a grid-stride loop, so the cost follows the number of shots hit.
+template <typename T>
+__global__ void __launch_bounds__(kTrThreads) k_tr_apply_pauli(vec2_t<T>* __restrict__ s, int n,
+                                                              const uint64_t* __restrict__ ax,
+                                                              const uint64_t* __restrict__ az,
+                                                              const uint32_t* __restrict__ any,
+                                                              const uint32_t* __restrict__ active,
+                                                              const uint32_t* __restrict__ n_active) {
+    const uint64_t half = 1ull << (n - 1);
+    const uint64_t total = static_cast<uint64_t>(*n_active) * half;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t shot = active[t / half];
+        const uint64_t g = t % half;
+        const uint64_t x = ax[shot], z = az[shot];
+        const uint32_t ny = any[shot];
+        vec2_t<T>* p = s + (static_cast<uint64_t>(shot) << n);
+        if (x == 0) {
+            for (uint64_t j = 2 * g; j < 2 * g + 2; ++j) p[j] = pauli_phase<T>(p[j], ny, __popcll(j & z) & 1);
+        } else {
+            const int hb = 63 - __clzll(x);
+            const uint64_t j = ((g >> hb) << (hb + 1)) | (g & ((1ull << hb) - 1ull));
+            const uint64_t j2 = j ^ x;
+            const vec2_t<T> a = p[j], b = p[j2];
+            p[j2] = pauli_phase<T>(a, ny, __popcll(j & z) & 1);
+            p[j] = pauli_phase<T>(b, ny, __popcll(j2 & z) & 1);
+        }
+    }
+}
+
+// Reduced density matrix of qubit q per (shot, chunk of 4096 pairs): r00, r11, Re r01, Im r01
+// with r01 = sum a0 conj(a1) (reduce_density_matrix_1q, noise_model.cpp:38-58).
+template <typename T>
+__global__ void __launch_bounds__(kTrThreads) k_tr_rho_chunks(const vec2_t<T>* __restrict__ s, int n, int q,
+                                                             double* __restrict__ out) {
+    __shared__ double red[kTrThreads / 32];
+    const int clog = min(n - 1, kTrChunkLog);
+    const uint64_t pairs = 1ull << clog;
+    const uint64_t per_shot = 1ull << (n - 1 - clog);
+    const uint64_t shot = blockIdx.x / per_shot, c = blockIdx.x % per_shot;
+    const vec2_t<T>* p = s + (shot << n);
+    const uint64_t qb = 1ull << q;
+    double r00 = 0.0, r11 = 0.0, rr = 0.0, ri = 0.0;
+    for (uint64_t i = threadIdx.x; i < pairs; i += blockDim.x) {
+        const uint64_t g = c * pairs + i;
+        const uint64_t i0 = ((g >> q) << (q + 1)) | (g & (qb - 1));
+        const vec2_t<T> a = p[i0], b = p[i0 | qb];
+        const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
+        r00 += ar * ar + ai * ai;
+        r11 += br * br + bi * bi;
+        rr += ar * br + ai * bi;
+        ri += ai * br - ar * bi;
+    }
+    double v[4] = {r00, r11, rr, ri};
+    for (int k = 0; k < 4; ++k) {
+        const double t = block_sum(v[k], red);
+        if (threadIdx.x == 0) out[blockIdx.x * 4ull + k] = t;
+        __syncthreads();
+    }
+}
+
+struct c2 {
+    double re, im;
+};
+__device__ __forceinline__ c2 cmul2(c2 a, c2 b) {
+    return c2{__dsub_rn(__dmul_rn(a.re, b.re), __dmul_rn(a.im, b.im)), __dadd_rn(__dmul_rn(a.re, b.im), __dmul_rn(a.im, b.re))};
+}
+__device__ __forceinline__ c2 cadd2(c2 a, c2 b) { return c2{__dadd_rn(a.re, b.re), __dadd_rn(a.im, b.im)}; }
+__device__ __forceinline__ c2 conj2(c2 a) { return c2{a.re, -a.im}; }
+
+// One-qubit Kraus channel choice (apply_kraus_channel_1q, noise_model.cpp:127-170): firing
+// probabilities p_i = max(0, Re tr(K_i rho K_i^dag)), normalised by their total (no draw when the
+// total is not positive), the draw, and the chosen operator scaled by 1/sqrt(p_i) into kmat.
+__global__ void k_tr_kraus_decide(const uint8_t* __restrict__ pass, const double* __restrict__ rho_chunks,
+                                  uint64_t per_shot, MtState mt, int n_shots, const double* __restrict__ kops,
+                                  int n_ops, int8_t* __restrict__ act, double* __restrict__ kmat) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_shots) return;
+    act[s] = 0;
+    if (!pass[s]) return;
+    double r00 = 0.0, r11 = 0.0, rr = 0.0, ri = 0.0;
+    for (uint64_t c = 0; c < per_shot; ++c) {
+        const double* v = rho_chunks + (static_cast<uint64_t>(s) * per_shot + c) * 4;
+        r00 += v[0];
+        r11 += v[1];
+        rr += v[2];
+        ri += v[3];
+    }
+    const c2 rho[2][2] = {{c2{r00, 0.0}, c2{rr, ri}}, {c2{rr, -ri}, c2{r11, 0.0}}};
+    double probs[8];
+    double total = 0.0;
+    for (int o = 0; o < n_ops; ++o) {
+        const double* k = kops + 8 * o;
+        const c2 K[2][2] = {{c2{k[0], k[1]}, c2{k[2], k[3]}}, {c2{k[4], k[5]}, c2{k[6], k[7]}}};
+        c2 tr{0.0, 0.0};
+        for (int i = 0; i < 2; ++i) {
+            c2 KR[2];
+            for (int j = 0; j < 2; ++j) KR[j] = cadd2(cmul2(K[i][0], rho[0][j]), cmul2(K[i][1], rho[1][j]));
+            tr = cadd2(tr, cadd2(cmul2(KR[0], conj2(K[i][0])), cmul2(KR[1], conj2(K[i][1]))));
+        }
+        probs[o] = fmax(0.0, tr.re);
+        total += probs[o];
+    }
+    if (total <= 0.0) return;
+    for (int o = 0; o < n_ops; ++o) probs[o] /= total;
+    const double r = mt.of(s).canonical();
+    double acc = 0.0;
+    for (int o = 0; o < n_ops; ++o) {
+        acc += probs[o];
+        if (r < acc) {
+            const double p_unnorm = probs[o] * total;
+            if (p_unnorm <= 0.0) return;
+            const double sc = 1.0 / sqrt(p_unnorm);
+            for (int e = 0; e < 8; ++e) kmat[8ull * s + e] = kops[8 * o + e] * sc;
+            act[s] = 1;
+            return;
+        }
+    }
+}
+
+// the chosen 2x2 operator on qubit q of every shot with act set
+template <typename T>
+__global__ void __launch_bounds__(kTrThreads) k_tr_apply_2x2(vec2_t<T>* __restrict__ s, int n, int n_shots, int q,
+                                                            const int8_t* __restrict__ act,
+                                                            const double* __restrict__ kmat) {
+    const uint64_t pairs = 1ull << (n - 1);
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= pairs * static_cast<uint64_t>(n_shots)) return;
+    const uint64_t shot = t / pairs, g = t % pairs;
+    if (!act[shot]) return;
+    const double* m = kmat + 8 * shot;
+    const uint64_t qb = 1ull << q;
+    const uint64_t i0 = ((g >> q) << (q + 1)) | (g & (qb - 1));
+    vec2_t<T>* p = s + (shot << n);
+    const vec2_t<T> a = p[i0], b = p[i0 | qb];
+    const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
+    const double y0r = (m[0] * ar - m[1] * ai) + (m[2] * br - m[3] * bi);
+    const double y0i = (m[0] * ai + m[1] * ar) + (m[2] * bi + m[3] * br);
+    const double y1r = (m[4] * ar - m[5] * ai) + (m[6] * br - m[7] * bi);
+    const double y1i = (m[4] * ai + m[5] * ar) + (m[6] * bi + m[7] * br);
+    p[i0] = mk<T>(static_cast<T>(y0r), static_cast<T>(y0i));
+    p[i0 | qb] = mk<T>(static_cast<T>(y1r), static_cast<T>(y1i));
 }
 
 // Projection and renormalisation on the pairs (i, i | 2^q) of every deciding shot; Reset moves
@@ -215,21 +449,15 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_collapse(vec2_t<T>* __restric
 // Final sample, step 1 (one thread per shot; run()'s CDF walk, qarp_simulator.cpp:1160-1172):
 // total = the shot's sum, threshold = u * total, and the chunk where the running chunk sum first
 // reaches the threshold (the last chunk when rounding never reaches it).
-__global__ void k_tr_pick_chunk(const double* __restrict__ chunk_sums, uint64_t n_chunks, int n_shots,
-                                const double* __restrict__ u, int u_stride, const uint32_t* __restrict__ upos,
+__global__ void k_tr_pick_chunk(const double* __restrict__ chunk_sums, uint64_t n_chunks, int n_shots, MtState mt,
                                 double* __restrict__ threshold, double* __restrict__ before,
-                                uint64_t* __restrict__ chunk_of, uint32_t* __restrict__ overrun) {
+                                uint64_t* __restrict__ chunk_of) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots) return;
     const double* cs = chunk_sums + static_cast<uint64_t>(s) * n_chunks;
     double total = 0.0;
     for (uint64_t c = 0; c < n_chunks; ++c) total += cs[c];
-    uint32_t k = upos[s];
-    if (k >= static_cast<uint32_t>(u_stride)) {
-        atomicAdd(overrun, 1u);
-        k = static_cast<uint32_t>(u_stride) - 1u;
-    }
-    const double thr = u[static_cast<uint64_t>(s) * u_stride + k] * total;
+    const double thr = mt.of(s).canonical() * total;
     double acc = 0.0;
     uint64_t c = 0;
     for (; c + 1 < n_chunks; ++c) {
@@ -325,7 +553,7 @@ struct TrGuard {
 };
 
 struct TrStep {
-    enum Kind { OPS, MDENSE, MSCALE, MOPS, MEASURE, BRANCH } kind = OPS;
+    enum Kind { OPS, MDENSE, MSCALE, MOPS, MEASURE, BRANCH, NOISE } kind = OPS;
     TrGuard g;
     std::vector<Op> ops;          // OPS: every shot; MOPS: every shot, failing shots restored
     int k = 0;                    // MDENSE width
@@ -336,13 +564,18 @@ struct TrStep {
     bool reset = false;           // MEASURE: Reset
     int flag = 0;                 // BRANCH: flag bit (= nesting depth)
     uint64_t bmask = 0, bwant = 0;   // BRANCH condition
+    int noise = NOISE_NONE;       // NOISE: channel kind, its parameters at poff in the table,
+    size_t poff = 0;              //        its qubits (the command's, in order)
+    int n_ops = 0;                //        Kraus operators
+    TrQubits nq{};
 };
 
 struct TrPlan {
     std::vector<TrStep> steps;
     std::vector<cplx<double>> mats;   // MDENSE matrices, row-major
-    int n_draws = 1;                  // uniforms a shot may consume (Measure / Reset + final)
+    std::vector<double> noise_prm;    // NOISE parameters
     bool needs_backup = false;
+    bool kraus = false;
 };
 
 // (mask, want) of an AND of cbit conditions; unsatisfiable when a bit is asked for both values
@@ -365,8 +598,17 @@ void condition_of(const Cmd& c, int n_cbits, uint64_t* mask, uint64_t* want, boo
     }
 }
 
-TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion_max, int fusion_min) {
+// Gates after which the reference injects no error (apply_post_gate_noise's exclusions,
+// qarp_simulator.cpp:707-717), and codes outside the gate table (engine records).
+bool noise_exempt(int g) {
+    return g == MEASURE || g == RESET || g == BARRIER || g == GPHASE || g == BRANCH_BEGIN || g == BRANCH_ELSE ||
+           g == BRANCH_END || g < 0 || g >= GATE_COUNT;
+}
+
+TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion_max, int fusion_min,
+                  const std::vector<NoiseSpec>* noise) {
     TrPlan plan;
+    const bool noisy = noise && !noise->empty();
     // branch structure first, with the reference's messages (build_branch_table,
     // qarp_simulator.cpp:298-337)
     {
@@ -495,7 +737,6 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
             if (static_cast<int>(c.q[0]) >= n)
                 throw std::invalid_argument("trajectory: measured qubit " + std::to_string(c.q[0]) +
                                             " outside a " + std::to_string(n) + "-qubit register");
-            plan.n_draws++;
             if (guard.never) continue;
             TrStep st;
             st.kind = TrStep::MEASURE;
@@ -518,35 +759,38 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
         if (!seg.empty() && !(guard == seg_guard)) flush();
         seg_guard = guard;
         seg.push_back(std::move(gate));
+        // the channel attached to the gate type runs after the gate, on the shots that applied it
+        if (!noisy || noise_exempt(g) || static_cast<size_t>(g) >= noise->size()) continue;
+        const NoiseSpec& ch = (*noise)[static_cast<size_t>(g)];
+        if (ch.kind == NOISE_NONE) continue;
+        flush();
+        if (guard.never) continue;
+        const int k = static_cast<int>(c.q.size());
+        TrStep st;
+        st.kind = TrStep::NOISE;
+        st.g = guard;
+        st.noise = ch.kind;
+        st.nq.k = k;
+        for (int b = 0; b < k && b < 32; ++b) st.nq.q[b] = static_cast<uint8_t>(c.q[b]);
+        if (ch.kind == NOISE_PAULI && k != 1)
+            throw std::runtime_error("apply_channel: PauliChannel requires exactly 1 target qubit");
+        if (ch.kind == NOISE_PAULI2 && k != 2)
+            throw std::runtime_error("apply_channel: PauliChannel2q requires exactly 2 target qubits");
+        if (ch.kind == NOISE_KRAUS && k != 1)
+            throw std::runtime_error("apply_channel: KrausChannel requires exactly 1 target qubit");
+        if (ch.kind == NOISE_PAULIK && (k == 0 || k > 31)) continue;   // the reference draws nothing
+        if (ch.kind == NOISE_KRAUS) {
+            st.n_ops = static_cast<int>(ch.p.size() / 8);
+            if (st.n_ops == 0) continue;                               // no operators: no draw
+            if (st.n_ops > kMaxKrausOps) throw capability_error("Kraus channel with more than 8 operators");
+            plan.kraus = true;
+        }
+        st.poff = plan.noise_prm.size();
+        plan.noise_prm.insert(plan.noise_prm.end(), ch.p.begin(), ch.p.end());
+        plan.steps.push_back(std::move(st));
     }
     flush();
     return plan;
-}
-
-// Shot s's uniform stream: std::mt19937(seed + s) through uniform_real_distribution(0, 1),
-// u[(s - s0) * stride + k] = its k-th draw.  Threads split the shots; every thread count gives
-// the same streams.
-void fill_uniforms(uint32_t seed, size_t s0, size_t nb, int stride, double* u) {
-    auto work = [=](size_t lo, size_t hi) {
-        std::uniform_real_distribution<double> u01(0.0, 1.0);
-        for (size_t s = lo; s < hi; ++s) {
-            std::mt19937 rng(seed + static_cast<uint32_t>(s0 + s));
-            for (int k = 0; k < stride; ++k) u[s * stride + k] = u01(rng);
-        }
-    };
-    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t n_thr = std::min<size_t>(std::min<size_t>(hw, 32), std::max<size_t>(1, nb / 64));
-    if (n_thr <= 1) {
-        work(0, nb);
-        return;
-    }
-    std::vector<std::thread> pool;
-    const size_t per = (nb + n_thr - 1) / n_thr;
-    for (size_t t = 0; t < n_thr; ++t) {
-        const size_t lo = t * per, hi = std::min(nb, lo + per);
-        if (lo < hi) pool.emplace_back(work, lo, hi);
-    }
-    for (auto& th : pool) th.join();
 }
 
 struct DeviceBuffer {
@@ -594,31 +838,32 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
                       size_t n_shots, const TrajOptions& opt, uint64_t* out_idx, uint64_t* out_cbits,
                       cudaStream_t st, Workspace& ws, uint64_t* launches) {
     if (n_cbits > 64) throw capability_error("trajectory: more than 64 classical bits");
-    const TrPlan plan = build_plan(suffix, n, n_cbits, opt.fusion_max, opt.fusion_min);
+    const TrPlan plan = build_plan(suffix, n, n_cbits, opt.fusion_max, opt.fusion_min, opt.noise);
     if (n_shots == 0) return;
     if (!out_idx || !out_cbits) throw std::invalid_argument("null output");
     uint64_t n_launch = 0;
 
-    // batch size: a power of two, bounded by the shots and by the device memory budget
-    const size_t state_bytes = sizeof(vec2_t<T>) << n;
-    size_t free_b = 0, total_b = 0;
-    check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-    size_t budget = free_b / 2;
-    if (plan.needs_backup) budget /= 2;
-    if (state_bytes > budget) throw std::bad_alloc();
-    const uint64_t cap = opt.max_batch_shots ? std::min<uint64_t>(opt.max_batch_shots, 1ull << 20) : 1ull << 20;
-    uint64_t B = 1;
-    while (B < n_shots && 2 * B <= cap && (2 * B) * state_bytes <= budget) B *= 2;
-
     const int clog = std::min(n, kTrChunkLog);
     const uint64_t n_chunks = 1ull << (n - clog);
-    const int stride = plan.n_draws;
+    const uint64_t n_pchunks = n >= 1 ? 1ull << (n - 1 - std::min(n - 1, kTrChunkLog)) : 1;
 
-    // device: the batch register, the backup (wide-command fallback), per-shot arrays
+    // batch size: a power of two, bounded by the shots and by the device memory budget
+    const size_t state_bytes = sizeof(vec2_t<T>) << n;
+    const size_t per_shot_bytes = 8 * 18 + 4 * (kMtN + 3) + 2 + 8 * n_chunks + (plan.kraus ? 32 * n_pchunks : 0);
+    size_t free_b = 0, total_b = 0;
+    check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const size_t budget = free_b / 2;
+    const size_t shot_cost = state_bytes * (plan.needs_backup ? 2 : 1) + per_shot_bytes;
+    if (shot_cost > budget) throw std::bad_alloc();
+    const uint64_t cap = opt.max_batch_shots ? std::min<uint64_t>(opt.max_batch_shots, 1ull << 20) : 1ull << 20;
+    uint64_t B = 1;
+    while (B < n_shots && 2 * B <= cap && (2 * B) * shot_cost <= budget) B *= 2;
+
+    // device: the batch register, the backup (wide guarded commands), per-shot arrays
     DeviceBuffer batch(B * state_bytes);
     DeviceBuffer backup(plan.needs_backup ? B * state_bytes : 0);
-    const size_t per_shot_bytes = 8 * 8 + 4 + 1 + 1 + 8 * static_cast<size_t>(stride) + 8 * n_chunks;
-    DeviceBuffer side(B * per_shot_bytes + 16 * 16 + plan.mats.size() * sizeof(cplx<double>));
+    const size_t tables = plan.mats.size() * sizeof(cplx<double>) + plan.noise_prm.size() * sizeof(double);
+    DeviceBuffer side(B * per_shot_bytes + 32 * 16 + tables);
     uint8_t* sp = static_cast<uint8_t*>(side.p);
     auto carve = [&](size_t bytes) {
         uint8_t* r = sp;
@@ -633,37 +878,49 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
     double* d_before = reinterpret_cast<double*>(carve(8 * B));
     uint64_t* d_chunk_of = reinterpret_cast<uint64_t*>(carve(8 * B));
     uint64_t* d_out = reinterpret_cast<uint64_t*>(carve(8 * B));
-    double* d_u = reinterpret_cast<double*>(carve(8 * B * stride));
+    uint64_t* d_ax = reinterpret_cast<uint64_t*>(carve(8 * B));
+    uint64_t* d_az = reinterpret_cast<uint64_t*>(carve(8 * B));
+    double* d_kmat = reinterpret_cast<double*>(carve(8 * 8 * B));
     double* d_chunks = reinterpret_cast<double*>(carve(8 * B * n_chunks));
-    uint32_t* d_upos = reinterpret_cast<uint32_t*>(carve(4 * B));
-    uint32_t* d_overrun = reinterpret_cast<uint32_t*>(carve(4));
+    double* d_rho = plan.kraus ? reinterpret_cast<double*>(carve(32 * B * n_pchunks)) : nullptr;
+    uint32_t* d_mt = reinterpret_cast<uint32_t*>(carve(4ull * kMtN * B));
+    uint32_t* d_mtidx = reinterpret_cast<uint32_t*>(carve(4 * B));
+    uint32_t* d_any = reinterpret_cast<uint32_t*>(carve(4 * B));
+    uint32_t* d_active = reinterpret_cast<uint32_t*>(carve(4 * B));
+    uint32_t* d_nactive = reinterpret_cast<uint32_t*>(carve(4));
     uint8_t* d_pass = carve(B);
     int8_t* d_outcome = reinterpret_cast<int8_t*>(carve(B));
     cplx<double>* d_mats = reinterpret_cast<cplx<double>*>(carve(plan.mats.size() * sizeof(cplx<double>)));
+    double* d_nprm = reinterpret_cast<double*>(carve(plan.noise_prm.size() * sizeof(double)));
+    if (sp > static_cast<uint8_t*>(side.p) + B * per_shot_bytes + 32 * 16 + tables)
+        throw std::logic_error("trajectory side buffer overrun");
     if (!plan.mats.empty())
         check_cuda(cudaMemcpyAsync(d_mats, plan.mats.data(), plan.mats.size() * sizeof(cplx<double>),
                                    cudaMemcpyHostToDevice, st), "trajectory matrices");
-    check_cuda(cudaMemsetAsync(d_overrun, 0, 4, st), "memset");
+    if (!plan.noise_prm.empty())
+        check_cuda(cudaMemcpyAsync(d_nprm, plan.noise_prm.data(), plan.noise_prm.size() * sizeof(double),
+                                   cudaMemcpyHostToDevice, st), "noise parameters");
+    const MtState mt{d_mt, d_mtidx, B};
 
-    PinnedBuffer h_u(8 * B * stride);
     PinnedBuffer h_res(16 * B);
-    double* hu = static_cast<double*>(h_u.p);
     uint64_t* hres = static_cast<uint64_t*>(h_res.p);
     vec2_t<T>* s = static_cast<vec2_t<T>*>(batch.p);
+    int sms = 148;
+    {
+        int dev = 0;
+        check_cuda(cudaGetDevice(&dev), "device");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+    }
 
     for (size_t s0 = 0; s0 < n_shots; s0 += B) {
         const int nb = static_cast<int>(std::min<uint64_t>(B, n_shots - s0));
         const int nw = n + log2_ceil(static_cast<uint64_t>(nb));   // the wide register
         const uint64_t wide = 1ull << nw;
-        // the previous batch ended with a stream synchronisation, so the pinned uniform buffer
-        // is free to refill
-        fill_uniforms(seed, s0, static_cast<size_t>(nb), stride, hu);
-        check_cuda(cudaMemcpyAsync(d_u, hu, 8ull * nb * stride, cudaMemcpyHostToDevice, st), "uniforms H2D");
+        k_tr_seed<<<blocks_for(nb), kTrThreads, 0, st>>>(mt, nb, seed + static_cast<uint32_t>(s0));
         k_tr_broadcast<T><<<stride_blocks(wide), kTrThreads, 0, st>>>(s, d_prefix, n, wide);
         check_cuda(cudaMemsetAsync(d_cbits, 0, 8ull * nb, st), "memset");
         check_cuda(cudaMemsetAsync(d_flags, 0, 8ull * nb, st), "memset");
-        check_cuda(cudaMemsetAsync(d_upos, 0, 4ull * nb, st), "memset");
-        n_launch++;
+        n_launch += 2;
         auto guard = [&](const TrGuard& g) {
             k_tr_guard<<<blocks_for(nb), kTrThreads, 0, st>>>(d_pass, d_cbits, d_flags, nb, g.fmask, g.fwant,
                                                               g.cmask, g.cwant);
@@ -715,8 +972,8 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
                     k_tr_chunk_sums<T><<<static_cast<unsigned>(nb * n_chunks), kTrThreads, 0, st>>>(
                         s, n, 1ull << step.qubit, d_chunks);
                     k_tr_shot_sums<<<blocks_for(nb), kTrThreads, 0, st>>>(d_chunks, n_chunks, nb, d_sum);
-                    k_tr_decide<<<blocks_for(nb), kTrThreads, 0, st>>>(d_pass, d_sum, d_u, stride, d_upos, d_cbits,
-                                                                       nb, step.cbit, d_outcome, d_scale, d_overrun);
+                    k_tr_decide<<<blocks_for(nb), kTrThreads, 0, st>>>(d_pass, d_sum, mt, d_cbits, nb, step.cbit,
+                                                                       d_outcome, d_scale);
                     k_tr_collapse<T><<<blocks_for((static_cast<uint64_t>(nb) << n) / 2), kTrThreads, 0, st>>>(
                         s, n, nb, step.qubit, step.reset ? 1 : 0, d_outcome, d_scale);
                     n_launch += 4;
@@ -727,13 +984,35 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
                                                                        step.bwant);
                     n_launch++;
                     break;
+                case TrStep::NOISE: {
+                    guard(step.g);
+                    if (step.noise == NOISE_KRAUS) {
+                        const int q = step.nq.q[0];
+                        k_tr_rho_chunks<T><<<static_cast<unsigned>(nb * n_pchunks), kTrThreads, 0, st>>>(s, n, q,
+                                                                                                      d_rho);
+                        k_tr_kraus_decide<<<blocks_for(nb), kTrThreads, 0, st>>>(
+                            d_pass, d_rho, n_pchunks, mt, nb, d_nprm + step.poff, step.n_ops, d_outcome, d_kmat);
+                        k_tr_apply_2x2<T><<<blocks_for((static_cast<uint64_t>(nb) << n) / 2), kTrThreads, 0, st>>>(
+                            s, n, nb, q, d_outcome, d_kmat);
+                        n_launch += 3;
+                    } else {
+                        check_cuda(cudaMemsetAsync(d_nactive, 0, 4, st), "memset");
+                        k_tr_noise_pauli<<<blocks_for(nb), kTrThreads, 0, st>>>(
+                            d_pass, mt, nb, step.noise, d_nprm + step.poff, step.nq, d_ax, d_az, d_any, d_active,
+                            d_nactive);
+                        k_tr_apply_pauli<T><<<static_cast<unsigned>(sms) * 8, kTrThreads, 0, st>>>(
+                            s, n, d_ax, d_az, d_any, d_active, d_nactive);
+                        n_launch += 2;
+                    }
+                    break;
+                }
             }
             check_cuda(cudaGetLastError(), "trajectory step");
         }
         // final sample of every shot
         k_tr_chunk_sums<T><<<static_cast<unsigned>(nb * n_chunks), kTrThreads, 0, st>>>(s, n, 0, d_chunks);
-        k_tr_pick_chunk<<<blocks_for(nb), kTrThreads, 0, st>>>(d_chunks, n_chunks, nb, d_u, stride, d_upos, d_thr,
-                                                               d_before, d_chunk_of, d_overrun);
+        k_tr_pick_chunk<<<blocks_for(nb), kTrThreads, 0, st>>>(d_chunks, n_chunks, nb, mt, d_thr, d_before,
+                                                               d_chunk_of);
         k_tr_pick_index<T><<<static_cast<unsigned>(nb), kTrThreads, 0, st>>>(s, n, d_thr, d_before, d_chunk_of,
                                                                              d_out);
         n_launch += 3;
@@ -744,10 +1023,6 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
         std::memcpy(out_idx + s0, hres, 8ull * nb);
         std::memcpy(out_cbits + s0, hres + B, 8ull * nb);
     }
-    uint32_t overrun = 0;
-    check_cuda(cudaMemcpyAsync(&overrun, d_overrun, 4, cudaMemcpyDeviceToHost, st), "D2H");
-    check_cuda(cudaStreamSynchronize(st), "trajectory");
-    if (overrun) throw std::runtime_error("trajectory: a shot used more uniforms than its stream holds");
     if (launches) *launches += n_launch;
 }
 

@@ -140,10 +140,19 @@ void parity_counts(const uint64_t* d_outcome, size_t n_shots, const uint64_t* d_
                    unsigned long long* d_odd, cudaStream_t st);
 
 // ---------------------------------------------------------------- trajectories (kern_traj.cu)
+// The noise channel attached to one gate type (qarpx::Channel, noise_model.h:18-60): kind 0 none,
+// 1 one-qubit Pauli (p_x, p_y, p_z), 2 two-qubit Pauli (15 weights, id = (p0 | p1 << 2) - 1),
+// 3 one-qubit Kraus (8 doubles per operator: K00, K01, K10, K11 as re, im), 4 depolarizing on
+// the command's k qubits (p_total).
+struct NoiseSpec {
+    int kind = 0;
+    std::vector<double> p;
+};
 struct TrajOptions {
     int fusion_max = 3;           // fusion of the gates every shot applies
     int fusion_min = 12;
     uint64_t max_batch_shots = 0; // shots per device batch (0: as many as half the free memory holds)
+    const std::vector<NoiseSpec>* noise = nullptr;   // per gate type; null or empty: noiseless
 };
 // Run n_shots trajectories of `suffix` from the n-qubit device state d_prefix (left unchanged):
 // out_idx[s] = shot s's final sampled index, out_cbits[s] = its classical register (bit c =

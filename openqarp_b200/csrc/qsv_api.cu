@@ -38,6 +38,7 @@ struct Handle {
     size_t aux_cap = 0;
     int checkpoint_interval = -1; // adjoint: commands between psi checkpoints (-1 auto, 0 none)
     uint64_t traj_batch = 0;      // trajectories: shots per device batch (0: memory-bound default)
+    std::vector<NoiseSpec> noise; // trajectories: channel per gate type (empty: noiseless)
     uint64_t dim() const { return 1ull << n; }
     size_t amp_bytes() const { return dtype == QSV_C128 ? 16 : 8; }
 };
@@ -348,6 +349,36 @@ int qsv_set_checkpoint_interval(void* hp, int k) {
     });
 }
 
+int qsv_set_noise(void* hp, int n_gate_types, const int32_t* kind, const int32_t* offset, const double* params) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (n_gate_types < 0 || n_gate_types > GATE_COUNT)
+            throw std::invalid_argument("qsv_set_noise: n_gate_types must be in [0, " + std::to_string(GATE_COUNT) +
+                                        "]");
+        std::vector<NoiseSpec> table;
+        bool any = false;
+        if (n_gate_types > 0) {
+            if (!kind || !offset) throw std::invalid_argument("qsv_set_noise: null channel table");
+            table.resize(GATE_COUNT);
+            for (int g = 0; g < n_gate_types; ++g) {
+                const int k = kind[g];
+                const int32_t lo = offset[g], hi = offset[g + 1];
+                if (hi < lo || lo < 0 || (hi > lo && !params))
+                    throw std::invalid_argument("qsv_set_noise: bad parameter offsets");
+                const size_t np = static_cast<size_t>(hi - lo);
+                const bool ok = (k == 0 && np == 0) || (k == 1 && np == 3) || (k == 2 && np == 15) ||
+                                (k == 3 && np % 8 == 0) || (k == 4 && np == 1);
+                if (!ok) throw std::invalid_argument("qsv_set_noise: channel kind and parameter count disagree");
+                table[g].kind = k;
+                table[g].p.assign(params + lo, params + hi);
+                any = any || k != 0;
+            }
+        }
+        if (!any) table.clear();
+        h->noise = std::move(table);
+    });
+}
+
 int qsv_set_trajectory_batch(void* hp, uint64_t max_shots) {
     return guarded([&] { H_(hp)->traj_batch = max_shots; });
 }
@@ -611,15 +642,17 @@ int qsv_run_trajectories(void* hp, const uint8_t* cmds, size_t nbytes, uint32_t 
         }
         if (n_cbits) *n_cbits = width;
         // unitary prefix once, on the handle's register (first_trajectory_index,
-        // qarp_simulator.cpp:273-278)
+        // qarp_simulator.cpp:273-278); with noise every command runs per shot
         size_t split = 0;
-        while (split < cs.size() && !needs_trajectory(cs[split])) ++split;
+        if (h->noise.empty())
+            while (split < cs.size() && !needs_trajectory(cs[split])) ++split;
         const std::vector<Cmd> prefix(cs.begin(), cs.begin() + static_cast<std::ptrdiff_t>(split));
         const std::vector<Cmd> suffix(cs.begin() + static_cast<std::ptrdiff_t>(split), cs.end());
         TrajOptions opt;
         opt.fusion_max = h->fusion_max;
         opt.fusion_min = h->fusion_min;
         opt.max_batch_shots = h->traj_batch;
+        opt.noise = &h->noise;
         if (!prefix.empty()) apply_cmds(h, prefix, true);
         if (h->dtype == QSV_C128)
             run_trajectories<double>(suffix, h->n, width, S128(h), seed, n_shots, opt, out_idx, out_cbits, h->stream,

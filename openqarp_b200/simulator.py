@@ -20,6 +20,7 @@ from ._lib import check, dptr, i32ptr, lib, u64ptr, u8ptr
 from .errors import CapabilityError
 from .ir import (PackedStream, cbit_register_width, measurements_are_terminal, needs_trajectory,
                  pack)
+from .noise import as_noise_model
 from .observable import PauliMasks, to_masks
 from .program import GatesKernel, as_program
 
@@ -178,6 +179,14 @@ class Register:
                 raise RuntimeError("exact readout count changed between passes")
         return keys.astype(np.int64), probs
 
+    def set_noise(self, model) -> None:
+        """Noise channels of run_trajectories (a noise.NoiseModel, or None for none)."""
+        if model is None:
+            check(lib.qsv_set_noise(self.handle, 0, None, None, None))
+            return
+        kind, offset, params = model.table()
+        check(lib.qsv_set_noise(self.handle, int(kind.shape[0]), i32ptr(kind), i32ptr(offset), dptr(params)))
+
     def set_trajectory_batch(self, max_shots: int):
         """Shots per device batch of run_trajectories (0: memory-bound default)."""
         check(lib.qsv_set_trajectory_batch(self.handle, int(max_shots)))
@@ -257,12 +266,19 @@ def _default_fusion_max() -> int:
     return 3
 
 
+_NOISY_STATEVECTOR = ("QarpSimulator::statevector: noise model is active — the noisy ensemble is not "
+                      "representable as a single statevector. Either disable the noise model "
+                      "(noise_model.enabled=False) or use run() for trajectory simulation.")
+
+
 class B200Simulator:
     """GPU drop-in for ``qx.QarpSimulator``.
 
     Args:
-        noise_model: accepted for signature parity; an enabled noise model needs the
-            trajectory path, which this engine does not provide (CapabilityError).
+        noise_model: a ``noise.NoiseModel`` (or the reference wrapper's duck type holding
+            one); when enabled with a channel, ``run`` samples every shot as a noisy
+            trajectory on the device and the statevector entry points refuse, as the
+            reference does.
         device: CUDA device index.
         dtype: ``"complex128"`` (default; the reference's arithmetic) or ``"complex64"``
             (bulk mode: complex64 storage, FP64 reductions).
@@ -274,12 +290,9 @@ class B200Simulator:
     kDefaultFusionMinQubits = 12
 
     def __init__(self, noise_model=None, *, device: int = 0, dtype: str = "complex128"):
-        if noise_model is not None and getattr(noise_model, "enabled", True):
-            raise CapabilityError("B200Simulator: active noise needs the per-shot trajectory path, "
-                                  "which the B200 engine does not implement")
         if dtype not in _DTYPES:
             raise ValueError(f"dtype must be one of {sorted(_DTYPES)}")
-        self._noise_model = noise_model
+        self._noise_model = None if noise_model is None else as_noise_model(noise_model)
         self.device = int(device)
         self.dtype = dtype
         self._fusion_max = _default_fusion_max()
@@ -291,6 +304,17 @@ class B200Simulator:
     @property
     def noise_model(self):
         return self._noise_model
+
+    @noise_model.setter
+    def noise_model(self, model):
+        self._noise_model = None if model is None else as_noise_model(model)
+
+    def _noise_active(self) -> bool:
+        return self._noise_model is not None and self._noise_model.active()
+
+    def _refuse_noise(self, msg: str):
+        if self._noise_active():
+            raise RuntimeError(msg)
 
     @property
     def fusion_max_qubits(self) -> int:
@@ -379,6 +403,7 @@ class B200Simulator:
                 "QarpSimulator::statevector: circuit contains mid-circuit measurement, Reset, or "
                 "classical condition — statevector is not deterministic. Use run() for trajectory "
                 "simulation.")
+        self._refuse_noise(_NOISY_STATEVECTOR)
         return self._prepared(commands, n_qubits, initial_state, "statevector").get_state()
 
     def run(self, commands, n_qubits: int, n_shots: int, seed: Optional[int] = None, *,
@@ -389,7 +414,7 @@ class B200Simulator:
         reference's draws."""
         commands = list(commands)
         base_s = int(seed) if seed is not None else int.from_bytes(os.urandom(4), "little")
-        if not measurements_are_terminal(commands):
+        if self._noise_active() or not measurements_are_terminal(commands):
             return self._trajectory_result(commands, n_qubits, n_shots, base_s, initial_state)
         reg = self._prepared(commands, n_qubits, initial_state, "run")
         return self._sample_result(reg, commands, n_qubits, n_shots, base_s)
@@ -399,6 +424,7 @@ class B200Simulator:
         device: counts of each shot's final sampled index and its classical register."""
         reg = self.register(n_qubits)
         self._seed(reg, n_qubits, initial_state, "run")
+        reg.set_noise(self._noise_model if self._noise_active() else None)
         idx, regs, width = reg.run_trajectories(pack(commands), base_s, int(n_shots))
         return self._counts_result(n_qubits, n_shots, idx, regs, width)
 
@@ -439,9 +465,10 @@ class B200Simulator:
         for i, values in enumerate(param_sets):
             s = None if seed is None else (int(seed) + i) & 0xFFFFFFFF
             base_s = s if s is not None else int.from_bytes(os.urandom(4), "little")
-            if not measurements_are_terminal(commands):
+            if self._noise_active() or not measurements_are_terminal(commands):
                 reg = self.register(n_qubits)
                 reg.reset()
+                reg.set_noise(self._noise_model if self._noise_active() else None)
                 idx, regs, width = reg.run_trajectories(pack(commands, values), base_s, int(n_shots))
                 out.append(self._counts_result(n_qubits, n_shots, idx, regs, width))
                 continue
@@ -461,6 +488,8 @@ class B200Simulator:
                     "QarpSimulator::program_statevector: program contains mid-circuit "
                     "measurement, Reset, or classical condition — statevector is not "
                     "deterministic.")
+        self._refuse_noise("QarpSimulator::program_statevector: noise model is active — the noisy "
+                           "ensemble is not representable as a single statevector.")
         return self._prepared(prog.to_stream(), n_qubits, initial_state,
                               "program_statevector").get_state()
 
@@ -469,6 +498,8 @@ class B200Simulator:
         (QarpSimulator::program_run, qarp_simulator.cpp:851-897)."""
         prog = as_program(program)
         _check_program_width(prog, n_qubits, "program_run")
+        self._refuse_noise("QarpSimulator::program_run: noise model is active — structured programs "
+                           "run the noiseless sample-once path only.")
         kernels = prog.kernels()
         last = None
         for i, k in enumerate(kernels):
@@ -511,12 +542,14 @@ class B200Simulator:
         if any(needs_trajectory(c) for c in commands):
             raise RuntimeError("QarpSimulator::statevector: circuit contains mid-circuit measurement, "
                                "Reset, or classical condition — statevector is not deterministic.")
+        self._refuse_noise(_NOISY_STATEVECTOR)
         masks = to_masks(observable, n_qubits)
         reg = self._prepared(commands, n_qubits, initial_state, "statevector")
         return reg.expectation(masks).real
 
     def batch_expectation(self, commands, n_qubits: int, observable, param_sets) -> list:
         commands = list(commands)
+        self._refuse_noise(_NOISY_STATEVECTOR)
         masks = to_masks(observable, n_qubits)
         out = []
         for values in param_sets:
@@ -571,6 +604,9 @@ class B200Simulator:
         if any(needs_trajectory(c) for c in commands):
             raise RuntimeError("QarpSimulator::unitary_matrix: circuit contains mid-circuit "
                                "measurement, Reset, or classical condition — output is not unitary.")
+        self._refuse_noise("QarpSimulator::unitary_matrix: noise model is active — noisy evolution is "
+                           "not unitary.  Disable noise (enabled=False) or use run() for stochastic "
+                           "sampling.")
         dim = 1 << n_qubits
         stream = pack(commands)
         reg = self.register(n_qubits)

@@ -167,6 +167,8 @@ class Reference:
         lib.qref_uniforms.argtypes = [c_uint32, c_size_t, PD]
         lib.qref_run_history.argtypes = [P8, c_size_t, c_int, c_int, c_uint32, c_int, c_int, PU64, PI32, c_size_t,
                                          POINTER(c_size_t), PU64, POINTER(c_int)]
+        lib.qref_run_noisy.argtypes = [P8, c_size_t, c_int, c_int, c_uint32, c_int, c_int, c_int, PI32, PD, PI32,
+                                       PI32, PU64, PI32, c_size_t, POINTER(c_size_t), PU64, POINTER(c_int)]
         lib.qref_run_gradient.argtypes = [P8, c_size_t, c_int, PI32, PI32, PD, c_int, PD, PU64, PU64, PD,
                                           c_size_t, PD, PD]
         lib.qref_program_new.restype = ctypes.c_void_p
@@ -254,6 +256,33 @@ class Reference:
         self._check(self.lib.qref_run_history(_u8(buf), len(buf), n, shots, seed & 0xFFFFFFFF, fusion_max,
                                               fusion_min, _u64(keys), _i32(cnts), cap, ctypes.byref(got),
                                               _u64(hist), ctypes.byref(ncb)))
+        return {int(keys[i]): int(cnts[i]) for i in range(got.value)}, hist[:shots], ncb.value
+
+    def run_noisy(self, buf, n, shots, seed, specs, fusion_max=-1, fusion_min=-1):
+        """run() under a noise model built by the reference's named builders: ``specs`` is a list
+        of (builder, params, gates) with builder in {"depolarizing", "pauli", "bit_flip",
+        "amplitude_damping"}, composed with + in order.  Returns (counts, histories, n_cbits)."""
+        codes = {"depolarizing": 0, "pauli": 1, "bit_flip": 2, "amplitude_damping": 3}
+        kind = np.array([codes[b] for b, _p, _g in specs], dtype=np.int32)
+        prm = np.zeros(3 * max(len(specs), 1))
+        ptr = [0]
+        gates = []
+        for i, (_b, p, g) in enumerate(specs):
+            p = list(p) if isinstance(p, (list, tuple)) else [p]
+            prm[3 * i:3 * i + len(p)] = p
+            gates += [int(x) for x in g]
+            ptr.append(len(gates))
+        ptr = np.array(ptr, dtype=np.int32)
+        gates = np.array(gates or [0], dtype=np.int32)
+        cap = max(1, min(shots, 1 << n))
+        keys = np.zeros(cap, dtype=np.uint64)
+        cnts = np.zeros(cap, dtype=np.int32)
+        hist = np.zeros(max(shots, 1), dtype=np.uint64)
+        got = c_size_t()
+        ncb = c_int()
+        self._check(self.lib.qref_run_noisy(_u8(buf), len(buf), n, shots, seed & 0xFFFFFFFF, fusion_max, fusion_min,
+                                            len(specs), _i32(kind), _d(prm), _i32(ptr), _i32(gates), _u64(keys),
+                                            _i32(cnts), cap, ctypes.byref(got), _u64(hist), ctypes.byref(ncb)))
         return {int(keys[i]): int(cnts[i]) for i in range(got.value)}, hist[:shots], ncb.value
 
     def uniforms(self, seed, shots):

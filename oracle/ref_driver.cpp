@@ -282,24 +282,56 @@ int qref_expectation(const uint8_t* cmds, size_t nbytes, int n, int fusion_max,
     }
 }
 
-int qref_run_history(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed,
-                     int fusion_max, int fusion_min, uint64_t* keys, int32_t* counts, size_t cap,
-                     size_t* n_out, uint64_t* history, int* n_cbits);
+int qref_run_noisy(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed, int fusion_max,
+                   int fusion_min, int n_specs, const int32_t* spec_kind, const double* spec_p,
+                   const int32_t* spec_gate_ptr, const int32_t* spec_gates, uint64_t* keys, int32_t* counts,
+                   size_t cap, size_t* n_out, uint64_t* history, int* n_cbits);
 
 int qref_run(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed,
              int fusion_max, int fusion_min, uint64_t* keys, int32_t* counts, size_t cap,
              size_t* n_out) {
-    return qref_run_history(cmds, nbytes, n, shots, seed, fusion_max, fusion_min, keys, counts, cap, n_out,
-                            nullptr, 0);
+    return qref_run_noisy(cmds, nbytes, n, shots, seed, fusion_max, fusion_min, 0, nullptr, nullptr, nullptr,
+                          nullptr, keys, counts, cap, n_out, nullptr, nullptr);
 }
 
-// run() with the per-shot classical register: history[s] holds shot s's cbits as a bitmask
-// (cbit c -> bit c), for registers of at most 64 cbits.
 int qref_run_history(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed,
                      int fusion_max, int fusion_min, uint64_t* keys, int32_t* counts, size_t cap,
                      size_t* n_out, uint64_t* history, int* n_cbits) {
+    return qref_run_noisy(cmds, nbytes, n, shots, seed, fusion_max, fusion_min, 0, nullptr, nullptr, nullptr,
+                          nullptr, keys, counts, cap, n_out, history, n_cbits);
+}
+
+// run() with the per-shot classical register: history[s] holds shot s's cbits as a bitmask
+// (cbit c -> bit c), for registers of at most 64 cbits.  With n_specs > 0 the simulator carries
+// the noise model made by the reference's named builders, composed with + in order: spec i is
+// kind 0 make_depolarizing(p0), 1 make_pauli(p0, p1, p2), 2 make_bit_flip(p0),
+// 3 make_amplitude_damping(p0) (three parameters per spec in spec_p) over the gates
+// spec_gates[spec_gate_ptr[i] .. spec_gate_ptr[i + 1]).
+int qref_run_noisy(const uint8_t* cmds, size_t nbytes, int n, int shots, uint32_t seed, int fusion_max,
+                   int fusion_min, int n_specs, const int32_t* spec_kind, const double* spec_p,
+                   const int32_t* spec_gate_ptr, const int32_t* spec_gates, uint64_t* keys, int32_t* counts,
+                   size_t cap, size_t* n_out, uint64_t* history, int* n_cbits) {
     try {
         auto sim = make_sim(fusion_max, fusion_min);
+        if (n_specs > 0) {
+            qarpx::NoiseModel nm;
+            for (int i = 0; i < n_specs; ++i) {
+                std::vector<qarpx::GateType> gates;
+                for (int j = spec_gate_ptr[i]; j < spec_gate_ptr[i + 1]; ++j)
+                    gates.push_back(static_cast<qarpx::GateType>(spec_gates[j]));
+                const double* p = spec_p + 3 * i;
+                qarpx::NoiseModel part;
+                switch (spec_kind[i]) {
+                    case 0: part = qarpx::make_depolarizing(p[0], gates); break;
+                    case 1: part = qarpx::make_pauli(p[0], p[1], p[2], gates); break;
+                    case 2: part = qarpx::make_bit_flip(p[0], gates); break;
+                    case 3: part = qarpx::make_amplitude_damping(p[0], gates); break;
+                    default: throw std::invalid_argument("qref_run_noisy: unknown builder");
+                }
+                nm = i == 0 ? part : nm + part;
+            }
+            sim.set_noise_model(std::move(nm));
+        }
         auto res = sim.run(to_commands(cmds, nbytes), n, shots, seed);
         if (history) {
             if (res.n_cbits > 64) throw std::invalid_argument("qref_run_history: more than 64 cbits");

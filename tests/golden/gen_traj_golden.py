@@ -6,7 +6,9 @@ the reference sources into oracle/_ref).
 
 ``traj_case`` rebuilds every case's command list from its name (seeded numpy draws), so the
 fixture holds only the reference's outputs: the per-shot classical registers (bit masks, shot
-order), the outcome counts and the register width.
+order), the outcome counts and the register width.  The noisy cases run under a noise model made
+by the reference's named builders (``noise_specs``); ``noise_model`` makes the engine's model from
+the same builders.
 """
 from __future__ import annotations
 
@@ -26,7 +28,48 @@ CASES = {   # name -> (n_qubits, shots, seed)
     "branches": (7, 1200, 5),
     "wide": (14, 300, 99),
     "dead_conditions": (4, 500, 3),
+    "noisy_teleport": (3, 2000, 8),
+    "noisy_damping": (5, 1500, 22),
+    "noisy_branches": (7, 1000, 6),
+    "noisy_terminal": (6, 1000, 12),
+    "noisy_wide_mcz": (17, 48, 31),
 }
+
+_1Q = ("X", "Y", "Z", "H", "S", "Sdg", "T", "Tdg", "SX", "SXdg", "Id", "Rx", "Ry", "Rz", "P", "U")
+_2Q = ("CX", "CY", "CZ", "SWAP", "ECR", "iSWAP", "iSWAPdg", "CH", "CS", "CSdg", "CSX", "CSXdg", "CRx", "CRy",
+       "CRz", "CP", "RZZ", "RXX", "RYY", "CU")
+
+
+def noise_specs(name: str):
+    """The noise model of a case as the reference's named builders, composed with + in order:
+    [(builder, params, gate names)]; empty for the noiseless cases."""
+    if name == "noisy_teleport":
+        return [("depolarizing", 0.05, _1Q + _2Q)]
+    if name == "noisy_damping":
+        return [("depolarizing", 0.03, _1Q + _2Q), ("amplitude_damping", 0.2, ("U", "H"))]
+    if name == "noisy_branches":
+        return [("pauli", (0.02, 0.03, 0.04), _1Q), ("depolarizing", 0.05, _2Q + ("MCZ",)),
+                ("amplitude_damping", 0.15, ("Rx", "U"))]
+    if name == "noisy_terminal":
+        return [("bit_flip", 0.05, _1Q), ("depolarizing", 0.1, ("CX", "RZZ"))]
+    if name == "noisy_wide_mcz":
+        return [("depolarizing", 0.9, ("MCZ",)), ("depolarizing", 0.02, ("CX",))]
+    return []
+
+
+def noise_model(name: str):
+    """The engine's NoiseModel for a case (None when noiseless), from the same builders."""
+    from openqarp_b200.ir import GateType
+    from openqarp_b200.noise import (make_amplitude_damping, make_bit_flip, make_depolarizing,
+                                     make_pauli)
+    nm = None
+    for builder, p, gates in noise_specs(name):
+        g = [GateType[x] for x in gates]
+        part = {"depolarizing": lambda: make_depolarizing(p, g), "pauli": lambda: make_pauli(*p, g),
+                "bit_flip": lambda: make_bit_flip(p, g),
+                "amplitude_damping": lambda: make_amplitude_damping(p, g)}[builder]()
+        nm = part if nm is None else nm + part
+    return nm
 
 
 def haar(rng, d):
@@ -83,6 +126,20 @@ def traj_case(name: str):
         cmds = _layer(rng, n) + _layer(rng, n) + [M(3, 0), M(13, 1)]
         cmds += [B((0,), (True,))] + _layer(rng, n) + [ELSE, Command(G.H, (12,)), END]
         cmds += _layer(rng, n, ((1,), (True,))) + [Command(G.Reset, (13,)), M(12, 2)]
+    elif name == "noisy_teleport":
+        return traj_case("teleport")[0], traj_case("teleport")[1], shots, seed
+    elif name == "noisy_damping":
+        return n, traj_case("reset_chain")[1], shots, seed
+    elif name == "noisy_branches":
+        return n, traj_case("branches")[1], shots, seed
+    elif name == "noisy_terminal":
+        cmds = _layer(rng, n) + _layer(rng, n) + [M(q, q) for q in range(n)]
+    elif name == "noisy_wide_mcz":
+        qs = list(range(n))
+        cmds = _layer(rng, n)
+        cmds += [Command(G.MCZ, tuple(qs)), Command(G.MCZ, tuple(qs[1:])), Command(G.MCZ, tuple(qs[2:])),
+                 Command(G.MCZ, tuple(qs[:3])), M(0, 0), C(G.MCZ, tuple(qs[::-1]), (0,), (True,))]
+        cmds += _layer(rng, n) + [Command(G.MCZ, tuple(qs)), M(1, 1), M(16, 2)]
     elif name == "dead_conditions":
         cmds = _layer(rng, n) + [M(0, 0)]
         cmds += [C(G.X, (1,), (3,), (True,)),                          # reads a cbit nothing wrote
@@ -94,14 +151,24 @@ def traj_case(name: str):
     return n, cmds, shots, seed
 
 
+def reference_run(ref, name: str):
+    """(counts, per-shot registers, width) of a case from the reference (oracle.Reference)."""
+    from openqarp_b200.ir import GateType, pack
+    n, cmds, shots, seed = traj_case(name)
+    specs = noise_specs(name)
+    if specs:
+        return ref.run_noisy(pack(cmds).buf, n, shots, seed,
+                             [(b, p, [int(GateType[x]) for x in g]) for b, p, g in specs])
+    return ref.run_history(pack(cmds).buf, n, shots, seed)
+
+
 def main():
     from oracle.oracle import Reference
-    from openqarp_b200.ir import pack
     ref = Reference()
     out = {}
     for name in CASES:
-        n, cmds, shots, seed = traj_case(name)
-        counts, hist, ncb = ref.run_history(pack(cmds).buf, n, shots, seed)
+        n, _cmds, shots, _seed = traj_case(name)
+        counts, hist, ncb = reference_run(ref, name)
         keys = np.array(sorted(counts), dtype=np.uint64)
         out[name + "_keys"] = keys
         out[name + "_counts"] = np.array([counts[int(k)] for k in keys], dtype=np.int64)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN
-from golden.gen_traj_golden import CASES, traj_case
+from golden.gen_traj_golden import CASES, noise_model, noise_specs, reference_run, traj_case
 
 
 @pytest.fixture(scope="module")
@@ -68,10 +68,8 @@ def test_register_marshalling_without_a_device():
 
 def test_fixture_is_the_reference_output(traj_golden, reference):
     """The committed vectors are what the reference's trajectory path returns today."""
-    from openqarp_b200.ir import pack
     for name in CASES:
-        n, cmds, shots, seed = traj_case(name)
-        counts, hist, ncb = reference.run_history(pack(cmds).buf, n, shots, seed)
+        counts, hist, ncb = reference_run(reference, name)
         assert counts == _counts(traj_golden, name), name
         np.testing.assert_array_equal(hist, traj_golden[name + "_hist"], err_msg=name)
         assert ncb == int(traj_golden[name + "_ncb"][0])
@@ -84,13 +82,121 @@ def test_reference_branch_table_errors(reference):
         reference.run_history(pack(stray).buf, 1, 4, 1)
 
 
+def test_noise_builders_follow_the_reference():
+    """Channel parameters of the named builders and their argument errors (noise_model.cpp)."""
+    from openqarp_b200.ir import GateType as G
+    from openqarp_b200.noise import (KrausChannel, NoiseModel, PauliChannel, PauliChannel2q,
+                                     PauliChannelKq, make_amplitude_damping, make_depolarizing,
+                                     make_pauli)
+    nm = make_depolarizing(0.3, [G.H, G.CX, G.MCZ])
+    assert nm.per_gate[int(G.H)] == PauliChannel(0.3 / 3.0, 0.3 / 3.0, 0.3 / 3.0)
+    assert nm.per_gate[int(G.CX)] == PauliChannel2q((0.3 / 15.0,) * 15)
+    assert nm.per_gate[int(G.MCZ)] == PauliChannelKq(0.3)
+    ad = make_amplitude_damping(0.36, [G.X]).per_gate[int(G.X)]
+    assert isinstance(ad, KrausChannel)
+    np.testing.assert_array_equal(ad.K[0], [[1, 0], [0, 0.8]])
+    np.testing.assert_array_equal(ad.K[1], [[0, 0.6], [0, 0]])
+    both = make_pauli(0.1, 0, 0, [G.X, G.Y]) + make_depolarizing(0.2, [G.Y])
+    assert both.per_gate[int(G.X)] == PauliChannel(0.1, 0, 0)
+    assert both.per_gate[int(G.Y)] == PauliChannel(0.2 / 3, 0.2 / 3, 0.2 / 3)
+    off = NoiseModel.depolarizing(0.1)
+    off.enabled = False
+    assert not (off + both).active() and both.active() and not NoiseModel().active()
+    kind, offset, params = make_depolarizing(0.3, [G.H, G.CX]).table()
+    assert kind[int(G.H)] == 1 and kind[int(G.CX)] == 2
+    assert offset[int(G.CX) + 1] - offset[int(G.CX)] == 15
+    for bad in (lambda: make_depolarizing(0.1, [G.CCX]), lambda: make_pauli(0.1, 0, 0, [G.CX]),
+                lambda: make_amplitude_damping(1.5, [G.X]), lambda: make_pauli(-0.1, 0, 0, [G.X])):
+        with pytest.raises(ValueError):
+            bad()
+
+
+def test_noise_builder_errors_match_reference(reference):
+    from openqarp_b200.ir import Command, GateType as G, pack
+    from openqarp_b200.noise import make_amplitude_damping, make_depolarizing, make_pauli
+    buf = pack([Command(G.H, (0,)), Command(G.Measure, (0,), (), None, (0,))]).buf
+    cases = [("depolarizing", 0.1, [G.CCX], lambda: make_depolarizing(0.1, [G.CCX])),
+             ("pauli", (0.1, 0, 0), [G.CX], lambda: make_pauli(0.1, 0, 0, [G.CX])),
+             ("amplitude_damping", 1.5, [G.X], lambda: make_amplitude_damping(1.5, [G.X])),
+             ("pauli", (0.5, 0.4, 0.3), [G.X], lambda: make_pauli(0.5, 0.4, 0.3, [G.X]))]
+    for builder, p, gates, ours in cases:
+        with pytest.raises(Exception) as ref_err:
+            reference.run_noisy(buf, 3, 4, 1, [(builder, p, [int(g) for g in gates])])
+        with pytest.raises(ValueError) as our_err:
+            ours()
+        assert str(our_err.value) in str(ref_err.value)
+
+
+_RNG_PIN = r"""
+#include <cstdio>
+#include <random>
+#include <vector>
+#include "traj_rng.cuh"
+int main() {
+    using namespace qsv;
+    std::vector<uint32_t> w(kMtN);
+    uint32_t idx = 0;
+    const MtView v{w.data(), 1, &idx};
+    const uint64_t ranges[] = {2, 3, 15, 255, 1000003, (1ull << 32) - 2, (1ull << 32) - 1, 1ull << 32,
+                               (1ull << 34) - 1, (1ull << 40) + 12345, (1ull << 62) - 1};
+    long bad = 0, total = 0;
+    for (uint32_t seed : {0u, 1u, 5489u, 123456789u, 4294967295u}) {
+        std::mt19937 g(seed);
+        v.seed(seed);
+        std::uniform_real_distribution<double> u01(0.0, 1.0);
+        for (int i = 0; i < 5000; ++i) {
+            const int r = i % 13;
+            if (r < 11) {
+                std::uniform_int_distribution<uint64_t> d(1, ranges[r]);
+                bad += d(g) != v.uniform(1, ranges[r]);
+            } else if (r == 11) {
+                bad += g() != v.next();
+            } else {
+                bad += u01(g) != v.canonical();
+            }
+            ++total;
+        }
+    }
+    std::printf("%ld %ld\n", bad, total);
+    return bad != 0;
+}
+"""
+
+
+def test_device_streams_restate_the_library(tmp_path):
+    """traj_rng.cuh (compiled for the host here) draws exactly what std::mt19937 with
+    uniform_real_distribution and uniform_int_distribution draw, across ranges that take the
+    multiply-and-reject path, the raw path and the composed wide path."""
+    import subprocess
+    src = tmp_path / "rng_pin.cpp"
+    src.write_text(_RNG_PIN)
+    exe = tmp_path / "rng_pin"
+    csrc = os.path.join(os.path.dirname(GOLDEN), "..", "openqarp_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", csrc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    bad, total = map(int, out.stdout.split())
+    assert total == 25000 and bad == 0, out.stdout
+
+
 # ---------------------------------------------------------------- GPU: device trajectories
+
+def _sim_for(name, dtype="complex128"):
+    from openqarp_b200 import B200Simulator
+    return B200Simulator(noise_model=noise_model(name), dtype=dtype)
+
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(CASES))
 def test_trajectories_match_reference(sim, traj_golden, name):
     n, cmds, shots, seed = traj_case(name)
-    res = sim.run(cmds, n, shots, seed)
+    if noise_specs(name):
+        noisy = _sim_for(name)
+        try:
+            res = noisy.run(cmds, n, shots, seed)
+        finally:
+            noisy.close()
+    else:
+        res = sim.run(cmds, n, shots, seed)
     width = int(traj_golden[name + "_ncb"][0])
     assert res.n_cbits == width
     assert len(res.cbit_history) == shots
@@ -99,18 +205,34 @@ def test_trajectories_match_reference(sim, traj_golden, name):
 
 
 @pytest.mark.gpu
-def test_trajectories_independent_of_batch(sim):
+@pytest.mark.parametrize("name", ["branches", "noisy_branches"])
+def test_trajectories_independent_of_batch(name):
     """Shots run in batches of the device register; the batch size changes no result."""
-    n, cmds, shots, seed = traj_case("branches")
-    full = sim.run(cmds, n, shots, seed)
-    reg = sim.register(n)
+    n, cmds, shots, seed = traj_case(name)
+    s = _sim_for(name)
     try:
-        reg.set_trajectory_batch(64)
-        small = sim.run(cmds, n, shots, seed)
+        full = s.run(cmds, n, shots, seed)
+        s.register(n).set_trajectory_batch(64)
+        small = s.run(cmds, n, shots, seed)
     finally:
-        reg.set_trajectory_batch(0)
+        s.close()
     assert small.cbit_history == full.cbit_history
     np.testing.assert_array_equal(small.outcomes, full.outcomes)
+
+
+@pytest.mark.gpu
+def test_noisy_statevector_entry_points_refuse():
+    from openqarp_b200.ir import Command, GateType as G
+    s = _sim_for("noisy_teleport")
+    try:
+        with pytest.raises(RuntimeError, match="noise model is active"):
+            s.statevector([Command(G.H, (0,))], 1)
+        with pytest.raises(RuntimeError, match="noise model is active"):
+            s.unitary_matrix([Command(G.H, (0,))], 1)
+        s.noise_model.enabled = False
+        assert s.statevector([Command(G.H, (0,))], 1).shape == (2,)
+    finally:
+        s.close()
 
 
 @pytest.mark.gpu
@@ -127,12 +249,16 @@ def test_trajectories_from_initial_state(sim):
 
 
 @pytest.mark.gpu
-def test_trajectories_complex64_follow_complex128(sim64, traj_golden):
+def test_trajectories_complex64_follow_complex128(traj_golden):
     """complex64 storage: per-shot decisions compare float-rounded probabilities with the same
     uniforms, so almost every shot takes the complex128 path."""
-    for name in ("teleport", "branches", "wide"):
+    for name in ("teleport", "branches", "wide", "noisy_damping"):
         n, cmds, shots, seed = traj_case(name)
-        res = sim64.run(cmds, n, shots, seed)
+        s = _sim_for(name, "complex64")
+        try:
+            res = s.run(cmds, n, shots, seed)
+        finally:
+            s.close()
         width = int(traj_golden[name + "_ncb"][0])
         same = np.mean(_masks(res.cbit_history, width) == traj_golden[name + "_hist"])
         assert same >= 0.98, (name, same)
