@@ -17,7 +17,10 @@ Also reported on the same line:
     bounded sample of the same workload;
   * structured_and_readouts: a phase-estimation-shaped structured program (controlled powers
     + inverse QFT) at 28 and 22 qubits with the reference's CPU program_statevector at 22, the
-    exact Born readout and the PauliAveraging parity counts on the device.
+    exact Born readout and the PauliAveraging parity counts on the device;
+  * trajectories: a 16-qubit feed-forward circuit (a mid-circuit measurement and a conditioned
+    gate per layer) sampled shot by shot on the device, noiseless and noisy, against the
+    reference's CPU run() on a bounded number of shots, with the per-shot registers compared.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 """
@@ -529,6 +532,11 @@ def b200_arm(args, rank, world, local_rank):
             reg.close()
             from openqarp_b200.workloads import structured_rows
             structured = structured_rows(device=device)
+        traj = None
+        if not args.skip_trajectories:
+            reg.close()
+            from openqarp_b200.workloads import trajectory_rows
+            traj = trajectory_rows(device=device)
         heis = None
         if not args.skip_heisenberg:
             reg.close()
@@ -568,6 +576,7 @@ def b200_arm(args, rank, world, local_rank):
             "heisenberg31_c64_bulk": heis,
             "qaoa_batched": qaoa,
             "structured_and_readouts": structured,
+            "trajectories": traj,
         }
     else:
         reg.close()
@@ -586,6 +595,7 @@ def main():
     ap.add_argument("--skip-qaoa", action="store_true")
     ap.add_argument("--skip-ksweep", action="store_true")
     ap.add_argument("--skip-structured", action="store_true")
+    ap.add_argument("--skip-trajectories", action="store_true")
     ap.add_argument("--executor", type=int, default=None, choices=[0, 1],
                     help="pin the executor (0 stream, 1 tiled) instead of autotuning; needs --k")
     ap.add_argument("--k", type=int, default=None, help="pin the fusion width; needs --executor")

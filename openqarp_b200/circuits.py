@@ -155,3 +155,21 @@ def heisenberg_observable(n: int, fields):
             obs.append(([(u, P), (v, P)], 1.0))
     obs += [([(q, "Z")], float(fields[q])) for q in range(n)]
     return obs
+
+
+def feedforward(n: int, depth: int, seed: int = 0):
+    """Mid-circuit measurement with feed-forward: ``depth`` layers of U on every qubit, CX on a
+    random pairing and an RZZ; after each layer qubit (d mod n) is measured into cbit (d mod 8)
+    and an X on the next qubit is conditioned on that cbit; every qubit is measured at the end
+    into cbit (q mod 8).  The trajectory path's benchmark shape."""
+    rng = np.random.default_rng(seed)
+    cmds = []
+    for d in range(depth):
+        cmds += [Command(G.U, (q,), tuple(rng.uniform(-3, 3, 3))) for q in range(n)]
+        qs = [int(x) for x in rng.permutation(n)]
+        cmds += [Command(G.CX, (a, b)) for a, b in zip(qs[::2], qs[1::2])]
+        cmds.append(Command(G.RZZ, (qs[0], qs[-1]), (float(rng.uniform(-3, 3)),)))
+        cmds.append(Command(G.Measure, (d % n,), (), None, (d % 8,)))
+        cmds.append(Command(G.X, ((d + 1) % n,), (), None, (), (d % 8,), (True,)))
+    cmds += [Command(G.Measure, (q,), (), None, (q % 8,)) for q in range(n)]
+    return cmds
