@@ -32,8 +32,7 @@
 #include <cmath>
 #include <cstring>
 
-#include "kernels.h"
-#include "traj_rng.cuh"
+#include "traj.h"
 
 namespace qsv {
 
@@ -41,13 +40,6 @@ namespace {
 
 constexpr int kTrThreads = 256;
 constexpr int kTrChunkLog = 12;            // amplitudes per partial sum: 4096
-constexpr int kTrMaskedMaxQubits = 4;      // widest masked dense block
-constexpr int kMaxKrausOps = 8;
-
-struct TrDenseArgs {
-    uint64_t off[16];   // index offset of local basis state l (local bit b <-> qubit q[b])
-    uint8_t pos[8];     // ascending target positions
-};
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
 #pragma unroll
@@ -59,12 +51,6 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     if (threadIdx.x == 0)
         for (int i = 0; i < static_cast<int>(blockDim.x + 31) / 32; ++i) t += red[i];
     return t;   // valid in thread 0
-}
-
-template <typename T>
-__device__ __forceinline__ double norm2(const vec2_t<T>& a) {
-    const double x = static_cast<double>(a.x), y = static_cast<double>(a.y);
-    return __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
 }
 
 // pass[s] = the shot's branch flags match (fmask, fwant) and its classical register matches the
@@ -148,7 +134,7 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_chunk_sums(const vec2_t<T>* _
     const uint64_t idx0 = (b << clog) & ((1ull << n) - 1ull);   // index within the shot
     double acc = 0.0;
     for (uint64_t i = threadIdx.x; i < chunk; i += blockDim.x)
-        if (!((idx0 + i) & zero_mask)) acc += norm2<T>(p[i]);
+        if (!((idx0 + i) & zero_mask)) acc += tr_norm2<T>(p[i]);
     const double tot = block_sum(acc, red);
     if (threadIdx.x == 0) out[b] = tot;
 }
@@ -178,9 +164,7 @@ __global__ void k_tr_seed(MtState mt, int n_shots, uint32_t seed) {
     mt.of(s).seed(seed + static_cast<uint32_t>(s));
 }
 
-// Measure / Reset decision per shot (qarp_simulator.cpp:636-690): r = the shot's next uniform,
-// outcome 1 when r >= p0; renormalisation factor sqrt(1 / p) with p = max(p_outcome, 0)
-// (csim normalize, update_ops_named_state.cpp:21-35); Measure records the outcome in its cbit.
+// Measure / Reset decision per shot (tr_decide); Measure records the outcome in its cbit.
 __global__ void k_tr_decide(const uint8_t* __restrict__ pass, const double* __restrict__ p0, MtState mt,
                             uint64_t* __restrict__ cbits, int n_shots, int cbit, int8_t* __restrict__ outcome,
                             double* __restrict__ scale) {
@@ -190,86 +174,32 @@ __global__ void k_tr_decide(const uint8_t* __restrict__ pass, const double* __re
         outcome[s] = -1;
         return;
     }
-    const double r = mt.of(s).canonical();
-    const bool one = r >= p0[s];
-    const double p = one ? fmax(1.0 - p0[s], 0.0) : fmax(p0[s], 0.0);
+    double sc = 0.0;
+    const bool one = tr_decide(p0[s], mt.of(s), &sc);
     outcome[s] = one ? 1 : 0;
-    scale[s] = sqrt(1.0 / p);
+    scale[s] = sc;
     if (cbit >= 0) cbits[s] = one ? (cbits[s] | (1ull << cbit)) : (cbits[s] & ~(1ull << cbit));
 }
 
 // ---------------------------------------------------------------- noise channels
 
-enum NoiseKind : int { NOISE_NONE = 0, NOISE_PAULI = 1, NOISE_PAULI2 = 2, NOISE_KRAUS = 3, NOISE_PAULIK = 4 };
-
-struct TrQubits {
-    uint8_t q[32];
-    int k;
-};
-
-__device__ __forceinline__ void add_pauli(int axis, int q, uint64_t& x, uint64_t& z, uint32_t& ny) {
-    const uint64_t bit = 1ull << q;
-    if (axis == 1) x |= bit;
-    else if (axis == 2) { x |= bit; z |= bit; ++ny; }
-    else if (axis == 3) z |= bit;
-}
-
-// Pauli channels (apply_pauli_channel_1q / _2q / _kq, noise_model.cpp:60-124): each passing shot
-// draws, the cumulative weights pick a Pauli string, and the shots where a non-identity string
-// fired are appended to `active` with their X mask, Z mask and Y count.
+// Pauli channels (tr_choose_pauli): each passing shot draws its string; the shots where a
+// non-identity string fired are appended to `active` with their X mask, Z mask and Y count.
 __global__ void k_tr_noise_pauli(const uint8_t* __restrict__ pass, MtState mt, int n_shots, int kind,
                                  const double* __restrict__ prm, const __grid_constant__ TrQubits tq,
                                  uint64_t* __restrict__ ax, uint64_t* __restrict__ az, uint32_t* __restrict__ any,
                                  uint32_t* __restrict__ active, uint32_t* __restrict__ n_active) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots || !pass[s]) return;
-    const MtView g = mt.of(s);
-    uint64_t x = 0, z = 0;
-    uint32_t ny = 0;
-    if (kind == NOISE_PAULI) {
-        const double r = g.canonical();
-        double acc = prm[0];
-        if (r < acc) add_pauli(1, tq.q[0], x, z, ny);
-        else if (r < (acc += prm[1])) add_pauli(2, tq.q[0], x, z, ny);
-        else if (r < (acc += prm[2])) add_pauli(3, tq.q[0], x, z, ny);
-    } else if (kind == NOISE_PAULI2) {
-        const double r = g.canonical();
-        double acc = 0.0;
-        for (int id = 0; id < 15; ++id) {
-            acc += prm[id];
-            if (r < acc) {
-                const int packed = id + 1;
-                add_pauli(packed & 3, tq.q[0], x, z, ny);
-                add_pauli((packed >> 2) & 3, tq.q[1], x, z, ny);
-                break;
-            }
-        }
-    } else {   // NOISE_PAULIK: k in [1, 31] (the host drops the others, which draw nothing)
-        if (g.canonical() < prm[0]) {
-            const uint64_t code = g.uniform(1, (1ull << (2 * tq.k)) - 1);
-            for (int i = 0; i < tq.k; ++i) add_pauli(static_cast<int>((code >> (2 * i)) & 3u), tq.q[i], x, z, ny);
-        }
-    }
+    uint64_t x, z;
+    uint32_t ny;
+    tr_choose_pauli(kind, prm, tq, mt.of(s), x, z, ny);
     if (x | z) {
         ax[s] = x;
         az[s] = z;
         any[s] = ny;
         active[atomicAdd(n_active, 1u)] = static_cast<uint32_t>(s);
     }
-}
-
-// c * a for c = i^ny * (-1)^neg; exact
-template <typename T>
-__device__ __forceinline__ vec2_t<T> pauli_phase(vec2_t<T> a, uint32_t ny, bool neg) {
-    vec2_t<T> r;
-    switch (ny & 3u) {
-        case 0: r = a; break;
-        case 1: r = mk<T>(-a.y, a.x); break;
-        case 2: r = mk<T>(-a.x, -a.y); break;
-        default: r = mk<T>(a.y, -a.x); break;
-    }
-    if (neg) r = mk<T>(-r.x, -r.y);
-    return r;
 }
 
 // P = i^nY X^x Z^z on every listed shot: |j> -> i^nY (-1)^popcount(j & z) |j ^ x>.  Work items are
@@ -291,14 +221,14 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_apply_pauli(vec2_t<T>* __rest
         const uint32_t ny = any[shot];
         vec2_t<T>* p = s + (static_cast<uint64_t>(shot) << n);
         if (x == 0) {
-            for (uint64_t j = 2 * g; j < 2 * g + 2; ++j) p[j] = pauli_phase<T>(p[j], ny, __popcll(j & z) & 1);
+            for (uint64_t j = 2 * g; j < 2 * g + 2; ++j) p[j] = tr_pauli_phase<T>(p[j], ny, __popcll(j & z) & 1);
         } else {
             const int hb = 63 - __clzll(x);
             const uint64_t j = ((g >> hb) << (hb + 1)) | (g & ((1ull << hb) - 1ull));
             const uint64_t j2 = j ^ x;
             const vec2_t<T> a = p[j], b = p[j2];
-            p[j2] = pauli_phase<T>(a, ny, __popcll(j & z) & 1);
-            p[j] = pauli_phase<T>(b, ny, __popcll(j2 & z) & 1);
+            p[j2] = tr_pauli_phase<T>(a, ny, __popcll(j & z) & 1);
+            p[j] = tr_pauli_phase<T>(b, ny, __popcll(j2 & z) & 1);
         }
     }
 }
@@ -334,18 +264,8 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_rho_chunks(const vec2_t<T>* _
     }
 }
 
-struct c2 {
-    double re, im;
-};
-__device__ __forceinline__ c2 cmul2(c2 a, c2 b) {
-    return c2{__dsub_rn(__dmul_rn(a.re, b.re), __dmul_rn(a.im, b.im)), __dadd_rn(__dmul_rn(a.re, b.im), __dmul_rn(a.im, b.re))};
-}
-__device__ __forceinline__ c2 cadd2(c2 a, c2 b) { return c2{__dadd_rn(a.re, b.re), __dadd_rn(a.im, b.im)}; }
-__device__ __forceinline__ c2 conj2(c2 a) { return c2{a.re, -a.im}; }
-
-// One-qubit Kraus channel choice (apply_kraus_channel_1q, noise_model.cpp:127-170): firing
-// probabilities p_i = max(0, Re tr(K_i rho K_i^dag)), normalised by their total (no draw when the
-// total is not positive), the draw, and the chosen operator scaled by 1/sqrt(p_i) into kmat.
+// One-qubit Kraus channel per shot: the reduced density matrix from the chunk sums, then
+// tr_choose_kraus.
 __global__ void k_tr_kraus_decide(const uint8_t* __restrict__ pass, const double* __restrict__ rho_chunks,
                                   uint64_t per_shot, MtState mt, int n_shots, const double* __restrict__ kops,
                                   int n_ops, int8_t* __restrict__ act, double* __restrict__ kmat) {
@@ -361,36 +281,7 @@ __global__ void k_tr_kraus_decide(const uint8_t* __restrict__ pass, const double
         rr += v[2];
         ri += v[3];
     }
-    const c2 rho[2][2] = {{c2{r00, 0.0}, c2{rr, ri}}, {c2{rr, -ri}, c2{r11, 0.0}}};
-    double probs[8];
-    double total = 0.0;
-    for (int o = 0; o < n_ops; ++o) {
-        const double* k = kops + 8 * o;
-        const c2 K[2][2] = {{c2{k[0], k[1]}, c2{k[2], k[3]}}, {c2{k[4], k[5]}, c2{k[6], k[7]}}};
-        c2 tr{0.0, 0.0};
-        for (int i = 0; i < 2; ++i) {
-            c2 KR[2];
-            for (int j = 0; j < 2; ++j) KR[j] = cadd2(cmul2(K[i][0], rho[0][j]), cmul2(K[i][1], rho[1][j]));
-            tr = cadd2(tr, cadd2(cmul2(KR[0], conj2(K[i][0])), cmul2(KR[1], conj2(K[i][1]))));
-        }
-        probs[o] = fmax(0.0, tr.re);
-        total += probs[o];
-    }
-    if (total <= 0.0) return;
-    for (int o = 0; o < n_ops; ++o) probs[o] /= total;
-    const double r = mt.of(s).canonical();
-    double acc = 0.0;
-    for (int o = 0; o < n_ops; ++o) {
-        acc += probs[o];
-        if (r < acc) {
-            const double p_unnorm = probs[o] * total;
-            if (p_unnorm <= 0.0) return;
-            const double sc = 1.0 / sqrt(p_unnorm);
-            for (int e = 0; e < 8; ++e) kmat[8ull * s + e] = kops[8 * o + e] * sc;
-            act[s] = 1;
-            return;
-        }
-    }
+    if (tr_choose_kraus(r00, r11, rr, ri, kops, n_ops, mt.of(s), kmat + 8ull * s)) act[s] = 1;
 }
 
 // the chosen 2x2 operator on qubit q of every shot with act set
@@ -485,7 +376,7 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_pick_index(const vec2_t<T>* _
     const vec2_t<T>* p = s + (shot << n) + start;
     const uint64_t lo = threadIdx.x * per;
     double run = 0.0;
-    for (uint64_t i = lo; i < lo + per && i < chunk; ++i) run += norm2<T>(p[i]);
+    for (uint64_t i = lo; i < lo + per && i < chunk; ++i) run += tr_norm2<T>(p[i]);
     part[threadIdx.x] = run;
     __syncthreads();
     if (threadIdx.x != 0) return;
@@ -499,7 +390,7 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_pick_index(const vec2_t<T>* _
         }
         bool hit = false;
         for (uint64_t i = t * per; i < t * per + per && i < chunk; ++i) {
-            acc += norm2<T>(p[i]);
+            acc += tr_norm2<T>(p[i]);
             if (acc >= thr) {
                 idx = i;
                 hit = true;
@@ -542,42 +433,6 @@ unsigned stride_blocks(uint64_t work) {
 
 // ---------------------------------------------------------------- the plan (host)
 
-struct TrGuard {
-    uint64_t fmask = 0, fwant = 0;   // branch flags (bit d: the enclosing branch at depth d taken)
-    uint64_t cmask = 0, cwant = 0;   // the command's own classical condition
-    bool never = false;              // a condition that lists one cbit with both values
-    bool trivial() const { return !never && !fmask && !cmask; }
-    bool operator==(const TrGuard& o) const {
-        return fmask == o.fmask && fwant == o.fwant && cmask == o.cmask && cwant == o.cwant && never == o.never;
-    }
-};
-
-struct TrStep {
-    enum Kind { OPS, MDENSE, MSCALE, MOPS, MEASURE, BRANCH, NOISE } kind = OPS;
-    TrGuard g;
-    std::vector<Op> ops;          // OPS: every shot; MOPS: every shot, failing shots restored
-    int k = 0;                    // MDENSE width
-    size_t moff = 0;              // MDENSE: first entry in the matrix table
-    TrDenseArgs args{};           // MDENSE
-    c128 phase{1.0, 0.0};         // MSCALE
-    int qubit = 0, cbit = -1;     // MEASURE (cbit -1: outcome not recorded)
-    bool reset = false;           // MEASURE: Reset
-    int flag = 0;                 // BRANCH: flag bit (= nesting depth)
-    uint64_t bmask = 0, bwant = 0;   // BRANCH condition
-    int noise = NOISE_NONE;       // NOISE: channel kind, its parameters at poff in the table,
-    size_t poff = 0;              //        its qubits (the command's, in order)
-    int n_ops = 0;                //        Kraus operators
-    TrQubits nq{};
-};
-
-struct TrPlan {
-    std::vector<TrStep> steps;
-    std::vector<cplx<double>> mats;   // MDENSE matrices, row-major
-    std::vector<double> noise_prm;    // NOISE parameters
-    bool needs_backup = false;
-    bool kraus = false;
-};
-
 // (mask, want) of an AND of cbit conditions; unsatisfiable when a bit is asked for both values
 void condition_of(const Cmd& c, int n_cbits, uint64_t* mask, uint64_t* want, bool* never) {
     *mask = 0;
@@ -604,6 +459,8 @@ bool noise_exempt(int g) {
     return g == MEASURE || g == RESET || g == BARRIER || g == GPHASE || g == BRANCH_BEGIN || g == BRANCH_ELSE ||
            g == BRANCH_END || g < 0 || g >= GATE_COUNT;
 }
+
+}  // namespace
 
 TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion_max, int fusion_min,
                   const std::vector<NoiseSpec>* noise) {
@@ -793,6 +650,8 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
     return plan;
 }
 
+namespace {
+
 struct DeviceBuffer {
     void* p = nullptr;
     explicit DeviceBuffer(size_t bytes) {
@@ -841,6 +700,9 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
     const TrPlan plan = build_plan(suffix, n, n_cbits, opt.fusion_max, opt.fusion_min, opt.noise);
     if (n_shots == 0) return;
     if (!out_idx || !out_cbits) throw std::invalid_argument("null output");
+    if (!opt.max_batch_shots &&
+        run_trajectories_fused<T>(plan, n, d_prefix, seed, n_shots, out_idx, out_cbits, st, launches))
+        return;
     uint64_t n_launch = 0;
 
     const int clog = std::min(n, kTrChunkLog);
