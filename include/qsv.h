@@ -261,8 +261,8 @@ QSV_API int qsv_set_noise(void* h, int n_gate_types, const int32_t* kind, const 
                           const double* params);
 /* Shots per device batch of qsv_run_trajectories (rounded down to a power of two; 0, the
  * default: as many as half the free device memory holds, at most 2^20).  With the default, a
- * register of at most 64 KiB runs each shot in one CTA's shared memory instead; a nonzero
- * value keeps such registers on the batched executor too.  Results do not depend on it. */
+ * register of 4 to 64 KiB runs each shot in one CTA's shared memory instead; a nonzero value
+ * keeps such registers on the batched executor too.  Results do not depend on it. */
 QSV_API int qsv_set_trajectory_batch(void* h, uint64_t max_shots);
 QSV_API int qsv_run_trajectories(void* h, const uint8_t* cmds, size_t nbytes, uint32_t seed, size_t n_shots,
                                  uint64_t* out_idx, uint64_t* out_cbits, int32_t* n_cbits);

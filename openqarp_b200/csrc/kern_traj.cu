@@ -701,7 +701,7 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
     if (n_shots == 0) return;
     if (!out_idx || !out_cbits) throw std::invalid_argument("null output");
     if (!opt.max_batch_shots &&
-        run_trajectories_fused<T>(plan, n, d_prefix, seed, n_shots, out_idx, out_cbits, st, launches))
+        run_trajectories_fused<T>(plan, n, d_prefix, seed, n_shots, out_idx, out_cbits, st, ws, launches))
         return;
     uint64_t n_launch = 0;
 

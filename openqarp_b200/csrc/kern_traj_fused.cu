@@ -1,7 +1,7 @@
 // kern_traj_fused.cu — trajectories of small registers with each shot held in one CTA's shared
 // memory from its first command to its final sample.
 //
-// For registers up to 64 KiB (complex128 n <= 12, complex64 n <= 13) the batched executor's
+// For registers of 4 to 64 KiB (complex128 n = 8..12, complex64 n = 9..13) the batched executor's
 // passes over the wide register in HBM are pure overhead: a shot fits on chip.  Here every CTA
 // runs one shot: it loads the prefix state into shared memory, seeds the shot's MT19937 engine
 // (std::mt19937(seed + shot)) in shared memory, and interprets the trajectory plan — fused
@@ -20,6 +20,13 @@ namespace {
 
 constexpr int kFsThreads = 256;
 constexpr int kFsMaxBytes = 64 * 1024;   // widest register held in shared memory
+// Below 4 KiB a shot leaves most of a CTA idle and its serial engine seeding dominates; the
+// batched executor's wide register then sits in L2 and wins (B200: 6 qubits, 20000 shots,
+// 3.1 ms batched vs 5.1 ms here; 10 qubits: 21.8 ms batched vs 10.5 ms here).
+constexpr int kFsMinBytes = 4 * 1024;
+constexpr int kFsMaxCoef = 512;          // doubles of one step's coefficients (a 4-qubit block)
+constexpr int kFsMtBytes = 4 * 624 + 16; // one MT19937 state, padded to keep the plan aligned
+constexpr size_t kFsResidentMax = 104 * 1024;   // dynamic shared memory with the plan resident
 
 enum FsKind : uint8_t {
     FS_DENSE = 0,     // k <= 4 unitary on q[0..k) where (i & ctrl) == ctrl; matrix at coef
@@ -41,9 +48,10 @@ struct FsStep {
     uint8_t flag = 0;
     int32_t cbit = -1;
     uint32_t coef = 0;       // offset in the coefficient table (doubles)
-    uint32_t pad = 0;
+    uint32_t ncoef = 0;      // doubles the step reads there (staged in shared memory)
     uint64_t fmask = 0, fwant = 0, cmask = 0, cwant = 0;   // guard
     uint64_t mask = 0, zmask = 0, ctrl = 0;
+    uint64_t reserved = 0;   // keeps the size a multiple of 16 bytes
     uint8_t q[32] = {};
 };
 
@@ -106,53 +114,91 @@ __device__ __forceinline__ void fs_dense(vec2_t<T>* a, int n, const FsStep& S, c
             xr[x] = static_cast<double>(v.x);
             xi[x] = static_cast<double>(v.y);
         }
-#pragma unroll
+        // rows one at a time (coefficients from shared memory), so the inputs are the only
+        // per-thread arrays held in registers
+#pragma unroll 1
         for (int y = 0; y < D; ++y) {
             double re = 0.0, im = 0.0;
+            const double2* row = reinterpret_cast<const double2*>(m) + y * D;
 #pragma unroll
             for (int x = 0; x < D; ++x) {
-                const double cr = m[2 * (y * D + x)], ci = m[2 * (y * D + x) + 1];
-                re = fma(cr, xr[x], re);
-                re = fma(-ci, xi[x], re);
-                im = fma(cr, xi[x], im);
-                im = fma(ci, xr[x], im);
+                const double2 cf = row[x];
+                re = fma(cf.x, xr[x], re);
+                re = fma(-cf.y, xi[x], re);
+                im = fma(cf.x, xi[x], im);
+                im = fma(cf.y, xr[x], im);
             }
-            a[base | off[y]] = mk<T>(static_cast<T>(re), static_cast<T>(im));
+            uint64_t oy = 0;
+#pragma unroll
+            for (int b = 0; b < K; ++b)
+                if ((y >> b) & 1) oy |= 1ull << S.q[b];
+            a[base | oy] = mk<T>(static_cast<T>(re), static_cast<T>(im));
         }
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kFsThreads) k_fs_run(const FsStep* __restrict__ steps, int n_steps,
-                                                      const double* __restrict__ coef,
+__global__ void __launch_bounds__(kFsThreads, 2) k_fs_run(const FsStep* __restrict__ steps, int n_steps,
+                                                      const double* __restrict__ coef, uint32_t n_coef, int resident,
                                                       const vec2_t<T>* __restrict__ prefix, int n, uint32_t seed,
-                                                      uint64_t shot0, uint64_t* __restrict__ out_idx,
+                                                      uint64_t shot0, uint64_t n_shots,
+                                                      uint64_t* __restrict__ out_idx,
                                                       uint64_t* __restrict__ out_cbits) {
+    // dynamic shared memory: the shot's amplitudes, its MT19937 words, and (resident) the plan
     extern __shared__ __align__(16) unsigned char fs_smem[];
     vec2_t<T>* a = reinterpret_cast<vec2_t<T>*>(fs_smem);
     const uint64_t dim = 1ull << n;
-    uint32_t* mtw = reinterpret_cast<uint32_t*>(fs_smem + dim * sizeof(vec2_t<T>));
+    const size_t amp_area = (dim * sizeof(vec2_t<T>) + 15) & ~size_t{15};
+    uint32_t* mtw = reinterpret_cast<uint32_t*>(fs_smem + amp_area);
+    uint64_t* rsteps = reinterpret_cast<uint64_t*>(fs_smem + amp_area + kFsMtBytes);
+    double* rcoef = reinterpret_cast<double*>(rsteps + static_cast<size_t>(n_steps) * (sizeof(FsStep) / 8));
     __shared__ double red[kFsThreads / 32];
     __shared__ double part[kFsThreads];
+    __shared__ uint64_t sstep[sizeof(FsStep) / 8];   // streamed plans: the current step and its
+    __shared__ __align__(16) double scoef[kFsMaxCoef];   //              coefficients, staged
     __shared__ double bc[10];
     __shared__ uint64_t cbits, flags, bx, bz;
     __shared__ uint32_t mt_idx, bny;
     __shared__ int bflag;
-    const uint64_t shot = shot0 + blockIdx.x;
     const MtView g{mtw, 1, &mt_idx};
+    static_assert(sizeof(FsStep) % 16 == 0, "FsStep is staged as 8-byte words and keeps rcoef aligned");
 
+    if (resident) {
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(steps);
+        const size_t words = static_cast<size_t>(n_steps) * (sizeof(FsStep) / 8);
+        for (size_t w = threadIdx.x; w < words; w += kFsThreads) rsteps[w] = __ldg(src + w);
+        for (uint32_t w = threadIdx.x; w < n_coef; w += kFsThreads) rcoef[w] = __ldg(coef + w);
+    }
+
+    // persistent CTAs: shots blockIdx.x, blockIdx.x + gridDim.x, ...
+    for (uint64_t shot = blockIdx.x; shot < n_shots; shot += gridDim.x) {
     for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = prefix[i];
     if (threadIdx.x == 0) {
-        g.seed(seed + static_cast<uint32_t>(shot));
+        g.seed(seed + static_cast<uint32_t>(shot0 + shot));
         cbits = 0;
         flags = 0;
     }
     __syncthreads();
 
     for (int si = 0; si < n_steps; ++si) {
-        const FsStep& S = steps[si];
-        if ((flags & S.fmask) != S.fwant || (cbits & S.cmask) != S.cwant) continue;   // uniform in the CTA
-        const double* c = coef + S.coef;
+        if (!resident) {
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(steps + si);
+            for (int w = threadIdx.x; w < static_cast<int>(sizeof(FsStep) / 8); w += kFsThreads)
+                sstep[w] = __ldg(src + w);
+            __syncthreads();
+        }
+        const FsStep& S = resident ? *reinterpret_cast<const FsStep*>(rsteps + si * (sizeof(FsStep) / 8))
+                                   : *reinterpret_cast<const FsStep*>(sstep);
+        if ((flags & S.fmask) != S.fwant || (cbits & S.cmask) != S.cwant) {   // uniform in the CTA
+            if (!resident) __syncthreads();                                      // sstep is read
+            continue;
+        }
+        const double* c = rcoef + S.coef;
+        if (!resident) {
+            for (uint32_t w = threadIdx.x; w < S.ncoef; w += kFsThreads) scoef[w] = __ldg(coef + S.coef + w);
+            __syncthreads();
+            c = scoef;
+        }
         switch (S.kind) {
             case FS_DENSE:
                 switch (S.k) {
@@ -323,7 +369,7 @@ __global__ void __launch_bounds__(kFsThreads) k_fs_run(const FsStep* __restrict_
         for (uint64_t i = lo; i < lo + per; ++i) run += tr_norm2<T>(a[i]);
     part[threadIdx.x] = run;
     __syncthreads();
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x == 0) {
     const uint32_t runs = static_cast<uint32_t>(dim >= kFsThreads ? kFsThreads : dim);
     double total = 0.0;
     for (uint32_t t = 0; t < runs; ++t) total += part[t];
@@ -346,17 +392,23 @@ __global__ void __launch_bounds__(kFsThreads) k_fs_run(const FsStep* __restrict_
         }
         if (hit) break;
     }
-    out_idx[blockIdx.x] = idx;
-    out_cbits[blockIdx.x] = cbits;
+    out_idx[shot] = idx;
+    out_cbits[shot] = cbits;
+    }
+    __syncthreads();   // the next shot overwrites the amplitudes, part[] and the engine
+    }
 }
 
 // host: the plan's steps as FsSteps; false when a step has no shared-memory form
 bool encode(const TrPlan& plan, std::vector<FsStep>& out, std::vector<double>& coef) {
-    auto guard_of = [](FsStep& f, const TrGuard& g) {
+    // every step's coefficients start on a 16-byte boundary (the dense rows are read as double2)
+    auto start = [&](FsStep& f, const TrGuard& g) {
         f.fmask = g.fmask;
         f.fwant = g.fwant;
         f.cmask = g.cmask;
         f.cwant = g.cwant;
+        if (coef.size() & 1) coef.push_back(0.0);
+        f.coef = static_cast<uint32_t>(coef.size());
     };
     auto push_c = [&](c128 v) {
         coef.push_back(v.real());
@@ -364,8 +416,7 @@ bool encode(const TrPlan& plan, std::vector<FsStep>& out, std::vector<double>& c
     };
     auto op_step = [&](const Op& o, const TrGuard& g) -> bool {
         FsStep f;
-        guard_of(f, g);
-        f.coef = static_cast<uint32_t>(coef.size());
+        start(f, g);
         switch (o.kind) {
             case OP_NOP: return true;
             case OP_DENSE:
@@ -416,9 +467,11 @@ bool encode(const TrPlan& plan, std::vector<FsStep>& out, std::vector<double>& c
             default:
                 return false;   // permutations
         }
+        f.ncoef = static_cast<uint32_t>(coef.size()) - f.coef;
         out.push_back(f);
         return true;
     };
+    auto finish = [&](FsStep& f) { f.ncoef = static_cast<uint32_t>(coef.size()) - f.coef; };
     for (const TrStep& st : plan.steps) {
         switch (st.kind) {
             case TrStep::OPS:
@@ -428,50 +481,52 @@ bool encode(const TrPlan& plan, std::vector<FsStep>& out, std::vector<double>& c
                 break;
             case TrStep::MDENSE: {
                 FsStep f;
-                guard_of(f, st.g);
+                start(f, st.g);
                 f.kind = FS_DENSE;
                 f.k = static_cast<uint8_t>(st.k);
                 for (int b = 0; b < st.k; ++b) f.q[b] = static_cast<uint8_t>(__builtin_ctzll(st.args.off[1 << b]));
-                f.coef = static_cast<uint32_t>(coef.size());
                 for (int e = 0; e < (1 << (2 * st.k)); ++e) {
                     coef.push_back(plan.mats[st.moff + e].re);
                     coef.push_back(plan.mats[st.moff + e].im);
                 }
+                finish(f);
                 out.push_back(f);
                 break;
             }
             case TrStep::MSCALE: {
                 FsStep f;
-                guard_of(f, st.g);
+                start(f, st.g);
                 f.kind = FS_SCALE;
-                f.coef = static_cast<uint32_t>(coef.size());
                 push_c(st.phase);
+                finish(f);
                 out.push_back(f);
                 break;
             }
             case TrStep::MEASURE: {
                 FsStep f;
-                guard_of(f, st.g);
+                start(f, st.g);
                 f.kind = FS_MEASURE;
                 f.q[0] = static_cast<uint8_t>(st.qubit);
                 f.cbit = st.cbit;
                 f.k = st.reset ? 1 : 0;
+                finish(f);
                 out.push_back(f);
                 break;
             }
             case TrStep::BRANCH: {
                 FsStep f;
+                start(f, TrGuard{});
                 f.kind = FS_BRANCH;
                 f.flag = static_cast<uint8_t>(st.flag);
                 f.mask = st.bmask;
                 f.zmask = st.bwant;
+                finish(f);
                 out.push_back(f);
                 break;
             }
             case TrStep::NOISE: {
                 FsStep f;
-                guard_of(f, st.g);
-                f.coef = static_cast<uint32_t>(coef.size());
+                start(f, st.g);
                 f.k = static_cast<uint8_t>(st.nq.k);
                 for (int b = 0; b < 32; ++b) f.q[b] = st.nq.q[b];
                 if (st.noise == NOISE_KRAUS) {
@@ -485,10 +540,17 @@ bool encode(const TrPlan& plan, std::vector<FsStep>& out, std::vector<double>& c
                     const size_t np = st.noise == NOISE_PAULI ? 3 : st.noise == NOISE_PAULI2 ? 15 : 1;
                     coef.insert(coef.end(), plan.noise_prm.begin() + st.poff, plan.noise_prm.begin() + st.poff + np);
                 }
+                finish(f);
                 out.push_back(f);
                 break;
             }
         }
+    }
+    for (const FsStep& f : out) {
+        if (f.ncoef > static_cast<uint32_t>(kFsMaxCoef)) return false;
+        // the kernel reads dense rows as double2 from f.coef and stages ncoef doubles
+        if ((f.coef & 1u) || static_cast<size_t>(f.coef) + f.ncoef > coef.size())
+            throw std::logic_error("fused trajectory plan: misplaced coefficients");
     }
     return true;
 }
@@ -497,9 +559,10 @@ bool encode(const TrPlan& plan, std::vector<FsStep>& out, std::vector<double>& c
 
 template <typename T>
 bool run_trajectories_fused(const TrPlan& plan, int n, const vec2_t<T>* d_prefix, uint32_t seed, size_t n_shots,
-                            uint64_t* out_idx, uint64_t* out_cbits, cudaStream_t st, uint64_t* launches) {
+                            uint64_t* out_idx, uint64_t* out_cbits, cudaStream_t st, Workspace& ws,
+                            uint64_t* launches) {
     const size_t amp_bytes = sizeof(vec2_t<T>) << n;
-    if (amp_bytes > static_cast<size_t>(kFsMaxBytes)) return false;
+    if (amp_bytes > static_cast<size_t>(kFsMaxBytes) || amp_bytes < static_cast<size_t>(kFsMinBytes)) return false;
     std::vector<FsStep> steps;
     std::vector<double> coef;
     if (!encode(plan, steps, coef)) return false;
@@ -508,61 +571,51 @@ bool run_trajectories_fused(const TrPlan& plan, int n, const vec2_t<T>* d_prefix
     constexpr uint64_t kChunk = 1ull << 20;   // shots per launch
     const uint64_t chunk = std::min<uint64_t>(kChunk, n_shots);
     const size_t steps_bytes = steps.size() * sizeof(FsStep);
-    const size_t bytes = steps_bytes + coef.size() * sizeof(double) + 16 * chunk + 64;
-    void* dbuf = nullptr;
-    if (cudaMalloc(&dbuf, bytes) != cudaSuccess) {
-        (void)cudaGetLastError();
-        throw std::bad_alloc();
+    const size_t coef_off = (steps_bytes + 15) & ~size_t{15};
+    const size_t out_off = coef_off + ((coef.size() * sizeof(double) + 15) & ~size_t{15});
+    uint8_t* p = static_cast<uint8_t*>(ws.shots(out_off + 16 * chunk));
+    FsStep* d_steps = reinterpret_cast<FsStep*>(p);
+    double* d_coef = reinterpret_cast<double*>(p + coef_off);
+    uint64_t* d_out = reinterpret_cast<uint64_t*>(p + out_off);
+    uint64_t* d_cb = d_out + chunk;
+    uint64_t* h = reinterpret_cast<uint64_t*>(ws.host_result(2 * chunk));
+    if (!steps.empty())
+        check_cuda(cudaMemcpyAsync(d_steps, steps.data(), steps_bytes, cudaMemcpyHostToDevice, st), "steps H2D");
+    check_cuda(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, st),
+               "coefficients H2D");
+    // the plan stays in shared memory when it fits next to the amplitudes, else each step is
+    // staged from global memory as it comes
+    const size_t prog_bytes = steps_bytes + coef.size() * sizeof(double);
+    const size_t amp_area = (amp_bytes + 15) & ~size_t{15};
+    const int resident = amp_area + kFsMtBytes + prog_bytes <= kFsResidentMax ? 1 : 0;
+    const size_t smem = amp_area + kFsMtBytes + (resident ? prog_bytes : 0);
+    check_cuda(cudaFuncSetAttribute(k_fs_run<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+               "fused trajectory smem");
+    int dev = 0, sms = 0, per_sm = 0;
+    check_cuda(cudaGetDevice(&dev), "device");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs_run<T>, kFsThreads, smem), "occupancy");
+    const uint64_t resident_ctas = static_cast<uint64_t>(sms) * std::max(per_sm, 1);
+    for (uint64_t s0 = 0; s0 < n_shots; s0 += chunk) {
+        const uint64_t nb = std::min<uint64_t>(chunk, n_shots - s0);
+        const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(nb, resident_ctas));
+        k_fs_run<T><<<grid, kFsThreads, smem, st>>>(d_steps, static_cast<int>(steps.size()), d_coef,
+                                                    static_cast<uint32_t>(coef.size()), resident, d_prefix, n, seed,
+                                                    s0, nb, d_out, d_cb);
+        check_cuda(cudaGetLastError(), "fused trajectory launch");
+        check_cuda(cudaMemcpyAsync(h, d_out, 8 * nb, cudaMemcpyDeviceToHost, st), "D2H");
+        check_cuda(cudaMemcpyAsync(h + chunk, d_cb, 8 * nb, cudaMemcpyDeviceToHost, st), "D2H");
+        check_cuda(cudaStreamSynchronize(st), "fused trajectories");   // the host copies and the
+        std::memcpy(out_idx + s0, h, 8 * nb);                          // step upload are done
+        std::memcpy(out_cbits + s0, h + chunk, 8 * nb);
+        if (launches) ++*launches;
     }
-    void* hbuf = nullptr;
-    if (cudaMallocHost(&hbuf, 16 * chunk) != cudaSuccess) {
-        (void)cudaGetLastError();
-        cudaFree(dbuf);
-        throw std::bad_alloc();
-    }
-    auto release = [&] {
-        cudaStreamSynchronize(st);
-        cudaFree(dbuf);
-        cudaFreeHost(hbuf);
-    };
-    try {
-        uint8_t* p = static_cast<uint8_t*>(dbuf);
-        FsStep* d_steps = reinterpret_cast<FsStep*>(p);
-        double* d_coef = reinterpret_cast<double*>(p + ((steps_bytes + 15) & ~size_t{15}));
-        uint64_t* d_out = reinterpret_cast<uint64_t*>(
-            reinterpret_cast<uint8_t*>(d_coef) + ((coef.size() * sizeof(double) + 15) & ~size_t{15}));
-        uint64_t* d_cb = d_out + chunk;
-        if (!steps.empty())
-            check_cuda(cudaMemcpyAsync(d_steps, steps.data(), steps_bytes, cudaMemcpyHostToDevice, st), "steps H2D");
-        check_cuda(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, st),
-                   "coefficients H2D");
-        const size_t smem = amp_bytes + sizeof(uint32_t) * kMtN;
-        check_cuda(cudaFuncSetAttribute(k_fs_run<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smem)), "fused trajectory smem");
-        uint64_t* h = static_cast<uint64_t*>(hbuf);
-        for (uint64_t s0 = 0; s0 < n_shots; s0 += chunk) {
-            const uint64_t nb = std::min<uint64_t>(chunk, n_shots - s0);
-            k_fs_run<T><<<static_cast<unsigned>(nb), kFsThreads, smem, st>>>(
-                d_steps, static_cast<int>(steps.size()), d_coef, d_prefix, n, seed, s0, d_out, d_cb);
-            check_cuda(cudaGetLastError(), "fused trajectory launch");
-            check_cuda(cudaMemcpyAsync(h, d_out, 8 * nb, cudaMemcpyDeviceToHost, st), "D2H");
-            check_cuda(cudaMemcpyAsync(h + chunk, d_cb, 8 * nb, cudaMemcpyDeviceToHost, st), "D2H");
-            check_cuda(cudaStreamSynchronize(st), "fused trajectories");
-            std::memcpy(out_idx + s0, h, 8 * nb);
-            std::memcpy(out_cbits + s0, h + chunk, 8 * nb);
-            if (launches) ++*launches;
-        }
-    } catch (...) {
-        release();
-        throw;
-    }
-    release();
     return true;
 }
 
 template bool run_trajectories_fused<double>(const TrPlan&, int, const double2*, uint32_t, size_t, uint64_t*,
-                                             uint64_t*, cudaStream_t, uint64_t*);
+                                             uint64_t*, cudaStream_t, Workspace&, uint64_t*);
 template bool run_trajectories_fused<float>(const TrPlan&, int, const float2*, uint32_t, size_t, uint64_t*,
-                                            uint64_t*, cudaStream_t, uint64_t*);
+                                            uint64_t*, cudaStream_t, Workspace&, uint64_t*);
 
 }  // namespace qsv

@@ -152,7 +152,7 @@ struct TrajOptions {
     int fusion_max = 3;           // fusion of the gates every shot applies
     int fusion_min = 12;
     uint64_t max_batch_shots = 0; // shots per device batch (0: as many as half the free memory holds,
-                                  // and registers of at most 64 KiB run shot by shot in shared memory)
+                                  // and registers of 4 to 64 KiB run shot by shot in shared memory)
     const std::vector<NoiseSpec>* noise = nullptr;   // per gate type; null or empty: noiseless
 };
 // Run n_shots trajectories of `suffix` from the n-qubit device state d_prefix (left unchanged):

@@ -66,12 +66,13 @@ struct TrPlan {
 TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion_max, int fusion_min,
                   const std::vector<NoiseSpec>* noise);
 
-// Whole shots in one CTA's shared memory, for registers of at most 64 KiB (kern_traj_fused.cu).
+// Whole shots in one CTA's shared memory, for registers of 4 to 64 KiB (kern_traj_fused.cu).
 // Returns false, having done nothing, when the register is too wide or the plan holds a step the
 // kernel does not run (a permutation, a dense block wider than four qubits).
 template <typename T>
 bool run_trajectories_fused(const TrPlan& plan, int n, const vec2_t<T>* d_prefix, uint32_t seed, size_t n_shots,
-                            uint64_t* out_idx, uint64_t* out_cbits, cudaStream_t st, uint64_t* launches);
+                            uint64_t* out_idx, uint64_t* out_cbits, cudaStream_t st, Workspace& ws,
+                            uint64_t* launches);
 
 #ifdef __CUDACC__
 

@@ -437,7 +437,7 @@ class B200Simulator:
             keys, cnt = np.unique(idx, return_counts=True)
             res.counts = {int(k): int(c) for k, c in zip(keys, cnt)}
         bits = ((regs[:, None] >> np.arange(width, dtype=np.uint64)[None, :]) & np.uint64(1)).astype(bool)
-        res.cbit_history = [list(map(bool, row)) for row in bits]
+        res.cbit_history = bits.tolist()
         return res
 
     def _sample_result(self, reg, commands, n_qubits, n_shots, base_s) -> SamplingResult:
@@ -456,7 +456,7 @@ class B200Simulator:
             hist = np.zeros((int(n_shots), res.n_cbits), dtype=bool)
             for q, cb in recorded:
                 hist[:, cb] = ((idx >> np.uint64(q)) & np.uint64(1)).astype(bool)
-            res.cbit_history = [list(map(bool, row)) for row in hist]
+            res.cbit_history = hist.tolist()
         return res
 
     def batch_run(self, commands, n_qubits: int, n_shots: int, param_sets, seed=None):
