@@ -18,9 +18,10 @@ Also reported on the same line:
   * structured_and_readouts: a phase-estimation-shaped structured program (controlled powers
     + inverse QFT) at 28 and 22 qubits with the reference's CPU program_statevector at 22, the
     exact Born readout and the PauliAveraging parity counts on the device;
-  * trajectories: a 16-qubit feed-forward circuit (a mid-circuit measurement and a conditioned
-    gate per layer) sampled shot by shot on the device, noiseless and noisy, against the
-    reference's CPU run() on a bounded number of shots, with the per-shot registers compared.
+  * trajectories: feed-forward circuits (a mid-circuit measurement and a conditioned gate per
+    layer) at 16 qubits (batched executor) and 10 qubits (shared-memory executor) sampled shot
+    by shot on the device, noiseless and noisy, against the reference's CPU run() on a bounded
+    number of shots, with the per-shot registers compared.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 """

@@ -177,20 +177,23 @@ def structured_rows(device: int = 0, n_big: int = 28, n_small: int = 22, shots: 
     return out
 
 
-def trajectory_rows(device: int = 0, n: int = 16, depth: int = 8, shots: int = 4096, ref_shots: int = 256,
+def trajectory_rows(device: int = 0, shapes=((16, 8, 4096), (10, 8, 20000)), ref_shots: int = 256,
                     seed: int = 1234) -> dict:
-    """The trajectory path: ``circuits.feedforward(n, depth)`` sampled shot by shot on the device,
-    noiseless and under depolarizing noise on every 1q/2q gate plus amplitude damping on U, and
-    the reference CPU simulator's own run() (oracle/_ref, all host threads) on the first
-    ``ref_shots`` shots of each — whose per-shot classical registers must equal the device's,
-    since shot s draws from std::mt19937(seed + s) on both."""
+    """The trajectory path: ``circuits.feedforward(n, depth)`` sampled shot by shot through
+    ``B200Simulator.run`` for each (n, depth, shots) shape — 16 qubits on the batched executor,
+    10 qubits on the shared-memory executor — noiseless and under depolarizing noise on every
+    1q/2q gate plus amplitude damping on U, with the reference CPU simulator's own run()
+    (oracle/_ref, all host threads) on the first ``ref_shots`` shots of each; their per-shot
+    classical registers must equal the device's, since shot s draws from std::mt19937(seed + s)
+    on both."""
     from . import B200Simulator
     from .ir import pack
     from .noise import _FULL_1Q, _FULL_2Q, NoiseModel
-    cmds = circuits.feedforward(n, depth, seed)
     noisy_model = NoiseModel.depolarizing(0.01, "all") + NoiseModel.amplitude_damping(0.02, ["U"])
-    out = {"workload": f"feedforward n={n} depth={depth}: a mid-circuit measurement and a conditioned X "
-                       f"per layer", "shots": shots}
+    noisy_specs = [("depolarizing", 0.01, [int(g) for g in _FULL_1Q + _FULL_2Q]),
+                   ("amplitude_damping", 0.02, [int(ir.GateType.U)])]
+    out = {"workload": "feedforward: per layer U on every qubit, CX pairs, RZZ, a mid-circuit measurement "
+                       "and a conditioned X"}
     ref = None
     try:
         import os
@@ -199,35 +202,31 @@ def trajectory_rows(device: int = 0, n: int = 16, depth: int = 8, shots: int = 4
         out["reference_cpu_cores"] = ref.set_threads(os.cpu_count() or 1)
     except (FileNotFoundError, ImportError, OSError):
         out["reference_cpu"] = "oracle/_ref not built on this machine"
-    for label, model in (("noiseless", None), ("noisy", noisy_model)):
-        sim = B200Simulator(noise_model=model, device=device)
-        sim.run(cmds, n, shots, seed)                       # warm: allocations, kernels
-        times = []
-        for _ in range(3):
-            t0 = time.perf_counter()
-            res = sim.run(cmds, n, shots, seed)
-            times.append(time.perf_counter() - t0)
-        dt = float(np.median(times))
-        row = {"s": dt, "shots_per_s": shots / dt}
-        if ref is not None:
-            buf = pack(cmds).buf
-            specs = [] if model is None else [
-                ("depolarizing", 0.01, [int(g) for g in _FULL_1Q + _FULL_2Q]),
-                ("amplitude_damping", 0.02, [int(ir.GateType.U)])]
-            t0 = time.perf_counter()
-            if specs:
-                _c, hist, width = ref.run_noisy(buf, n, ref_shots, seed, specs)
-            else:
-                _c, hist, width = ref.run_history(buf, n, ref_shots, seed)
-            rdt = time.perf_counter() - t0
-            row["reference_cpu_shots_per_s"] = ref_shots / rdt
-            row["speedup"] = row["shots_per_s"] / row["reference_cpu_shots_per_s"]
-            mine = np.zeros(ref_shots, dtype=np.uint64)
-            for s_, bits in enumerate(res.cbit_history[:ref_shots]):
-                for c, v in enumerate(bits):
-                    if v:
-                        mine[s_] |= np.uint64(1) << np.uint64(c)
-            row["registers_equal_reference"] = bool(np.array_equal(mine, np.asarray(hist, dtype=np.uint64)))
-        out[label] = row
-        sim.close()
+    for n, depth, shots in shapes:
+        cmds = circuits.feedforward(n, depth, seed)
+        buf = pack(cmds).buf
+        for label, model in (("noiseless", None), ("noisy", noisy_model)):
+            sim = B200Simulator(noise_model=model, device=device)
+            sim.run(cmds, n, shots, seed)                       # warm: allocations, kernels
+            times = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                res = sim.run(cmds, n, shots, seed)
+                times.append(time.perf_counter() - t0)
+            dt = float(np.median(times))
+            row = {"shots": shots, "s": dt, "shots_per_s": shots / dt}
+            if ref is not None:
+                t0 = time.perf_counter()
+                if model is not None:
+                    _c, hist, _w = ref.run_noisy(buf, n, ref_shots, seed, noisy_specs)
+                else:
+                    _c, hist, _w = ref.run_history(buf, n, ref_shots, seed)
+                rdt = time.perf_counter() - t0
+                row["reference_cpu_shots_per_s"] = ref_shots / rdt
+                row["speedup"] = row["shots_per_s"] / row["reference_cpu_shots_per_s"]
+                bits = np.asarray(res.cbit_history[:ref_shots], dtype=np.uint64).reshape(ref_shots, -1)
+                mine = (bits << np.arange(bits.shape[1], dtype=np.uint64)[None, :]).sum(axis=1, dtype=np.uint64)
+                row["registers_equal_reference"] = bool(np.array_equal(mine, np.asarray(hist, dtype=np.uint64)))
+            out[f"n{n}_depth{depth}_{label}"] = row
+            sim.close()
     return out
