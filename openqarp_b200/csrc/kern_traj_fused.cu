@@ -138,7 +138,7 @@ __device__ __forceinline__ void fs_dense(vec2_t<T>* a, int n, const FsStep& S, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kFsThreads, 2) k_fs_run(const FsStep* __restrict__ steps, int n_steps,
+__global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restrict__ steps, int n_steps,
                                                       const double* __restrict__ coef, uint32_t n_coef, int resident,
                                                       const vec2_t<T>* __restrict__ prefix, int n, uint32_t seed,
                                                       uint64_t shot0, uint64_t n_shots,
@@ -591,6 +591,8 @@ bool run_trajectories_fused(const TrPlan& plan, int n, const vec2_t<T>* d_prefix
     const size_t smem = amp_area + kFsMtBytes + (resident ? prog_bytes : 0);
     check_cuda(cudaFuncSetAttribute(k_fs_run<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                "fused trajectory smem");
+    check_cuda(cudaFuncSetAttribute(k_fs_run<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared), "fused trajectory carveout");
     int dev = 0, sms = 0, per_sm = 0;
     check_cuda(cudaGetDevice(&dev), "device");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");

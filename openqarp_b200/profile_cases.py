@@ -8,6 +8,7 @@
     python -m openqarp_b200.profile_cases exact --n 26
     python -m openqarp_b200.profile_cases parity --n 26 --shots 1048576 --terms 512
     python -m openqarp_b200.profile_cases perm --n 26
+    python -m openqarp_b200.profile_cases traj --n 16 --depth 8 --shots 4096 [--noisy] [--batch 0]
 
 Registers of 2^26 complex128 amplitudes (1 GiB) exceed L2 (126 MB), so DRAM counters are
 meaningful, and stay small enough for a full-set capture to end within minutes.
@@ -24,7 +25,7 @@ from . import Register, circuits, ir, observable
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["dense", "brickwork", "transition", "adjoint", "sample", "exact", "parity",
-                                     "perm"])
+                                     "perm", "traj"])
     ap.add_argument("--n", type=int, default=26)
     ap.add_argument("--k", type=int, default=3)
     ap.add_argument("--reps", type=int, default=5)
@@ -34,6 +35,8 @@ def main(argv=None):
     ap.add_argument("--shots", type=int, default=100000)
     ap.add_argument("--dtype", default="complex128")
     ap.add_argument("--executor", type=int, default=-1)
+    ap.add_argument("--noisy", action="store_true")
+    ap.add_argument("--batch", type=int, default=0, help="trajectory shots per batch (0: default executor)")
     a = ap.parse_args(argv)
     rng = np.random.default_rng(7)
     reg = Register(a.n, a.dtype)
@@ -76,6 +79,15 @@ def main(argv=None):
         reg.configure(0, 0, 0)
         for _ in range(a.reps):
             reg.apply(ir.pack([rec]).buf)
+    elif a.case == "traj":
+        from .noise import NoiseModel
+        if a.noisy:
+            reg.set_noise(NoiseModel.depolarizing(0.01, "all") + NoiseModel.amplitude_damping(0.02, ["U"]))
+        reg.set_trajectory_batch(a.batch)
+        buf = ir.pack(circuits.feedforward(a.n, a.depth, 1234)).buf
+        for _ in range(a.reps):
+            reg.reset()
+            reg.run_trajectories(buf, 1234, a.shots)
     reg.synchronize()
     reg.close()
     print("ok", a.case)
