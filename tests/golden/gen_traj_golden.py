@@ -33,6 +33,11 @@ CASES = {   # name -> (n_qubits, shots, seed)
     "noisy_branches": (7, 1000, 6),
     "noisy_terminal": (6, 1000, 12),
     "noisy_wide_mcz": (17, 48, 31),
+    # 4-64 KiB registers: the shared-memory executor
+    "branches9": (9, 1000, 41),
+    "noisy_branches9": (9, 800, 42),
+    "noisy_feedforward10": (10, 800, 43),
+    "reset_chain12": (12, 300, 44),
 }
 
 _1Q = ("X", "Y", "Z", "H", "S", "Sdg", "T", "Tdg", "SX", "SXdg", "Id", "Rx", "Ry", "Rz", "P", "U")
@@ -54,6 +59,10 @@ def noise_specs(name: str):
         return [("bit_flip", 0.05, _1Q), ("depolarizing", 0.1, ("CX", "RZZ"))]
     if name == "noisy_wide_mcz":
         return [("depolarizing", 0.9, ("MCZ",)), ("depolarizing", 0.02, ("CX",))]
+    if name == "noisy_branches9":
+        return noise_specs("noisy_branches")
+    if name == "noisy_feedforward10":
+        return [("depolarizing", 0.02, _1Q + _2Q), ("amplitude_damping", 0.05, ("U",))]
     return []
 
 
@@ -140,6 +149,13 @@ def traj_case(name: str):
         cmds += [Command(G.MCZ, tuple(qs)), Command(G.MCZ, tuple(qs[1:])), Command(G.MCZ, tuple(qs[2:])),
                  Command(G.MCZ, tuple(qs[:3])), M(0, 0), C(G.MCZ, tuple(qs[::-1]), (0,), (True,))]
         cmds += _layer(rng, n) + [Command(G.MCZ, tuple(qs)), M(1, 1), M(16, 2)]
+    elif name in ("branches9", "noisy_branches9"):
+        return n, traj_case("branches")[1], shots, seed
+    elif name == "noisy_feedforward10":
+        from openqarp_b200 import circuits
+        cmds = circuits.feedforward(n, 4, seed)
+    elif name == "reset_chain12":
+        cmds = traj_case("reset_chain")[1] + _layer(rng, n) + [M(q, q % 3) for q in range(7, n)]
     elif name == "dead_conditions":
         cmds = _layer(rng, n) + [M(0, 0)]
         cmds += [C(G.X, (1,), (3,), (True,)),                          # reads a cbit nothing wrote

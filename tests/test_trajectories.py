@@ -205,9 +205,11 @@ def test_trajectories_match_reference(sim, traj_golden, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["branches", "noisy_branches"])
+@pytest.mark.parametrize("name", ["branches", "noisy_branches", "branches9", "noisy_feedforward10"])
 def test_trajectories_independent_of_batch(name):
-    """Shots run in batches of the device register; the batch size changes no result."""
+    """Shots run in batches of the device register; the batch size changes no result.  A set
+    batch size also keeps 4-64 KiB registers off the shared-memory executor, so for those cases
+    this compares the two executors."""
     n, cmds, shots, seed = traj_case(name)
     s = _sim_for(name)
     try:
@@ -252,7 +254,7 @@ def test_trajectories_from_initial_state(sim):
 def test_trajectories_complex64_follow_complex128(traj_golden):
     """complex64 storage: per-shot decisions compare float-rounded probabilities with the same
     uniforms, so almost every shot takes the complex128 path."""
-    for name in ("teleport", "branches", "wide", "noisy_damping"):
+    for name in ("teleport", "branches", "wide", "noisy_damping", "branches9", "noisy_feedforward10"):
         n, cmds, shots, seed = traj_case(name)
         s = _sim_for(name, "complex64")
         try:
@@ -280,3 +282,108 @@ def test_trajectory_edge_cases(sim):
         sim.run([Command(G.H, (0,)), M, Command(G.BranchElse, ())], 1 + 1, 4, 1)
     with pytest.raises(RuntimeError, match="unterminated BranchBegin"):
         sim.run([Command(G.H, (0,)), M, Command(G.BranchBegin, (), (), None, (), (1,), (True,))], 2, 4, 1)
+
+
+# ---------------------------------------------------------------- shots sharded over ranks
+
+def test_shot_ranges_cover_in_order():
+    from openqarp_b200.shots import shot_range
+    for n, w in ((10, 3), (2, 4), (0, 2), (1000, 8)):
+        ranges = [shot_range(n, r, w) for r in range(w)]
+        assert ranges[0][0] == 0 and ranges[-1][1] == n
+        assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
+        assert max(h - l for l, h in ranges) - min(h - l for l, h in ranges) <= 1
+
+
+class _HostSim:
+    """The pieces of B200Simulator that run_sharded uses, with the reference as the runner."""
+
+    def _noise_active(self):
+        return False
+
+    @staticmethod
+    def _counts_result(n_qubits, n_shots, idx, regs, width):
+        from openqarp_b200.simulator import B200Simulator
+        return B200Simulator._counts_result(n_qubits, n_shots, idx, regs, width)
+
+
+def _reference_runner(name):
+    """(seed, count) -> per-shot outcomes and registers of the reference's run(), for a case
+    whose outcomes are all distinct per shot so that counts pin each shot's index."""
+    from oracle.oracle import Reference
+    from openqarp_b200.ir import pack
+    ref = Reference()
+    n, cmds, _shots, _seed = traj_case(name)
+    buf = pack(cmds).buf
+
+    def run(seed, count):
+        counts, hist, width = ref.run_history(buf, n, count, seed)
+        return counts, hist, width
+    return run
+
+
+def _sharded_worker(rank, world, port, out_path):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from openqarp_b200.shots import run_sharded
+    name = "branches"
+    n, cmds, shots, seed = traj_case(name)
+    ref_run = _reference_runner(name)
+    seen = {}
+
+    def runner(seed_, count):
+        counts, hist, width = ref_run(seed_, count)
+        seen["counts"] = counts
+        return np.zeros(count, dtype=np.uint64), hist, width
+    res = run_sharded(_HostSim(), cmds, n, shots, seed, rank, world, dist=dist, runner=runner)
+    np.save(f"{out_path}.{rank}.npy", _masks(res.cbit_history, res.n_cbits))
+    gathered = [None] * world
+    dist.all_gather_object(gathered, seen["counts"])
+    if rank == 0:
+        total = {}
+        for c in gathered:
+            for k, v in c.items():
+                total[k] = total.get(k, 0) + v
+        np.save(f"{out_path}.counts.npy", np.array(sorted(total.items()), dtype=np.int64))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_shots_gloo_world2(tmp_path, traj_golden, reference):
+    """Two gloo ranks, each running its contiguous share of the shots with seed + first shot,
+    gather exactly the single run's per-shot registers and counts (the reference stands in for
+    the GPU runner)."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "res")
+    mp.spawn(_sharded_worker, args=(2, port, out), nprocs=2, join=True)
+    for r in range(2):
+        np.testing.assert_array_equal(np.load(f"{out}.{r}.npy"), traj_golden["branches_hist"])
+    counts = {int(k): int(v) for k, v in np.load(f"{out}.counts.npy")}
+    assert counts == _counts(traj_golden, "branches")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["noisy_branches", "noisy_feedforward10"])
+def test_shot_ranges_reproduce_the_full_run(name):
+    """A rank's share [lo, hi) run with seed + lo gives exactly shots lo..hi-1 of the full run
+    (what run_sharded relies on), on the batched and the shared-memory executor."""
+    from openqarp_b200.shots import run_sharded, shot_range
+    n, cmds, shots, seed = traj_case(name)
+    s = _sim_for(name)
+    try:
+        full = s.run(cmds, n, shots, seed)
+        for rank in range(3):
+            lo, hi = shot_range(shots, rank, 3)
+            part = s.run(cmds, n, hi - lo, seed + lo)
+            assert part.cbit_history == full.cbit_history[lo:hi]
+            np.testing.assert_array_equal(part.outcomes, full.outcomes[lo:hi])
+        one = run_sharded(s, cmds, n, shots, seed, 0, 1)
+        assert one.cbit_history == full.cbit_history and one.counts == full.counts
+    finally:
+        s.close()
