@@ -18,6 +18,8 @@ Also reported on the same line:
   * structured_and_readouts: a phase-estimation-shaped structured program (controlled powers
     + inverse QFT) at 28 and 22 qubits with the reference's CPU program_statevector at 22, the
     exact Born readout and the PauliAveraging parity counts on the device;
+  * plain_12q_latency: the CPU-runnable 12-qubit configuration (HEA, 64-term <H>, 4000 shots)
+    as microseconds per statevector / expectation / run call, beside the reference's calls;
   * trajectories: feed-forward circuits (a mid-circuit measurement and a conditioned gate per
     layer) at 16 qubits (batched executor) and 10 qubits (shared-memory executor) sampled shot
     by shot on the device, noiseless and noisy, against the reference's CPU run() on a bounded
@@ -533,6 +535,10 @@ def b200_arm(args, rank, world, local_rank):
             reg.close()
             from openqarp_b200.workloads import structured_rows
             structured = structured_rows(device=device)
+        plain12 = None
+        if not args.skip_structured:
+            from openqarp_b200.workloads import config1_latency
+            plain12 = config1_latency(device=device)
         traj = None
         if not args.skip_trajectories:
             reg.close()
@@ -578,6 +584,7 @@ def b200_arm(args, rank, world, local_rank):
             "qaoa_batched": qaoa,
             "structured_and_readouts": structured,
             "trajectories": traj,
+            "plain_12q_latency": plain12,
         }
     else:
         reg.close()

@@ -230,3 +230,49 @@ def trajectory_rows(device: int = 0, shapes=((16, 8, 4096), (10, 8, 20000)), ref
             out[f"n{n}_depth{depth}_{label}"] = row
             sim.close()
     return out
+
+
+def config1_latency(device: int = 0, n: int = 12, layers: int = 10, n_terms: int = 64, shots: int = 4000,
+                    seed: int = 1234, reps: int = 50) -> dict:
+    """The plain 12-qubit configuration: an HEA of ``layers`` Ry Rz layers with a CX ladder
+    (angles seeded uniform on [0, 2 pi)), <H> of a random ``n_terms``-term Pauli sum (each qubit
+    I/X/Y/Z uniform, coefficients N(0, 1)) and ``shots`` seeded samples of all qubits, through
+    ``B200Simulator`` (statevector to host, expectation, run) — microseconds per call, median
+    of ``reps`` — next to the reference CPU simulator's own calls on the host cores.  A 64 KiB
+    register: every call is launch- and transfer-latency bound."""
+    from . import B200Simulator
+    from .ir import pack
+    cmds, vals, names = circuits.hea(n, layers, seed=seed)
+    concrete = [ir.Command(c.gate, c.qubits, tuple(p.evaluate(vals) for p in c.params)) for c in cmds]
+    obs = circuits.random_pauli_sum(n, n_terms, seed=seed + 1)
+    sim = B200Simulator(device=device)
+
+    def med_us(f):
+        f()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            f()
+            ts.append(time.perf_counter() - t0)
+        return 1e6 * float(np.median(ts))
+
+    out = {"workload": f"HEA n={n} layers={layers}, {n_terms}-term Pauli sum, {shots} shots",
+           "statevector_us": med_us(lambda: sim.statevector(concrete, n)),
+           "expectation_us": med_us(lambda: sim.expectation(concrete, n, obs)),
+           "run_us": med_us(lambda: sim.run(concrete + [ir.Command(ir.GateType.Measure, (q,), (), None, (q,))
+                                                        for q in range(n)], n, shots, seed))}
+    sim.close()
+    try:
+        import os
+        from oracle.oracle import Reference
+        ref = Reference()
+        out["reference_cpu_cores"] = ref.set_threads(os.cpu_count() or 1)
+        buf = pack(concrete).buf
+        mbuf = pack(concrete + [ir.Command(ir.GateType.Measure, (q,), (), None, (q,)) for q in range(n)]).buf
+        masks = observable.to_masks(obs, n)
+        out["reference_statevector_us"] = med_us(lambda: ref.statevector(buf, n))
+        out["reference_expectation_us"] = med_us(lambda: ref.expectation(buf, n, masks))
+        out["reference_run_us"] = med_us(lambda: ref.run(mbuf, n, shots, seed))
+    except (FileNotFoundError, ImportError, OSError):
+        out["reference_cpu"] = "oracle/_ref not built on this machine"
+    return out
