@@ -183,17 +183,39 @@ __global__ void k_tr_decide(const uint8_t* __restrict__ pass, const double* __re
 
 // ---------------------------------------------------------------- noise channels
 
-// Pauli channels (tr_choose_pauli): each passing shot draws its string; the shots where a
-// non-identity string fired are appended to `active` with their X mask, Z mask and Y count.
-__global__ void k_tr_noise_pauli(const uint8_t* __restrict__ pass, MtState mt, int n_shots, int kind,
-                                 const double* __restrict__ prm, const __grid_constant__ TrQubits tq,
+// One Pauli channel of a group: kind, qubits, parameters at poff in the noise table.
+struct TrChannelDev {
+    int32_t kind;
+    int32_t k;
+    uint32_t poff;
+    uint32_t pad;
+    uint8_t q[32];
+};
+
+// A group of Pauli channels on disjoint qubits that follow one another in the plan with one
+// guard (tr_choose_pauli for each, in order): each passing shot draws every channel's string and
+// the product — X masks or-ed, Z masks or-ed, Y counts added, exact for disjoint supports — is
+// one Pauli string; the shots where it is not the identity are appended to `active`.
+__global__ void k_tr_noise_group(const uint8_t* __restrict__ pass, MtState mt, int n_shots,
+                                 const TrChannelDev* __restrict__ ch, int n_ch, const double* __restrict__ prm,
                                  uint64_t* __restrict__ ax, uint64_t* __restrict__ az, uint32_t* __restrict__ any,
                                  uint32_t* __restrict__ active, uint32_t* __restrict__ n_active) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots || !pass[s]) return;
-    uint64_t x, z;
-    uint32_t ny;
-    tr_choose_pauli(kind, prm, tq, mt.of(s), x, z, ny);
+    const MtView g = mt.of(s);
+    uint64_t x = 0, z = 0;
+    uint32_t ny = 0;
+    for (int c = 0; c < n_ch; ++c) {
+        TrQubits tq;
+        tq.k = ch[c].k;
+        for (int b = 0; b < 32; ++b) tq.q[b] = ch[c].q[b];
+        uint64_t xi, zi;
+        uint32_t nyi;
+        tr_choose_pauli(ch[c].kind, prm + ch[c].poff, tq, g, xi, zi, nyi);
+        x |= xi;
+        z |= zi;
+        ny += nyi;
+    }
     if (x | z) {
         ax[s] = x;
         az[s] = z;
@@ -554,10 +576,25 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
         }
     };
 
+    // Noise steps wait in `pending` while later gates of the segment act on other qubits: a
+    // channel on qubits Q commutes with a unitary on qubits disjoint from Q (Pauli strings and
+    // Kraus operators alike, and the Kraus probabilities depend only on the reduced state of Q),
+    // so the segment keeps fusing.  They are emitted, in their own order, before the first gate
+    // that touches their qubits and before any step that draws or reads cbits, so every shot
+    // still consumes its draws in the reference's order.
+    std::vector<TrStep> pending;
+    uint64_t pending_q = 0;
+    auto flush_all = [&] {
+        flush();
+        for (TrStep& p : pending) plan.steps.push_back(std::move(p));
+        pending.clear();
+        pending_q = 0;
+    };
+
     for (const Cmd& c : suffix) {
         const int g = c.gate;
         if (g == BRANCH_BEGIN) {
-            flush();
+            flush_all();
             if (open_want.size() >= 64)
                 throw capability_error("trajectory: branches nested deeper than 64 levels");
             TrStep st;
@@ -574,12 +611,12 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
             continue;
         }
         if (g == BRANCH_ELSE) {
-            flush();
+            flush_all();
             open_want.back() = 0;
             continue;
         }
         if (g == BRANCH_END) {
-            flush();
+            flush_all();
             open_want.pop_back();
             continue;
         }
@@ -587,7 +624,7 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
         TrGuard guard = branch_guard();
         condition_of(c, n_cbits, &guard.cmask, &guard.cwant, &guard.never);
         if (g == MEASURE || g == RESET) {
-            flush();
+            flush_all();
             if (c.q.empty())
                 throw std::runtime_error(std::string("trajectory: ") + (g == MEASURE ? "Measure" : "Reset") +
                                          " requires a qubit");
@@ -613,14 +650,16 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
         gate.cond_bits.clear();
         gate.cond_values.clear();
         gate.flags &= ~1;
-        if (!seg.empty() && !(guard == seg_guard)) flush();
+        uint64_t qmask = 0;
+        for (uint32_t q : c.q) qmask |= q < 64 ? 1ull << q : 0;
+        if ((!seg.empty() || !pending.empty()) && !(guard == seg_guard)) flush_all();
+        if (qmask & pending_q) flush_all();
         seg_guard = guard;
         seg.push_back(std::move(gate));
         // the channel attached to the gate type runs after the gate, on the shots that applied it
         if (!noisy || noise_exempt(g) || static_cast<size_t>(g) >= noise->size()) continue;
         const NoiseSpec& ch = (*noise)[static_cast<size_t>(g)];
         if (ch.kind == NOISE_NONE) continue;
-        flush();
         if (guard.never) continue;
         const int k = static_cast<int>(c.q.size());
         TrStep st;
@@ -644,9 +683,10 @@ TrPlan build_plan(const std::vector<Cmd>& suffix, int n, int n_cbits, int fusion
         }
         st.poff = plan.noise_prm.size();
         plan.noise_prm.insert(plan.noise_prm.end(), ch.p.begin(), ch.p.end());
-        plan.steps.push_back(std::move(st));
+        pending.push_back(std::move(st));
+        pending_q |= qmask;
     }
-    flush();
+    flush_all();
     return plan;
 }
 
@@ -764,6 +804,43 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
                                    cudaMemcpyHostToDevice, st), "noise parameters");
     const MtState mt{d_mt, d_mtidx, B};
 
+    // consecutive Pauli noise steps with one guard and disjoint qubits run as one group
+    std::vector<TrChannelDev> chans;
+    std::vector<uint32_t> group_len(plan.steps.size(), 0), group_off(plan.steps.size(), 0);
+    for (size_t i = 0; i < plan.steps.size();) {
+        const TrStep& a = plan.steps[i];
+        if (a.kind != TrStep::NOISE || a.noise == NOISE_KRAUS) {
+            ++i;
+            continue;
+        }
+        size_t j = i;
+        group_off[i] = static_cast<uint32_t>(chans.size());
+        uint64_t used = 0;   // a group's supports must be disjoint for the product rule
+        auto support = [](const TrStep& t) {
+            uint64_t m = 0;
+            for (int b = 0; b < t.nq.k && b < 32; ++b) m |= 1ull << t.nq.q[b];
+            return m;
+        };
+        while (j < plan.steps.size() && plan.steps[j].kind == TrStep::NOISE && plan.steps[j].noise != NOISE_KRAUS &&
+               plan.steps[j].g == a.g && !(support(plan.steps[j]) & used)) {
+            used |= support(plan.steps[j]);
+            TrChannelDev cd{};
+            cd.kind = plan.steps[j].noise;
+            cd.k = plan.steps[j].nq.k;
+            cd.poff = static_cast<uint32_t>(plan.steps[j].poff);
+            for (int b = 0; b < 32; ++b) cd.q[b] = plan.steps[j].nq.q[b];
+            chans.push_back(cd);
+            ++j;
+        }
+        group_len[i] = static_cast<uint32_t>(j - i);
+        i = j;
+    }
+    DeviceBuffer chan_buf(chans.size() * sizeof(TrChannelDev));
+    TrChannelDev* d_chans = static_cast<TrChannelDev*>(chan_buf.p);
+    if (!chans.empty())
+        check_cuda(cudaMemcpyAsync(d_chans, chans.data(), chans.size() * sizeof(TrChannelDev), cudaMemcpyHostToDevice,
+                                   st), "noise channels");
+
     PinnedBuffer h_res(16 * B);
     uint64_t* hres = static_cast<uint64_t*>(h_res.p);
     vec2_t<T>* s = static_cast<vec2_t<T>*>(batch.p);
@@ -788,7 +865,8 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
                                                               g.cmask, g.cwant);
             n_launch++;
         };
-        for (const TrStep& step : plan.steps) {
+        for (size_t si = 0; si < plan.steps.size(); ++si) {
+            const TrStep& step = plan.steps[si];
             switch (step.kind) {
                 case TrStep::OPS:
                     for (const Op& o : step.ops) {
@@ -859,12 +937,13 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
                         n_launch += 3;
                     } else {
                         check_cuda(cudaMemsetAsync(d_nactive, 0, 4, st), "memset");
-                        k_tr_noise_pauli<<<blocks_for(nb), kTrThreads, 0, st>>>(
-                            d_pass, mt, nb, step.noise, d_nprm + step.poff, step.nq, d_ax, d_az, d_any, d_active,
-                            d_nactive);
+                        k_tr_noise_group<<<blocks_for(nb), kTrThreads, 0, st>>>(
+                            d_pass, mt, nb, d_chans + group_off[si], static_cast<int>(group_len[si]), d_nprm, d_ax,
+                            d_az, d_any, d_active, d_nactive);
                         k_tr_apply_pauli<T><<<static_cast<unsigned>(sms) * 8, kTrThreads, 0, st>>>(
                             s, n, d_ax, d_az, d_any, d_active, d_nactive);
                         n_launch += 2;
+                        si += group_len[si] - 1;   // the group's other steps ran with it
                     }
                     break;
                 }
