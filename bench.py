@@ -48,6 +48,11 @@ SEED = 1234
 ADJ_N, ADJ_LAYERS, ADJ_TERMS = 24, 8, 500
 
 
+# DRAM bytes per launch of the dominant kernel (k_dense_reg<double,4>): 2092.9 MB captured by ncu on
+# a 26-qubit register (profiles/k_dense_reg_c128_k4_26q.md), scaled to the 28-qubit register
+DENSE4_TRAFFIC_28Q = 4 * 2092.9e6
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -566,7 +571,10 @@ def b200_arm(args, rank, world, local_rank):
             "pct_hbm_peak": 100.0 * value / (world * peak),
             "physical_gbs": physical, "physical_pct_hbm_peak": 100.0 * physical / (world * peak),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": kernel,
+                         "frac": achieved / peak, "traffic": DENSE4_TRAFFIC_28Q, "kernel": kernel,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                           "k_dense_reg<double,4> at 26 qubits, x4 to 2^28 amplitudes "
+                                           "(profiles/k_dense_reg_c128_k4_26q.md)",
                          "peak_source": peak_kind},
             "roofline_fp64": {"achieved": fp64_achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                               "frac": (fp64_achieved / fp64_peak) if fp64_peak else None,
