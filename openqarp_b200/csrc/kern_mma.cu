@@ -133,9 +133,8 @@ void launch_dmma(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& 
             W[static_cast<size_t>(y + Sh::D) * Sh::R + Sh::D + x] = u.real();
         }
     double* dW = static_cast<double*>(ws.matrix(W.size() * sizeof(double)));
-    // the previous user of the matrix buffer must be done before it is overwritten; a pageable
-    // source makes cudaMemcpyAsync return only after W has been staged, so W may go out of scope
-    check_cuda(cudaStreamSynchronize(st), "matrix buffer reuse");
+    // stream order keeps the previous pass's reads of the matrix buffer ahead of this upload, and
+    // a pageable source is staged before cudaMemcpyAsync returns, so W may go out of scope
     check_cuda(cudaMemcpyAsync(dW, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, st), "W upload");
     check_cuda(cudaFuncSetAttribute(k_dense_dmma<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(Sh::smem)), "dmma smem");

@@ -46,7 +46,17 @@ double* Workspace::host_result(size_t n) {
     return host_;
 }
 
+int* Workspace::tensor_flag() {
+    if (!flag_) {
+        check_cuda(cudaMalloc(reinterpret_cast<void**>(&flag_), 256), "tensor flag");
+        check_cuda(cudaMemset(flag_, 0, 256), "tensor flag");
+    }
+    return flag_;
+}
+
 void Workspace::release() {
+    if (flag_) cudaFree(flag_);
+    flag_ = nullptr;
     if (mat_) cudaFree(mat_);
     if (copy_) cudaFree(copy_);
     if (scr_) cudaFree(scr_);

@@ -964,6 +964,7 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
         std::memcpy(out_idx + s0, hres, 8ull * nb);
         std::memcpy(out_cbits + s0, hres + B, 8ull * nb);
     }
+    check_tensor_flag(ws, st);
     if (launches) *launches += n_launch;
 }
 

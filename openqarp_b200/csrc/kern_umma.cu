@@ -32,7 +32,9 @@ constexpr uint32_t kUCols = 64;                // TMEM columns (MMA N, fp32)
 constexpr int kUChunks = kUR / 4;              // 16-byte K chunks per row (16)
 constexpr int kUOperandA = kUM * kUR * 4;      // bytes of one A plane (32 KiB)
 constexpr int kUOperandB = kUR * kUR * 4;      // bytes of one B plane (16 KiB)
-constexpr size_t kUSmem = 2 * kUOperandA + 2 * kUOperandB + 1024;
+constexpr int kUStages = 3;                    // raw tiles in flight (cp.async ring)
+constexpr int kURaw = kUM * kUD * 8;           // bytes of one raw tile (float2 amplitudes)
+constexpr size_t kUSmem = 2 * kUOperandA + 2 * kUOperandB + kUStages * kURaw + 1024;
 constexpr long long kUWaitLimit = 1ll << 26;   // mbarrier polls before giving up
 
 struct UmmaArgs {
@@ -103,6 +105,7 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
     unsigned char* a_lo = a_hi + kUOperandA;
     unsigned char* b_hi = a_lo + kUOperandA;
     unsigned char* b_lo = b_hi + kUOperandB;
+    float2* raw = reinterpret_cast<float2*>(b_lo + kUOperandB);   // [stage][x][row], row fastest
     __shared__ uint32_t s_tmem;
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ int s_fail;
@@ -139,15 +142,41 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
     const uint32_t sb_hi = static_cast<uint32_t>(__cvta_generic_to_shared(b_hi));
     const uint32_t sb_lo = static_cast<uint32_t>(__cvta_generic_to_shared(b_lo));
     uint32_t phase = 0;
-    for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kUM; t0 < n_groups; t0 += static_cast<uint64_t>(gridDim.x) * kUM) {
-        // gather: thread `tid` owns group t0 + tid (row tid of A)
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * kUM;
+    // Pipeline: thread `tid` owns group t + tid of every tile (row tid of A).  Its 32 amplitudes
+    // are copied global -> shared with cp.async into a ring of kUStages raw tiles issued
+    // kUStages - 1 tiles ahead, so HBM reads stay in flight while earlier tiles are split into
+    // the MMA operand, multiplied on the tensor cores, read back from TMEM and stored.  Each
+    // thread reads back only the raw slots it copied itself.
+    auto issue = [&](uint64_t t, int stage) {
+        const uint64_t g = t + tid;
+        if (t < n_groups && g < n_groups) {
+            const uint64_t gb = insert_zeros(g, a.pos, kUK);
+            float2* dst = raw + static_cast<size_t>(stage) * kUM * kUD + tid;
+#pragma unroll
+            for (int x = 0; x < kUD; ++x) {
+                const uint32_t sd = static_cast<uint32_t>(__cvta_generic_to_shared(dst + x * kUM));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sd), "l"(s + (gb | a.off[x]))
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kUM;
+#pragma unroll
+    for (int p = 0; p < kUStages - 1; ++p) issue(first + p * stride, p);
+    int it = 0;
+    for (uint64_t t0 = first; t0 < n_groups; t0 += stride, ++it) {
+        issue(t0 + (kUStages - 1) * stride, (it + kUStages - 1) % kUStages);
+        asm volatile("cp.async.wait_group %0;" ::"n"(kUStages - 1) : "memory");
         const uint64_t g = t0 + tid;
         const bool live = g < n_groups;
         const uint64_t gb = live ? insert_zeros(g, a.pos, kUK) : 0;
+        const float2* src = raw + static_cast<size_t>(it % kUStages) * kUM * kUD + tid;
         float re[kUD], im[kUD];
 #pragma unroll
         for (int x = 0; x < kUD; ++x) {
-            const float2 v = live ? __ldcs(s + (gb | a.off[x])) : make_float2(0.f, 0.f);
+            const float2 v = live ? src[x * kUM] : make_float2(0.f, 0.f);
             re[x] = v.x;
             im[x] = v.y;
         }
@@ -211,6 +240,7 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");   // no copy outlives the kernel's shared memory
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kUCols));
 }
@@ -239,12 +269,11 @@ bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspac
             W[static_cast<size_t>(y + kUD) * kUR + x] = static_cast<float>(u.imag());
             W[static_cast<size_t>(y + kUD) * kUR + kUD + x] = static_cast<float>(u.real());
         }
-    uint8_t* buf = static_cast<uint8_t*>(ws.matrix(W.size() * sizeof(float) + 256));
-    float* dW = reinterpret_cast<float*>(buf);
-    int* d_err = reinterpret_cast<int*>(buf + W.size() * sizeof(float));
-    check_cuda(cudaStreamSynchronize(st), "matrix buffer reuse");
+    // stream order keeps the previous pass's reads of the matrix buffer ahead of this upload, and
+    // a pageable source is staged before cudaMemcpyAsync returns, so W may go out of scope
+    float* dW = static_cast<float*>(ws.matrix(W.size() * sizeof(float)));
+    int* d_err = ws.tensor_flag();
     check_cuda(cudaMemcpyAsync(dW, W.data(), W.size() * sizeof(float), cudaMemcpyHostToDevice, st), "W upload");
-    check_cuda(cudaMemsetAsync(d_err, 0, sizeof(int), st), "error flag");
     check_cuda(cudaFuncSetAttribute(k_dense5_umma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kUSmem)), "umma smem");
     int device = 0, sms = 0, per_sm = 0;
@@ -256,11 +285,22 @@ bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspac
     const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(sms) * std::max(per_sm, 1)));
     k_dense5_umma<<<static_cast<unsigned>(grid), kUThreads, kUSmem, st>>>(s, groups, dW, a, d_err);
     check_cuda(cudaGetLastError(), "umma launch");
-    int h_err = 0;
-    check_cuda(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "error flag");
-    check_cuda(cudaStreamSynchronize(st), "umma pass");
-    if (h_err) throw std::runtime_error("tensor-core pass timed out waiting for its MMA commit");
+    ws.tensor_pending = true;   // the caller checks the flag once its passes are queued
     return true;
+}
+
+void check_tensor_flag(Workspace& ws, cudaStream_t st) {
+    if (!ws.tensor_pending) return;
+    ws.tensor_pending = false;
+    int h_err = 0;
+    int* d_err = ws.tensor_flag();
+    check_cuda(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "tensor flag");
+    check_cuda(cudaStreamSynchronize(st), "tensor passes");
+    if (h_err) {
+        check_cuda(cudaMemsetAsync(d_err, 0, sizeof(int), st), "tensor flag");
+        check_cuda(cudaStreamSynchronize(st), "tensor flag");
+        throw std::runtime_error("tensor-core pass timed out waiting for its MMA commit");
+    }
 }
 
 }  // namespace qsv

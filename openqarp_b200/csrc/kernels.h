@@ -37,6 +37,9 @@ public:
     void* rt_tiles(size_t bytes) { return grow(rtile_, rtile_cap_, bytes); }
     // pinned host staging for small results
     double* host_result(size_t n_doubles);
+    // device int the tensor-core kernels set when a bounded wait gives up; zero at allocation
+    int* tensor_flag();
+    bool tensor_pending = false;   // a tensor-core pass ran since the flag was last checked
 
 private:
     static void* grow(void*& p, size_t& cap, size_t bytes);
@@ -47,6 +50,7 @@ private:
     void* tile_ = nullptr; size_t tile_cap_ = 0;
     void* rtile_ = nullptr; size_t rtile_cap_ = 0;
     double* host_ = nullptr; size_t host_cap_ = 0;
+    int* flag_ = nullptr;
 };
 
 // ---------------------------------------------------------------- gates (kern_gates.cu)
@@ -61,6 +65,9 @@ void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& 
 bool launch_dense_tensor(const Op& op, double2* s, int n, cudaStream_t st, Workspace& ws);
 // Dense k = 5 blocks in complex64 on tcgen05 (kern_umma.cu); false when not such a block.
 bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws);
+// After tensor-core passes (launched without host synchronisation): synchronise `st`, read and
+// clear the workspace's flag, and throw if a pass gave up waiting for its MMA commit.
+void check_tensor_flag(Workspace& ws, cudaStream_t st);
 // Dense k = 5, 6 blocks of a complex64 register on the FP64 tensor pipe (kern_mma.cu): the k = 6
 // path, and k = 5 where the tcgen05 kernel declines.
 bool launch_dense_tensor_f32(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws);

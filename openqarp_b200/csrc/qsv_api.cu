@@ -175,6 +175,7 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
         for (const Op& o : ops) launch(h, o, h->state);
     }
     check_cuda(cudaEventRecord(h->e1, h->stream), "event");
+    check_tensor_flag(h->ws, h->stream);
 }
 
 PauliTerms terms_of(Handle* h, const uint64_t* xm, const uint64_t* zm, const double* coeff,
