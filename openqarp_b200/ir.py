@@ -322,6 +322,21 @@ def _gate_code(g) -> int:
     return int(v)
 
 
+_FAST: dict = {}
+
+
+def _fast_struct(nq: int, nv: int) -> struct.Struct:
+    """Header + qubits (+ padding to 8 bytes) + params of a command without cbits, conditions
+    or a matrix, as one struct."""
+    key = (nq, nv)
+    st = _FAST.get(key)
+    if st is None:
+        pad = (8 - (8 + 4 * nq) % 8) % 8
+        st = struct.Struct(f"<HBBBBBB{nq}I{pad}x{nv}d")
+        _FAST[key] = st
+    return st
+
+
 def _cmd_fields(cmd):
     g = _gate_code(cmd.gate)
     qubits = [int(q) for q in cmd.qubits]
@@ -361,6 +376,17 @@ def pack(commands: Iterable, values: Optional[Mapping[str, float]] = None,
     dep_alpha: list[float] = []
     n = 0
     for cmd in commands:
+        # common case: a plain gate of this module's Command with numeric parameters
+        if (type(cmd) is Command and not cmd.cbits and not cmd.condition_bits and cmd.unitary is None
+                and all(type(p) is float or type(p) is int for p in cmd.params)):
+            qs, ps = cmd.qubits, cmd.params
+            if len(qs) > 255 or len(ps) > 255:
+                raise ValueError("command too wide to pack")
+            out += _fast_struct(len(qs), len(ps)).pack(int(cmd.gate), len(qs), len(ps), 0, 0, 0, 0, *qs, *ps)
+            if index is not None:
+                dep_ptr.append(len(dep_param))
+            n += 1
+            continue
         if isinstance(cmd, (PermutationRecord, ControlledUnitaryRecord)):
             _pack_record(out, cmd)
             if index is not None:
@@ -424,7 +450,10 @@ def measurements_are_terminal(commands: Sequence) -> bool:
     measurements_are_terminal, qarp_simulator.cpp:283-310)."""
     measured = 0
     for cmd in commands:
-        g, qubits, _params, cbits, cond, _u = _cmd_fields(cmd)
+        if type(cmd) is Command:
+            g, qubits, cbits, cond = int(cmd.gate), cmd.qubits, cmd.cbits, cmd.condition_bits
+        else:
+            g, qubits, _params, cbits, cond, _u = _cmd_fields(cmd)
         if g == GateType.Reset or cond:
             return False
         if g in (GateType.BranchBegin, GateType.BranchElse, GateType.BranchEnd):
@@ -443,7 +472,14 @@ def measurements_are_terminal(commands: Sequence) -> bool:
     return True
 
 
+_RESET, _MEASURE, _BRANCH_BEGIN = int(GateType.Reset), int(GateType.Measure), int(GateType.BranchBegin)
+
+
 def needs_trajectory(cmd) -> bool:
+    if type(cmd) is Command:   # fast path: fields already normalised by Command.__post_init__
+        g = int(cmd.gate)
+        return (g == _RESET or (g == _MEASURE and bool(cmd.cbits)) or bool(cmd.condition_bits)
+                or g == _BRANCH_BEGIN)
     g, _q, _p, cbits, cond, _u = _cmd_fields(cmd)
     return (g == GateType.Reset or (g == GateType.Measure and bool(cbits)) or bool(cond)
             or g == GateType.BranchBegin)
