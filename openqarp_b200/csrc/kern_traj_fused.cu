@@ -27,6 +27,7 @@ constexpr int kFsMinBytes = 4 * 1024;
 constexpr int kFsMaxCoef = 512;          // doubles of one step's coefficients (a 4-qubit block)
 constexpr int kFsMtBytes = 4 * 624 + 16; // one MT19937 state, padded to keep the plan aligned
 constexpr size_t kFsResidentMax = 104 * 1024;   // dynamic shared memory with the plan resident
+constexpr size_t kFsApplyResidentMax = 200 * 1024;   // the same for the one-CTA gate sequence
 
 enum FsKind : uint8_t {
     FS_DENSE = 0,     // k <= 4 unitary on q[0..k) where (i & ctrl) == ctrl; matrix at coef
@@ -137,6 +138,71 @@ __device__ __forceinline__ void fs_dense(vec2_t<T>* a, int n, const FsStep& S, c
     }
 }
 
+// The gate steps (dense, diagonal, phase, scale, swap, Pauli rotation) on the amplitudes in
+// shared memory; false for the other kinds.  Every thread of the CTA calls it with the same step.
+template <typename T>
+__device__ __forceinline__ bool fs_gate(vec2_t<T>* a, int n, const FsStep& S, const double* c) {
+    const uint64_t dim = 1ull << n;
+    switch (S.kind) {
+        case FS_DENSE:
+            switch (S.k) {
+                case 1: fs_dense<T, 1>(a, n, S, c); break;
+                case 2: fs_dense<T, 2>(a, n, S, c); break;
+                case 3: fs_dense<T, 3>(a, n, S, c); break;
+                default: fs_dense<T, 4>(a, n, S, c); break;
+            }
+            break;
+        case FS_DIAG:
+            for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) {
+                uint32_t l = 0;
+                for (int b = 0; b < S.k; ++b) l |= static_cast<uint32_t>((i >> S.q[b]) & 1ull) << b;
+                a[i] = cmul_d<T>(c[2 * l], c[2 * l + 1], a[i]);
+            }
+            break;
+        case FS_PHASE:
+            for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads)
+                if ((i & S.mask) == S.mask) a[i] = cmul_d<T>(c[0], c[1], a[i]);
+            break;
+        case FS_SCALE:
+            for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = cmul_d<T>(c[0], c[1], a[i]);
+            break;
+        case FS_SWAP: {
+            const uint64_t A = 1ull << S.q[0], B = 1ull << S.q[1];
+            for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads)
+                if ((i & A) && !(i & B)) {
+                    const uint64_t j = (i & ~A) | B;
+                    const vec2_t<T> t = a[i];
+                    a[i] = a[j];
+                    a[j] = t;
+                }
+            break;
+        }
+        case FS_PROT: {
+            // exp(-i theta/2 P) on pairs (i, i ^ x), i without the lowest bit of x
+            const double cs = c[0], sn = c[1];
+            const uint64_t x = S.mask, z = S.zmask, pivot = x & (~x + 1);
+            const uint32_t ny = static_cast<uint32_t>(__popcll(x & z));
+            for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) {
+                if (i & pivot) continue;
+                const uint64_t j = i ^ x;
+                const vec2_t<T> ai = a[i], aj = a[j];
+                // s[i] = c ai - i sn phase(j) aj,  phase(j) = i^ny (-1)^popcount(j & z)
+                const vec2_t<T> pj = tr_pauli_phase<T>(aj, ny + 1, __popcll(j & z) & 1);
+                const vec2_t<T> pi = tr_pauli_phase<T>(ai, ny + 1, __popcll(i & z) & 1);
+                a[i] = mk<T>(static_cast<T>(cs * static_cast<double>(ai.x) - sn * static_cast<double>(pj.x)),
+                             static_cast<T>(cs * static_cast<double>(ai.y) - sn * static_cast<double>(pj.y)));
+                if (j != i)
+                    a[j] = mk<T>(static_cast<T>(cs * static_cast<double>(aj.x) - sn * static_cast<double>(pi.x)),
+                                 static_cast<T>(cs * static_cast<double>(aj.y) - sn * static_cast<double>(pi.y)));
+            }
+            break;
+        }
+        default:
+            return false;
+    }
+    return true;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restrict__ steps, int n_steps,
                                                       const double* __restrict__ coef, uint32_t n_coef, int resident,
@@ -199,60 +265,7 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
             __syncthreads();
             c = scoef;
         }
-        switch (S.kind) {
-            case FS_DENSE:
-                switch (S.k) {
-                    case 1: fs_dense<T, 1>(a, n, S, c); break;
-                    case 2: fs_dense<T, 2>(a, n, S, c); break;
-                    case 3: fs_dense<T, 3>(a, n, S, c); break;
-                    default: fs_dense<T, 4>(a, n, S, c); break;
-                }
-                break;
-            case FS_DIAG:
-                for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) {
-                    uint32_t l = 0;
-                    for (int b = 0; b < S.k; ++b) l |= static_cast<uint32_t>((i >> S.q[b]) & 1ull) << b;
-                    a[i] = cmul_d<T>(c[2 * l], c[2 * l + 1], a[i]);
-                }
-                break;
-            case FS_PHASE:
-                for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads)
-                    if ((i & S.mask) == S.mask) a[i] = cmul_d<T>(c[0], c[1], a[i]);
-                break;
-            case FS_SCALE:
-                for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = cmul_d<T>(c[0], c[1], a[i]);
-                break;
-            case FS_SWAP: {
-                const uint64_t A = 1ull << S.q[0], B = 1ull << S.q[1];
-                for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads)
-                    if ((i & A) && !(i & B)) {
-                        const uint64_t j = (i & ~A) | B;
-                        const vec2_t<T> t = a[i];
-                        a[i] = a[j];
-                        a[j] = t;
-                    }
-                break;
-            }
-            case FS_PROT: {
-                // exp(-i theta/2 P) on pairs (i, i ^ x), i without the lowest bit of x
-                const double cs = c[0], sn = c[1];
-                const uint64_t x = S.mask, z = S.zmask, pivot = x & (~x + 1);
-                const uint32_t ny = static_cast<uint32_t>(__popcll(x & z));
-                for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) {
-                    if (i & pivot) continue;
-                    const uint64_t j = i ^ x;
-                    const vec2_t<T> ai = a[i], aj = a[j];
-                    // s[i] = c ai - i sn phase(j) aj,  phase(j) = i^ny (-1)^popcount(j & z)
-                    const vec2_t<T> pj = tr_pauli_phase<T>(aj, ny + 1, __popcll(j & z) & 1);
-                    const vec2_t<T> pi = tr_pauli_phase<T>(ai, ny + 1, __popcll(i & z) & 1);
-                    a[i] = mk<T>(static_cast<T>(cs * static_cast<double>(ai.x) - sn * static_cast<double>(pj.x)),
-                                 static_cast<T>(cs * static_cast<double>(ai.y) - sn * static_cast<double>(pj.y)));
-                    if (j != i)
-                        a[j] = mk<T>(static_cast<T>(cs * static_cast<double>(aj.x) - sn * static_cast<double>(pi.x)),
-                                     static_cast<T>(cs * static_cast<double>(aj.y) - sn * static_cast<double>(pi.y)));
-                }
-                break;
-            }
+        if (!fs_gate<T>(a, n, S, c)) switch (S.kind) {
             case FS_MEASURE: {
                 const uint64_t qb = 1ull << S.q[0];
                 double acc = 0.0;
@@ -397,6 +410,51 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
     }
     __syncthreads();   // the next shot overwrites the amplitudes, part[] and the engine
     }
+}
+
+// A whole gate sequence on a small register in one CTA: the register is loaded into shared
+// memory, every step applied there, and written back in place.  Replaces one launch per gate
+// (each a few microseconds of launch latency for a few kilobytes of work) by one launch.
+template <typename T>
+__global__ void __launch_bounds__(kFsThreads) k_fs_apply(const FsStep* __restrict__ steps, int n_steps,
+                                                        const double* __restrict__ coef, uint32_t n_coef,
+                                                        int resident, vec2_t<T>* __restrict__ state, int n) {
+    extern __shared__ __align__(16) unsigned char fa_smem[];
+    vec2_t<T>* a = reinterpret_cast<vec2_t<T>*>(fa_smem);
+    const uint64_t dim = 1ull << n;
+    const size_t amp_area = (dim * sizeof(vec2_t<T>) + 15) & ~size_t{15};
+    uint64_t* rsteps = reinterpret_cast<uint64_t*>(fa_smem + amp_area);
+    double* rcoef = reinterpret_cast<double*>(rsteps + static_cast<size_t>(n_steps) * (sizeof(FsStep) / 8));
+    __shared__ uint64_t sstep[sizeof(FsStep) / 8];
+    __shared__ __align__(16) double scoef[kFsMaxCoef];
+    if (resident) {
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(steps);
+        const size_t words = static_cast<size_t>(n_steps) * (sizeof(FsStep) / 8);
+        for (size_t w = threadIdx.x; w < words; w += kFsThreads) rsteps[w] = __ldg(src + w);
+        for (uint32_t w = threadIdx.x; w < n_coef; w += kFsThreads) rcoef[w] = __ldg(coef + w);
+    }
+    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = state[i];
+    __syncthreads();
+    for (int si = 0; si < n_steps; ++si) {
+        const double* c;
+        const FsStep* S;
+        if (resident) {
+            S = reinterpret_cast<const FsStep*>(rsteps + si * (sizeof(FsStep) / 8));
+            c = rcoef + S->coef;
+        } else {
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(steps + si);
+            for (int w = threadIdx.x; w < static_cast<int>(sizeof(FsStep) / 8); w += kFsThreads)
+                sstep[w] = __ldg(src + w);
+            __syncthreads();
+            S = reinterpret_cast<const FsStep*>(sstep);
+            for (uint32_t w = threadIdx.x; w < S->ncoef; w += kFsThreads) scoef[w] = __ldg(coef + S->coef + w);
+            __syncthreads();
+            c = scoef;
+        }
+        fs_gate<T>(a, n, *S, c);
+        __syncthreads();
+    }
+    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) state[i] = a[i];
 }
 
 // host: the plan's steps as FsSteps; false when a step has no shared-memory form
@@ -614,6 +672,43 @@ bool run_trajectories_fused(const TrPlan& plan, int n, const vec2_t<T>* d_prefix
     }
     return true;
 }
+
+template <typename T>
+bool apply_ops_small(const std::vector<Op>& ops, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws) {
+    const size_t amp_bytes = sizeof(vec2_t<T>) << n;
+    if (amp_bytes > static_cast<size_t>(kFsMaxBytes) || ops.size() < 2) return false;
+    TrPlan plan;
+    plan.steps.emplace_back();
+    plan.steps.back().kind = TrStep::OPS;
+    plan.steps.back().ops = ops;
+    std::vector<FsStep> steps;
+    std::vector<double> coef;
+    if (!encode(plan, steps, coef)) return false;
+    if (steps.empty()) return true;
+    if (coef.empty()) coef.push_back(0.0);
+    const size_t steps_bytes = steps.size() * sizeof(FsStep);
+    const size_t coef_off = (steps_bytes + 15) & ~size_t{15};
+    std::vector<unsigned char> blob(coef_off + coef.size() * sizeof(double));
+    std::memcpy(blob.data(), steps.data(), steps_bytes);
+    std::memcpy(blob.data() + coef_off, coef.data(), coef.size() * sizeof(double));
+    unsigned char* d = static_cast<unsigned char*>(ws.shots(blob.size()));
+    // pageable source: staged before cudaMemcpyAsync returns; stream order protects the buffer
+    check_cuda(cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, st), "gate program H2D");
+    const size_t amp_area = (amp_bytes + 15) & ~size_t{15};
+    const size_t prog_bytes = steps_bytes + coef.size() * sizeof(double);
+    const int resident = amp_area + prog_bytes <= kFsApplyResidentMax ? 1 : 0;
+    const size_t smem = amp_area + (resident ? prog_bytes : 0);
+    check_cuda(cudaFuncSetAttribute(k_fs_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)), "small-register smem");
+    k_fs_apply<T><<<1, kFsThreads, smem, st>>>(reinterpret_cast<const FsStep*>(d), static_cast<int>(steps.size()),
+                                               reinterpret_cast<const double*>(d + coef_off),
+                                               static_cast<uint32_t>(coef.size()), resident, s, n);
+    check_cuda(cudaGetLastError(), "small-register launch");
+    return true;
+}
+
+template bool apply_ops_small<double>(const std::vector<Op>&, double2*, int, cudaStream_t, Workspace&);
+template bool apply_ops_small<float>(const std::vector<Op>&, float2*, int, cudaStream_t, Workspace&);
 
 template bool run_trajectories_fused<double>(const TrPlan&, int, const double2*, uint32_t, size_t, uint64_t*,
                                              uint64_t*, cudaStream_t, Workspace&, uint64_t*);

@@ -72,6 +72,12 @@ void check_tensor_flag(Workspace& ws, cudaStream_t st);
 // path, and k = 5 where the tcgen05 kernel declines.
 bool launch_dense_tensor_f32(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws);
 
+// A gate sequence on a register of at most 64 KiB as one single-CTA launch in shared memory
+// (kern_traj_fused.cu); false, having done nothing, when the register is wider, there are fewer
+// than two ops, or an op has no shared-memory form (permutations, dense blocks over 4 qubits).
+template <typename T>
+bool apply_ops_small(const std::vector<Op>& ops, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
+
 // ---------------------------------------------------------------- tiled executor (kern_tile.cu)
 // Launch the planned passes; one-op stream passes (empty tile_qubits) go to `stream_op`.
 // With register_tiles, passes plan_rt accepts run on the register-tile kernel.

@@ -437,6 +437,18 @@ std::vector<c128> local_unitary(const Cmd& c) {
     if (k == 0 || k > QSV_MAX_BLOCK_QUBITS)
         throw std::invalid_argument("local_unitary: gate acts on " + std::to_string(k) + " qubits");
     if (c.gate == CUSTOM) return c.u;
+    if (k == 1) {   // one-qubit gates: the matrix lowering applies to basis columns, directly
+        switch (c.gate) {
+            case X: case Y: case Z: case H: case S: case SDG: case T: case TDG: case SX: case SXDG:
+                return fixed(c.gate);
+            case RX: return m_rx(param(c, 0));
+            case RY: return m_ry(param(c, 0));
+            case RZ: return m_rz(param(c, 0));
+            case P: return m_p(param(c, 0));
+            case U: return m_u(param(c, 0), param(c, 1), param(c, 2));
+            default: break;
+        }
+    }
     Cmd local = c;
     for (int b = 0; b < k; ++b) local.q[b] = static_cast<uint32_t>(b);
     local.flags = 0;

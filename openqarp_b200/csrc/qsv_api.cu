@@ -171,6 +171,14 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
             for (const Op& o : p.ops)
                 if (o.kind == OP_DENSE && o.k >= 2) h->stats.fused_blocks++;
         }
+    } else if (h->dtype == QSV_C128 ? apply_ops_small<double>(ops, S128(h), h->n, h->stream, h->ws)
+                                    : apply_ops_small<float>(ops, S64(h), h->n, h->stream, h->ws)) {
+        // a register of at most 64 KiB: the whole sequence in one launch, in shared memory
+        h->stats.launches++;
+        h->stats.passes += ops.size();
+        h->stats.hbm_bytes += 2ull * h->dim() * h->amp_bytes();
+        for (const Op& o : ops)
+            if (o.kind == OP_DENSE && o.k >= 2) h->stats.fused_blocks++;
     } else {
         for (const Op& o : ops) launch(h, o, h->state);
     }
