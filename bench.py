@@ -425,8 +425,11 @@ def reference_arm(args, rank, world):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * float(np.median(times)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": f"brickwork n={N_QUBITS} depth=1 sample of depth {DEPTH}, fusion k=3",
-                   "l2": "register 4 GiB > L2"},
+        "config": {"workload": f"brickwork n={N_QUBITS} depth={DEPTH} Haar SU(2)+CZ, seed {SEED}",
+                   "fusion_k": 3,
+                   "work_definition": f"fused-gate passes of the reference plan (k=3) x 2 x 2^{N_QUBITS} x 16 B",
+                   "sample": "each step times one of the circuit's layers (its fused passes) on the host cores",
+                   "l2": "register 4 GiB > L2", "parallelism": "host threads"},
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": kind,
                          "sample": f"1 brickwork layer at {N_QUBITS} qubits per step ({passes} fused passes)"},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -68,6 +68,27 @@ __device__ __forceinline__ double fs_block_sum(double v, double* red) {
     return t;          // valid in thread 0
 }
 
+// Four block sums with one pair of barriers (the reduced density matrix of a Kraus step);
+// red must hold 4 * warps doubles.  Results valid in thread 0.
+__device__ __forceinline__ void fs_block_sum4(double v[4], double* red) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) red[4 * (threadIdx.x >> 5) + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            double t = 0.0;
+            for (int w = 0; w < kFsThreads / 32; ++w) t += red[4 * w + k];
+            v[k] = t;
+        }
+    __syncthreads();   // red is free again
+}
+
 template <typename T>
 __device__ __forceinline__ vec2_t<T> cmul_d(double re, double im, vec2_t<T> a) {
     const double x = static_cast<double>(a.x), y = static_cast<double>(a.y);
@@ -218,7 +239,7 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
     uint32_t* mtw = reinterpret_cast<uint32_t*>(fs_smem + amp_area);
     uint64_t* rsteps = reinterpret_cast<uint64_t*>(fs_smem + amp_area + kFsMtBytes);
     double* rcoef = reinterpret_cast<double*>(rsteps + static_cast<size_t>(n_steps) * (sizeof(FsStep) / 8));
-    __shared__ double red[kFsThreads / 32];
+    __shared__ double red[4 * (kFsThreads / 32)];
     __shared__ double part[kFsThreads];
     __shared__ uint64_t sstep[sizeof(FsStep) / 8];   // streamed plans: the current step and its
     __shared__ __align__(16) double scoef[kFsMaxCoef];   //              coefficients, staged
@@ -347,10 +368,12 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
                     rr += ar * br + ai * bi;
                     ri += ai * br - ar * bi;
                 }
-                r00 = fs_block_sum(r00, red);
-                r11 = fs_block_sum(r11, red);
-                rr = fs_block_sum(rr, red);
-                ri = fs_block_sum(ri, red);
+                double rho[4] = {r00, r11, rr, ri};
+                fs_block_sum4(rho, red);
+                r00 = rho[0];
+                r11 = rho[1];
+                rr = rho[2];
+                ri = rho[3];
                 if (threadIdx.x == 0) bflag = tr_choose_kraus(r00, r11, rr, ri, c, S.k2, g, bc) ? 1 : 0;
                 __syncthreads();
                 if (!bflag) break;
