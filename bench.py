@@ -524,6 +524,8 @@ def b200_arm(args, rank, world, local_rank):
     result = None
     if rank == 0:
         cpu = None
+        # the single-GPU rows run only at N = 1: at N > 1 every GPU would wait for rank 0
+        single = world == 1
         if world == 1 and not args.skip_cpu:
             layer = ir.pack(circuits.brickwork(N_QUBITS, 1, seed=SEED)).buf
             gbs, dt, cpasses, cores, kind = cpu_baseline_sample(layer, N_QUBITS)
@@ -531,29 +533,29 @@ def b200_arm(args, rank, world, local_rank):
                    "sample": f"1 brickwork layer at {N_QUBITS} qubits ({cpasses} fused passes, k=3), "
                              f"{dt:.1f} s"}
         adj = None
-        if not args.skip_adjoint:
+        if single and not args.skip_adjoint:
             reg.close()
             adj = adjoint_vs_param_shift(device)
         sweep_k = None
-        if not args.skip_ksweep:
+        if single and not args.skip_ksweep:
             reg.close()
             sweep_k = k_sweep(device, buf)
         structured = None
-        if not args.skip_structured:
+        if single and not args.skip_structured:
             reg.close()
             from openqarp_b200.workloads import structured_rows
             structured = structured_rows(device=device)
         plain12 = None
-        if not args.skip_structured:
+        if single and not args.skip_structured:
             from openqarp_b200.workloads import config1_latency
             plain12 = config1_latency(device=device)
         traj = None
-        if not args.skip_trajectories:
+        if single and not args.skip_trajectories:
             reg.close()
             from openqarp_b200.workloads import trajectory_rows
             traj = trajectory_rows(device=device)
         heis = None
-        if not args.skip_heisenberg:
+        if single and not args.skip_heisenberg:
             reg.close()
             from openqarp_b200.workloads import heisenberg_bulk
             heis = heisenberg_bulk(n=31, steps=50, dt=0.05, seed=SEED, device=device)
