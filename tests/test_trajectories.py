@@ -387,3 +387,96 @@ def test_shot_ranges_reproduce_the_full_run(name):
         assert one.cbit_history == full.cbit_history and one.counts == full.counts
     finally:
         s.close()
+
+
+# ---------------------------------------------------------------- random streams against the reference
+
+def _random_trajectory_stream(rng, n):
+    """A random stream with every trajectory feature: gates, recorded and unrecorded
+    measurements, Resets, conditioned gates and (nested) branches with else-parts."""
+    from openqarp_b200.ir import Command, GateType as G
+    one_q = [G.H, G.X, G.S, G.T, G.SX, G.Rx, G.Ry, G.Rz, G.U]
+    two_q = [G.CX, G.CZ, G.RZZ, G.SWAP, G.CRy]
+    n_cbits = 4
+    cmds, depth = [], 0
+    written = set()
+
+    def gate():
+        if rng.random() < 0.6 or n < 2:
+            g = one_q[rng.integers(len(one_q))]
+            q = (int(rng.integers(n)),)
+        else:
+            g = two_q[rng.integers(len(two_q))]
+            q = tuple(int(x) for x in rng.choice(n, 2, replace=False))
+        p = {G.Rx: 1, G.Ry: 1, G.Rz: 1, G.RZZ: 1, G.CRy: 1, G.U: 3}.get(g, 0)
+        return Command(g, q, tuple(float(v) for v in rng.uniform(-3, 3, p)))
+
+    for _ in range(int(rng.integers(20, 45))):
+        r = rng.random()
+        if r < 0.55:
+            c = gate()
+            if written and rng.random() < 0.25:
+                b = int(rng.choice(sorted(written)))
+                c = Command(c.gate, c.qubits, c.params, None, (), (b,), (bool(rng.integers(2)),))
+            cmds.append(c)
+        elif r < 0.72:
+            cb = int(rng.integers(n_cbits))
+            cmds.append(Command(G.Measure, (int(rng.integers(n)),), (), None, (cb,)))
+            written.add(cb)
+        elif r < 0.78:
+            cmds.append(Command(G.Reset, (int(rng.integers(n)),)))
+        elif r < 0.82:
+            cmds.append(Command(G.Measure, (int(rng.integers(n)),)))
+        elif r < 0.92 and written and depth < 2:
+            b = int(rng.choice(sorted(written)))
+            cmds.append(Command(G.BranchBegin, (), (), None, (), (b,), (bool(rng.integers(2)),)))
+            depth += 1
+            cmds += [gate() for _ in range(int(rng.integers(1, 4)))]
+            if rng.random() < 0.5:
+                cmds.append(Command(G.BranchElse, ()))
+                cmds += [gate() for _ in range(int(rng.integers(1, 3)))]
+            cmds.append(Command(G.BranchEnd, ()))
+            depth -= 1
+        else:
+            cmds.append(gate())
+    cmds += [Command(G.Measure, (q,), (), None, (q % n_cbits,)) for q in range(min(n, n_cbits))]
+    return cmds
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(12))
+def test_random_trajectory_streams_match_reference(seed, reference):
+    """Seeded random streams (3 to 10 qubits, so both executors run them), noiseless and under
+    a random noise model, against the reference's own run(): identical per-shot registers and
+    counts."""
+    from openqarp_b200 import B200Simulator
+    from openqarp_b200.ir import GateType, pack
+    rng = np.random.default_rng(1000 + seed)
+    n = int(rng.choice([3, 5, 8, 9, 10]))
+    cmds = _random_trajectory_stream(rng, n)
+    shots = 200
+    names1 = ["H", "X", "S", "T", "SX", "Rx", "Ry", "Rz", "U"]
+    names2 = ["CX", "CZ", "RZZ", "SWAP", "CRy"]
+    specs = []
+    if seed % 2:
+        specs = [("depolarizing", float(rng.uniform(0.01, 0.2)), names1 + names2),
+                 ("amplitude_damping", float(rng.uniform(0.05, 0.3)), ["U", "Ry"])]
+    buf = pack(cmds).buf
+    if specs:
+        counts, hist, width = reference.run_noisy(buf, n, shots, seed,
+                                                  [(b, p, [int(GateType[x]) for x in g]) for b, p, g in specs])
+    else:
+        counts, hist, width = reference.run_history(buf, n, shots, seed)
+    model = None
+    if specs:
+        from openqarp_b200.noise import make_amplitude_damping, make_depolarizing
+        model = make_depolarizing(specs[0][1], [GateType[x] for x in specs[0][2]]) + \
+            make_amplitude_damping(specs[1][1], [GateType[x] for x in specs[1][2]])
+    sim = B200Simulator(noise_model=model)
+    try:
+        res = sim.run(cmds, n, shots, seed)
+    finally:
+        sim.close()
+    assert res.n_cbits == width
+    np.testing.assert_array_equal(_masks(res.cbit_history, width), np.asarray(hist, dtype=np.uint64))
+    assert res.counts == counts
