@@ -65,6 +65,13 @@ __global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(vec2_t<T>* __restric
     const int nb = warp % Sh::NB;
     const int mrow0 = (warp / Sh::NB) * Sh::MPW * 8;
     constexpr int EL = Sh::NG * Sh::D;    // amplitudes per tile
+    static_assert(K != 5 || (Sh::R / 8 == kMmaThreads / 32 && Sh::NB == 8), "k = 5: one 8-row block per warp");
+    double afrag[K == 5 ? Sh::R / 4 : 1];
+    if constexpr (K == 5) {
+        __syncthreads();                  // W is in shared memory
+#pragma unroll
+        for (int ks = 0; ks < Sh::R / 4; ++ks) afrag[ks] = w[(warp * 8 + gid) * Sh::WS + ks * 4 + tig];
+    }
     for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * Sh::NG; t0 < n_groups;
          t0 += static_cast<uint64_t>(gridDim.x) * Sh::NG) {
         __syncthreads();                  // W loaded / previous tile stored
@@ -77,26 +84,50 @@ __global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(vec2_t<T>* __restric
             xi[x * Sh::S + j] = static_cast<double>(v.y);
         }
         __syncthreads();
-        double acc[Sh::MPW][2];
+        if constexpr (K == 5) {
+            // warp w owns output rows 8w..8w+7 for every group of the tile: its A fragments (the
+            // constant matrix) stay in registers, so each MMA reads only its B operand from
+            // shared memory
+            double acc[Sh::NB][2];
 #pragma unroll
-        for (int mi = 0; mi < Sh::MPW; ++mi) acc[mi][0] = acc[mi][1] = 0.0;
+            for (int nbk = 0; nbk < Sh::NB; ++nbk) acc[nbk][0] = acc[nbk][1] = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < Sh::R / 4; ++ks) {
+                const int krow = ks * 4 + tig;
+                const double* brow = krow < Sh::D ? xr + krow * Sh::S : xi + (krow - Sh::D) * Sh::S;
+#pragma unroll
+                for (int nbk = 0; nbk < Sh::NB; ++nbk) dmma_8x8x4(acc[nbk][0], acc[nbk][1], afrag[ks], brow[nbk * 8 + gid]);
+            }
+            __syncthreads();              // every warp has read the planes
+            const int row = warp * 8 + gid;
+            double* plane = row < Sh::D ? xr + row * Sh::S : xi + (row - Sh::D) * Sh::S;
+#pragma unroll
+            for (int nbk = 0; nbk < Sh::NB; ++nbk) {
+                plane[nbk * 8 + 2 * tig] = acc[nbk][0];
+                plane[nbk * 8 + 2 * tig + 1] = acc[nbk][1];
+            }
+        } else {
+            double acc[Sh::MPW][2];
+#pragma unroll
+            for (int mi = 0; mi < Sh::MPW; ++mi) acc[mi][0] = acc[mi][1] = 0.0;
 #pragma unroll 4
-        for (int kk = 0; kk < Sh::R; kk += 4) {
-            const int krow = kk + tig;
-            const double b = kk < Sh::D ? xr[krow * Sh::S + nb * 8 + gid] : xi[(krow - Sh::D) * Sh::S + nb * 8 + gid];
+            for (int kk = 0; kk < Sh::R; kk += 4) {
+                const int krow = kk + tig;
+                const double b = kk < Sh::D ? xr[krow * Sh::S + nb * 8 + gid] : xi[(krow - Sh::D) * Sh::S + nb * 8 + gid];
+#pragma unroll
+                for (int mi = 0; mi < Sh::MPW; ++mi) {
+                    const double av = w[(mrow0 + mi * 8 + gid) * Sh::WS + krow];
+                    dmma_8x8x4(acc[mi][0], acc[mi][1], av, b);
+                }
+            }
+            __syncthreads();              // every warp has read the planes
 #pragma unroll
             for (int mi = 0; mi < Sh::MPW; ++mi) {
-                const double av = w[(mrow0 + mi * 8 + gid) * Sh::WS + krow];
-                dmma_8x8x4(acc[mi][0], acc[mi][1], av, b);
+                const int row = mrow0 + mi * 8 + gid;
+                double* plane = row < Sh::D ? xr + row * Sh::S : xi + (row - Sh::D) * Sh::S;
+                plane[nb * 8 + 2 * tig] = acc[mi][0];
+                plane[nb * 8 + 2 * tig + 1] = acc[mi][1];
             }
-        }
-        __syncthreads();                  // every warp has read the planes
-#pragma unroll
-        for (int mi = 0; mi < Sh::MPW; ++mi) {
-            const int row = mrow0 + mi * 8 + gid;
-            double* plane = row < Sh::D ? xr + row * Sh::S : xi + (row - Sh::D) * Sh::S;
-            plane[nb * 8 + 2 * tig] = acc[mi][0];
-            plane[nb * 8 + 2 * tig + 1] = acc[mi][1];
         }
         __syncthreads();
         for (int e = threadIdx.x; e < EL; e += blockDim.x) {
