@@ -245,6 +245,167 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kUCols));
 }
 
+// Paired variant for blocks that leave qubit 0 alone: groups 2j and 2j + 1 then sit in adjacent
+// amplitudes, so thread j moves both with 16-byte copies and stores.  A tile is 256 groups: the
+// even groups form MMA operand A0 and the odd ones A1 (128 rows each, row j = thread j), with
+// accumulators D0 and D1 side by side in TMEM.  One 64 KiB raw stage is filled by cp.async for the
+// next tile while the current tile's MMAs run and its results are stored; half the memory
+// instructions of the one-group kernel, whose load/store queue limits it.
+constexpr uint32_t kU2Cols = 2 * kUCols;                           // D0 | D1
+constexpr int kU2Raw = kUM * kUD * 16;                             // float4 (two groups' amplitude)
+constexpr size_t kU2Smem = 4 * kUOperandA + 2 * kUOperandB + kU2Raw + 1024;
+
+__global__ void __launch_bounds__(kUThreads, 1) k_dense5_umma2(float2* __restrict__ s, uint64_t n_groups,
+                                                               const float* __restrict__ W,
+                                                               const __grid_constant__ UmmaArgs a,
+                                                               int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char usm2[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(usm2) + 1023) & ~uintptr_t{1023});
+    unsigned char* a0_hi = base;
+    unsigned char* a0_lo = a0_hi + kUOperandA;
+    unsigned char* a1_hi = a0_lo + kUOperandA;
+    unsigned char* a1_lo = a1_hi + kUOperandA;
+    unsigned char* b_hi = a1_lo + kUOperandA;
+    unsigned char* b_lo = b_hi + kUOperandB;
+    float4* raw = reinterpret_cast<float4*>(b_lo + kUOperandB);   // [x][row]
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    for (int e = tid; e < kUR * kUChunks; e += blockDim.x) {
+        const int r = e / kUChunks, kc = e % kUChunks;
+        const float4 v = make_float4(W[r * kUR + 4 * kc], W[r * kUR + 4 * kc + 1], W[r * kUR + 4 * kc + 2],
+                                     W[r * kUR + 4 * kc + 3]);
+        split_store(b_hi, b_lo, kmajor_offset(r, 4 * kc), v);
+    }
+    if (tid == 0) {
+        s_fail = 0;
+        const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&s_bar));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&s_tmem));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kU2Cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&s_bar));
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((kUCols >> 3) << 17) | ((kUM >> 4) << 24);
+    const uint32_t sa0_hi = static_cast<uint32_t>(__cvta_generic_to_shared(a0_hi));
+    const uint32_t sa0_lo = static_cast<uint32_t>(__cvta_generic_to_shared(a0_lo));
+    const uint32_t sa1_hi = static_cast<uint32_t>(__cvta_generic_to_shared(a1_hi));
+    const uint32_t sa1_lo = static_cast<uint32_t>(__cvta_generic_to_shared(a1_lo));
+    const uint32_t sb_hi = static_cast<uint32_t>(__cvta_generic_to_shared(b_hi));
+    const uint32_t sb_lo = static_cast<uint32_t>(__cvta_generic_to_shared(b_lo));
+    uint32_t phase = 0;
+    constexpr uint64_t kTile = 2 * kUM;   // groups per tile
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * kTile;
+    auto issue = [&](uint64_t t) {
+        const uint64_t g0 = t + 2 * tid;
+        if (t < n_groups && g0 < n_groups) {
+            const uint64_t gb = insert_zeros(g0, a.pos, kUK);   // even: qubit 0 is not a target
+#pragma unroll
+            for (int x = 0; x < kUD; ++x) {
+                const uint32_t sd = static_cast<uint32_t>(__cvta_generic_to_shared(raw + x * kUM + tid));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sd), "l"(s + (gb | a.off[x]))
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * kTile;
+    issue(first);
+    for (uint64_t t0 = first; t0 < n_groups; t0 += stride) {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        const uint64_t g0 = t0 + 2 * tid;
+        const bool live = g0 < n_groups;
+        const uint64_t gb = live ? insert_zeros(g0, a.pos, kUK) : 0;
+#pragma unroll
+        for (int kc = 0; kc < kUD / 4; ++kc) {
+            float4 v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = live ? raw[(4 * kc + j) * kUM + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
+            split_store(a0_hi, a0_lo, kmajor_offset(tid, 4 * kc), make_float4(v[0].x, v[1].x, v[2].x, v[3].x));
+            split_store(a0_hi, a0_lo, kmajor_offset(tid, kUD + 4 * kc), make_float4(v[0].y, v[1].y, v[2].y, v[3].y));
+            split_store(a1_hi, a1_lo, kmajor_offset(tid, 4 * kc), make_float4(v[0].z, v[1].z, v[2].z, v[3].z));
+            split_store(a1_hi, a1_lo, kmajor_offset(tid, kUD + 4 * kc), make_float4(v[0].w, v[1].w, v[2].w, v[3].w));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+#pragma unroll
+            for (int ks = 0; ks < kUR / 8; ++ks) {
+                const uint32_t koff = ks * 256;
+                umma_tf32(tmem, smem_desc(sa0_hi + koff), smem_desc(sb_hi + koff), idesc, ks > 0 ? 1u : 0u);
+                umma_tf32(tmem, smem_desc(sa0_hi + koff), smem_desc(sb_lo + koff), idesc, 1u);
+                umma_tf32(tmem, smem_desc(sa0_lo + koff), smem_desc(sb_hi + koff), idesc, 1u);
+                umma_tf32(tmem + kUCols, smem_desc(sa1_hi + koff), smem_desc(sb_hi + koff), idesc, ks > 0 ? 1u : 0u);
+                umma_tf32(tmem + kUCols, smem_desc(sa1_hi + koff), smem_desc(sb_lo + koff), idesc, 1u);
+                umma_tf32(tmem + kUCols, smem_desc(sa1_lo + koff), smem_desc(sb_hi + koff), idesc, 1u);
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        // the raw slots this thread reads are its own and already converted: refill them
+        issue(t0 + stride);
+        const bool ok = mbar_wait(bar, phase);
+        phase ^= 1u;
+        if (!ok) s_fail = 1;
+        __syncthreads();
+        if (s_fail) {
+            if (tid == 0) atomicExch(err, 1);
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t d0[kUCols], d1[kUCols];
+        const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+#define QSV_TMEM_LD64(dst, addr)                                                                              \
+        asm volatile(                                                                                         \
+            "tcgen05.ld.sync.aligned.32x32b.x64.b32 "                                                         \
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"                                         \
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"                                \
+            "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"                                \
+            "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"                        \
+            : "=r"(dst[0]), "=r"(dst[1]), "=r"(dst[2]), "=r"(dst[3]), "=r"(dst[4]), "=r"(dst[5]), "=r"(dst[6]), \
+              "=r"(dst[7]), "=r"(dst[8]), "=r"(dst[9]), "=r"(dst[10]), "=r"(dst[11]), "=r"(dst[12]),          \
+              "=r"(dst[13]), "=r"(dst[14]), "=r"(dst[15]), "=r"(dst[16]), "=r"(dst[17]), "=r"(dst[18]),       \
+              "=r"(dst[19]), "=r"(dst[20]), "=r"(dst[21]), "=r"(dst[22]), "=r"(dst[23]), "=r"(dst[24]),       \
+              "=r"(dst[25]), "=r"(dst[26]), "=r"(dst[27]), "=r"(dst[28]), "=r"(dst[29]), "=r"(dst[30]),       \
+              "=r"(dst[31]), "=r"(dst[32]), "=r"(dst[33]), "=r"(dst[34]), "=r"(dst[35]), "=r"(dst[36]),       \
+              "=r"(dst[37]), "=r"(dst[38]), "=r"(dst[39]), "=r"(dst[40]), "=r"(dst[41]), "=r"(dst[42]),       \
+              "=r"(dst[43]), "=r"(dst[44]), "=r"(dst[45]), "=r"(dst[46]), "=r"(dst[47]), "=r"(dst[48]),       \
+              "=r"(dst[49]), "=r"(dst[50]), "=r"(dst[51]), "=r"(dst[52]), "=r"(dst[53]), "=r"(dst[54]),       \
+              "=r"(dst[55]), "=r"(dst[56]), "=r"(dst[57]), "=r"(dst[58]), "=r"(dst[59]), "=r"(dst[60]),       \
+              "=r"(dst[61]), "=r"(dst[62]), "=r"(dst[63])                                                     \
+            : "r"(addr))
+        QSV_TMEM_LD64(d0, taddr);
+        QSV_TMEM_LD64(d1, taddr + kUCols);
+#undef QSV_TMEM_LD64
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (live) {
+#pragma unroll
+            for (int x = 0; x < kUD; ++x)
+                __stcs(reinterpret_cast<float4*>(s + (gb | a.off[x])),
+                       make_float4(__uint_as_float(d0[x]), __uint_as_float(d0[kUD + x]), __uint_as_float(d1[x]),
+                                   __uint_as_float(d1[kUD + x])));
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kU2Cols));
+}
+
 }  // namespace
 
 bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspace& ws) {
@@ -281,6 +442,19 @@ bool launch_dense_umma(const Op& op, float2* s, int n, cudaStream_t st, Workspac
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense5_umma, kUThreads, kUSmem), "occupancy");
     const uint64_t groups = (1ull << n) >> kUK;
+    if (sorted[0] > 0) {   // qubit 0 untouched: neighbouring groups are adjacent amplitudes
+        check_cuda(cudaFuncSetAttribute(k_dense5_umma2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kU2Smem)), "umma2 smem");
+        int dev2 = 0, sms2 = 0;
+        check_cuda(cudaGetDevice(&dev2), "device");
+        check_cuda(cudaDeviceGetAttribute(&sms2, cudaDevAttrMultiProcessorCount, dev2), "sm count");
+        const uint64_t tiles2 = (groups + 2 * kUM - 1) / (2 * kUM);
+        const uint64_t grid2 = std::max<uint64_t>(1, std::min<uint64_t>(tiles2, static_cast<uint64_t>(sms2)));
+        k_dense5_umma2<<<static_cast<unsigned>(grid2), kUThreads, kU2Smem, st>>>(s, groups, dW, a, d_err);
+        check_cuda(cudaGetLastError(), "umma2 launch");
+        ws.tensor_pending = true;
+        return true;
+    }
     const uint64_t tiles = (groups + kUM - 1) / kUM;
     const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(sms) * std::max(per_sm, 1)));
     k_dense5_umma<<<static_cast<unsigned>(grid), kUThreads, kUSmem, st>>>(s, groups, dW, a, d_err);
