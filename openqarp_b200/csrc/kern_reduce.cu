@@ -137,58 +137,116 @@ struct TermPtrs {
     int n_groups;
 };
 
-template <typename T>
-__global__ void __launch_bounds__(kRed) k_transition(const vec2_t<T>* __restrict__ bra, const vec2_t<T>* __restrict__ ket,
-                                                     uint64_t dim, TermPtrs tp, double2* __restrict__ partials) {
-    double2 acc = make_double2(0, 0);
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
-        double tr = 0, ti = 0;   // sum_g conj(bra[i^x_g]) * w_g(i)
-        for (int g = 0; g < tp.n_groups; ++g) {
-            double wr = 0, wi = 0;
-            const int j1 = __ldg(tp.gstart + g + 1);
-            for (int j = __ldg(tp.gstart + g); j < j1; ++j) {
-                const double2 c = __ldg(tp.c + j);
-                const bool neg = __popcll(i & __ldg(tp.z + j)) & 1;
-                wr += neg ? -c.x : c.x;
-                wi += neg ? -c.y : c.y;
-            }
-            const vec2_t<T> b = bra[i ^ __ldg(tp.gx + g)];
-            const double br = b.x, bi = b.y;
-            tr = fma(br, wr, tr); tr = fma(bi, wi, tr);
-            ti = fma(br, wi, ti); ti = fma(-bi, wr, ti);
+// Index runs.  A warp step covers kRuns runs of 32 consecutive indices, i = base | r << 5 | lane,
+// with the low 5 + log2(kRuns) bits of base zero.  For any Z mask,
+//     parity(i & z) = parity((base | lane) & z) ^ parity(r & (z >> 5)),
+// so one 64-bit popcount gives a term's sign at all kRuns indices of a thread, the term tables
+// are read once per kRuns indices, and the kRuns loads of bra[i ^ x] are independent.  Each
+// index still sums its groups and terms in table order.
+constexpr int kRuns = 4;
+constexpr uint64_t kRunSpan = 32 * kRuns;
+
+__device__ __forceinline__ double unit_sign(uint32_t odd) {
+    return __longlong_as_double(0x3ff0000000000000ll | (static_cast<long long>(odd & 1u) << 63));
+}
+
+// w[r] = sum_j c_j (-1)^{parity((ib ^ r << 5) & z_j)} over the terms of group g
+__device__ __forceinline__ void group_weights(const TermPtrs& tp, int g, uint64_t ib, double (&wr)[kRuns],
+                                              double (&wi)[kRuns]) {
+#pragma unroll
+    for (int r = 0; r < kRuns; ++r) wr[r] = wi[r] = 0.0;
+    const int j1 = __ldg(tp.gstart + g + 1);
+    for (int j = __ldg(tp.gstart + g); j < j1; ++j) {
+        const uint64_t z = __ldg(tp.z + j);
+        const double2 c = __ldg(tp.c + j);
+        const uint32_t p = static_cast<uint32_t>(__popcll(ib & z));
+        const uint32_t q = static_cast<uint32_t>(z >> 5);
+#pragma unroll
+        for (int r = 0; r < kRuns; ++r) {
+            const double sg = unit_sign(p + static_cast<uint32_t>(__popc(static_cast<uint32_t>(r) & q)));
+            wr[r] = fma(sg, c.x, wr[r]);
+            wi[r] = fma(sg, c.y, wi[r]);
         }
-        const vec2_t<T> k = ket[i];
-        const double kr = k.x, ki = k.y;
-        acc.x = fma(tr, kr, acc.x); acc.x = fma(-ti, ki, acc.x);
-        acc.y = fma(tr, ki, acc.y); acc.y = fma(ti, kr, acc.y);
     }
-    acc = block_sum(acc);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRed, 3) k_transition(const vec2_t<T>* __restrict__ bra, const vec2_t<T>* __restrict__ ket,
+                                                        uint64_t dim, TermPtrs tp, double2* __restrict__ partials) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t step = ((static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5) * kRunSpan;
+    double ar = 0, ai = 0;
+    for (uint64_t base = warp * kRunSpan; base < dim; base += step) {
+        double tr[kRuns], ti[kRuns];   // sum_g conj(bra[i ^ x_g]) * w_g(i)
+        bool ok[kRuns];
+#pragma unroll
+        for (int r = 0; r < kRuns; ++r) {
+            tr[r] = ti[r] = 0.0;
+            ok[r] = (base | (static_cast<uint64_t>(r) << 5) | lane) < dim;
+        }
+        for (int g = 0; g < tp.n_groups; ++g) {
+            const uint64_t x = __ldg(tp.gx + g);
+            vec2_t<T> b[kRuns];
+#pragma unroll
+            for (int r = 0; r < kRuns; ++r)
+                b[r] = ok[r] ? bra[(base | (static_cast<uint64_t>(r) << 5) | lane) ^ x] : mk<T>(T(0), T(0));
+            double wr[kRuns], wi[kRuns];
+            group_weights(tp, g, base | lane, wr, wi);
+#pragma unroll
+            for (int r = 0; r < kRuns; ++r) {
+                const double br = b[r].x, bi = b[r].y;
+                tr[r] = fma(br, wr[r], tr[r]); tr[r] = fma(bi, wi[r], tr[r]);
+                ti[r] = fma(br, wi[r], ti[r]); ti[r] = fma(-bi, wr[r], ti[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kRuns; ++r) {
+            if (!ok[r]) continue;
+            const vec2_t<T> k = ket[base | (static_cast<uint64_t>(r) << 5) | lane];
+            const double kr = k.x, ki = k.y;
+            ar = fma(tr[r], kr, ar); ar = fma(-ti[r], ki, ar);
+            ai = fma(tr[r], ki, ai); ai = fma(ti[r], kr, ai);
+        }
+    }
+    const double2 acc = block_sum(make_double2(ar, ai));
     if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
-// out[k] = sum_g psi[k^x_g] * sum_j c_j (-1)^{popcount((k^x_g) & z_j)}
+// out[k] = sum_g psi[k^x_g] * sum_j c_j (-1)^{popcount((k^x_g) & z_j)}, in the index runs above
 template <typename T>
-__global__ void __launch_bounds__(kRed) k_apply_obs(const vec2_t<T>* __restrict__ psi, vec2_t<T>* __restrict__ out,
-                                                    uint64_t dim, TermPtrs tp) {
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < dim; k += stride) {
-        double orr = 0, oi = 0;
-        for (int g = 0; g < tp.n_groups; ++g) {
-            const uint64_t src = k ^ __ldg(tp.gx + g);
-            double wr = 0, wi = 0;
-            const int j1 = __ldg(tp.gstart + g + 1);
-            for (int j = __ldg(tp.gstart + g); j < j1; ++j) {
-                const double2 c = __ldg(tp.c + j);
-                const bool neg = __popcll(src & __ldg(tp.z + j)) & 1;
-                wr += neg ? -c.x : c.x;
-                wi += neg ? -c.y : c.y;
-            }
-            const vec2_t<T> p = psi[src];
-            orr = fma(wr, p.x, orr); orr = fma(-wi, p.y, orr);
-            oi = fma(wr, p.y, oi); oi = fma(wi, p.x, oi);
+__global__ void __launch_bounds__(kRed, 3) k_apply_obs(const vec2_t<T>* __restrict__ psi, vec2_t<T>* __restrict__ out,
+                                                       uint64_t dim, TermPtrs tp) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t step = ((static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5) * kRunSpan;
+    for (uint64_t base = warp * kRunSpan; base < dim; base += step) {
+        double orr[kRuns], oi[kRuns];
+        bool ok[kRuns];
+#pragma unroll
+        for (int r = 0; r < kRuns; ++r) {
+            orr[r] = oi[r] = 0.0;
+            ok[r] = (base | (static_cast<uint64_t>(r) << 5) | lane) < dim;
         }
-        out[k] = mk<T>(static_cast<T>(orr), static_cast<T>(oi));
+        for (int g = 0; g < tp.n_groups; ++g) {
+            const uint64_t x = __ldg(tp.gx + g);
+            vec2_t<T> p[kRuns];
+#pragma unroll
+            for (int r = 0; r < kRuns; ++r)
+                p[r] = ok[r] ? psi[(base | (static_cast<uint64_t>(r) << 5) | lane) ^ x] : mk<T>(T(0), T(0));
+            double wr[kRuns], wi[kRuns];
+            group_weights(tp, g, (base | lane) ^ x, wr, wi);
+#pragma unroll
+            for (int r = 0; r < kRuns; ++r) {
+                const double pr = p[r].x, pi = p[r].y;
+                orr[r] = fma(wr[r], pr, orr[r]); orr[r] = fma(-wi[r], pi, orr[r]);
+                oi[r] = fma(wr[r], pi, oi[r]); oi[r] = fma(wi[r], pr, oi[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kRuns; ++r)
+            if (ok[r])
+                out[base | (static_cast<uint64_t>(r) << 5) | lane] = mk<T>(static_cast<T>(orr[r]), static_cast<T>(oi[r]));
     }
 }
 
@@ -512,7 +570,9 @@ void apply_observable(const vec2_t<T>* psi, vec2_t<T>* out, int n, const PauliTe
         return;
     }
     TermPtrs tp = upload_terms(terms, st, ws);
-    k_apply_obs<T><<<grid_for(dim, 1, 1u << 20), kRed, 0, st>>>(psi, out, dim, tp);
+    const uint64_t warps = (dim + kRunSpan - 1) / kRunSpan;
+    const unsigned nb = static_cast<unsigned>(std::min<uint64_t>((warps + kRed / 32 - 1) / (kRed / 32), kRedBlocks));
+    k_apply_obs<T><<<nb, kRed, 0, st>>>(psi, out, dim, tp);
     check_cuda(cudaGetLastError(), "observable launch");
 }
 

@@ -9,6 +9,8 @@
     python -m openqarp_b200.profile_cases parity --n 26 --shots 1048576 --terms 512
     python -m openqarp_b200.profile_cases perm --n 26
     python -m openqarp_b200.profile_cases traj --n 16 --depth 8 --shots 4096 [--noisy] [--batch 0]
+    python -m openqarp_b200.profile_cases heisenberg --n 26 --dtype complex64 --k 0
+    python -m openqarp_b200.profile_cases qaoa --shots 256
 
 Registers of 2^26 complex128 amplitudes (1 GiB) exceed L2 (126 MB), so DRAM counters are
 meaningful, and stay small enough for a full-set capture to end within minutes.
@@ -25,7 +27,7 @@ from . import Register, circuits, ir, observable
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["dense", "brickwork", "transition", "adjoint", "sample", "exact", "parity",
-                                     "perm", "traj"])
+                                     "perm", "traj", "heisenberg", "qaoa"])
     ap.add_argument("--n", type=int, default=26)
     ap.add_argument("--k", type=int, default=3)
     ap.add_argument("--reps", type=int, default=5)
@@ -88,6 +90,19 @@ def main(argv=None):
         for _ in range(a.reps):
             reg.reset()
             reg.run_trajectories(buf, 1234, a.shots)
+    elif a.case == "heisenberg":
+        # one second-order Trotter step of the 31-qubit configuration's chain at width n; with
+        # --k 0 every bond rotation and field runs as its own elementwise pass
+        fields = np.random.default_rng(1234).uniform(-1.0, 1.0, a.n)
+        reg.apply(ir.pack(circuits.heisenberg_trotter(a.n, 1, 0.05, fields)).buf)
+    elif a.case == "qaoa":
+        # the batched-QAOA configuration's instance mix, --shots instances, one persistent launch
+        from .batch import QaoaBatch, config4_instances
+        inst, params = config4_instances(count=a.shots)
+        qb = QaoaBatch(inst)
+        for _ in range(a.reps):
+            qb.run(params, with_gradient=True)
+        qb.close()
     reg.synchronize()
     reg.close()
     print("ok", a.case)
