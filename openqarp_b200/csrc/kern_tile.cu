@@ -20,14 +20,17 @@ namespace {
 
 constexpr int kTileThreads = 512;
 constexpr int kTileCoefMax = 256;   // widest op: a 4-qubit dense block or an 8-qubit diagonal
+constexpr int kAdjSlotsMax = 64;    // ADJ steps per adjoint tile pass (shared-memory accumulators)
 
-enum : uint8_t { T_DENSE = 1, T_DIAG, T_PHASE, T_CTRL1, T_SWAP, T_PAULI, T_SCALE };
+enum : uint8_t { T_DENSE = 1, T_DIAG, T_PHASE, T_CTRL1, T_SWAP, T_PAULI, T_SCALE, T_ADJ };
 
 struct TileOpDev {
     uint8_t kind, k, nlz, pad0;
     uint32_t coef;          // offset into the coefficient array
     uint32_t ncoef;         // coefficients of this op (staged in shared memory before use)
-    uint32_t pad1;
+    uint32_t slot;          // ADJ: pass-local inner-product slot (the kernel's accumulators)
+    uint32_t gslot;         // ADJ: slot of the sweep (row of the partials table)
+    uint32_t pad2;
     uint8_t lpos[8];        // local bit of op-local bit b (0xff: outside the tile)
     uint8_t gq[8];          // global qubit of op-local bit b (DIAG)
     uint64_t lmask;         // PHASE/CTRL1 local controls; PAULI local x mask
@@ -40,6 +43,7 @@ struct TilePassDev {
     uint32_t op_begin, op_end;
     int32_t m;
     uint8_t tq[16];         // global qubit of local bit j, ascending
+    uint32_t n_adj;         // ADJ steps of the pass (adjoint sweep)
 };
 
 __device__ __forceinline__ uint32_t ins_zero32(uint32_t g, uint32_t p) {
@@ -293,6 +297,190 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
     cp_async_wait0();
 }
 
+// ---------------------------------------------------------------- adjoint reverse sweep
+// One reverse step of a parametric gate on a tile pair: with a, f the tiles of psi and phi after
+// the gate, accumulate <phi| G |psi> over the tile (FP64) and apply D (the gate's dagger) to both.
+// coef holds D then G, each 2^K x 2^K.  A thread owns the same groups in both parts, so the step
+// needs no barrier of its own; the caller reduces the returned per-thread partial.
+template <typename T, int K>
+__device__ __forceinline__ double2 tile_adj(vec2_t<T>* a, vec2_t<T>* f, int m, const TileOpDev& op,
+                                            const cplx<T>* coef) {
+    constexpr int D = 1 << K;
+    uint32_t loff[D];
+    uint8_t sp[K > 0 ? K : 1];
+#pragma unroll
+    for (int x = 0; x < D; ++x) {
+        uint32_t o = 0;
+#pragma unroll
+        for (int b = 0; b < K; ++b) if ((x >> b) & 1) o |= 1u << op.lpos[b];
+        loff[x] = o;
+    }
+#pragma unroll
+    for (int b = 0; b < K; ++b) sp[b] = op.lpos[b];
+    if constexpr (K == 2)
+        if (sp[1] < sp[0]) { const uint8_t t = sp[0]; sp[0] = sp[1]; sp[1] = t; }
+    const cplx<T>* Dm = coef;
+    const cplx<T>* Gm = coef + D * D;
+    double ar = 0, ai = 0;
+    const uint32_t groups = 1u << (m - K);
+    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
+        uint32_t b0 = g;
+#pragma unroll
+        for (int b = 0; b < K; ++b) b0 = ins_zero32(b0, sp[b]);
+        vec2_t<T> ps[D], ph[D];
+#pragma unroll
+        for (int x = 0; x < D; ++x) {
+            ps[x] = a[b0 | loff[x]];
+            ph[x] = f[b0 | loff[x]];
+        }
+#pragma unroll
+        for (int y = 0; y < D; ++y) {
+            double gr = 0, gi = 0;
+#pragma unroll
+            for (int x = 0; x < D; ++x) {
+                const double cr = static_cast<double>(Gm[y * D + x].re), ci = static_cast<double>(Gm[y * D + x].im);
+                const double xr = static_cast<double>(ps[x].x), xi = static_cast<double>(ps[x].y);
+                gr = fma(cr, xr, gr); gr = fma(-ci, xi, gr);
+                gi = fma(cr, xi, gi); gi = fma(ci, xr, gi);
+            }
+            const double fr = static_cast<double>(ph[y].x), fi = static_cast<double>(ph[y].y);
+            ar = fma(fr, gr, ar); ar = fma(fi, gi, ar);
+            ai = fma(fr, gi, ai); ai = fma(-fi, gr, ai);
+        }
+#pragma unroll
+        for (int y = 0; y < D; ++y) {
+            vec2_t<T> o1 = cmul<T>(Dm[y * D], ps[0]);
+            vec2_t<T> o2 = cmul<T>(Dm[y * D], ph[0]);
+#pragma unroll
+            for (int x = 1; x < D; ++x) {
+                o1 = cfma<T>(Dm[y * D + x], ps[x], o1);
+                o2 = cfma<T>(Dm[y * D + x], ph[x], o2);
+            }
+            a[b0 | loff[y]] = o1;
+            f[b0 | loff[y]] = o2;
+        }
+    }
+    return make_double2(ar, ai);
+}
+
+constexpr int kAdjWarps = kTileThreads / 32;
+
+__device__ __forceinline__ double2 warp_sum2(double2 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+
+// The reverse sweep's tile pass: k_tile_pass over the tile pair (psi, phi), every op applied
+// to both, and ADJ steps accumulating their inner products per warp in shared memory (each
+// warp adds only to its own entry, in tile order).  At the end the CTA writes one partial per
+// ADJ step: partials[slot * gridDim.x + blockIdx.x], summed over warps in fixed order.
+template <typename T>
+__global__ void __launch_bounds__(kTileThreads, 1) k_adj_tile(vec2_t<T>* __restrict__ psi, vec2_t<T>* __restrict__ phi,
+                                                              int n, const TilePassDev* __restrict__ passes, int pass_idx,
+                                                              const TileOpDev* __restrict__ ops,
+                                                              const cplx<T>* __restrict__ coef,
+                                                              double2* __restrict__ partials) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const TilePassDev P = passes[pass_idx];
+    const int m = P.m;
+    const uint32_t M = 1u << m;
+    vec2_t<T>* bufs = reinterpret_cast<vec2_t<T>*>(smem_raw);   // [psi0, phi0, psi1, phi1]
+    cplx<T>* scoef = reinterpret_cast<cplx<T>*>(bufs + 4 * M);
+    double2* acc = reinterpret_cast<double2*>(scoef + kTileCoefMax);   // [local slot][warp]
+    const uint32_t n_adj = P.n_adj;
+    for (uint32_t e = threadIdx.x; e < n_adj * kAdjWarps; e += blockDim.x) acc[e] = make_double2(0, 0);
+    constexpr int kAmpsPerChunk = 16 / sizeof(vec2_t<T>);
+    constexpr int acl = kAmpsPerChunk == 2 ? 1 : 0;
+    constexpr int hi_shift = 9 + acl;
+    const uint32_t R = M >> hi_shift;
+    const uint32_t lt = threadIdx.x << acl;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t dep_lo = 0;
+    for (int j = 0; j < hi_shift && j < m; ++j)
+        if ((lt >> j) & 1u) dep_lo |= 1ull << P.tq[j];
+    auto dep_hi = [&](uint32_t r) {
+        uint64_t d = 0;
+        for (int j = hi_shift; j < m; ++j)
+            if ((r >> (j - hi_shift)) & 1u) d |= 1ull << P.tq[j];
+        return d;
+    };
+    auto tile_base = [&](uint64_t t) {
+        uint64_t base = t;
+        for (int j = 0; j < m; ++j) {
+            const uint64_t p = P.tq[j];
+            base = ((base >> p) << (p + 1)) | (base & ((1ull << p) - 1ull));
+        }
+        return base;
+    };
+    auto issue = [&](vec2_t<T>* dst, uint64_t base) {
+        for (uint32_t r = 0; r < R; ++r) {
+            const uint64_t gi = base | dep_lo | dep_hi(r);
+            cp_async16(dst + (lt + (r << hi_shift)), psi + gi);
+            cp_async16(dst + M + (lt + (r << hi_shift)), phi + gi);
+        }
+    };
+    const uint64_t n_tiles = 1ull << (n - m);
+    const uint64_t G = gridDim.x;
+    uint64_t t = blockIdx.x;
+    if (t < n_tiles) issue(bufs, tile_base(t));
+    cp_async_commit();
+    for (uint32_t i = 0; t < n_tiles; t += G, ++i) {
+        vec2_t<T>* cur = (i & 1u) ? bufs + 2 * M : bufs;
+        vec2_t<T>* nxt = (i & 1u) ? bufs : bufs + 2 * M;
+        if (t + G < n_tiles) issue(nxt, tile_base(t + G));
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        const uint64_t base = tile_base(t);
+        for (uint32_t o = P.op_begin; o < P.op_end; ++o) {
+            const TileOpDev& op = ops[o];
+            for (uint32_t e = threadIdx.x; e < op.ncoef; e += blockDim.x) scoef[e] = coef[op.coef + e];
+            __syncthreads();
+            if (op.kind == T_ADJ) {
+                double2 v;
+                switch (op.k) {
+                    case 0: v = tile_adj<T, 0>(cur, cur + M, m, op, scoef); break;
+                    case 1: v = tile_adj<T, 1>(cur, cur + M, m, op, scoef); break;
+                    default: v = tile_adj<T, 2>(cur, cur + M, m, op, scoef); break;
+                }
+                v = warp_sum2(v);
+                if (lane == 0) {
+                    double2& e = acc[op.slot * kAdjWarps + warp];
+                    e.x += v.x;
+                    e.y += v.y;
+                }
+            } else {
+                tile_op<T>(cur, m, base, op, scoef);
+                tile_op<T>(cur + M, m, base, op, scoef);
+            }
+            __syncthreads();
+        }
+        for (uint32_t r = 0; r < R; ++r) {
+            const uint32_t l = lt + (r << hi_shift);
+            const uint64_t gi = base | dep_lo | dep_hi(r);
+            __stcs(reinterpret_cast<float4*>(psi + gi), *reinterpret_cast<const float4*>(cur + l));
+            __stcs(reinterpret_cast<float4*>(phi + gi), *reinterpret_cast<const float4*>(cur + M + l));
+        }
+        __syncthreads();
+    }
+    cp_async_wait0();
+    __syncthreads();
+    for (uint32_t o = P.op_begin + threadIdx.x; o < P.op_end; o += blockDim.x) {
+        const TileOpDev& op = ops[o];
+        if (op.kind != T_ADJ) continue;
+        double2 v = make_double2(0, 0);
+        for (int w = 0; w < kAdjWarps; ++w) {
+            v.x += acc[op.slot * kAdjWarps + w].x;
+            v.y += acc[op.slot * kAdjWarps + w].y;
+        }
+        partials[static_cast<size_t>(op.gslot) * gridDim.x + blockIdx.x] = v;
+    }
+}
+
 }  // namespace
 
 // Encode the passes for the device and launch them in order on `st`.
@@ -441,6 +629,187 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
     }
     // `host` is pageable: cudaMemcpyAsync returned only after staging it, so it may go now
 }
+
+unsigned adjoint_tile_grid(int n, int m) {
+    int sms = 0, device = 0;
+    check_cuda(cudaGetDevice(&device), "device");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
+    const uint64_t n_tiles = 1ull << (n - std::min(m, n));
+    return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sms))));
+}
+
+template <typename T>
+void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* phi, int n, int m,
+                       double* d_partials, unsigned nb, cudaStream_t st, Workspace& ws,
+                       const std::function<void(const Op&)>& stream_op, uint64_t* launches) {
+    if (ops.empty()) return;
+    if (m < kTileMinQubits || m > n) throw std::logic_error("adjoint tile width outside the kernel's range");
+    const std::vector<TilePass> planned = plan_tiles(ops, n, m);
+    // split tile passes whose ADJ steps overflow the kernel's accumulators
+    std::vector<TilePass> passes;
+    for (const TilePass& p : planned) {
+        if (p.tile_qubits.empty()) { passes.push_back(p); continue; }
+        TilePass cur;
+        cur.tile_qubits = p.tile_qubits;
+        int adj = 0;
+        for (const Op& o : p.ops) {
+            if (o.kind == OP_ADJ && adj == kAdjSlotsMax) {
+                passes.push_back(std::move(cur));
+                cur = TilePass{};
+                cur.tile_qubits = p.tile_qubits;
+                adj = 0;
+            }
+            if (o.kind == OP_ADJ) ++adj;
+            cur.ops.push_back(o);
+        }
+        passes.push_back(std::move(cur));
+    }
+    std::vector<TilePassDev> pdev;
+    std::vector<TileOpDev> odev;
+    std::vector<cplx<T>> cdev;
+    for (const TilePass& p : passes) {
+        if (p.tile_qubits.empty()) continue;
+        TilePassDev pd{};
+        pd.m = static_cast<int32_t>(p.tile_qubits.size());
+        if (pd.m != m) throw std::logic_error("adjoint tile pass of an unexpected width");
+        for (size_t j = 0; j < p.tile_qubits.size(); ++j) pd.tq[j] = static_cast<uint8_t>(p.tile_qubits[j]);
+        int local_of[64];
+        for (int q = 0; q < 64; ++q) local_of[q] = -1;
+        for (size_t j = 0; j < p.tile_qubits.size(); ++j) local_of[p.tile_qubits[j]] = static_cast<int>(j);
+        auto lmask_of = [&](uint64_t gm, uint64_t* outside) {
+            uint64_t lm = 0, out = 0;
+            for (int q = 0; q < 64; ++q)
+                if ((gm >> q) & 1) {
+                    if (local_of[q] >= 0) lm |= 1ull << local_of[q];
+                    else out |= 1ull << q;
+                }
+            if (outside) *outside = out;
+            return lm;
+        };
+        pd.op_begin = static_cast<uint32_t>(odev.size());
+        for (const Op& o : p.ops) {
+            const uint64_t mix = op_mixing_mask(o);
+            for (int q = 0; q < 64; ++q)
+                if (((mix >> q) & 1) && (q >= n || local_of[q] < 0))
+                    throw std::logic_error("tile planner placed an op whose qubit " + std::to_string(q) +
+                                           " is outside its tile");
+            if (o.kind == OP_DENSE && o.k > 4) throw std::logic_error("dense block too wide for a tile");
+            if (o.kind == OP_DIAG && o.k > 8) throw std::logic_error("diagonal too wide for a tile");
+            TileOpDev d{};
+            std::memset(d.lpos, 0xff, sizeof d.lpos);
+            d.coef = static_cast<uint32_t>(cdev.size());
+            d.k = static_cast<uint8_t>(o.k);
+            auto push = [&](c128 v) { cdev.push_back(cplx<T>{static_cast<T>(v.real()), static_cast<T>(v.imag())}); };
+            switch (o.kind) {
+                case OP_ADJ: {
+                    if (o.k < 0 || o.k > 2) throw std::logic_error("adjoint step wider than two qubits");
+                    const size_t dd = size_t{1} << (2 * o.k);
+                    if (o.m.size() != dd || o.g.size() != dd) throw std::logic_error("adjoint step matrices");
+                    d.kind = T_ADJ;
+                    for (int b = 0; b < o.k; ++b) d.lpos[b] = static_cast<uint8_t>(local_of[o.qubits[b]]);
+                    for (const c128& v : o.m) push(v);
+                    for (const c128& v : o.g) {
+                        // generators are sums of Pauli products and projectors with coefficients
+                        // 0, +-1/2, +-1: exact in either precision
+                        if (static_cast<double>(static_cast<T>(v.real())) != v.real() ||
+                            static_cast<double>(static_cast<T>(v.imag())) != v.imag())
+                            throw std::logic_error("adjoint generator not exact in the register precision");
+                        push(v);
+                    }
+                    d.slot = pd.n_adj++;
+                    d.gslot = static_cast<uint32_t>(o.slot);
+                    break;
+                }
+                case OP_DENSE:
+                    d.kind = T_DENSE;
+                    for (int b = 0; b < o.k; ++b) d.lpos[b] = static_cast<uint8_t>(local_of[o.qubits[b]]);
+                    for (const c128& v : o.m) push(v);
+                    break;
+                case OP_DIAG:
+                    d.kind = T_DIAG;
+                    for (int b = 0; b < o.k; ++b) {
+                        d.gq[b] = static_cast<uint8_t>(o.qubits[b]);
+                        d.lpos[b] = local_of[o.qubits[b]] >= 0 ? static_cast<uint8_t>(local_of[o.qubits[b]]) : 0xff;
+                    }
+                    for (const c128& v : o.m) push(v);
+                    break;
+                case OP_PHASE:
+                    d.kind = T_PHASE;
+                    d.lmask = lmask_of(o.mask, &d.gmask);
+                    push(o.m[0]);
+                    break;
+                case OP_CTRL1:
+                    d.kind = T_CTRL1;
+                    d.lmask = lmask_of(o.mask, &d.gmask);
+                    d.lpos[0] = static_cast<uint8_t>(local_of[o.target]);
+                    for (int e = 0; e < 4; ++e) push(o.m[e]);
+                    break;
+                case OP_SWAP:
+                    d.kind = T_SWAP;
+                    d.lpos[0] = static_cast<uint8_t>(local_of[o.qubits[0]]);
+                    d.lpos[1] = static_cast<uint8_t>(local_of[o.qubits[1]]);
+                    break;
+                case OP_PAULI_ROT:
+                    d.kind = T_PAULI;
+                    d.lmask = lmask_of(o.mask, nullptr);
+                    d.lz = lmask_of(o.zmask, &d.gz);
+                    d.nlz = static_cast<uint8_t>(__builtin_popcountll(o.mask & o.zmask) & 3);
+                    push(o.m[0]);
+                    break;
+                case OP_SCALE:
+                    d.kind = T_SCALE;
+                    push(o.m[0]);
+                    break;
+                default:
+                    throw std::logic_error("adjoint tile pass holds an op the tile kernel cannot apply");
+            }
+            d.ncoef = static_cast<uint32_t>(cdev.size()) - d.coef;
+            if (d.ncoef > static_cast<uint32_t>(kTileCoefMax)) throw std::logic_error("tile op coefficients overflow");
+            odev.push_back(d);
+        }
+        pd.op_end = static_cast<uint32_t>(odev.size());
+        pdev.push_back(pd);
+    }
+    const size_t a_p = 0;
+    const size_t a_o = (pdev.size() * sizeof(TilePassDev) + 255) & ~size_t{255};
+    const size_t a_c = a_o + ((odev.size() * sizeof(TileOpDev) + 255) & ~size_t{255});
+    const size_t total = a_c + cdev.size() * sizeof(cplx<T>) + 256;
+    std::vector<uint8_t> host(total, 0);
+    if (!pdev.empty()) std::memcpy(host.data() + a_p, pdev.data(), pdev.size() * sizeof(TilePassDev));
+    if (!odev.empty()) std::memcpy(host.data() + a_o, odev.data(), odev.size() * sizeof(TileOpDev));
+    if (!cdev.empty()) std::memcpy(host.data() + a_c, cdev.data(), cdev.size() * sizeof(cplx<T>));
+    check_cuda(cudaStreamSynchronize(st), "tile descriptor reuse");
+    uint8_t* dev = static_cast<uint8_t*>(ws.tiles(total));
+    check_cuda(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, st), "tile descriptors");
+    const TilePassDev* d_p = reinterpret_cast<const TilePassDev*>(dev + a_p);
+    const TileOpDev* d_o = reinterpret_cast<const TileOpDev*>(dev + a_o);
+    const cplx<T>* d_c = reinterpret_cast<const cplx<T>*>(dev + a_c);
+    if (nb != adjoint_tile_grid(n, m)) throw std::logic_error("adjoint partials sized for another grid");
+    const size_t smem = 4 * (size_t{1} << m) * sizeof(vec2_t<T>) + kTileCoefMax * sizeof(cplx<T>) +
+                        static_cast<size_t>(kAdjSlotsMax) * kAdjWarps * sizeof(double2);
+    check_cuda(cudaFuncSetAttribute(k_adj_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)), "adjoint tile smem");
+    int pi = 0;
+    for (const TilePass& p : passes) {
+        if (p.tile_qubits.empty()) {
+            for (const Op& o : p.ops) {
+                if (o.kind == OP_ADJ) throw std::logic_error("adjoint step planned outside a tile");
+                stream_op(o);
+            }
+            continue;
+        }
+        k_adj_tile<T><<<nb, kTileThreads, smem, st>>>(psi, phi, n, d_p, pi, d_o, d_c,
+                                                      reinterpret_cast<double2*>(d_partials));
+        check_cuda(cudaGetLastError(), "adjoint tile pass launch");
+        if (launches) ++*launches;
+        ++pi;
+    }
+}
+
+template void run_adjoint_tiled<double>(const std::vector<Op>&, double2*, double2*, int, int, double*, unsigned,
+                                        cudaStream_t, Workspace&, const std::function<void(const Op&)>&, uint64_t*);
+template void run_adjoint_tiled<float>(const std::vector<Op>&, float2*, float2*, int, int, double*, unsigned,
+                                       cudaStream_t, Workspace&, const std::function<void(const Op&)>&, uint64_t*);
 
 template void run_tiled<double>(const std::vector<TilePass>&, double2*, int, cudaStream_t, Workspace&,
                                 const std::function<void(const Op&)>&, bool);

@@ -85,6 +85,17 @@ template <typename T>
 void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
                const std::function<void(const Op&)>& stream_op, bool register_tiles);
 
+// The adjoint's reverse sweep in tile passes (kern_tile.cu): `ops` is the reverse stream (the
+// lowered daggers of non-parametric commands and OP_ADJ steps), planned into passes of m tile
+// qubits over both states; every OP_ADJ step writes partials[slot * nb + b] (double2) for the
+// nb = adjoint_tile_grid(n, m) CTAs.  Ops no tile holds go to `stream_op`, which applies them to
+// both states.
+unsigned adjoint_tile_grid(int n, int m);
+template <typename T>
+void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* phi, int n, int m,
+                       double* d_partials, unsigned nb, cudaStream_t st, Workspace& ws,
+                       const std::function<void(const Op&)>& stream_op, uint64_t* launches);
+
 // ---------------------------------------------------------------- register tiles (kern_tile_rt.cu)
 struct RtUpload {
     const void* passes = nullptr;

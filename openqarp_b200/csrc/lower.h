@@ -80,6 +80,8 @@ enum OpKind : int {
     OP_PAULI_ROT,   // exp(-i theta/2 P), P by (mask = X|Y bits, zmask = Z|Y bits); m[0] = (cos, sin)
     OP_SCALE,       // every amplitude times m[0]
     OP_PERM,        // out-of-place permutation of basis states on qubits[0..k) (table)
+    OP_ADJ,         // adjoint reverse step on qubits[0..k) (k <= 2): accumulate <phi| g |psi> into
+                    // `slot`, then apply m (the gate's dagger) to both states
 };
 
 struct Op {
@@ -92,6 +94,8 @@ struct Op {
     std::vector<c128> m;
     std::vector<uint64_t> table;   // OP_PERM
     std::vector<uint32_t> pq;      // OP_PERM qubits (may exceed 8)
+    std::vector<c128> g;           // OP_ADJ: generator matrix (2^k x 2^k)
+    int slot = -1;                 // OP_ADJ: inner-product slot
     int n_gates = 1;
 };
 

@@ -810,56 +810,113 @@ void adjoint_forward(Handle* h, const std::vector<Cmd>& cs, Checkpoints& ck) {
     }
 }
 
+// Tile width of the reverse sweep's passes: the tile pair (psi and phi), double-buffered, takes
+// 4 x 2^m amplitudes of shared memory — 128 KiB at m = 11 (complex128) or 12 (complex64).
+template <typename T>
+constexpr int adjoint_tile_qubits() {
+    return sizeof(T) == sizeof(double) ? 11 : 12;
+}
+
 template <typename T>
 void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps, vec2_t<T>* psi,
                    vec2_t<T>* phi, double* grad, const Checkpoints& ck) {
     const int n = h->n;
-    // count parametric steps, build them
     struct Slot { size_t cmd; c128 pref; };
     std::vector<Slot> slots;
-    const unsigned nb = adjoint_blocks(n);
     size_t n_param_steps = 0;
     for (size_t i = 0; i < cmds.size(); ++i)
         if (deps.ptr[i + 1] > deps.ptr[i]) ++n_param_steps;
+    // the reverse step of parametric command c: its generator G, the dagger D and their qubits
+    auto param_step = [&](const Cmd& c, c128* pref) {
+        AdjStep st;
+        if (!generator(c, pref, &st.G, &st.k))
+            throw capability_error(
+                "run_gradient: gate '" + std::to_string(c.gate) +
+                "' carries a symbolic parameter but has no adjoint generator rule "
+                "(Rx/Ry/Rz/P/GPhase/CRx/CRy/CRz/CP/RXX/RYY/RZZ); rebase it to those gates "
+                "before differentiating.");
+        st.qubits[0] = st.k > 0 ? c.q[0] : 0;
+        st.qubits[1] = st.k > 1 ? c.q[1] : 0;
+        for (int b = 0; b < st.k; ++b)
+            if (static_cast<int>(c.q[b]) >= n) throw std::invalid_argument("gate qubit outside the register");
+        if (st.k == 0) {
+            const double th = -c.p.at(0);
+            st.D = {c128(std::cos(th), std::sin(th))};
+        } else {
+            st.D = local_unitary(dagger(c));
+        }
+        return st;
+    };
+    // psi is now the state before command idx: restart it from the checkpoint there
+    auto at_checkpoint = [&](size_t idx) { return ck.K && idx > 0 && idx % ck.K == 0; };
+    auto restore = [&](size_t idx) {
+        check_cuda(cudaMemcpyAsync(psi, ck.bufs.at(idx / ck.K - 1), h->dim() * h->amp_bytes(),
+                                   cudaMemcpyDeviceToDevice, h->stream), "checkpoint restore");
+    };
+    const int mt = adjoint_tile_qubits<T>();
+    const bool tiled = n >= mt + 3;
+    // tiled: the reverse stream runs as tile passes over both states, several reverse steps a
+    // pass; narrower registers take one launch per reverse step
+    const unsigned nb = tiled ? adjoint_tile_grid(n, mt) : adjoint_blocks(n);
     double* partials = static_cast<double*>(
         h->ws.scratch((n_param_steps * nb + n_param_steps + 1) * 2 * sizeof(double)));
-    for (size_t idx = cmds.size(); idx-- > 0;) {
-        const Cmd& c = cmds[idx];
-        const Cmd d = dagger(c);
-        if (deps.ptr[idx + 1] > deps.ptr[idx]) {
-            AdjStep st;
-            c128 pref;
-            if (!generator(c, &pref, &st.G, &st.k))
-                throw capability_error(
-                    "run_gradient: gate '" + std::to_string(c.gate) +
-                    "' carries a symbolic parameter but has no adjoint generator rule "
-                    "(Rx/Ry/Rz/P/GPhase/CRx/CRy/CRz/CP/RXX/RYY/RZZ); rebase it to those gates "
-                    "before differentiating.");
-            st.qubits[0] = st.k > 0 ? c.q[0] : 0;
-            st.qubits[1] = st.k > 1 ? c.q[1] : 0;
-            for (int b = 0; b < st.k; ++b)
-                if (static_cast<int>(c.q[b]) >= n) throw std::invalid_argument("gate qubit outside the register");
-            if (st.k == 0) {
-                const double th = -c.p.at(0);
-                st.D = {c128(std::cos(th), std::sin(th))};
+    if (tiled) {
+        std::vector<Op> segment;
+        auto stream_op = [&](const Op& o) {
+            launch(h, o, psi);
+            launch(h, o, phi);
+        };
+        auto flush = [&]() {
+            uint64_t launches = 0;
+            run_adjoint_tiled<T>(segment, psi, phi, n, mt, partials, nb, h->stream, h->ws, stream_op, &launches);
+            h->stats.launches += launches;
+            h->stats.passes += launches;
+            h->stats.hbm_bytes += launches * 4ull * h->dim() * h->amp_bytes();
+            segment.clear();
+        };
+        for (size_t idx = cmds.size(); idx-- > 0;) {
+            const Cmd& c = cmds[idx];
+            if (deps.ptr[idx + 1] > deps.ptr[idx]) {
+                c128 pref;
+                AdjStep st = param_step(c, &pref);
+                Op o;
+                o.kind = OP_ADJ;
+                o.k = st.k;
+                o.qubits[0] = st.qubits[0];
+                o.qubits[1] = st.qubits[1];
+                o.m = std::move(st.D);
+                o.g = std::move(st.G);
+                o.slot = static_cast<int>(slots.size());
+                segment.push_back(std::move(o));
+                slots.push_back({idx, pref});
             } else {
-                st.D = local_unitary(d);
+                for (Op& o : lower(dagger(c), n)) segment.push_back(std::move(o));
             }
-            adjoint_param_step<T>(psi, phi, n, st, partials + 2 * slots.size() * nb, nb, h->stream);
-            h->stats.launches++;
-            h->stats.passes++;
-            h->stats.hbm_bytes += 4ull * h->dim() * h->amp_bytes();
-            slots.push_back({idx, pref});
-        } else {
-            for (const Op& o : lower(d, n)) {
-                launch(h, o, psi);
-                launch(h, o, phi);
+            if (at_checkpoint(idx)) {
+                flush();
+                restore(idx);
             }
         }
-        // psi is now the state before command idx: restart it from the checkpoint there
-        if (ck.K && idx > 0 && idx % ck.K == 0)
-            check_cuda(cudaMemcpyAsync(psi, ck.bufs.at(idx / ck.K - 1), h->dim() * h->amp_bytes(),
-                                       cudaMemcpyDeviceToDevice, h->stream), "checkpoint restore");
+        flush();
+    } else {
+        for (size_t idx = cmds.size(); idx-- > 0;) {
+            const Cmd& c = cmds[idx];
+            if (deps.ptr[idx + 1] > deps.ptr[idx]) {
+                c128 pref;
+                const AdjStep st = param_step(c, &pref);
+                adjoint_param_step<T>(psi, phi, n, st, partials + 2 * slots.size() * nb, nb, h->stream);
+                h->stats.launches++;
+                h->stats.passes++;
+                h->stats.hbm_bytes += 4ull * h->dim() * h->amp_bytes();
+                slots.push_back({idx, pref});
+            } else {
+                for (const Op& o : lower(dagger(c), n)) {
+                    launch(h, o, psi);
+                    launch(h, o, phi);
+                }
+            }
+            if (at_checkpoint(idx)) restore(idx);
+        }
     }
     std::vector<double> ips;
     reduce_slots(partials, static_cast<int>(slots.size()), nb, h->stream, h->ws, ips);

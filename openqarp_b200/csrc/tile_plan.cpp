@@ -26,6 +26,9 @@ uint64_t op_mixing_mask(const Op& op) {
         case OP_PERM:
             for (uint32_t q : op.pq) m |= bit(q);
             return m;
+        case OP_ADJ:
+            for (int b = 0; b < op.k; ++b) m |= bit(op.qubits[b]);
+            return m;
         default: return 0;
     }
 }
@@ -41,6 +44,9 @@ uint64_t op_support_mask(const Op& op) {
         case OP_PAULI_ROT: return op.mask | op.zmask;
         case OP_PERM:
             for (uint32_t q : op.pq) m |= bit(q);
+            return m;
+        case OP_ADJ:
+            for (int b = 0; b < op.k; ++b) m |= bit(op.qubits[b]);
             return m;
         default: return 0;
     }

@@ -527,6 +527,122 @@ def test_complex128_adjoint_with_checkpoints_matches(sim):
     assert np.max(np.abs(res[0][1] - res[1][1])) < 1e-10
 
 
+# ---------------------------------------------------------------- tiled reverse sweep
+# Registers of 14 qubits and more (complex128; 15 for complex64) run the adjoint's reverse
+# sweep as tile passes over both states; these cases pin that path against the oracle.
+
+def _generator_circuit(n, seed, reps=2, wide=False):
+    gens = [G.Rx, G.Ry, G.Rz, G.P, G.CRx, G.CRy, G.CRz, G.CP, G.RXX, G.RYY, G.RZZ, G.GPhase]
+    rng = np.random.default_rng(seed)
+    cmds, names = [Command(G.H, (q,)) for q in range(n)], []
+    for i, g in enumerate(gens * reps):
+        nm = f"p{i % 9}"
+        if nm not in names:
+            names.append(nm)
+        qs = tuple(int(q) for q in rng.permutation(n)[:2])
+        p = (Param.linear(float(rng.uniform(-2, 2)), nm, float(rng.uniform(-1, 1))),)
+        if g == G.GPhase:
+            cmds.append(Command(g, (), p))
+        elif g in (G.Rx, G.Ry, G.Rz, G.P):
+            cmds.append(Command(g, qs[:1], p))
+        else:
+            cmds.append(Command(g, qs, p))
+        cmds.append(Command(G.SX, (int(rng.integers(n)),)))
+        cmds.append(Command(G.CX, (int(qs[1]), int(qs[0]))))
+        if wide and i % 5 == 0:
+            # a 6-qubit Custom block: no tile holds it, so it runs as a stream pass on both states
+            z = rng.standard_normal((64, 64)) + 1j * rng.standard_normal((64, 64))
+            u, _ = np.linalg.qr(z)
+            cmds.append(ir.custom(tuple(int(q) for q in rng.permutation(n)[:6]), u))
+    vals = {nm: float(rng.uniform(-3, 3)) for nm in names}
+    return cmds, vals, names
+
+
+@pytest.mark.parametrize("n,wide", [(14, False), (16, True)])
+def test_tiled_adjoint_every_generator_against_oracle(restatement, n, wide):
+    from openqarp_b200 import Register
+    cmds, vals, names = _generator_circuit(n, 11 + n, wide=wide)
+    obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, 20, seed=n, max_weight=4, coeff_std=0.3)
+    stream = ir.pack(cmds, vals, names)
+    m = observable.to_masks(obs, n)
+    e_or, g_or = restatement.adjoint(stream, n, len(names), m)
+    reg = Register(n)
+    e, g = reg.adjoint(stream, len(names), m)
+    st = reg.stats()
+    reg.close()
+    np.testing.assert_allclose(g, g_or, atol=1e-10, rtol=0)
+    assert abs(e - e_or) < EV_TOL
+    # far fewer passes than one per reverse step
+    assert st["passes"] < len(cmds)
+
+
+def test_tiled_adjoint_hea_against_oracle(restatement):
+    from openqarp_b200 import Register
+    n = 16
+    cmds, vals, names = circuits.hea(n, 4, seed=21)
+    obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, 40, seed=22, max_weight=4, coeff_std=0.1)
+    stream = ir.pack(cmds, vals, names)
+    m = observable.to_masks(obs, n)
+    e_or, g_or = restatement.adjoint(stream, n, len(names), m)
+    reg = Register(n)
+    e, g = reg.adjoint(stream, len(names), m)
+    reg.close()
+    np.testing.assert_allclose(g, g_or, atol=1e-10, rtol=0)
+    assert abs(e - e_or) < EV_TOL
+
+
+def test_tiled_adjoint_many_steps_in_one_pass(restatement):
+    """200 parametric steps on the low qubits all fit one tile: the pass is split at the
+    kernel's accumulator limit and every slot still lands in its own row."""
+    from openqarp_b200 import Register
+    n = 14
+    rng = np.random.default_rng(5)
+    cmds, names = [Command(G.H, (q,)) for q in range(n)], []
+    for i in range(200):
+        nm = f"t{i}"
+        names.append(nm)
+        q = int(rng.integers(0, 4))
+        gate = (G.Rx, G.Ry, G.Rz, G.RZZ)[i % 4]
+        qs = (q, q + 1) if gate == G.RZZ else (q,)
+        cmds.append(Command(gate, qs, (Param.symbol(nm),)))
+    vals = {nm: float(rng.uniform(-3, 3)) for nm in names}
+    obs = circuits.random_pauli_sum(n, 15, seed=6, max_weight=3)
+    stream = ir.pack(cmds, vals, names)
+    m = observable.to_masks(obs, n)
+    e_or, g_or = restatement.adjoint(stream, n, len(names), m)
+    reg = Register(n)
+    e, g = reg.adjoint(stream, len(names), m)
+    reg.close()
+    np.testing.assert_allclose(g, g_or, atol=1e-10, rtol=0)
+
+
+def test_tiled_adjoint_complex64_with_checkpoints(restatement):
+    from openqarp_b200 import Register
+    n = 15
+    cmds, vals, names = circuits.hea(n, 6, seed=31)
+    obs = circuits.tfim_chain(n)
+    stream = ir.pack(cmds, vals, names)
+    m = observable.to_masks(obs, n)
+    _, g_or = restatement.adjoint(stream, n, len(names), m)
+    for k in (-1, 0, 40):
+        reg = Register(n, "complex64")
+        reg.set_checkpoint_interval(k)
+        reg.reset()
+        _, g = reg.adjoint(stream, len(names), m)
+        reg.close()
+        assert np.max(np.abs(np.asarray(g) - g_or)) < 1e-4, k
+
+
+def test_tiled_adjoint_phi_overlap(restatement, sim):
+    n = 14
+    cmds, vals, names = circuits.hea(n, 2, seed=7)
+    phi = random_state(n, 8)
+    stream = ir.pack(cmds, vals, names)
+    want = restatement.adjoint_phi(stream, n, len(names), phi)
+    got = sim.run_gradient_phi(cmds, n, phi, vals, names)
+    np.testing.assert_allclose(got, want, atol=1e-10, rtol=0)
+
+
 # ---------------------------------------------------------------- error paths
 
 def test_error_paths(sim):
