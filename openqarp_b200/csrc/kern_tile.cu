@@ -21,6 +21,7 @@ namespace {
 constexpr int kTileThreads = 512;
 constexpr int kTileCoefMax = 256;   // widest op: a 4-qubit dense block or an 8-qubit diagonal
 constexpr int kAdjSlotsMax = 64;    // ADJ steps per adjoint tile pass (shared-memory accumulators)
+constexpr size_t kAdjStageBytes = 40 * 1024;   // an adjoint pass's op table + coefficients in shared memory
 
 enum : uint8_t { T_DENSE = 1, T_DIAG, T_PHASE, T_CTRL1, T_SWAP, T_PAULI, T_SCALE, T_ADJ };
 
@@ -30,7 +31,7 @@ struct TileOpDev {
     uint32_t ncoef;         // coefficients of this op (staged in shared memory before use)
     uint32_t slot;          // ADJ: pass-local inner-product slot (the kernel's accumulators)
     uint32_t gslot;         // ADJ: slot of the sweep (row of the partials table)
-    uint32_t pad2;
+    uint32_t pad2[3];
     uint8_t lpos[8];        // local bit of op-local bit b (0xff: outside the tile)
     uint8_t gq[8];          // global qubit of op-local bit b (DIAG)
     uint64_t lmask;         // PHASE/CTRL1 local controls; PAULI local x mask
@@ -39,11 +40,15 @@ struct TileOpDev {
     uint64_t gz;            // PAULI z bits outside the tile (global)
 };
 
+// 16-byte multiple: a staged op table keeps the coefficients after it 16-byte aligned
+static_assert(sizeof(TileOpDev) % 16 == 0, "TileOpDev size");
+
 struct TilePassDev {
     uint32_t op_begin, op_end;
     int32_t m;
     uint8_t tq[16];         // global qubit of local bit j, ascending
     uint32_t n_adj;         // ADJ steps of the pass (adjoint sweep)
+    uint32_t coef_begin, coef_end;   // the pass's coefficients (adjoint sweep: staged once per CTA)
 };
 
 __device__ __forceinline__ uint32_t ins_zero32(uint32_t g, uint32_t p) {
@@ -363,7 +368,10 @@ __device__ __forceinline__ double2 tile_adj(vec2_t<T>* a, vec2_t<T>* f, int m, c
     return make_double2(ar, ai);
 }
 
-constexpr int kAdjWarps = kTileThreads / 32;
+constexpr int kAdjThreads = kTileThreads;   // 256 threads (no spills, 8 warps) measured no faster
+constexpr int kAdjLogThreads = 9;
+static_assert((1 << kAdjLogThreads) == kAdjThreads, "adjoint tile threads");
+constexpr int kAdjWarps = kAdjThreads / 32;
 
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
 #pragma unroll
@@ -379,7 +387,7 @@ __device__ __forceinline__ double2 warp_sum2(double2 v) {
 // warp adds only to its own entry, in tile order).  At the end the CTA writes one partial per
 // ADJ step: partials[slot * gridDim.x + blockIdx.x], summed over warps in fixed order.
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads, 1) k_adj_tile(vec2_t<T>* __restrict__ psi, vec2_t<T>* __restrict__ phi,
+__global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restrict__ psi, vec2_t<T>* __restrict__ phi,
                                                               int n, const TilePassDev* __restrict__ passes, int pass_idx,
                                                               const TileOpDev* __restrict__ ops,
                                                               const cplx<T>* __restrict__ coef,
@@ -389,13 +397,24 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_adj_tile(vec2_t<T>* __restr
     const int m = P.m;
     const uint32_t M = 1u << m;
     vec2_t<T>* bufs = reinterpret_cast<vec2_t<T>*>(smem_raw);   // [psi0, phi0, psi1, phi1]
-    cplx<T>* scoef = reinterpret_cast<cplx<T>*>(bufs + 4 * M);
-    double2* acc = reinterpret_cast<double2*>(scoef + kTileCoefMax);   // [local slot][warp]
+    double2* acc = reinterpret_cast<double2*>(bufs + 4 * M);      // [local slot][warp]
+    TileOpDev* sops = reinterpret_cast<TileOpDev*>(acc + kAdjSlotsMax * kAdjWarps);
+    const uint32_t n_ops = P.op_end - P.op_begin;
+    cplx<T>* scoef = reinterpret_cast<cplx<T>*>(sops + n_ops);
     const uint32_t n_adj = P.n_adj;
     for (uint32_t e = threadIdx.x; e < n_adj * kAdjWarps; e += blockDim.x) acc[e] = make_double2(0, 0);
+    // every tile runs the same ops: their descriptors and coefficients are staged once
+    {
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(ops + P.op_begin);
+        uint64_t* dst = reinterpret_cast<uint64_t*>(sops);
+        const uint32_t words = n_ops * static_cast<uint32_t>(sizeof(TileOpDev) / 8);
+        for (uint32_t e = threadIdx.x; e < words; e += blockDim.x) dst[e] = src[e];
+        for (uint32_t e = P.coef_begin + threadIdx.x; e < P.coef_end; e += blockDim.x)
+            scoef[e - P.coef_begin] = coef[e];
+    }
     constexpr int kAmpsPerChunk = 16 / sizeof(vec2_t<T>);
     constexpr int acl = kAmpsPerChunk == 2 ? 1 : 0;
-    constexpr int hi_shift = 9 + acl;
+    constexpr int hi_shift = kAdjLogThreads + acl;
     const uint32_t R = M >> hi_shift;
     const uint32_t lt = threadIdx.x << acl;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -436,16 +455,15 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_adj_tile(vec2_t<T>* __restr
         cp_async_wait1();
         __syncthreads();
         const uint64_t base = tile_base(t);
-        for (uint32_t o = P.op_begin; o < P.op_end; ++o) {
-            const TileOpDev& op = ops[o];
-            for (uint32_t e = threadIdx.x; e < op.ncoef; e += blockDim.x) scoef[e] = coef[op.coef + e];
-            __syncthreads();
+        for (uint32_t o = 0; o < n_ops; ++o) {
+            const TileOpDev& op = sops[o];
+            const cplx<T>* oc = scoef + (op.coef - P.coef_begin);
             if (op.kind == T_ADJ) {
                 double2 v;
                 switch (op.k) {
-                    case 0: v = tile_adj<T, 0>(cur, cur + M, m, op, scoef); break;
-                    case 1: v = tile_adj<T, 1>(cur, cur + M, m, op, scoef); break;
-                    default: v = tile_adj<T, 2>(cur, cur + M, m, op, scoef); break;
+                    case 0: v = tile_adj<T, 0>(cur, cur + M, m, op, oc); break;
+                    case 1: v = tile_adj<T, 1>(cur, cur + M, m, op, oc); break;
+                    default: v = tile_adj<T, 2>(cur, cur + M, m, op, oc); break;
                 }
                 v = warp_sum2(v);
                 if (lane == 0) {
@@ -454,8 +472,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_adj_tile(vec2_t<T>* __restr
                     e.y += v.y;
                 }
             } else {
-                tile_op<T>(cur, m, base, op, scoef);
-                tile_op<T>(cur + M, m, base, op, scoef);
+                tile_op<T>(cur, m, base, op, oc);
+                tile_op<T>(cur + M, m, base, op, oc);
             }
             __syncthreads();
         }
@@ -469,8 +487,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_adj_tile(vec2_t<T>* __restr
     }
     cp_async_wait0();
     __syncthreads();
-    for (uint32_t o = P.op_begin + threadIdx.x; o < P.op_end; o += blockDim.x) {
-        const TileOpDev& op = ops[o];
+    for (uint32_t o = threadIdx.x; o < n_ops; o += blockDim.x) {
+        const TileOpDev& op = sops[o];
         if (op.kind != T_ADJ) continue;
         double2 v = make_double2(0, 0);
         for (int w = 0; w < kAdjWarps; ++w) {
@@ -645,21 +663,36 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
     if (ops.empty()) return;
     if (m < kTileMinQubits || m > n) throw std::logic_error("adjoint tile width outside the kernel's range");
     const std::vector<TilePass> planned = plan_tiles(ops, n, m);
-    // split tile passes whose ADJ steps overflow the kernel's accumulators
+    // split tile passes whose ADJ steps overflow the kernel's accumulators or whose op table
+    // and coefficients overflow its staging area
+    auto coef_count = [](const Op& o) -> size_t {
+        switch (o.kind) {
+            case OP_ADJ: return size_t{2} << (2 * o.k);
+            case OP_DENSE: return size_t{1} << (2 * o.k);
+            case OP_DIAG: return size_t{1} << o.k;
+            case OP_CTRL1: return 4;
+            case OP_SWAP: return 0;
+            default: return 1;
+        }
+    };
     std::vector<TilePass> passes;
     for (const TilePass& p : planned) {
         if (p.tile_qubits.empty()) { passes.push_back(p); continue; }
         TilePass cur;
         cur.tile_qubits = p.tile_qubits;
         int adj = 0;
+        size_t staged = 0;
         for (const Op& o : p.ops) {
-            if (o.kind == OP_ADJ && adj == kAdjSlotsMax) {
+            const size_t bytes = sizeof(TileOpDev) + coef_count(o) * sizeof(cplx<T>);
+            if (!cur.ops.empty() && ((o.kind == OP_ADJ && adj == kAdjSlotsMax) || staged + bytes > kAdjStageBytes)) {
                 passes.push_back(std::move(cur));
                 cur = TilePass{};
                 cur.tile_qubits = p.tile_qubits;
                 adj = 0;
+                staged = 0;
             }
             if (o.kind == OP_ADJ) ++adj;
+            staged += bytes;
             cur.ops.push_back(o);
         }
         passes.push_back(std::move(cur));
@@ -687,6 +720,7 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
             return lm;
         };
         pd.op_begin = static_cast<uint32_t>(odev.size());
+        pd.coef_begin = static_cast<uint32_t>(cdev.size());
         for (const Op& o : p.ops) {
             const uint64_t mix = op_mixing_mask(o);
             for (int q = 0; q < 64; ++q)
@@ -764,10 +798,14 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
                     throw std::logic_error("adjoint tile pass holds an op the tile kernel cannot apply");
             }
             d.ncoef = static_cast<uint32_t>(cdev.size()) - d.coef;
-            if (d.ncoef > static_cast<uint32_t>(kTileCoefMax)) throw std::logic_error("tile op coefficients overflow");
+            if (d.ncoef != coef_count(o)) throw std::logic_error("tile op coefficient count");
             odev.push_back(d);
         }
         pd.op_end = static_cast<uint32_t>(odev.size());
+        pd.coef_end = static_cast<uint32_t>(cdev.size());
+        if ((pd.op_end - pd.op_begin) * sizeof(TileOpDev) + (pd.coef_end - pd.coef_begin) * sizeof(cplx<T>) >
+            kAdjStageBytes)
+            throw std::logic_error("adjoint tile pass overflows its staging area");
         pdev.push_back(pd);
     }
     const size_t a_p = 0;
@@ -785,8 +823,8 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
     const TileOpDev* d_o = reinterpret_cast<const TileOpDev*>(dev + a_o);
     const cplx<T>* d_c = reinterpret_cast<const cplx<T>*>(dev + a_c);
     if (nb != adjoint_tile_grid(n, m)) throw std::logic_error("adjoint partials sized for another grid");
-    const size_t smem = 4 * (size_t{1} << m) * sizeof(vec2_t<T>) + kTileCoefMax * sizeof(cplx<T>) +
-                        static_cast<size_t>(kAdjSlotsMax) * kAdjWarps * sizeof(double2);
+    const size_t smem = 4 * (size_t{1} << m) * sizeof(vec2_t<T>) +
+                        static_cast<size_t>(kAdjSlotsMax) * kAdjWarps * sizeof(double2) + kAdjStageBytes;
     check_cuda(cudaFuncSetAttribute(k_adj_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)), "adjoint tile smem");
     int pi = 0;
@@ -798,7 +836,7 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
             }
             continue;
         }
-        k_adj_tile<T><<<nb, kTileThreads, smem, st>>>(psi, phi, n, d_p, pi, d_o, d_c,
+        k_adj_tile<T><<<nb, kAdjThreads, smem, st>>>(psi, phi, n, d_p, pi, d_o, d_c,
                                                       reinterpret_cast<double2*>(d_partials));
         check_cuda(cudaGetLastError(), "adjoint tile pass launch");
         if (launches) ++*launches;
