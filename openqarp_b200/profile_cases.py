@@ -61,6 +61,8 @@ def main(argv=None):
     elif a.case == "adjoint":
         cmds, vals, names = circuits.hea(a.n, a.layers, seed=3)
         obs = circuits.tfim_chain(a.n)
+        if a.terms > 2 * a.n - 1:   # the adjoint configuration's observable: TFIM + random weight <= 4 terms
+            obs = obs + circuits.random_pauli_sum(a.n, a.terms - (2 * a.n - 1), seed=2, max_weight=4, coeff_std=0.1)
         reg.adjoint(ir.pack(cmds, vals, names), len(names), observable.to_masks(obs, a.n))
     elif a.case == "sample":
         reg.apply(ir.pack(circuits.brickwork(a.n, 1, seed=1)).buf)
