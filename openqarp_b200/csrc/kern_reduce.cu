@@ -386,15 +386,36 @@ __global__ void __launch_bounds__(kChunkThreads) k_chunk_totals(const vec2_t<T>*
     if (threadIdx.x == 0) chunk_total[blockIdx.x] = tot;
 }
 
-// exclusive prefix of the chunk totals, sequential (one thread): off[c] = sum_{c' < c}
-__global__ void k_chunk_offsets(const double* __restrict__ chunk_total, unsigned n_chunks, double* __restrict__ off) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// exclusive prefix of the chunk totals, off[c] = sum_{c' < c}, in a fixed order: thread t sums
+// its contiguous run of chunks left to right, one thread scans the run totals left to right, and
+// each thread then writes its run's offsets.  (A single sequential thread took 0.67 ms for the
+// 16384 chunks of a 26-qubit register.)
+constexpr int kOffThreads = 1024;
+__global__ void __launch_bounds__(kOffThreads) k_chunk_offsets(const double* __restrict__ chunk_total, unsigned n_chunks,
+                                                               double* __restrict__ off) {
+    __shared__ double run_base[kOffThreads + 1];
+    const unsigned per = (n_chunks + kOffThreads - 1) / kOffThreads;
+    const unsigned c0 = min(n_chunks, threadIdx.x * per), c1 = min(n_chunks, c0 + per);
     double acc = 0;
-    for (unsigned c = 0; c < n_chunks; ++c) {
-        off[c] = acc;
-        acc = __dadd_rn(acc, chunk_total[c]);
+    for (unsigned c = c0; c < c1; ++c) acc = __dadd_rn(acc, chunk_total[c]);
+    run_base[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0;
+        for (int t = 0; t < kOffThreads; ++t) {
+            const double x = run_base[t];
+            run_base[t] = a;
+            a = __dadd_rn(a, x);
+        }
+        run_base[kOffThreads] = a;
     }
-    off[n_chunks] = acc;
+    __syncthreads();
+    double a = run_base[threadIdx.x];
+    for (unsigned c = c0; c < c1; ++c) {
+        off[c] = a;
+        a = __dadd_rn(a, chunk_total[c]);
+    }
+    if (threadIdx.x == 0) off[n_chunks] = run_base[kOffThreads];
 }
 
 __device__ __forceinline__ size_t first_greater(const double* u, size_t n, double x) {
@@ -621,7 +642,7 @@ void sample_sorted(const vec2_t<T>* s, int n, const double* d_u, size_t n_shots,
     k_prob_total<T><<<nb, kRed, 0, st>>>(s, dim, partials);
     k_final<<<1, kRed, 0, st>>>(partials, nb, partials + nb);
     k_chunk_totals<T><<<n_chunks, kChunkThreads, 0, st>>>(s, dim, partials + nb, chunk_total);
-    k_chunk_offsets<<<1, 32, 0, st>>>(chunk_total, n_chunks, off);
+    k_chunk_offsets<<<1, kOffThreads, 0, st>>>(chunk_total, n_chunks, off);
     k_sample_chunks<T><<<n_chunks, kChunkThreads, 0, st>>>(s, dim, partials + nb, off, n_chunks, d_u,
                                                           n_shots, d_out);
     check_cuda(cudaGetLastError(), "sampling launch");
