@@ -45,7 +45,7 @@ sys.path.insert(0, ROOT)
 N_QUBITS = 28
 DEPTH = 20
 SEED = 1234
-CPU_LAYERS = 8      # host-core sample of the b200 arm's cpu_baseline
+CPU_LAYERS = 4      # host-core sample (the circuit's first layers) of cpu_baseline and of each reference-arm step
 ADJ_N, ADJ_LAYERS, ADJ_TERMS = 24, 8, 500
 
 
@@ -411,7 +411,7 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     from openqarp_b200 import circuits, ir
-    layer = ir.pack(circuits.brickwork(N_QUBITS, 1, seed=SEED)).buf
+    layer = ir.pack(circuits.brickwork(N_QUBITS, CPU_LAYERS, seed=SEED)).buf
     for _ in range(args.warmup):
         cpu_baseline_sample(layer, N_QUBITS)
     times, rates = [], []
@@ -429,10 +429,11 @@ def reference_arm(args, rank, world):
         "config": {"workload": f"brickwork n={N_QUBITS} depth={DEPTH} Haar SU(2)+CZ, seed {SEED}",
                    "fusion_k": 3,
                    "work_definition": f"fused-gate passes of the reference plan (k=3) x 2 x 2^{N_QUBITS} x 16 B",
-                   "sample": "each step times one of the circuit's layers (its fused passes) on the host cores",
+                   "sample": f"each step times the circuit's first {CPU_LAYERS} layers (their fused passes) on the host cores",
                    "l2": "register 4 GiB > L2", "parallelism": "host threads"},
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": kind,
-                         "sample": f"1 brickwork layer at {N_QUBITS} qubits per step ({passes} fused passes)"},
+                         "sample": f"the circuit's first {CPU_LAYERS} layers at {N_QUBITS} qubits per step "
+                                   f"({passes} fused passes)"},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -528,7 +529,7 @@ def b200_arm(args, rank, world, local_rank):
         # the single-GPU rows run only at N = 1: at N > 1 every GPU would wait for rank 0
         single = world == 1
         if world == 1 and not args.skip_cpu:
-            # the circuit's first CPU_LAYERS layers: about 10 s of host work
+            # the circuit's first CPU_LAYERS layers: a few seconds of host work
             prefix = ir.pack(circuits.brickwork(N_QUBITS, CPU_LAYERS, seed=SEED)).buf
             gbs, dt, cpasses, cores, kind = cpu_baseline_sample(prefix, N_QUBITS)
             cpu = {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind,
