@@ -332,6 +332,25 @@ def test_sampling_chi2_and_large_register(restatement):
     reg.close()
 
 
+@pytest.mark.parametrize("n", [13, 21, 22, 23])
+def test_sampling_chunk_offsets_across_chunk_counts(restatement, n):
+    """2 to 2048 chunks of 4096 amplitudes: the chunk-offset scan runs over 1024 threads with
+    runs of zero, one or two chunks; indices equal the oracle's except at a cumulative
+    boundary within the reassociation error of the sums."""
+    psi = random_state(n, 40 + n)
+    reg = Register(n)
+    reg.set_state(psi)
+    u = np.sort(np.random.default_rng(n).random(20000))
+    got = reg.sample(u)
+    reg.close()
+    want, cp = restatement.sample(psi, n, u, with_cdf=True)
+    bad = np.nonzero(got != want)[0]
+    for s in bad:
+        j = int(want[s])
+        assert min(abs(u[s] - cp[j]), abs(u[s] - (cp[j - 1] if j else 0.0))) < 1e-11
+    assert len(bad) <= 2
+
+
 def test_terminal_measurements_fill_cbit_history(sim):
     cmds = [Command(G.H, (0,)), Command(G.CX, (0, 1)),
             Command(G.Measure, (0,), cbits=(1,)), Command(G.Measure, (1,), cbits=(0,))]
