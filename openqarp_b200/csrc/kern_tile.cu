@@ -382,8 +382,8 @@ __device__ __forceinline__ double2 warp_sum2(double2 v) {
     return v;
 }
 
-// The reverse sweep's tile pass: k_tile_pass over the tile pair (psi, phi), every op applied
-// to both, and ADJ steps accumulating their inner products per warp in shared memory (each
+// The reverse sweep's tile pass: a k_tile_pass-like loop over the tile pair (psi, phi), every op
+// applied to both, and ADJ steps accumulating their inner products per warp in shared memory (each
 // warp adds only to its own entry, in tile order).  At the end the CTA writes one partial per
 // ADJ step: partials[slot * gridDim.x + blockIdx.x], summed over warps in fixed order.
 template <typename T>
@@ -396,8 +396,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
     const TilePassDev P = passes[pass_idx];
     const int m = P.m;
     const uint32_t M = 1u << m;
-    vec2_t<T>* bufs = reinterpret_cast<vec2_t<T>*>(smem_raw);   // [psi0, phi0, psi1, phi1]
-    double2* acc = reinterpret_cast<double2*>(bufs + 4 * M);      // [local slot][warp]
+    vec2_t<T>* bufs = reinterpret_cast<vec2_t<T>*>(smem_raw);   // [psi, phi]
+    double2* acc = reinterpret_cast<double2*>(bufs + 2 * M);      // [local slot][warp]
     TileOpDev* sops = reinterpret_cast<TileOpDev*>(acc + kAdjSlotsMax * kAdjWarps);
     const uint32_t n_ops = P.op_end - P.op_begin;
     cplx<T>* scoef = reinterpret_cast<cplx<T>*>(sops + n_ops);
@@ -445,14 +445,14 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
     const uint64_t n_tiles = 1ull << (n - m);
     const uint64_t G = gridDim.x;
     uint64_t t = blockIdx.x;
+    // one tile pair in flight: its load is not overlapped with this CTA's arithmetic, but the
+    // wider tile (twice the groups per thread between barriers, one more tile qubit) more than
+    // pays for it
+    vec2_t<T>* cur = bufs;
     if (t < n_tiles) issue(bufs, tile_base(t));
     cp_async_commit();
-    for (uint32_t i = 0; t < n_tiles; t += G, ++i) {
-        vec2_t<T>* cur = (i & 1u) ? bufs + 2 * M : bufs;
-        vec2_t<T>* nxt = (i & 1u) ? bufs : bufs + 2 * M;
-        if (t + G < n_tiles) issue(nxt, tile_base(t + G));
-        cp_async_commit();
-        cp_async_wait1();
+    for (; t < n_tiles; t += G) {
+        cp_async_wait0();
         __syncthreads();
         const uint64_t base = tile_base(t);
         for (uint32_t o = 0; o < n_ops; ++o) {
@@ -483,7 +483,9 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
             __stcs(reinterpret_cast<float4*>(psi + gi), *reinterpret_cast<const float4*>(cur + l));
             __stcs(reinterpret_cast<float4*>(phi + gi), *reinterpret_cast<const float4*>(cur + M + l));
         }
-        __syncthreads();
+        __syncthreads();   // every thread has read the tile out before the next copies land
+        if (t + G < n_tiles) issue(bufs, tile_base(t + G));
+        cp_async_commit();
     }
     cp_async_wait0();
     __syncthreads();
@@ -823,7 +825,7 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
     const TileOpDev* d_o = reinterpret_cast<const TileOpDev*>(dev + a_o);
     const cplx<T>* d_c = reinterpret_cast<const cplx<T>*>(dev + a_c);
     if (nb != adjoint_tile_grid(n, m)) throw std::logic_error("adjoint partials sized for another grid");
-    const size_t smem = 4 * (size_t{1} << m) * sizeof(vec2_t<T>) +
+    const size_t smem = 2 * (size_t{1} << m) * sizeof(vec2_t<T>) +
                         static_cast<size_t>(kAdjSlotsMax) * kAdjWarps * sizeof(double2) + kAdjStageBytes;
     check_cuda(cudaFuncSetAttribute(k_adj_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)), "adjoint tile smem");

@@ -810,11 +810,11 @@ void adjoint_forward(Handle* h, const std::vector<Cmd>& cs, Checkpoints& ck) {
     }
 }
 
-// Tile width of the reverse sweep's passes: the tile pair (psi and phi), double-buffered, takes
-// 4 x 2^m amplitudes of shared memory — 128 KiB at m = 11 (complex128) or 12 (complex64).
+// Tile width of the reverse sweep's passes: the tile pair (psi and phi) takes 2 x 2^m amplitudes
+// of shared memory — 128 KiB at m = 12 (complex128) or 13 (complex64).
 template <typename T>
 constexpr int adjoint_tile_qubits() {
-    return sizeof(T) == sizeof(double) ? 11 : 12;
+    return sizeof(T) == sizeof(double) ? 12 : 13;
 }
 
 template <typename T>
@@ -854,7 +854,7 @@ void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps
                                    cudaMemcpyDeviceToDevice, h->stream), "checkpoint restore");
     };
     const int mt = adjoint_tile_qubits<T>();
-    const bool tiled = n >= mt + 3;
+    const bool tiled = n >= mt + 2;
     // tiled: the reverse stream runs as tile passes over both states, several reverse steps a
     // pass; narrower registers take one launch per reverse step
     const unsigned nb = tiled ? adjoint_tile_grid(n, mt) : adjoint_blocks(n);
