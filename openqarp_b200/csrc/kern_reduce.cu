@@ -28,6 +28,7 @@ void* Workspace::grow(void*& p, size_t& cap, size_t bytes) {
     const size_t want = std::max<size_t>(bytes, 4096);
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
+        (void)cudaGetLastError();   // a failed allocation leaves no error for the next launch check
         p = nullptr;
         throw std::bad_alloc();
     }
@@ -63,10 +64,14 @@ void Workspace::release() {
     if (shot_) cudaFree(shot_);
     if (tile_) cudaFree(tile_);
     if (rtile_) cudaFree(rtile_);
+    if (tb_) cudaFree(tb_);
+    if (tk_) cudaFree(tk_);
+    if (ts_) cudaFree(ts_);
     if (host_) cudaFreeHost(host_);
-    mat_ = copy_ = scr_ = shot_ = tile_ = rtile_ = nullptr;
+    mat_ = copy_ = scr_ = shot_ = tile_ = rtile_ = tb_ = tk_ = ts_ = nullptr;
     host_ = nullptr;
     mat_cap_ = copy_cap_ = scr_cap_ = shot_cap_ = tile_cap_ = rtile_cap_ = host_cap_ = 0;
+    tb_cap_ = tk_cap_ = ts_cap_ = 0;
 }
 
 namespace {

@@ -754,7 +754,7 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
     const size_t per_shot_bytes = 8 * 18 + 4 * (kMtN + 3) + 2 + 8 * n_chunks + (plan.kraus ? 32 * n_pchunks : 0);
     size_t free_b = 0, total_b = 0;
     check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-    const size_t budget = free_b / 2;
+    const size_t budget = (free_b + ws.traj_held()) / 2;   // buffers kept from an earlier run count as free
     const size_t shot_cost = state_bytes * (plan.needs_backup ? 2 : 1) + per_shot_bytes;
     if (shot_cost > budget) throw std::bad_alloc();
     const uint64_t cap = opt.max_batch_shots ? std::min<uint64_t>(opt.max_batch_shots, 1ull << 20) : 1ull << 20;
@@ -762,10 +762,12 @@ void run_trajectories(const std::vector<Cmd>& suffix, int n, int n_cbits, const 
     while (B < n_shots && 2 * B <= cap && (2 * B) * shot_cost <= budget) B *= 2;
 
     // device: the batch register, the backup (wide guarded commands), per-shot arrays
-    DeviceBuffer batch(B * state_bytes);
-    DeviceBuffer backup(plan.needs_backup ? B * state_bytes : 0);
+    // the earlier run's work on these buffers is ordered before this run's on the same stream
+    struct Held { void* p; };
+    const Held batch{ws.traj_batch(B * state_bytes)};
+    const Held backup{plan.needs_backup ? ws.traj_backup(B * state_bytes) : nullptr};
     const size_t tables = plan.mats.size() * sizeof(cplx<double>) + plan.noise_prm.size() * sizeof(double);
-    DeviceBuffer side(B * per_shot_bytes + 32 * 16 + tables);
+    const Held side{ws.traj_side(B * per_shot_bytes + 32 * 16 + tables)};
     uint8_t* sp = static_cast<uint8_t*>(side.p);
     auto carve = [&](size_t bytes) {
         uint8_t* r = sp;

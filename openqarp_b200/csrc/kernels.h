@@ -35,6 +35,12 @@ public:
     void* shots(size_t bytes) { return grow(shot_, shot_cap_, bytes); }
     void* tiles(size_t bytes) { return grow(tile_, tile_cap_, bytes); }
     void* rt_tiles(size_t bytes) { return grow(rtile_, rtile_cap_, bytes); }
+    // batched trajectories: the batch register, its backup and the per-shot arrays, kept between
+    // runs so a repeated run allocates nothing
+    void* traj_batch(size_t bytes) { return grow(tb_, tb_cap_, bytes); }
+    void* traj_backup(size_t bytes) { return grow(tk_, tk_cap_, bytes); }
+    void* traj_side(size_t bytes) { return grow(ts_, ts_cap_, bytes); }
+    size_t traj_held() const { return tb_cap_ + tk_cap_ + ts_cap_; }
     // pinned host staging for small results
     double* host_result(size_t n_doubles);
     // device int the tensor-core kernels set when a bounded wait gives up; zero at allocation
@@ -49,6 +55,9 @@ private:
     void* shot_ = nullptr; size_t shot_cap_ = 0;
     void* tile_ = nullptr; size_t tile_cap_ = 0;
     void* rtile_ = nullptr; size_t rtile_cap_ = 0;
+    void* tb_ = nullptr; size_t tb_cap_ = 0;
+    void* tk_ = nullptr; size_t tk_cap_ = 0;
+    void* ts_ = nullptr; size_t ts_cap_ = 0;
     double* host_ = nullptr; size_t host_cap_ = 0;
     int* flag_ = nullptr;
 };
