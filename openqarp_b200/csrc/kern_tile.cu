@@ -324,8 +324,19 @@ __device__ __forceinline__ double2 tile_adj(vec2_t<T>* a, vec2_t<T>* f, int m, c
     for (int b = 0; b < K; ++b) sp[b] = op.lpos[b];
     if constexpr (K == 2)
         if (sp[1] < sp[0]) { const uint8_t t = sp[0]; sp[0] = sp[1]; sp[1] = t; }
-    const cplx<T>* Dm = coef;
-    const cplx<T>* Gm = coef + D * D;
+    // the matrices in registers for one- and zero-qubit steps: the tile stores inside the loop
+    // would otherwise make the compiler re-read them from shared memory for every group
+    constexpr int DH = K <= 1 ? D * D : 1;
+    cplx<T> Dh[DH], Gh[DH];
+    if constexpr (K <= 1) {
+#pragma unroll
+        for (int e = 0; e < D * D; ++e) {
+            Dh[e] = coef[e];
+            Gh[e] = coef[D * D + e];
+        }
+    }
+    const cplx<T>* Dm = K <= 1 ? Dh : coef;
+    const cplx<T>* Gm = K <= 1 ? Gh : coef + D * D;
     double ar = 0, ai = 0;
     const uint32_t groups = 1u << (m - K);
     for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
