@@ -625,6 +625,10 @@ def main():
     ap.add_argument("--k", type=int, default=None, help="pin the fusion width; needs --executor")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    # the reference CPU simulator sizes its thread pool from QARP_NUM_THREADS, then
+    # OMP_NUM_THREADS, on first use; torchrun sets OMP_NUM_THREADS=1 per rank, so give the host
+    # timings every core explicitly
+    os.environ.setdefault("QARP_NUM_THREADS", str(os.cpu_count() or 1))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
