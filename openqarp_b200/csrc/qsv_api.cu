@@ -36,6 +36,8 @@ struct Handle {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     void* aux = nullptr;          // second register (adjoint's |phi>)
     size_t aux_cap = 0;
+    std::vector<void*> ckpt;      // adjoint: |psi> checkpoint buffers kept between calls
+    size_t ckpt_bytes = 0;        // size of each
     int checkpoint_interval = -1; // adjoint: commands between psi checkpoints (-1 auto, 0 none)
     uint64_t traj_batch = 0;      // trajectories: shots per device batch (0: memory-bound default)
     std::vector<NoiseSpec> noise; // trajectories: channel per gate type (empty: noiseless)
@@ -322,6 +324,7 @@ int qsv_destroy(void* hp) {
         h->ws.release();
         if (h->state) cudaFree(h->state);
         if (h->aux) cudaFree(h->aux);
+        for (void* b : h->ckpt) cudaFree(b);
         if (h->e0) cudaEventDestroy(h->e0);
         if (h->e1) cudaEventDestroy(h->e1);
         if (h->stream) cudaStreamDestroy(h->stream);
@@ -761,16 +764,12 @@ struct DepTable {
 // |psi> checkpoints of the adjoint sweep: bufs[s - 1] holds the state before command s * K.
 // The reverse sweep uncomputes psi through the inverse gates of one segment at most and then
 // restarts from the stored state, so the rounding drift of uncomputation (which complex64
-// accumulates over a long circuit) stays bounded by K gates.
+// accumulates over a long circuit) stays bounded by K gates.  The buffers belong to the handle
+// and are reused by its next adjoint call (allocating them per call made repeated gradients
+// vary by up to 5x).
 struct Checkpoints {
     size_t K = 0;                 // 0: no checkpoints
-    std::vector<void*> bufs;
-    Checkpoints() = default;
-    Checkpoints(const Checkpoints&) = delete;
-    Checkpoints& operator=(const Checkpoints&) = delete;
-    ~Checkpoints() {
-        for (void* b : bufs) cudaFree(b);
-    }
+    std::vector<void*> bufs;      // borrowed from the handle
 };
 
 size_t checkpoint_interval(const Handle* h, size_t n_cmds) {
@@ -787,21 +786,31 @@ void adjoint_forward(Handle* h, const std::vector<Cmd>& cs, Checkpoints& ck) {
     const size_t K = checkpoint_interval(h, cs.size());
     const size_t bytes = h->dim() * h->amp_bytes();
     const size_t S = K ? (cs.size() + K - 1) / K : 1;
+    if (h->ckpt_bytes != bytes) {   // kept buffers of another register size cannot be reused
+        for (void* b : h->ckpt) cudaFree(b);
+        h->ckpt.clear();
+        h->ckpt_bytes = bytes;
+    }
     size_t free_b = 0, total_b = 0;
     if (S > 1) check_cuda(cudaMemGetInfo(&free_b, &total_b), "memory info");
-    if (S <= 1 || (S - 1) * bytes > free_b / 2) {
+    const size_t held = h->ckpt.size() * bytes;
+    if (S <= 1 || (S - 1) * bytes > (free_b + held) / 2) {
         ck.K = 0;
         apply_cmds(h, cs, true);
         return;
     }
     ck.K = K;
+    while (h->ckpt.size() < S - 1) {
+        void* b = nullptr;
+        if (cudaMalloc(&b, bytes) != cudaSuccess) {
+            (void)cudaGetLastError();
+            throw std::bad_alloc();
+        }
+        h->ckpt.push_back(b);
+    }
     for (size_t s = 0; s < S; ++s) {
         if (s > 0) {
-            void* b = nullptr;
-            if (cudaMalloc(&b, bytes) != cudaSuccess) {
-                (void)cudaGetLastError();
-                throw std::bad_alloc();
-            }
+            void* b = h->ckpt[s - 1];
             ck.bufs.push_back(b);
             check_cuda(cudaMemcpyAsync(b, h->state, bytes, cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
         }
