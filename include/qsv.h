@@ -184,6 +184,13 @@ QSV_API int qsv_copy_state(void* dst, const void* src);
  * (reference: qarp_simulator.cpp:120-129, fusion.cpp:120-268) for plan inspection. */
 QSV_API int qsv_fuse_count(const uint8_t* cmds, size_t nbytes, int n_qubits, int max_qubits,
                            int min_qubits, int32_t* n_out, int32_t* widths_hist);
+/* Host-only (no device work): the fused stream itself, as packed records in the format
+ * above (fused blocks as QSV_GATE_CUSTOM records).  *nbytes_out receives the size; the
+ * records are written only when out != NULL and cap >= that size.  Replaces the command list
+ * fuse_for_dispatch returns (reference: qarp_simulator.cpp:120-129, fusion.cpp:120-268,
+ * transpiler/fusion.cpp:196-300), for plan inspection and plan parity. */
+QSV_API int qsv_fuse_plan(const uint8_t* cmds, size_t nbytes, int n_qubits, int max_qubits,
+                          int min_qubits, uint8_t* out, size_t cap, size_t* nbytes_out);
 /* Host-only (no device work): the tiled executor's plan for a stream — how many
  * shared-memory tile passes and how many single-op HBM passes (ops a tile cannot hold) it
  * launches for the given fusion knobs and tile width (0 = the default for complex128).  An

@@ -9,7 +9,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <deque>
 
 #include "../../include/qsv.h"
 
@@ -547,224 +546,10 @@ bool generator(const Cmd& c, c128* pref, std::vector<c128>* G, int* k) {
     }
 }
 
-// ---------------------------------------------------------------- fusion
+// ---------------------------------------------------------------- one-qubit matrices
 
-namespace {
-
-struct Block {
-    size_t id = 0;
-    std::vector<uint32_t> qubits;   // local bit b <-> qubits[b]
-    std::vector<uint32_t> wires;    // qubit wires + cbit wires
-    std::vector<c128> u;            // empty until a second gate folds in
-    int n_gates = 0;
-    int src_gates = 0;
-    Cmd first;
-};
-
-bool is_marker(int g) {
-    return g == BARRIER || g == MEASURE || g == RESET || g == BRANCH_BEGIN ||
-           g == BRANCH_ELSE || g == BRANCH_END;
-}
-
-bool contains(const std::vector<uint32_t>& v, uint32_t x) {
-    return std::find(v.begin(), v.end(), x) != v.end();
-}
-
-bool fusible(const Cmd& c, int k) {
-    if (c.gate == PERMUTATION || c.gate == CONTROLLED_UNITARY) return false;
-    if (c.q.empty() || static_cast<int>(c.q.size()) > k) return false;
-    if (is_marker(c.gate) || c.gate == GPHASE) return false;
-    if (c.flags & 1) return false;
-    return true;
-}
-
-// widening past two qubits needs a shared qubit (fusion.cpp:57-65)
-bool can_join(const std::vector<uint32_t>& block, const std::vector<uint32_t>& gate, int k) {
-    int shared = 0, fresh = 0;
-    for (uint32_t q : gate) (contains(block, q) ? shared : fresh)++;
-    if (fresh == 0) return true;
-    const int width = static_cast<int>(block.size()) + fresh;
-    if (width > k) return false;
-    return shared > 0 || width <= 2;
-}
-
-// U <- I (x) U: new qubits become the high local bits
-void extend(Block& b, const std::vector<uint32_t>& fresh) {
-    const size_t old = size_t{1} << b.qubits.size();
-    const size_t copies = size_t{1} << fresh.size();
-    const size_t nd = old * copies;
-    std::vector<c128> out(nd * nd, I0);
-    for (size_t h = 0; h < copies; ++h)
-        for (size_t i = 0; i < old; ++i)
-            for (size_t j = 0; j < old; ++j) out[(h * old + i) * nd + h * old + j] = b.u[i * old + j];
-    b.u.swap(out);
-    b.qubits.insert(b.qubits.end(), fresh.begin(), fresh.end());
-}
-
-// U <- E(g) U with gate-local bit b <-> block bit pos[b]
-void left_apply(std::vector<c128>& u, size_t dim, const std::vector<c128>& g,
-                const std::vector<int>& pos) {
-    const size_t m = pos.size(), gd = size_t{1} << m;
-    std::vector<c128> out(dim * dim, I0);
-    for (size_t i = 0; i < dim; ++i) {
-        size_t li = 0, rest = i;
-        for (size_t b = 0; b < m; ++b) {
-            li |= ((i >> pos[b]) & 1u) << b;
-            rest &= ~(size_t{1} << pos[b]);
-        }
-        for (size_t lo = 0; lo < gd; ++lo) {
-            const c128 coeff = g[lo * gd + li];
-            if (coeff == I0) continue;
-            size_t io = rest;
-            for (size_t b = 0; b < m; ++b) if ((lo >> b) & 1u) io |= size_t{1} << pos[b];
-            const c128* src = &u[i * dim];
-            c128* dst = &out[io * dim];
-            for (size_t x = 0; x < dim; ++x) dst[x] += coeff * src[x];
-        }
-    }
-    u.swap(out);
-}
-
-double frob_dist_identity(const std::vector<c128>& u, size_t d) {
-    double s = 0;
-    for (size_t y = 0; y < d; ++y)
-        for (size_t x = 0; x < d; ++x) {
-            const c128 e = u[y * d + x] - (x == y ? I1 : I0);
-            s += std::norm(e);
-        }
-    return std::sqrt(s);
-}
-
-}  // namespace
-
-std::vector<Cmd> fuse_blocks(const std::vector<Cmd>& in, int max_qubits) {
-    if (max_qubits == 0 || in.empty()) return in;
-    uint32_t max_q = 0, max_c = 0;
-    bool any_c = false;
-    for (const Cmd& c : in) {
-        for (uint32_t q : c.q) max_q = std::max(max_q, q);
-        for (uint32_t b : c.cbits) { max_c = std::max(max_c, b); any_c = true; }
-    }
-    const uint32_t nqw = max_q + 1;
-    const size_t n_wires = nqw + (any_c ? max_c + 1 : 0);
-    std::vector<size_t> front(n_wires, 0);
-    std::deque<Block> open;
-    size_t next_id = 1;
-    std::vector<Cmd> out;
-    out.reserve(in.size());
-
-    auto wires_of = [&](const Cmd& c) {
-        std::vector<uint32_t> ws(c.q.begin(), c.q.end());
-        for (uint32_t b : c.cbits) ws.push_back(nqw + b);
-        return ws;
-    };
-    auto emit = [&](Block& b) {
-        if (b.n_gates == 1) { out.push_back(std::move(b.first)); return; }
-        const size_t d = size_t{1} << b.qubits.size();
-        if (b.qubits.size() == 1 && frob_dist_identity(b.u, d) < 1e-12) return;
-        Cmd f;
-        f.gate = CUSTOM;
-        f.q = b.qubits;
-        f.u = std::move(b.u);
-        f.n_gates = b.src_gates;
-        out.push_back(std::move(f));
-    };
-    auto shares_wire = [](const Block& a, const Block& b) {
-        for (uint32_t w : a.wires) if (contains(b.wires, w)) return true;
-        return false;
-    };
-    auto flush_wires = [&](const std::vector<uint32_t>& ws) {
-        if (open.empty()) return;
-        std::vector<char> mark(open.size(), 0);
-        for (size_t i = 0; i < open.size(); ++i)
-            for (uint32_t w : ws) if (contains(open[i].wires, w)) { mark[i] = 1; break; }
-        for (size_t i = open.size(); i-- > 0;)
-            if (mark[i])
-                for (size_t j = 0; j < i; ++j)
-                    if (!mark[j] && shares_wire(open[j], open[i])) mark[j] = 1;
-        std::deque<Block> keep;
-        for (size_t i = 0; i < open.size(); ++i) {
-            if (mark[i]) emit(open[i]);
-            else keep.push_back(std::move(open[i]));
-        }
-        open.swap(keep);
-    };
-    auto flush_all = [&]() {
-        for (Block& b : open) emit(b);
-        open.clear();
-    };
-
-    for (const Cmd& c : in) {
-        if (c.gate == GPHASE) { out.push_back(c); continue; }
-        if (c.gate == BRANCH_BEGIN || c.gate == BRANCH_ELSE || c.gate == BRANCH_END ||
-            (c.gate == BARRIER && c.q.empty())) {
-            flush_all();
-            out.push_back(c);
-            continue;
-        }
-        const std::vector<uint32_t> ws = wires_of(c);
-        if (fusible(c, max_qubits)) {
-            Block* target = nullptr;
-            for (auto it = open.rbegin(); it != open.rend(); ++it) {
-                if (!can_join(it->qubits, c.q, max_qubits)) continue;
-                bool ok = true;
-                for (uint32_t w : ws) if (front[w] > it->id) { ok = false; break; }
-                if (ok) { target = &*it; break; }
-            }
-            if (!target) {
-                Block b;
-                b.id = next_id++;
-                b.qubits = c.q;
-                b.wires = ws;
-                b.n_gates = 1;
-                b.src_gates = c.n_gates;
-                b.first = c;
-                for (uint32_t w : ws) front[w] = b.id;
-                open.push_back(std::move(b));
-                continue;
-            }
-            Block& b = *target;
-            if (b.n_gates == 1) b.u = local_unitary(b.first);
-            std::vector<uint32_t> fresh;
-            for (uint32_t q : c.q) if (!contains(b.qubits, q)) fresh.push_back(q);
-            if (!fresh.empty()) extend(b, fresh);
-            std::vector<int> pos;
-            for (uint32_t q : c.q)
-                pos.push_back(static_cast<int>(std::find(b.qubits.begin(), b.qubits.end(), q) -
-                                               b.qubits.begin()));
-            left_apply(b.u, size_t{1} << b.qubits.size(), local_unitary(c), pos);
-            ++b.n_gates;
-            b.src_gates += c.n_gates;
-            for (uint32_t w : ws) {
-                if (!contains(b.wires, w)) b.wires.push_back(w);
-                front[w] = b.id;
-            }
-            continue;
-        }
-        flush_wires(ws);
-        out.push_back(c);
-        const size_t id = next_id++;
-        for (uint32_t w : ws) front[w] = id;
-    }
-    flush_all();
-    return out;
-}
-
-namespace {
-
-bool fusible_1q(const Cmd& c) {
-    if (c.q.size() != 1) return false;
-    switch (c.gate) {
-        case X: case Y: case Z: case H: case S: case SDG: case T: case TDG:
-        case RX: case RY: case RZ: case P: case U:
-            return true;
-        default:
-            return false;
-    }
-}
-
-// the reference's transpiler-side 2x2 gate table (transpiler/fusion.cpp gate_matrix)
-M2 matrix_1q(const Cmd& c) {
+// The transpiler-side 2x2 table of the named one-qubit gates (transpiler/fusion.cpp).
+std::vector<c128> matrix_1q(const Cmd& c) {
     switch (c.gate) {
         case RX: return m_rx(param(c, 0));
         case RY: return m_ry(param(c, 0));
@@ -773,89 +558,6 @@ M2 matrix_1q(const Cmd& c) {
         case U: return m_u(param(c, 0), param(c, 1), param(c, 2));
         default: return fixed(c.gate);
     }
-}
-
-struct Acc {
-    M2 m = {I1, I0, I0, I1};
-    int n = 0;
-    int src = 0;
-    uint32_t q = 0;
-    Cmd first;
-};
-
-}  // namespace
-
-std::vector<Cmd> fuse_single_qubit(const std::vector<Cmd>& in) {
-    if (in.empty()) return {};
-    uint32_t max_q = 0;
-    for (const Cmd& c : in) for (uint32_t q : c.q) max_q = std::max(max_q, q);
-    std::vector<Acc> accs(max_q + 1);
-    for (uint32_t q = 0; q <= max_q; ++q) accs[q].q = q;
-    std::vector<Cmd> out;
-    out.reserve(in.size());
-    auto flush = [&](Acc& a) {
-        if (a.n == 0) return;
-        if (a.n == 1) {
-            out.push_back(std::move(a.first));
-        } else {
-            const bool ident = std::abs(a.m[0] - I1) < 1e-12 && std::abs(a.m[1]) < 1e-12 &&
-                               std::abs(a.m[2]) < 1e-12 && std::abs(a.m[3] - I1) < 1e-12;
-            if (!ident) {
-                Cmd f;
-                f.gate = CUSTOM;
-                f.q = {a.q};
-                f.u = a.m;
-                f.n_gates = a.src;
-                out.push_back(std::move(f));
-            }
-        }
-        a.m = {I1, I0, I0, I1};
-        a.n = 0;
-        a.src = 0;
-        a.first = Cmd{};
-    };
-    for (const Cmd& c : in) {
-        if (fusible_1q(c) && !(c.flags & 1)) {
-            Acc& a = accs[c.q[0]];
-            if (a.n == 0) a.first = c;
-            const M2 b = matrix_1q(c);
-            const M2 A = a.m;
-            a.m = {b[0] * A[0] + b[1] * A[2], b[0] * A[1] + b[1] * A[3],
-                   b[2] * A[0] + b[3] * A[2], b[2] * A[1] + b[3] * A[3]};
-            ++a.n;
-            a.src += c.n_gates;
-            continue;
-        }
-        if (c.gate == BARRIER) {
-            if (c.q.empty()) for (Acc& a : accs) flush(a);
-            else for (uint32_t q : c.q) flush(accs[q]);
-            out.push_back(c);
-            continue;
-        }
-        if (c.q.size() == 1 && c.gate != MEASURE && c.gate != RESET) {
-            flush(accs[c.q[0]]);
-            out.push_back(c);
-            continue;
-        }
-        if (c.q.size() >= 2) {
-            for (uint32_t q : c.q) flush(accs[q]);
-            out.push_back(c);
-            continue;
-        }
-        if ((c.gate == MEASURE || c.gate == RESET) && !c.q.empty()) flush(accs[c.q[0]]);
-        if (c.gate == BRANCH_BEGIN || c.gate == BRANCH_ELSE || c.gate == BRANCH_END)
-            for (Acc& a : accs) flush(a);
-        out.push_back(c);
-    }
-    for (Acc& a : accs) flush(a);
-    return out;
-}
-
-std::vector<Cmd> fuse_for_dispatch(const std::vector<Cmd>& in, int n, int max_qubits,
-                                   int min_qubits) {
-    if (max_qubits == 0) return in;
-    if (max_qubits == 1 || n < min_qubits) return fuse_single_qubit(in);
-    return fuse_blocks(in, max_qubits);
 }
 
 }  // namespace qsv

@@ -59,13 +59,21 @@ std::vector<c128> local_unitary(const Cmd& c);
 // Command::dagger (reference: src/qarpx/src/core/command.cpp:19-59).
 Cmd dagger(const Cmd& c);
 
-// fuse_for_simulation (reference: src/qarpx/src/simulator/fusion.cpp:120-268).
+// 2x2 matrix of a named one-qubit gate (X, Y, Z, H, S, Sdg, T, Tdg, Rx, Ry, Rz, P, U),
+// row-major, as the transpiler's one-qubit fusion multiplies them (transpiler/fusion.cpp).
+std::vector<c128> matrix_1q(const Cmd& c);
+
+// Simulation fusion (fuse.cpp): the plans of fuse_for_simulation (reference:
+// src/qarpx/src/simulator/fusion.cpp:120-268), fuse_single_qubit_gates (reference:
+// src/qarpx/src/transpiler/fusion.cpp:196-300) and the selection between them that
+// fuse_for_dispatch makes (reference: qarp_simulator.cpp:120-129).
 std::vector<Cmd> fuse_blocks(const std::vector<Cmd>& in, int max_qubits);
-// fuse_single_qubit_gates (reference: src/qarpx/src/transpiler/fusion.cpp:196-300).
 std::vector<Cmd> fuse_single_qubit(const std::vector<Cmd>& in);
-// fuse_for_dispatch (reference: qarp_simulator.cpp:120-129).
 std::vector<Cmd> fuse_for_dispatch(const std::vector<Cmd>& in, int n_qubits, int max_qubits,
                                    int min_qubits);
+
+// The packed byte form of a command list (the inverse of decode).
+std::vector<uint8_t> encode(const std::vector<Cmd>& cmds);
 
 // ---------------------------------------------------------------- device operations
 // widest dense op: a controlled-powers unitary on up to 12 targets

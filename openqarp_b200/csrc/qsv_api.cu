@@ -493,6 +493,17 @@ int qsv_fuse_count(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min
     });
 }
 
+int qsv_fuse_plan(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min_q, uint8_t* out,
+                  size_t cap, size_t* nbytes_out) {
+    return guarded([&] {
+        if (!nbytes_out) throw std::invalid_argument("null output");
+        if (max_q < 0 || max_q > QSV_MAX_BLOCK_QUBITS) throw std::invalid_argument("fusion width out of range");
+        const std::vector<uint8_t> packed = encode(fuse_for_dispatch(decode(cmds, nbytes), n, max_q, min_q));
+        *nbytes_out = packed.size();
+        if (out && cap >= packed.size() && !packed.empty()) std::memcpy(out, packed.data(), packed.size());
+    });
+}
+
 int qsv_tile_plan_count(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min_q, int tile_qubits,
                         int32_t* tile_passes, int32_t* stream_passes) {
     return guarded([&] {

@@ -433,6 +433,43 @@ def pack(commands: Iterable, values: Optional[Mapping[str, float]] = None,
                         values)
 
 
+def unpack(buf: bytes) -> list:
+    """Decode a packed stream (include/qsv.h layout) back into commands: Command records
+    (Custom with its matrix), PermutationRecord and ControlledUnitaryRecord."""
+    out = []
+    off = 0
+    mv = memoryview(buf)
+    while off < len(buf):
+        g, nq, npar, ncb, flags, ncond, _ = _HDR.unpack_from(mv, off)
+        o = off + _HDR.size
+        ints = struct.unpack_from(f"<{nq + ncb + 2 * ncond}I", mv, o)
+        o += 4 * len(ints)
+        o = (o + 7) & ~7
+        vals = struct.unpack_from(f"<{npar}d", mv, o)
+        o += 8 * npar
+        qubits, cbits = ints[:nq], ints[nq:nq + ncb]
+        cond_bits, cond_vals = ints[nq + ncb:nq + ncb + ncond], ints[nq + ncb + ncond:]
+        if g == PERMUTATION_CODE:
+            d = 1 << nq
+            out.append(PermutationRecord(tuple(qubits), np.frombuffer(buf, np.uint64, d, o).copy()))
+            o += 8 * d
+        elif g == CONTROLLED_UNITARY_CODE:
+            d = 1 << (nq - 1)
+            m = np.frombuffer(buf, np.complex128, d * d, o).reshape(d, d).copy()
+            out.append(ControlledUnitaryRecord(tuple(qubits[:-1]), qubits[-1], m))
+            o += 16 * d * d
+        else:
+            u = None
+            if g == GateType.Custom:
+                d = 1 << nq
+                u = np.frombuffer(buf, np.complex128, d * d, o).reshape(d, d).copy()
+                o += 16 * d * d
+            out.append(Command(g, qubits, tuple(vals), u, cbits, tuple(cond_bits),
+                               tuple(bool(v) for v in cond_vals)))
+        off = o
+    return out
+
+
 def cbit_register_width(commands: Iterable) -> int:
     """Width of the per-shot classical register: one past the highest cbit any command
     writes or reads (reference: cbit_register_width, core/command.h)."""

@@ -19,7 +19,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_SO = os.path.join(HERE, "_build", "liboracle.so")
 REFERENCE_SO = os.path.join(HERE, "_ref", "libqarpref.so")
-REF_ROOT = os.environ.get("QSV_REFERENCE_ROOT", "/root/reference")
+# root of the reference source tree; the reference library is built only when it is given
+REF_ROOT = os.environ.get("QSV_REFERENCE_ROOT")
 
 PD = POINTER(c_double)
 PU64 = POINTER(c_uint64)
@@ -28,11 +29,14 @@ P8 = POINTER(c_uint8)
 PU32 = POINTER(c_uint32)
 
 
-def build(reference: bool = True) -> None:
-    """Compile the restatement, and the reference library when its sources are present."""
+def build(reference: bool = True, ref_root: str | None = None) -> None:
+    """Compile the restatement, and the reference library when the root of the reference
+    source tree is given (``ref_root`` or the QSV_REFERENCE_ROOT environment variable) and
+    holds its sources."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if reference and os.path.isdir(os.path.join(REF_ROOT, "src", "qarpx")):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"], check=True)
+    root = ref_root or REF_ROOT
+    if reference and root and os.path.isdir(os.path.join(root, "src", "qarpx")):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF_ROOT={root}"], check=True)
 
 
 def _d(a):
@@ -160,6 +164,8 @@ class Reference:
         lib.qref_apply_inplace.argtypes = [P8, c_size_t, c_int, PD]
         lib.qref_apply_fused_inplace.argtypes = [P8, c_size_t, c_int, c_int, c_int, PD, PI32]
         lib.qref_fuse_count.argtypes = [P8, c_size_t, c_int, c_int, c_int, PI32, PI32]
+        lib.qref_fuse_plan.argtypes = [P8, c_size_t, c_int, c_int, c_int, ctypes.c_void_p, c_size_t,
+                                       POINTER(c_size_t)]
         lib.qref_transition.argtypes = [PD, PD, c_int, PU64, PU64, PD, c_size_t, PD]
         lib.qref_expectation.argtypes = [P8, c_size_t, c_int, c_int, c_int, PU64, PU64, PD, c_size_t, PD]
         lib.qref_run.argtypes = [P8, c_size_t, c_int, c_int, c_uint32, c_int, c_int, PU64, PI32, c_size_t,
@@ -212,6 +218,15 @@ class Reference:
         self._check(self.lib.qref_apply_fused_inplace(_u8(buf), len(buf), n, fusion_max, fusion_min,
                                                       _d(state.view(np.float64)), ctypes.byref(cnt)))
         return cnt.value
+
+    def fuse_plan(self, buf, n, fusion_max, fusion_min=-1) -> bytes:
+        size = c_size_t()
+        self._check(self.lib.qref_fuse_plan(_u8(buf), len(buf), n, fusion_max, fusion_min, None, 0,
+                                            ctypes.byref(size)))
+        out = ctypes.create_string_buffer(max(size.value, 1))
+        self._check(self.lib.qref_fuse_plan(_u8(buf), len(buf), n, fusion_max, fusion_min, out, size,
+                                            ctypes.byref(size)))
+        return out.raw[:size.value]
 
     def fuse_count(self, buf, n, fusion_max, fusion_min=-1):
         cnt = c_int32()

@@ -13,6 +13,7 @@
 //   qref_run           -> QarpSimulator::run                (qarp_simulator.cpp:988-1244)
 //   qref_run_gradient  -> QarpSimulator::run_gradient       (qarp_simulator.cpp:1607-1618)
 //   qref_fuse_count    -> fuse_for_simulation               (fusion.cpp:120-268), block count
+//   qref_fuse_plan     -> the fused command list itself, packed as include/qsv.h records
 //   qref_program_*     -> qarpx::Program + QarpSimulator::program_statevector / program_run
 //                         (program.h:51-86, qarp_simulator.cpp:821-897)
 //
@@ -248,6 +249,59 @@ int qref_fuse_count(const uint8_t* cmds, size_t nbytes, int n, int fusion_max,
                 if (c.gate == GateType::Custom && c.qubits.size() <= 8)
                     widths_hist[c.qubits.size()]++;
         }
+        return QSV_OK;
+    } catch (...) {
+        return translate(std::current_exception());
+    }
+}
+
+// The fused stream itself, packed in the engine's record format (include/qsv.h): gate code,
+// qubits, cbits, condition, params, and the Custom matrix of each fused block.
+int qref_fuse_plan(const uint8_t* cmds, size_t nbytes, int n, int fusion_max, int fusion_min,
+                   uint8_t* out, size_t cap, size_t* nbytes_out) {
+    try {
+        auto sim = make_sim(fusion_max, fusion_min);
+        auto in = to_commands(cmds, nbytes);
+        std::vector<Command> fused;
+        if (fusion_max == 0) fused = in;
+        else if (fusion_max == 1 || static_cast<std::size_t>(std::max(n, 0)) < sim.fusion_min_qubits())
+            fused = qarpx::fuse_single_qubit_gates(in);
+        else fused = qarpx::fuse_for_simulation(
+            in, static_cast<std::size_t>(fusion_max),
+            [&sim](const Command& c) { return sim.local_unitary(c); });
+        std::vector<uint8_t> buf;
+        auto put = [&buf](const void* p, size_t nb) {
+            const size_t o = buf.size();
+            buf.resize(o + nb);
+            if (nb) std::memcpy(&buf[o], p, nb);
+        };
+        for (const Command& c : fused) {
+            qsv_cmd_header h{};
+            h.gate = static_cast<uint16_t>(c.gate);
+            h.n_qubits = static_cast<uint8_t>(c.qubits.size());
+            h.n_params = static_cast<uint8_t>(c.params.size());
+            h.n_cbits = static_cast<uint8_t>(c.cbits.size());
+            h.n_cond = static_cast<uint8_t>(c.condition_bits.size());
+            h.flags = h.n_cond ? 1 : 0;
+            put(&h, sizeof h);
+            for (auto q : c.qubits) put(&q, 4);
+            for (auto b : c.cbits) put(&b, 4);
+            for (auto b : c.condition_bits) put(&b, 4);
+            for (bool v : c.condition_values) { const uint32_t x = v ? 1u : 0u; put(&x, 4); }
+            buf.resize((buf.size() + 7) & ~size_t{7}, 0);
+            for (const auto& p : c.params) { const double v = p.evaluate({}); put(&v, 8); }
+            if (c.gate == GateType::Custom && c.unitary) {
+                const auto& U = *c.unitary;
+                for (Eigen::Index y = 0; y < U.rows(); ++y)
+                    for (Eigen::Index x = 0; x < U.cols(); ++x) {
+                        const double re = U(y, x).real(), im = U(y, x).imag();
+                        put(&re, 8);
+                        put(&im, 8);
+                    }
+            }
+        }
+        *nbytes_out = buf.size();
+        if (out && cap >= buf.size() && !buf.empty()) std::memcpy(out, buf.data(), buf.size());
         return QSV_OK;
     } catch (...) {
         return translate(std::current_exception());

@@ -2,7 +2,7 @@
 
 Run where the reference tree is available (it builds oracle/_ref from the reference sources):
 
-    python tests/golden/gen_golden.py
+    QSV_REFERENCE_ROOT=<root of the reference tree> python tests/golden/gen_golden.py
 
 Outputs:
   reference_vectors.npz — packed command streams (include/qsv.h layout), observables as
@@ -132,6 +132,8 @@ def main():
 
     np.savez_compressed(os.path.join(OUT, "reference_vectors.npz"), **data)
 
+    if not orc.REF_ROOT:
+        raise SystemExit("set QSV_REFERENCE_ROOT to the root of the reference tree")
     h2_src = os.path.join(orc.REF_ROOT, "benchmarks", "statevector", "data", "h2.json")
     with open(h2_src) as f:
         h2 = json.load(f)

@@ -2,7 +2,7 @@
 execution (qarpx::Program + QarpSimulator::program_statevector / program_run, built from the
 reference sources into oracle/_ref).
 
-    python tests/golden/gen_program_golden.py
+    QSV_REFERENCE_ROOT=<root of the reference tree> python tests/golden/gen_program_golden.py
 
 Each case is a list of kernel specs added to the reference Program in order (the reference
 composes adjacent permutations itself), an optional initial state, and the reference outputs:

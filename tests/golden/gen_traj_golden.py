@@ -2,7 +2,7 @@
 (QarpSimulator::run with mid-circuit Measure, Reset, classical conditions and branches, built from
 the reference sources into oracle/_ref).
 
-    python tests/golden/gen_traj_golden.py
+    QSV_REFERENCE_ROOT=<root of the reference tree> python tests/golden/gen_traj_golden.py
 
 ``traj_case`` rebuilds every case's command list from its name (seeded numpy draws), so the
 fixture holds only the reference's outputs: the per-shot classical registers (bit masks, shot
