@@ -546,21 +546,21 @@ def b200_arm(args, rank, world, local_rank):
         structured = None
         if single and not args.skip_structured:
             reg.close()
-            from openqarp_b200.workloads import structured_rows
+            from bench_workloads import structured_rows
             structured = structured_rows(device=device)
         plain12 = None
         if single and not args.skip_structured:
-            from openqarp_b200.workloads import config1_latency
+            from bench_workloads import config1_latency
             plain12 = config1_latency(device=device)
         traj = None
         if single and not args.skip_trajectories:
             reg.close()
-            from openqarp_b200.workloads import trajectory_rows
+            from bench_workloads import trajectory_rows
             traj = trajectory_rows(device=device)
         heis = None
         if single and not args.skip_heisenberg:
             reg.close()
-            from openqarp_b200.workloads import heisenberg_bulk
+            from bench_workloads import heisenberg_bulk
             heis = heisenberg_bulk(n=31, steps=50, dt=0.05, seed=SEED, device=device)
         fp64_achieved = flops / (ms_step * 1e-3) / 1e12
         result = {

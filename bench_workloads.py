@@ -12,7 +12,7 @@ import time
 
 import numpy as np
 
-from . import Register, circuits, ir, observable
+from openqarp_b200 import Register, circuits, ir, observable
 
 
 def heisenberg_bulk(n: int = 31, steps: int = 50, dt: float = 0.05, seed: int = 1234, device: int = 0,
@@ -68,7 +68,7 @@ def qpe_program(n_count: int, n_target: int, seed: int = 1234):
     0..n_count-1, one controlled-powers kernel U^(2^j) under counting qubit j on the target
     register (U a seeded Haar unitary on n_target qubits), then the inverse QFT on the counting
     register as a gates kernel (H, controlled phases, reversing swaps)."""
-    from .program import Program
+    from openqarp_b200.program import Program
     G = ir.GateType
     rng = np.random.default_rng(seed)
     d = 1 << n_target
@@ -102,8 +102,8 @@ def structured_rows(device: int = 0, n_big: int = 28, n_small: int = 22, shots: 
       register (count pass, and count + write pass with the survivors copied to host);
     * parities: seeded sampling of ``shots`` outcomes plus the odd-parity counts of ``n_masks``
       Z masks on the device, against the same counts by numpy on the host outcomes."""
-    from . import Register
-    from .ir import pack
+    from openqarp_b200 import Register
+    from openqarp_b200.ir import pack
     out = {}
     for n in (n_big, n_small):
         prog = qpe_program(n - 4, 4, seed)
@@ -147,7 +147,7 @@ def structured_rows(device: int = 0, n_big: int = 28, n_small: int = 22, shots: 
     reg.apply(pack(circuits.brickwork(n_big, 4, seed=seed)).buf)
     reg.synchronize()
     import ctypes
-    from ._lib import lib, check
+    from openqarp_b200._lib import lib, check
     cnt = ctypes.c_uint64()
     t0 = time.perf_counter()
     check(lib.qsv_exact_probs(reg.handle, 1e-12, None, None, 0, ctypes.byref(cnt)))
@@ -186,9 +186,9 @@ def trajectory_rows(device: int = 0, shapes=((16, 8, 4096), (10, 8, 20000)), ref
     (oracle/_ref, all host threads) on the first ``ref_shots`` shots of each; their per-shot
     classical registers must equal the device's, since shot s draws from std::mt19937(seed + s)
     on both."""
-    from . import B200Simulator
-    from .ir import pack
-    from .noise import _FULL_1Q, _FULL_2Q, NoiseModel
+    from openqarp_b200 import B200Simulator
+    from openqarp_b200.ir import pack
+    from openqarp_b200.noise import _FULL_1Q, _FULL_2Q, NoiseModel
     noisy_model = NoiseModel.depolarizing(0.01, "all") + NoiseModel.amplitude_damping(0.02, ["U"])
     noisy_specs = [("depolarizing", 0.01, [int(g) for g in _FULL_1Q + _FULL_2Q]),
                    ("amplitude_damping", 0.02, [int(ir.GateType.U)])]
@@ -240,8 +240,8 @@ def config1_latency(device: int = 0, n: int = 12, layers: int = 10, n_terms: int
     ``B200Simulator`` (statevector to host, expectation, run) — microseconds per call, median
     of ``reps`` — next to the reference CPU simulator's own calls on the host cores.  A 64 KiB
     register: every call is launch- and transfer-latency bound."""
-    from . import B200Simulator
-    from .ir import pack
+    from openqarp_b200 import B200Simulator
+    from openqarp_b200.ir import pack
     cmds, vals, names = circuits.hea(n, layers, seed=seed)
     concrete = [ir.Command(c.gate, c.qubits, tuple(p.evaluate(vals) for p in c.params)) for c in cmds]
     obs = circuits.random_pauli_sum(n, n_terms, seed=seed + 1)

@@ -322,10 +322,12 @@ QSV_API int qsv_qaoa_destroy(void* q);
  * allocator, an inference server's arena), or a latency-critical path that cannot take the
  * device-wide synchronisation cudaMalloc/cudaFree imply.  Same value as qsv_transition,
  * <bra|H|ket>, for caller-owned DEVICE registers d_bra/d_ket (double2* for QSV_C128, float2*
- * for QSV_C64, 2^n_qubits amplitudes on the same device), host observable arrays and a host
- * out[2], on the caller's stream (NULL = legacy default stream); returns after the result
- * is in out.  It allocates nothing: its scratch (term tables + partial sums) is one
- * file-scope device array of 256 KiB that every GPU loading the library holds until exit.
+ * for QSV_C64, 2^n_qubits amplitudes on the same device; anything else, a host pointer
+ * included, is rejected with QSV_EINVAL), host observable arrays and a host out[2], on the
+ * caller's stream (NULL = legacy default stream); returns after the result is in out.  It
+ * allocates no device memory: its scratch (term tables + partial sums) is one file-scope
+ * device array of 256 KiB that every GPU loading the library holds until exit.  A call that
+ * succeeds makes no host allocation either; a failing call builds its message on the host.
  * Limits and rules: at most QSV_STATIC_MAX_TERMS terms (more -> QSV_EINVAL); every call on a
  * device shares that array and leaves its contents behind, so calls that overlap on the GPU
  * race and must be serialised by the caller; the first call on a device looks up the

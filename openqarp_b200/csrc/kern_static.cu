@@ -17,7 +17,9 @@
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call before any
 //     stream capture begins.
-// No call here allocates: no cudaMalloc / cudaFree, no host heap, no library allocator.
+// No call here allocates device memory: no cudaMalloc / cudaFree, no library allocator.  A
+// call that succeeds makes no host allocation either; a call that fails builds its error
+// message (read back with qsv_last_error) on the host heap.
 #include <mutex>
 #include <string>
 
@@ -187,6 +189,15 @@ extern "C" QSV_API int qsv_transition_static(const void* d_bra, const void* d_ke
     if (e != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
         cudaGetLastError();
         set_last_error("ket is not device memory");
+        return QSV_EINVAL;
+    }
+    // the bra must live on the same device: a host pointer, managed memory or another
+    // device's register would reach the kernel as an address it cannot read
+    cudaPointerAttributes battr{};
+    e = cudaPointerGetAttributes(&battr, d_bra);
+    if (e != cudaSuccess || battr.type != cudaMemoryTypeDevice || battr.device != attr.device) {
+        cudaGetLastError();
+        set_last_error("bra is not device memory on the ket's device");
         return QSV_EINVAL;
     }
     int prev = 0;

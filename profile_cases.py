@@ -1,16 +1,16 @@
 """Small, self-contained cases of each hot kernel for profiling under ncu.
 
-    python -m openqarp_b200.profile_cases dense --n 26 --k 3 --reps 5
-    python -m openqarp_b200.profile_cases brickwork --n 26 --depth 4 --k 3
-    python -m openqarp_b200.profile_cases transition --n 24 --terms 547
-    python -m openqarp_b200.profile_cases adjoint --n 22 --layers 2
-    python -m openqarp_b200.profile_cases sample --n 26 --shots 100000
-    python -m openqarp_b200.profile_cases exact --n 26
-    python -m openqarp_b200.profile_cases parity --n 26 --shots 1048576 --terms 512
-    python -m openqarp_b200.profile_cases perm --n 26
-    python -m openqarp_b200.profile_cases traj --n 16 --depth 8 --shots 4096 [--noisy] [--batch 0]
-    python -m openqarp_b200.profile_cases heisenberg --n 26 --dtype complex64 --k 0
-    python -m openqarp_b200.profile_cases qaoa --shots 256
+    python profile_cases.py dense --n 26 --k 3 --reps 5
+    python profile_cases.py brickwork --n 26 --depth 4 --k 3
+    python profile_cases.py transition --n 24 --terms 547
+    python profile_cases.py adjoint --n 22 --layers 2
+    python profile_cases.py sample --n 26 --shots 100000
+    python profile_cases.py exact --n 26
+    python profile_cases.py parity --n 26 --shots 1048576 --terms 512
+    python profile_cases.py perm --n 26
+    python profile_cases.py traj --n 16 --depth 8 --shots 4096 [--noisy] [--batch 0]
+    python profile_cases.py heisenberg --n 26 --dtype complex64 --k 0
+    python profile_cases.py qaoa --shots 256
 
 Registers of 2^26 complex128 amplitudes (1 GiB) exceed L2 (126 MB), so DRAM counters are
 meaningful, and stay small enough for a full-set capture to end within minutes.
@@ -21,7 +21,7 @@ import argparse
 
 import numpy as np
 
-from . import Register, circuits, ir, observable
+from openqarp_b200 import Register, circuits, ir, observable
 
 
 def main(argv=None):
@@ -77,14 +77,14 @@ def main(argv=None):
         for _ in range(a.reps):
             reg.sample_parities(7, a.shots, masks)
     elif a.case == "perm":
-        from .ir import PermutationRecord
+        from openqarp_b200.ir import PermutationRecord
         qs = tuple(int(q) for q in rng.permutation(a.n)[:16])
         rec = PermutationRecord(qs, rng.permutation(1 << 16).astype(np.uint64))
         reg.configure(0, 0, 0)
         for _ in range(a.reps):
             reg.apply(ir.pack([rec]).buf)
     elif a.case == "traj":
-        from .noise import NoiseModel
+        from openqarp_b200.noise import NoiseModel
         if a.noisy:
             reg.set_noise(NoiseModel.depolarizing(0.01, "all") + NoiseModel.amplitude_damping(0.02, ["U"]))
         reg.set_trajectory_batch(a.batch)
@@ -99,7 +99,7 @@ def main(argv=None):
         reg.apply(ir.pack(circuits.heisenberg_trotter(a.n, 1, 0.05, fields)).buf)
     elif a.case == "qaoa":
         # the batched-QAOA configuration's instance mix, --shots instances, one persistent launch
-        from .batch import QaoaBatch, config4_instances
+        from openqarp_b200.batch import QaoaBatch, config4_instances
         inst, params = config4_instances(count=a.shots)
         qb = QaoaBatch(inst)
         for _ in range(a.reps):

@@ -481,7 +481,7 @@ def test_complex64_bulk_mode_error_bounds(restatement, sim64):
 def test_heisenberg_bulk_complex64_against_oracle(restatement):
     """Config-5 shape at 16 qubits: complex64 bulk evolution with FP64 renormalisation per
     Trotter step against the complex128 CPU oracle."""
-    from openqarp_b200.workloads import heisenberg_bulk
+    from bench_workloads import heisenberg_bulk
     n, steps, dt = 16, 12, 0.05
     res = heisenberg_bulk(n=n, steps=steps, dt=dt, seed=3)
     fields = np.random.default_rng(3).uniform(-1.0, 1.0, n)

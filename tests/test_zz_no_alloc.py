@@ -5,8 +5,9 @@ their own pool allocator, or latency-critical paths that cannot take the synchro
 cudaMalloc/cudaFree imply — so it takes caller-owned device registers and keeps its scratch
 in a fixed file-scope device array.  This file checks it through the C-ABI against the
 handle-based qsv_transition on two calls in a row (the second call sees the first call's
-leftovers in the shared array), in both storage precisions, and that it rejects term counts
-above its static limit.  It is named to be collected last, and passes both alone in a fresh
+leftovers in the shared array), in both storage precisions, against the CPU oracle on a
+register wide enough to cap the grid, and that it rejects term counts above its static limit
+and a bra that is not device memory.  It is named to be collected last, and passes both alone in a fresh
 process and after the rest of the suite.
 """
 import ctypes
@@ -60,6 +61,50 @@ def test_static_matches_handle_path_twice(dtype, tol):
     finally:
         bra.close()
         ket.close()
+
+
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+def test_static_full_grid_against_oracle(dtype, restatement):
+    """A 21-qubit register needs more blocks than the static partials array holds, so the
+    grid is capped and every block walks several strides; the fixed-order final sum then
+    reads every partial.  Checked against the CPU oracle on the amplitudes the registers
+    actually hold (complex64 rounding included), twice in a row."""
+    n = 21
+    bra, ket = Register(n, dtype), Register(n, dtype)
+    try:
+        for seed in (5, 6):
+            bra.set_state(random_state(n, seed), validate=False)
+            ket.set_state(random_state(n, seed + 10), validate=False)
+            obs = circuits.random_pauli_sum(n, 48, seed=seed, max_weight=4) + circuits.tfim_chain(n)
+            masks = observable.to_masks(obs, n)
+            got = static_transition(bra, ket, masks)
+            want = restatement.transition(bra.get_state(), ket.get_state(), n, masks)
+            assert abs(got - want) < EV_TOL, (got, want)
+            assert abs(got - bra.transition(ket, masks)) < EV_TOL
+    finally:
+        bra.close()
+        ket.close()
+
+
+def test_static_rejects_a_bra_outside_device_memory():
+    """A host array passed as the bra is refused before any kernel runs."""
+    n = 8
+    reg = Register(n)
+    try:
+        host = np.zeros(1 << n, dtype=np.complex128)
+        masks = observable.to_masks(circuits.tfim_chain(n), n)
+        out = np.zeros(2)
+        d_ket, s = reg.device_pointer()
+        rc = _lib.lib.qsv_transition_static(
+            ctypes.c_void_p(host.ctypes.data), ctypes.c_void_p(d_ket), n, _lib.QSV_C128,
+            _lib.u64ptr(masks.x), _lib.u64ptr(masks.z), _lib.dptr(masks.coeff), masks.n_terms,
+            ctypes.c_void_p(s), _lib.dptr(out))
+        assert rc == _lib.QSV_EINVAL
+        assert "bra is not device memory" in _lib.lib.qsv_last_error().decode()
+        # the entry point still works afterwards
+        assert abs(static_transition(reg, reg, masks) - reg.expectation(masks)) < EV_TOL
+    finally:
+        reg.close()
 
 
 def test_static_rejects_too_many_terms():
