@@ -2,19 +2,30 @@
 """Benchmark of the B200 statevector engine.
 
 Headline workload (one "step"): one application of a 28-qubit random brickwork circuit of
-depth 20 (Haar SU(2) on every qubit + alternating CZ layers), complex128, with the fusion
-width chosen by the autotuner.  Metric: gate GB/s = algorithmic HBM bytes of the fused-gate
-passes (2 x 2^n x 16 B per full-register pass) / device time.  The register (4 GiB) is larger
-than L2 (126 MB), so no L2 flush is needed between steps.
+depth 20 (Haar SU(2) on every qubit + alternating CZ layers), complex128, with the executor
+and fusion width the engine's autotuner chooses (openqarp_b200/autotune.py).  The register
+(4 GiB) is larger than L2 (126 MB), so no L2 flush is needed between steps.
+
+Metric, "gate GB/s": the workload's fixed gate work per step — the reference's own fused plan
+for the circuit (fusion width 3: 140 full-register passes) x 2 x 2^28 x 16 B — divided by the
+device time of one step.  It is an effective rate (work fixed by the workload, like tokens/s),
+not a count of the engine's own traffic: the engine's plan moves fewer bytes (83 passes at
+width 4), so it can exceed the HBM peak.  The engine's own HBM traffic is reported beside it
+(`hbm_gbs`, `hbm_frac_of_peak`).
 
 Also reported on the same line:
-  * roofline of the dominant kernel (the fused dense-block pass) against measured HBM peak;
-  * e2e: the same metric through the public Register API with the command stream uploaded
-    and the final state read back into pinned host memory inside the timed region;
+  * roofline of the dominant pass class, from per-pass CUDA events recorded on the engine's
+    stream inside the timed region (the engine's pass timer): its algorithmic bytes per
+    launch over its average launch duration, against the measured HBM peak;
+  * e2e: the same metric through the plugin call a QarpEngine makes,
+    B200Simulator.statevector(commands, 28) with default knobs (autotuned plan), the command
+    stream packed and uploaded and the 4 GiB state read back into pinned host memory inside
+    every timed step;
+  * scale_30q: the same circuit shape at 30 qubits (16 GiB register);
   * adjoint: 24-qubit HEA (8 layers, 384 parameters) with TFIM + 500 random weight<=4
     terms, gradients/s of the adjoint sweep vs the parameter-shift rule on the same GPU;
-  * cpu_baseline: the reference's own CPU simulator (oracle/_ref) on the host cores over a
-    bounded sample of the same workload;
+  * cpu_baseline: the reference's own CPU simulator (oracle/_ref) on the host cores, the whole
+    circuit once;
   * structured_and_readouts: a phase-estimation-shaped structured program (controlled powers
     + inverse QFT) at 28 and 22 qubits with the reference's CPU program_statevector at 22, the
     exact Born readout and the PauliAveraging parity counts on the device;
@@ -49,9 +60,14 @@ CPU_LAYERS = 4      # host-core sample (the circuit's first layers) of cpu_basel
 ADJ_N, ADJ_LAYERS, ADJ_TERMS = 24, 8, 500
 
 
-# DRAM bytes per launch of the dominant kernel (k_dense_reg<double,4>): 2092.9 MB captured by ncu on
-# a 26-qubit register (profiles/k_dense_reg_c128_k4_26q.md), scaled to the 28-qubit register
-DENSE4_TRAFFIC_28Q = 4 * 2092.9e6
+# DRAM bytes per launch of the 4-qubit dense pass (k_dense_reg<double,4>): 2092.9 MB captured
+# by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a 26-qubit register, x4 for 2^28
+# amplitudes (traffic grows with the register: one read and one write of every amplitude)
+MEASURED_TRAFFIC_28Q = {"dense4": 4 * 2092.9e6}
+KERNEL_OF_CLASS = {"dense1": "k_dense_reg<double,1>", "dense2": "k_dense_reg<double,2>",
+                   "dense3": "k_dense_reg<double,3>", "dense4": "k_dense_reg<double,4>",
+                   "dense5": "k_dense_dmma<double,5>", "dense6": "k_dense_dmma<double,6>",
+                   "tile_rt": "k_tile_rt<double>", "tile_pass": "k_tile_pass<double>"}
 
 
 def measured_peaks():
@@ -148,24 +164,20 @@ class StreamTimer:
 
 
 EXECUTORS = {0: "stream", 1: "tiled"}
-CANDIDATES = ((0, 2), (0, 3), (0, 4), (1, 1), (1, 2), (1, 3), (1, 4))
 
 
-def autotune(reg, buf, timer, candidates=CANDIDATES):
-    """Pick the (executor, fusion width) with the shortest device time for this circuit: one
-    timed application per candidate after one warm-up."""
-    res = {}
-    for executor, k in candidates:
-        reg.configure(k, 12, executor)
-        reg.apply(buf)
-        reg.synchronize()
-        e0 = timer.event()
-        reg.apply(buf)
-        e1 = timer.event()
-        e1.synchronize()
-        res[(executor, k)] = e0.elapsed_time(e1)
-    best = min(res, key=res.get)
-    return best, {f"{EXECUTORS[e]}_k{k}": round(v, 3) for (e, k), v in res.items()}
+def dominant_pass(times: dict, amp_bytes: int = 16):
+    """The pass class with the largest device time in a pass-timer record, with its launches,
+    algorithmic bytes per launch and average launch duration."""
+    label = max(times, key=lambda k: times[k]["ms"])
+    t = times[label]
+    per_launch_ms = t["ms"] / t["launches"]
+    bytes_per_launch = t["bytes"] / t["launches"]
+    total_ms = sum(v["ms"] for v in times.values())
+    return {"class": label, "kernel": KERNEL_OF_CLASS.get(label, label) if amp_bytes == 16 else label,
+            "launches": t["launches"], "bytes_per_launch": bytes_per_launch,
+            "avg_launch_ms": per_launch_ms, "share_of_pass_time": t["ms"] / total_ms if total_ms else None,
+            "achieved_gbs": bytes_per_launch / (per_launch_ms * 1e-3) / 1e9}
 
 
 def fp64_peak_tflops(device):
@@ -224,28 +236,28 @@ def dense_flops(buf, n, k, executor):
     return float(dense + other) * (1 << n)
 
 
-def cpu_baseline_sample(buf_layer, n, threads=None):
-    """The reference CPU simulator (oracle/_ref, its own fused dispatch at k=3) on a few
-    brickwork layers at the full register width: returns (GB/s, seconds, passes, cores)."""
+def cpu_baseline_sample(buf, n, threads=None):
+    """The reference CPU simulator (oracle/_ref: its own fusion at width 3, then apply_command
+    per block on a caller-owned register) on ``buf`` at the full register width: returns
+    (gate GB/s, seconds, fused passes, cores, kind).  Without the compiled reference the C
+    restatement stands in (one thread, unfused)."""
     from oracle.oracle import Reference, Restatement
     cores = threads or os.cpu_count() or 1
+    state = np.zeros(1 << n, dtype=np.complex128)
+    state[0] = 1
     try:
         ref = Reference()
         ref.set_threads(cores)
-        state = np.zeros(1 << n, dtype=np.complex128)
-        state[0] = 1
         t0 = time.perf_counter()
-        passes = ref.apply_fused_inplace(state, n, buf_layer, 3, 12)
+        passes = ref.apply_fused_inplace(state, n, buf, 3, 12)
         dt = time.perf_counter() - t0
         kind = "reference"
     except FileNotFoundError:
         rs = Restatement()
-        state = np.zeros(1 << n, dtype=np.complex128)
-        state[0] = 1
         t0 = time.perf_counter()
-        rs.apply(state, n, buf_layer)
+        rs.apply(state, n, buf)
         dt = time.perf_counter() - t0
-        passes = fused_passes(buf_layer, n, 0)[0]
+        passes = fused_passes(buf, n, 0)[0]
         kind, cores = "port", 1
     gbs = passes * 2 * (1 << n) * 16 / dt / 1e9
     return gbs, dt, passes, cores, kind
@@ -421,6 +433,10 @@ def reference_arm(args, rank, world):
         times.append(dt)
         rates.append(gbs)
     v = float(np.median(rates))
+    # once, outside the timed steps: the whole circuit, to show the rate of the first layers
+    # holds for all of them
+    _, full = brickwork_stream()
+    fgbs, fdt, fpasses, _, _ = cpu_baseline_sample(full, N_QUBITS)
     print(json.dumps({
         "metric": "gate GB/s (%HBM peak) @28q", "value": v, "unit": "GB/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -434,29 +450,81 @@ def reference_arm(args, rank, world):
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": kind,
                          "sample": f"the circuit's first {CPU_LAYERS} layers at {N_QUBITS} qubits per step "
                                    f"({passes} fused passes)"},
+        "full_circuit_check": {"gbs": fgbs, "s": fdt, "passes": fpasses,
+                               "note": f"the whole depth-{DEPTH} circuit once on the same cores"},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
+def pinned_buffer(n_amps):
+    import torch
+    return torch.empty(2 * n_amps, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+
+
+def scale_row(device, n, depth=DEPTH, steps=3):
+    """The brickwork shape at another width through the plugin surface: autotuned plan, then
+    ``steps`` timed applications with the pass timer on."""
+    from openqarp_b200 import B200Simulator, circuits, ir
+    cmds = circuits.brickwork(n, depth, seed=SEED)
+    buf = ir.pack(cmds).buf
+    sim = B200Simulator(device=device)
+    try:
+        reg = sim.prepared_register(cmds, n)          # tunes (or reads the cache) and applies once
+        plan = dict(sim.last_plan)
+        timer = StreamTimer(reg)
+        reg.synchronize()
+        s0 = reg.stats()
+        reg.set_timing(True)
+        e0 = timer.event()
+        for _ in range(steps):
+            reg.apply(buf)
+        e1 = timer.event()
+        e1.synchronize()
+        times = reg.pass_times()
+        reg.set_timing(False)
+        s1 = reg.stats()
+        ms = e0.elapsed_time(e1) / steps
+        peak, peak_kind = measured_peaks()
+        dom = dominant_pass(times)
+        hbm = (s1["hbm_bytes"] - s0["hbm_bytes"]) / steps / (ms * 1e-3) / 1e9
+        ref_passes, _ = fused_passes(buf, n, 3)
+        return {"n_qubits": n, "depth": depth, "ms_per_circuit": ms,
+                "plan": {"executor": EXECUTORS.get(plan["executor"], plan["executor"]),
+                         "fusion_k": plan["fusion_k"], "source": plan["source"]},
+                "gate_gbs": ref_passes * 2 * (1 << n) * 16 / (ms * 1e-3) / 1e9,
+                "hbm_gbs": hbm, "hbm_frac_of_peak": hbm / peak,
+                "dominant_pass": dom, "dominant_frac_of_peak": dom["achieved_gbs"] / peak,
+                "peak_gbs": peak, "peak_source": peak_kind}
+    finally:
+        sim.close()
+
+
 def b200_arm(args, rank, world, local_rank):
     import torch
-    from openqarp_b200 import Register, circuits, ir
+    from openqarp_b200 import B200Simulator
     device = local_rank
     torch.cuda.set_device(device)
     dist = None
     if world > 1:
         import torch.distributed as dist  # noqa: F811
     cmds, buf = brickwork_stream()
-    reg = Register(N_QUBITS, "complex128", device)
-    timer = StreamTimer(reg)
+    sim = B200Simulator(device=device)
     if args.executor is not None and args.k is not None:
-        best_exec, best_k, sweep = args.executor, args.k, "fixed by --executor/--k"
-    else:
-        (best_exec, best_k), sweep = autotune(reg, buf, timer)
-    reg.configure(best_k, 12, best_exec)
+        sim.executor = args.executor
+        sim.fusion_max_qubits = args.k
+    out = pinned_buffer(1 << N_QUBITS)
+    # the plugin call once: the autotuner times its candidate plans here (or reads its cache)
+    sim.statevector(cmds, N_QUBITS, out=out)
+    plan = dict(sim.last_plan)
+    tune_entry = None
+    if plan.get("key"):
+        from openqarp_b200.autotune import default_tuner
+        tune_entry = default_tuner().entry(plan["key"])
+    best_exec, best_k = plan["executor"], plan["fusion_k"]
+    reg = sim.prepared_register(cmds, N_QUBITS)      # the simulator's register, plan applied
+    timer = StreamTimer(reg)
     passes, hist = fused_passes(buf, N_QUBITS, best_k)
     ref_passes, _ = fused_passes(buf, N_QUBITS, 3)          # the reference's default plan
-    pass_bytes = 2 * (1 << N_QUBITS) * 16
     for _ in range(args.warmup):
         reg.apply(buf)
     reg.synchronize()
@@ -464,6 +532,7 @@ def b200_arm(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize(device)
     s0 = reg.stats()
+    reg.set_timing(True)
     with ClockSampler(device) as clocks:
         e0 = timer.event()
         for _ in range(args.steps):
@@ -471,6 +540,8 @@ def b200_arm(args, rank, world, local_rank):
         e1 = timer.event()
         e1.synchronize()
     torch.cuda.synchronize(device)
+    pass_times = reg.pass_times()
+    reg.set_timing(False)
     s1 = reg.stats()
     ms = e0.elapsed_time(e1)
     if dist is not None:
@@ -484,40 +555,29 @@ def b200_arm(args, rank, world, local_rank):
     # work per step, fixed by the workload: the fused-gate passes of the reference's own plan
     # (fusion k = 3), each 2 x 2^n x 16 bytes — the same count the reference arm uses, so the
     # ratio of the two arms is the ratio of their circuit times
-    work_bytes = ref_passes * pass_bytes
+    work_bytes = ref_passes * (2 * (1 << N_QUBITS) * 16)
     value = world * work_bytes / (ms_step * 1e-3) / 1e9
-    physical = world * phys_bytes_per_step / (ms_step * 1e-3) / 1e9
+    hbm_gbs = world * phys_bytes_per_step / (ms_step * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-
-    # dominant kernel: its algorithmic bytes (one read + one write of the register per launch)
-    # over its average launch time in the timed region
-    if best_exec == 1:
-        avg_ms = ms_step / max(hbm_passes_per_step, 1)
-        kernel = "k_tile_pass<double>"
-    else:
-        probe_ms, probe_q = kernel_probe(reg, timer, best_k)
-        avg_ms = probe_ms
-        kernel = f"k_dense_reg<double,{best_k}> on qubits {list(probe_q)}"
-    achieved = pass_bytes / (avg_ms * 1e-3) / 1e9
+    dom = dominant_pass(pass_times)
     flops = dense_flops(buf, N_QUBITS, best_k, best_exec)
     fp64_peak = fp64_peak_tflops(device) if rank == 0 else None
-    reg.configure(best_k, 12, best_exec)
 
-    # end to end through the public API: upload commands, apply from |0>, read back
-    out = torch.empty(2 * (1 << N_QUBITS), dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
-    reg.reset()
-    reg.apply(buf)
-    reg.get_state(out)
+    # end to end through the plugin call: pack + upload the commands, apply from |0> with the
+    # autotuned plan, read the 4 GiB state back into pinned host memory
     e2e_times = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(args.steps):
         t0 = time.perf_counter()
-        stream = ir.pack(cmds)
-        reg.reset()
-        reg.apply(stream)
-        reg.get_state(out)
+        sim.statevector(cmds, N_QUBITS, out=out)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = float(np.median(e2e_times))
     e2e_value = world * work_bytes / e2e_s / 1e9
+    # the same call into a fresh pageable array (the reference's return convention), once
+    t0 = time.perf_counter()
+    sim.statevector(cmds, N_QUBITS)
+    e2e_pageable_s = time.perf_counter() - t0
+    sim.close()
+    del out
 
     qaoa = None
     if not args.skip_qaoa:
@@ -529,23 +589,21 @@ def b200_arm(args, rank, world, local_rank):
         # the single-GPU rows run only at N = 1: at N > 1 every GPU would wait for rank 0
         single = world == 1
         if world == 1 and not args.skip_cpu:
-            # the circuit's first CPU_LAYERS layers: a few seconds of host work
-            prefix = ir.pack(circuits.brickwork(N_QUBITS, CPU_LAYERS, seed=SEED)).buf
-            gbs, dt, cpasses, cores, kind = cpu_baseline_sample(prefix, N_QUBITS)
+            gbs, dt, cpasses, cores, kind = cpu_baseline_sample(buf, N_QUBITS)
             cpu = {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind,
-                   "sample": f"the circuit's first {CPU_LAYERS} layers at {N_QUBITS} qubits ({cpasses} fused "
+                   "sample": f"the whole depth-{DEPTH} circuit once at {N_QUBITS} qubits ({cpasses} fused "
                              f"passes, k=3), {dt:.1f} s"}
+        scale30 = None
+        if single and not args.skip_scale:
+            scale30 = scale_row(device, 30)
         adj = None
         if single and not args.skip_adjoint:
-            reg.close()
             adj = adjoint_vs_param_shift(device)
         sweep_k = None
         if single and not args.skip_ksweep:
-            reg.close()
             sweep_k = k_sweep(device, buf)
         structured = None
         if single and not args.skip_structured:
-            reg.close()
             from bench_workloads import structured_rows
             structured = structured_rows(device=device)
         plain12 = None
@@ -554,12 +612,10 @@ def b200_arm(args, rank, world, local_rank):
             plain12 = config1_latency(device=device)
         traj = None
         if single and not args.skip_trajectories:
-            reg.close()
             from bench_workloads import trajectory_rows
             traj = trajectory_rows(device=device)
         heis = None
         if single and not args.skip_heisenberg:
-            reg.close()
             from bench_workloads import heisenberg_bulk
             heis = heisenberg_bulk(n=31, steps=50, dt=0.05, seed=SEED, device=device)
         fp64_achieved = flops / (ms_step * 1e-3) / 1e12
@@ -569,31 +625,42 @@ def b200_arm(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic",
             "config": {"workload": f"brickwork n={N_QUBITS} depth={DEPTH} Haar SU(2)+CZ, seed {SEED}",
-                       "executor": EXECUTORS[best_exec], "fusion_k": best_k, "autotune_ms": sweep,
+                       "executor": EXECUTORS.get(best_exec, best_exec), "fusion_k": best_k,
+                       "plan_source": plan["source"],
+                       "autotune_ms": (tune_entry or {}).get("ms"),
                        "fused_blocks": passes, "hbm_passes_per_step": hbm_passes_per_step,
                        "block_widths": {str(k): int(c) for k, c in enumerate(hist) if c},
                        "work_definition": f"{ref_passes} fused-gate passes of the reference plan "
                                           f"(k=3) x 2 x 2^{N_QUBITS} x 16 B per step",
                        "l2": "register 4 GiB > L2 126 MB: no flush needed",
                        "parallelism": f"replicas x{world}"},
-            "pct_hbm_peak": 100.0 * value / (world * peak),
-            "physical_gbs": physical, "physical_pct_hbm_peak": 100.0 * physical / (world * peak),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": DENSE4_TRAFFIC_28Q, "kernel": kernel,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                                           "k_dense_reg<double,4> at 26 qubits, x4 to 2^28 amplitudes "
-                                           "(profiles/k_dense_reg_c128_k4_26q.md)",
+            "hbm_gbs": hbm_gbs, "hbm_frac_of_peak": hbm_gbs / (world * peak),
+            "roofline": {"bound": "hbm", "achieved": dom["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": dom["achieved_gbs"] / peak,
+                         "traffic": MEASURED_TRAFFIC_28Q.get(dom["class"]),
+                         "kernel": dom["kernel"], "pass_class": dom["class"],
+                         "launches_in_timed_region": dom["launches"],
+                         "avg_launch_ms": dom["avg_launch_ms"],
+                         "share_of_pass_time": dom["share_of_pass_time"],
+                         "bytes_per_launch": dom["bytes_per_launch"],
+                         "method": "per-pass CUDA events on the engine stream inside the timed region",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                           "4-qubit pass at 26 qubits, x4 to 2^28 amplitudes",
                          "peak_source": peak_kind},
+            "pass_times": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in pass_times.items()},
             "roofline_fp64": {"achieved": fp64_achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                               "frac": (fp64_achieved / fp64_peak) if fp64_peak else None,
                               "peak_source": "measured: cuBLAS DGEMM 8192^3 via torch",
                               "flops_per_step": flops},
             "e2e": {"value": e2e_value, "unit": "GB/s",
                     "h2d_bytes_per_step": len(buf), "d2h_bytes_per_step": (1 << N_QUBITS) * 16,
-                    "ms_per_step": 1e3 * e2e_s},
+                    "ms_per_step": 1e3 * e2e_s,
+                    "call": "B200Simulator.statevector(commands, 28, out=pinned) with default knobs",
+                    "pageable_ms": 1e3 * e2e_pageable_s},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "scale_30q": scale30,
             "adjoint": adj,
             "k_sweep_28q": sweep_k,
             "heisenberg31_c64_bulk": heis,
@@ -602,8 +669,6 @@ def b200_arm(args, rank, world, local_rank):
             "trajectories": traj,
             "plain_12q_latency": plain12,
         }
-    else:
-        reg.close()
     return result
 
 
@@ -620,6 +685,7 @@ def main():
     ap.add_argument("--skip-ksweep", action="store_true")
     ap.add_argument("--skip-structured", action="store_true")
     ap.add_argument("--skip-trajectories", action="store_true")
+    ap.add_argument("--skip-scale", action="store_true")
     ap.add_argument("--executor", type=int, default=None, choices=[0, 1],
                     help="pin the executor (0 stream, 1 tiled) instead of autotuning; needs --k")
     ap.add_argument("--k", type=int, default=None, help="pin the fusion width; needs --executor")

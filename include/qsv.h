@@ -340,6 +340,28 @@ QSV_API int qsv_transition_static(const void* d_bra, const void* d_ket, int n_qu
 QSV_API int qsv_synchronize(void* h);
 QSV_API int qsv_stats(void* h, qsv_stats_t* out);
 
+/* Name, compute capability and SM count of a CUDA device (keys of the engine's autotuning
+ * cache).  No reference counterpart. */
+QSV_API int qsv_device_info(int device, char* name, size_t cap, int* cc_major, int* cc_minor,
+                            int* sm_count);
+
+/* ---- per-pass device timing ---------------------------------------------------------- *
+ * No reference counterpart (the reference times nothing below a whole call).  With timing on,
+ * every gate pass the handle launches (stream passes, tile passes, the single-CTA small-register
+ * pass) is bracketed by a pair of CUDA events on the handle's stream; qsv_pass_times waits for
+ * them and returns per-class totals since timing was switched on: class label ("dense4",
+ * "diag", "pauli_rot", "tile_rt", "tile_pass", "fs_apply", ...), launches, algorithmic HBM
+ * bytes (one read + one write of every amplitude a pass touches) and device milliseconds.
+ * qsv_set_timing clears the totals.  Up to `cap` entries are written; *n_out = the count. */
+typedef struct qsv_pass_time_t {
+    char     label[24];
+    uint64_t launches;
+    uint64_t bytes;
+    double   ms;
+} qsv_pass_time_t;
+QSV_API int qsv_set_timing(void* h, int on);
+QSV_API int qsv_pass_times(void* h, qsv_pass_time_t* out, int cap, int* n_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,10 @@ QSV_OK, QSV_EINVAL, QSV_ERUNTIME, QSV_ECAPABILITY, QSV_ECUDA, QSV_ENOMEM = range
 QSV_C128, QSV_C64 = 0, 1
 
 
+class PassTime(ctypes.Structure):
+    _fields_ = [("label", ctypes.c_char * 24), ("launches", c_uint64), ("bytes", c_uint64), ("ms", c_double)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("launches", c_uint64), ("passes", c_uint64), ("hbm_bytes", c_uint64),
                 ("fused_blocks", c_uint64), ("last_apply_ms", c_double)]
@@ -72,6 +76,9 @@ def _load():
         "qsv_inner": (c_int, [c_void_p, c_void_p, PD]),
         "qsv_synchronize": (c_int, [c_void_p]),
         "qsv_stats": (c_int, [c_void_p, POINTER(Stats)]),
+        "qsv_device_info": (c_int, [c_int, c_char_p, c_size_t, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+        "qsv_set_timing": (c_int, [c_void_p, c_int]),
+        "qsv_pass_times": (c_int, [c_void_p, POINTER(PassTime), c_int, POINTER(c_int)]),
         "qsv_qaoa_create": (c_int, [c_int, c_int, PI32, PI32, PI32, PI32, POINTER(c_void_p)]),
         "qsv_qaoa_run": (c_int, [c_void_p, PD, c_int, PD, PD, PD]),
         "qsv_qaoa_destroy": (c_int, [c_void_p]),
@@ -92,7 +99,8 @@ DECLARED = (
     "qsv_set_executor", "qsv_set_tile_qubits", "qsv_set_checkpoint_interval", "qsv_reset", "qsv_set_state", "qsv_get_state", "qsv_device_state",
     "qsv_copy_state", "qsv_fuse_count", "qsv_fuse_plan", "qsv_tile_plan_count", "qsv_apply", "qsv_apply_unfused", "qsv_transition", "qsv_sample",
     "qsv_sample_seeded", "qsv_uniforms", "qsv_sample_parities", "qsv_exact_probs", "qsv_set_noise", "qsv_set_trajectory_batch", "qsv_run_trajectories", "qsv_adjoint", "qsv_adjoint_phi", "qsv_norm2",
-    "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_transition_static",
+    "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_device_info", "qsv_set_timing",
+    "qsv_pass_times", "qsv_transition_static",
     "qsv_qaoa_create", "qsv_qaoa_run", "qsv_qaoa_destroy",
 )
 STATIC_MAX_TERMS = 4096

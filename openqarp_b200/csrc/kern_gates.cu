@@ -515,6 +515,23 @@ void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& 
 template void launch_op<double>(const Op&, double2*, int, cudaStream_t, Workspace&);
 template void launch_op<float>(const Op&, float2*, int, cudaStream_t, Workspace&);
 
+const char* op_label(const Op& op) {
+    static const char* const dense[] = {"dense0", "dense1", "dense2", "dense3", "dense4", "dense5", "dense6",
+                                        "dense7", "dense8", "dense9", "dense10", "dense11", "dense12"};
+    switch (op.kind) {
+        case OP_DENSE: return op.ctrl ? "dense_ctrl" : (op.k >= 0 && op.k <= 12 ? dense[op.k] : "dense");
+        case OP_DIAG: return "diag";
+        case OP_PHASE: return "phase";
+        case OP_CTRL1: return "ctrl1";
+        case OP_SWAP: return "swap";
+        case OP_PAULI_ROT: return "pauli_rot";
+        case OP_SCALE: return "scale";
+        case OP_PERM: return "perm";
+        case OP_ADJ: return "adj";
+        default: return "nop";
+    }
+}
+
 // algorithmic HBM bytes of one op (read + write of every amplitude it touches)
 uint64_t op_bytes(const Op& op, int n, int amp_bytes) {
     const uint64_t dim = 1ull << n;

@@ -20,6 +20,68 @@ namespace qsv {
 
 // ---------------------------------------------------------------- workspace
 
+PassTimer::~PassTimer() {
+    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+}
+
+void PassTimer::enable(bool on) {
+    on_ = on;
+    pending_.clear();
+    totals_.clear();
+    used_ = 0;
+}
+
+cudaEvent_t PassTimer::event(size_t i) {
+    while (pool_.size() <= i) {
+        cudaEvent_t e = nullptr;
+        check_cuda(cudaEventCreate(&e), "timing event");
+        pool_.push_back(e);
+    }
+    return pool_[i];
+}
+
+void PassTimer::begin(cudaStream_t st, const char* label, uint64_t bytes) {
+    if (!on_) return;
+    // a long timed region folds what it has recorded so far before reusing the events
+    if (used_ + 2 > kMaxPending) collect();
+    check_cuda(cudaEventRecord(event(used_), st), "timing event");
+    pending_.push_back(Rec{used_, label, bytes});
+    used_ += 2;
+}
+
+void PassTimer::end(cudaStream_t st) {
+    if (!on_ || pending_.empty()) return;
+    check_cuda(cudaEventRecord(event(pending_.back().ev + 1), st), "timing event");
+}
+
+void PassTimer::cancel() {
+    if (!on_ || pending_.empty()) return;
+    used_ = pending_.back().ev;
+    pending_.pop_back();
+}
+
+const std::vector<PassTimer::Total>& PassTimer::collect() {
+    for (const Rec& r : pending_) {
+        check_cuda(cudaEventSynchronize(pool_[r.ev + 1]), "timing event");
+        float ms = 0;
+        check_cuda(cudaEventElapsedTime(&ms, pool_[r.ev], pool_[r.ev + 1]), "timing event");
+        Total* t = nullptr;
+        for (Total& x : totals_)
+            if (x.label == r.label) { t = &x; break; }
+        if (!t) {
+            totals_.push_back(Total{});
+            t = &totals_.back();
+            t->label = r.label;
+        }
+        t->launches++;
+        t->bytes += r.bytes;
+        t->ms += ms;
+    }
+    pending_.clear();
+    used_ = 0;
+    return totals_;
+}
+
 void* Workspace::grow(void*& p, size_t& cap, size_t bytes) {
     if (bytes <= cap && p) return p;
     if (p) cudaFree(p);

@@ -643,8 +643,11 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
             for (const Op& o : p.ops) stream_op(o);
             continue;
         }
+        const uint64_t pass_bytes = 2ull * (1ull << n) * sizeof(vec2_t<T>);
         if (rt_idx[i] >= 0) {
+            ws.timer.begin(st, "tile_rt", pass_bytes);
             launch_rt<T>(rt, rt_idx[i], s, n, st);
+            ws.timer.end(st);
             continue;
         }
         const int m = static_cast<int>(p.tile_qubits.size());
@@ -654,8 +657,10 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
                                         static_cast<int>(smem)), "tile smem");
         const uint64_t n_tiles = 1ull << (n - m);
         const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sms));
+        ws.timer.begin(st, "tile_pass", pass_bytes);
         k_tile_pass<T><<<static_cast<unsigned>(grid), kTileThreads, smem, st>>>(s, n, d_p, pi, d_o, d_c);
         check_cuda(cudaGetLastError(), "tile pass launch");
+        ws.timer.end(st);
         ++pi;
     }
     // `host` is pageable: cudaMemcpyAsync returned only after staging it, so it may go now

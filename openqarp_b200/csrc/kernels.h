@@ -24,6 +24,36 @@ inline void check_cuda(cudaError_t e, const char* what) {
         throw cuda_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Device time of a handle's passes, by pass class: when enabled, every pass launch is
+// bracketed by a pair of CUDA events recorded on the handle's stream; collect() waits for
+// them and folds the durations into per-class totals.  Labels are string literals.
+class PassTimer {
+public:
+    struct Total {
+        const char* label = "";
+        uint64_t launches = 0;
+        uint64_t bytes = 0;    // algorithmic HBM bytes of those launches
+        double ms = 0;
+    };
+    ~PassTimer();
+    void enable(bool on);                  // clears the totals
+    bool enabled() const { return on_; }
+    void begin(cudaStream_t st, const char* label, uint64_t bytes);
+    void end(cudaStream_t st);
+    void cancel();                         // drop the last begin (the pass did not launch)
+    const std::vector<Total>& collect();   // waits for the recorded events
+
+private:
+    static constexpr size_t kMaxPending = 8192;   // events in flight before a fold
+    struct Rec { size_t ev; const char* label; uint64_t bytes; };
+    cudaEvent_t event(size_t i);
+    bool on_ = false;
+    std::vector<cudaEvent_t> pool_;
+    std::vector<Rec> pending_;
+    std::vector<Total> totals_;
+    size_t used_ = 0;
+};
+
 // Device scratch owned by a handle; grows on demand, freed with the handle.
 class Workspace {
 public:
@@ -46,6 +76,7 @@ public:
     // device int the tensor-core kernels set when a bounded wait gives up; zero at allocation
     int* tensor_flag();
     bool tensor_pending = false;   // a tensor-core pass ran since the flag was last checked
+    PassTimer timer;               // per-pass device times (qsv_set_timing)
 
 private:
     static void* grow(void*& p, size_t& cap, size_t bytes);
@@ -66,6 +97,9 @@ private:
 template <typename T>
 void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
 uint64_t op_bytes(const Op& op, int n, int amp_bytes);
+// Pass class of an op for the pass timer: "dense1".."dense12" (controlled dense blocks as
+// "dense_ctrl"), "diag", "phase", "ctrl1", "swap", "pauli_rot", "scale", "perm", "adj".
+const char* op_label(const Op& op);
 // Permutation op (kern_gates.cu): through the workspace copy, register address unchanged.
 template <typename T>
 void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);

@@ -111,11 +111,13 @@ void* aux_state(Handle* h) {
 }
 
 void launch(Handle* h, const Op& op, void* target) {
+    if (op.kind != OP_NOP) h->ws.timer.begin(h->stream, op_label(op), op_bytes(op, h->n, static_cast<int>(h->amp_bytes())));
     if (h->dtype == QSV_C128)
         launch_op<double>(op, static_cast<double2*>(target), h->n, h->stream, h->ws);
     else
         launch_op<float>(op, static_cast<float2*>(target), h->n, h->stream, h->ws);
     check_cuda(cudaGetLastError(), "gate launch");
+    if (op.kind != OP_NOP) h->ws.timer.end(h->stream);
     if (op.kind != OP_NOP) {
         h->stats.launches++;
         h->stats.passes++;
@@ -173,16 +175,22 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
             for (const Op& o : p.ops)
                 if (o.kind == OP_DENSE && o.k >= 2) h->stats.fused_blocks++;
         }
-    } else if (h->dtype == QSV_C128 ? apply_ops_small<double>(ops, S128(h), h->n, h->stream, h->ws)
-                                    : apply_ops_small<float>(ops, S64(h), h->n, h->stream, h->ws)) {
-        // a register of at most 64 KiB: the whole sequence in one launch, in shared memory
-        h->stats.launches++;
-        h->stats.passes += ops.size();
-        h->stats.hbm_bytes += 2ull * h->dim() * h->amp_bytes();
-        for (const Op& o : ops)
-            if (o.kind == OP_DENSE && o.k >= 2) h->stats.fused_blocks++;
     } else {
-        for (const Op& o : ops) launch(h, o, h->state);
+        h->ws.timer.begin(h->stream, "fs_apply", 2ull * h->dim() * h->amp_bytes());
+        const bool small = h->dtype == QSV_C128 ? apply_ops_small<double>(ops, S128(h), h->n, h->stream, h->ws)
+                                                : apply_ops_small<float>(ops, S64(h), h->n, h->stream, h->ws);
+        if (small) {
+            // a register of at most 64 KiB: the whole sequence in one launch, in shared memory
+            h->ws.timer.end(h->stream);
+            h->stats.launches++;
+            h->stats.passes += ops.size();
+            h->stats.hbm_bytes += 2ull * h->dim() * h->amp_bytes();
+            for (const Op& o : ops)
+                if (o.kind == OP_DENSE && o.k >= 2) h->stats.fused_blocks++;
+        } else {
+            h->ws.timer.cancel();
+            for (const Op& o : ops) launch(h, o, h->state);
+        }
     }
     check_cuda(cudaEventRecord(h->e1, h->stream), "event");
     check_tensor_flag(h->ws, h->stream);
@@ -743,6 +751,44 @@ int qsv_synchronize(void* hp) {
     return guarded([&] {
         Handle* h = H_(hp);
         check_cuda(cudaStreamSynchronize(h->stream), "synchronize");
+    });
+}
+
+int qsv_device_info(int device, char* name, size_t cap, int* cc_major, int* cc_minor, int* sm_count) {
+    return guarded([&] {
+        cudaDeviceProp p{};
+        check_cuda(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
+        if (name && cap) {
+            std::strncpy(name, p.name, cap - 1);
+            name[cap - 1] = '\0';
+        }
+        if (cc_major) *cc_major = p.major;
+        if (cc_minor) *cc_minor = p.minor;
+        if (sm_count) *sm_count = p.multiProcessorCount;
+    });
+}
+
+int qsv_set_timing(void* hp, int on) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        h->ws.timer.enable(on != 0);
+    });
+}
+
+int qsv_pass_times(void* hp, qsv_pass_time_t* out, int cap, int* n_out) {
+    return guarded([&] {
+        Handle* h = H_(hp);
+        if (!n_out || (cap > 0 && !out)) throw std::invalid_argument("null output");
+        const std::vector<PassTimer::Total>& t = h->ws.timer.collect();
+        *n_out = static_cast<int>(t.size());
+        for (int i = 0; i < cap && i < static_cast<int>(t.size()); ++i) {
+            qsv_pass_time_t& o = out[i];
+            std::memset(o.label, 0, sizeof o.label);
+            std::strncpy(o.label, t[i].label, sizeof o.label - 1);
+            o.launches = t[i].launches;
+            o.bytes = t[i].bytes;
+            o.ms = t[i].ms;
+        }
     });
 }
 

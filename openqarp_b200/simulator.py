@@ -143,6 +143,21 @@ class Register:
         check(lib.qsv_stats(self.handle, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in _lib.Stats._fields_}
 
+    def set_timing(self, on: bool = True):
+        """Per-pass device timing: CUDA events around every gate pass on this register's
+        stream, totals by pass class (clears earlier totals)."""
+        check(lib.qsv_set_timing(self.handle, 1 if on else 0))
+
+    def pass_times(self) -> dict:
+        """{pass class: {"launches", "bytes", "ms"}} since timing was switched on (waits for
+        the recorded passes)."""
+        cnt = ctypes.c_int()
+        check(lib.qsv_pass_times(self.handle, None, 0, ctypes.byref(cnt)))
+        arr = (_lib.PassTime * max(cnt.value, 1))()
+        check(lib.qsv_pass_times(self.handle, arr, cnt.value, ctypes.byref(cnt)))
+        return {arr[i].label.decode(): {"launches": int(arr[i].launches), "bytes": int(arr[i].bytes),
+                                        "ms": float(arr[i].ms)} for i in range(cnt.value)}
+
     # sampling ------------------------------------------------------------------------
     def sample(self, u: np.ndarray) -> np.ndarray:
         u = np.ascontiguousarray(np.asarray(u, dtype=np.float64))
@@ -289,15 +304,22 @@ class B200Simulator:
     kDefaultFusionQubits = 3
     kDefaultFusionMinQubits = 12
 
-    def __init__(self, noise_model=None, *, device: int = 0, dtype: str = "complex128"):
+    def __init__(self, noise_model=None, *, device: int = 0, dtype: str = "complex128",
+                 autotune: bool = True):
         if dtype not in _DTYPES:
             raise ValueError(f"dtype must be one of {sorted(_DTYPES)}")
         self._noise_model = None if noise_model is None else as_noise_model(noise_model)
         self.device = int(device)
         self.dtype = dtype
         self._fusion_max = _default_fusion_max()
+        # the plan is the caller's once a width is pinned (QARP_FUSION_MAX_QUBITS, the
+        # fusion_max_qubits setter, or an explicit executor)
+        self._fusion_pinned = os.environ.get("QARP_FUSION_MAX_QUBITS") is not None
         self._fusion_min = self.kDefaultFusionMinQubits
         self.executor = -1
+        self.autotune = bool(autotune)
+        self.last_plan: Optional[dict] = None
+        self._tag: Optional[str] = None
         self._regs: dict[tuple, Register] = {}
 
     # knobs -------------------------------------------------------------------------------
@@ -327,6 +349,7 @@ class B200Simulator:
             raise ValueError(f"QarpSimulator::set_fusion_max_qubits: {k} exceeds the maximum block "
                              f"width {self.kMaxFusionQubits}")
         self._fusion_max = k
+        self._fusion_pinned = True
 
     @property
     def fusion_min_qubits(self) -> int:
@@ -359,6 +382,29 @@ class B200Simulator:
         r.configure(self._fusion_max, self._fusion_min, self.executor)
         return r
 
+    def _tuned(self) -> bool:
+        return self.autotune and not self._fusion_pinned and self.executor == -1
+
+    def _plan_for(self, reg: Register, commands, buf: bytes, seed) -> None:
+        """Configure ``reg`` with the autotuned (executor, fusion width) for this circuit: from
+        the cache, or measured once on the device and stored (autotune.py)."""
+        from . import autotune
+        if not self._tuned() or reg.n < autotune.MIN_TUNED_QUBITS:
+            self.last_plan = {"executor": max(self.executor, 0), "fusion_k": self._fusion_max,
+                              "source": "knobs"}
+            return
+        if self._tag is None:
+            self._tag = autotune.device_tag(self.device)
+        tuner = autotune.default_tuner()
+        key = tuner.key(self._tag, reg.n, reg.dtype, autotune.structure_key(commands))
+        plan = tuner.lookup(key)
+        source = "cache"
+        if plan is None:
+            plan = tuner.tune(key, reg, buf, seed)
+            source = "measured"
+        reg.configure(plan[1], self._fusion_min, plan[0])
+        self.last_plan = {"executor": plan[0], "fusion_k": plan[1], "source": source, "key": key}
+
     def _prepared(self, commands, n_qubits, initial_state, where, values=None) -> Register:
         reg = self.register(n_qubits)
         if initial_state is not None:
@@ -366,10 +412,15 @@ class B200Simulator:
             if a.shape[0] != (1 << n_qubits):
                 raise ValueError(f"QarpSimulator::{where}: initial_state length {a.shape[0]} != "
                                  f"2^n_qubits = {1 << n_qubits}")
-            reg.set_state(a, validate=True)
+
+            def seed():
+                reg.set_state(a, validate=True)
         else:
-            reg.reset()
-        reg.apply(pack(commands, values))
+            seed = reg.reset
+        buf = pack(commands, values).buf
+        self._plan_for(reg, commands, buf, seed)
+        seed()
+        reg.apply(buf)
         return reg
 
     def prepared_register(self, commands, n_qubits, initial_state=None, where="statevector") -> Register:
@@ -394,9 +445,12 @@ class B200Simulator:
         return exact_program_result(self, program, n_qubits, initial_state)
 
     # QarpSimulator surface ---------------------------------------------------------------
-    def statevector(self, commands, n_qubits: int, *, initial_state=None) -> np.ndarray:
+    def statevector(self, commands, n_qubits: int, *, initial_state=None,
+                    out: Optional[np.ndarray] = None) -> np.ndarray:
         """Final amplitudes of ``commands`` from |0...0> (or ``initial_state``)
-        (QarpSimulator::statevector, qarp_simulator.cpp:901-943)."""
+        (QarpSimulator::statevector, qarp_simulator.cpp:901-943).  ``out`` (an engine
+        extension) receives the amplitudes instead of a new array: a contiguous complex128
+        array of length 2^n, e.g. in pinned host memory for a faster copy."""
         commands = list(commands)
         if any(needs_trajectory(c) for c in commands):
             raise RuntimeError(
@@ -404,7 +458,7 @@ class B200Simulator:
                 "classical condition — statevector is not deterministic. Use run() for trajectory "
                 "simulation.")
         self._refuse_noise(_NOISY_STATEVECTOR)
-        return self._prepared(commands, n_qubits, initial_state, "statevector").get_state()
+        return self._prepared(commands, n_qubits, initial_state, "statevector").get_state(out)
 
     def run(self, commands, n_qubits: int, n_shots: int, seed: Optional[int] = None, *,
             initial_state=None) -> SamplingResult:
