@@ -14,7 +14,7 @@ import pytest
 
 from conftest import GOLDEN
 from golden.gen_program_golden import CASES, KIND_CODES, RUN_SEED, RUN_SHOTS, program_specs
-from openqarp_b200 import _lib
+from openqarp_b200 import B200Simulator, _lib
 from openqarp_b200.ir import Command, GateType as G, pack
 from openqarp_b200.program import Program
 
@@ -183,9 +183,12 @@ def test_program_kernels_between_tiled_and_stream_passes(executor, pgold):
 
 
 @pytest.mark.gpu
-def test_large_register_permutation_round_trip(sim):
+def test_large_register_permutation_round_trip():
     """At 24 qubits: a permutation on 20 qubits followed by its inverse restores the state
-    exactly, and the register's device address does not move."""
+    exactly, and the register's device address does not move.  The fusion knobs are fixed, so
+    both programs apply their gates with the same plan (the autotuner may choose different
+    plans for the two structures, which changes the last bits)."""
+    sim = B200Simulator(autotune=False)
     n = 24
     rng = np.random.default_rng(5)
     qs = [int(q) for q in rng.permutation(n)[:20]]
@@ -206,3 +209,4 @@ def test_large_register_permutation_round_trip(sim):
     after = sim.program_statevector(b, n)
     assert sim.register(n).device_pointer()[0] == addr
     assert np.array_equal(before, after)
+    sim.close()
