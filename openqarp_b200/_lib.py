@@ -15,7 +15,9 @@ import numpy as np
 from .errors import CapabilityError, CudaError
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libqsv.so")
+# QSV_LIBRARY loads another build of the same C-ABI (e.g. one compiled with different tile
+# parameters); by default the in-tree build next to this file
+LIB_PATH = os.environ.get("QSV_LIBRARY") or os.path.join(_HERE, "libqsv.so")
 
 QSV_OK, QSV_EINVAL, QSV_ERUNTIME, QSV_ECAPABILITY, QSV_ECUDA, QSV_ENOMEM = range(6)
 QSV_C128, QSV_C64 = 0, 1

@@ -305,7 +305,8 @@ class B200Simulator:
     kDefaultFusionMinQubits = 12
 
     def __init__(self, noise_model=None, *, device: int = 0, dtype: str = "complex128",
-                 autotune: bool = True):
+                 autotune: bool = True, error_report: Optional[str] = None,
+                 renormalize: Optional[bool] = None):
         if dtype not in _DTYPES:
             raise ValueError(f"dtype must be one of {sorted(_DTYPES)}")
         self._noise_model = None if noise_model is None else as_noise_model(noise_model)
@@ -319,6 +320,15 @@ class B200Simulator:
         self.executor = -1
         self.autotune = bool(autotune)
         self.last_plan: Optional[dict] = None
+        # complex64 bulk mode: FP64 renormalisation after each circuit (default on) and an
+        # error report per result (precision.py); "shadow" repeats each call in complex128
+        if error_report not in (None, "bound", "shadow"):
+            raise ValueError("error_report must be None, 'bound' or 'shadow'")
+        self._c64 = _DTYPES[dtype] == _lib.QSV_C64
+        self.error_report = error_report
+        self.renormalize = self._c64 if renormalize is None else bool(renormalize)
+        self.last_error = None
+        self._shadow: Optional["B200Simulator"] = None
         self._tag: Optional[str] = None
         self._regs: dict[tuple, Register] = {}
 
@@ -365,6 +375,53 @@ class B200Simulator:
         for r in self._regs.values():
             r.close()
         self._regs.clear()
+        if self._shadow is not None:
+            self._shadow.close()
+            self._shadow = None
+
+    # complex64 error reports -------------------------------------------------------------
+    def _shadow_sim(self) -> Optional["B200Simulator"]:
+        """The complex128 twin that shadow reports repeat each call on (same knobs)."""
+        if not (self._c64 and self.error_report == "shadow"):
+            return None
+        if self._shadow is None:
+            self._shadow = B200Simulator(self._noise_model, device=self.device, dtype="complex128",
+                                         autotune=self.autotune)
+        sh = self._shadow
+        sh._fusion_max, sh._fusion_min = self._fusion_max, self._fusion_min
+        sh._fusion_pinned, sh.executor = self._fusion_pinned, self.executor
+        return sh
+
+    def _plan_widths(self, buf: bytes, n_qubits: int) -> list:
+        """Widths of the fused commands the register's knobs apply to ``buf``."""
+        from .ir import GateType, unpack
+        k = (self.last_plan or {}).get("fusion_k", self._fusion_max)
+        size = ctypes.c_size_t()
+        check(lib.qsv_fuse_plan(u8ptr(buf), len(buf), n_qubits, int(k), self._fusion_min, None, 0,
+                                ctypes.byref(size)))
+        raw = ctypes.create_string_buffer(max(size.value, 1))
+        check(lib.qsv_fuse_plan(u8ptr(buf), len(buf), n_qubits, int(k), self._fusion_min, raw, size,
+                                ctypes.byref(size)))
+        skip = (GateType.Barrier, GateType.Measure, GateType.GPhase)
+        out = []
+        for c in unpack(raw.raw[:size.value]):
+            qs = getattr(c, "qubits", ()) or getattr(c, "targets", ())
+            if getattr(c, "gate", None) in skip or not qs:
+                continue
+            out.append(len(qs) + (1 if hasattr(c, "control") else 0))
+        return out
+
+    def _state_report(self, reg: Register, buf: bytes, n_qubits: int):
+        """Norm check, FP64 renormalisation and the a-priori bound after a complex64 apply."""
+        from .precision import Complex64Report, plan_bound
+        n2 = reg.norm2()
+        if self.renormalize and n2 > 0:
+            reg.scale(1.0 / np.sqrt(n2))
+        widths = self._plan_widths(buf, n_qubits)
+        stream_tensor = (self.last_plan or {}).get("executor", 0) == 0
+        return Complex64Report(mode=self.error_report or "bound", norm2=n2, norm_drift=abs(n2 - 1.0),
+                               commands=len(widths),
+                               l2_bound=plan_bound(widths, 5 if stream_tensor else None))
 
     # registers ---------------------------------------------------------------------------
     def register(self, n_qubits: int, slot: int = 0) -> Register:
@@ -421,6 +478,7 @@ class B200Simulator:
         self._plan_for(reg, commands, buf, seed)
         seed()
         reg.apply(buf)
+        self.last_error = self._state_report(reg, buf, n_qubits) if self._c64 else None
         return reg
 
     def prepared_register(self, commands, n_qubits, initial_state=None, where="statevector") -> Register:
@@ -458,7 +516,14 @@ class B200Simulator:
                 "classical condition — statevector is not deterministic. Use run() for trajectory "
                 "simulation.")
         self._refuse_noise(_NOISY_STATEVECTOR)
-        return self._prepared(commands, n_qubits, initial_state, "statevector").get_state(out)
+        res = self._prepared(commands, n_qubits, initial_state, "statevector").get_state(out)
+        sh = self._shadow_sim()
+        if sh is not None:
+            from .precision import state_diff
+            rep = self.last_error
+            rep.l2_vs_complex128, rep.max_abs_vs_complex128 = state_diff(
+                res, sh.statevector(commands, n_qubits, initial_state=initial_state))
+        return res
 
     def run(self, commands, n_qubits: int, n_shots: int, seed: Optional[int] = None, *,
             initial_state=None) -> SamplingResult:
@@ -587,7 +652,18 @@ class B200Simulator:
         rb = self.register(n_qubits, slot=1)
         rk.set_state(k, validate=False)
         rb.set_state(b, validate=False)
-        return rb.transition(rk, masks)
+        t = rb.transition(rk, masks)
+        if self._c64:
+            # the inputs are rounded to FP32 on upload: |b~ - b| <= u |b| elementwise
+            from .precision import U_FP32, Complex64Report, h_norm1
+            nb, nk = float(np.linalg.norm(b)), float(np.linalg.norm(k))
+            rep = Complex64Report(mode=self.error_report or "bound",
+                                  value_bound=h_norm1(masks) * (2 * U_FP32 + U_FP32 ** 2) * nb * nk)
+            sh = self._shadow_sim()
+            if sh is not None:
+                rep.value_abs_vs_complex128 = abs(t - sh.transition(bra, ket, n_qubits, observable))
+            self.last_error = rep
+        return t
 
     def expectation(self, commands, n_qubits: int, observable, *, initial_state=None) -> float:
         """Re <psi|H|psi> with psi = circuit(initial or |0...0>), computed on the device
@@ -599,16 +675,44 @@ class B200Simulator:
         self._refuse_noise(_NOISY_STATEVECTOR)
         masks = to_masks(observable, n_qubits)
         reg = self._prepared(commands, n_qubits, initial_state, "statevector")
-        return reg.expectation(masks).real
+        e = reg.expectation(masks).real
+        if self._c64:
+            self._value_report(self.last_error, masks, e,
+                               lambda sh: sh.expectation(commands, n_qubits, observable,
+                                                         initial_state=initial_state))
+        return e
+
+    def _value_report(self, rep, masks, value, shadow_call):
+        from .precision import h_norm1
+        h1 = h_norm1(masks)
+        d = rep.l2_bound
+        rep.value_bound = 2 * h1 * d + h1 * d * d
+        sh = self._shadow_sim()
+        if sh is not None:
+            rep.value_abs_vs_complex128 = abs(value - shadow_call(sh))
 
     def batch_expectation(self, commands, n_qubits: int, observable, param_sets) -> list:
         commands = list(commands)
         self._refuse_noise(_NOISY_STATEVECTOR)
         masks = to_masks(observable, n_qubits)
-        out = []
+        out, reports = [], []
         for values in param_sets:
             reg = self._prepared(commands, n_qubits, None, "statevector", values)
             out.append(reg.expectation(masks).real)
+            if self._c64:
+                self._value_report(self.last_error, masks, out[-1],
+                                   lambda sh, v=values: sh.batch_expectation(commands, n_qubits,
+                                                                             observable, [v])[0])
+                reports.append(self.last_error)
+        if self._c64:
+            from .precision import Complex64Report
+            self.last_error = Complex64Report(
+                mode=self.error_report or "bound", commands=max((r.commands for r in reports), default=0),
+                l2_bound=max((r.l2_bound for r in reports), default=0.0),
+                value_bound=max((r.value_bound for r in reports), default=0.0),
+                value_abs_vs_complex128=(max(r.value_abs_vs_complex128 for r in reports)
+                                         if reports and reports[0].value_abs_vs_complex128 is not None else None),
+                per_set=reports)
         return out
 
     def run_gradient(self, commands, n_qubits: int, observable, params: Mapping[str, float],
@@ -629,6 +733,21 @@ class B200Simulator:
         reg = self.register(n_qubits)
         self._seed(reg, n_qubits, initial_state, "run_gradient")
         energy, grad = reg.adjoint(stream, len(param_order), masks)
+        if self._c64:
+            from .precision import Complex64Report, h_norm1, plan_bound
+            d = plan_bound(self._plan_widths(stream.buf, n_qubits), 5)
+            h1 = h_norm1(masks)
+            rep = Complex64Report(mode=self.error_report or "bound",
+                                  commands=len(self._plan_widths(stream.buf, n_qubits)),
+                                  l2_bound=d, value_bound=2 * h1 * d + h1 * d * d)
+            sh = self._shadow_sim()
+            if sh is not None:
+                e128, g128 = sh.energy_and_gradient(commands, n_qubits, observable, params, param_order,
+                                                    initial_state=initial_state)
+                rep.value_abs_vs_complex128 = abs(energy - e128)
+                rep.grad_max_abs_vs_complex128 = float(np.max(np.abs(np.asarray(grad) - np.asarray(g128)))
+                                                       if len(grad) else 0.0)
+            self.last_error = rep
         return energy, grad
 
     def run_gradient_phi(self, commands, n_qubits: int, phi, params, param_order, *,

@@ -99,3 +99,51 @@ def test_qaoa_batch_against_oracle(restatement):
     np.testing.assert_allclose(e, e_or, atol=1e-10)
     for a, b in zip(g, g_or):
         np.testing.assert_allclose(a, b, atol=1e-10)
+
+
+# ---------------------------------------------------------------- batch_expectation / batch_run
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [8, 14])
+def test_batch_expectation_matches_reference_per_set(reference, n):
+    """B200Simulator.batch_expectation over several parameter sets of one symbolic circuit
+    equals the reference's QarpSimulator::expectation of each substituted circuit
+    (batch_expectation, qarp_simulator.cpp:971-984), at 1e-10."""
+    from openqarp_b200 import B200Simulator
+    cmds, vals, names = circuits.hea(n, 3, seed=n)
+    obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, 40, seed=3, max_weight=3)
+    masks = observable.to_masks(obs, n)
+    rng = np.random.default_rng(1)
+    sets = [dict(zip(names, rng.uniform(0, 2 * np.pi, len(names)))) for _ in range(5)]
+    sim = B200Simulator()
+    try:
+        got = sim.batch_expectation(cmds, n, obs, sets)
+    finally:
+        sim.close()
+    want = [reference.expectation(ir.pack(cmds, s).buf, n, masks) for s in sets]
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-10)
+
+
+@pytest.mark.gpu
+def test_batch_run_seeds_step_per_set(reference):
+    """batch_run draws set i with seed + i (qarp_simulator.cpp:1248-1267): counts identical to
+    the reference's run() per substituted circuit, on the terminal-sampling path and on the
+    trajectory path (a mid-circuit measurement with a conditioned gate)."""
+    from openqarp_b200 import B200Simulator
+    from openqarp_b200.ir import Command, GateType as G
+    n = 6
+    cmds, vals, names = circuits.hea(n, 2, seed=4)
+    terminal = cmds + [Command(G.Measure, (q,), cbits=(q,)) for q in range(n)]
+    mid = (cmds[:n] + [Command(G.Measure, (0,), cbits=(0,))] +
+           [Command(G.X, (1,), condition_bits=(0,), condition_values=(True,))] + cmds[n:] +
+           [Command(G.Measure, (q,), cbits=(q,)) for q in range(n)])
+    rng = np.random.default_rng(2)
+    sets = [dict(zip(names, rng.uniform(0, 2 * np.pi, len(names)))) for _ in range(3)]
+    sim = B200Simulator()
+    try:
+        for stream in (terminal, mid):
+            got = sim.batch_run(stream, n, 500, sets, seed=77)
+            for i, (res, s) in enumerate(zip(got, sets)):
+                assert res.counts == reference.run(ir.pack(stream, s).buf, n, 500, 77 + i)
+    finally:
+        sim.close()
