@@ -67,7 +67,8 @@ MEASURED_TRAFFIC_28Q = {"dense4": 4 * 2092.9e6}
 KERNEL_OF_CLASS = {"dense1": "k_dense_reg<double,1>", "dense2": "k_dense_reg<double,2>",
                    "dense3": "k_dense_reg<double,3>", "dense4": "k_dense_reg<double,4>",
                    "dense5": "k_dense_dmma<double,5>", "dense6": "k_dense_dmma<double,6>",
-                   "tile_rt": "k_tile_rt<double>", "tile_pass": "k_tile_pass<double>"}
+                   "tile_rt": "k_tile_rt<double>", "tile_pass": "k_tile_pass<double>",
+                   "tile_jit": "qsv_jit_0 (register-tile pass compiled for its plan)"}
 
 
 def measured_peaks():

@@ -27,10 +27,12 @@ import threading
 from typing import Optional, Sequence
 
 from ._lib import check, lib
+from .errors import CudaError
 
 # (executor, fusion width): executor 0 = one HBM pass per fused block, 1 = tile passes with
-# 2^12 (complex128) / 2^13 (complex64) amplitude tiles held in registers
-CANDIDATES_C128 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3))
+# 2^12 (complex128) / 2^13 (complex64) amplitude tiles held in registers, 3 = those passes
+# compiled at run time for their own layouts (complex128)
+CANDIDATES_C128 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3), (3, 1), (3, 3))
 CANDIDATES_C64 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3))
 # registers narrower than this run too briefly for a measurement to pay for itself; they use
 # the fixed defaults
@@ -131,7 +133,11 @@ class Autotuner:
                 reg.apply(buf)
                 seed_register()
                 ms = _timed_apply(reg, buf)
-            except MemoryError:
+            except CudaError:
+                raise
+            except (MemoryError, RuntimeError):
+                # a candidate this machine cannot run (no room for its buffers, no run-time
+                # compiler for executor 3) is skipped
                 continue
             times[(executor, k)] = ms
         best = min(times, key=times.get)

@@ -517,14 +517,24 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
 // Encode the passes for the device and launch them in order on `st`.
 template <typename T>
 void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
-               const std::function<void(const Op&)>& stream_op, bool register_tiles) {
-    // passes the register-tile kernel can run go there; the rest use shared-memory ops
+               const std::function<void(const Op&)>& stream_op, bool register_tiles, bool jit) {
+    // compiled passes first (complex128), then the register-tile interpreter, then shared-memory ops
+    JitPlan jp;
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (jit) {
+            std::vector<const TilePass*> cand;
+            for (const TilePass& p : passes) cand.push_back(&p);
+            int device = 0;
+            check_cuda(cudaGetDevice(&device), "device");
+            jp = jit_prepare(cand, n, device);
+        }
+    }
     std::vector<int> rt_idx(passes.size(), -1);
     std::vector<const TilePass*> rt_passes;
-    if (register_tiles) {
+    if (register_tiles || jit) {
         RtPlan probe;
         for (size_t i = 0; i < passes.size(); ++i)
-            if (!passes[i].tile_qubits.empty() && plan_rt(passes[i], &probe)) {
+            if (!passes[i].tile_qubits.empty() && (jp.idx.empty() || jp.idx[i] < 0) && plan_rt(passes[i], &probe)) {
                 rt_idx[i] = static_cast<int>(rt_passes.size());
                 rt_passes.push_back(&passes[i]);
             }
@@ -644,6 +654,14 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
             continue;
         }
         const uint64_t pass_bytes = 2ull * (1ull << n) * sizeof(vec2_t<T>);
+        if constexpr (sizeof(T) == sizeof(double)) {
+            if (!jp.idx.empty() && jp.idx[i] >= 0) {
+                ws.timer.begin(st, "tile_jit", pass_bytes);
+                jit_launch(jp, static_cast<int>(i), reinterpret_cast<double2*>(s), n, st);
+                ws.timer.end(st);
+                continue;
+            }
+        }
         if (rt_idx[i] >= 0) {
             ws.timer.begin(st, "tile_rt", pass_bytes);
             launch_rt<T>(rt, rt_idx[i], s, n, st);
@@ -868,8 +886,8 @@ template void run_adjoint_tiled<float>(const std::vector<Op>&, float2*, float2*,
                                        cudaStream_t, Workspace&, const std::function<void(const Op&)>&, uint64_t*);
 
 template void run_tiled<double>(const std::vector<TilePass>&, double2*, int, cudaStream_t, Workspace&,
-                                const std::function<void(const Op&)>&, bool);
+                                const std::function<void(const Op&)>&, bool, bool);
 template void run_tiled<float>(const std::vector<TilePass>&, float2*, int, cudaStream_t, Workspace&,
-                               const std::function<void(const Op&)>&, bool);
+                               const std::function<void(const Op&)>&, bool, bool);
 
 }  // namespace qsv

@@ -124,9 +124,23 @@ bool apply_ops_small(const std::vector<Op>& ops, vec2_t<T>* s, int n, cudaStream
 // ---------------------------------------------------------------- tiled executor (kern_tile.cu)
 // Launch the planned passes; one-op stream passes (empty tile_qubits) go to `stream_op`.
 // With register_tiles, passes plan_rt accepts run on the register-tile kernel.
+// With jit (complex128), passes the JIT generator handles run as compiled straight-line kernels.
 template <typename T>
 void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws,
-               const std::function<void(const Op&)>& stream_op, bool register_tiles);
+               const std::function<void(const Op&)>& stream_op, bool register_tiles, bool jit = false);
+
+// ---------------------------------------------------------------- JIT register tiles (kern_tile_jit.cu)
+// The register-tile passes of a stream compiled to straight-line kernels (complex128).
+struct JitPlan {
+    std::vector<int> idx;                   // per pass: kernel index, -1 = not compiled
+    std::vector<std::vector<double>> coef;  // per kernel: its coefficients (kernel parameters)
+    std::vector<void*> fns;                 // per kernel: the loaded function (CUfunction)
+};
+JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int device);
+void jit_launch(const JitPlan& plan, int pass, double2* s, int n, cudaStream_t st);
+// host-only helpers for plan inspection and tests (no device work)
+std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int n, size_t* n_kernels);
+std::vector<char> jit_compile_for_test(const std::string& src, int cc_major, int cc_minor);
 
 // The adjoint's reverse sweep in tile passes (kern_tile.cu): `ops` is the reverse stream (the
 // lowered daggers of non-parametric commands and OP_ADJ steps), planned into passes of m tile

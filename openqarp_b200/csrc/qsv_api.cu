@@ -142,7 +142,7 @@ void check_stream(const std::vector<Cmd>& cmds) {
 // least kTileMinQubits qubits.
 bool use_tiled(const Handle* h) {
     if (h->n < kTileMinQubits) return false;
-    return h->executor == 1 || h->executor == 2;
+    return h->executor == 1 || h->executor == 2 || h->executor == 3;
 }
 
 void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse);
@@ -164,8 +164,9 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
                                          : default_tile_qubits(h->n, static_cast<int>(h->amp_bytes()));
         const std::vector<TilePass> passes = plan_tiles(ops, h->n, m);
         auto stream_op = [h](const Op& o) { launch(h, o, h->state); };
-        const bool rt = h->executor == 1;
-        if (h->dtype == QSV_C128) run_tiled<double>(passes, S128(h), h->n, h->stream, h->ws, stream_op, rt);
+        const bool rt = h->executor == 1 || h->executor == 3;
+        const bool jit = h->executor == 3;
+        if (h->dtype == QSV_C128) run_tiled<double>(passes, S128(h), h->n, h->stream, h->ws, stream_op, rt, jit);
         else run_tiled<float>(passes, S64(h), h->n, h->stream, h->ws, stream_op, rt);
         for (const TilePass& p : passes) {
             if (p.tile_qubits.empty()) continue;   // counted by launch()
@@ -356,7 +357,7 @@ int qsv_set_fusion(void* hp, int max_q, int min_q) {
 int qsv_set_executor(void* hp, int mode) {
     return guarded([&] {
         Handle* h = H_(hp);
-        if (mode < -1 || mode > 2) throw std::invalid_argument("executor mode must be -1, 0, 1 or 2");
+        if (mode < -1 || mode > 3) throw std::invalid_argument("executor mode must be -1, 0, 1, 2 or 3");
         h->executor = mode;
     });
 }
@@ -527,6 +528,32 @@ int qsv_tile_plan_count(const uint8_t* cmds, size_t nbytes, int n, int max_q, in
         for (const TilePass& p : plan_tiles(ops, n, m)) (p.tile_qubits.empty() ? st : t)++;
         *tile_passes = t;
         *stream_passes = st;
+    });
+}
+
+int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min_q, int cc_major, int cc_minor,
+                  int32_t* n_passes, int32_t* n_kernels, uint64_t* cubin_bytes) {
+    return guarded([&] {
+        if (!n_passes || !n_kernels || !cubin_bytes) throw std::invalid_argument("null output");
+        if (max_q < 0 || max_q > QSV_MAX_BLOCK_QUBITS) throw std::invalid_argument("fusion width out of range");
+        if (n < kRtQubits || n > QSV_MAX_QUBITS) throw std::invalid_argument("register too narrow for register tiles");
+        std::vector<Op> ops;
+        for (const Cmd& c : fuse_for_dispatch(decode(cmds, nbytes), n, max_q, min_q))
+            for (Op& o : lower(c, n)) ops.push_back(std::move(o));
+        const std::vector<TilePass> passes = plan_tiles(ops, n, kRtQubits);
+        std::vector<const TilePass*> ptrs;
+        for (const TilePass& p : passes) ptrs.push_back(&p);
+        size_t k = 0;
+        const std::string src = jit_source_for_test(ptrs, n, &k);
+        if (const char* dump = std::getenv("QSV_JIT_DUMP")) {
+            if (FILE* f = std::fopen(dump, "w")) {
+                std::fwrite(src.data(), 1, src.size(), f);
+                std::fclose(f);
+            }
+        }
+        *n_passes = static_cast<int32_t>(passes.size());
+        *n_kernels = static_cast<int32_t>(k);
+        *cubin_bytes = k ? jit_compile_for_test(src, cc_major, cc_minor).size() : 0;
     });
 }
 

@@ -53,7 +53,7 @@ def brickwork28(reference):
     return n, buf, psi
 
 
-@pytest.mark.parametrize("executor,k", [(0, 4), (0, 3), (1, 1), (1, 3)])
+@pytest.mark.parametrize("executor,k", [(0, 4), (0, 3), (1, 1), (1, 3), (3, 1), (3, 3)])
 def test_brickwork_28q_depth20_matches_reference(brickwork28, executor, k):
     n, buf, want = brickwork28
     reg = Register(n)

@@ -170,10 +170,12 @@ def mixed_circuits(n):
     }
 
 
-@pytest.mark.parametrize("m,executor", [(10, 2), (11, 2), (12, 2), (12, 1)])
+@pytest.mark.parametrize("m,executor", [(10, 2), (11, 2), (12, 2), (12, 1), (12, 3)])
 def test_tiled_executor_matches_oracle(m, executor, restatement):
     """executor 1: passes on 12-qubit tiles run in registers (k <= 3 blocks), the rest in
-    shared memory; executor 2: every pass in shared memory."""
+    shared memory; executor 2: every pass in shared memory; executor 3: the register-tile
+    passes compiled at run time into straight-line kernels (passes with Pauli rotations stay
+    on the register-tile interpreter)."""
     n = 14
     for name, cmds in mixed_circuits(n).items():
         buf = ir.pack(cmds).buf

@@ -199,3 +199,14 @@ def test_random_regular_graph_is_regular():
             deg[v] += 1
         assert (deg == 3).all()
         assert len(set(edges)) == len(edges)
+
+
+def test_jit_tile_kernels_compile_without_a_gpu():
+    """Executor 3's pass kernels are generated and compiled by NVRTC for sm_100a on the host."""
+    import ctypes
+    n = 16
+    buf = ir.pack(circuits.brickwork(n, 6, seed=3) + circuits.hea(n, 2, seed=1)[0][:0]).buf
+    p, k, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_uint64()
+    _lib.check(_lib.lib.qsv_jit_check(_lib.u8ptr(buf), len(buf), n, 1, 12, 10, 0, ctypes.byref(p),
+                                      ctypes.byref(k), ctypes.byref(b)))
+    assert k.value == p.value > 0 and b.value > 0
