@@ -21,6 +21,8 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -150,21 +152,75 @@ uint32_t reg_local(const RtLayout& L, int r) {
     return i;
 }
 
+// One-qubit unitary as U = D1 R D2: D1 = diag(d1[0], d1[1]) and D2 = diag(d2[0], d2[1]) unit
+// phases, R = [[c, -s], [s, c]] real with c, s >= 0.  From the entries of D1 R D2 —
+// c d1_0 d2_0, -s d1_0 d2_1, s d1_1 d2_0, c d1_1 d2_1 — with one phase fixed to 1 per factor
+// (the larger of c, s keeps its entries' phases exact).
+struct Factor1q {
+    c128 d1[2], d2[2];
+    double c = 1, s = 0;
+};
+
+c128 unit_phase(c128 v) {
+    const double a = std::abs(v);
+    return a > 0 ? v / a : c128(1.0, 0.0);
+}
+
+Factor1q factor_1q(const std::vector<c128>& u) {
+    Factor1q f;
+    double c = std::abs(u[0]), s = std::abs(u[2]);
+    const double r = std::sqrt(c * c + s * s);
+    if (r > 0) { c /= r; s /= r; }
+    f.c = c;
+    f.s = s;
+    if (c >= s) {
+        const c128 P = unit_phase(u[0]);
+        const c128 T = s > 0 ? unit_phase(-u[1]) / P : c128(1.0, 0.0);
+        f.d1[0] = P; f.d1[1] = unit_phase(u[3]) / T;
+        f.d2[0] = c128(1.0, 0.0); f.d2[1] = T;
+    } else {
+        const c128 P = unit_phase(-u[1]);
+        const c128 R = c > 0 ? unit_phase(u[0]) / P : c128(1.0, 0.0);
+        f.d1[0] = P; f.d1[1] = unit_phase(u[2]) / R;
+        f.d2[0] = R; f.d2[1] = c128(1.0, 0.0);
+    }
+    // the factors must reproduce the gate: a planner or rounding surprise becomes a host error
+    const c128 m[4] = {c * f.d1[0] * f.d2[0], -s * f.d1[0] * f.d2[1], s * f.d1[1] * f.d2[0], c * f.d1[1] * f.d2[1]};
+    for (int e = 0; e < 4; ++e)
+        if (std::abs(m[e] - u[e]) > 1e-12 * std::max(1.0, std::abs(u[e])))
+            throw std::logic_error("JIT tiles: one-qubit factorisation does not reproduce the gate");
+    return f;
+}
+
+// Code generator of one pass.  With emit off it only walks the plan, collecting the
+// coefficients and the structural signature (everything the source depends on), so a pass
+// whose kernel is already compiled costs no source generation.
 struct Gen {
+    bool emit = true;
     std::ostringstream o;
     std::vector<double> coef;
-    const uint32_t* tq = nullptr;     // local bit j -> global qubit
+    std::vector<uint64_t> sig;
     int local_of[64];
+    // deferred one-qubit phases per local bit: amplitudes with the bit 0 / 1 owe pend[b][0/1]
+    c128 pend[kRtQubits][2];
+    bool has[kRtQubits] = {};
 
     size_t push(c128 v) {
         coef.push_back(v.real());
         coef.push_back(v.imag());
         return coef.size() - 2;
     }
-    std::string cr(size_t at) { return "P.c[" + std::to_string(at) + "]"; }
-    std::string ci(size_t at) { return "P.c[" + std::to_string(at + 1) + "]"; }
+    static std::string cr(size_t at) { return "P.c[" + std::to_string(at) + "]"; }
+    static std::string ci(size_t at) { return "P.c[" + std::to_string(at + 1) + "]"; }
     static std::string ar(int r) { return "a" + std::to_string(r) + "r"; }
     static std::string ai(int r) { return "a" + std::to_string(r) + "i"; }
+    void mark(uint64_t a, uint64_t b = 0) { sig.push_back(a); sig.push_back(b); }
+    void mark_layout(const RtLayout& L) {
+        uint64_t x = 0, y = 0;
+        std::memcpy(&x, &L, 8);
+        std::memcpy(&y, reinterpret_cast<const uint8_t*>(&L) + 8, sizeof(RtLayout) - 8);
+        mark(x, y);
+    }
 
     // per-thread local index bits of layout L (lane and warp bits), as an expression
     static std::string lfix_expr(const RtLayout& L) {
@@ -176,27 +232,32 @@ struct Gen {
         return e;
     }
 
-    // Runtime part of a condition "all of these local bits are 1" for the bits held by lanes
-    // and warps; the register-slot part is returned as a slot pattern.
-    std::string thread_cond(const RtLayout& L, uint32_t lm, uint32_t* slot_pattern) {
+    // where local bit b lives in layout L: 'r' slot p, 'l' lane bit k, 'w' warp bit k
+    static char place(const RtLayout& L, int b, int* k) {
+        for (int p = 0; p < kRtRegBits; ++p) if (L.reg[p] == b) { *k = p; return 'r'; }
+        for (int j = 0; j < kRtLaneBits; ++j) if (L.lane[j] == b) { *k = j; return 'l'; }
+        for (int j = 0; j < kRtWarpBits; ++j) if (L.warp[j] == b) { *k = j; return 'w'; }
+        throw std::logic_error("JIT tiles: local bit outside the layout");
+    }
+
+    // Runtime part of "all of these local bits are 1" (lane and warp bits); the register-slot
+    // part is returned as a slot pattern.
+    static std::string thread_cond(const RtLayout& L, uint32_t lm, uint32_t* slot_pattern) {
         uint32_t rm = 0;
         std::string c;
         for (int b = 0; b < kRtQubits; ++b) {
             if (!((lm >> b) & 1)) continue;
-            bool done = false;
-            for (int p = 0; p < kRtRegBits && !done; ++p)
-                if (L.reg[p] == b) { rm |= 1u << p; done = true; }
-            for (int k = 0; k < kRtLaneBits && !done; ++k)
-                if (L.lane[k] == b) { c += (c.empty() ? "" : " && ") + std::string("((lane >> ") + std::to_string(k) + ") & 1u)"; done = true; }
-            for (int k = 0; k < kRtWarpBits && !done; ++k)
-                if (L.warp[k] == b) { c += (c.empty() ? "" : " && ") + std::string("((warp >> ") + std::to_string(k) + ") & 1u)"; done = true; }
+            int k = 0;
+            const char w = place(L, b, &k);
+            if (w == 'r') rm |= 1u << k;
+            else c += (c.empty() ? "" : " && ") + std::string(w == 'l' ? "((lane >> " : "((warp >> ") +
+                      std::to_string(k) + ") & 1u)";
         }
         *slot_pattern = rm;
         return c;
     }
 
-    // split a global qubit mask into its local part (tile bits) and the part outside the tile
-    uint32_t split(uint64_t gm, uint64_t* outside) {
+    uint32_t split(uint64_t gm, uint64_t* outside) const {
         uint32_t lm = 0;
         uint64_t out = 0;
         for (int q = 0; q < 64; ++q)
@@ -212,14 +273,106 @@ struct Gen {
         uint64_t outside = 0;
         const uint32_t lm = split(gmask, &outside);
         std::string c = thread_cond(L, lm, rm);
+        mark(lm, outside);
         if (outside) c = "((base & " + hex64(outside) + ") == " + hex64(outside) + ")" + (c.empty() ? "" : " && " + c);
         return c;
     }
 
-    void cmul_into(int r, size_t at) {
+    void cmul_into(int r, const std::string& pr, const std::string& pi) {
         o << "    { const double xr = " << ar(r) << ", xi = " << ai(r) << "; "
-          << ar(r) << " = " << cr(at) << " * xr - " << ci(at) << " * xi; "
-          << ai(r) << " = " << cr(at) << " * xi + " << ci(at) << " * xr; }\n";
+          << ar(r) << " = " << pr << " * xr - " << pi << " * xi; "
+          << ai(r) << " = " << pr << " * xi + " << pi << " * xr; }\n";
+    }
+
+    // apply the deferred phases of the local bits now in register slots: one table over those
+    // slots, one complex multiply per amplitude
+    void flush_slots(const RtLayout& L) {
+        int slots[kRtRegBits], m = 0;
+        for (int p = 0; p < kRtRegBits; ++p)
+            if (has[L.reg[p]]) slots[m++] = p;
+        uint32_t smask = 0;
+        for (int j = 0; j < m; ++j) smask |= 1u << slots[j];
+        mark(0xF1u, smask);
+        if (m == 0) return;
+        const size_t at = coef.size();
+        for (int idx = 0; idx < (1 << m); ++idx) {
+            c128 t(1.0, 0.0);
+            for (int j = 0; j < m; ++j) t *= pend[L.reg[slots[j]]][(idx >> j) & 1];
+            push(t);
+        }
+        for (int j = 0; j < m; ++j) has[L.reg[slots[j]]] = false;
+        if (!emit) return;
+        for (int r = 0; r < kJitAmps; ++r) {
+            int idx = 0;
+            for (int j = 0; j < m; ++j) idx |= ((r >> slots[j]) & 1) << j;
+            cmul_into(r, cr(at + 2 * static_cast<size_t>(idx)), ci(at + 2 * static_cast<size_t>(idx)));
+        }
+    }
+
+    // end of the pass: the deferred phases of lane and warp bits as one factor per thread,
+    // after the slot table
+    void flush_all(const RtLayout& L) {
+        flush_slots(L);
+        std::vector<std::pair<int, size_t>> bits;   // (place code, coefficient offset)
+        uint64_t m = 0;
+        for (int b = 0; b < kRtQubits; ++b) {
+            if (!has[b]) continue;
+            int k = 0;
+            const char w = place(L, b, &k);
+            bits.push_back({(w == 'l' ? 0 : 16) + k, push(pend[b][0])});
+            push(pend[b][1]);
+            m |= 1ull << ((w == 'l' ? 0 : 16) + k);
+            has[b] = false;
+        }
+        mark(0xF2u, m);
+        if (bits.empty() || !emit) return;
+        o << "  { double fr = 1.0, fi = 0.0;\n";
+        for (const auto& [code, at] : bits) {
+            const std::string on = code < 16 ? "((lane >> " + std::to_string(code) + ") & 1u)"
+                                              : "((warp >> " + std::to_string(code - 16) + ") & 1u)";
+            o << "    { const bool on = " << on << "; const double pr = on ? " << cr(at + 2) << " : " << cr(at)
+              << ", pi = on ? " << ci(at + 2) << " : " << ci(at) << "; const double nr = fr * pr - fi * pi;"
+              << " fi = fr * pi + fi * pr; fr = nr; }\n";
+        }
+        for (int r = 0; r < kJitAmps; ++r) cmul_into(r, "fr", "fi");
+        o << "  }\n";
+    }
+
+    // consecutive one-qubit gates on distinct register slots: their D2 factors join the
+    // deferred phases, one table applies them, then the real rotations; D1 is deferred
+    void gate_batch(const std::vector<const RtStep*>& gates, const RtLayout& L, int local_bit_of_slot[]) {
+        std::vector<Factor1q> f;
+        uint32_t smask = 0;
+        for (const RtStep* st : gates) {
+            const int p = st->slot_of[0];
+            const int b = local_bit_of_slot[p];
+            f.push_back(factor_1q(st->op->m));
+            const Factor1q& z = f.back();
+            for (int v = 0; v < 2; ++v) pend[b][v] = (has[b] ? pend[b][v] : c128(1.0, 0.0)) * z.d2[v];
+            has[b] = true;
+            smask |= 1u << p;
+        }
+        mark(0xB0u, smask);
+        flush_slots(L);
+        for (size_t i = 0; i < gates.size(); ++i) {
+            const int p = gates[i]->slot_of[0];
+            const int b = local_bit_of_slot[p];
+            const size_t at = push(c128(f[i].c, f[i].s));
+            pend[b][0] = f[i].d1[0];
+            pend[b][1] = f[i].d1[1];
+            has[b] = true;
+            mark(0xB1u, static_cast<uint64_t>(p));
+            if (!emit) continue;
+            const int B = 1 << p;
+            for (int g = 0; g < kJitAmps; ++g) {
+                if (g & B) continue;
+                const int h = g | B;
+                o << "  { const double c = " << cr(at) << ", s = " << ci(at) << ";\n"
+                  << "    const double x0r = " << ar(g) << ", x0i = " << ai(g) << ", x1r = " << ar(h) << ", x1i = " << ai(h) << ";\n"
+                  << "    " << ar(g) << " = c * x0r - s * x1r; " << ai(g) << " = c * x0i - s * x1i;\n"
+                  << "    " << ar(h) << " = s * x0r + c * x1r; " << ai(h) << " = s * x0i + c * x1i; }\n";
+            }
+        }
     }
 
     void dense(const Op& op, const std::vector<int>& slot_of) {
@@ -227,7 +380,13 @@ struct Gen {
         const size_t at = coef.size();
         for (const c128& v : op.m) push(v);
         uint32_t slots = 0;
-        for (int b = 0; b < k; ++b) slots |= 1u << slot_of[b];
+        uint64_t so = 0;
+        for (int b = 0; b < k; ++b) {
+            slots |= 1u << slot_of[b];
+            so |= static_cast<uint64_t>(slot_of[b]) << (4 * b);
+        }
+        mark(0xD0u + static_cast<uint64_t>(k), so);
+        if (!emit) return;
         for (int g = 0; g < kJitAmps; ++g) {
             if (g & static_cast<int>(slots)) continue;
             std::vector<int> reg(D);
@@ -260,13 +419,16 @@ struct Gen {
         uint32_t rm = 0;
         const std::string c = full_cond(L, op.mask, &rm);
         const bool sign = op.m[0] == c128(-1.0, 0.0);
+        mark(sign ? 0xA1u : 0xA2u, rm);
         if (sign && c.empty()) {
-            for (int r = 0; r < kJitAmps; ++r)
-                if ((static_cast<uint32_t>(r) & rm) == rm) o << "  " << ar(r) << " = -" << ar(r) << "; " << ai(r) << " = -" << ai(r) << ";\n";
+            if (emit)
+                for (int r = 0; r < kJitAmps; ++r)
+                    if ((static_cast<uint32_t>(r) & rm) == rm) o << "  " << ar(r) << " = -" << ar(r) << "; " << ai(r) << " = -" << ai(r) << ";\n";
             return;
         }
         if (sign) {
             // a sign flip under a runtime condition: XOR of the sign bits (integer pipe)
+            if (!emit) return;
             o << "  { const int sm = (" << c << ") ? (int)0x80000000 : 0;\n";
             for (int r = 0; r < kJitAmps; ++r)
                 if ((static_cast<uint32_t>(r) & rm) == rm)
@@ -275,9 +437,10 @@ struct Gen {
             return;
         }
         const size_t at = push(op.m[0]);
+        if (!emit) return;
         o << "  if (" << (c.empty() ? "true" : c) << ") {\n";
         for (int r = 0; r < kJitAmps; ++r)
-            if ((static_cast<uint32_t>(r) & rm) == rm) cmul_into(r, at);
+            if ((static_cast<uint32_t>(r) & rm) == rm) cmul_into(r, cr(at), ci(at));
         o << "  }\n";
     }
 
@@ -286,6 +449,8 @@ struct Gen {
         const std::string c = full_cond(L, op.mask, &rm);
         const size_t at = coef.size();
         for (int e = 0; e < 4; ++e) push(op.m[e]);
+        mark(0xC1u, slots);
+        if (!emit) return;
         const int tb = slots;
         o << "  if (" << (c.empty() ? "true" : c) << ") {\n";
         for (int g = 0; g < kJitAmps; ++g) {
@@ -303,25 +468,27 @@ struct Gen {
     void diag(const Op& op, const RtLayout& L) {
         const size_t at = coef.size();
         for (const c128& v : op.m) push(v);
-        // table index bit b <- qubit op.qubits[b]: slot bits are constants per register, lane,
+        // table index bit b <- qubit op.qubits[b]: slot bits are constants per register; lane,
         // warp and outside bits form a per-thread base index
         std::string thr = "0u";
         std::vector<int> slot_bit(op.k, -1);
+        uint64_t so = 0;
         for (int b = 0; b < op.k; ++b) {
             const int q = static_cast<int>(op.qubits[b]);
+            so = so * 131 + static_cast<uint64_t>(q);
             const int lb = local_of[q];
             if (lb < 0) {
                 thr += " | ((unsigned)((base >> " + std::to_string(q) + ") & 1ull) << " + std::to_string(b) + ")";
                 continue;
             }
-            bool done = false;
-            for (int p = 0; p < kRtRegBits && !done; ++p)
-                if (L.reg[p] == lb) { slot_bit[b] = p; done = true; }
-            for (int k = 0; k < kRtLaneBits && !done; ++k)
-                if (L.lane[k] == lb) { thr += " | (((lane >> " + std::to_string(k) + ") & 1u) << " + std::to_string(b) + ")"; done = true; }
-            for (int k = 0; k < kRtWarpBits && !done; ++k)
-                if (L.warp[k] == lb) { thr += " | (((warp >> " + std::to_string(k) + ") & 1u) << " + std::to_string(b) + ")"; done = true; }
+            int k = 0;
+            const char w = place(L, lb, &k);
+            if (w == 'r') slot_bit[b] = k;
+            else thr += std::string(" | (((") + (w == 'l' ? "lane" : "warp") + " >> " + std::to_string(k) + ") & 1u) << " +
+                        std::to_string(b) + ")";
         }
+        mark(0xE0u + static_cast<uint64_t>(op.k), so);
+        if (!emit) return;
         o << "  { const unsigned di = " << thr << ";\n";
         for (int r = 0; r < kJitAmps; ++r) {
             uint32_t cst = 0;
@@ -336,10 +503,15 @@ struct Gen {
 
     void scale(const Op& op) {
         const size_t at = push(op.m[0]);
-        for (int r = 0; r < kJitAmps; ++r) cmul_into(r, at);
+        mark(0x5Cu);
+        if (!emit) return;
+        for (int r = 0; r < kJitAmps; ++r) cmul_into(r, cr(at), ci(at));
     }
 
     void move_to(const RtLayout& from, const RtLayout& to, bool first) {
+        mark(0x7Au);
+        mark_layout(to);
+        if (!emit) return;
         if (!first) o << "  __syncthreads();\n";
         o << "  { const unsigned sf = swz(" << lfix_expr(from) << ");\n";
         for (int r = 0; r < kJitAmps; ++r)
@@ -370,79 +542,105 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
 }
 )";
 
-// Source of one pass kernel; coefficients appended to `coef`.  Returns false when the pass
-// needs an op the generator does not handle or too many coefficients.
-bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, std::string* src,
-              std::vector<double>* coef) {
+// Walk one pass's plan: coefficients, structural signature and (with emit) the steps' source.
+// Returns false when the pass needs an op the generator does not handle or too many
+// coefficients.
+bool walk_pass(const TilePass& pass, const RtPlan& plan, int n, Gen* g, RtLayout* last) {
     if (!jit_capable(plan)) return false;
-    Gen g;
-    g.tq = pass.tile_qubits.data();
-    for (int q = 0; q < 64; ++q) g.local_of[q] = -1;
-    for (int j = 0; j < kRtQubits; ++j) g.local_of[pass.tile_qubits[j]] = j;
-    std::ostringstream body;
-    std::swap(g.o, body);
+    for (int q = 0; q < 64; ++q) g->local_of[q] = -1;
+    for (int j = 0; j < kRtQubits; ++j) g->local_of[pass.tile_qubits[j]] = j;
+    g->mark(static_cast<uint64_t>(n), 0x715Eu);
+    for (int j = 0; j < kRtQubits; ++j) g->mark(pass.tile_qubits[j]);
+    g->mark_layout(plan.load);
     RtLayout L = plan.load;
     bool first_move = true;
-    for (const RtStep& st : plan.steps) {
+    const size_t ns = plan.steps.size();
+    for (size_t i = 0; i < ns; ++i) {
+        const RtStep& st = plan.steps[i];
         switch (st.kind) {
             case RT_XPOSE:
-                g.move_to(L, st.layout, first_move);
+                g->move_to(L, st.layout, first_move);
                 first_move = false;
                 L = st.layout;
                 break;
-            case RT_RELABEL: L = st.layout; break;
-            case RT_DENSE: g.dense(*st.op, st.slot_of); break;
-            case RT_PHASE: g.phase(*st.op, L); break;
-            case RT_CTRL1: g.ctrl1(*st.op, L, st.slots); break;
-            case RT_DIAG: g.diag(*st.op, L); break;
-            case RT_SCALE: g.scale(*st.op); break;
+            case RT_RELABEL: {
+                // a SWAP renames two local bits; their deferred phases follow the data
+                const int a = g->local_of[st.op->qubits[0]], b = g->local_of[st.op->qubits[1]];
+                std::swap(g->pend[a][0], g->pend[b][0]);
+                std::swap(g->pend[a][1], g->pend[b][1]);
+                std::swap(g->has[a], g->has[b]);
+                g->mark(0x7Bu);
+                g->mark_layout(st.layout);
+                L = st.layout;
+                break;
+            }
+            case RT_DENSE:
+                if (st.op->k == 1) {
+                    std::vector<const RtStep*> batch;
+                    uint32_t used = 0;
+                    size_t j = i;
+                    for (; j < ns && plan.steps[j].kind == RT_DENSE && plan.steps[j].op->k == 1 &&
+                           !((used >> plan.steps[j].slot_of[0]) & 1u); ++j) {
+                        batch.push_back(&plan.steps[j]);
+                        used |= 1u << plan.steps[j].slot_of[0];
+                    }
+                    int bit_of_slot[kRtRegBits];
+                    for (int p = 0; p < kRtRegBits; ++p) bit_of_slot[p] = L.reg[p];
+                    g->gate_batch(batch, L, bit_of_slot);
+                    i = j - 1;
+                } else {
+                    g->flush_slots(L);
+                    g->dense(*st.op, st.slot_of);
+                }
+                break;
+            case RT_PHASE: g->phase(*st.op, L); break;
+            case RT_CTRL1:
+                g->flush_slots(L);
+                g->ctrl1(*st.op, L, st.slots);
+                break;
+            case RT_DIAG: g->diag(*st.op, L); break;
+            case RT_SCALE: g->scale(*st.op); break;
             default: return false;
         }
     }
-    std::swap(g.o, body);
-    if (g.coef.size() > kJitMaxCoefDoubles) return false;
-    const std::string steps = body.str();
-    const size_t nc = std::max<size_t>(g.coef.size(), 1);
+    g->flush_all(L);
+    *last = L;
+    return g->coef.size() <= kJitMaxCoefDoubles;
+}
 
+// Source of one pass kernel (qsv_jit_<idx>) from a walk with emit on.
+std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx, const std::string& steps,
+                        size_t n_coef, const RtLayout& F) {
+    const size_t nc = std::max<size_t>(n_coef, 1);
     // tile base: the bits of t deposited into the non-tile qubit positions, ascending
     std::vector<int> outside;
     uint32_t in_tile[64] = {};
     for (int j = 0; j < kRtQubits; ++j) in_tile[pass.tile_qubits[j]] = 1;
     for (int q = 0; q < n; ++q)
         if (!in_tile[q]) outside.push_back(q);
-    std::string base = "0ull";
-    for (size_t j = 0; j < outside.size();) {
-        size_t e = j;
-        while (e + 1 < outside.size() && outside[e + 1] - static_cast<int>(e + 1) == outside[j] - static_cast<int>(j)) ++e;
-        const uint64_t mask = ((e - j + 1) >= 64 ? ~0ull : ((1ull << (e - j + 1)) - 1)) << j;
-        base += " | ((t & " + hex64(mask) + ") << " + std::to_string(outside[j] - static_cast<int>(j)) + ")";
-        j = e + 1;
-    }
+    auto deposit = [&](const char* var) {
+        std::string base = "0ull";
+        for (size_t j = 0; j < outside.size();) {
+            size_t e = j;
+            while (e + 1 < outside.size() &&
+                   outside[e + 1] - static_cast<int>(e + 1) == outside[j] - static_cast<int>(j)) ++e;
+            const uint64_t mask = ((e - j + 1) >= 64 ? ~0ull : ((1ull << (e - j + 1)) - 1)) << j;
+            base += std::string(" | ((") + var + " & " + hex64(mask) + ") << " + std::to_string(outside[j] - static_cast<int>(j)) + ")";
+            j = e + 1;
+        }
+        return base;
+    };
     const uint32_t* tq = pass.tile_qubits.data();
     // staging: chunk c = tid + 256 j holds local amplitude c
     std::string gtid = "(u64)(tid & 31u)";
     for (int b = 5; b < 8; ++b)
         gtid += " | ((u64)((tid >> " + std::to_string(b) + ") & 1u) << " + std::to_string(tq[b]) + ")";
     // store: the last layout's lanes are local bits 0..4
-    const RtLayout& F = L;
     std::string gfin = "0ull";
     for (int k = 0; k < kRtLaneBits; ++k)
         gfin += " | ((u64)((lane >> " + std::to_string(k) + ") & 1u) << " + std::to_string(tq[F.lane[k]]) + ")";
     for (int k = 0; k < kRtWarpBits; ++k)
         gfin += " | ((u64)((warp >> " + std::to_string(k) + ") & 1u) << " + std::to_string(tq[F.warp[k]]) + ")";
-
-    std::ostringstream s;
-    s << "struct __align__(8) C" << idx << " { double c[" << nc << "]; };\n"
-      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", 1) qsv_jit_" << idx
-      << "(double2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P) {\n"
-      << "  extern __shared__ __align__(16) unsigned char smem[];\n"
-      << "  double2* xb = reinterpret_cast<double2*>(smem);\n"
-      << "  double2* stage = xb + " << (1 << kRtQubits) << ";\n"
-      << "  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;\n"
-      << "  const u64 gtid = " << gtid << ";\n"
-      << "  const unsigned stid = swz(tid);\n"
-      << "  const u64 gfin = " << gfin << ";\n"
-      << "  u64 t = blockIdx.x;\n";
     auto issue = [&](const std::string& b) {
         std::ostringstream x;
         for (int j = 0; j < (1 << kRtQubits) / kJitThreads; ++j) {
@@ -454,10 +652,22 @@ bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, std::str
         }
         return x.str();
     };
-    s << "  if (t < n_tiles) {\n    const u64 b0 = " << base << ";\n" << issue("b0") << "  }\n"
+    std::ostringstream s;
+    s << "struct __align__(8) C" << idx << " { double c[" << nc << "]; };\n"
+      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", 1) qsv_jit_" << idx
+      << "(double2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P) {\n"
+      << "  extern __shared__ __align__(16) unsigned char smem[];\n"
+      << "  double2* xb = reinterpret_cast<double2*>(smem);\n"
+      << "  double2* stage = xb + " << (1 << kRtQubits) << ";\n"
+      << "  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;\n"
+      << "  const u64 gtid = " << gtid << ";\n"
+      << "  const unsigned stid = swz(tid);\n"
+      << "  const u64 gfin = " << gfin << ";\n"
+      << "  u64 t = blockIdx.x;\n"
+      << "  if (t < n_tiles) {\n    const u64 b0 = " << deposit("t") << ";\n" << issue("b0") << "  }\n"
       << "  asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");\n"
       << "  for (; t < n_tiles; t += gridDim.x) {\n"
-      << "  const u64 base = " << base << ";\n"
+      << "  const u64 base = " << deposit("t") << ";\n"
       << "  asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n"
       << "  __syncthreads();\n"
       << "  double ";
@@ -467,11 +677,8 @@ bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, std::str
         s << "    { const double2 x = stage[sf ^ " << swz(reg_local(plan.load, r)) << "u]; " << Gen::ar(r) << " = x.x; "
           << Gen::ai(r) << " = x.y; }\n";
     s << "  }\n  __syncthreads();\n"
-      << "  if (t + gridDim.x < n_tiles) {\n    const u64 tn = t + gridDim.x;\n    const u64 b1 = ";
-    std::string bn = base;
-    // the same deposit for the next tile index
-    for (size_t pos = bn.find("(t &"); pos != std::string::npos; pos = bn.find("(t &", pos + 1)) bn.replace(pos, 4, "(tn &");
-    s << bn << ";\n" << issue("b1") << "  }\n"
+      << "  if (t + gridDim.x < n_tiles) {\n    const u64 tn = t + gridDim.x;\n    const u64 b1 = " << deposit("tn")
+      << ";\n" << issue("b1") << "  }\n"
       << "  asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");\n"
       << steps;
     for (int r = 0; r < kJitAmps; ++r) {
@@ -481,7 +688,24 @@ bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, std::str
         s << "  __stcs(s + (base | gfin | " << hex64(gc) << "), make_double2(" << Gen::ar(r) << ", " << Gen::ai(r) << "));\n";
     }
     s << "  }\n  asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n}\n";
-    *src = s.str();
+    return s.str();
+}
+
+// Source (with emit) or only the signature and coefficients (without) of one pass.
+bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emit, std::string* src,
+              std::vector<double>* coef, uint64_t* sig_hash) {
+    Gen g;
+    g.emit = emit;
+    RtLayout last{};
+    if (!walk_pass(pass, plan, n, &g, &last)) return false;
+    uint64_t h = 1469598103934665603ull;
+    for (uint64_t v : g.sig)
+        for (int b = 0; b < 8; ++b) {
+            h ^= (v >> (8 * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    *sig_hash = h;
+    if (emit) *src = pass_source(pass, plan, n, idx, g.o.str(), g.coef.size(), last);
     coef->swap(g.coef);
     if (coef->empty()) coef->push_back(0.0);
     return true;
@@ -565,73 +789,82 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
     check_cuda(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "compute capability");
     check_cuda(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device), "compute capability");
     const std::string tag = "// sm_" + std::to_string(major) + std::to_string(minor) + "\n";
-    // one program per pass (kernel qsv_jit_0), so passes compile in parallel and cache alone
-    std::vector<std::string> srcs;
-    std::vector<uint64_t> hashes;
-    for (size_t i = 0; i < passes.size(); ++i) {
-        if (passes[i]->tile_qubits.empty()) continue;
-        RtPlan plan;
-        if (!plan_rt(*passes[i], &plan)) continue;
-        std::string ps;
-        std::vector<double> coef;
-        if (!gen_pass(*passes[i], plan, n, 0, &ps, &coef)) continue;
-        std::string src = std::string(kPrelude) + ps + tag;
-        out.idx[i] = static_cast<int>(srcs.size());
-        hashes.push_back(fnv1a(src));
-        srcs.push_back(std::move(src));
-        out.coef.push_back(std::move(coef));
-    }
-    if (srcs.empty()) return out;
     const Driver& drv = driver();
     CUcontext ctx = nullptr;
     check_cu(drv.current(&ctx), "cuCtxGetCurrent");
+    // walk every pass without emitting source: its signature finds a compiled kernel
+    std::vector<size_t> pass_of;
+    std::vector<uint64_t> sigs;
+    std::vector<RtPlan> plans(passes.size());
+    for (size_t i = 0; i < passes.size(); ++i) {
+        if (passes[i]->tile_qubits.empty()) continue;
+        if (!plan_rt(*passes[i], &plans[i])) continue;
+        std::vector<double> coef;
+        uint64_t sig = 0;
+        std::string unused;
+        if (!gen_pass(*passes[i], plans[i], n, 0, false, &unused, &coef, &sig)) continue;
+        sig ^= (static_cast<uint64_t>(major) << 56) ^ (static_cast<uint64_t>(minor) << 48);
+        out.idx[i] = static_cast<int>(sigs.size());
+        sigs.push_back(sig);
+        pass_of.push_back(i);
+        out.coef.push_back(std::move(coef));
+    }
+    if (sigs.empty()) return out;
     std::lock_guard<std::mutex> lock(g_jit_mu);
     std::vector<size_t> missing;
-    std::vector<std::vector<char>> cubins(srcs.size());
-    for (size_t k = 0; k < srcs.size(); ++k) {
-        if (g_kernels.count({hashes[k], ctx})) continue;
-        char name[40];
-        std::snprintf(name, sizeof name, "%016llx.cubin", static_cast<unsigned long long>(hashes[k]));
-        cubins[k] = read_file(cache_dir() + "/" + name);
-        if (cubins[k].empty()) missing.push_back(k);
-    }
+    for (size_t k = 0; k < sigs.size(); ++k)
+        if (!g_kernels.count({sigs[k], ctx})) missing.push_back(k);
     if (!missing.empty()) {
-        // compile the missing passes on the host cores
-        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        std::vector<std::thread> pool;
-        std::vector<std::string> errors(missing.size());
-        std::atomic<size_t> next{0};
-        for (unsigned w = 0; w < std::min<size_t>(hw, missing.size()); ++w)
-            pool.emplace_back([&] {
-                for (size_t j = next++; j < missing.size(); j = next++) {
-                    try {
-                        cubins[missing[j]] = compile_cubin(srcs[missing[j]], major, minor);
-                    } catch (const std::exception& e) {
-                        errors[j] = e.what();
-                    }
-                }
-            });
-        for (std::thread& t : pool) t.join();
-        for (const std::string& e : errors)
-            if (!e.empty()) throw std::runtime_error(e);
-        for (size_t k : missing) {
+        // sources of the missing passes; their cubins from the disk cache or compiled on the
+        // host cores in parallel
+        std::vector<std::string> srcs(missing.size());
+        std::vector<std::string> files(missing.size());
+        std::vector<std::vector<char>> cubins(missing.size());
+        std::vector<size_t> todo;
+        for (size_t j = 0; j < missing.size(); ++j) {
+            const size_t i = pass_of[missing[j]];
+            std::vector<double> coef;
+            uint64_t sig = 0;
+            gen_pass(*passes[i], plans[i], n, 0, true, &srcs[j], &coef, &sig);
+            srcs[j] = std::string(kPrelude) + srcs[j] + tag;
             char name[40];
-            std::snprintf(name, sizeof name, "%016llx.cubin", static_cast<unsigned long long>(hashes[k]));
-            write_file(cache_dir() + "/" + name, cubins[k]);
+            std::snprintf(name, sizeof name, "%016llx.cubin", static_cast<unsigned long long>(fnv1a(srcs[j])));
+            files[j] = cache_dir() + "/" + name;
+            cubins[j] = read_file(files[j]);
+            if (cubins[j].empty()) todo.push_back(j);
+        }
+        if (!todo.empty()) {
+            const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+            std::vector<std::thread> pool;
+            std::vector<std::string> errors(todo.size());
+            std::atomic<size_t> next{0};
+            for (unsigned w = 0; w < std::min<size_t>(hw, todo.size()); ++w)
+                pool.emplace_back([&] {
+                    for (size_t t = next++; t < todo.size(); t = next++) {
+                        try {
+                            cubins[todo[t]] = compile_cubin(srcs[todo[t]], major, minor);
+                        } catch (const std::exception& e) {
+                            errors[t] = e.what();
+                        }
+                    }
+                });
+            for (std::thread& t : pool) t.join();
+            for (const std::string& e : errors)
+                if (!e.empty()) throw std::runtime_error(e);
+            for (size_t j : todo) write_file(files[j], cubins[j]);
+        }
+        for (size_t j = 0; j < missing.size(); ++j) {
+            CUmodule mod = nullptr;
+            check_cu(drv.load(&mod, cubins[j].data()), "cuModuleLoadData (JIT tiles)");
+            CUfunction f = nullptr;
+            check_cu(drv.get_function(&f, mod, "qsv_jit_0"), "cuModuleGetFunction (JIT tiles)");
+            check_cu(drv.set_attribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
+                                       static_cast<int>(2 * (size_t{1} << kRtQubits) * sizeof(double2))),
+                     "cuFuncSetAttribute (JIT tiles)");
+            g_kernels[{sigs[missing[j]], ctx}] = f;
         }
     }
-    for (size_t k = 0; k < srcs.size(); ++k) {
-        if (g_kernels.count({hashes[k], ctx})) continue;
-        CUmodule mod = nullptr;
-        check_cu(drv.load(&mod, cubins[k].data()), "cuModuleLoadData (JIT tiles)");
-        CUfunction f = nullptr;
-        check_cu(drv.get_function(&f, mod, "qsv_jit_0"), "cuModuleGetFunction (JIT tiles)");
-        check_cu(drv.set_attribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
-                                   static_cast<int>(2 * (size_t{1} << kRtQubits) * sizeof(double2))),
-                 "cuFuncSetAttribute (JIT tiles)");
-        g_kernels[{hashes[k], ctx}] = f;
-    }
-    for (size_t k = 0; k < srcs.size(); ++k) out.fns.push_back(g_kernels[{hashes[k], ctx}]);
+    for (size_t k = 0; k < sigs.size(); ++k) out.fns.push_back(g_kernels[{sigs[k], ctx}]);
     return out;
 }
 
@@ -659,7 +892,8 @@ std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int 
         if (!plan_rt(*passes[i], &plan)) continue;
         std::string ps;
         std::vector<double> coef;
-        if (!gen_pass(*passes[i], plan, n, next, &ps, &coef)) continue;
+        uint64_t sig = 0;
+        if (!gen_pass(*passes[i], plan, n, next, true, &ps, &coef, &sig)) continue;
         src += ps;
         ++next;
     }
