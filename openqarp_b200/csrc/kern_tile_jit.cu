@@ -339,7 +339,12 @@ struct Gen {
     }
 
     // consecutive one-qubit gates on distinct register slots: their D2 factors join the
-    // deferred phases, one table applies them, then the real rotations; D1 is deferred
+    // deferred phases, one table applies them, then the real rotations; D1 is deferred.
+    // A rotation is divided by its larger entry, so each output component is one FMA:
+    //   c >= s:  R = c [[1, -t], [t, 1]],  t = s / c
+    //   s >  c:  R = s [[u, -1], [1, u]],  u = c / s
+    // the scale (c or s, the same for both basis states) joins the deferred phases, and the
+    // form is a uniform branch on a coefficient, so the kernel does not depend on the angles
     void gate_batch(const std::vector<const RtStep*>& gates, const RtLayout& L, int local_bit_of_slot[]) {
         std::vector<Factor1q> f;
         uint32_t smask = 0;
@@ -357,21 +362,30 @@ struct Gen {
         for (size_t i = 0; i < gates.size(); ++i) {
             const int p = gates[i]->slot_of[0];
             const int b = local_bit_of_slot[p];
-            const size_t at = push(c128(f[i].c, f[i].s));
-            pend[b][0] = f[i].d1[0];
-            pend[b][1] = f[i].d1[1];
+            const bool cos_form = f[i].c >= f[i].s;
+            const double scale = cos_form ? f[i].c : f[i].s;
+            const double ratio = cos_form ? f[i].s / f[i].c : f[i].c / f[i].s;
+            const size_t at = push(c128(ratio, cos_form ? 0.0 : 1.0));
+            pend[b][0] = f[i].d1[0] * scale;
+            pend[b][1] = f[i].d1[1] * scale;
             has[b] = true;
             mark(0xB1u, static_cast<uint64_t>(p));
             if (!emit) continue;
             const int B = 1 << p;
+            std::ostringstream a, bb;
             for (int g = 0; g < kJitAmps; ++g) {
                 if (g & B) continue;
                 const int h = g | B;
-                o << "  { const double c = " << cr(at) << ", s = " << ci(at) << ";\n"
-                  << "    const double x0r = " << ar(g) << ", x0i = " << ai(g) << ", x1r = " << ar(h) << ", x1i = " << ai(h) << ";\n"
-                  << "    " << ar(g) << " = c * x0r - s * x1r; " << ai(g) << " = c * x0i - s * x1i;\n"
-                  << "    " << ar(h) << " = s * x0r + c * x1r; " << ai(h) << " = s * x0i + c * x1i; }\n";
+                const std::string x0r = ar(g), x0i = ai(g), x1r = ar(h), x1i = ai(h);
+                a << "    { const double y0r = " << x0r << ", y0i = " << x0i << "; "
+                  << x0r << " = fma(-t, " << x1r << ", y0r); " << x0i << " = fma(-t, " << x1i << ", y0i); "
+                  << x1r << " = fma(t, y0r, " << x1r << "); " << x1i << " = fma(t, y0i, " << x1i << "); }\n";
+                bb << "    { const double y0r = " << x0r << ", y0i = " << x0i << "; "
+                   << x0r << " = fma(t, y0r, -" << x1r << "); " << x0i << " = fma(t, y0i, -" << x1i << "); "
+                   << x1r << " = fma(t, " << x1r << ", y0r); " << x1i << " = fma(t, " << x1i << ", y0i); }\n";
             }
+            o << "  { const double t = " << cr(at) << ";\n  if (" << ci(at) << " != 0.0) {\n" << bb.str()
+              << "  } else {\n" << a.str() << "  } }\n";
         }
     }
 
