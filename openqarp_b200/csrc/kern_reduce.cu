@@ -347,12 +347,14 @@ __global__ void __launch_bounds__(kRed) k_inner(const vec2_t<TA>* __restrict__ a
 }
 
 template <typename T>
-__global__ void k_scale_real(vec2_t<T>* __restrict__ s, uint64_t dim, T f) {
+// the product is formed in FP64 and rounded once to the storage type: a renormalising factor
+// within 1e-8 of 1 would vanish if it were itself rounded to FP32 first
+__global__ void k_scale_real(vec2_t<T>* __restrict__ s, uint64_t dim, double f) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
         vec2_t<T> a = s[i];
-        a.x *= f;
-        a.y *= f;
+        a.x = static_cast<T>(static_cast<double>(a.x) * f);
+        a.y = static_cast<T>(static_cast<double>(a.y) * f);
         s[i] = a;
     }
 }
@@ -691,7 +693,7 @@ void inner(const vec2_t<TA>* a, const vec2_t<TB>* b, int n, cudaStream_t st, Wor
 template <typename T>
 void scale_real(vec2_t<T>* s, int n, double f, cudaStream_t st) {
     const uint64_t dim = 1ull << n;
-    k_scale_real<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(s, dim, static_cast<T>(f));
+    k_scale_real<T><<<grid_for(dim, 1, 1u << 20), kThreads, 0, st>>>(s, dim, f);
     check_cuda(cudaGetLastError(), "scale launch");
 }
 
