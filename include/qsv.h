@@ -361,13 +361,17 @@ QSV_API int qsv_device_info(int device, char* name, size_t cap, int* cc_major, i
  * every gate pass the handle launches (stream passes, tile passes, the single-CTA small-register
  * pass) is bracketed by a pair of CUDA events on the handle's stream; qsv_pass_times waits for
  * them and returns per-class totals since timing was switched on: class label ("dense4",
- * "diag", "pauli_rot", "tile_rt", "tile_pass", "fs_apply", ...), launches, algorithmic HBM
- * bytes (one read + one write of every amplitude a pass touches) and device milliseconds.
+ * "diag", "pauli_rot", "tile_rt", "tile_pass", "tile_jit", "fs_apply", ...), launches,
+ * algorithmic HBM bytes (one read + one write of every amplitude a pass touches), the
+ * floating-point operations the kernels execute (FMA = 2; for compiled tile passes counted
+ * from their generated code, else the ops' dense-matrix arithmetic, 8 x 2^k per amplitude for a
+ * k-qubit block) and device milliseconds.
  * qsv_set_timing clears the totals.  Up to `cap` entries are written; *n_out = the count. */
 typedef struct qsv_pass_time_t {
     char     label[24];
     uint64_t launches;
     uint64_t bytes;
+    double   flops;
     double   ms;
 } qsv_pass_time_t;
 QSV_API int qsv_set_timing(void* h, int on);

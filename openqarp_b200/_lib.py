@@ -24,7 +24,8 @@ QSV_C128, QSV_C64 = 0, 1
 
 
 class PassTime(ctypes.Structure):
-    _fields_ = [("label", ctypes.c_char * 24), ("launches", c_uint64), ("bytes", c_uint64), ("ms", c_double)]
+    _fields_ = [("label", ctypes.c_char * 24), ("launches", c_uint64), ("bytes", c_uint64), ("flops", c_double),
+                ("ms", c_double)]
 
 
 class Stats(ctypes.Structure):

@@ -515,6 +515,17 @@ void launch_perm(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& 
 template void launch_op<double>(const Op&, double2*, int, cudaStream_t, Workspace&);
 template void launch_op<float>(const Op&, float2*, int, cudaStream_t, Workspace&);
 
+double op_flops_per_amp(const Op& op) {
+    switch (op.kind) {
+        case OP_DENSE: return 8.0 * static_cast<double>(1ull << op.k) / static_cast<double>(1ull << __builtin_popcountll(op.ctrl));
+        case OP_DIAG: case OP_SCALE: return 6.0;
+        case OP_PHASE: return 6.0 / static_cast<double>(1ull << __builtin_popcountll(op.mask));
+        case OP_CTRL1: return 16.0 / static_cast<double>(1ull << __builtin_popcountll(op.mask));
+        case OP_PAULI_ROT: return 6.0;
+        default: return 0.0;
+    }
+}
+
 const char* op_label(const Op& op) {
     static const char* const dense[] = {"dense0", "dense1", "dense2", "dense3", "dense4", "dense5", "dense6",
                                         "dense7", "dense8", "dense9", "dense10", "dense11", "dense12"};

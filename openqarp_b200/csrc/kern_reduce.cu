@@ -40,12 +40,12 @@ cudaEvent_t PassTimer::event(size_t i) {
     return pool_[i];
 }
 
-void PassTimer::begin(cudaStream_t st, const char* label, uint64_t bytes) {
+void PassTimer::begin(cudaStream_t st, const char* label, uint64_t bytes, double flops) {
     if (!on_) return;
     // a long timed region folds what it has recorded so far before reusing the events
     if (used_ + 2 > kMaxPending) collect();
     check_cuda(cudaEventRecord(event(used_), st), "timing event");
-    pending_.push_back(Rec{used_, label, bytes});
+    pending_.push_back(Rec{used_, label, bytes, flops});
     used_ += 2;
 }
 
@@ -75,6 +75,7 @@ const std::vector<PassTimer::Total>& PassTimer::collect() {
         }
         t->launches++;
         t->bytes += r.bytes;
+        t->flops += r.flops;
         t->ms += ms;
     }
     pending_.clear();

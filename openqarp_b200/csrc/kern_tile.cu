@@ -654,16 +654,20 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
             continue;
         }
         const uint64_t pass_bytes = 2ull * (1ull << n) * sizeof(vec2_t<T>);
+        double pass_flops = 0;
+        for (const Op& o : p.ops) pass_flops += op_flops_per_amp(o);
+        pass_flops *= static_cast<double>(1ull << n);
         if constexpr (sizeof(T) == sizeof(double)) {
             if (!jp.idx.empty() && jp.idx[i] >= 0) {
-                ws.timer.begin(st, "tile_jit", pass_bytes);
+                ws.timer.begin(st, "tile_jit", pass_bytes,
+                               jp.flops_per_amp[static_cast<size_t>(jp.idx[i])] * static_cast<double>(1ull << n));
                 jit_launch(jp, static_cast<int>(i), reinterpret_cast<double2*>(s), n, st);
                 ws.timer.end(st);
                 continue;
             }
         }
         if (rt_idx[i] >= 0) {
-            ws.timer.begin(st, "tile_rt", pass_bytes);
+            ws.timer.begin(st, "tile_rt", pass_bytes, pass_flops);
             launch_rt<T>(rt, rt_idx[i], s, n, st);
             ws.timer.end(st);
             continue;
@@ -675,7 +679,7 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
                                         static_cast<int>(smem)), "tile smem");
         const uint64_t n_tiles = 1ull << (n - m);
         const uint64_t grid = std::min<uint64_t>(n_tiles, static_cast<uint64_t>(sms));
-        ws.timer.begin(st, "tile_pass", pass_bytes);
+        ws.timer.begin(st, "tile_pass", pass_bytes, pass_flops);
         k_tile_pass<T><<<static_cast<unsigned>(grid), kTileThreads, smem, st>>>(s, n, d_p, pi, d_o, d_c);
         check_cuda(cudaGetLastError(), "tile pass launch");
         ws.timer.end(st);

@@ -204,6 +204,7 @@ struct Gen {
     // deferred one-qubit phases per local bit: amplitudes with the bit 0 / 1 owe pend[b][0/1]
     c128 pend[kRtQubits][2];
     bool has[kRtQubits] = {};
+    double flops = 0;   // FP64 operations per thread per tile (FMA = 2, MUL = 1)
 
     size_t push(c128 v) {
         coef.push_back(v.real());
@@ -301,6 +302,7 @@ struct Gen {
             push(t);
         }
         for (int j = 0; j < m; ++j) has[L.reg[slots[j]]] = false;
+        flops += 6.0 * kJitAmps;
         if (!emit) return;
         for (int r = 0; r < kJitAmps; ++r) {
             int idx = 0;
@@ -325,6 +327,7 @@ struct Gen {
             has[b] = false;
         }
         mark(0xF2u, m);
+        if (!bits.empty()) flops += 6.0 * kJitAmps + 6.0 * static_cast<double>(bits.size());
         if (bits.empty() || !emit) return;
         o << "  { double fr = 1.0, fi = 0.0;\n";
         for (const auto& [code, at] : bits) {
@@ -384,6 +387,7 @@ struct Gen {
                    << x0r << " = fma(t, y0r, -" << x1r << "); " << x0i << " = fma(t, y0i, -" << x1i << "); "
                    << x1r << " = fma(t, " << x1r << ", y0r); " << x1i << " = fma(t, " << x1i << ", y0i); }\n";
             }
+            flops += 8.0 * (kJitAmps / 2);
             o << "  { const double t = " << cr(at) << ";\n  if (" << ci(at) << " != 0.0) {\n" << bb.str()
               << "  } else {\n" << a.str() << "  } }\n";
         }
@@ -400,6 +404,7 @@ struct Gen {
             so |= static_cast<uint64_t>(slot_of[b]) << (4 * b);
         }
         mark(0xD0u + static_cast<uint64_t>(k), so);
+        flops += static_cast<double>(kJitAmps / D) * D * D * 8.0;
         if (!emit) return;
         for (int g = 0; g < kJitAmps; ++g) {
             if (g & static_cast<int>(slots)) continue;
@@ -451,6 +456,7 @@ struct Gen {
             return;
         }
         const size_t at = push(op.m[0]);
+        flops += 6.0 * static_cast<double>(kJitAmps >> __builtin_popcount(rm));
         if (!emit) return;
         o << "  if (" << (c.empty() ? "true" : c) << ") {\n";
         for (int r = 0; r < kJitAmps; ++r)
@@ -464,6 +470,7 @@ struct Gen {
         const size_t at = coef.size();
         for (int e = 0; e < 4; ++e) push(op.m[e]);
         mark(0xC1u, slots);
+        flops += 16.0 * (kJitAmps / 2);
         if (!emit) return;
         const int tb = slots;
         o << "  if (" << (c.empty() ? "true" : c) << ") {\n";
@@ -502,6 +509,7 @@ struct Gen {
                         std::to_string(b) + ")";
         }
         mark(0xE0u + static_cast<uint64_t>(op.k), so);
+        flops += 6.0 * kJitAmps;
         if (!emit) return;
         o << "  { const unsigned di = " << thr << ";\n";
         for (int r = 0; r < kJitAmps; ++r) {
@@ -518,6 +526,7 @@ struct Gen {
     void scale(const Op& op) {
         const size_t at = push(op.m[0]);
         mark(0x5Cu);
+        flops += 6.0 * kJitAmps;
         if (!emit) return;
         for (int r = 0; r < kJitAmps; ++r) cmul_into(r, cr(at), ci(at));
     }
@@ -707,7 +716,7 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
 
 // Source (with emit) or only the signature and coefficients (without) of one pass.
 bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emit, std::string* src,
-              std::vector<double>* coef, uint64_t* sig_hash) {
+              std::vector<double>* coef, uint64_t* sig_hash, double* flops_per_amp = nullptr) {
     Gen g;
     g.emit = emit;
     RtLayout last{};
@@ -719,6 +728,7 @@ bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emi
             h *= 1099511628211ull;
         }
     *sig_hash = h;
+    if (flops_per_amp) *flops_per_amp = g.flops / kJitAmps;
     if (emit) *src = pass_source(pass, plan, n, idx, g.o.str(), g.coef.size(), last);
     coef->swap(g.coef);
     if (coef->empty()) coef->push_back(0.0);
@@ -816,7 +826,9 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
         std::vector<double> coef;
         uint64_t sig = 0;
         std::string unused;
-        if (!gen_pass(*passes[i], plans[i], n, 0, false, &unused, &coef, &sig)) continue;
+        double fpa = 0;
+        if (!gen_pass(*passes[i], plans[i], n, 0, false, &unused, &coef, &sig, &fpa)) continue;
+        out.flops_per_amp.push_back(fpa);
         sig ^= (static_cast<uint64_t>(major) << 56) ^ (static_cast<uint64_t>(minor) << 48);
         out.idx[i] = static_cast<int>(sigs.size());
         sigs.push_back(sig);

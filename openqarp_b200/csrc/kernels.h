@@ -33,19 +33,20 @@ public:
         const char* label = "";
         uint64_t launches = 0;
         uint64_t bytes = 0;    // algorithmic HBM bytes of those launches
+        double flops = 0;      // floating-point operations the launches execute (FMA = 2)
         double ms = 0;
     };
     ~PassTimer();
     void enable(bool on);                  // clears the totals
     bool enabled() const { return on_; }
-    void begin(cudaStream_t st, const char* label, uint64_t bytes);
+    void begin(cudaStream_t st, const char* label, uint64_t bytes, double flops = 0);
     void end(cudaStream_t st);
     void cancel();                         // drop the last begin (the pass did not launch)
     const std::vector<Total>& collect();   // waits for the recorded events
 
 private:
     static constexpr size_t kMaxPending = 8192;   // events in flight before a fold
-    struct Rec { size_t ev; const char* label; uint64_t bytes; };
+    struct Rec { size_t ev; const char* label; uint64_t bytes; double flops; };
     cudaEvent_t event(size_t i);
     bool on_ = false;
     std::vector<cudaEvent_t> pool_;
@@ -97,6 +98,9 @@ private:
 template <typename T>
 void launch_op(const Op& op, vec2_t<T>* s, int n, cudaStream_t st, Workspace& ws);
 uint64_t op_bytes(const Op& op, int n, int amp_bytes);
+// Floating-point operations per amplitude of an op in the stream executor's kernels (a complex
+// multiply-add = 8, FMA = 2): 8 x 2^k for a dense block, 6 for a diagonal factor.
+double op_flops_per_amp(const Op& op);
 // Pass class of an op for the pass timer: "dense1".."dense12" (controlled dense blocks as
 // "dense_ctrl"), "diag", "phase", "ctrl1", "swap", "pauli_rot", "scale", "perm", "adj".
 const char* op_label(const Op& op);
@@ -135,6 +139,7 @@ struct JitPlan {
     std::vector<int> idx;                   // per pass: kernel index, -1 = not compiled
     std::vector<std::vector<double>> coef;  // per kernel: its coefficients (kernel parameters)
     std::vector<void*> fns;                 // per kernel: the loaded function (CUfunction)
+    std::vector<double> flops_per_amp;      // per kernel: FP64 operations per amplitude (FMA = 2)
 };
 JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int device);
 void jit_launch(const JitPlan& plan, int pass, double2* s, int n, cudaStream_t st);

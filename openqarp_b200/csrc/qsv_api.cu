@@ -111,7 +111,9 @@ void* aux_state(Handle* h) {
 }
 
 void launch(Handle* h, const Op& op, void* target) {
-    if (op.kind != OP_NOP) h->ws.timer.begin(h->stream, op_label(op), op_bytes(op, h->n, static_cast<int>(h->amp_bytes())));
+    if (op.kind != OP_NOP)
+        h->ws.timer.begin(h->stream, op_label(op), op_bytes(op, h->n, static_cast<int>(h->amp_bytes())),
+                          op_flops_per_amp(op) * static_cast<double>(h->dim()));
     if (h->dtype == QSV_C128)
         launch_op<double>(op, static_cast<double2*>(target), h->n, h->stream, h->ws);
     else
@@ -814,6 +816,7 @@ int qsv_pass_times(void* hp, qsv_pass_time_t* out, int cap, int* n_out) {
             std::strncpy(o.label, t[i].label, sizeof o.label - 1);
             o.launches = t[i].launches;
             o.bytes = t[i].bytes;
+            o.flops = t[i].flops;
             o.ms = t[i].ms;
         }
     });

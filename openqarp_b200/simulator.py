@@ -156,7 +156,8 @@ class Register:
         arr = (_lib.PassTime * max(cnt.value, 1))()
         check(lib.qsv_pass_times(self.handle, arr, cnt.value, ctypes.byref(cnt)))
         return {arr[i].label.decode(): {"launches": int(arr[i].launches), "bytes": int(arr[i].bytes),
-                                        "ms": float(arr[i].ms)} for i in range(cnt.value)}
+                                        "flops": float(arr[i].flops), "ms": float(arr[i].ms)}
+                for i in range(cnt.value)}
 
     # sampling ------------------------------------------------------------------------
     def sample(self, u: np.ndarray) -> np.ndarray:
