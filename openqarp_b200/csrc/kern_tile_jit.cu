@@ -135,6 +135,8 @@ void check_cu(CUresult r, const char* what) {
 constexpr int kJitAmps = 1 << kRtRegBits;                 // 16 amplitudes per thread
 constexpr int kJitThreads = 1 << (kRtLaneBits + kRtWarpBits);
 constexpr size_t kJitMaxCoefDoubles = 3400;               // kernel parameters stay under 28 KiB
+constexpr int kJitCtasPerSm = 2;                          // 64 KiB of shared memory and <= 128 registers each
+constexpr size_t kJitSmem = (size_t{1} << kRtQubits) * 16;
 
 uint32_t swz(uint32_t i) { return i ^ ((i >> 3 ^ i >> 6 ^ i >> 9) & 7u); }
 
@@ -670,18 +672,17 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
             uint64_t gj = 0;
             for (int b2 = 0; b2 < 4; ++b2)
                 if ((j >> b2) & 1) gj |= 1ull << tq[8 + b2];
-            x << "    cp16(stage + (stid ^ " << swz(static_cast<uint32_t>(j) * kJitThreads) << "u), s + ((" << b
+            x << "    cp16(xb + (stid ^ " << swz(static_cast<uint32_t>(j) * kJitThreads) << "u), s + ((" << b
               << ") | gtid | " << hex64(gj) << "));\n";
         }
         return x.str();
     };
     std::ostringstream s;
     s << "struct __align__(8) C" << idx << " { double c[" << nc << "]; };\n"
-      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", 1) qsv_jit_" << idx
+      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", " << kJitCtasPerSm << ") qsv_jit_" << idx
       << "(double2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P) {\n"
       << "  extern __shared__ __align__(16) unsigned char smem[];\n"
       << "  double2* xb = reinterpret_cast<double2*>(smem);\n"
-      << "  double2* stage = xb + " << (1 << kRtQubits) << ";\n"
       << "  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;\n"
       << "  const u64 gtid = " << gtid << ";\n"
       << "  const unsigned stid = swz(tid);\n"
@@ -697,13 +698,17 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
     for (int r = 0; r < kJitAmps; ++r) s << (r ? ", " : "") << Gen::ar(r) << ", " << Gen::ai(r);
     s << ";\n  { const unsigned sf = swz(" << Gen::lfix_expr(plan.load) << ");\n";
     for (int r = 0; r < kJitAmps; ++r)
-        s << "    { const double2 x = stage[sf ^ " << swz(reg_local(plan.load, r)) << "u]; " << Gen::ar(r) << " = x.x; "
+        s << "    { const double2 x = xb[sf ^ " << swz(reg_local(plan.load, r)) << "u]; " << Gen::ar(r) << " = x.x; "
           << Gen::ai(r) << " = x.y; }\n";
+    // one buffer serves the tile's loads and its transposes: the next tile's copies start once
+    // the last transpose has been read, and run under this tile's stores (and the other CTA
+    // on the SM computes meanwhile)
     s << "  }\n  __syncthreads();\n"
+      << steps
+      << "  __syncthreads();\n"
       << "  if (t + gridDim.x < n_tiles) {\n    const u64 tn = t + gridDim.x;\n    const u64 b1 = " << deposit("tn")
       << ";\n" << issue("b1") << "  }\n"
-      << "  asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");\n"
-      << steps;
+      << "  asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");\n";
     for (int r = 0; r < kJitAmps; ++r) {
         uint64_t gc = 0;
         for (int p = 0; p < kRtRegBits; ++p)
@@ -885,7 +890,7 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
             CUfunction f = nullptr;
             check_cu(drv.get_function(&f, mod, "qsv_jit_0"), "cuModuleGetFunction (JIT tiles)");
             check_cu(drv.set_attribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
-                                       static_cast<int>(2 * (size_t{1} << kRtQubits) * sizeof(double2))),
+                                       static_cast<int>(kJitSmem)),
                      "cuFuncSetAttribute (JIT tiles)");
             g_kernels[{sigs[missing[j]], ctx}] = f;
         }
@@ -901,11 +906,12 @@ void jit_launch(const JitPlan& plan, int pass, double2* s, int n, cudaStream_t s
     check_cuda(cudaGetDevice(&device), "device");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
     unsigned long long n_tiles = 1ull << (n - kRtQubits);
-    const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>(n_tiles, static_cast<unsigned long long>(sms)));
+    const unsigned grid = static_cast<unsigned>(
+        std::min<unsigned long long>(n_tiles, static_cast<unsigned long long>(kJitCtasPerSm) * sms));
     const std::vector<double>& c = plan.coef[static_cast<size_t>(k)];
     void* args[] = {&s, &n_tiles, const_cast<double*>(c.data())};
     check_cu(driver().launch(static_cast<CUfunction>(plan.fns[static_cast<size_t>(k)]), grid, 1, 1, kJitThreads, 1, 1,
-                             static_cast<unsigned>(2 * (size_t{1} << kRtQubits) * sizeof(double2)),
+                             static_cast<unsigned>(kJitSmem),
                              reinterpret_cast<CUstream>(st), args, nullptr),
              "cuLaunchKernel (JIT tiles)");
 }
