@@ -60,10 +60,11 @@ CPU_LAYERS = 4      # host-core sample (the circuit's first layers) of cpu_basel
 ADJ_N, ADJ_LAYERS, ADJ_TERMS = 24, 8, 500
 
 
-# DRAM bytes per launch of the 4-qubit dense pass (k_dense_reg<double,4>): 2092.9 MB captured
-# by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a 26-qubit register, x4 for 2^28
-# amplitudes (traffic grows with the register: one read and one write of every amplitude)
-MEASURED_TRAFFIC_28Q = {"dense4": 4 * 2092.9e6}
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture on a
+# 26-qubit register, x4 for 2^28 amplitudes: traffic grows with the register, one read and one
+# write of every amplitude): the 4-qubit dense pass (k_dense_reg<double,4>) 2092.9 MB, the
+# compiled register-tile pass 2089.4 MB (mean of three launches)
+MEASURED_TRAFFIC_28Q = {"dense4": 4 * 2092.9e6, "tile_jit": 4 * 2089.4e6}
 KERNEL_OF_CLASS = {"dense1": "k_dense_reg<double,1>", "dense2": "k_dense_reg<double,2>",
                    "dense3": "k_dense_reg<double,3>", "dense4": "k_dense_reg<double,4>",
                    "dense5": "k_dense_dmma<double,5>", "dense6": "k_dense_dmma<double,6>",
@@ -649,8 +650,8 @@ def b200_arm(args, rank, world, local_rank):
                          "share_of_pass_time": dom["share_of_pass_time"],
                          "bytes_per_launch": dom["bytes_per_launch"],
                          "method": "per-pass CUDA events on the engine stream inside the timed region",
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
-                                           "4-qubit pass at 26 qubits, x4 to 2^28 amplitudes",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same "
+                                           "pass class at 26 qubits, x4 to 2^28 amplitudes",
                          "peak_source": peak_kind},
             "pass_times": {k: {"launches": v["launches"], "ms": round(v["ms"], 3)} for k, v in pass_times.items()},
             "roofline_fp64": {"achieved": dom["achieved_tflops"], "peak": fp64_peak, "unit": "TFLOP/s",

@@ -151,8 +151,8 @@ QSV_API int qsv_set_fusion(void* h, int max_qubits, int min_qubits);
  * 2^12-amplitude tiles held in registers, with shared-memory transposes between layouts
  * ("tiled"; passes it cannot hold fall back to 2), 2 = several ops per pass applied to tiles
  * staged in shared memory, 3 = executor 1 with each pass compiled at run time (NVRTC) into a
- * straight-line kernel for its own layouts (complex128; a pass it cannot compile, and complex64
- * registers, run as executor 1), -1 = the default (stream). */
+ * straight-line kernel for its own layouts (a pass it cannot compile runs as executor 1),
+ * -1 = the default (stream). */
 QSV_API int qsv_set_executor(void* h, int mode);
 /* Tile width of the tiled executor: qubits held in shared memory per tile, 8..13
  * (0 = the default: 12 for complex128, 13 for complex64).  No reference counterpart: the
@@ -202,11 +202,11 @@ QSV_API int qsv_tile_plan_count(const uint8_t* cmds, size_t nbytes, int n_qubits
                                 int32_t* stream_passes);
 
 /* Host-only (no device work, no GPU needed): the executor-3 kernels of a stream for a register
- * of n_qubits (>= 12) and the given fusion knobs — plans the tile passes, generates their source
- * and compiles it with NVRTC for compute capability cc_major.cc_minor; returns the number of
- * tile passes, of compiled pass kernels and the cubin size.  An engine extension with no
- * reference counterpart (plan inspection and build checks). */
-QSV_API int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n_qubits, int max_qubits,
+ * of n_qubits (>= 12), storage type dtype and the given fusion knobs — plans the tile passes,
+ * generates their source and compiles it with NVRTC for compute capability cc_major.cc_minor;
+ * returns the number of tile passes, of compiled pass kernels and the cubin size.  An engine
+ * extension with no reference counterpart (plan inspection and build checks). */
+QSV_API int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n_qubits, int dtype, int max_qubits,
                           int min_qubits, int cc_major, int cc_minor, int32_t* n_passes,
                           int32_t* n_kernels, uint64_t* cubin_bytes);
 

@@ -60,7 +60,7 @@ def _load():
         "qsv_fuse_count": (c_int, [P8, c_size_t, c_int, c_int, c_int, PI32, PI32]),
         "qsv_fuse_plan": (c_int, [P8, c_size_t, c_int, c_int, c_int, c_void_p, c_size_t, POINTER(c_size_t)]),
         "qsv_tile_plan_count": (c_int, [P8, c_size_t, c_int, c_int, c_int, c_int, PI32, PI32]),
-        "qsv_jit_check": (c_int, [P8, c_size_t, c_int, c_int, c_int, c_int, c_int, PI32, PI32, PU64]),
+        "qsv_jit_check": (c_int, [P8, c_size_t, c_int, c_int, c_int, c_int, c_int, c_int, PI32, PI32, PU64]),
         "qsv_apply": (c_int, [c_void_p, P8, c_size_t]),
         "qsv_apply_unfused": (c_int, [c_void_p, P8, c_size_t]),
         "qsv_transition": (c_int, [c_void_p, c_void_p, PU64, PU64, PD, c_size_t, PD]),

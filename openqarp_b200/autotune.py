@@ -31,9 +31,9 @@ from .errors import CudaError
 
 # (executor, fusion width): executor 0 = one HBM pass per fused block, 1 = tile passes with
 # 2^12 (complex128) / 2^13 (complex64) amplitude tiles held in registers, 3 = those passes
-# compiled at run time for their own layouts (complex128)
+# compiled at run time for their own layouts
 CANDIDATES_C128 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3), (3, 1), (3, 3))
-CANDIDATES_C64 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3))
+CANDIDATES_C64 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3), (3, 1), (3, 3))
 # registers narrower than this run too briefly for a measurement to pay for itself; they use
 # the fixed defaults
 MIN_TUNED_QUBITS = 20

@@ -520,14 +520,12 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
                const std::function<void(const Op&)>& stream_op, bool register_tiles, bool jit) {
     // compiled passes first (complex128), then the register-tile interpreter, then shared-memory ops
     JitPlan jp;
-    if constexpr (sizeof(T) == sizeof(double)) {
-        if (jit) {
-            std::vector<const TilePass*> cand;
-            for (const TilePass& p : passes) cand.push_back(&p);
-            int device = 0;
-            check_cuda(cudaGetDevice(&device), "device");
-            jp = jit_prepare(cand, n, device);
-        }
+    if (jit) {
+        std::vector<const TilePass*> cand;
+        for (const TilePass& p : passes) cand.push_back(&p);
+        int device = 0;
+        check_cuda(cudaGetDevice(&device), "device");
+        jp = jit_prepare(cand, n, device, sizeof(T) == sizeof(float));
     }
     std::vector<int> rt_idx(passes.size(), -1);
     std::vector<const TilePass*> rt_passes;
@@ -657,14 +655,12 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
         double pass_flops = 0;
         for (const Op& o : p.ops) pass_flops += op_flops_per_amp(o);
         pass_flops *= static_cast<double>(1ull << n);
-        if constexpr (sizeof(T) == sizeof(double)) {
-            if (!jp.idx.empty() && jp.idx[i] >= 0) {
-                ws.timer.begin(st, "tile_jit", pass_bytes,
-                               jp.flops_per_amp[static_cast<size_t>(jp.idx[i])] * static_cast<double>(1ull << n));
-                jit_launch(jp, static_cast<int>(i), reinterpret_cast<double2*>(s), n, st);
-                ws.timer.end(st);
-                continue;
-            }
+        if (!jp.idx.empty() && jp.idx[i] >= 0) {
+            ws.timer.begin(st, "tile_jit", pass_bytes,
+                           jp.flops_per_amp[static_cast<size_t>(jp.idx[i])] * static_cast<double>(1ull << n));
+            jit_launch(jp, static_cast<int>(i), s, n, st);
+            ws.timer.end(st);
+            continue;
         }
         if (rt_idx[i] >= 0) {
             ws.timer.begin(st, "tile_rt", pass_bytes, pass_flops);

@@ -15,8 +15,7 @@
 // ~/.cache/openqarp_b200/jit).
 //
 // NVRTC and the CUDA driver API are opened with dlopen on first use, so the library loads
-// (and every other executor runs) where they are absent.  Complex128 only; passes with ops
-// this generator does not handle (Pauli rotations) run on the interpreter kernel.
+// (and every other executor runs) where they are absent.  Complex128 only.
 #include <dlfcn.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -135,8 +134,9 @@ void check_cu(CUresult r, const char* what) {
 constexpr int kJitAmps = 1 << kRtRegBits;                 // 16 amplitudes per thread
 constexpr int kJitThreads = 1 << (kRtLaneBits + kRtWarpBits);
 constexpr size_t kJitMaxCoefDoubles = 3400;               // kernel parameters stay under 28 KiB
-constexpr int kJitCtasPerSm = 2;                          // 64 KiB of shared memory and <= 128 registers each
-constexpr size_t kJitSmem = (size_t{1} << kRtQubits) * 16;
+constexpr int kJitCtasPerSm = 2;                          // complex128: 64 KiB of shared memory, <= 128 registers
+constexpr int kJitCtasPerSmF32 = 2;                       // complex64: 32 KiB, <= 128 registers
+size_t jit_smem(bool f32) { return (size_t{1} << kRtQubits) * (f32 ? 8 : 16); }
 
 uint32_t swz(uint32_t i) { return i ^ ((i >> 3 ^ i >> 6 ^ i >> 9) & 7u); }
 
@@ -282,7 +282,7 @@ struct Gen {
     }
 
     void cmul_into(int r, const std::string& pr, const std::string& pi) {
-        o << "    { const double xr = " << ar(r) << ", xi = " << ai(r) << "; "
+        o << "    { const R xr = " << ar(r) << ", xi = " << ai(r) << "; "
           << ar(r) << " = " << pr << " * xr - " << pi << " * xi; "
           << ai(r) << " = " << pr << " * xi + " << pi << " * xr; }\n";
     }
@@ -331,12 +331,12 @@ struct Gen {
         mark(0xF2u, m);
         if (!bits.empty()) flops += 6.0 * kJitAmps + 6.0 * static_cast<double>(bits.size());
         if (bits.empty() || !emit) return;
-        o << "  { double fr = 1.0, fi = 0.0;\n";
+        o << "  { R fr = 1, fi = 0;\n";
         for (const auto& [code, at] : bits) {
             const std::string on = code < 16 ? "((lane >> " + std::to_string(code) + ") & 1u)"
                                               : "((warp >> " + std::to_string(code - 16) + ") & 1u)";
-            o << "    { const bool on = " << on << "; const double pr = on ? " << cr(at + 2) << " : " << cr(at)
-              << ", pi = on ? " << ci(at + 2) << " : " << ci(at) << "; const double nr = fr * pr - fi * pi;"
+            o << "    { const bool on = " << on << "; const R pr = on ? " << cr(at + 2) << " : " << cr(at)
+              << ", pi = on ? " << ci(at + 2) << " : " << ci(at) << "; const R nr = fr * pr - fi * pi;"
               << " fi = fr * pi + fi * pr; fr = nr; }\n";
         }
         for (int r = 0; r < kJitAmps; ++r) cmul_into(r, "fr", "fi");
@@ -375,6 +375,7 @@ struct Gen {
             pend[b][1] = f[i].d1[1] * scale;
             has[b] = true;
             mark(0xB1u, static_cast<uint64_t>(p));
+            flops += 8.0 * (kJitAmps / 2);
             if (!emit) continue;
             const int B = 1 << p;
             std::ostringstream a, bb;
@@ -382,15 +383,14 @@ struct Gen {
                 if (g & B) continue;
                 const int h = g | B;
                 const std::string x0r = ar(g), x0i = ai(g), x1r = ar(h), x1i = ai(h);
-                a << "    { const double y0r = " << x0r << ", y0i = " << x0i << "; "
-                  << x0r << " = fma(-t, " << x1r << ", y0r); " << x0i << " = fma(-t, " << x1i << ", y0i); "
-                  << x1r << " = fma(t, y0r, " << x1r << "); " << x1i << " = fma(t, y0i, " << x1i << "); }\n";
-                bb << "    { const double y0r = " << x0r << ", y0i = " << x0i << "; "
-                   << x0r << " = fma(t, y0r, -" << x1r << "); " << x0i << " = fma(t, y0i, -" << x1i << "); "
-                   << x1r << " = fma(t, " << x1r << ", y0r); " << x1i << " = fma(t, " << x1i << ", y0i); }\n";
+                a << "    { const R y0r = " << x0r << ", y0i = " << x0i << "; "
+                  << x0r << " = FMA(-t, " << x1r << ", y0r); " << x0i << " = FMA(-t, " << x1i << ", y0i); "
+                  << x1r << " = FMA(t, y0r, " << x1r << "); " << x1i << " = FMA(t, y0i, " << x1i << "); }\n";
+                bb << "    { const R y0r = " << x0r << ", y0i = " << x0i << "; "
+                   << x0r << " = FMA(t, y0r, -" << x1r << "); " << x0i << " = FMA(t, y0i, -" << x1i << "); "
+                   << x1r << " = FMA(t, " << x1r << ", y0r); " << x1i << " = FMA(t, " << x1i << ", y0i); }\n";
             }
-            flops += 8.0 * (kJitAmps / 2);
-            o << "  { const double t = " << cr(at) << ";\n  if (" << ci(at) << " != 0.0) {\n" << bb.str()
+            o << "  { const R t = " << cr(at) << ";\n  if (" << ci(at) << " != 0) {\n" << bb.str()
               << "  } else {\n" << a.str() << "  } }\n";
         }
     }
@@ -419,12 +419,12 @@ struct Gen {
             }
             o << "  {\n";
             for (int y = 0; y < D; ++y) {
-                o << "    const double o" << y << "r = ";
+                o << "    const R o" << y << "r = ";
                 for (int x = 0; x < D; ++x) {
                     const size_t e = at + 2 * static_cast<size_t>(y * D + x);
                     o << (x ? " + " : "") << cr(e) << " * " << ar(reg[x]) << " - " << ci(e) << " * " << ai(reg[x]);
                 }
-                o << ";\n    const double o" << y << "i = ";
+                o << ";\n    const R o" << y << "i = ";
                 for (int x = 0; x < D; ++x) {
                     const size_t e = at + 2 * static_cast<size_t>(y * D + x);
                     o << (x ? " + " : "") << cr(e) << " * " << ai(reg[x]) << " + " << ci(e) << " * " << ar(reg[x]);
@@ -479,7 +479,7 @@ struct Gen {
         for (int g = 0; g < kJitAmps; ++g) {
             if ((g & tb) || (static_cast<uint32_t>(g) & rm) != rm) continue;
             const int h = g | tb;
-            o << "    { const double x0r = " << ar(g) << ", x0i = " << ai(g) << ", x1r = " << ar(h) << ", x1i = " << ai(h) << ";\n"
+            o << "    { const R x0r = " << ar(g) << ", x0i = " << ai(g) << ", x1r = " << ar(h) << ", x1i = " << ai(h) << ";\n"
               << "      " << ar(g) << " = " << cr(at) << " * x0r - " << ci(at) << " * x0i + " << cr(at + 2) << " * x1r - " << ci(at + 2) << " * x1i;\n"
               << "      " << ai(g) << " = " << cr(at) << " * x0i + " << ci(at) << " * x0r + " << cr(at + 2) << " * x1i + " << ci(at + 2) << " * x1r;\n"
               << "      " << ar(h) << " = " << cr(at + 4) << " * x0r - " << ci(at + 4) << " * x0i + " << cr(at + 6) << " * x1r - " << ci(at + 6) << " * x1i;\n"
@@ -518,9 +518,68 @@ struct Gen {
             uint32_t cst = 0;
             for (int b = 0; b < op.k; ++b)
                 if (slot_bit[b] >= 0 && ((r >> slot_bit[b]) & 1)) cst |= 1u << b;
-            o << "    { const unsigned e = " << at << "u + 2u * (di | " << cst << "u); const double pr = P.c[e], pi = P.c[e + 1];"
-              << " const double xr = " << ar(r) << ", xi = " << ai(r) << "; "
+            o << "    { const unsigned e = " << at << "u + 2u * (di | " << cst << "u); const R pr = P.c[e], pi = P.c[e + 1];"
+              << " const R xr = " << ar(r) << ", xi = " << ai(r) << "; "
               << ar(r) << " = pr * xr - pi * xi; " << ai(r) << " = pr * xi + pi * xr; }\n";
+        }
+        o << "  }\n";
+    }
+
+    // exp(-i theta/2 P): P's X/Y bits are register slots (pairs g, g ^ xm); its Z parity splits
+    // into a per-register constant, a per-thread part (lane and warp bits) and a per-tile part
+    // (qubits outside the tile).  new_g = c a_g + s i^(nY+3) (-1)^parity(h & z) a_h, h = g ^ xm.
+    void pauli(const Op& op, const RtLayout& L) {
+        uint64_t outx = 0, outz = 0;
+        const uint32_t lx = split(op.mask, &outx), lz = split(op.zmask, &outz);
+        if (outx) throw std::logic_error("JIT tiles: Pauli rotation with an X bit outside the tile");
+        uint32_t xm = 0, zm = 0;
+        std::string tz = "0u";
+        for (int b = 0; b < kRtQubits; ++b) {
+            int k = 0;
+            if ((lx >> b) & 1) {
+                if (place(L, b, &k) != 'r') throw std::logic_error("JIT tiles: Pauli X bit outside the register slots");
+                xm |= 1u << k;
+            }
+            if ((lz >> b) & 1) {
+                const char w = place(L, b, &k);
+                if (w == 'r') zm |= 1u << k;
+                else tz += std::string(" ^ ((") + (w == 'l' ? "lane" : "warp") + " >> " + std::to_string(k) + ") & 1u)";
+            }
+        }
+        if (outz) tz += " ^ ((unsigned)__popcll(base & " + hex64(outz) + ") & 1u)";
+        const int e = (__builtin_popcountll(op.mask & op.zmask) + 3) & 3;
+        const size_t at = push(op.m[0]);
+        mark(0x9Au, xm | (zm << 8) | (static_cast<uint64_t>(e) << 16));
+        mark(outz, static_cast<uint64_t>(lz));
+        flops += 6.0 * kJitAmps;
+        if (!emit) return;
+        const int pivot = static_cast<int>(xm & (~xm + 1));
+        auto term = [&](int src, std::string* tr, std::string* ti) {
+            // (-1)^{parity(src slots & z)} * i^e * a_src, as expressions of the saved values
+            const bool neg = __builtin_popcount(static_cast<uint32_t>(src) & zm) & 1;
+            const std::string xr = "v" + std::to_string(src) + "r", xi = "v" + std::to_string(src) + "i";
+            std::string r, i;
+            switch (e) {
+                case 0: r = xr; i = xi; break;
+                case 1: r = "(-" + xi + ")"; i = xr; break;
+                case 2: r = "(-" + xr + ")"; i = "(-" + xi + ")"; break;
+                default: r = xi; i = "(-" + xr + ")"; break;
+            }
+            *tr = neg ? "(-" + r + ")" : r;
+            *ti = neg ? "(-" + i + ")" : i;
+        };
+        o << "  { const unsigned tp = (" << tz << ") & 1u; const R c = " << cr(at) << ", sp = tp ? -" << ci(at)
+          << " : " << ci(at) << ";\n";
+        for (int g = 0; g < kJitAmps; ++g) {
+            if (g & pivot) continue;
+            const int h = g ^ static_cast<int>(xm);
+            std::string hr, hi, gr, gi;
+            term(h, &hr, &hi);
+            term(g, &gr, &gi);
+            o << "    { const R v" << g << "r = " << ar(g) << ", v" << g << "i = " << ai(g) << ", v" << h << "r = "
+              << ar(h) << ", v" << h << "i = " << ai(h) << ";\n"
+              << "      " << ar(g) << " = c * v" << g << "r + sp * " << hr << "; " << ai(g) << " = c * v" << g << "i + sp * " << hi << ";\n"
+              << "      " << ar(h) << " = c * v" << h << "r + sp * " << gr << "; " << ai(h) << " = c * v" << h << "i + sp * " << gi << "; }\n";
         }
         o << "  }\n";
     }
@@ -533,17 +592,32 @@ struct Gen {
         for (int r = 0; r < kJitAmps; ++r) cmul_into(r, cr(at), ci(at));
     }
 
+    // shared-memory slot of register r in layout L: complex128 amplitudes take one 16-byte slot
+    // each (index swz(local)); complex64 amplitudes are the halves of 16-byte chunks (chunk
+    // swz(local >> 1), half local & 1)
+    static std::string slot_setup(const RtLayout& L, bool f32) {
+        if (!f32) return "const unsigned sf = swz(" + lfix_expr(L) + ");";
+        return "const unsigned lf = " + lfix_expr(L) + "; const unsigned sf = swz(lf >> 1), e0 = lf & 1u;";
+    }
+    static std::string slot_of(const RtLayout& L, int r, bool f32) {
+        const uint32_t lr = reg_local(L, r);
+        if (!f32) return "xb[sf ^ " + std::to_string(swz(lr)) + "u]";
+        return "xf[2u * (sf ^ " + std::to_string(swz(lr >> 1)) + "u) + (e0 ^ " + std::to_string(lr & 1u) + "u)]";
+    }
+
+    bool f32 = false;
+
     void move_to(const RtLayout& from, const RtLayout& to, bool first) {
         mark(0x7Au);
         mark_layout(to);
         if (!emit) return;
         if (!first) o << "  __syncthreads();\n";
-        o << "  { const unsigned sf = swz(" << lfix_expr(from) << ");\n";
+        o << "  { " << slot_setup(from, f32) << "\n";
         for (int r = 0; r < kJitAmps; ++r)
-            o << "    xb[sf ^ " << swz(reg_local(from, r)) << "u] = make_double2(" << ar(r) << ", " << ai(r) << ");\n";
-        o << "  }\n  __syncthreads();\n  { const unsigned sf = swz(" << lfix_expr(to) << ");\n";
+            o << "    " << slot_of(from, r, f32) << " = MK(" << ar(r) << ", " << ai(r) << ");\n";
+        o << "  }\n  __syncthreads();\n  { " << slot_setup(to, f32) << "\n";
         for (int r = 0; r < kJitAmps; ++r)
-            o << "    { const double2 x = xb[sf ^ " << swz(reg_local(to, r)) << "u]; " << ar(r) << " = x.x; " << ai(r) << " = x.y; }\n";
+            o << "    { const R2 x = " << slot_of(to, r, f32) << "; " << ar(r) << " = x.x; " << ai(r) << " = x.y; }\n";
         o << "  }\n";
     }
 };
@@ -551,7 +625,9 @@ struct Gen {
 // Is every op of the pass one the generator handles?
 bool jit_capable(const RtPlan& plan) {
     for (const RtStep& s : plan.steps)
-        if (s.kind == RT_PAULI) return false;
+        if (s.kind != RT_XPOSE && s.kind != RT_RELABEL && s.kind != RT_DENSE && s.kind != RT_PHASE &&
+            s.kind != RT_CTRL1 && s.kind != RT_DIAG && s.kind != RT_SCALE && s.kind != RT_PAULI)
+            return false;
     return true;
 }
 
@@ -561,6 +637,7 @@ __device__ __forceinline__ unsigned swz(unsigned i) { return i ^ ((i >> 3 ^ i >>
 __device__ __forceinline__ double flip(double a, int m) {
     return __hiloint2double(__double2hiint(a) ^ m, __double2loint(a));
 }
+__device__ __forceinline__ float flip(float a, int m) { return __int_as_float(__float_as_int(a) ^ m); }
 __device__ __forceinline__ void cp16(void* dst, const void* src) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src) : "memory");
@@ -625,6 +702,10 @@ bool walk_pass(const TilePass& pass, const RtPlan& plan, int n, Gen* g, RtLayout
                 break;
             case RT_DIAG: g->diag(*st.op, L); break;
             case RT_SCALE: g->scale(*st.op); break;
+            case RT_PAULI:
+                g->flush_slots(L);
+                g->pauli(*st.op, L);
+                break;
             default: return false;
         }
     }
@@ -633,9 +714,12 @@ bool walk_pass(const TilePass& pass, const RtPlan& plan, int n, Gen* g, RtLayout
     return g->coef.size() <= kJitMaxCoefDoubles;
 }
 
-// Source of one pass kernel (qsv_jit_<idx>) from a walk with emit on.
+// Source of one pass kernel (qsv_jit_<idx>) from a walk with emit on.  Complex128: 16-byte
+// amplitudes, 16 staged copies of one amplitude per thread, 64 KiB of shared memory, two CTAs
+// per SM.  Complex64: 8-byte amplitudes, 8 staged copies of two amplitudes per thread, 32 KiB,
+// two CTAs per SM (three would cap registers at 85 and spill).
 std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx, const std::string& steps,
-                        size_t n_coef, const RtLayout& F) {
+                        size_t n_coef, const RtLayout& F, bool f32) {
     const size_t nc = std::max<size_t>(n_coef, 1);
     // tile base: the bits of t deposited into the non-tile qubit positions, ascending
     std::vector<int> outside;
@@ -656,10 +740,13 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
         return base;
     };
     const uint32_t* tq = pass.tile_qubits.data();
-    // staging: chunk c = tid + 256 j holds local amplitude c
-    std::string gtid = "(u64)(tid & 31u)";
-    for (int b = 5; b < 8; ++b)
-        gtid += " | ((u64)((tid >> " + std::to_string(b) + ") & 1u) << " + std::to_string(tq[b]) + ")";
+    // staging: 16-byte chunk c = tid + 256 j holds local amplitude c (complex128) or the pair
+    // 2c, 2c + 1 (complex64); local bit b of the chunk's first amplitude sits at qubit tq[b]
+    const int low = f32 ? 1 : 0;                 // local bits below the chunk index
+    const int chunks = (1 << kRtQubits) >> low;
+    std::string gtid = "0ull";
+    for (int b = 0; b < 8; ++b)
+        gtid += " | ((u64)((tid >> " + std::to_string(b) + ") & 1u) << " + std::to_string(tq[b + low]) + ")";
     // store: the last layout's lanes are local bits 0..4
     std::string gfin = "0ull";
     for (int k = 0; k < kRtLaneBits; ++k)
@@ -668,21 +755,26 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
         gfin += " | ((u64)((warp >> " + std::to_string(k) + ") & 1u) << " + std::to_string(tq[F.warp[k]]) + ")";
     auto issue = [&](const std::string& b) {
         std::ostringstream x;
-        for (int j = 0; j < (1 << kRtQubits) / kJitThreads; ++j) {
+        for (int j = 0; j < chunks / kJitThreads; ++j) {
             uint64_t gj = 0;
-            for (int b2 = 0; b2 < 4; ++b2)
-                if ((j >> b2) & 1) gj |= 1ull << tq[8 + b2];
+            for (int b2 = 0; b2 < 4 && 8 + low + b2 < kRtQubits; ++b2)
+                if ((j >> b2) & 1) gj |= 1ull << tq[8 + low + b2];
             x << "    cp16(xb + (stid ^ " << swz(static_cast<uint32_t>(j) * kJitThreads) << "u), s + ((" << b
               << ") | gtid | " << hex64(gj) << "));\n";
         }
         return x.str();
     };
     std::ostringstream s;
-    s << "struct __align__(8) C" << idx << " { double c[" << nc << "]; };\n"
-      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", " << kJitCtasPerSm << ") qsv_jit_" << idx
-      << "(double2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P) {\n"
+    if (f32)
+        s << "typedef float R; typedef float2 R2;\n#define FMA fmaf\n#define MK make_float2\n";
+    else
+        s << "typedef double R; typedef double2 R2;\n#define FMA fma\n#define MK make_double2\n";
+    s << "struct __align__(8) C" << idx << " { R c[" << nc << "]; };\n"
+      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", " << (f32 ? kJitCtasPerSmF32 : kJitCtasPerSm)
+      << ") qsv_jit_" << idx << "(R2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P) {\n"
       << "  extern __shared__ __align__(16) unsigned char smem[];\n"
       << "  double2* xb = reinterpret_cast<double2*>(smem);\n"
+      << "  R2* xf = reinterpret_cast<R2*>(smem);\n"
       << "  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;\n"
       << "  const u64 gtid = " << gtid << ";\n"
       << "  const unsigned stid = swz(tid);\n"
@@ -694,15 +786,15 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
       << "  const u64 base = " << deposit("t") << ";\n"
       << "  asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n"
       << "  __syncthreads();\n"
-      << "  double ";
+      << "  R ";
     for (int r = 0; r < kJitAmps; ++r) s << (r ? ", " : "") << Gen::ar(r) << ", " << Gen::ai(r);
-    s << ";\n  { const unsigned sf = swz(" << Gen::lfix_expr(plan.load) << ");\n";
+    s << ";\n  { " << Gen::slot_setup(plan.load, f32) << "\n";
     for (int r = 0; r < kJitAmps; ++r)
-        s << "    { const double2 x = xb[sf ^ " << swz(reg_local(plan.load, r)) << "u]; " << Gen::ar(r) << " = x.x; "
+        s << "    { const R2 x = " << Gen::slot_of(plan.load, r, f32) << "; " << Gen::ar(r) << " = x.x; "
           << Gen::ai(r) << " = x.y; }\n";
     // one buffer serves the tile's loads and its transposes: the next tile's copies start once
-    // the last transpose has been read, and run under this tile's stores (and the other CTA
-    // on the SM computes meanwhile)
+    // the last transpose has been read, and run under this tile's stores (and the other CTAs
+    // on the SM compute meanwhile)
     s << "  }\n  __syncthreads();\n"
       << steps
       << "  __syncthreads();\n"
@@ -713,17 +805,19 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
         uint64_t gc = 0;
         for (int p = 0; p < kRtRegBits; ++p)
             if ((r >> p) & 1) gc |= 1ull << tq[F.reg[p]];
-        s << "  __stcs(s + (base | gfin | " << hex64(gc) << "), make_double2(" << Gen::ar(r) << ", " << Gen::ai(r) << "));\n";
+        s << "  __stcs(s + (base | gfin | " << hex64(gc) << "), MK(" << Gen::ar(r) << ", " << Gen::ai(r) << "));\n";
     }
     s << "  }\n  asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n}\n";
     return s.str();
 }
 
 // Source (with emit) or only the signature and coefficients (without) of one pass.
-bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emit, std::string* src,
+bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emit, bool f32, std::string* src,
               std::vector<double>* coef, uint64_t* sig_hash, double* flops_per_amp = nullptr) {
     Gen g;
     g.emit = emit;
+    g.f32 = f32;
+    g.mark(f32 ? 0xF32u : 0xF64u);
     RtLayout last{};
     if (!walk_pass(pass, plan, n, &g, &last)) return false;
     uint64_t h = 1469598103934665603ull;
@@ -734,7 +828,7 @@ bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emi
         }
     *sig_hash = h;
     if (flops_per_amp) *flops_per_amp = g.flops / kJitAmps;
-    if (emit) *src = pass_source(pass, plan, n, idx, g.o.str(), g.coef.size(), last);
+    if (emit) *src = pass_source(pass, plan, n, idx, g.o.str(), g.coef.size(), last, f32);
     coef->swap(g.coef);
     if (coef->empty()) coef->push_back(0.0);
     return true;
@@ -811,8 +905,9 @@ std::map<std::pair<uint64_t, CUcontext>, CUfunction> g_kernels;
 
 // ---------------------------------------------------------------- public
 
-JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int device) {
+JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int device, bool f32) {
     JitPlan out;
+    out.f32 = f32;
     out.idx.assign(passes.size(), -1);
     int major = 0, minor = 0;
     check_cuda(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "compute capability");
@@ -832,13 +927,22 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
         uint64_t sig = 0;
         std::string unused;
         double fpa = 0;
-        if (!gen_pass(*passes[i], plans[i], n, 0, false, &unused, &coef, &sig, &fpa)) continue;
+        if (!gen_pass(*passes[i], plans[i], n, 0, false, f32, &unused, &coef, &sig, &fpa)) continue;
         out.flops_per_amp.push_back(fpa);
         sig ^= (static_cast<uint64_t>(major) << 56) ^ (static_cast<uint64_t>(minor) << 48);
         out.idx[i] = static_cast<int>(sigs.size());
         sigs.push_back(sig);
         pass_of.push_back(i);
-        out.coef.push_back(std::move(coef));
+        // kernel parameters in the storage type's precision
+        std::vector<uint8_t> arg;
+        if (f32) {
+            std::vector<float> c(coef.begin(), coef.end());
+            arg.assign(reinterpret_cast<const uint8_t*>(c.data()), reinterpret_cast<const uint8_t*>(c.data() + c.size()));
+        } else {
+            arg.assign(reinterpret_cast<const uint8_t*>(coef.data()),
+                       reinterpret_cast<const uint8_t*>(coef.data() + coef.size()));
+        }
+        out.coef.push_back(std::move(arg));
     }
     if (sigs.empty()) return out;
     std::lock_guard<std::mutex> lock(g_jit_mu);
@@ -856,7 +960,7 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
             const size_t i = pass_of[missing[j]];
             std::vector<double> coef;
             uint64_t sig = 0;
-            gen_pass(*passes[i], plans[i], n, 0, true, &srcs[j], &coef, &sig);
+            gen_pass(*passes[i], plans[i], n, 0, true, f32, &srcs[j], &coef, &sig);
             srcs[j] = std::string(kPrelude) + srcs[j] + tag;
             char name[40];
             std::snprintf(name, sizeof name, "%016llx.cubin", static_cast<unsigned long long>(fnv1a(srcs[j])));
@@ -890,7 +994,7 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
             CUfunction f = nullptr;
             check_cu(drv.get_function(&f, mod, "qsv_jit_0"), "cuModuleGetFunction (JIT tiles)");
             check_cu(drv.set_attribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
-                                       static_cast<int>(kJitSmem)),
+                                       static_cast<int>(jit_smem(f32))),
                      "cuFuncSetAttribute (JIT tiles)");
             g_kernels[{sigs[missing[j]], ctx}] = f;
         }
@@ -899,7 +1003,7 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
     return out;
 }
 
-void jit_launch(const JitPlan& plan, int pass, double2* s, int n, cudaStream_t st) {
+void jit_launch(const JitPlan& plan, int pass, void* s, int n, cudaStream_t st) {
     const int k = plan.idx.at(pass);
     if (k < 0) throw std::logic_error("JIT tiles: pass was not compiled");
     int sms = 0, device = 0;
@@ -907,16 +1011,16 @@ void jit_launch(const JitPlan& plan, int pass, double2* s, int n, cudaStream_t s
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
     unsigned long long n_tiles = 1ull << (n - kRtQubits);
     const unsigned grid = static_cast<unsigned>(
-        std::min<unsigned long long>(n_tiles, static_cast<unsigned long long>(kJitCtasPerSm) * sms));
-    const std::vector<double>& c = plan.coef[static_cast<size_t>(k)];
-    void* args[] = {&s, &n_tiles, const_cast<double*>(c.data())};
+        std::min<unsigned long long>(n_tiles, static_cast<unsigned long long>(plan.f32 ? kJitCtasPerSmF32 : kJitCtasPerSm) * sms));
+    const std::vector<uint8_t>& c = plan.coef[static_cast<size_t>(k)];
+    void* args[] = {&s, &n_tiles, const_cast<uint8_t*>(c.data())};
     check_cu(driver().launch(static_cast<CUfunction>(plan.fns[static_cast<size_t>(k)]), grid, 1, 1, kJitThreads, 1, 1,
-                             static_cast<unsigned>(kJitSmem),
+                             static_cast<unsigned>(jit_smem(plan.f32)),
                              reinterpret_cast<CUstream>(st), args, nullptr),
              "cuLaunchKernel (JIT tiles)");
 }
 
-std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int n, size_t* n_kernels) {
+std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int n, bool f32, size_t* n_kernels) {
     std::string src = kPrelude;
     int next = 0;
     for (size_t i = 0; i < passes.size(); ++i) {
@@ -925,7 +1029,12 @@ std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int 
         std::string ps;
         std::vector<double> coef;
         uint64_t sig = 0;
-        if (!gen_pass(*passes[i], plan, n, next, true, &ps, &coef, &sig)) continue;
+        if (!gen_pass(*passes[i], plan, n, next, true, f32, &ps, &coef, &sig)) continue;
+        if (next > 0) {
+            // one program holds every pass: the type definitions come once, with the first
+            const size_t cut = ps.find("struct __align__");
+            ps = ps.substr(cut);
+        }
         src += ps;
         ++next;
     }

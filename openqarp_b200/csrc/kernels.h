@@ -134,17 +134,18 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
                const std::function<void(const Op&)>& stream_op, bool register_tiles, bool jit = false);
 
 // ---------------------------------------------------------------- JIT register tiles (kern_tile_jit.cu)
-// The register-tile passes of a stream compiled to straight-line kernels (complex128).
+// The register-tile passes of a stream compiled to straight-line kernels.
 struct JitPlan {
+    bool f32 = false;                       // complex64 storage
     std::vector<int> idx;                   // per pass: kernel index, -1 = not compiled
-    std::vector<std::vector<double>> coef;  // per kernel: its coefficients (kernel parameters)
+    std::vector<std::vector<uint8_t>> coef; // per kernel: its coefficients (kernel parameters)
     std::vector<void*> fns;                 // per kernel: the loaded function (CUfunction)
     std::vector<double> flops_per_amp;      // per kernel: FP64 operations per amplitude (FMA = 2)
 };
-JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int device);
-void jit_launch(const JitPlan& plan, int pass, double2* s, int n, cudaStream_t st);
+JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int device, bool f32);
+void jit_launch(const JitPlan& plan, int pass, void* s, int n, cudaStream_t st);
 // host-only helpers for plan inspection and tests (no device work)
-std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int n, size_t* n_kernels);
+std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int n, bool f32, size_t* n_kernels);
 std::vector<char> jit_compile_for_test(const std::string& src, int cc_major, int cc_minor);
 
 // The adjoint's reverse sweep in tile passes (kern_tile.cu): `ops` is the reverse stream (the

@@ -169,7 +169,7 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
         const bool rt = h->executor == 1 || h->executor == 3;
         const bool jit = h->executor == 3;
         if (h->dtype == QSV_C128) run_tiled<double>(passes, S128(h), h->n, h->stream, h->ws, stream_op, rt, jit);
-        else run_tiled<float>(passes, S64(h), h->n, h->stream, h->ws, stream_op, rt);
+        else run_tiled<float>(passes, S64(h), h->n, h->stream, h->ws, stream_op, rt, jit);
         for (const TilePass& p : passes) {
             if (p.tile_qubits.empty()) continue;   // counted by launch()
             h->stats.launches++;
@@ -533,8 +533,8 @@ int qsv_tile_plan_count(const uint8_t* cmds, size_t nbytes, int n, int max_q, in
     });
 }
 
-int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min_q, int cc_major, int cc_minor,
-                  int32_t* n_passes, int32_t* n_kernels, uint64_t* cubin_bytes) {
+int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int dtype, int max_q, int min_q, int cc_major,
+                  int cc_minor, int32_t* n_passes, int32_t* n_kernels, uint64_t* cubin_bytes) {
     return guarded([&] {
         if (!n_passes || !n_kernels || !cubin_bytes) throw std::invalid_argument("null output");
         if (max_q < 0 || max_q > QSV_MAX_BLOCK_QUBITS) throw std::invalid_argument("fusion width out of range");
@@ -546,7 +546,8 @@ int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int max_q, int min_
         std::vector<const TilePass*> ptrs;
         for (const TilePass& p : passes) ptrs.push_back(&p);
         size_t k = 0;
-        const std::string src = jit_source_for_test(ptrs, n, &k);
+        if (dtype != QSV_C128 && dtype != QSV_C64) throw std::invalid_argument("dtype must be QSV_C128 or QSV_C64");
+        const std::string src = jit_source_for_test(ptrs, n, dtype == QSV_C64, &k);
         if (const char* dump = std::getenv("QSV_JIT_DUMP")) {
             if (FILE* f = std::fopen(dump, "w")) {
                 std::fwrite(src.data(), 1, src.size(), f);

@@ -189,7 +189,7 @@ def test_tiled_executor_matches_oracle(m, executor, restatement):
             np.testing.assert_allclose(got, want, atol=AMP_TOL, rtol=0, err_msg=f"{name} k={k} m={m}")
 
 
-@pytest.mark.parametrize("m,executor", [(13, 2), (12, 1)])
+@pytest.mark.parametrize("m,executor", [(13, 2), (12, 1), (12, 3)])
 def test_tiled_executor_complex64(m, executor, restatement):
     n = 16
     for name, cmds in mixed_circuits(n).items():
@@ -211,7 +211,7 @@ def test_tiled_and_stream_agree_at_24q(dtype, tol):
     cmds = circuits.brickwork(n, 10, seed=8) + mixed_circuits(n)["allgates"]
     buf = ir.pack(cmds).buf
     out = []
-    for executor, k, m in ((0, 3, 0), (1, 1, 12), (1, 3, 12), (2, 3, 12)):
+    for executor, k, m in ((0, 3, 0), (1, 1, 12), (1, 3, 12), (2, 3, 12), (3, 1, 12), (3, 3, 12)):
         reg = Register(n, dtype)
         reg.configure(k, 12, executor, m)
         reg.apply(buf)

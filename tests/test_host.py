@@ -201,12 +201,17 @@ def test_random_regular_graph_is_regular():
         assert len(set(edges)) == len(edges)
 
 
-def test_jit_tile_kernels_compile_without_a_gpu():
-    """Executor 3's pass kernels are generated and compiled by NVRTC for sm_100a on the host."""
+@pytest.mark.parametrize("dtype", [_lib.QSV_C128, _lib.QSV_C64])
+def test_jit_tile_kernels_compile_without_a_gpu(dtype):
+    """Executor 3's pass kernels are generated and compiled by NVRTC for sm_100a on the host:
+    one-qubit gate layers with CZ signs, and Pauli rotations with a field term."""
     import ctypes
     n = 16
-    buf = ir.pack(circuits.brickwork(n, 6, seed=3) + circuits.hea(n, 2, seed=1)[0][:0]).buf
-    p, k, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_uint64()
-    _lib.check(_lib.lib.qsv_jit_check(_lib.u8ptr(buf), len(buf), n, 1, 12, 10, 0, ctypes.byref(p),
-                                      ctypes.byref(k), ctypes.byref(b)))
-    assert k.value == p.value > 0 and b.value > 0
+    streams = (circuits.brickwork(n, 6, seed=3),
+               circuits.heisenberg_trotter(n, 1, 0.05, np.linspace(-1, 1, n)))
+    for cmds in streams:
+        buf = ir.pack(cmds).buf
+        p, k, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_uint64()
+        _lib.check(_lib.lib.qsv_jit_check(_lib.u8ptr(buf), len(buf), n, dtype, 1, 12, 10, 0, ctypes.byref(p),
+                                          ctypes.byref(k), ctypes.byref(b)))
+        assert k.value == p.value > 0 and b.value > 0
