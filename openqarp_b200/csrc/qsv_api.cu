@@ -162,8 +162,10 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
         for (Op& o : lower(c, h->n)) ops.push_back(std::move(o));
     check_cuda(cudaEventRecord(h->e0, h->stream), "event");
     if (fuse && use_tiled(h)) {
+        // register tiles (executors 1 and 3) hold 2^12 amplitudes whatever the storage type
         const int m = h->tile_qubits > 0 ? std::min(h->tile_qubits, h->n)
-                                         : default_tile_qubits(h->n, static_cast<int>(h->amp_bytes()));
+                      : (h->executor == 1 || h->executor == 3) ? std::min(kRtQubits, h->n)
+                                                               : default_tile_qubits(h->n, static_cast<int>(h->amp_bytes()));
         const std::vector<TilePass> passes = plan_tiles(ops, h->n, m);
         auto stream_op = [h](const Op& o) { launch(h, o, h->state); };
         const bool rt = h->executor == 1 || h->executor == 3;
