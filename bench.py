@@ -338,9 +338,10 @@ def adjoint_vs_param_shift(device, shift_sample=12):
 
 
 def k_sweep(device, buf):
-    """Config 2's fusion-width sweep at 28 qubits in complex128 and complex64 (stream
-    executor): circuit time per k, and for the tensor-core widths (k = 5, 6) a probe of one
-    dense pass (FP64 DMMA in complex128; tcgen05 3xTF32 at k = 5 in complex64)."""
+    """Config 2's fusion-width sweep at 28 qubits in complex128 and complex64: the stream
+    executor's circuit time per k, for the tensor-core widths (k = 5, 6) a probe of one dense
+    pass (FP64 DMMA in complex128; tcgen05 3xTF32 at k = 5 in complex64), and the compiled
+    register-tile executor (executor 3) at k = 1 and 3."""
     from openqarp_b200 import Register
     out = {}
     pass_amps = 1 << N_QUBITS
@@ -369,6 +370,20 @@ def k_sweep(device, buf):
             rows[f"k{k}"]["kernel"] = ("k_dense_dmma (FP64 mma.sync)" if dtype == "complex128" else
                                       ("k_dense5_umma (tcgen05 kind::tf32, 3 products)" if k == 5
                                        else "k_dense_gen (no tensor path)"))
+        for k in (1, 3):
+            reg.configure(k, 12, 3)
+            reg.apply(buf)                     # compiles the passes (or finds them compiled)
+            reg.synchronize()
+            s0 = reg.stats()
+            e0 = timer.event()
+            reg.apply(buf)
+            e1 = timer.event()
+            e1.synchronize()
+            s1 = reg.stats()
+            ms = e0.elapsed_time(e1)
+            rows[f"jit_k{k}"] = {"ms": round(ms, 3), "passes": int(s1["passes"] - s0["passes"]),
+                                 "physical_gbs": round((s1["hbm_bytes"] - s0["hbm_bytes"]) / (ms * 1e-3) / 1e9, 1),
+                                 "kernel": "register-tile passes compiled for their plan (executor 3)"}
         reg.close()
         out[dtype] = rows
     return out
@@ -623,7 +638,9 @@ def b200_arm(args, rank, world, local_rank):
         heis = None
         if single and not args.skip_heisenberg:
             from bench_workloads import heisenberg_bulk
-            heis = heisenberg_bulk(n=31, steps=50, dt=0.05, seed=SEED, device=device)
+            # the chain's plan: register-tile passes compiled for their layouts (executor 3, k = 1),
+            # 1.4-1.5x the stream executor's 4-qubit blocks on this chain in both storage types
+            heis = heisenberg_bulk(n=31, steps=50, dt=0.05, seed=SEED, device=device, fusion_k=1, executor=3)
         fp64_achieved = flops / (ms_step * 1e-3) / 1e12
         result = {
             "metric": "gate GB/s (%HBM peak) @28q", "value": value, "unit": "GB/s",
