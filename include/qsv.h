@@ -327,6 +327,31 @@ QSV_API int qsv_qaoa_run(void* q, const double* params, int with_gradient, doubl
                          double* grads, double* device_ms);
 QSV_API int qsv_qaoa_destroy(void* q);
 
+/* ---- circuit batches ---------------------------------------------------------------- *
+ * Many circuits of uneven width (1..12 qubits, complex128), each with its own observable and
+ * parameter values, evaluated in one persistent launch captured in a CUDA graph: a CTA takes
+ * the next instance from a queue (costliest first) and keeps its |psi> and |phi> = H|psi> in
+ * shared memory for the forward gates, <H>, and the adjoint reverse sweep.  Replaces the
+ * serial per-circuit loop of QarpSimulator::batch_expectation (reference:
+ * qarp_simulator.cpp:971-984) and of the engine sweep (src/qarp/engines/_qarp_engine.py:
+ * 450-503), with the adjoint of run_gradient_core (qarp_simulator.cpp:1519-1605) per instance.
+ * qsv_cbatch_add takes an instance as a packed stream with its parameters substituted, the
+ * stream's dependency table (as qsv_adjoint; dep_ptr NULL: no gradient) and its observable;
+ * *index receives its position.  qsv_cbatch_set replaces instance `index`'s parameter values
+ * (a stream of the same structure: same commands and qubits); the next run uploads them
+ * inside the graph.  qsv_cbatch_run: energies[i] <- <H> of instance i; with_gradient batches
+ * also fill grads, the instances' gradients back to back (n_params each); device_ms (may be
+ * NULL) <- device time of the graph.  The first run builds the graph; instances are added
+ * before it.  Registers wider than 12 qubits are refused with QSV_ECAPABILITY. */
+QSV_API int qsv_cbatch_create(int device, int with_gradient, void** out);
+QSV_API int qsv_cbatch_add(void* b, int n_qubits, const uint8_t* cmds, size_t nbytes, const int32_t* dep_ptr,
+                           const int32_t* dep_param, const double* dep_alpha, int n_params,
+                           const uint64_t* xmask, const uint64_t* zmask, const double* coeff, size_t n_terms,
+                           int32_t* index);
+QSV_API int qsv_cbatch_set(void* b, int index, const uint8_t* cmds, size_t nbytes);
+QSV_API int qsv_cbatch_run(void* b, double* energies, double* grads, double* device_ms);
+QSV_API int qsv_cbatch_destroy(void* b);
+
 /* ---- allocation-free variant ------------------------------------------------------- *
  * No counterpart in the reference: it exists for callers that cannot call cudaMalloc —
  * a process whose device memory is owned by its own pool allocator (PyTorch's caching

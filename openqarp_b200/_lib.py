@@ -86,6 +86,12 @@ def _load():
         "qsv_qaoa_create": (c_int, [c_int, c_int, PI32, PI32, PI32, PI32, POINTER(c_void_p)]),
         "qsv_qaoa_run": (c_int, [c_void_p, PD, c_int, PD, PD, PD]),
         "qsv_qaoa_destroy": (c_int, [c_void_p]),
+        "qsv_cbatch_create": (c_int, [c_int, c_int, POINTER(c_void_p)]),
+        "qsv_cbatch_add": (c_int, [c_void_p, c_int, P8, c_size_t, PI32, PI32, PD, c_int, PU64, PU64, PD, c_size_t,
+                                   PI32]),
+        "qsv_cbatch_set": (c_int, [c_void_p, c_int, P8, c_size_t]),
+        "qsv_cbatch_run": (c_int, [c_void_p, PD, PD, PD]),
+        "qsv_cbatch_destroy": (c_int, [c_void_p]),
         "qsv_transition_static": (c_int, [c_void_p, c_void_p, c_int, c_int, PU64, PU64, PD, c_size_t,
                                           c_void_p, PD]),
     }
@@ -106,6 +112,7 @@ DECLARED = (
     "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_device_info", "qsv_set_timing",
     "qsv_pass_times", "qsv_transition_static",
     "qsv_qaoa_create", "qsv_qaoa_run", "qsv_qaoa_destroy",
+    "qsv_cbatch_create", "qsv_cbatch_add", "qsv_cbatch_set", "qsv_cbatch_run", "qsv_cbatch_destroy",
 )
 STATIC_MAX_TERMS = 4096
 

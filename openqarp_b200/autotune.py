@@ -34,9 +34,10 @@ from .errors import CudaError
 # compiled at run time for their own layouts
 CANDIDATES_C128 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3), (3, 1), (3, 3))
 CANDIDATES_C64 = ((0, 3), (0, 4), (0, 5), (1, 1), (1, 3), (3, 1), (3, 3))
-# registers narrower than this run too briefly for a measurement to pay for itself; they use
-# the fixed defaults
-MIN_TUNED_QUBITS = 20
+# registers narrower than this run too briefly for a measurement (and, for executor 3, a
+# compilation of a few seconds) to pay for itself unless the same structure runs many times;
+# they use the fixed defaults (B200Simulator.autotune_min_qubits changes the bound)
+MIN_TUNED_QUBITS = 24
 
 
 def default_cache_path() -> str:

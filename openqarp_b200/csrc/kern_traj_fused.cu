@@ -40,6 +40,8 @@ enum FsKind : uint8_t {
     FS_BRANCH,        // flag bit `flag` <- (cbits & mask) == zmask
     FS_PAULI_NOISE,   // channel kind k2 on q[0..k); parameters at coef
     FS_KRAUS_NOISE,   // k2 operators on q[0]; 8 doubles each at coef
+    FS_ADJ,           // circuit batches: adjoint step on q[0..k) (k <= 2): slot cbit <- <phi| G |psi>, then
+                      // D on both registers; G then D (2^k x 2^k each) at coef
 };
 
 struct FsStep {
@@ -737,5 +739,461 @@ template bool run_trajectories_fused<double>(const TrPlan&, int, const double2*,
                                              uint64_t*, cudaStream_t, Workspace&, uint64_t*);
 template bool run_trajectories_fused<float>(const TrPlan&, int, const float2*, uint32_t, size_t, uint64_t*,
                                             uint64_t*, cudaStream_t, Workspace&, uint64_t*);
+
+// ---------------------------------------------------------------- circuit batches
+//
+// Many circuits of up to 12 qubits (complex128), each with its own observable and parameter
+// values, in one persistent launch: a CTA takes the next instance from a queue (widest first),
+// keeps |psi> and |phi> = H|psi> in shared memory, runs the forward gate steps, <H>, and — for
+// gradients — the reverse sweep of run_gradient_core (qarp_simulator.cpp:1519-1605): for each
+// parametric command, last first, <phi| G |psi> into its slot and the command's dagger applied
+// to both registers; other commands' daggers to both.  The reference evaluates such batches one
+// circuit at a time (QarpSimulator::batch_expectation, qarp_simulator.cpp:971-984; the engine
+// sweep, _qarp_engine.py:450-503).
+
+namespace {
+
+constexpr int kCbMaxQubits = 12;
+
+struct CbInstDev {
+    int32_t n, pad;
+    uint32_t f0, f1;        // forward steps
+    uint32_t r0, r1;        // reverse steps
+    uint32_t t0, t1;        // Pauli terms
+    uint32_t slot0, nslot;  // adjoint slots
+};
+
+__device__ __forceinline__ double2 cb_block_sum2(double2 v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[2 * (threadIdx.x >> 5)] = v.x;
+        red[2 * (threadIdx.x >> 5) + 1] = v.y;
+    }
+    __syncthreads();
+    double2 t = make_double2(0.0, 0.0);
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kFsThreads / 32; ++w) {
+            t.x += red[2 * w];
+            t.y += red[2 * w + 1];
+        }
+    __syncthreads();
+    return t;   // valid in thread 0
+}
+
+// <phi| G |psi> for a k <= 2 generator on q[0..k) (k = 0: G is a scalar), summed by one thread
+// per group of 2^k amplitudes, then over the block
+__device__ double2 cb_adj_inner(const double2* psi, const double2* phi, int n, const FsStep& S, const double* g,
+                                double* red) {
+    const int k = S.k, D = 1 << k;
+    double ar = 0.0, ai = 0.0;
+    const uint64_t groups = 1ull << (n - k);
+    int pos[2] = {S.q[0], S.q[1]};
+    if (k == 2 && pos[1] < pos[0]) { const int t = pos[0]; pos[0] = pos[1]; pos[1] = t; }
+    for (uint64_t gi = threadIdx.x; gi < groups; gi += kFsThreads) {
+        uint64_t base = gi;
+        for (int b = 0; b < k; ++b) {
+            const uint64_t p = static_cast<uint64_t>(pos[b]);
+            base = ((base >> p) << (p + 1)) | (base & ((1ull << p) - 1ull));
+        }
+        uint64_t off[4];
+        for (int l = 0; l < D; ++l) {
+            uint64_t o = 0;
+            for (int b = 0; b < k; ++b)
+                if ((l >> b) & 1) o |= 1ull << S.q[b];
+            off[l] = base | o;
+        }
+        for (int y = 0; y < D; ++y) {
+            double gr = 0.0, gim = 0.0;   // (G psi)[y]
+            for (int x = 0; x < D; ++x) {
+                const double cr = g[2 * (y * D + x)], ci = g[2 * (y * D + x) + 1];
+                const double2 v = psi[off[x]];
+                gr = fma(cr, v.x, gr);
+                gr = fma(-ci, v.y, gr);
+                gim = fma(cr, v.y, gim);
+                gim = fma(ci, v.x, gim);
+            }
+            const double2 f = phi[off[y]];   // conj(f) * (G psi)
+            ar = fma(f.x, gr, ar);
+            ar = fma(f.y, gim, ar);
+            ai = fma(f.x, gim, ai);
+            ai = fma(-f.y, gr, ai);
+        }
+    }
+    return cb_block_sum2(make_double2(ar, ai), red);
+}
+
+__global__ void __launch_bounds__(kFsThreads) k_cb_run(const CbInstDev* __restrict__ inst, int n_inst,
+                                                      const FsStep* __restrict__ steps, const double* __restrict__ coef,
+                                                      const uint64_t* __restrict__ tx, const uint64_t* __restrict__ tz,
+                                                      const double2* __restrict__ tc, int with_grad,
+                                                      int* __restrict__ queue, double* __restrict__ energy,
+                                                      double2* __restrict__ slots) {
+    extern __shared__ __align__(16) unsigned char cb_smem[];
+    double2* psi = reinterpret_cast<double2*>(cb_smem);
+    double2* phi = psi + (1 << kCbMaxQubits);
+    __shared__ uint64_t sstep[sizeof(FsStep) / 8];
+    __shared__ __align__(16) double scoef[kFsMaxCoef];
+    __shared__ double red[2 * kFsThreads / 32];
+    __shared__ int cur;
+    for (;;) {
+        if (threadIdx.x == 0) cur = atomicAdd(queue, 1);
+        __syncthreads();
+        const int i = cur;
+        if (i >= n_inst) break;
+        const CbInstDev I = inst[i];
+        const int n = I.n;
+        const uint64_t dim = 1ull << n;
+        for (uint64_t j = threadIdx.x; j < dim; j += kFsThreads) psi[j] = make_double2(j == 0 ? 1.0 : 0.0, 0.0);
+        // one step into shared memory: its record and its coefficients
+        auto stage = [&](uint32_t s) -> const FsStep& {
+            __syncthreads();
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(steps + s);
+            for (int w = threadIdx.x; w < static_cast<int>(sizeof(FsStep) / 8); w += kFsThreads) sstep[w] = __ldg(src + w);
+            __syncthreads();
+            const FsStep& S = *reinterpret_cast<const FsStep*>(sstep);
+            for (uint32_t w = threadIdx.x; w < S.ncoef && w < static_cast<uint32_t>(kFsMaxCoef); w += kFsThreads)
+                scoef[w] = __ldg(coef + S.coef + w);
+            __syncthreads();
+            return S;
+        };
+        for (uint32_t s = I.f0; s < I.f1; ++s) {
+            const FsStep& S = stage(s);
+            fs_gate<double>(psi, n, S, scoef);
+        }
+        __syncthreads();
+        // phi = H psi: phi[j] = sum_t c_t (-1)^popcount((j ^ x_t) & z_t) psi[j ^ x_t]
+        double er = 0.0;
+        for (uint64_t j = threadIdx.x; j < dim; j += kFsThreads) {
+            double fr = 0.0, fi = 0.0;
+            for (uint32_t t = I.t0; t < I.t1; ++t) {
+                const uint64_t x = __ldg(tx + t), z = __ldg(tz + t);
+                const double2 c = __ldg(tc + t);
+                const double2 v = psi[j ^ x];
+                const double sg = (__popcll((j ^ x) & z) & 1) ? -1.0 : 1.0;
+                fr = fma(sg, c.x * v.x - c.y * v.y, fr);
+                fi = fma(sg, c.x * v.y + c.y * v.x, fi);
+            }
+            phi[j] = make_double2(fr, fi);
+            const double2 p = psi[j];
+            er = fma(p.x, fr, er);
+            er = fma(p.y, fi, er);
+        }
+        const double2 e = cb_block_sum2(make_double2(er, 0.0), red);
+        if (threadIdx.x == 0) energy[I.pad] = e.x;   // at the caller's instance index
+        if (with_grad) {
+            for (uint32_t s = I.r0; s < I.r1; ++s) {
+                const FsStep& S = stage(s);
+                if (S.kind == FS_ADJ) {
+                    const int D = 1 << S.k;
+                    const double2 ip = cb_adj_inner(psi, phi, n, S, scoef, red);
+                    if (threadIdx.x == 0) slots[I.slot0 + static_cast<uint32_t>(S.cbit)] = ip;
+                    const double* d = scoef + 2 * D * D;
+                    if (S.k == 0) {
+                        for (uint64_t j = threadIdx.x; j < dim; j += kFsThreads) {
+                            psi[j] = cmul_d<double>(d[0], d[1], psi[j]);
+                            phi[j] = cmul_d<double>(d[0], d[1], phi[j]);
+                        }
+                    } else if (S.k == 1) {
+                        fs_dense<double, 1>(psi, n, S, d);
+                        fs_dense<double, 1>(phi, n, S, d);
+                    } else {
+                        fs_dense<double, 2>(psi, n, S, d);
+                        fs_dense<double, 2>(phi, n, S, d);
+                    }
+                } else {
+                    fs_gate<double>(psi, n, S, scoef);
+                    fs_gate<double>(phi, n, S, scoef);
+                }
+            }
+        }
+        __syncthreads();   // the registers and `cur` are free for the next instance
+    }
+}
+
+struct CbInstHost {
+    int n = 0;
+    int n_params = 0;
+    uint32_t f0 = 0, f1 = 0, r0 = 0, r1 = 0, t0 = 0, t1 = 0, slot0 = 0;
+    uint32_t coef0 = 0, coef1 = 0;   // the instance's coefficient range
+    std::vector<int32_t> slot_cmd;   // per slot: the parametric command
+    std::vector<c128> slot_pref;
+    std::vector<int32_t> dep_ptr, dep_param;
+    std::vector<double> dep_alpha;
+};
+
+// the forward steps, reverse steps and coefficients of one instance (its parameters in place)
+void cb_encode(const std::vector<Cmd>& cmds, int n, const int32_t* dep_ptr, bool grad, std::vector<FsStep>& fwd,
+               std::vector<FsStep>& rev, std::vector<double>& coef, std::vector<c128>* prefs) {
+    TrPlan fp;
+    fp.steps.emplace_back();
+    fp.steps.back().kind = TrStep::OPS;
+    for (const Cmd& c : fuse_for_dispatch(cmds, n, 3, 0))
+        for (Op& o : lower(c, n)) fp.steps.back().ops.push_back(std::move(o));
+    if (!encode(fp, fwd, coef)) throw capability_error("circuit batch: a command has no shared-memory form");
+    if (!grad) return;
+    int slot = 0;
+    for (size_t idx = cmds.size(); idx-- > 0;) {
+        const Cmd& c = cmds[idx];
+        if (dep_ptr[idx + 1] > dep_ptr[idx]) {
+            c128 pref;
+            std::vector<c128> G;
+            int k = 0;
+            if (!generator(c, &pref, &G, &k))
+                throw capability_error("run_gradient: gate '" + std::to_string(c.gate) +
+                                       "' carries a symbolic parameter but has no adjoint generator rule");
+            std::vector<c128> D;
+            if (k == 0) {
+                const double th = -c.p.at(0);
+                D = {c128(std::cos(th), std::sin(th))};
+            } else {
+                D = local_unitary(dagger(c));
+            }
+            FsStep f;
+            if (coef.size() & 1) coef.push_back(0.0);
+            f.kind = FS_ADJ;
+            f.k = static_cast<uint8_t>(k);
+            for (int b = 0; b < k; ++b) f.q[b] = static_cast<uint8_t>(c.q[b]);
+            f.cbit = slot++;
+            f.coef = static_cast<uint32_t>(coef.size());
+            for (const c128& v : G) { coef.push_back(v.real()); coef.push_back(v.imag()); }
+            for (const c128& v : D) { coef.push_back(v.real()); coef.push_back(v.imag()); }
+            f.ncoef = static_cast<uint32_t>(coef.size()) - f.coef;
+            rev.push_back(f);
+            if (prefs) prefs->push_back(pref);
+        } else {
+            TrPlan rp;
+            rp.steps.emplace_back();
+            rp.steps.back().kind = TrStep::OPS;
+            for (Op& o : lower(dagger(c), n)) rp.steps.back().ops.push_back(std::move(o));
+            if (!encode(rp, rev, coef)) throw capability_error("circuit batch: a command has no shared-memory form");
+        }
+    }
+}
+
+}  // namespace
+
+struct CircuitBatch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<CbInstHost> inst;
+    std::vector<FsStep> steps;
+    std::vector<double> coef;
+    std::vector<uint64_t> tx, tz;
+    std::vector<double> tc;
+    uint32_t n_slots = 0;
+    bool grad = false;
+    // device side, built by finalize
+    unsigned char* dev = nullptr;
+    double* host_coef = nullptr;       // pinned: the graph's source of coefficients
+    double* host_out = nullptr;        // pinned: energies then slots
+    size_t off_inst = 0, off_steps = 0, off_coef = 0, off_tx = 0, off_tz = 0, off_tc = 0, off_queue = 0,
+           off_energy = 0, off_slots = 0, total = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+    ~CircuitBatch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (dev) cudaFree(dev);
+        if (host_coef) cudaFreeHost(host_coef);
+        if (host_out) cudaFreeHost(host_out);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+void* cbatch_create(int device, bool with_gradient) {
+    auto* b = new CircuitBatch();
+    b->device = device;
+    b->grad = with_gradient;
+    return b;
+}
+
+int cbatch_add(void* bp, const std::vector<Cmd>& cmds, int n, const int32_t* dep_ptr, const int32_t* dep_param,
+               const double* dep_alpha, int n_params, const PauliTerms& terms) {
+    CircuitBatch* b = static_cast<CircuitBatch*>(bp);
+    if (b->exec) throw std::invalid_argument("circuit batch: instances are added before the first run");
+    if (n < 1 || n > kCbMaxQubits)
+        throw capability_error("circuit batch: registers of 1.." + std::to_string(kCbMaxQubits) + " qubits");
+    CbInstHost h;
+    h.n = n;
+    h.n_params = b->grad ? n_params : 0;
+    std::vector<FsStep> fwd, rev;
+    const size_t c0 = b->coef.size();
+    cb_encode(cmds, n, dep_ptr, b->grad, fwd, rev, b->coef, &h.slot_pref);
+    h.coef0 = static_cast<uint32_t>(c0);
+    h.coef1 = static_cast<uint32_t>(b->coef.size());
+    h.f0 = static_cast<uint32_t>(b->steps.size());
+    b->steps.insert(b->steps.end(), fwd.begin(), fwd.end());
+    h.f1 = h.r0 = static_cast<uint32_t>(b->steps.size());
+    b->steps.insert(b->steps.end(), rev.begin(), rev.end());
+    h.r1 = static_cast<uint32_t>(b->steps.size());
+    if (b->grad) {
+        for (size_t idx = cmds.size(); idx-- > 0;)
+            if (dep_ptr[idx + 1] > dep_ptr[idx]) h.slot_cmd.push_back(static_cast<int32_t>(idx));
+        h.dep_ptr.assign(dep_ptr, dep_ptr + cmds.size() + 1);
+        h.dep_param.assign(dep_param, dep_param + dep_ptr[cmds.size()]);
+        h.dep_alpha.assign(dep_alpha, dep_alpha + dep_ptr[cmds.size()]);
+    }
+    h.slot0 = b->n_slots;
+    b->n_slots += static_cast<uint32_t>(h.slot_cmd.size());
+    h.t0 = static_cast<uint32_t>(b->tx.size());
+    for (size_t g = 0; g < terms.gx.size(); ++g)
+        for (int32_t t = terms.gstart[g]; t < terms.gstart[g + 1]; ++t) {
+            b->tx.push_back(terms.gx[g]);
+            b->tz.push_back(terms.z[t]);
+            b->tc.push_back(terms.c[2 * t]);
+            b->tc.push_back(terms.c[2 * t + 1]);
+        }
+    h.t1 = static_cast<uint32_t>(b->tx.size());
+    b->inst.push_back(std::move(h));
+    return static_cast<int>(b->inst.size()) - 1;
+}
+
+// new parameter values for instance idx: the same structure, so only its coefficients change
+void cbatch_set(void* bp, int idx, const std::vector<Cmd>& cmds) {
+    CircuitBatch* b = static_cast<CircuitBatch*>(bp);
+    if (idx < 0 || idx >= static_cast<int>(b->inst.size())) throw std::invalid_argument("circuit batch: no such instance");
+    CbInstHost& h = b->inst[static_cast<size_t>(idx)];
+    std::vector<FsStep> fwd, rev;
+    std::vector<double> coef;
+    std::vector<c128> prefs;
+    cb_encode(cmds, h.n, h.dep_ptr.empty() ? nullptr : h.dep_ptr.data(), b->grad && !h.dep_ptr.empty(), fwd, rev,
+              coef, &prefs);
+    if (coef.size() != h.coef1 - h.coef0 || fwd.size() != h.f1 - h.f0 || rev.size() != h.r1 - h.r0)
+        throw std::invalid_argument("circuit batch: the new stream's structure differs from the instance's");
+    for (size_t s = 0; s < fwd.size(); ++s)
+        if (fwd[s].kind != b->steps[h.f0 + s].kind || fwd[s].coef + h.coef0 != b->steps[h.f0 + s].coef)
+            throw std::invalid_argument("circuit batch: the new stream's structure differs from the instance's");
+    std::copy(coef.begin(), coef.end(), b->coef.begin() + h.coef0);
+    h.slot_pref = prefs;
+    if (b->host_coef) std::copy(coef.begin(), coef.end(), b->host_coef + h.coef0);
+}
+
+namespace {
+
+void cb_finalize(CircuitBatch* b) {
+    check_cuda(cudaSetDevice(b->device), "cudaSetDevice");
+    check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch stream");
+    check_cuda(cudaEventCreate(&b->e0), "event");
+    check_cuda(cudaEventCreate(&b->e1), "event");
+    // the instance's coefficients move with it: steps index the batch-wide table
+    for (CbInstHost& h : b->inst)
+        for (uint32_t s = h.f0; s < h.r1; ++s) b->steps[s].coef += h.coef0;
+    // widest (costliest) instances first: the queue order
+    std::vector<size_t> order(b->inst.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) {
+        const double wa = std::ldexp(1.0, b->inst[a].n) * (b->inst[a].r1 - b->inst[a].f0 + b->inst[a].t1 - b->inst[a].t0);
+        const double wc = std::ldexp(1.0, b->inst[c].n) * (b->inst[c].r1 - b->inst[c].f0 + b->inst[c].t1 - b->inst[c].t0);
+        return wa > wc;
+    });
+    std::vector<CbInstDev> idev;
+    for (size_t oi : order) {
+        const CbInstHost& h = b->inst[oi];
+        CbInstDev d{};
+        d.n = h.n;
+        d.pad = static_cast<int32_t>(oi);   // the caller's index: results are written there
+        d.f0 = h.f0; d.f1 = h.f1; d.r0 = h.r0; d.r1 = h.r1; d.t0 = h.t0; d.t1 = h.t1;
+        d.slot0 = h.slot0; d.nslot = static_cast<uint32_t>(h.slot_cmd.size());
+        idev.push_back(d);
+    }
+    if (b->coef.empty()) b->coef.push_back(0.0);
+    if (b->tx.empty()) { b->tx.push_back(0); b->tz.push_back(0); b->tc.push_back(0.0); b->tc.push_back(0.0); }
+    auto align = [](size_t x) { return (x + 255) & ~size_t{255}; };
+    const size_t n_inst = b->inst.size();
+    b->off_inst = 0;
+    b->off_steps = align(idev.size() * sizeof(CbInstDev));
+    b->off_coef = b->off_steps + align(std::max<size_t>(b->steps.size(), 1) * sizeof(FsStep));
+    b->off_tx = b->off_coef + align(b->coef.size() * sizeof(double));
+    b->off_tz = b->off_tx + align(b->tx.size() * 8);
+    b->off_tc = b->off_tz + align(b->tz.size() * 8);
+    b->off_queue = b->off_tc + align(b->tc.size() * 8);
+    b->off_energy = b->off_queue + 256;
+    b->off_slots = b->off_energy + align(n_inst * 8);
+    b->total = b->off_slots + align(std::max<uint32_t>(b->n_slots, 1) * 16);
+    check_cuda(cudaMalloc(&b->dev, b->total), "circuit batch buffers");
+    check_cuda(cudaMallocHost(&b->host_coef, b->coef.size() * sizeof(double)), "pinned coefficients");
+    check_cuda(cudaMallocHost(&b->host_out, (n_inst + 2 * std::max<uint32_t>(b->n_slots, 1)) * sizeof(double)),
+               "pinned results");
+    std::copy(b->coef.begin(), b->coef.end(), b->host_coef);
+    auto up = [&](size_t off, const void* src, size_t bytes) {
+        if (bytes) check_cuda(cudaMemcpyAsync(b->dev + off, src, bytes, cudaMemcpyHostToDevice, b->stream), "batch upload");
+    };
+    up(b->off_inst, idev.data(), idev.size() * sizeof(CbInstDev));
+    up(b->off_steps, b->steps.data(), b->steps.size() * sizeof(FsStep));
+    up(b->off_tx, b->tx.data(), b->tx.size() * 8);
+    up(b->off_tz, b->tz.data(), b->tz.size() * 8);
+    up(b->off_tc, b->tc.data(), b->tc.size() * 8);
+    check_cuda(cudaStreamSynchronize(b->stream), "batch upload");
+    int sms = 0;
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "sm count");
+    const size_t smem = 2 * (size_t{1} << kCbMaxQubits) * sizeof(double2);
+    check_cuda(cudaFuncSetAttribute(k_cb_run, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+               "batch smem");
+    const unsigned grid = static_cast<unsigned>(std::min<size_t>(n_inst, static_cast<size_t>(sms)));
+    // one graph: coefficients up, queue reset, the persistent kernel, results down
+    check_cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "batch capture");
+    check_cuda(cudaMemcpyAsync(b->dev + b->off_coef, b->host_coef, b->coef.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, b->stream), "batch coefficients");
+    check_cuda(cudaMemsetAsync(b->dev + b->off_queue, 0, sizeof(int), b->stream), "batch queue");
+    k_cb_run<<<grid, kFsThreads, smem, b->stream>>>(
+        reinterpret_cast<const CbInstDev*>(b->dev + b->off_inst), static_cast<int>(n_inst),
+        reinterpret_cast<const FsStep*>(b->dev + b->off_steps), reinterpret_cast<const double*>(b->dev + b->off_coef),
+        reinterpret_cast<const uint64_t*>(b->dev + b->off_tx), reinterpret_cast<const uint64_t*>(b->dev + b->off_tz),
+        reinterpret_cast<const double2*>(b->dev + b->off_tc), b->grad ? 1 : 0, reinterpret_cast<int*>(b->dev + b->off_queue),
+        reinterpret_cast<double*>(b->dev + b->off_energy), reinterpret_cast<double2*>(b->dev + b->off_slots));
+    check_cuda(cudaMemcpyAsync(b->host_out, b->dev + b->off_energy, n_inst * sizeof(double), cudaMemcpyDeviceToHost,
+                               b->stream), "batch energies");
+    if (b->n_slots)
+        check_cuda(cudaMemcpyAsync(b->host_out + n_inst, b->dev + b->off_slots, b->n_slots * 16,
+                                   cudaMemcpyDeviceToHost, b->stream), "batch slots");
+    check_cuda(cudaStreamEndCapture(b->stream, &b->graph), "batch capture");
+    check_cuda(cudaGraphInstantiate(&b->exec, b->graph, 0), "batch graph");
+}
+
+}  // namespace
+
+void cbatch_run(void* bp, double* energies, double* grads, double* device_ms) {
+    CircuitBatch* b = static_cast<CircuitBatch*>(bp);
+    if (b->inst.empty()) return;
+    if (!b->exec) cb_finalize(b);
+    check_cuda(cudaSetDevice(b->device), "cudaSetDevice");
+    check_cuda(cudaEventRecord(b->e0, b->stream), "event");
+    check_cuda(cudaGraphLaunch(b->exec, b->stream), "batch graph launch");
+    check_cuda(cudaEventRecord(b->e1, b->stream), "event");
+    check_cuda(cudaStreamSynchronize(b->stream), "circuit batch");
+    if (device_ms) {
+        float ms = 0;
+        check_cuda(cudaEventElapsedTime(&ms, b->e0, b->e1), "event");
+        *device_ms = ms;
+    }
+    const size_t n_inst = b->inst.size();
+    // the kernel wrote results at the caller's instance index (CbInstDev::pad)
+    if (energies) std::copy(b->host_out, b->host_out + n_inst, energies);
+    if (grads && b->grad) {
+        size_t g0 = 0;
+        for (const CbInstHost& h : b->inst) {
+            for (int p = 0; p < h.n_params; ++p) grads[g0 + static_cast<size_t>(p)] = 0.0;
+            for (size_t s = 0; s < h.slot_cmd.size(); ++s) {
+                const double* ipd = b->host_out + n_inst + 2 * (h.slot0 + s);
+                const c128 ip(ipd[0], ipd[1]);
+                const double base = 2.0 * std::real(h.slot_pref[s] * ip);
+                const int32_t i = h.slot_cmd[s];
+                for (int32_t d = h.dep_ptr[i]; d < h.dep_ptr[i + 1]; ++d)
+                    grads[g0 + static_cast<size_t>(h.dep_param[d])] += h.dep_alpha[d] * base;
+            }
+            g0 += static_cast<size_t>(h.n_params);
+        }
+    }
+}
+
+void cbatch_destroy(void* bp) { delete static_cast<CircuitBatch*>(bp); }
 
 }  // namespace qsv

@@ -191,6 +191,17 @@ struct PauliTerms {
 PauliTerms prepare_terms(const uint64_t* xmask, const uint64_t* zmask, const double* coeff,
                          size_t n_terms, int n_qubits);
 
+// ---------------------------------------------------------------- circuit batches (kern_traj_fused.cu)
+// Many circuits of at most 12 qubits (complex128) in one persistent graph-captured launch:
+// forward, <H> and (with_gradient) the adjoint slots of every instance.
+void* cbatch_create(int device, bool with_gradient);
+int cbatch_add(void* b, const std::vector<Cmd>& cmds, int n, const int32_t* dep_ptr, const int32_t* dep_param,
+               const double* dep_alpha, int n_params, const PauliTerms& terms);
+void cbatch_set(void* b, int idx, const std::vector<Cmd>& cmds);
+void cbatch_run(void* b, double* energies, double* grads, double* device_ms);
+void cbatch_destroy(void* b);
+
+
 // <bra|H|ket> (FP64 accumulation); result written to out[2] (host), stream synchronised.
 template <typename T>
 void transition(const vec2_t<T>* bra, const vec2_t<T>* ket, int n, const PauliTerms& terms,

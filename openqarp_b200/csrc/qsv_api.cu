@@ -779,6 +779,67 @@ int qsv_qaoa_destroy(void* q) {
     return guarded([&] { qaoa_destroy(q); });
 }
 
+int qsv_cbatch_create(int device, int with_gradient, void** out) {
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("null output");
+        int count = 0;
+        check_cuda(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+        if (device < 0 || device >= count) throw std::invalid_argument("no such CUDA device");
+        *out = cbatch_create(device, with_gradient != 0);
+    });
+}
+
+int qsv_cbatch_add(void* b, int n_qubits, const uint8_t* cmds, size_t nbytes, const int32_t* dep_ptr,
+                   const int32_t* dep_param, const double* dep_alpha, int n_params, const uint64_t* xm,
+                   const uint64_t* zm, const double* coeff, size_t nt, int32_t* index) {
+    return guarded([&] {
+        if (!b) throw std::invalid_argument("null batch");
+        if (nt && (!xm || !zm || !coeff)) throw std::invalid_argument("null observable arrays");
+        std::vector<Cmd> cs = decode(cmds, nbytes);
+        for (const Cmd& c : cs) {
+            if (needs_trajectory(c))
+                throw std::runtime_error("circuit batch: mid-circuit measurement, Reset or a classical condition "
+                                         "has no single statevector");
+            for (uint32_t q : c.q)
+                if (static_cast<int>(q) >= n_qubits) throw std::invalid_argument("command acts on a qubit outside the register");
+        }
+        if (dep_ptr) {
+            if (dep_ptr[0] != 0) throw std::invalid_argument("dep_ptr[0] must be 0");
+            for (size_t i = 0; i < cs.size(); ++i) {
+                if (dep_ptr[i + 1] < dep_ptr[i]) throw std::invalid_argument("dep_ptr must be non-decreasing");
+                for (int d = dep_ptr[i]; d < dep_ptr[i + 1]; ++d)
+                    if (dep_param[d] < 0 || dep_param[d] >= n_params)
+                        throw std::invalid_argument("dependency names a parameter outside [0, n_params)");
+            }
+        }
+        std::vector<int32_t> none(cs.size() + 1, 0);
+        const PauliTerms terms = prepare_terms(xm, zm, coeff, nt, n_qubits);
+        const int idx = cbatch_add(b, cs, n_qubits, dep_ptr ? dep_ptr : none.data(), dep_param, dep_alpha,
+                                   dep_ptr ? n_params : 0, terms);
+        if (index) *index = idx;
+    });
+}
+
+int qsv_cbatch_set(void* b, int index, const uint8_t* cmds, size_t nbytes) {
+    return guarded([&] {
+        if (!b) throw std::invalid_argument("null batch");
+        cbatch_set(b, index, decode(cmds, nbytes));
+    });
+}
+
+int qsv_cbatch_run(void* b, double* energies, double* grads, double* device_ms) {
+    return guarded([&] {
+        if (!b) throw std::invalid_argument("null batch");
+        cbatch_run(b, energies, grads, device_ms);
+    });
+}
+
+int qsv_cbatch_destroy(void* b) {
+    return guarded([&] {
+        if (b) cbatch_destroy(b);
+    });
+}
+
 int qsv_synchronize(void* hp) {
     return guarded([&] {
         Handle* h = H_(hp);

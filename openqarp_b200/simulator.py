@@ -320,6 +320,8 @@ class B200Simulator:
         self._fusion_min = self.kDefaultFusionMinQubits
         self.executor = -1
         self.autotune = bool(autotune)
+        from .autotune import MIN_TUNED_QUBITS
+        self.autotune_min_qubits = MIN_TUNED_QUBITS
         self.last_plan: Optional[dict] = None
         # complex64 bulk mode: FP64 renormalisation after each circuit (default on) and an
         # error report per result (precision.py); "shadow" repeats each call in complex128
@@ -447,7 +449,7 @@ class B200Simulator:
         """Configure ``reg`` with the autotuned (executor, fusion width) for this circuit: from
         the cache, or measured once on the device and stored (autotune.py)."""
         from . import autotune
-        if not self._tuned() or reg.n < autotune.MIN_TUNED_QUBITS:
+        if not self._tuned() or reg.n < self.autotune_min_qubits:
             self.last_plan = {"executor": max(self.executor, 0), "fusion_k": self._fusion_max,
                               "source": "knobs"}
             return

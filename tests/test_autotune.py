@@ -46,6 +46,7 @@ def test_plugin_call_tunes_once_then_reads_the_cache(tmp_path, restatement, monk
     cmds = circuits.brickwork(n, 6, seed=9)
     want = restatement.statevector(ir.pack(cmds).buf, n)
     sim = B200Simulator()
+    sim.autotune_min_qubits = n
     try:
         got = sim.statevector(cmds, n)
         assert sim.last_plan["source"] == "measured"
