@@ -31,6 +31,8 @@ Also reported on the same line:
     exact Born readout and the PauliAveraging parity counts on the device;
   * plain_12q_latency: the CPU-runnable 12-qubit configuration (HEA, 64-term <H>, 4000 shots)
     as microseconds per statevector / expectation / run call, beside the reference's calls;
+  * circuit_batch: 1024 VQE-shaped circuits of 6..12 qubits, each with its own parameters and
+    observable, <H> and adjoint gradients of all of them in one graph-captured launch;
   * trajectories: feed-forward circuits (a mid-circuit measurement and a conditioned gate per
     layer) at 16 qubits (batched executor) and 10 qubits (shared-memory executor) sampled shot
     by shot on the device, noiseless and noisy, against the reference's CPU run() on a bounded
@@ -635,6 +637,10 @@ def b200_arm(args, rank, world, local_rank):
         if single and not args.skip_trajectories:
             from bench_workloads import trajectory_rows
             traj = trajectory_rows(device=device)
+        cbatch = None
+        if single and not args.skip_qaoa:
+            from bench_workloads import circuit_batch_rows
+            cbatch = circuit_batch_rows(device=device)
         heis = None
         if single and not args.skip_heisenberg:
             from bench_workloads import heisenberg_bulk
@@ -696,6 +702,7 @@ def b200_arm(args, rank, world, local_rank):
             "k_sweep_28q": sweep_k,
             "heisenberg31_c64_bulk": heis,
             "qaoa_batched": qaoa,
+            "circuit_batch": cbatch,
             "structured_and_readouts": structured,
             "trajectories": traj,
             "plain_12q_latency": plain12,

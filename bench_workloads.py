@@ -276,3 +276,72 @@ def config1_latency(device: int = 0, n: int = 12, layers: int = 10, n_terms: int
     except (FileNotFoundError, ImportError, OSError):
         out["reference_cpu"] = "oracle/_ref not built on this machine"
     return out
+
+
+# ---------------------------------------------------------------- general circuit batches
+
+def circuit_batch_rows(device: int = 0, count: int = 1024, seed: int = 1234, sample: int = 16) -> dict:
+    """Many small VQE-shaped circuits in one persistent graph-captured launch: ``count``
+    hardware-efficient ansaetze of 6..12 qubits (1..4 layers), each with its own random
+    parameters and its own observable (TFIM chain + random weight <= 3 terms), <H> and the
+    adjoint gradient of every instance.  Compared with the same instances one at a time through
+    B200Simulator.energy_and_gradient and through the reference's run_gradient on the host
+    cores (timed samples, scaled by total cost)."""
+    import os
+    from openqarp_b200 import B200Simulator
+    from openqarp_b200.batch import CircuitBatch
+    rng = np.random.default_rng(seed)
+    insts = []
+    for _ in range(count):
+        n = int(rng.integers(6, 13))
+        layers = int(rng.integers(1, 5))
+        cmds, vals, names = circuits.hea(n, layers, seed=int(rng.integers(1 << 30)))
+        obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, int(rng.integers(4, 32)),
+                                                                  seed=int(rng.integers(1 << 30)), max_weight=3)
+        insts.append((cmds, n, obs, vals, names))
+    cost = [float(2 ** n) * (len(c) + len(o)) for c, n, o, _, _ in insts]
+    b = CircuitBatch(device, with_gradient=True)
+    try:
+        for cmds, n, obs, vals, names in insts:
+            b.add(cmds, n, obs, vals, names)
+        b.run()                                   # builds and warms the graph
+        times = []
+        for _ in range(5):
+            energies, grads, ms = b.run()
+            times.append(ms)
+    finally:
+        b.close()
+    ms = float(np.median(times))
+    pick = rng.choice(count, size=sample, replace=False)
+    sim = B200Simulator(device=device)
+    t0 = time.perf_counter()
+    err = 0.0
+    for j in pick:
+        cmds, n, obs, vals, names = insts[int(j)]
+        e, g = sim.energy_and_gradient(cmds, n, obs, vals, names)
+        err = max(err, abs(e - energies[int(j)]), float(np.max(np.abs(np.asarray(g) - grads[int(j)]))))
+    dt = time.perf_counter() - t0
+    sim.close()
+    scale = sum(cost) / sum(cost[int(j)] for j in pick)
+    out = {"instances": count, "widths": "6..12", "layers": "1..4", "ms_per_batch": ms,
+           "instances_per_s": count / (ms * 1e-3),
+           "gradients": "adjoint, every parameter of every instance",
+           "graph": "one CUDA graph: coefficients H2D, queue reset, persistent kernel, results D2H",
+           "per_circuit_engine_ms_est": dt * 1e3 * scale, "speedup_vs_per_circuit": dt * 1e3 * scale / ms,
+           "max_abs_diff_vs_per_circuit": err,
+           "per_circuit_sample": f"{sample} instances through B200Simulator.energy_and_gradient, scaled by cost"}
+    try:
+        from oracle.oracle import Reference
+        ref = Reference()
+        ref.set_threads(os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        for j in pick:
+            cmds, n, obs, vals, names = insts[int(j)]
+            ref.run_gradient(ir.pack(cmds, vals, names), n, len(names), np.array([vals[k] for k in names]),
+                             observable.to_masks(obs, n))
+        rdt = time.perf_counter() - t0
+        out.update({"reference_cpu_ms_est": rdt * 1e3 * scale, "speedup_vs_reference_cpu": rdt * 1e3 * scale / ms,
+                    "reference_cpu_cores": os.cpu_count()})
+    except FileNotFoundError:
+        pass
+    return out

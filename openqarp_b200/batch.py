@@ -1,4 +1,11 @@
-"""Batched QAOA MaxCut: many instances of uneven width, one persistent graph-captured launch.
+"""Batched circuits: many instances of uneven width, one persistent graph-captured launch.
+
+``CircuitBatch`` wraps qsv_cbatch_* (include/qsv.h): arbitrary circuits of 1..12 qubits, each
+with its own observable and parameter values, evaluated together — forward gates, <H> and,
+optionally, the adjoint gradient of every instance — in one CUDA graph; ``set`` swaps in new
+parameter values of an instance and the next ``run`` replays the graph.
+
+Batched QAOA MaxCut: many instances of uneven width, one persistent graph-captured launch.
 
 ``QaoaBatch`` wraps qsv_qaoa_create / qsv_qaoa_run (include/qsv.h).  Each instance is the
 circuit ``circuits.qaoa_maxcut`` emits — H on every qubit, then per round RZZ(2 gamma) on every
@@ -17,7 +24,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib, circuits
-from ._lib import check, dptr, i32ptr, lib
+from ._lib import check, dptr, i32ptr, lib, u64ptr, u8ptr
 
 
 @dataclass
@@ -139,3 +146,75 @@ def run_sharded(instances, params, rank: int, world: int, device: int, runner=No
             if part["g"]:
                 grads[i] = np.asarray(part["g"][j])
     return energies, grads, max(p["ms"] for p in gathered), mine
+
+
+class CircuitBatch:
+    """Many circuits (1..12 qubits each, complex128) evaluated in one persistent launch.
+
+    ``add(commands, n_qubits, observable, values, param_order)`` appends an instance: its
+    commands (symbolic parameters are substituted from ``values``), its Pauli-sum observable,
+    and — for a gradient batch — the order of the parameters to differentiate.  ``run()``
+    returns (energies, gradients, device_ms): one <H> per instance and, with
+    ``with_gradient``, one gradient array per instance (in its ``param_order``).
+    ``set(index, values)`` replaces an instance's parameter values; the structure stays."""
+
+    MAX_QUBITS = 12
+
+    def __init__(self, device: int = 0, with_gradient: bool = True):
+        self.device = int(device)
+        self.with_gradient = bool(with_gradient)
+        self._inst = []
+        h = ctypes.c_void_p()
+        check(lib.qsv_cbatch_create(self.device, 1 if self.with_gradient else 0, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.qsv_cbatch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def __len__(self):
+        return len(self._inst)
+
+    def add(self, commands, n_qubits: int, observable, values=None, param_order=None) -> int:
+        from .ir import pack
+        from .observable import to_masks
+        commands = list(commands)
+        order = list(param_order) if (self.with_gradient and param_order is not None) else None
+        stream = pack(commands, values, order)
+        masks = to_masks(observable, n_qubits)
+        idx = ctypes.c_int32()
+        dep = order is not None
+        check(lib.qsv_cbatch_add(self._h, int(n_qubits), u8ptr(stream.buf), len(stream.buf),
+                                 i32ptr(stream.dep_ptr) if dep else None,
+                                 i32ptr(stream.dep_param) if dep else None,
+                                 dptr(stream.dep_alpha) if dep else None, len(order) if dep else 0,
+                                 u64ptr(masks.x), u64ptr(masks.z), dptr(masks.coeff), masks.n_terms,
+                                 ctypes.byref(idx)))
+        self._inst.append((commands, int(n_qubits), order))
+        return idx.value
+
+    def set(self, index: int, values) -> None:
+        from .ir import pack
+        commands, _, order = self._inst[index]
+        buf = pack(commands, values, order).buf
+        check(lib.qsv_cbatch_set(self._h, int(index), u8ptr(buf), len(buf)))
+
+    def run(self):
+        n = len(self._inst)
+        energies = np.zeros(max(n, 1))
+        sizes = [len(o) if o is not None else 0 for _, _, o in self._inst]
+        grads = np.zeros(max(sum(sizes), 1))
+        ms = ctypes.c_double()
+        check(lib.qsv_cbatch_run(self._h, dptr(energies), dptr(grads), ctypes.byref(ms)))
+        out, g0 = [], 0
+        for s in sizes:
+            out.append(grads[g0:g0 + s].copy())
+            g0 += s
+        return energies[:n], (out if self.with_gradient else None), ms.value

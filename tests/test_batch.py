@@ -147,3 +147,82 @@ def test_batch_run_seeds_step_per_set(reference):
                 assert res.counts == reference.run(ir.pack(stream, s).buf, n, 500, 77 + i)
     finally:
         sim.close()
+
+
+# ---------------------------------------------------------------- general circuit batches
+
+def _random_instance(rng, i):
+    n = int(rng.integers(2, 13))
+    kind = i % 3
+    if kind == 0:
+        cmds, vals, names = circuits.hea(n, int(rng.integers(1, 4)), seed=int(rng.integers(1 << 30)))
+    elif kind == 1:
+        edges = [(q, (q + 1) % n) for q in range(n)] if n > 2 else [(0, 1)]
+        cmds, names, _ = circuits.qaoa_maxcut(n, edges, int(rng.integers(1, 3)))
+        vals = dict(zip(names, rng.uniform(0, np.pi, len(names))))
+    else:
+        cmds, vals, names = circuits.hea(n, 2, seed=int(rng.integers(1 << 30)), entangler="cz")
+        cmds = circuits.brickwork(n, 2, seed=int(rng.integers(1 << 30))) + cmds
+    obs = circuits.random_pauli_sum(n, int(rng.integers(1, 30)), seed=int(rng.integers(1 << 30)),
+                                    max_weight=min(3, n)) + circuits.tfim_chain(n)
+    return cmds, n, obs, vals, names
+
+
+@pytest.mark.gpu
+def test_circuit_batch_energies_and_gradients_against_oracle(restatement):
+    """40 circuits of 2..12 qubits (HEA, QAOA, brickwork + HEA), each with its own observable
+    and parameters, in one graph-captured launch: every <H> and every gradient equals the CPU
+    oracle's adjoint at 1e-10; new parameter values through set() equal it too."""
+    from openqarp_b200.batch import CircuitBatch
+    rng = np.random.default_rng(11)
+    insts = [_random_instance(rng, i) for i in range(40)]
+    b = CircuitBatch(with_gradient=True)
+    try:
+        for cmds, n, obs, vals, names in insts:
+            b.add(cmds, n, obs, vals, names)
+        for rnd in range(2):
+            energies, grads, ms = b.run()
+            assert ms > 0
+            for j, (cmds, n, obs, vals, names) in enumerate(insts):
+                e, g = restatement.adjoint(ir.pack(cmds, vals, names), n, len(names), observable.to_masks(obs, n))
+                assert abs(energies[j] - e) < 1e-10, (rnd, j)
+                np.testing.assert_allclose(grads[j], g, rtol=0, atol=1e-10, err_msg=f"round {rnd} instance {j}")
+            # new parameter values for every other instance, same structure
+            for j in range(0, len(insts), 2):
+                cmds, n, obs, vals, names = insts[j]
+                vals = {k: float(v) + 0.37 for k, v in vals.items()}
+                insts[j] = (cmds, n, obs, vals, names)
+                b.set(j, vals)
+    finally:
+        b.close()
+
+
+@pytest.mark.gpu
+def test_circuit_batch_refuses_wide_registers_and_routes_batch_expectation(restatement):
+    from openqarp_b200 import B200Simulator
+    from openqarp_b200.batch import CircuitBatch
+    from openqarp_b200.errors import CapabilityError
+    b = CircuitBatch(with_gradient=False)
+    try:
+        cmds, vals, names = circuits.hea(13, 1, seed=1)
+        with pytest.raises(CapabilityError, match="1..12 qubits"):
+            b.add(cmds, 13, circuits.tfim_chain(13), vals)
+    finally:
+        b.close()
+    n = 10
+    cmds, vals, names = circuits.hea(n, 3, seed=4)
+    obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, 20, seed=5, max_weight=3)
+    rng = np.random.default_rng(6)
+    sets = [dict(zip(names, rng.uniform(0, 2 * np.pi, len(names)))) for _ in range(64)]
+    sim = B200Simulator()
+    try:
+        got = sim.batch_expectation(cmds, n, obs, sets)
+    finally:
+        sim.close()
+    masks = observable.to_masks(obs, n)
+    want = []
+    for s in sets[:8]:
+        psi = restatement.statevector(ir.pack(cmds, s).buf, n)
+        want.append(restatement.transition(psi, psi, n, masks).real)
+    np.testing.assert_allclose(got[:8], want, rtol=0, atol=1e-10)
+    assert len(got) == 64
