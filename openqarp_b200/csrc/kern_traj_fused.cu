@@ -1083,9 +1083,14 @@ void cb_finalize(CircuitBatch* b) {
     check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch stream");
     check_cuda(cudaEventCreate(&b->e0), "event");
     check_cuda(cudaEventCreate(&b->e1), "event");
-    // the instance's coefficients move with it: steps index the batch-wide table
-    for (CbInstHost& h : b->inst)
-        for (uint32_t s = h.f0; s < h.r1; ++s) b->steps[s].coef += h.coef0;
+    // every step reads its coefficients from the batch-wide table (encode appended each
+    // instance's to it, so the offsets are absolute already): check that every read stays in it
+    for (const FsStep& f : b->steps)
+        if (static_cast<size_t>(f.coef) + f.ncoef > b->coef.size() || f.ncoef > static_cast<uint32_t>(kFsMaxCoef))
+            throw std::logic_error("circuit batch: a step's coefficients lie outside the table");
+    for (const CbInstHost& h : b->inst)
+        for (uint32_t t = h.t0; t < h.t1; ++t)
+            if (t >= b->tx.size()) throw std::logic_error("circuit batch: a term lies outside the table");
     // widest (costliest) instances first: the queue order
     std::vector<size_t> order(b->inst.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = i;
