@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/qsv.h"
 #include "kernels.h"
 #include "lower.h"
@@ -20,6 +22,13 @@ namespace qsv {
 namespace {
 
 thread_local std::string g_err;
+
+// An NVTX range over an entry point: profilers that attach (Nsight Systems, ncu --nvtx) see each
+// call by name; without a tool attached a push/pop is a no-op.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
 
 struct Handle {
     int n = 0;
@@ -563,6 +572,7 @@ int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int dtype, int max_
 }
 
 int qsv_apply(void* hp, const uint8_t* cmds, size_t nbytes) {
+    Range range("qsv_apply");
     return guarded([&] {
         Handle* h = H_(hp);
         if (!cmds && nbytes) throw std::invalid_argument("null command buffer");
@@ -580,6 +590,7 @@ int qsv_apply_unfused(void* hp, const uint8_t* cmds, size_t nbytes) {
 
 int qsv_transition(void* bp, void* kp, const uint64_t* xm, const uint64_t* zm, const double* coeff,
                    size_t nt, double out[2]) {
+    Range range("qsv_transition");
     return guarded([&] {
         Handle* b = H_(bp);
         Handle* k = static_cast<Handle*>(kp);
@@ -627,6 +638,7 @@ int qsv_sample(void* hp, const double* u, size_t n_shots, uint64_t* out) {
 }
 
 int qsv_sample_seeded(void* hp, uint32_t seed, size_t n_shots, uint64_t* out) {
+    Range range("qsv_sample_seeded");
     std::vector<double> u(n_shots);
     int rc = qsv_uniforms(seed, n_shots, u.data());
     if (rc) return rc;
@@ -692,6 +704,7 @@ int qsv_exact_probs(void* hp, double threshold, uint64_t* keys, double* probs, u
 
 int qsv_run_trajectories(void* hp, const uint8_t* cmds, size_t nbytes, uint32_t seed, size_t n_shots,
                          uint64_t* out_idx, uint64_t* out_cbits, int32_t* n_cbits) {
+    Range range("qsv_run_trajectories");
     return guarded([&] {
         Handle* h = H_(hp);
         if (!cmds && nbytes) throw std::invalid_argument("null command buffer");
@@ -828,6 +841,7 @@ int qsv_cbatch_set(void* b, int index, const uint8_t* cmds, size_t nbytes) {
 }
 
 int qsv_cbatch_run(void* b, double* energies, double* grads, double* device_ms) {
+    Range range("qsv_cbatch_run");
     return guarded([&] {
         if (!b) throw std::invalid_argument("null batch");
         cbatch_run(b, energies, grads, device_ms);
@@ -1118,6 +1132,7 @@ extern "C" {
 int qsv_adjoint(void* hp, const uint8_t* cmds, size_t nbytes, const int32_t* dep_ptr,
                 const int32_t* dep_param, const double* dep_alpha, int n_params, const uint64_t* xm,
                 const uint64_t* zm, const double* coeff, size_t nt, double* grad, double* energy) {
+    Range range("qsv_adjoint");
     return guarded([&] {
         Handle* h = H_(hp);
         if (n_params < 0 || (n_params > 0 && !grad)) throw std::invalid_argument("bad gradient output");
