@@ -135,7 +135,8 @@ constexpr int kJitAmps = 1 << kRtRegBits;                 // 16 amplitudes per t
 constexpr int kJitThreads = 1 << (kRtLaneBits + kRtWarpBits);
 constexpr size_t kJitMaxCoefDoubles = 3400;               // kernel parameters stay under 28 KiB
 constexpr int kJitCtasPerSm = 2;                          // complex128: 64 KiB of shared memory, <= 128 registers
-constexpr int kJitCtasPerSmF32 = 2;                       // complex64: 32 KiB, <= 128 registers
+constexpr int kJitCtasPerSmF32 = 3;                       // complex64: 32 KiB, <= 85 registers
+int jit_ctas(bool f32) { return f32 ? kJitCtasPerSmF32 : kJitCtasPerSm; }
 size_t jit_smem(bool f32) { return (size_t{1} << kRtQubits) * (f32 ? 8 : 16); }
 
 uint32_t swz(uint32_t i) { return i ^ ((i >> 3 ^ i >> 6 ^ i >> 9) & 7u); }
@@ -206,6 +207,9 @@ struct Gen {
     // deferred one-qubit phases per local bit: amplitudes with the bit 0 / 1 owe pend[b][0/1]
     c128 pend[kRtQubits][2];
     bool has[kRtQubits] = {};
+    // a factor owed by every amplitude of the tile: the bit-0 phases of normalised tables
+    c128 cglob{1.0, 0.0};
+    int normalised = 0;   // normalised tables since cglob was last applied
     double flops = 0;   // FP64 operations per thread per tile (FMA = 2, MUL = 1)
 
     size_t push(c128 v) {
@@ -288,50 +292,89 @@ struct Gen {
     }
 
     // apply the deferred phases of the local bits now in register slots: one table over those
-    // slots, one complex multiply per amplitude
-    void flush_slots(const RtLayout& L) {
+    // slots, one complex multiply per amplitude.  The table is normalised: each bit's phase
+    // pair pend[b] = (p0, p1) becomes (1, p1 / p0) with p0 joining the tile constant cglob, so
+    // the amplitudes whose slot bits are all 0 need no multiply.  A full table (every entry
+    // times cglob, every amplitude multiplied) ends the pass and, every 16 tables, keeps the
+    // deferred rotation scales (each >= 1/sqrt(2)) from growing the amplitudes past 2^32.
+    void flush_slots(const RtLayout& L, bool full = false) {
         int slots[kRtRegBits], m = 0;
         for (int p = 0; p < kRtRegBits; ++p)
             if (has[L.reg[p]]) slots[m++] = p;
+        if (m > 0 && !full && ++normalised >= 16) full = true;
         uint32_t smask = 0;
         for (int j = 0; j < m; ++j) smask |= 1u << slots[j];
-        mark(0xF1u, smask);
-        if (m == 0) return;
+        mark(full ? 0xF3u : 0xF1u, smask);
+        if (m == 0 && !full) return;
         const size_t at = coef.size();
-        for (int idx = 0; idx < (1 << m); ++idx) {
-            c128 t(1.0, 0.0);
-            for (int j = 0; j < m; ++j) t *= pend[L.reg[slots[j]]][(idx >> j) & 1];
-            push(t);
+        if (full) {
+            for (int idx = 0; idx < (1 << m); ++idx) {
+                c128 t = cglob;
+                for (int j = 0; j < m; ++j) t *= pend[L.reg[slots[j]]][(idx >> j) & 1];
+                push(t);
+            }
+            cglob = c128(1.0, 0.0);
+            normalised = 0;
+            flops += 6.0 * kJitAmps;
+        } else {
+            c128 ratio[kRtRegBits];
+            for (int j = 0; j < m; ++j) {
+                const c128* pb = pend[L.reg[slots[j]]];
+                cglob *= pb[0];
+                ratio[j] = pb[1] / pb[0];
+            }
+            for (int idx = 1; idx < (1 << m); ++idx) {
+                c128 t(1.0, 0.0);
+                for (int j = 0; j < m; ++j)
+                    if ((idx >> j) & 1) t *= ratio[j];
+                push(t);
+            }
+            flops += 6.0 * (kJitAmps - (kJitAmps >> m));
         }
         for (int j = 0; j < m; ++j) has[L.reg[slots[j]]] = false;
-        flops += 6.0 * kJitAmps;
         if (!emit) return;
         for (int r = 0; r < kJitAmps; ++r) {
             int idx = 0;
             for (int j = 0; j < m; ++j) idx |= ((r >> slots[j]) & 1) << j;
-            cmul_into(r, cr(at + 2 * static_cast<size_t>(idx)), ci(at + 2 * static_cast<size_t>(idx)));
+            if (!full && idx == 0) continue;
+            const size_t e = at + 2 * static_cast<size_t>(full ? idx : idx - 1);
+            cmul_into(r, cr(e), ci(e));
         }
     }
 
-    // end of the pass: the deferred phases of lane and warp bits as one factor per thread,
-    // after the slot table
+    // end of the pass: the deferred phases of lane and warp bits as one factor per thread
+    // (starting from the tile constant), after the slot table; without lane or warp phases the
+    // slot table is the full one
     void flush_all(const RtLayout& L) {
-        flush_slots(L);
-        std::vector<std::pair<int, size_t>> bits;   // (place code, coefficient offset)
         uint64_t m = 0;
+        for (int b = 0; b < kRtQubits; ++b) {
+            if (!has[b]) continue;
+            int k = 0;
+            const char w = place(L, b, &k);
+            if (w == 'r') continue;
+            m |= 1ull << ((w == 'l' ? 0 : 16) + k);
+        }
+        mark(0xF2u, m);
+        if (m == 0) {
+            flush_slots(L, true);
+            return;
+        }
+        flush_slots(L);
+        const size_t c0 = push(cglob);
+        cglob = c128(1.0, 0.0);
+        normalised = 0;
+        std::vector<std::pair<int, size_t>> bits;   // (place code, coefficient offset)
         for (int b = 0; b < kRtQubits; ++b) {
             if (!has[b]) continue;
             int k = 0;
             const char w = place(L, b, &k);
             bits.push_back({(w == 'l' ? 0 : 16) + k, push(pend[b][0])});
             push(pend[b][1]);
-            m |= 1ull << ((w == 'l' ? 0 : 16) + k);
             has[b] = false;
         }
-        mark(0xF2u, m);
-        if (!bits.empty()) flops += 6.0 * kJitAmps + 6.0 * static_cast<double>(bits.size());
-        if (bits.empty() || !emit) return;
-        o << "  { R fr = 1, fi = 0;\n";
+        flops += 6.0 * kJitAmps + 6.0 * static_cast<double>(bits.size());
+        if (!emit) return;
+        o << "  { R fr = " << cr(c0) << ", fi = " << ci(c0) << ";\n";
         for (const auto& [code, at] : bits) {
             const std::string on = code < 16 ? "((lane >> " + std::to_string(code) + ") & 1u)"
                                               : "((warp >> " + std::to_string(code - 16) + ") & 1u)";
@@ -379,6 +422,21 @@ struct Gen {
             if (!emit) continue;
             const int B = 1 << p;
             std::ostringstream a, bb;
+            if (f32) {
+                // complex64: each amplitude is one float2, and a rotation updates both of its
+                // components with one packed FMA (__ffma2_rn, rounding as fmaf per component)
+                for (int g = 0; g < kJitAmps; ++g) {
+                    if (g & B) continue;
+                    const std::string x0 = "a" + std::to_string(g), x1 = "a" + std::to_string(g | B);
+                    a << "    { const R2 y0 = " << x0 << "; " << x0 << " = __ffma2_rn(nt2, " << x1 << ", y0); "
+                      << x1 << " = __ffma2_rn(t2, y0, " << x1 << "); }\n";
+                    bb << "    { const R2 y0 = " << x0 << "; " << x0 << " = __ffma2_rn(t2, y0, make_float2(-" << x1
+                       << ".x, -" << x1 << ".y)); " << x1 << " = __ffma2_rn(t2, " << x1 << ", y0); }\n";
+                }
+                o << "  { const R t = " << cr(at) << "; const R2 t2 = make_float2(t, t), nt2 = make_float2(-t, -t);\n"
+                  << "  if (" << ci(at) << " != 0) {\n" << bb.str() << "  } else {\n" << a.str() << "  } }\n";
+                continue;
+            }
             for (int g = 0; g < kJitAmps; ++g) {
                 if (g & B) continue;
                 const int h = g | B;
@@ -716,8 +774,9 @@ bool walk_pass(const TilePass& pass, const RtPlan& plan, int n, Gen* g, RtLayout
 
 // Source of one pass kernel (qsv_jit_<idx>) from a walk with emit on.  Complex128: 16-byte
 // amplitudes, 16 staged copies of one amplitude per thread, 64 KiB of shared memory, two CTAs
-// per SM.  Complex64: 8-byte amplitudes, 8 staged copies of two amplitudes per thread, 32 KiB,
-// two CTAs per SM (three would cap registers at 85 and spill).
+// per SM.  Complex64: 8-byte amplitudes held as float2 (packed FMAs), 8 staged copies of two
+// amplitudes per thread, 32 KiB, three CTAs per SM (85 registers; 31.6 ms against 34.4 ms with
+// two on the 28-qubit brickwork, and four no faster).
 std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx, const std::string& steps,
                         size_t n_coef, const RtLayout& F, bool f32) {
     const size_t nc = std::max<size_t>(n_coef, 1);
@@ -765,12 +824,14 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
         return x.str();
     };
     std::ostringstream s;
-    if (f32)
+    if (f32) {
         s << "typedef float R; typedef float2 R2;\n#define FMA fmaf\n#define MK make_float2\n";
-    else
+        for (int r = 0; r < kJitAmps; ++r) s << "#define a" << r << "r a" << r << ".x\n#define a" << r << "i a" << r << ".y\n";
+    } else {
         s << "typedef double R; typedef double2 R2;\n#define FMA fma\n#define MK make_double2\n";
+    }
     s << "struct __align__(8) C" << idx << " { R c[" << nc << "]; };\n"
-      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", " << (f32 ? kJitCtasPerSmF32 : kJitCtasPerSm)
+      << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", " << jit_ctas(f32)
       << ") qsv_jit_" << idx << "(R2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P) {\n"
       << "  extern __shared__ __align__(16) unsigned char smem[];\n"
       << "  double2* xb = reinterpret_cast<double2*>(smem);\n"
@@ -786,8 +847,15 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
       << "  const u64 base = " << deposit("t") << ";\n"
       << "  asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n"
       << "  __syncthreads();\n"
-      << "  R ";
-    for (int r = 0; r < kJitAmps; ++r) s << (r ? ", " : "") << Gen::ar(r) << ", " << Gen::ai(r);
+      << "  ";
+    if (f32) {
+        // complex64 amplitudes are float2 pairs (packed FMAs); aNr / aNi name their halves
+        s << "R2 ";
+        for (int r = 0; r < kJitAmps; ++r) s << (r ? ", a" : "a") << r;
+    } else {
+        s << "R ";
+        for (int r = 0; r < kJitAmps; ++r) s << (r ? ", " : "") << Gen::ar(r) << ", " << Gen::ai(r);
+    }
     s << ";\n  { " << Gen::slot_setup(plan.load, f32) << "\n";
     for (int r = 0; r < kJitAmps; ++r)
         s << "    { const R2 x = " << Gen::slot_of(plan.load, r, f32) << "; " << Gen::ar(r) << " = x.x; "
@@ -922,7 +990,7 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
     std::vector<RtPlan> plans(passes.size());
     for (size_t i = 0; i < passes.size(); ++i) {
         if (passes[i]->tile_qubits.empty()) continue;
-        if (!plan_rt(*passes[i], &plans[i])) continue;
+        if (!plan_rt(*passes[i], &plans[i], f32 ? 8 : 16)) continue;
         std::vector<double> coef;
         uint64_t sig = 0;
         std::string unused;
@@ -1011,7 +1079,7 @@ void jit_launch(const JitPlan& plan, int pass, void* s, int n, cudaStream_t st) 
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
     unsigned long long n_tiles = 1ull << (n - kRtQubits);
     const unsigned grid = static_cast<unsigned>(
-        std::min<unsigned long long>(n_tiles, static_cast<unsigned long long>(plan.f32 ? kJitCtasPerSmF32 : kJitCtasPerSm) * sms));
+        std::min<unsigned long long>(n_tiles, static_cast<unsigned long long>(jit_ctas(plan.f32)) * sms));
     const std::vector<uint8_t>& c = plan.coef[static_cast<size_t>(k)];
     void* args[] = {&s, &n_tiles, const_cast<uint8_t*>(c.data())};
     check_cu(driver().launch(static_cast<CUfunction>(plan.fns[static_cast<size_t>(k)]), grid, 1, 1, kJitThreads, 1, 1,
@@ -1025,7 +1093,7 @@ std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int 
     int next = 0;
     for (size_t i = 0; i < passes.size(); ++i) {
         RtPlan plan;
-        if (!plan_rt(*passes[i], &plan)) continue;
+        if (!plan_rt(*passes[i], &plan, f32 ? 8 : 16)) continue;
         std::string ps;
         std::vector<double> coef;
         uint64_t sig = 0;

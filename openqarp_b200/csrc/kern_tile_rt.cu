@@ -592,7 +592,7 @@ RtUpload encode_rt(const std::vector<const TilePass*>& passes, cudaStream_t st, 
     for (const TilePass* pp : passes) {
         const TilePass& p = *pp;
         RtPlan plan;
-        if (!plan_rt(p, &plan)) throw std::logic_error("pass is not register-tile capable");
+        if (!plan_rt(p, &plan, static_cast<int>(sizeof(vec2_t<T>)))) throw std::logic_error("pass is not register-tile capable");
         int local_of[64];
         for (int q = 0; q < 64; ++q) local_of[q] = -1;
         for (int j = 0; j < kRtQubits; ++j) local_of[p.tile_qubits[j]] = j;

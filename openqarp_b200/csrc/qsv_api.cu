@@ -175,7 +175,9 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
         const int m = h->tile_qubits > 0 ? std::min(h->tile_qubits, h->n)
                       : (h->executor == 1 || h->executor == 3) ? std::min(kRtQubits, h->n)
                                                                : default_tile_qubits(h->n, static_cast<int>(h->amp_bytes()));
-        const std::vector<TilePass> passes = plan_tiles(ops, h->n, m);
+        // the compiled passes generate their own addressing and need only line-sized runs
+        const int low = h->executor == 3 ? coalesced_low_qubits(static_cast<int>(h->amp_bytes())) : kTileLowQubits;
+        const std::vector<TilePass> passes = plan_tiles(ops, h->n, m, low);
         auto stream_op = [h](const Op& o) { launch(h, o, h->state); };
         const bool rt = h->executor == 1 || h->executor == 3;
         const bool jit = h->executor == 3;
@@ -553,11 +555,12 @@ int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int dtype, int max_
         std::vector<Op> ops;
         for (const Cmd& c : fuse_for_dispatch(decode(cmds, nbytes), n, max_q, min_q))
             for (Op& o : lower(c, n)) ops.push_back(std::move(o));
-        const std::vector<TilePass> passes = plan_tiles(ops, n, kRtQubits);
+        if (dtype != QSV_C128 && dtype != QSV_C64) throw std::invalid_argument("dtype must be QSV_C128 or QSV_C64");
+        const std::vector<TilePass> passes =
+            plan_tiles(ops, n, kRtQubits, coalesced_low_qubits(dtype == QSV_C128 ? 16 : 8));
         std::vector<const TilePass*> ptrs;
         for (const TilePass& p : passes) ptrs.push_back(&p);
         size_t k = 0;
-        if (dtype != QSV_C128 && dtype != QSV_C64) throw std::invalid_argument("dtype must be QSV_C128 or QSV_C64");
         const std::string src = jit_source_for_test(ptrs, n, dtype == QSV_C64, &k);
         if (const char* dump = std::getenv("QSV_JIT_DUMP")) {
             if (FILE* f = std::fopen(dump, "w")) {

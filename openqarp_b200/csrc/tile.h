@@ -26,8 +26,9 @@ struct TilePlanOp {
 };
 
 struct TilePass {
-    std::vector<uint32_t> tile_qubits;   // local bit j <-> tile_qubits[j]; first c are 0..c-1
+    std::vector<uint32_t> tile_qubits;   // local bit j <-> tile_qubits[j]; first `low` are 0..low-1
     std::vector<Op> ops;                 // in application order
+    int low = kTileLowQubits;            // contiguous low qubits the planner put in the tile
 };
 
 // Non-diagonal qubits of an op: the ones it mixes amplitudes across.
@@ -36,6 +37,12 @@ uint64_t op_mixing_mask(const Op& op);
 uint64_t op_support_mask(const Op& op);
 
 std::vector<TilePass> plan_tiles(const std::vector<Op>& ops, int n, int m, int c = kTileLowQubits);
+
+// Contiguous low qubits in the tiles of the compiled register-tile passes: one 128-byte line
+// per run (8 complex128 or 16 complex64 amplitudes), so loads and stores stay whole-line while
+// every other tile qubit is free for the circuit.  On a 28-qubit brickwork, 12-qubit tiles then
+// take 16 passes (complex128) instead of the 25 that five mandatory low qubits leave.
+inline int coalesced_low_qubits(int amp_bytes) { return amp_bytes == 16 ? 3 : 4; }
 
 // ---------------------------------------------------------------- register-resident tiles
 // The register-tile kernel (kern_tile_rt.cu) holds a 2^12-amplitude tile in the registers of
@@ -81,8 +88,9 @@ struct RtPlan {
 };
 
 // Plan one tile pass for the register-tile kernel; false when the pass has an op the kernel
-// cannot apply in registers (then the shared-memory tile kernel runs it).
-bool plan_rt(const TilePass& pass, RtPlan* out);
+// cannot apply in registers (then the shared-memory tile kernel runs it).  The layouts'
+// lanes follow the storage type's shared-memory banks (amp_bytes 16 or 8).
+bool plan_rt(const TilePass& pass, RtPlan* out, int amp_bytes = 16);
 
 // Tiles per register width and storage: 2^12 complex128 or 2^13 complex64 (64 KiB).
 inline int default_tile_qubits(int n, int amp_bytes) {

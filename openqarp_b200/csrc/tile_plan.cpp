@@ -80,6 +80,7 @@ std::vector<TilePass> plan_tiles(const std::vector<Op>& ops_in, int n, int m, in
         int width = c;
         uint64_t blocked = 0;
         TilePass pass;
+        pass.low = c;
         std::vector<Op> deferred;
         deferred.reserve(remaining.size());
         for (Op& o : remaining) {
@@ -144,36 +145,48 @@ bool rt_capable(const Op& o, uint32_t mix) {
     }
 }
 
-// lanes cover all three residues of the local bit index mod 3: the shared-memory swizzle
-// then spreads a warp's 16-byte accesses over all eight bank groups
-bool residues_covered(const uint8_t* lane) {
-    int seen = 0;
-    for (int k = 0; k < kRtLaneBits; ++k) seen |= 1 << (lane[k] % 3);
-    return seen == 7;
+// Lanes of a transpose layout, chosen for the shared-memory banks.  Amplitude (local index i)
+// sits in 16-byte slot swz(i) (complex128) or in half i & 1 of 16-byte chunk swz(i >> 1)
+// (complex64), and swz XOR-folds the index in groups of three bits, so local bit b moves an
+// access to bank group b mod 3 (complex128) or, for b >= 1, (b - 1) mod 3 (complex64; bit 0
+// picks the 8-byte half).  A warp's 16-byte accesses are served eight lanes at a time and its
+// 8-byte accesses sixteen at a time: the first three lanes (complex128) or four (complex64:
+// bit 0 and one bit of each class) must span every group for one wavefront per phase.  The
+// classes are filled with the lowest free bits; the other lanes take the lowest bits left.
+void choose_lanes(uint32_t used, int amp_bytes, uint8_t* lane) {
+    const bool c64 = amp_bytes == 8;
+    int k = 0;
+    auto take = [&](int b) {
+        lane[k++] = static_cast<uint8_t>(b);
+        used |= 1u << b;
+    };
+    if (c64 && !(used & 1u)) take(0);
+    for (int cls = 0; cls < 3; ++cls)
+        for (int b = c64 ? 1 : 0; b < kRtQubits; ++b)
+            if (!((used >> b) & 1) && (c64 ? (b - 1) % 3 : b % 3) == cls) {
+                take(b);
+                break;
+            }
+    for (int b = 0; b < kRtQubits && k < kRtLaneBits; ++b)
+        if (!((used >> b) & 1)) take(b);
 }
 
-// A layout with the given register bits; lanes are the lowest remaining bits (local bits 0..4
-// when the register bits are all high, the form loads and stores want), traded for a higher
-// bit when that leaves a residue mod 3 uncovered; warps take the rest.
-RtLayout make_layout(const std::vector<int>& reg_bits, bool store_form) {
+// A layout with the given register bits.  The store form's lanes are local bits 0..4 in order
+// (32 consecutive amplitudes per warp: whole lines to HBM, and conflict-free for both storage
+// types); other layouts take bank-spreading lanes (choose_lanes); warps take the rest.
+RtLayout make_layout(const std::vector<int>& reg_bits, bool store_form, int amp_bytes) {
     RtLayout L{};
     uint32_t used = 0;
     for (int p = 0; p < kRtRegBits; ++p) {
         L.reg[p] = static_cast<uint8_t>(reg_bits[p]);
         used |= 1u << reg_bits[p];
     }
-    std::vector<int> rest;
-    for (int b = 0; b < kRtQubits; ++b)
-        if (!((used >> b) & 1)) rest.push_back(b);
-    for (int k = 0; k < kRtLaneBits; ++k) L.lane[k] = static_cast<uint8_t>(rest[k]);
-    if (!store_form && !residues_covered(L.lane)) {
-        for (int w = kRtLaneBits; w < static_cast<int>(rest.size()) && !residues_covered(L.lane); ++w)
-            for (int k = kRtLaneBits - 1; k >= 0; --k) {
-                const uint8_t keep = L.lane[k];
-                L.lane[k] = static_cast<uint8_t>(rest[w]);
-                if (residues_covered(L.lane)) break;
-                L.lane[k] = keep;
-            }
+    if (store_form) {
+        int k = 0;
+        for (int b = 0; b < kRtQubits && k < kRtLaneBits; ++b)
+            if (!((used >> b) & 1)) L.lane[k++] = static_cast<uint8_t>(b);
+    } else {
+        choose_lanes(used, amp_bytes, L.lane);
     }
     uint32_t taken = used;
     for (int k = 0; k < kRtLaneBits; ++k) taken |= 1u << L.lane[k];
@@ -192,9 +205,11 @@ int slot_of_bit(const RtLayout& l, int b) {
 
 }  // namespace
 
-bool plan_rt(const TilePass& pass, RtPlan* out) {
+bool plan_rt(const TilePass& pass, RtPlan* out, int amp_bytes) {
     if (static_cast<int>(pass.tile_qubits.size()) != kRtQubits) return false;
-    for (int j = 0; j < kTileLowQubits; ++j)
+    // loads and stores move runs of at least 8 consecutive amplitudes (128 or 64 bytes)
+    if (pass.low < 3) return false;
+    for (int j = 0; j < pass.low; ++j)
         if (pass.tile_qubits[j] != static_cast<uint32_t>(j)) return false;
     int local_of[64];
     for (int q = 0; q < 64; ++q) local_of[q] = -1;
@@ -299,7 +314,7 @@ bool plan_rt(const TilePass& pass, RtPlan* out) {
     out->steps.clear();
     out->transposes = 0;
     // the tile is read from the staging buffer straight into the first layout chosen
-    RtLayout L = make_layout(choose(0), false);
+    RtLayout L = make_layout(choose(0), false, amp_bytes);
     out->load = L;
     size_t remaining = 0;
     for (size_t i = 0; i < n_ops; ++i) {
@@ -371,7 +386,7 @@ bool plan_rt(const TilePass& pass, RtPlan* out) {
         for (int b : bits) m |= 1u << b;
         if (m == before && !progress) throw std::logic_error("register-tile planner made no progress");
         if (m == before) continue;
-        L = make_layout(bits, false);
+        L = make_layout(bits, false, amp_bytes);
         RtStep st;
         st.kind = RT_XPOSE;
         st.layout = L;
@@ -394,7 +409,7 @@ bool plan_rt(const TilePass& pass, RtPlan* out) {
                 sb.push_back(b);
                 got |= 1u << b;
             }
-        L = make_layout(sb, true);
+        L = make_layout(sb, true, amp_bytes);
         RtStep st;
         st.kind = RT_XPOSE;
         st.layout = L;
