@@ -195,6 +195,22 @@ Factor1q factor_1q(const std::vector<c128>& u) {
     return f;
 }
 
+// A deferred one-qubit phase pair on global qubit q: amplitudes with the bit 0 / 1 owe p[0/1].
+struct QubitPhase {
+    int q = 0;
+    c128 p[2];
+};
+
+// What one compiled pass hands to the next of its chain instead of applying it: the deferred
+// phases of the qubits it touched (and those it carried through untouched), and the tile
+// constant with its table count.  Every amplitude of the register owes the same factors, so
+// the next pass can fold them into its own tables.
+struct Carry {
+    std::vector<QubitPhase> phases;   // ascending q, at most one entry per qubit
+    c128 cglob{1.0, 0.0};
+    int normalised = 0;
+};
+
 // Code generator of one pass.  With emit off it only walks the plan, collecting the
 // coefficients and the structural signature (everything the source depends on), so a pass
 // whose kernel is already compiled costs no source generation.
@@ -342,11 +358,12 @@ struct Gen {
         }
     }
 
-    // end of the pass: the deferred phases of lane and warp bits as one factor per thread
-    // (starting from the tile constant), after the slot table; without lane or warp phases the
-    // slot table is the full one
-    void flush_all(const RtLayout& L) {
-        uint64_t m = 0;
+    // end of a chain of passes: the deferred phases of lane and warp bits, and those carried
+    // in on qubits outside the tile (constants of the tile's base index), as one factor per
+    // thread (starting from the tile constant), after the slot table; without lane, warp or
+    // outside phases the slot table is the full one
+    void flush_all(const RtLayout& L, const std::vector<QubitPhase>& outside = {}) {
+        uint64_t m = 0, om = 0;
         for (int b = 0; b < kRtQubits; ++b) {
             if (!has[b]) continue;
             int k = 0;
@@ -354,8 +371,10 @@ struct Gen {
             if (w == 'r') continue;
             m |= 1ull << ((w == 'l' ? 0 : 16) + k);
         }
+        for (const QubitPhase& x : outside) om |= 1ull << x.q;
         mark(0xF2u, m);
-        if (m == 0) {
+        mark(0xF4u, om);
+        if (m == 0 && om == 0) {
             flush_slots(L, true);
             return;
         }
@@ -372,12 +391,17 @@ struct Gen {
             push(pend[b][1]);
             has[b] = false;
         }
+        for (const QubitPhase& x : outside) {
+            bits.push_back({64 + x.q, push(x.p[0])});
+            push(x.p[1]);
+        }
         flops += 6.0 * kJitAmps + 6.0 * static_cast<double>(bits.size());
         if (!emit) return;
         o << "  { R fr = " << cr(c0) << ", fi = " << ci(c0) << ";\n";
         for (const auto& [code, at] : bits) {
-            const std::string on = code < 16 ? "((lane >> " + std::to_string(code) + ") & 1u)"
-                                              : "((warp >> " + std::to_string(code - 16) + ") & 1u)";
+            const std::string on = code >= 64 ? "((base >> " + std::to_string(code - 64) + ") & 1ull)"
+                                   : code < 16 ? "((lane >> " + std::to_string(code) + ") & 1u)"
+                                               : "((warp >> " + std::to_string(code - 16) + ") & 1u)";
             o << "    { const bool on = " << on << "; const R pr = on ? " << cr(at + 2) << " : " << cr(at)
               << ", pi = on ? " << ci(at + 2) << " : " << ci(at) << "; const R nr = fr * pr - fi * pi;"
               << " fi = fr * pi + fi * pr; fr = nr; }\n";
@@ -705,13 +729,36 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
 // Walk one pass's plan: coefficients, structural signature and (with emit) the steps' source.
 // Returns false when the pass needs an op the generator does not handle or too many
 // coefficients.
-bool walk_pass(const TilePass& pass, const RtPlan& plan, int n, Gen* g, RtLayout* last) {
+// A pass of a chain starts from the carry of the pass before (cin: phases on its tile qubits
+// become its own deferred phases, the others pass through) and, unless it ends the chain,
+// hands its deferred phases on (cout) instead of applying them.
+bool walk_pass(const TilePass& pass, const RtPlan& plan, int n, Gen* g, RtLayout* last, const Carry* cin,
+               bool final, Carry* cout) {
     if (!jit_capable(plan)) return false;
     for (int q = 0; q < 64; ++q) g->local_of[q] = -1;
     for (int j = 0; j < kRtQubits; ++j) g->local_of[pass.tile_qubits[j]] = j;
     g->mark(static_cast<uint64_t>(n), 0x715Eu);
     for (int j = 0; j < kRtQubits; ++j) g->mark(pass.tile_qubits[j]);
     g->mark_layout(plan.load);
+    std::vector<QubitPhase> through;   // carried phases of qubits outside the tile
+    if (cin) {
+        uint64_t in_mask = 0;
+        for (const QubitPhase& x : cin->phases) {
+            const int b = g->local_of[x.q];
+            if (b >= 0) {
+                g->pend[b][0] = x.p[0];
+                g->pend[b][1] = x.p[1];
+                g->has[b] = true;
+            } else {
+                through.push_back(x);
+            }
+            in_mask |= 1ull << x.q;
+        }
+        g->cglob = cin->cglob;
+        g->normalised = cin->normalised;
+        g->mark(0xCA11u, in_mask);
+        g->mark(static_cast<uint64_t>(cin->normalised), final ? 1u : 0u);
+    }
     RtLayout L = plan.load;
     bool first_move = true;
     const size_t ns = plan.steps.size();
@@ -767,7 +814,24 @@ bool walk_pass(const TilePass& pass, const RtPlan& plan, int n, Gen* g, RtLayout
             default: return false;
         }
     }
-    g->flush_all(L);
+    if (final || !cout) {
+        g->flush_all(L, through);
+    } else {
+        cout->phases = through;
+        for (int b = 0; b < kRtQubits; ++b)
+            if (g->has[b]) {
+                QubitPhase x;
+                x.q = static_cast<int>(pass.tile_qubits[b]);
+                x.p[0] = g->pend[b][0];
+                x.p[1] = g->pend[b][1];
+                cout->phases.push_back(x);
+            }
+        std::sort(cout->phases.begin(), cout->phases.end(),
+                  [](const QubitPhase& a, const QubitPhase& b) { return a.q < b.q; });
+        cout->cglob = g->cglob;
+        cout->normalised = g->normalised;
+        g->mark(0xCA12u);
+    }
     *last = L;
     return g->coef.size() <= kJitMaxCoefDoubles;
 }
@@ -881,13 +945,14 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
 
 // Source (with emit) or only the signature and coefficients (without) of one pass.
 bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emit, bool f32, std::string* src,
-              std::vector<double>* coef, uint64_t* sig_hash, double* flops_per_amp = nullptr) {
+              std::vector<double>* coef, uint64_t* sig_hash, double* flops_per_amp = nullptr,
+              const Carry* cin = nullptr, bool final = true, Carry* cout = nullptr) {
     Gen g;
     g.emit = emit;
     g.f32 = f32;
     g.mark(f32 ? 0xF32u : 0xF64u);
     RtLayout last{};
-    if (!walk_pass(pass, plan, n, &g, &last)) return false;
+    if (!walk_pass(pass, plan, n, &g, &last, cin, final, cout)) return false;
     uint64_t h = 1469598103934665603ull;
     for (uint64_t v : g.sig)
         for (int b = 0; b < 8; ++b) {
@@ -965,6 +1030,57 @@ std::vector<char> compile_cubin(const std::string& src, int cc_major, int cc_min
     return cubin;
 }
 
+// Walk every pass of a plan without emitting source.  Consecutive compiled passes form a
+// chain: each hands its deferred phases to the next (one fewer full-register multiply per
+// pass, and the next pass's first table absorbs them), and the chain's last pass applies
+// everything owed.  A pass that breaks a chain (not compiled, or a stream pass) ends it.  If a
+// pass fails only with carried phases (too many coefficients), the plan is walked without
+// carrying.
+struct PassWalk {
+    bool ok = false;
+    uint64_t sig = 0;
+    std::vector<double> coef;
+    double flops_per_amp = 0;
+    bool has_cin = false;
+    Carry cin;
+    bool final = true;
+};
+
+std::vector<PassWalk> walk_all(const std::vector<const TilePass*>& passes, std::vector<RtPlan>& plans, int n,
+                               bool f32) {
+    const size_t np = passes.size();
+    plans.assign(np, RtPlan{});
+    std::vector<PassWalk> alone(np);
+    for (size_t i = 0; i < np; ++i) {
+        if (passes[i]->tile_qubits.empty()) continue;
+        if (!plan_rt(*passes[i], &plans[i], f32 ? 8 : 16)) continue;
+        std::string unused;
+        PassWalk& w = alone[i];
+        w.ok = gen_pass(*passes[i], plans[i], n, 0, false, f32, &unused, &w.coef, &w.sig, &w.flops_per_amp);
+    }
+    std::vector<PassWalk> chained(np);
+    Carry cur;
+    bool in_chain = false;
+    for (size_t i = 0; i < np; ++i) {
+        if (!alone[i].ok) {
+            in_chain = false;
+            continue;
+        }
+        PassWalk& w = chained[i];
+        w.final = !(i + 1 < np && alone[i + 1].ok);
+        w.has_cin = in_chain;
+        if (in_chain) w.cin = cur;
+        Carry next;
+        std::string unused;
+        w.ok = gen_pass(*passes[i], plans[i], n, 0, false, f32, &unused, &w.coef, &w.sig, &w.flops_per_amp,
+                        w.has_cin ? &w.cin : nullptr, w.final, w.final ? nullptr : &next);
+        if (!w.ok) return alone;
+        cur = std::move(next);
+        in_chain = !w.final;
+    }
+    return chained;
+}
+
 std::mutex g_jit_mu;
 // compiled pass kernels, by (source hash, context); modules stay loaded until exit
 std::map<std::pair<uint64_t, CUcontext>, CUfunction> g_kernels;
@@ -987,28 +1103,24 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
     // walk every pass without emitting source: its signature finds a compiled kernel
     std::vector<size_t> pass_of;
     std::vector<uint64_t> sigs;
-    std::vector<RtPlan> plans(passes.size());
+    std::vector<RtPlan> plans;
+    std::vector<PassWalk> walks = walk_all(passes, plans, n, f32);
     for (size_t i = 0; i < passes.size(); ++i) {
-        if (passes[i]->tile_qubits.empty()) continue;
-        if (!plan_rt(*passes[i], &plans[i], f32 ? 8 : 16)) continue;
-        std::vector<double> coef;
-        uint64_t sig = 0;
-        std::string unused;
-        double fpa = 0;
-        if (!gen_pass(*passes[i], plans[i], n, 0, false, f32, &unused, &coef, &sig, &fpa)) continue;
-        out.flops_per_amp.push_back(fpa);
-        sig ^= (static_cast<uint64_t>(major) << 56) ^ (static_cast<uint64_t>(minor) << 48);
+        PassWalk& w = walks[i];
+        if (!w.ok) continue;
+        out.flops_per_amp.push_back(w.flops_per_amp);
+        const uint64_t sig = w.sig ^ (static_cast<uint64_t>(major) << 56) ^ (static_cast<uint64_t>(minor) << 48);
         out.idx[i] = static_cast<int>(sigs.size());
         sigs.push_back(sig);
         pass_of.push_back(i);
         // kernel parameters in the storage type's precision
         std::vector<uint8_t> arg;
         if (f32) {
-            std::vector<float> c(coef.begin(), coef.end());
+            std::vector<float> c(w.coef.begin(), w.coef.end());
             arg.assign(reinterpret_cast<const uint8_t*>(c.data()), reinterpret_cast<const uint8_t*>(c.data() + c.size()));
         } else {
-            arg.assign(reinterpret_cast<const uint8_t*>(coef.data()),
-                       reinterpret_cast<const uint8_t*>(coef.data() + coef.size()));
+            arg.assign(reinterpret_cast<const uint8_t*>(w.coef.data()),
+                       reinterpret_cast<const uint8_t*>(w.coef.data() + w.coef.size()));
         }
         out.coef.push_back(std::move(arg));
     }
@@ -1026,9 +1138,12 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
         std::vector<size_t> todo;
         for (size_t j = 0; j < missing.size(); ++j) {
             const size_t i = pass_of[missing[j]];
+            const PassWalk& w = walks[i];
             std::vector<double> coef;
             uint64_t sig = 0;
-            gen_pass(*passes[i], plans[i], n, 0, true, f32, &srcs[j], &coef, &sig);
+            Carry next;
+            gen_pass(*passes[i], plans[i], n, 0, true, f32, &srcs[j], &coef, &sig, nullptr,
+                     w.has_cin ? &w.cin : nullptr, w.final, w.final ? nullptr : &next);
             srcs[j] = std::string(kPrelude) + srcs[j] + tag;
             char name[40];
             std::snprintf(name, sizeof name, "%016llx.cubin", static_cast<unsigned long long>(fnv1a(srcs[j])));
@@ -1091,13 +1206,18 @@ void jit_launch(const JitPlan& plan, int pass, void* s, int n, cudaStream_t st) 
 std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int n, bool f32, size_t* n_kernels) {
     std::string src = kPrelude;
     int next = 0;
+    std::vector<RtPlan> plans;
+    const std::vector<PassWalk> walks = walk_all(passes, plans, n, f32);
     for (size_t i = 0; i < passes.size(); ++i) {
-        RtPlan plan;
-        if (!plan_rt(*passes[i], &plan, f32 ? 8 : 16)) continue;
+        const PassWalk& w = walks[i];
+        if (!w.ok) continue;
         std::string ps;
         std::vector<double> coef;
         uint64_t sig = 0;
-        if (!gen_pass(*passes[i], plan, n, next, true, f32, &ps, &coef, &sig)) continue;
+        Carry out;
+        if (!gen_pass(*passes[i], plans[i], n, next, true, f32, &ps, &coef, &sig, nullptr, w.has_cin ? &w.cin : nullptr,
+                      w.final, w.final ? nullptr : &out))
+            continue;
         if (next > 0) {
             // one program holds every pass: the type definitions come once, with the first
             const size_t cut = ps.find("struct __align__");
