@@ -381,6 +381,21 @@ QSV_API int qsv_stats(void* h, qsv_stats_t* out);
 QSV_API int qsv_device_info(int device, char* name, size_t cap, int* cc_major, int* cc_minor,
                             int* sm_count);
 
+/* ---- bounds-checked debug build ------------------------------------------------------ *
+ * No reference counterpart (the reference has no device code).  libqsv_debug.so (make
+ * DEBUG_BOUNDS=1) checks every instrumented global access of its kernels against the device
+ * buffers the library holds (and, during qsv_transition_static, the caller's two registers); an
+ * access outside all of them is sent to a sink buffer instead and counted, and the entry point
+ * that launched it returns QSV_ERUNTIME with the address and source line in qsv_last_error().
+ * Every entry point of the debug build synchronises the device.  The compiled tile passes check
+ * their amplitude indices against the register instead.
+ * qsv_debug_bounds_selftest: on `device`, a one-thread kernel reads one amplitude inside a 1 KiB
+ * range the checks know and one 2 KiB past it (inside the 4 KiB buffer the self-test allocated,
+ * so no read can leave device memory even if a check were wrong); *caught_in and *caught_out
+ * say whether each read was flagged (a working build gives 0 and 1).  The release build returns
+ * QSV_ECAPABILITY. */
+QSV_API int qsv_debug_bounds_selftest(int device, int32_t* caught_in, int32_t* caught_out);
+
 /* ---- per-pass device timing ---------------------------------------------------------- *
  * No reference counterpart (the reference times nothing below a whole call).  With timing on,
  * every gate pass the handle launches (stream passes, tile passes, the single-CTA small-register

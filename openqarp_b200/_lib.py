@@ -60,6 +60,7 @@ def _load():
         "qsv_fuse_count": (c_int, [P8, c_size_t, c_int, c_int, c_int, PI32, PI32]),
         "qsv_fuse_plan": (c_int, [P8, c_size_t, c_int, c_int, c_int, c_void_p, c_size_t, POINTER(c_size_t)]),
         "qsv_tile_plan_count": (c_int, [P8, c_size_t, c_int, c_int, c_int, c_int, PI32, PI32]),
+        "qsv_debug_bounds_selftest": (c_int, [c_int, PI32, PI32]),
         "qsv_jit_check": (c_int, [P8, c_size_t, c_int, c_int, c_int, c_int, c_int, c_int, PI32, PI32, PU64]),
         "qsv_apply": (c_int, [c_void_p, P8, c_size_t]),
         "qsv_apply_unfused": (c_int, [c_void_p, P8, c_size_t]),
@@ -107,7 +108,7 @@ lib = _load()
 DECLARED = (
     "qsv_last_error", "qsv_abi_version", "qsv_create", "qsv_destroy", "qsv_set_fusion",
     "qsv_set_executor", "qsv_set_tile_qubits", "qsv_set_checkpoint_interval", "qsv_reset", "qsv_set_state", "qsv_get_state", "qsv_device_state",
-    "qsv_copy_state", "qsv_fuse_count", "qsv_fuse_plan", "qsv_tile_plan_count", "qsv_jit_check", "qsv_apply", "qsv_apply_unfused", "qsv_transition", "qsv_sample",
+    "qsv_copy_state", "qsv_fuse_count", "qsv_fuse_plan", "qsv_tile_plan_count", "qsv_jit_check", "qsv_debug_bounds_selftest", "qsv_apply", "qsv_apply_unfused", "qsv_transition", "qsv_sample",
     "qsv_sample_seeded", "qsv_uniforms", "qsv_sample_parities", "qsv_exact_probs", "qsv_set_noise", "qsv_set_trajectory_batch", "qsv_run_trajectories", "qsv_adjoint", "qsv_adjoint_phi", "qsv_norm2",
     "qsv_scale", "qsv_inner", "qsv_synchronize", "qsv_stats", "qsv_device_info", "qsv_set_timing",
     "qsv_pass_times", "qsv_transition_static",

@@ -91,13 +91,13 @@ __global__ void __launch_bounds__(kThreads, (dense_min_blocks<T, K>()))
     if constexpr (C != 0) base |= a.ctrl;
     vec2_t<T> in[D];
 #pragma unroll
-    for (int l = 0; l < D; ++l) in[l] = __ldcs(s + (base | a.off[l]));
+    for (int l = 0; l < D; ++l) in[l] = __ldcs(QSV_DBG(s + (base | a.off[l])));
 #pragma unroll
     for (int y = 0; y < D; ++y) {
         vec2_t<T> acc = cmul<T>(a.m[y * D], in[0]);
 #pragma unroll
         for (int x = 1; x < D; ++x) acc = cfma<T>(a.m[y * D + x], in[x], acc);
-        __stcs(s + (base | a.off[y]), acc);
+        __stcs(QSV_DBG(s + (base | a.off[y])), acc);
     }
 }
 
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kThreads, (K <= 3 ? 4 : 3))   // 4 qubits: bot
     uint64_t in[D], sw[D];
 #pragma unroll
     for (int l = 0; l < D; ++l) {
-        const float2 v = __ldcs(s + (base | a.off[l]));
+        const float2 v = __ldcs(QSV_DBG(s + (base | a.off[l])));
         in[l] = pack_f32x2(v.x, v.y);
         sw[l] = pack_f32x2(v.y, v.x);
     }
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(kThreads, (K <= 3 ? 4 : 3))   // 4 qubits: bot
             acc = fma_f32x2(a.mr[y * D + x], in[x], acc);
             acc = fma_f32x2(a.mi[y * D + x], sw[x], acc);
         }
-        __stcs(s + (base | a.off[y]),
+        __stcs(QSV_DBG(s + (base | a.off[y])),
                make_float2(__uint_as_float(static_cast<uint32_t>(acc)), __uint_as_float(static_cast<uint32_t>(acc >> 32))));
     }
 }
@@ -188,14 +188,14 @@ __global__ void __launch_bounds__(kThreads) k_dense_gen(const vec2_t<T>* __restr
         base |= a.ctrl;
         double re = 0, im = 0;
         for (int x = 0; x < D; ++x) {
-            const vec2_t<T> v = src[base | __ldg(off + x)];
-            const cplx<T> c = m[y * D + x];
+            const vec2_t<T> v = *QSV_DBG(src + (base | __ldg(QSV_DBG(off + x))));
+            const cplx<T> c = *QSV_DBG(m + (y * D + x));
             re = fma(static_cast<double>(c.re), v.x, re);
             re = fma(-static_cast<double>(c.im), v.y, re);
             im = fma(static_cast<double>(c.re), v.y, im);
             im = fma(static_cast<double>(c.im), v.x, im);
         }
-        dst[base | __ldg(off + y)] = mk<T>(static_cast<T>(re), static_cast<T>(im));
+        *QSV_DBG(dst + (base | __ldg(QSV_DBG(off + y)))) = mk<T>(static_cast<T>(re), static_cast<T>(im));
     }
 }
 
@@ -217,7 +217,8 @@ __global__ void __launch_bounds__(kThreads) k_diag(vec2_t<T>* __restrict__ s, ui
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
         uint32_t l = 0;
         for (int b = 0; b < a.k; ++b) l |= static_cast<uint32_t>((i >> a.q[b]) & 1ull) << b;
-        s[i] = cmul<T>(d[l], s[i]);
+        vec2_t<T>* const si = QSV_DBG(s + i);
+        *si = cmul<T>(d[l], *si);
     }
 }
 
@@ -227,8 +228,8 @@ __global__ void __launch_bounds__(kThreads) k_phase(vec2_t<T>* __restrict__ s, u
                                                     const __grid_constant__ BitPlan p, cplx<T> ph) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_idx; g += stride) {
-        const uint64_t i = insert_bits(g, p);
-        s[i] = cmul<T>(ph, s[i]);
+        vec2_t<T>* const si = QSV_DBG(s + insert_bits(g, p));
+        *si = cmul<T>(ph, *si);
     }
 }
 
@@ -240,9 +241,11 @@ __global__ void __launch_bounds__(kThreads) k_ctrl1(vec2_t<T>* __restrict__ s, u
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_pairs; g += stride) {
         const uint64_t i0 = insert_bits(g, p);
-        const vec2_t<T> a0 = s[i0], a1 = s[i0 | tbit];
-        s[i0] = cfma<T>(m1, a1, cmul<T>(m0, a0));
-        s[i0 | tbit] = cfma<T>(m3, a1, cmul<T>(m2, a0));
+        vec2_t<T>* const p0 = QSV_DBG(s + i0);
+        vec2_t<T>* const p1 = QSV_DBG(s + (i0 | tbit));
+        const vec2_t<T> a0 = *p0, a1 = *p1;
+        *p0 = cfma<T>(m1, a1, cmul<T>(m0, a0));
+        *p1 = cfma<T>(m3, a1, cmul<T>(m2, a0));
     }
 }
 
@@ -253,9 +256,11 @@ __global__ void __launch_bounds__(kThreads) k_swap(vec2_t<T>* __restrict__ s, ui
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_idx; g += stride) {
         const uint64_t i = insert_bits(g, p);
-        const vec2_t<T> x = s[i | abit], y = s[i | bbit];
-        s[i | abit] = y;
-        s[i | bbit] = x;
+        vec2_t<T>* const pa = QSV_DBG(s + (i | abit));
+        vec2_t<T>* const pb = QSV_DBG(s + (i | bbit));
+        const vec2_t<T> x = *pa, y = *pb;
+        *pa = y;
+        *pb = x;
     }
 }
 
@@ -268,7 +273,9 @@ __global__ void __launch_bounds__(kThreads) k_pauli_rot(vec2_t<T>* __restrict__ 
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_pairs; g += stride) {
         const uint64_t i = insert_bits(g, p), j = i ^ x;
-        const vec2_t<T> ai = s[i], aj = s[j];
+        vec2_t<T>* const si = QSV_DBG(s + i);
+        vec2_t<T>* const sj = QSV_DBG(s + j);
+        const vec2_t<T> ai = *si, aj = *sj;
         // phase(i) = i^{ny} * sign(i); -i * sn * phase * a
         auto rot = [&](uint64_t idx, vec2_t<T> a) {
             const int e = (ny + 2 * (__popcll(idx & z) & 1) + 3) & 3;  // (-i) * i^ny * sign
@@ -283,8 +290,8 @@ __global__ void __launch_bounds__(kThreads) k_pauli_rot(vec2_t<T>* __restrict__ 
             return r;
         };
         const vec2_t<T> pj = rot(j, aj), pi = rot(i, ai);
-        s[i] = mk<T>(c * ai.x + sn * pj.x, c * ai.y + sn * pj.y);
-        s[j] = mk<T>(c * aj.x + sn * pi.x, c * aj.y + sn * pi.y);
+        *si = mk<T>(c * ai.x + sn * pj.x, c * ai.y + sn * pj.y);
+        *sj = mk<T>(c * aj.x + sn * pi.x, c * aj.y + sn * pi.y);
     }
 }
 
@@ -305,18 +312,20 @@ __global__ void __launch_bounds__(kThreads) k_perm(const vec2_t<T>* __restrict__
         // the reads are scattered (a scattered 16-byte write costs a sector read-modify-write)
         uint64_t y = 0;
         for (int b = 0; b < a.k; ++b) y |= ((i >> a.q[b]) & 1ull) << b;
-        const uint64_t x = __ldg(table + y);
+        const uint64_t x = __ldg(QSV_DBG(table + y));
         uint64_t j = i & a.keep;
         for (int b = 0; b < a.k; ++b) j |= ((x >> b) & 1ull) << a.q[b];
-        dst[i] = src[j];
+        *QSV_DBG(dst + i) = *QSV_DBG(src + j);
     }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_scale(vec2_t<T>* __restrict__ s, uint64_t dim, cplx<T> f) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride)
-        s[i] = cmul<T>(f, s[i]);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
+        vec2_t<T>* const si = QSV_DBG(s + i);
+        *si = cmul<T>(f, *si);
+    }
 }
 
 template <typename T, int K>

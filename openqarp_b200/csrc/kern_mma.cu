@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(vec2_t<T>* __restric
     double* w = msm;                      // R x WS
     double* xr = w + Sh::R * Sh::WS;      // D x S   (real planes)
     double* xi = xr + Sh::D * Sh::S;      // D x S   (imaginary planes)
-    for (int i = threadIdx.x; i < Sh::R * Sh::R; i += blockDim.x) w[(i / Sh::R) * Sh::WS + (i % Sh::R)] = W[i];
+    for (int i = threadIdx.x; i < Sh::R * Sh::R; i += blockDim.x) w[(i / Sh::R) * Sh::WS + (i % Sh::R)] = *QSV_DBG(W + i);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gid = lane >> 2, tig = lane & 3;
     const int nb = warp % Sh::NB;
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(vec2_t<T>* __restric
             const int j = e % Sh::NG, x = e / Sh::NG;
             const uint64_t g = t0 + j;
             vec2_t<T> v = mk<T>(T(0), T(0));
-            if (g < n_groups) v = __ldcs(s + (insert_zeros(g, a.pos, K) | a.off[x]));
+            if (g < n_groups) v = __ldcs(QSV_DBG(s + (insert_zeros(g, a.pos, K) | a.off[x])));
             xr[x * Sh::S + j] = static_cast<double>(v.x);
             xi[x * Sh::S + j] = static_cast<double>(v.y);
         }
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(kMmaThreads) k_dense_dmma(vec2_t<T>* __restric
             const int j = e % Sh::NG, x = e / Sh::NG;
             const uint64_t g = t0 + j;
             if (g < n_groups)
-                __stcs(s + (insert_zeros(g, a.pos, K) | a.off[x]),
+                __stcs(QSV_DBG(s + (insert_zeros(g, a.pos, K) | a.off[x])),
                        mk<T>(static_cast<T>(xr[x * Sh::S + j]), static_cast<T>(xi[x * Sh::S + j])));
         }
     }

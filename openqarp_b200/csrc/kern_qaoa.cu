@@ -120,13 +120,13 @@ __global__ void __launch_bounds__(kQThreads, 1)
     __shared__ double2 s_ph[kQMaxEdges + 1];                // exp(-i gamma (E - 2c)), c = 0..E
     __shared__ double2 red[kQThreads / 32];
     for (;;) {
-        if (threadIdx.x == 0) s_w = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) s_w = atomicAdd(QSV_DBG(counter), 1);
         __syncthreads();
         const int w = s_w;
         if (w >= n_inst) break;
-        const QaoaInst I = inst[order[w]];
+        const QaoaInst I = (*QSV_DBG(inst + ((*QSV_DBG(order + (w))))));
         const int n = I.n, p = I.p, E = I.n_edges;
-        for (int e = threadIdx.x; e < 2 * E; e += blockDim.x) s_ed[e] = edges[2 * I.edge_off + e];
+        for (int e = threadIdx.x; e < 2 * E; e += blockDim.x) s_ed[e] = (*QSV_DBG(edges + (2 * I.edge_off + e)));
         const double* prm = params + I.param_off;
         double* grd = grads + I.param_off;
         const double amp0 = exp2(-0.5 * n);
@@ -145,11 +145,11 @@ __global__ void __launch_bounds__(kQThreads, 1)
             for (uint32_t l = threadIdx.x; l < M; l += blockDim.x) A[l] = make_double2(amp0, 0.0);
             __syncthreads();
             for (int r = 0; r < p; ++r) {
-                phase_table(prm[2 * r], false);
+                phase_table((*QSV_DBG(prm + (2 * r))), false);
                 for (uint32_t l = threadIdx.x; l < M; l += blockDim.x) A[l] = cmul2(s_ph[cut_of(l, s_ed, E)], A[l]);
                 __syncthreads();
                 double sb, cb;
-                sincos(prm[2 * r + 1], &sb, &cb);
+                sincos((*QSV_DBG(prm + (2 * r + 1))), &sb, &cb);
                 for (int q = 0; q < n; ++q) {
                     rx_layer_bit(A, n, q, cb, sb);
                     __syncthreads();
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kQThreads, 1)
                 acc.x += (a.x * a.x + a.y * a.y) * cut_of(l, s_ed, E);
             }
             const double2 en = qblock_sum(acc, red);
-            if (threadIdx.x == 0) energy[order[w]] = en.x;
+            if (threadIdx.x == 0) (*QSV_DBG(energy + ((*QSV_DBG(order + (w)))))) = en.x;
             if (with_grad) {
                 for (uint32_t l = threadIdx.x; l < M; l += blockDim.x) {
                     const double cv = cut_of(l, s_ed, E);
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kQThreads, 1)
                     }
                     gb = qblock_sum(gb, red);
                     double sb, cb;
-                    sincos(prm[2 * r + 1], &sb, &cb);
+                    sincos((*QSV_DBG(prm + (2 * r + 1))), &sb, &cb);
                     for (int q = 0; q < n; ++q) {
                         rx_layer_bit(A, n, q, cb, -sb);
                         rx_layer_bit(B, n, q, cb, -sb);
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kQThreads, 1)
                         gg.y += d * v.y;
                     }
                     gg = qblock_sum(gg, red);
-                    phase_table(prm[2 * r], true);
+                    phase_table((*QSV_DBG(prm + (2 * r))), true);
                     for (uint32_t l = threadIdx.x; l < M; l += blockDim.x) {
                         const double2 ph = s_ph[cut_of(l, s_ed, E)];
                         A[l] = cmul2(ph, A[l]);
@@ -199,8 +199,8 @@ __global__ void __launch_bounds__(kQThreads, 1)
                     }
                     __syncthreads();
                     if (threadIdx.x == 0) {
-                        grd[2 * r] = 2.0 * gg.y;
-                        grd[2 * r + 1] = 2.0 * gb.y;
+                        (*QSV_DBG(grd + (2 * r))) = 2.0 * gg.y;
+                        (*QSV_DBG(grd + (2 * r + 1))) = 2.0 * gb.y;
                     }
                 }
             }
@@ -214,13 +214,13 @@ __global__ void __launch_bounds__(kQThreads, 1)
         const int L = 2 * kQTileLog - n;        // low qubits kept in a layout-B tile
         const int nh = n - kQTileLog;           // qubits 12..n-1
         for (int r = 0; r < p; ++r) {
-            phase_table(prm[2 * r], false);
+            phase_table((*QSV_DBG(prm + (2 * r))), false);
             double sb, cb;
-            sincos(prm[2 * r + 1], &sb, &cb);
+            sincos((*QSV_DBG(prm + (2 * r + 1))), &sb, &cb);
             for (uint64_t t = 0; t < n_tiles; ++t) {      // layout A: phase + RX on qubits 0..11
                 for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) {
                     const uint64_t gi = gidx_a(t, l);
-                    const double2 a = r == 0 ? make_double2(amp0, 0.0) : psi[gi];
+                    const double2 a = r == 0 ? make_double2(amp0, 0.0) : (*QSV_DBG(psi + (gi)));
                     A[l] = cmul2(s_ph[cut_of(gi, s_ed, E)], a);
                 }
                 __syncthreads();
@@ -228,17 +228,17 @@ __global__ void __launch_bounds__(kQThreads, 1)
                     rx_layer_bit(A, kQTileLog, q, cb, sb);
                     __syncthreads();
                 }
-                for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) psi[gidx_a(t, l)] = A[l];
+                for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) (*QSV_DBG(psi + (gidx_a(t, l)))) = A[l];
                 __syncthreads();
             }
             for (uint64_t t = 0; t < n_tiles; ++t) {      // layout B: RX on qubits 12..n-1
-                for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) A[l] = psi[gidx_b(t, l, L)];
+                for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) A[l] = (*QSV_DBG(psi + (gidx_b(t, l, L))));
                 __syncthreads();
                 for (int q = 0; q < nh; ++q) {
                     rx_layer_bit(A, kQTileLog, L + q, cb, sb);
                     __syncthreads();
                 }
-                for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) psi[gidx_b(t, l, L)] = A[l];
+                for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) (*QSV_DBG(psi + (gidx_b(t, l, L)))) = A[l];
                 __syncthreads();
             }
         }
@@ -246,25 +246,25 @@ __global__ void __launch_bounds__(kQThreads, 1)
         for (uint64_t t = 0; t < n_tiles; ++t)
             for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) {
                 const uint64_t gi = gidx_a(t, l);
-                const double2 a = psi[gi];
+                const double2 a = (*QSV_DBG(psi + (gi)));
                 const double cv = cut_of(gi, s_ed, E);
                 acc.x += (a.x * a.x + a.y * a.y) * cv;
-                if (with_grad) phi[gi] = make_double2(cv * a.x, cv * a.y);
+                if (with_grad) (*QSV_DBG(phi + (gi))) = make_double2(cv * a.x, cv * a.y);
             }
         const double2 en = qblock_sum(acc, red);
-        if (threadIdx.x == 0) energy[order[w]] = en.x;
+        if (threadIdx.x == 0) (*QSV_DBG(energy + ((*QSV_DBG(order + (w)))))) = en.x;
         if (with_grad) {
             __threadfence_block();
             __syncthreads();
             for (int r = p - 1; r >= 0; --r) {
                 double sb, cb;
-                sincos(prm[2 * r + 1], &sb, &cb);
+                sincos((*QSV_DBG(prm + (2 * r + 1))), &sb, &cb);
                 double2 gb = make_double2(0, 0), gg = make_double2(0, 0);
                 for (uint64_t t = 0; t < n_tiles; ++t) {      // layout B: X overlaps + un-apply RX 12..n-1
                     for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) {
                         const uint64_t gi = gidx_b(t, l, L);
-                        A[l] = psi[gi];
-                        B[l] = phi[gi];
+                        A[l] = (*QSV_DBG(psi + (gi)));
+                        B[l] = (*QSV_DBG(phi + (gi)));
                     }
                     __syncthreads();
                     for (int q = 0; q < nh; ++q) {
@@ -280,16 +280,16 @@ __global__ void __launch_bounds__(kQThreads, 1)
                     }
                     for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) {
                         const uint64_t gi = gidx_b(t, l, L);
-                        psi[gi] = A[l];
-                        phi[gi] = B[l];
+                        (*QSV_DBG(psi + (gi))) = A[l];
+                        (*QSV_DBG(phi + (gi))) = B[l];
                     }
                     __syncthreads();
                 }
-                phase_table(prm[2 * r], true);
+                phase_table((*QSV_DBG(prm + (2 * r))), true);
                 for (uint64_t t = 0; t < n_tiles; ++t) {      // layout A: X overlaps, un-apply RX 0..11, D overlap, un-apply phase
                     for (uint32_t l = threadIdx.x; l < kQTile; l += blockDim.x) {
-                        A[l] = psi[gidx_a(t, l)];
-                        B[l] = phi[gidx_a(t, l)];
+                        A[l] = (*QSV_DBG(psi + (gidx_a(t, l))));
+                        B[l] = (*QSV_DBG(phi + (gidx_a(t, l))));
                     }
                     __syncthreads();
                     for (int q = 0; q < kQTileLog; ++q) {
@@ -311,16 +311,16 @@ __global__ void __launch_bounds__(kQThreads, 1)
                         gg.x += d * v.x;
                         gg.y += d * v.y;
                         const double2 ph = s_ph[cv];
-                        psi[gi] = cmul2(ph, A[l]);
-                        phi[gi] = cmul2(ph, B[l]);
+                        (*QSV_DBG(psi + (gi))) = cmul2(ph, A[l]);
+                        (*QSV_DBG(phi + (gi))) = cmul2(ph, B[l]);
                     }
                     __syncthreads();
                 }
                 gb = qblock_sum(gb, red);
                 gg = qblock_sum(gg, red);
                 if (threadIdx.x == 0) {
-                    grd[2 * r] = 2.0 * gg.y;
-                    grd[2 * r + 1] = 2.0 * gb.y;
+                    (*QSV_DBG(grd + (2 * r))) = 2.0 * gg.y;
+                    (*QSV_DBG(grd + (2 * r + 1))) = 2.0 * gb.y;
                 }
             }
         }
@@ -372,8 +372,8 @@ void release(QaoaBatch* q) {
         if (q->exec[i]) cudaGraphExecDestroy(q->exec[i]);
         if (q->graph[i]) cudaGraphDestroy(q->graph[i]);
     }
-    if (q->dev) cudaFree(q->dev);
-    if (q->pool) cudaFree(q->pool);
+    if (q->dev) dev_free(q->dev);
+    if (q->pool) dev_free(q->pool);
     if (q->h_params) cudaFreeHost(q->h_params);
     if (q->h_out) cudaFreeHost(q->h_out);
     if (q->e0) cudaEventDestroy(q->e0);
@@ -426,7 +426,7 @@ void* qaoa_create(int device, int n_inst, const int32_t* n_qubits, const int32_t
         const size_t b_inst = al(n_inst * sizeof(QaoaInst)), b_order = al(n_inst * 4), b_edges = al(2 * n_edges * 4 + 4);
         const size_t b_params = al(n_params * 8), b_energy = al(n_inst * 8), b_grads = al(n_params * 8), b_cnt = 256;
         const size_t total = b_inst + b_order + b_edges + b_params + b_energy + b_grads + b_cnt;
-        check_cuda(cudaMalloc(&q->dev, total), "QAOA descriptors");
+        check_cuda(dev_malloc(&q->dev, total), "QAOA descriptors");
         uint8_t* d = static_cast<uint8_t*>(q->dev);
         q->d_inst = reinterpret_cast<QaoaInst*>(d);
         q->d_order = reinterpret_cast<int32_t*>(d + b_inst);
@@ -435,7 +435,7 @@ void* qaoa_create(int device, int n_inst, const int32_t* n_qubits, const int32_t
         q->d_energy = reinterpret_cast<double*>(d + b_inst + b_order + b_edges + b_params);
         q->d_grads = reinterpret_cast<double*>(d + b_inst + b_order + b_edges + b_params + b_energy);
         q->d_counter = reinterpret_cast<int*>(d + b_inst + b_order + b_edges + b_params + b_energy + b_grads);
-        if (pool_amps > 0) check_cuda(cudaMalloc(&q->pool, static_cast<size_t>(pool_amps) * sizeof(double2)), "QAOA state pool");
+        if (pool_amps > 0) check_cuda(dev_malloc(&q->pool, static_cast<size_t>(pool_amps) * sizeof(double2)), "QAOA state pool");
         check_cuda(cudaMallocHost(reinterpret_cast<void**>(&q->h_params), std::max<size_t>(n_params, 1) * 8), "pinned params");
         check_cuda(cudaMallocHost(reinterpret_cast<void**>(&q->h_out), (n_inst + n_params) * 8), "pinned results");
         check_cuda(cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking), "stream");

@@ -66,10 +66,10 @@ __global__ void __launch_bounds__(kRoThreads) k_exact_count(const vec2_t<T>* __r
 #pragma unroll
     for (int r = 0; r < kRoPer; ++r) {
         const uint64_t i = start + static_cast<uint64_t>(r) * kRoThreads + threadIdx.x;
-        if (i < dim && born<T>(__ldcs(s + i)) > thr) ++c;
+        if (i < dim && born<T>(__ldcs(QSV_DBG(s + i))) > thr) ++c;
     }
     block_exclusive_scan(c, warp_tot, &total);
-    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+    if (threadIdx.x == 0) *QSV_DBG(counts + blockIdx.x) = total;
 }
 
 // exclusive prefix of the chunk counts in one block: off[c] = sum_{c' < c}, off[n] = total
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kScanThreads) k_exact_offsets(const uint32_t* 
     const uint64_t per = (n + kScanThreads - 1) / kScanThreads;
     const uint64_t lo = min(n, per * threadIdx.x), hi = min(n, lo + per);
     uint64_t sum = 0;
-    for (uint64_t c = lo; c < hi; ++c) sum += counts[c];
+    for (uint64_t c = lo; c < hi; ++c) sum += *QSV_DBG(counts + c);
     part[threadIdx.x] = sum;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -89,13 +89,13 @@ __global__ void __launch_bounds__(kScanThreads) k_exact_offsets(const uint32_t* 
             part[t] = acc;
             acc += x;
         }
-        off[n] = acc;
+        *QSV_DBG(off + n) = acc;
     }
     __syncthreads();
     uint64_t acc = part[threadIdx.x];
     for (uint64_t c = lo; c < hi; ++c) {
-        off[c] = acc;
-        acc += counts[c];
+        *QSV_DBG(off + c) = acc;
+        acc += *QSV_DBG(counts + c);
     }
 }
 
@@ -116,12 +116,12 @@ __global__ void __launch_bounds__(kRoThreads) k_exact_write(const vec2_t<T>* __r
 #pragma unroll
     for (int r = 0; r < kRoPer; ++r) {
         const uint64_t i = start + static_cast<uint64_t>(r) * kRoThreads + threadIdx.x;
-        p[r] = i < dim ? born<T>(__ldcs(s + i)) : 0.0;
+        p[r] = i < dim ? born<T>(__ldcs(QSV_DBG(s + i))) : 0.0;
         ball[r] = __ballot_sync(0xffffffffu, i < dim && p[r] > thr);
         if (lane == 0) wcount[r][warp] = __popc(ball[r]);
     }
     __syncthreads();
-    uint64_t o = off[blockIdx.x];
+    uint64_t o = *QSV_DBG(off + blockIdx.x);
 #pragma unroll
     for (int r = 0; r < kRoPer; ++r) {
         uint32_t before = 0, round = 0;
@@ -133,8 +133,8 @@ __global__ void __launch_bounds__(kRoThreads) k_exact_write(const vec2_t<T>* __r
         }
         if ((ball[r] >> lane) & 1u) {
             const uint64_t dst = o + before + __popc(ball[r] & lt);
-            keys[dst] = start + static_cast<uint64_t>(r) * kRoThreads + threadIdx.x;
-            probs[dst] = p[r];
+            *QSV_DBG(keys + dst) = start + static_cast<uint64_t>(r) * kRoThreads + threadIdx.x;
+            *QSV_DBG(probs + dst) = p[r];
         }
         o += round;
     }
@@ -153,13 +153,13 @@ __global__ void __launch_bounds__(kParThreads) k_parity_counts(const uint64_t* _
     for (size_t t0 = 0; t0 < n_masks; t0 += kParMaskTile) {
         const int nt = static_cast<int>(min(static_cast<size_t>(kParMaskTile), n_masks - t0));
         for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-            m[t] = masks[t0 + t];
+            m[t] = *QSV_DBG(masks + (t0 + t));
             cnt[t] = 0;
         }
         __syncthreads();
         for (size_t s0 = static_cast<size_t>(blockIdx.x) * blockDim.x; s0 < n_shots; s0 += stride) {
             const size_t sidx = s0 + threadIdx.x;
-            const uint64_t x = sidx < n_shots ? outcome[sidx] : 0ull;
+            const uint64_t x = sidx < n_shots ? *QSV_DBG(outcome + sidx) : 0ull;
             const bool live = sidx < n_shots;
             for (int t = 0; t < nt; ++t) {
                 const unsigned b = __ballot_sync(0xffffffffu, live && (__popcll(x & m[t]) & 1));
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kParThreads) k_parity_counts(const uint64_t* _
         }
         __syncthreads();
         for (int t = threadIdx.x; t < nt; t += blockDim.x)
-            if (cnt[t]) atomicAdd(odd + t0 + t, static_cast<unsigned long long>(cnt[t]));
+            if (cnt[t]) atomicAdd(QSV_DBG(odd + (t0 + t)), static_cast<unsigned long long>(cnt[t]));
         __syncthreads();
     }
 }

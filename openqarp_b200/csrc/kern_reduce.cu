@@ -85,11 +85,11 @@ const std::vector<PassTimer::Total>& PassTimer::collect() {
 
 void* Workspace::grow(void*& p, size_t& cap, size_t bytes) {
     if (bytes <= cap && p) return p;
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
     p = nullptr;
     cap = 0;
     const size_t want = std::max<size_t>(bytes, 4096);
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = dev_malloc(&p, want);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();   // a failed allocation leaves no error for the next launch check
         p = nullptr;
@@ -112,24 +112,24 @@ double* Workspace::host_result(size_t n) {
 
 int* Workspace::tensor_flag() {
     if (!flag_) {
-        check_cuda(cudaMalloc(reinterpret_cast<void**>(&flag_), 256), "tensor flag");
+        check_cuda(dev_malloc(reinterpret_cast<void**>(&flag_), 256), "tensor flag");
         check_cuda(cudaMemset(flag_, 0, 256), "tensor flag");
     }
     return flag_;
 }
 
 void Workspace::release() {
-    if (flag_) cudaFree(flag_);
+    if (flag_) dev_free(flag_);
     flag_ = nullptr;
-    if (mat_) cudaFree(mat_);
-    if (copy_) cudaFree(copy_);
-    if (scr_) cudaFree(scr_);
-    if (shot_) cudaFree(shot_);
-    if (tile_) cudaFree(tile_);
-    if (rtile_) cudaFree(rtile_);
-    if (tb_) cudaFree(tb_);
-    if (tk_) cudaFree(tk_);
-    if (ts_) cudaFree(ts_);
+    if (mat_) dev_free(mat_);
+    if (copy_) dev_free(copy_);
+    if (scr_) dev_free(scr_);
+    if (shot_) dev_free(shot_);
+    if (tile_) dev_free(tile_);
+    if (rtile_) dev_free(rtile_);
+    if (tb_) dev_free(tb_);
+    if (tk_) dev_free(tk_);
+    if (ts_) dev_free(ts_);
     if (host_) cudaFreeHost(host_);
     mat_ = copy_ = scr_ = shot_ = tile_ = rtile_ = tb_ = tk_ = ts_ = nullptr;
     host_ = nullptr;
@@ -172,11 +172,12 @@ __global__ void k_final(const double2* __restrict__ partials, unsigned nb, doubl
     const double2* p = partials + static_cast<size_t>(blockIdx.x) * nb;
     double2 acc = make_double2(0, 0);
     for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) {
-        acc.x += p[b].x;
-        acc.y += p[b].y;
+        const double2 v = *QSV_DBG(p + b);
+        acc.x += v.x;
+        acc.y += v.y;
     }
     acc = block_sum(acc);
-    if (threadIdx.x == 0) out[blockIdx.x] = acc;
+    if (threadIdx.x == 0) *QSV_DBG(out + blockIdx.x) = acc;
 }
 
 unsigned red_blocks(uint64_t work) {
@@ -224,10 +225,10 @@ __device__ __forceinline__ void group_weights(const TermPtrs& tp, int g, uint64_
                                               double (&wi)[kRuns]) {
 #pragma unroll
     for (int r = 0; r < kRuns; ++r) wr[r] = wi[r] = 0.0;
-    const int j1 = __ldg(tp.gstart + g + 1);
-    for (int j = __ldg(tp.gstart + g); j < j1; ++j) {
-        const uint64_t z = __ldg(tp.z + j);
-        const double2 c = __ldg(tp.c + j);
+    const int j1 = __ldg(QSV_DBG(tp.gstart + (g + 1)));
+    for (int j = __ldg(QSV_DBG(tp.gstart + g)); j < j1; ++j) {
+        const uint64_t z = __ldg(QSV_DBG(tp.z + j));
+        const double2 c = __ldg(QSV_DBG(tp.c + j));
         const uint32_t p = static_cast<uint32_t>(__popcll(ib & z));
         const uint32_t q = static_cast<uint32_t>(z >> 5);
 #pragma unroll
@@ -255,11 +256,11 @@ __global__ void __launch_bounds__(kRed, 2) k_transition(const vec2_t<T>* __restr
             ok[r] = (base | (static_cast<uint64_t>(r) << 5) | lane) < dim;
         }
         for (int g = 0; g < tp.n_groups; ++g) {
-            const uint64_t x = __ldg(tp.gx + g);
+            const uint64_t x = __ldg(QSV_DBG(tp.gx + g));
             vec2_t<T> b[kRuns];
 #pragma unroll
             for (int r = 0; r < kRuns; ++r)
-                b[r] = ok[r] ? bra[(base | (static_cast<uint64_t>(r) << 5) | lane) ^ x] : mk<T>(T(0), T(0));
+                b[r] = ok[r] ? *QSV_DBG(bra + ((base | (static_cast<uint64_t>(r) << 5) | lane) ^ x)) : mk<T>(T(0), T(0));
             double wr[kRuns], wi[kRuns];
             group_weights(tp, g, base | lane, wr, wi);
 #pragma unroll
@@ -272,14 +273,14 @@ __global__ void __launch_bounds__(kRed, 2) k_transition(const vec2_t<T>* __restr
 #pragma unroll
         for (int r = 0; r < kRuns; ++r) {
             if (!ok[r]) continue;
-            const vec2_t<T> k = ket[base | (static_cast<uint64_t>(r) << 5) | lane];
+            const vec2_t<T> k = *QSV_DBG(ket + (base | (static_cast<uint64_t>(r) << 5) | lane));
             const double kr = k.x, ki = k.y;
             ar = fma(tr[r], kr, ar); ar = fma(-ti[r], ki, ar);
             ai = fma(tr[r], ki, ai); ai = fma(ti[r], kr, ai);
         }
     }
     const double2 acc = block_sum(make_double2(ar, ai));
-    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+    if (threadIdx.x == 0) *QSV_DBG(partials + blockIdx.x) = acc;
 }
 
 // out[k] = sum_g psi[k^x_g] * sum_j c_j (-1)^{popcount((k^x_g) & z_j)}, in the index runs above
@@ -298,11 +299,11 @@ __global__ void __launch_bounds__(kRed, 2) k_apply_obs(const vec2_t<T>* __restri
             ok[r] = (base | (static_cast<uint64_t>(r) << 5) | lane) < dim;
         }
         for (int g = 0; g < tp.n_groups; ++g) {
-            const uint64_t x = __ldg(tp.gx + g);
+            const uint64_t x = __ldg(QSV_DBG(tp.gx + g));
             vec2_t<T> p[kRuns];
 #pragma unroll
             for (int r = 0; r < kRuns; ++r)
-                p[r] = ok[r] ? psi[(base | (static_cast<uint64_t>(r) << 5) | lane) ^ x] : mk<T>(T(0), T(0));
+                p[r] = ok[r] ? *QSV_DBG(psi + ((base | (static_cast<uint64_t>(r) << 5) | lane) ^ x)) : mk<T>(T(0), T(0));
             double wr[kRuns], wi[kRuns];
             group_weights(tp, g, (base | lane) ^ x, wr, wi);
 #pragma unroll
@@ -315,7 +316,8 @@ __global__ void __launch_bounds__(kRed, 2) k_apply_obs(const vec2_t<T>* __restri
 #pragma unroll
         for (int r = 0; r < kRuns; ++r)
             if (ok[r])
-                out[base | (static_cast<uint64_t>(r) << 5) | lane] = mk<T>(static_cast<T>(orr[r]), static_cast<T>(oi[r]));
+                *QSV_DBG(out + (base | (static_cast<uint64_t>(r) << 5) | lane)) =
+                    mk<T>(static_cast<T>(orr[r]), static_cast<T>(oi[r]));
     }
 }
 
@@ -324,13 +326,13 @@ __global__ void __launch_bounds__(kRed) k_norm2(const vec2_t<T>* __restrict__ s,
     double2 acc = make_double2(0, 0);
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
-        const vec2_t<T> a = s[i];
+        const vec2_t<T> a = *QSV_DBG(s + i);
         const double x = a.x, y = a.y;
         acc.x = fma(x, x, acc.x);
         acc.x = fma(y, y, acc.x);
     }
     acc = block_sum(acc);
-    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+    if (threadIdx.x == 0) *QSV_DBG(partials + blockIdx.x) = acc;
 }
 
 template <typename TA, typename TB>
@@ -339,12 +341,12 @@ __global__ void __launch_bounds__(kRed) k_inner(const vec2_t<TA>* __restrict__ a
     dcplx acc{0, 0};
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
-        const vec2_t<TA> x = a[i];
-        const vec2_t<TB> y = b[i];
+        const vec2_t<TA> x = *QSV_DBG(a + i);
+        const vec2_t<TB> y = *QSV_DBG(b + i);
         dacc_conj_mul(acc, x.x, x.y, y.x, y.y);
     }
     double2 v = block_sum(make_double2(acc.re, acc.im));
-    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+    if (threadIdx.x == 0) *QSV_DBG(partials + blockIdx.x) = v;
 }
 
 template <typename T>
@@ -353,10 +355,11 @@ template <typename T>
 __global__ void k_scale_real(vec2_t<T>* __restrict__ s, uint64_t dim, double f) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
-        vec2_t<T> a = s[i];
+        vec2_t<T>* const si = QSV_DBG(s + i);
+        vec2_t<T> a = *si;
         a.x = static_cast<T>(static_cast<double>(a.x) * f);
         a.y = static_cast<T>(static_cast<double>(a.y) * f);
-        s[i] = a;
+        *si = a;
     }
 }
 
@@ -407,9 +410,9 @@ __global__ void __launch_bounds__(kRed) k_prob_total(const vec2_t<T>* __restrict
     double2 acc = make_double2(0, 0);
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride)
-        acc.x += prob<T>(s[i]);
+        acc.x += prob<T>(*QSV_DBG(s + i));
     acc = block_sum(acc);
-    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+    if (threadIdx.x == 0) *QSV_DBG(partials + blockIdx.x) = acc;
 }
 
 // in-chunk inclusive scan of p_i / S: thread t owns amplitudes [t*16, t*16+16) of the chunk.
@@ -423,7 +426,7 @@ __device__ void chunk_scan(const vec2_t<T>* __restrict__ s, uint64_t start, uint
 #pragma unroll
     for (int r = 0; r < kPerThread; ++r) {
         const uint64_t i = start + static_cast<uint64_t>(t) * kPerThread + r;
-        const double q = i < dim ? __ddiv_rn(prob<T>(s[i]), total) : 0.0;
+        const double q = i < dim ? __ddiv_rn(prob<T>(*QSV_DBG(s + i)), total) : 0.0;
         run = __dadd_rn(run, q);
         v[r] = run;
     }
@@ -453,8 +456,8 @@ __global__ void __launch_bounds__(kChunkThreads) k_chunk_totals(const vec2_t<T>*
     __shared__ double tot;
     double v[kPerThread];
     const uint64_t start = static_cast<uint64_t>(blockIdx.x) << kChunkLog;
-    chunk_scan<T>(s, start, dim, 0.0, total_p->x, v, sh, &tot);
-    if (threadIdx.x == 0) chunk_total[blockIdx.x] = tot;
+    chunk_scan<T>(s, start, dim, 0.0, QSV_DBG(total_p)->x, v, sh, &tot);
+    if (threadIdx.x == 0) *QSV_DBG(chunk_total + blockIdx.x) = tot;
 }
 
 // exclusive prefix of the chunk totals, off[c] = sum_{c' < c}, in a fixed order: thread t sums
@@ -468,7 +471,7 @@ __global__ void __launch_bounds__(kOffThreads) k_chunk_offsets(const double* __r
     const unsigned per = (n_chunks + kOffThreads - 1) / kOffThreads;
     const unsigned c0 = min(n_chunks, threadIdx.x * per), c1 = min(n_chunks, c0 + per);
     double acc = 0;
-    for (unsigned c = c0; c < c1; ++c) acc = __dadd_rn(acc, chunk_total[c]);
+    for (unsigned c = c0; c < c1; ++c) acc = __dadd_rn(acc, *QSV_DBG(chunk_total + c));
     run_base[threadIdx.x] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -483,17 +486,17 @@ __global__ void __launch_bounds__(kOffThreads) k_chunk_offsets(const double* __r
     __syncthreads();
     double a = run_base[threadIdx.x];
     for (unsigned c = c0; c < c1; ++c) {
-        off[c] = a;
-        a = __dadd_rn(a, chunk_total[c]);
+        *QSV_DBG(off + c) = a;
+        a = __dadd_rn(a, *QSV_DBG(chunk_total + c));
     }
-    if (threadIdx.x == 0) off[n_chunks] = run_base[kOffThreads];
+    if (threadIdx.x == 0) *QSV_DBG(off + n_chunks) = run_base[kOffThreads];
 }
 
 __device__ __forceinline__ size_t first_greater(const double* u, size_t n, double x) {
     size_t lo = 0, hi = n;   // first s with u[s] > x
     while (lo < hi) {
         const size_t mid = lo + (hi - lo) / 2;
-        if (u[mid] > x) hi = mid; else lo = mid + 1;
+        if (*QSV_DBG(u + mid) > x) hi = mid; else lo = mid + 1;
     }
     return lo;
 }
@@ -509,25 +512,26 @@ __global__ void __launch_bounds__(kChunkThreads) k_sample_chunks(const vec2_t<T>
     __shared__ double tot;
     const unsigned c = blockIdx.x;
     // shots whose lower_bound lands in this chunk: off[c] < u <= off[c+1] (first/last chunk open)
-    const size_t lo = c == 0 ? 0 : first_greater(u, n_shots, off[c]);
-    const size_t hi = c + 1 == n_chunks ? n_shots : first_greater(u, n_shots, off[c + 1]);
+    const size_t lo = c == 0 ? 0 : first_greater(u, n_shots, *QSV_DBG(off + c));
+    const size_t hi = c + 1 == n_chunks ? n_shots : first_greater(u, n_shots, *QSV_DBG(off + (c + 1)));
     if (lo >= hi) return;
     double v[kPerThread];
     const uint64_t start = static_cast<uint64_t>(c) << kChunkLog;
-    chunk_scan<T>(s, start, dim, 0.0, total_p->x, v, sh, &tot);
+    chunk_scan<T>(s, start, dim, 0.0, QSV_DBG(total_p)->x, v, sh, &tot);
+    const double off_c = *QSV_DBG(off + c);
 #pragma unroll
-    for (int r = 0; r < kPerThread; ++r) cp[threadIdx.x * kPerThread + r] = __dadd_rn(off[c], v[r]);
+    for (int r = 0; r < kPerThread; ++r) cp[threadIdx.x * kPerThread + r] = __dadd_rn(off_c, v[r]);
     __syncthreads();
     const uint64_t len = min(static_cast<uint64_t>(1) << kChunkLog, dim - start);
     for (size_t sidx = lo + threadIdx.x; sidx < hi; sidx += blockDim.x) {
-        const double x = u[sidx];
+        const double x = *QSV_DBG(u + sidx);
         uint64_t a = 0, b = len;   // first j with cp[j] >= x
         while (a < b) {
             const uint64_t mid = (a + b) >> 1;
             if (cp[mid] < x) a = mid + 1; else b = mid;
         }
         if (a >= len) a = len - 1;   // rounding past the chunk's last cumulative: stay in it
-        out[sidx] = start + a;
+        *QSV_DBG(out + sidx) = start + a;
     }
 }
 
@@ -552,8 +556,8 @@ __global__ void __launch_bounds__(kRed) k_adj_step(vec2_t<T>* __restrict__ psi, 
         vec2_t<T> ps[Dm], ph[Dm];
 #pragma unroll
         for (int l = 0; l < Dm; ++l) {
-            ps[l] = psi[base | a.off[l]];
-            ph[l] = phi[base | a.off[l]];
+            ps[l] = *QSV_DBG(psi + (base | a.off[l]));
+            ph[l] = *QSV_DBG(phi + (base | a.off[l]));
         }
         // <phi| G |psi> restricted to this group
 #pragma unroll
@@ -580,12 +584,12 @@ __global__ void __launch_bounds__(kRed) k_adj_step(vec2_t<T>* __restrict__ psi, 
                 o1 = cfma<T>(a.D[y * Dm + x], ps[x], o1);
                 o2 = cfma<T>(a.D[y * Dm + x], ph[x], o2);
             }
-            psi[base | a.off[y]] = o1;
-            phi[base | a.off[y]] = o2;
+            *QSV_DBG(psi + (base | a.off[y])) = o1;
+            *QSV_DBG(phi + (base | a.off[y])) = o2;
         }
     }
     double2 v = block_sum(make_double2(acc.re, acc.im));
-    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+    if (threadIdx.x == 0) *QSV_DBG(partials + blockIdx.x) = v;
 }
 
 template <typename T, int K>

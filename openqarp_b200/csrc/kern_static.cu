@@ -85,11 +85,11 @@ __global__ void __launch_bounds__(kStaticThreads) k_static_transition(const vec2
     double ar = 0, ai = 0;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < dim; i += stride) {
-        const vec2_t<T> k = ket[i];
+        const vec2_t<T> k = *QSV_DBG(ket + i);
         double tr = 0, ti = 0;   // sum_t conj(bra[i ^ x_t]) * w_t(i)
         for (unsigned t = 0; t < n_terms; ++t) {
-            const uint64_t x = xs[t], z = zs[t];
-            const double2 c = cs[t];
+            const uint64_t x = *QSV_DBG(xs + t), z = *QSV_DBG(zs + t);
+            const double2 c = *QSV_DBG(cs + t);
             // c * i^{nY} * (-1)^{popcount(i & z)}
             const int e = (__popcll(x & z) + 2 * (__popcll(i & z) & 1)) & 3;
             double wr, wi;
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kStaticThreads) k_static_transition(const vec2
                 case 2: wr = -c.x; wi = -c.y; break;
                 default: wr = c.y; wi = -c.x; break;
             }
-            const vec2_t<T> b = bra[i ^ x];
+            const vec2_t<T> b = *QSV_DBG(bra + (i ^ x));
             const double br = b.x, bi = b.y;
             tr = fma(br, wr, tr); tr = fma(bi, wi, tr);
             ti = fma(br, wi, ti); ti = fma(-bi, wr, ti);
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kStaticThreads) k_static_transition(const vec2
         ai = fma(tr, ki, ai); ai = fma(ti, kr, ai);
     }
     const double2 v = block_sum2(make_double2(ar, ai));
-    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+    if (threadIdx.x == 0) *QSV_DBG(partials + blockIdx.x) = v;
 }
 
 // fixed-order sum of the block partials into the slot after them
@@ -117,11 +117,12 @@ __global__ void k_static_final(unsigned char* __restrict__ scratch, unsigned nb)
     double2* partials = reinterpret_cast<double2*>(scratch + kOffPartials);
     double2 acc = make_double2(0, 0);
     for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) {
-        acc.x += partials[b].x;
-        acc.y += partials[b].y;
+        const double2 p = *QSV_DBG(partials + b);
+        acc.x += p.x;
+        acc.y += p.y;
     }
     acc = block_sum2(acc);
-    if (threadIdx.x == 0) partials[nb] = acc;
+    if (threadIdx.x == 0) *QSV_DBG(partials + nb) = acc;
 }
 
 std::mutex g_addr_mu;
@@ -212,6 +213,23 @@ extern "C" QSV_API int qsv_transition_static(const void* d_bra, const void* d_ke
     int rc = static_scratch_address(attr.device, reinterpret_cast<void**>(&scratch));
     if (rc != QSV_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+#ifdef QSV_DEBUG_BOUNDS
+    // debug build only: the caller's registers and the scratch join the range table for the
+    // length of the call (its bookkeeping allocates on the host)
+    const size_t reg_bytes = (size_t{1} << n_qubits) * (dtype == QSV_C128 ? 16 : 8);
+    QSV_DBG_TRACK(d_bra, reg_bytes);
+    QSV_DBG_TRACK(d_ket, reg_bytes);
+    QSV_DBG_TRACK(scratch, kStaticScratchBytes);
+    struct Untrack {
+        const void *a, *b, *c;
+        ~Untrack() {
+            cudaDeviceSynchronize();
+            QSV_DBG_UNTRACK(a);
+            QSV_DBG_UNTRACK(b);
+            QSV_DBG_UNTRACK(c);
+        }
+    } untrack{d_bra, d_ket, scratch};
+#endif
     // every slot the kernels read is written first in this call: the term tables by these
     // copies, each block's partial by its block, the result slot by the final kernel
     if ((e = cudaMemcpyAsync(scratch + kOffX, xmask, 8 * n_terms, cudaMemcpyHostToDevice, st)) != cudaSuccess)
@@ -240,5 +258,13 @@ extern "C" QSV_API int qsv_transition_static(const void* d_bra, const void* d_ke
                              st)) != cudaSuccess)
         return cuda_fail(e, "result copy");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "static transition");
+#ifdef QSV_DEBUG_BOUNDS
+    try {
+        ::qsv::dbg::after_call();
+    } catch (const std::exception& x) {
+        set_last_error(x.what());
+        return QSV_ERUNTIME;
+    }
+#endif
     return QSV_OK;
 }

@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
                                                                const TileOpDev* __restrict__ ops,
                                                                const cplx<T>* __restrict__ coef) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const TilePassDev P = passes[pass_idx];
+    const TilePassDev P = *QSV_DBG(passes + pass_idx);
     const int m = P.m;
     const uint32_t M = 1u << m;
     vec2_t<T>* buf0 = reinterpret_cast<vec2_t<T>*>(smem_raw);
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
     };
     auto issue = [&](vec2_t<T>* dst, uint64_t base) {
         for (uint32_t r = 0; r < R; ++r)
-            cp_async16(dst + (lt + (r << hi_shift)), s + (base | dep_lo | dep_hi(r)));
+            cp_async16(dst + (lt + (r << hi_shift)), QSV_DBG_N(s + (base | dep_lo | dep_hi(r)), 16));
     };
     const uint64_t n_tiles = 1ull << (n - m);
     const uint64_t G = gridDim.x;
@@ -283,11 +283,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
         __syncthreads();      // ... and everybody else's
         const uint64_t base = tile_base(t);
         for (uint32_t o = P.op_begin; o < P.op_end; ++o) {
-            const TileOpDev& op = ops[o];
+            const TileOpDev& op = *QSV_DBG(ops + o);
             // stage the op's coefficients next to the tile: reads inside the group loops then
             // cannot be hoisted past the tile stores (same address space), so the matrix is
             // not pinned in registers
-            for (uint32_t e = threadIdx.x; e < op.ncoef; e += blockDim.x) scoef[e] = coef[op.coef + e];
+            for (uint32_t e = threadIdx.x; e < op.ncoef; e += blockDim.x) scoef[e] = *QSV_DBG(coef + (op.coef + e));
             __syncthreads();
             tile_op<T>(cur, m, base, op, scoef);
             __syncthreads();
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
         for (uint32_t r = 0; r < R; ++r) {
             const uint32_t l = lt + (r << hi_shift);
             const float4 v = *reinterpret_cast<const float4*>(cur + l);
-            __stcs(reinterpret_cast<float4*>(s + (base | dep_lo | dep_hi(r))), v);
+            __stcs(reinterpret_cast<float4*>(QSV_DBG_N(s + (base | dep_lo | dep_hi(r)), 16)), v);
         }
         __syncthreads();      // the buffer is refilled two iterations from now
     }
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
                                                               const cplx<T>* __restrict__ coef,
                                                               double2* __restrict__ partials) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const TilePassDev P = passes[pass_idx];
+    const TilePassDev P = *QSV_DBG(passes + pass_idx);
     const int m = P.m;
     const uint32_t M = 1u << m;
     vec2_t<T>* bufs = reinterpret_cast<vec2_t<T>*>(smem_raw);   // [psi, phi]
@@ -419,9 +419,9 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
         const uint64_t* src = reinterpret_cast<const uint64_t*>(ops + P.op_begin);
         uint64_t* dst = reinterpret_cast<uint64_t*>(sops);
         const uint32_t words = n_ops * static_cast<uint32_t>(sizeof(TileOpDev) / 8);
-        for (uint32_t e = threadIdx.x; e < words; e += blockDim.x) dst[e] = src[e];
+        for (uint32_t e = threadIdx.x; e < words; e += blockDim.x) dst[e] = *QSV_DBG(src + e);
         for (uint32_t e = P.coef_begin + threadIdx.x; e < P.coef_end; e += blockDim.x)
-            scoef[e - P.coef_begin] = coef[e];
+            scoef[e - P.coef_begin] = *QSV_DBG(coef + e);
     }
     constexpr int kAmpsPerChunk = 16 / sizeof(vec2_t<T>);
     constexpr int acl = kAmpsPerChunk == 2 ? 1 : 0;
@@ -449,8 +449,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
     auto issue = [&](vec2_t<T>* dst, uint64_t base) {
         for (uint32_t r = 0; r < R; ++r) {
             const uint64_t gi = base | dep_lo | dep_hi(r);
-            cp_async16(dst + (lt + (r << hi_shift)), psi + gi);
-            cp_async16(dst + M + (lt + (r << hi_shift)), phi + gi);
+            cp_async16(dst + (lt + (r << hi_shift)), QSV_DBG_N(psi + gi, 16));
+            cp_async16(dst + M + (lt + (r << hi_shift)), QSV_DBG_N(phi + gi, 16));
         }
     };
     const uint64_t n_tiles = 1ull << (n - m);
@@ -491,8 +491,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
         for (uint32_t r = 0; r < R; ++r) {
             const uint32_t l = lt + (r << hi_shift);
             const uint64_t gi = base | dep_lo | dep_hi(r);
-            __stcs(reinterpret_cast<float4*>(psi + gi), *reinterpret_cast<const float4*>(cur + l));
-            __stcs(reinterpret_cast<float4*>(phi + gi), *reinterpret_cast<const float4*>(cur + M + l));
+            __stcs(reinterpret_cast<float4*>(QSV_DBG_N(psi + gi, 16)), *reinterpret_cast<const float4*>(cur + l));
+            __stcs(reinterpret_cast<float4*>(QSV_DBG_N(phi + gi, 16)), *reinterpret_cast<const float4*>(cur + M + l));
         }
         __syncthreads();   // every thread has read the tile out before the next copies land
         if (t + G < n_tiles) issue(bufs, tile_base(t + G));
@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
             v.x += acc[op.slot * kAdjWarps + w].x;
             v.y += acc[op.slot * kAdjWarps + w].y;
         }
-        partials[static_cast<size_t>(op.gslot) * gridDim.x + blockIdx.x] = v;
+        *QSV_DBG(partials + (static_cast<size_t>(op.gslot) * gridDim.x + blockIdx.x)) = v;
     }
 }
 

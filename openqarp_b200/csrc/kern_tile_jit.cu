@@ -725,6 +725,22 @@ __device__ __forceinline__ void cp16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src) : "memory");
 }
 )";
+#ifdef QSV_DEBUG_BOUNDS
+// debug build: every global index of a compiled pass is checked against the register; a miss
+// is counted in dbg[0] (first index in dbg[1]) and the access goes to amplitude 0 instead
+const char* kPreludeDebug = R"(
+__device__ __forceinline__ u64 dbg_idx(u64 i, u64 dim, unsigned long long* dbg) {
+    if (i < dim) return i;
+    if (atomicAdd(dbg, 1ull) == 0ull) dbg[1] = i;
+    return 0ull;
+}
+)";
+constexpr bool kJitDebug = true;
+#else
+const char* kPreludeDebug = "";
+constexpr bool kJitDebug = false;
+#endif
+
 
 // Walk one pass's plan: coefficients, structural signature and (with emit) the steps' source.
 // Returns false when the pass needs an op the generator does not handle or too many
@@ -876,14 +892,19 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
         gfin += " | ((u64)((lane >> " + std::to_string(k) + ") & 1u) << " + std::to_string(tq[F.lane[k]]) + ")";
     for (int k = 0; k < kRtWarpBits; ++k)
         gfin += " | ((u64)((warp >> " + std::to_string(k) + ") & 1u) << " + std::to_string(tq[F.warp[k]]) + ")";
+    // a global amplitude index: checked against the register in the debug build
+    const std::string dim = hex64(1ull << n);
+    auto at = [&](const std::string& e) {
+        return kJitDebug ? "dbg_idx(" + e + ", " + dim + ", dbg)" : "(" + e + ")";
+    };
     auto issue = [&](const std::string& b) {
         std::ostringstream x;
         for (int j = 0; j < chunks / kJitThreads; ++j) {
             uint64_t gj = 0;
             for (int b2 = 0; b2 < 4 && 8 + low + b2 < kRtQubits; ++b2)
                 if ((j >> b2) & 1) gj |= 1ull << tq[8 + low + b2];
-            x << "    cp16(xb + (stid ^ " << swz(static_cast<uint32_t>(j) * kJitThreads) << "u), s + ((" << b
-              << ") | gtid | " << hex64(gj) << "));\n";
+            x << "    cp16(xb + (stid ^ " << swz(static_cast<uint32_t>(j) * kJitThreads) << "u), s + "
+              << at("(" + b + ") | gtid | " + hex64(gj)) << ");\n";
         }
         return x.str();
     };
@@ -896,7 +917,8 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
     }
     s << "struct __align__(8) C" << idx << " { R c[" << nc << "]; };\n"
       << "extern \"C\" __global__ void __launch_bounds__(" << kJitThreads << ", " << jit_ctas(f32)
-      << ") qsv_jit_" << idx << "(R2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P) {\n"
+      << ") qsv_jit_" << idx << "(R2* __restrict__ s, u64 n_tiles, const __grid_constant__ C" << idx << " P"
+      << (kJitDebug ? ", unsigned long long* __restrict__ dbg" : "") << ") {\n"
       << "  extern __shared__ __align__(16) unsigned char smem[];\n"
       << "  double2* xb = reinterpret_cast<double2*>(smem);\n"
       << "  R2* xf = reinterpret_cast<R2*>(smem);\n"
@@ -937,7 +959,7 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
         uint64_t gc = 0;
         for (int p = 0; p < kRtRegBits; ++p)
             if ((r >> p) & 1) gc |= 1ull << tq[F.reg[p]];
-        s << "  __stcs(s + (base | gfin | " << hex64(gc) << "), MK(" << Gen::ar(r) << ", " << Gen::ai(r) << "));\n";
+        s << "  __stcs(s + " << at("base | gfin | " + hex64(gc)) << ", MK(" << Gen::ar(r) << ", " << Gen::ai(r) << "));\n";
     }
     s << "  }\n  asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");\n}\n";
     return s.str();
@@ -1082,6 +1104,49 @@ std::vector<PassWalk> walk_all(const std::vector<const TilePass*>& passes, std::
 }
 
 std::mutex g_jit_mu;
+
+#ifdef QSV_DEBUG_BOUNDS
+// the compiled passes' fault words (count, first index), one per device, polled with the other
+// translation units' records after every entry point
+std::mutex g_dbg_mu;
+std::map<int, unsigned long long*> g_dbg_words;
+
+unsigned long long* jit_fault_word(int device) {
+    std::lock_guard<std::mutex> lock(g_dbg_mu);
+    unsigned long long*& w = g_dbg_words[device];
+    if (!w) {
+        check_cuda(dev_malloc(&w, 2 * sizeof(unsigned long long)), "JIT debug word");
+        check_cuda(cudaMemset(w, 0, 2 * sizeof(unsigned long long)), "JIT debug word");
+    }
+    return w;
+}
+
+void jit_dbg_sync(const ::qsv::dbg::Ranges&) {}
+
+void jit_dbg_poll(::qsv::dbg::Fault* out) {
+    *out = ::qsv::dbg::Fault{};
+    int device = 0;
+    cudaGetDevice(&device);
+    unsigned long long* w = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_dbg_mu);
+        auto it = g_dbg_words.find(device);
+        if (it == g_dbg_words.end()) return;
+        w = it->second;
+    }
+    unsigned long long h[2] = {0, 0};
+    cudaMemcpy(h, w, sizeof h, cudaMemcpyDeviceToHost);
+    if (!h[0]) return;
+    out->count = h[0];
+    out->addr = h[1];   // an amplitude index, not an address
+    out->line = 0;
+    out->bytes = 0;
+    cudaMemset(w, 0, sizeof h);
+}
+
+[[maybe_unused]] const bool g_jit_dbg_registered =
+    ::qsv::dbg::register_unit("compiled tile pass (index)", &jit_dbg_sync, &jit_dbg_poll);
+#endif
 // compiled pass kernels, by (source hash, context); modules stay loaded until exit
 std::map<std::pair<uint64_t, CUcontext>, CUfunction> g_kernels;
 
@@ -1144,7 +1209,7 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
             Carry next;
             gen_pass(*passes[i], plans[i], n, 0, true, f32, &srcs[j], &coef, &sig, nullptr,
                      w.has_cin ? &w.cin : nullptr, w.final, w.final ? nullptr : &next);
-            srcs[j] = std::string(kPrelude) + srcs[j] + tag;
+            srcs[j] = std::string(kPrelude) + kPreludeDebug + srcs[j] + tag;
             char name[40];
             std::snprintf(name, sizeof name, "%016llx.cubin", static_cast<unsigned long long>(fnv1a(srcs[j])));
             files[j] = cache_dir() + "/" + name;
@@ -1196,7 +1261,12 @@ void jit_launch(const JitPlan& plan, int pass, void* s, int n, cudaStream_t st) 
     const unsigned grid = static_cast<unsigned>(
         std::min<unsigned long long>(n_tiles, static_cast<unsigned long long>(jit_ctas(plan.f32)) * sms));
     const std::vector<uint8_t>& c = plan.coef[static_cast<size_t>(k)];
+#ifdef QSV_DEBUG_BOUNDS
+    unsigned long long* dbg = jit_fault_word(device);
+    void* args[] = {&s, &n_tiles, const_cast<uint8_t*>(c.data()), &dbg};
+#else
     void* args[] = {&s, &n_tiles, const_cast<uint8_t*>(c.data())};
+#endif
     check_cu(driver().launch(static_cast<CUfunction>(plan.fns[static_cast<size_t>(k)]), grid, 1, 1, kJitThreads, 1, 1,
                              static_cast<unsigned>(jit_smem(plan.f32)),
                              reinterpret_cast<CUstream>(st), args, nullptr),
@@ -1204,7 +1274,7 @@ void jit_launch(const JitPlan& plan, int pass, void* s, int n, cudaStream_t st) 
 }
 
 std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int n, bool f32, size_t* n_kernels) {
-    std::string src = kPrelude;
+    std::string src = std::string(kPrelude) + kPreludeDebug;
     int next = 0;
     std::vector<RtPlan> plans;
     const std::vector<PassWalk> walks = walk_all(passes, plans, n, f32);

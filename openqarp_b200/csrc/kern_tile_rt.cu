@@ -399,6 +399,7 @@ __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict
     __shared__ uint8_t tq[kRtQubits];
     __shared__ uint8_t load[12];
     const RtPassDev* P = passes + pass_idx;
+    if (!QSV_DBG_RANGE_OK(P, sizeof(RtPassDev))) return;
     if (threadIdx.x < kRtQubits) tq[threadIdx.x] = P->tq[threadIdx.x];
     if (threadIdx.x < 12) load[threadIdx.x] = P->load[threadIdx.x];
     const uint32_t n_steps = P->step_end - P->step_begin;
@@ -406,6 +407,8 @@ __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict
     // every tile reads the pass's steps and coefficients: keep them on chip when they fit
     const RtStepDev* stp = steps + P->step_begin;
     const cplx<T>* cf = coef + P->coef_begin;
+    if (!QSV_DBG_RANGE_OK(stp, n_steps * sizeof(RtStepDev)) || !QSV_DBG_RANGE_OK(cf, n_coef * sizeof(cplx<T>)))
+        return;
     if constexpr (SMEM) {
         RtStepDev* ss = reinterpret_cast<RtStepDev*>(stage + (1 << kRtQubits));
         cplx<T>* sc = reinterpret_cast<cplx<T>*>(ss + ((n_steps + 1) & ~1u));
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict
             for (int b = 0; b < 4; ++b)
                 if ((j >> b) & 1) g |= gj[b];
             const uint32_t c = threadIdx.x + kRtThreads * j;
-            cp_async16(stage + swz(c), s + g);
+            cp_async16(stage + swz(c), QSV_DBG_N(s + g, 16));
         }
     };
     vec2_t<T> v[kRtAmps];
@@ -558,7 +561,7 @@ __global__ void __launch_bounds__(kRtThreads, 1) k_tile_rt(vec2_t<T>* __restrict
         }
         // the last layout has lanes = local bits 0..4: 32 consecutive amplitudes per warp store
 #pragma unroll
-        for (int r = 0; r < kRtAmps; ++r) __stcs(s + (base | L.glob(r)), v[r]);
+        for (int r = 0; r < kRtAmps; ++r) __stcs(QSV_DBG(s + (base | L.glob(r))), v[r]);
     }
     cp_async_wait0();
 }

@@ -60,7 +60,7 @@ __global__ void k_tr_guard(uint8_t* __restrict__ pass, const uint64_t* __restric
                            uint64_t cmask, uint64_t cwant) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots) return;
-    pass[s] = ((flags[s] & fmask) == fwant) && ((cbits[s] & cmask) == cwant);
+    (*QSV_DBG(pass + (s))) = (((*QSV_DBG(flags + (s))) & fmask) == fwant) && (((*QSV_DBG(cbits + (s))) & cmask) == cwant);
 }
 
 // BranchBegin (branch_condition_holds, qarp_simulator.cpp:340-350): flag bit `flag` = whether
@@ -69,8 +69,8 @@ __global__ void k_tr_branch(uint64_t* __restrict__ flags, const uint64_t* __rest
                             int flag, uint64_t cmask, uint64_t cwant) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots) return;
-    const uint64_t holds = (cbits[s] & cmask) == cwant ? 1ull : 0ull;
-    flags[s] = (flags[s] & ~(1ull << flag)) | (holds << flag);
+    const uint64_t holds = ((*QSV_DBG(cbits + (s))) & cmask) == cwant ? 1ull : 0ull;
+    (*QSV_DBG(flags + (s))) = ((*QSV_DBG(flags + (s))) & ~(1ull << flag)) | (holds << flag);
 }
 
 // A K-qubit unitary on the shots whose pass flag is set; one thread per (shot, group).
@@ -84,13 +84,13 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_dense(vec2_t<T>* __restrict__
     const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= groups * static_cast<uint64_t>(n_shots)) return;
     const uint64_t shot = t / groups, g = t % groups;
-    if (!pass[shot]) return;
+    if (!(*QSV_DBG(pass + (shot)))) return;
     vec2_t<T>* p = s + (shot << n);
     const uint64_t base = insert_zeros(g, a.pos, K);
     double xr[D], xi[D];
 #pragma unroll
     for (int x = 0; x < D; ++x) {
-        const vec2_t<T> v = p[base | a.off[x]];
+        const vec2_t<T> v = (*QSV_DBG(p + (base | a.off[x])));
         xr[x] = static_cast<double>(v.x);
         xi[x] = static_cast<double>(v.y);
     }
@@ -99,13 +99,13 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_dense(vec2_t<T>* __restrict__
         double re = 0.0, im = 0.0;
 #pragma unroll
         for (int x = 0; x < D; ++x) {
-            const cplx<double> c = m[y * D + x];
+            const cplx<double> c = (*QSV_DBG(m + (y * D + x)));
             re = fma(c.re, xr[x], re);
             re = fma(-c.im, xi[x], re);
             im = fma(c.re, xi[x], im);
             im = fma(c.im, xr[x], im);
         }
-        p[base | a.off[y]] = mk<T>(static_cast<T>(re), static_cast<T>(im));
+        (*QSV_DBG(p + (base | a.off[y]))) = mk<T>(static_cast<T>(re), static_cast<T>(im));
     }
 }
 
@@ -115,10 +115,10 @@ __global__ void k_tr_scale(vec2_t<T>* __restrict__ s, int n, int n_shots, const 
                            double re, double im) {
     const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= (static_cast<uint64_t>(n_shots) << n)) return;
-    if (!pass[t >> n]) return;
-    const vec2_t<T> a = s[t];
+    if (!(*QSV_DBG(pass + (t >> n)))) return;
+    const vec2_t<T> a = (*QSV_DBG(s + (t)));
     const double x = static_cast<double>(a.x), y = static_cast<double>(a.y);
-    s[t] = mk<T>(static_cast<T>(re * x - im * y), static_cast<T>(re * y + im * x));
+    (*QSV_DBG(s + (t))) = mk<T>(static_cast<T>(re * x - im * y), static_cast<T>(re * y + im * x));
 }
 
 // Partial sums of |a|^2 per (shot, 4096-amplitude chunk): over the amplitudes whose index has no
@@ -134,9 +134,9 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_chunk_sums(const vec2_t<T>* _
     const uint64_t idx0 = (b << clog) & ((1ull << n) - 1ull);   // index within the shot
     double acc = 0.0;
     for (uint64_t i = threadIdx.x; i < chunk; i += blockDim.x)
-        if (!((idx0 + i) & zero_mask)) acc += tr_norm2<T>(p[i]);
+        if (!((idx0 + i) & zero_mask)) acc += tr_norm2<T>((*QSV_DBG(p + (i))));
     const double tot = block_sum(acc, red);
-    if (threadIdx.x == 0) out[b] = tot;
+    if (threadIdx.x == 0) (*QSV_DBG(out + (b))) = tot;
 }
 
 // per shot: the chunk sums in index order -> the shot's sum
@@ -145,8 +145,8 @@ __global__ void k_tr_shot_sums(const double* __restrict__ chunk_sums, uint64_t n
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots) return;
     double t = 0.0;
-    for (uint64_t c = 0; c < n_chunks; ++c) t += chunk_sums[static_cast<uint64_t>(s) * n_chunks + c];
-    sum[s] = t;
+    for (uint64_t c = 0; c < n_chunks; ++c) t += (*QSV_DBG(chunk_sums + (static_cast<uint64_t>(s) * n_chunks + c)));
+    (*QSV_DBG(sum + (s))) = t;
 }
 
 // The shot-minor MT19937 states of a batch: word i of shot s at w[i * stride + s].
@@ -170,15 +170,15 @@ __global__ void k_tr_decide(const uint8_t* __restrict__ pass, const double* __re
                             double* __restrict__ scale) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots) return;
-    if (!pass[s]) {
-        outcome[s] = -1;
+    if (!(*QSV_DBG(pass + (s)))) {
+        (*QSV_DBG(outcome + (s))) = -1;
         return;
     }
     double sc = 0.0;
-    const bool one = tr_decide(p0[s], mt.of(s), &sc);
-    outcome[s] = one ? 1 : 0;
-    scale[s] = sc;
-    if (cbit >= 0) cbits[s] = one ? (cbits[s] | (1ull << cbit)) : (cbits[s] & ~(1ull << cbit));
+    const bool one = tr_decide((*QSV_DBG(p0 + (s))), mt.of(s), &sc);
+    (*QSV_DBG(outcome + (s))) = one ? 1 : 0;
+    (*QSV_DBG(scale + (s))) = sc;
+    if (cbit >= 0) (*QSV_DBG(cbits + (s))) = one ? ((*QSV_DBG(cbits + (s))) | (1ull << cbit)) : ((*QSV_DBG(cbits + (s))) & ~(1ull << cbit));
 }
 
 // ---------------------------------------------------------------- noise channels
@@ -201,26 +201,26 @@ __global__ void k_tr_noise_group(const uint8_t* __restrict__ pass, MtState mt, i
                                  uint64_t* __restrict__ ax, uint64_t* __restrict__ az, uint32_t* __restrict__ any,
                                  uint32_t* __restrict__ active, uint32_t* __restrict__ n_active) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n_shots || !pass[s]) return;
+    if (s >= n_shots || !(*QSV_DBG(pass + (s)))) return;
     const MtView g = mt.of(s);
     uint64_t x = 0, z = 0;
     uint32_t ny = 0;
     for (int c = 0; c < n_ch; ++c) {
         TrQubits tq;
-        tq.k = ch[c].k;
-        for (int b = 0; b < 32; ++b) tq.q[b] = ch[c].q[b];
+        tq.k = (*QSV_DBG(ch + (c))).k;
+        for (int b = 0; b < 32; ++b) tq.q[b] = (*QSV_DBG(ch + (c))).q[b];
         uint64_t xi, zi;
         uint32_t nyi;
-        tr_choose_pauli(ch[c].kind, prm + ch[c].poff, tq, g, xi, zi, nyi);
+        tr_choose_pauli((*QSV_DBG(ch + (c))).kind, prm + (*QSV_DBG(ch + (c))).poff, tq, g, xi, zi, nyi);
         x |= xi;
         z |= zi;
         ny += nyi;
     }
     if (x | z) {
-        ax[s] = x;
-        az[s] = z;
-        any[s] = ny;
-        active[atomicAdd(n_active, 1u)] = static_cast<uint32_t>(s);
+        (*QSV_DBG(ax + (s))) = x;
+        (*QSV_DBG(az + (s))) = z;
+        (*QSV_DBG(any + (s))) = ny;
+        (*QSV_DBG(active + (atomicAdd(QSV_DBG(n_active), 1u)))) = static_cast<uint32_t>(s);
     }
 }
 
@@ -234,23 +234,23 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_apply_pauli(vec2_t<T>* __rest
                                                               const uint32_t* __restrict__ active,
                                                               const uint32_t* __restrict__ n_active) {
     const uint64_t half = 1ull << (n - 1);
-    const uint64_t total = static_cast<uint64_t>(*n_active) * half;
+    const uint64_t total = static_cast<uint64_t>(*QSV_DBG(n_active)) * half;
     for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
          t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t shot = active[t / half];
+        const uint32_t shot = (*QSV_DBG(active + (t / half)));
         const uint64_t g = t % half;
-        const uint64_t x = ax[shot], z = az[shot];
-        const uint32_t ny = any[shot];
+        const uint64_t x = (*QSV_DBG(ax + (shot))), z = (*QSV_DBG(az + (shot)));
+        const uint32_t ny = (*QSV_DBG(any + (shot)));
         vec2_t<T>* p = s + (static_cast<uint64_t>(shot) << n);
         if (x == 0) {
-            for (uint64_t j = 2 * g; j < 2 * g + 2; ++j) p[j] = tr_pauli_phase<T>(p[j], ny, __popcll(j & z) & 1);
+            for (uint64_t j = 2 * g; j < 2 * g + 2; ++j) (*QSV_DBG(p + (j))) = tr_pauli_phase<T>((*QSV_DBG(p + (j))), ny, __popcll(j & z) & 1);
         } else {
             const int hb = 63 - __clzll(x);
             const uint64_t j = ((g >> hb) << (hb + 1)) | (g & ((1ull << hb) - 1ull));
             const uint64_t j2 = j ^ x;
-            const vec2_t<T> a = p[j], b = p[j2];
-            p[j2] = tr_pauli_phase<T>(a, ny, __popcll(j & z) & 1);
-            p[j] = tr_pauli_phase<T>(b, ny, __popcll(j2 & z) & 1);
+            const vec2_t<T> a = (*QSV_DBG(p + (j))), b = (*QSV_DBG(p + (j2)));
+            (*QSV_DBG(p + (j2))) = tr_pauli_phase<T>(a, ny, __popcll(j & z) & 1);
+            (*QSV_DBG(p + (j))) = tr_pauli_phase<T>(b, ny, __popcll(j2 & z) & 1);
         }
     }
 }
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_rho_chunks(const vec2_t<T>* _
     for (uint64_t i = threadIdx.x; i < pairs; i += blockDim.x) {
         const uint64_t g = c * pairs + i;
         const uint64_t i0 = ((g >> q) << (q + 1)) | (g & (qb - 1));
-        const vec2_t<T> a = p[i0], b = p[i0 | qb];
+        const vec2_t<T> a = (*QSV_DBG(p + (i0))), b = (*QSV_DBG(p + (i0 | qb)));
         const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
         r00 += ar * ar + ai * ai;
         r11 += br * br + bi * bi;
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_rho_chunks(const vec2_t<T>* _
     double v[4] = {r00, r11, rr, ri};
     for (int k = 0; k < 4; ++k) {
         const double t = block_sum(v[k], red);
-        if (threadIdx.x == 0) out[blockIdx.x * 4ull + k] = t;
+        if (threadIdx.x == 0) (*QSV_DBG(out + (blockIdx.x * 4ull + k))) = t;
         __syncthreads();
     }
 }
@@ -293,17 +293,17 @@ __global__ void k_tr_kraus_decide(const uint8_t* __restrict__ pass, const double
                                   int n_ops, int8_t* __restrict__ act, double* __restrict__ kmat) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_shots) return;
-    act[s] = 0;
-    if (!pass[s]) return;
+    (*QSV_DBG(act + (s))) = 0;
+    if (!(*QSV_DBG(pass + (s)))) return;
     double r00 = 0.0, r11 = 0.0, rr = 0.0, ri = 0.0;
     for (uint64_t c = 0; c < per_shot; ++c) {
-        const double* v = rho_chunks + (static_cast<uint64_t>(s) * per_shot + c) * 4;
+        const double* v = QSV_DBG_N(rho_chunks + (static_cast<uint64_t>(s) * per_shot + c) * 4, 32);
         r00 += v[0];
         r11 += v[1];
         rr += v[2];
         ri += v[3];
     }
-    if (tr_choose_kraus(r00, r11, rr, ri, kops, n_ops, mt.of(s), kmat + 8ull * s)) act[s] = 1;
+    if (tr_choose_kraus(r00, r11, rr, ri, kops, n_ops, mt.of(s), kmat + 8ull * s)) (*QSV_DBG(act + (s))) = 1;
 }
 
 // the chosen 2x2 operator on qubit q of every shot with act set
@@ -315,19 +315,19 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_apply_2x2(vec2_t<T>* __restri
     const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= pairs * static_cast<uint64_t>(n_shots)) return;
     const uint64_t shot = t / pairs, g = t % pairs;
-    if (!act[shot]) return;
+    if (!(*QSV_DBG(act + (shot)))) return;
     const double* m = kmat + 8 * shot;
     const uint64_t qb = 1ull << q;
     const uint64_t i0 = ((g >> q) << (q + 1)) | (g & (qb - 1));
     vec2_t<T>* p = s + (shot << n);
-    const vec2_t<T> a = p[i0], b = p[i0 | qb];
+    const vec2_t<T> a = (*QSV_DBG(p + (i0))), b = (*QSV_DBG(p + (i0 | qb)));
     const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
-    const double y0r = (m[0] * ar - m[1] * ai) + (m[2] * br - m[3] * bi);
-    const double y0i = (m[0] * ai + m[1] * ar) + (m[2] * bi + m[3] * br);
-    const double y1r = (m[4] * ar - m[5] * ai) + (m[6] * br - m[7] * bi);
-    const double y1i = (m[4] * ai + m[5] * ar) + (m[6] * bi + m[7] * br);
-    p[i0] = mk<T>(static_cast<T>(y0r), static_cast<T>(y0i));
-    p[i0 | qb] = mk<T>(static_cast<T>(y1r), static_cast<T>(y1i));
+    const double y0r = ((*QSV_DBG(m + (0))) * ar - (*QSV_DBG(m + (1))) * ai) + ((*QSV_DBG(m + (2))) * br - (*QSV_DBG(m + (3))) * bi);
+    const double y0i = ((*QSV_DBG(m + (0))) * ai + (*QSV_DBG(m + (1))) * ar) + ((*QSV_DBG(m + (2))) * bi + (*QSV_DBG(m + (3))) * br);
+    const double y1r = ((*QSV_DBG(m + (4))) * ar - (*QSV_DBG(m + (5))) * ai) + ((*QSV_DBG(m + (6))) * br - (*QSV_DBG(m + (7))) * bi);
+    const double y1i = ((*QSV_DBG(m + (4))) * ai + (*QSV_DBG(m + (5))) * ar) + ((*QSV_DBG(m + (6))) * bi + (*QSV_DBG(m + (7))) * br);
+    (*QSV_DBG(p + (i0))) = mk<T>(static_cast<T>(y0r), static_cast<T>(y0i));
+    (*QSV_DBG(p + (i0 | qb))) = mk<T>(static_cast<T>(y1r), static_cast<T>(y1i));
 }
 
 // Projection and renormalisation on the pairs (i, i | 2^q) of every deciding shot; Reset moves
@@ -340,22 +340,22 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_collapse(vec2_t<T>* __restric
     const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= pairs * static_cast<uint64_t>(n_shots)) return;
     const uint64_t shot = t / pairs, g = t % pairs;
-    const int o = outcome[shot];
+    const int o = (*QSV_DBG(outcome + (shot)));
     if (o < 0) return;
     const uint64_t qb = 1ull << q;
     const uint64_t i = ((g >> q) << (q + 1)) | (g & (qb - 1));
     vec2_t<T>* p = s + (shot << n);
-    const double sc = scale[shot];
-    const vec2_t<T> keep = o == 1 ? p[i | qb] : p[i];
+    const double sc = (*QSV_DBG(scale + (shot)));
+    const vec2_t<T> keep = o == 1 ? (*QSV_DBG(p + (i | qb))) : (*QSV_DBG(p + (i)));
     const vec2_t<T> v = mk<T>(static_cast<T>(static_cast<double>(keep.x) * sc),
                               static_cast<T>(static_cast<double>(keep.y) * sc));
     const vec2_t<T> z = mk<T>(T(0), T(0));
     if (o == 1 && !reset) {
-        p[i] = z;
-        p[i | qb] = v;
+        (*QSV_DBG(p + (i))) = z;
+        (*QSV_DBG(p + (i | qb))) = v;
     } else {
-        p[i] = v;
-        p[i | qb] = z;
+        (*QSV_DBG(p + (i))) = v;
+        (*QSV_DBG(p + (i | qb))) = z;
     }
 }
 
@@ -369,17 +369,17 @@ __global__ void k_tr_pick_chunk(const double* __restrict__ chunk_sums, uint64_t 
     if (s >= n_shots) return;
     const double* cs = chunk_sums + static_cast<uint64_t>(s) * n_chunks;
     double total = 0.0;
-    for (uint64_t c = 0; c < n_chunks; ++c) total += cs[c];
+    for (uint64_t c = 0; c < n_chunks; ++c) total += (*QSV_DBG(cs + (c)));
     const double thr = mt.of(s).canonical() * total;
     double acc = 0.0;
     uint64_t c = 0;
     for (; c + 1 < n_chunks; ++c) {
-        if (acc + cs[c] >= thr) break;
-        acc += cs[c];
+        if (acc + (*QSV_DBG(cs + (c))) >= thr) break;
+        acc += (*QSV_DBG(cs + (c)));
     }
-    threshold[s] = thr;
-    before[s] = acc;
-    chunk_of[s] = c;
+    (*QSV_DBG(threshold + (s))) = thr;
+    (*QSV_DBG(before + (s))) = acc;
+    (*QSV_DBG(chunk_of + (s))) = c;
 }
 
 // Final sample, step 2 (one block per shot): the first index of the chosen chunk whose running
@@ -394,16 +394,16 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_pick_index(const vec2_t<T>* _
     const uint64_t shot = blockIdx.x;
     const uint64_t chunk = 1ull << min(n, kTrChunkLog);
     const uint64_t per = chunk >= kTrThreads ? chunk / kTrThreads : 1;
-    const uint64_t start = chunk_of[shot] * chunk;
+    const uint64_t start = (*QSV_DBG(chunk_of + (shot))) * chunk;
     const vec2_t<T>* p = s + (shot << n) + start;
     const uint64_t lo = threadIdx.x * per;
     double run = 0.0;
-    for (uint64_t i = lo; i < lo + per && i < chunk; ++i) run += tr_norm2<T>(p[i]);
+    for (uint64_t i = lo; i < lo + per && i < chunk; ++i) run += tr_norm2<T>((*QSV_DBG(p + (i))));
     part[threadIdx.x] = run;
     __syncthreads();
     if (threadIdx.x != 0) return;
-    double acc = before[shot];
-    const double thr = threshold[shot];
+    double acc = (*QSV_DBG(before + (shot)));
+    const double thr = (*QSV_DBG(threshold + (shot)));
     uint64_t idx = chunk - 1;
     for (uint32_t t = 0; t < kTrThreads && t * per < chunk; ++t) {
         if (acc + part[t] < thr) {
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_pick_index(const vec2_t<T>* _
         }
         bool hit = false;
         for (uint64_t i = t * per; i < t * per + per && i < chunk; ++i) {
-            acc += tr_norm2<T>(p[i]);
+            acc += tr_norm2<T>((*QSV_DBG(p + (i))));
             if (acc >= thr) {
                 idx = i;
                 hit = true;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(kTrThreads) k_tr_pick_index(const vec2_t<T>* _
         }
         if (hit) break;
     }
-    out[shot] = start + idx;
+    (*QSV_DBG(out + (shot))) = start + idx;
 }
 
 // every shot of the batch starts from the prefix state
@@ -431,7 +431,7 @@ __global__ void k_tr_broadcast(vec2_t<T>* __restrict__ dst, const vec2_t<T>* __r
     const uint64_t mask = (1ull << n) - 1ull;
     for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
          t += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        dst[t] = src[t & mask];
+        (*QSV_DBG(dst + (t))) = (*QSV_DBG(src + (t & mask)));
 }
 
 // dst <- src on the shots whose pass flag is 0 (the wide-command fallback's restore)
@@ -441,7 +441,7 @@ __global__ void k_tr_restore(vec2_t<T>* __restrict__ dst, const vec2_t<T>* __res
     const uint64_t total = static_cast<uint64_t>(n_shots) << n;
     for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
          t += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        if (!pass[t >> n]) dst[t] = src[t];
+        if (!(*QSV_DBG(pass + (t >> n)))) (*QSV_DBG(dst + (t))) = (*QSV_DBG(src + (t)));
 }
 
 unsigned blocks_for(uint64_t work) {
@@ -695,14 +695,14 @@ namespace {
 struct DeviceBuffer {
     void* p = nullptr;
     explicit DeviceBuffer(size_t bytes) {
-        if (bytes && cudaMalloc(&p, bytes) != cudaSuccess) {
+        if (bytes && dev_malloc(&p, bytes) != cudaSuccess) {
             (void)cudaGetLastError();
             p = nullptr;
             throw std::bad_alloc();
         }
     }
     ~DeviceBuffer() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
     }
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;

@@ -255,13 +255,13 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
     if (resident) {
         const uint64_t* src = reinterpret_cast<const uint64_t*>(steps);
         const size_t words = static_cast<size_t>(n_steps) * (sizeof(FsStep) / 8);
-        for (size_t w = threadIdx.x; w < words; w += kFsThreads) rsteps[w] = __ldg(src + w);
-        for (uint32_t w = threadIdx.x; w < n_coef; w += kFsThreads) rcoef[w] = __ldg(coef + w);
+        for (size_t w = threadIdx.x; w < words; w += kFsThreads) rsteps[w] = __ldg(QSV_DBG(src + w));
+        for (uint32_t w = threadIdx.x; w < n_coef; w += kFsThreads) rcoef[w] = __ldg(QSV_DBG(coef + w));
     }
 
     // persistent CTAs: shots blockIdx.x, blockIdx.x + gridDim.x, ...
     for (uint64_t shot = blockIdx.x; shot < n_shots; shot += gridDim.x) {
-    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = prefix[i];
+    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = *QSV_DBG(prefix + i);
     if (threadIdx.x == 0) {
         g.seed(seed + static_cast<uint32_t>(shot0 + shot));
         cbits = 0;
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
         if (!resident) {
             const uint64_t* src = reinterpret_cast<const uint64_t*>(steps + si);
             for (int w = threadIdx.x; w < static_cast<int>(sizeof(FsStep) / 8); w += kFsThreads)
-                sstep[w] = __ldg(src + w);
+                sstep[w] = __ldg(QSV_DBG(src + w));
             __syncthreads();
         }
         const FsStep& S = resident ? *reinterpret_cast<const FsStep*>(rsteps + si * (sizeof(FsStep) / 8))
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
         }
         const double* c = rcoef + S.coef;
         if (!resident) {
-            for (uint32_t w = threadIdx.x; w < S.ncoef; w += kFsThreads) scoef[w] = __ldg(coef + S.coef + w);
+            for (uint32_t w = threadIdx.x; w < S.ncoef; w += kFsThreads) scoef[w] = __ldg(QSV_DBG(coef + (S.coef + w)));
             __syncthreads();
             c = scoef;
         }
@@ -430,8 +430,8 @@ __global__ void __launch_bounds__(kFsThreads, 3) k_fs_run(const FsStep* __restri
         }
         if (hit) break;
     }
-    out_idx[shot] = idx;
-    out_cbits[shot] = cbits;
+    *QSV_DBG(out_idx + shot) = idx;
+    *QSV_DBG(out_cbits + shot) = cbits;
     }
     __syncthreads();   // the next shot overwrites the amplitudes, part[] and the engine
     }
@@ -455,10 +455,10 @@ __global__ void __launch_bounds__(kFsThreads) k_fs_apply(const FsStep* __restric
     if (resident) {
         const uint64_t* src = reinterpret_cast<const uint64_t*>(steps);
         const size_t words = static_cast<size_t>(n_steps) * (sizeof(FsStep) / 8);
-        for (size_t w = threadIdx.x; w < words; w += kFsThreads) rsteps[w] = __ldg(src + w);
-        for (uint32_t w = threadIdx.x; w < n_coef; w += kFsThreads) rcoef[w] = __ldg(coef + w);
+        for (size_t w = threadIdx.x; w < words; w += kFsThreads) rsteps[w] = __ldg(QSV_DBG(src + w));
+        for (uint32_t w = threadIdx.x; w < n_coef; w += kFsThreads) rcoef[w] = __ldg(QSV_DBG(coef + w));
     }
-    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = state[i];
+    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) a[i] = *QSV_DBG(state + i);
     __syncthreads();
     for (int si = 0; si < n_steps; ++si) {
         const double* c;
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(kFsThreads) k_fs_apply(const FsStep* __restric
         } else {
             const uint64_t* src = reinterpret_cast<const uint64_t*>(steps + si);
             for (int w = threadIdx.x; w < static_cast<int>(sizeof(FsStep) / 8); w += kFsThreads)
-                sstep[w] = __ldg(src + w);
+                sstep[w] = __ldg(QSV_DBG(src + w));
             __syncthreads();
             S = reinterpret_cast<const FsStep*>(sstep);
             for (uint32_t w = threadIdx.x; w < S->ncoef; w += kFsThreads) scoef[w] = __ldg(coef + S->coef + w);
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(kFsThreads) k_fs_apply(const FsStep* __restric
         fs_gate<T>(a, n, *S, c);
         __syncthreads();
     }
-    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) state[i] = a[i];
+    for (uint64_t i = threadIdx.x; i < dim; i += kFsThreads) *QSV_DBG(state + i) = a[i];
 }
 
 // host: the plan's steps as FsSteps; false when a step has no shared-memory form
@@ -840,11 +840,11 @@ __global__ void __launch_bounds__(kFsThreads) k_cb_run(const CbInstDev* __restri
     __shared__ double red[2 * kFsThreads / 32];
     __shared__ int cur;
     for (;;) {
-        if (threadIdx.x == 0) cur = atomicAdd(queue, 1);
+        if (threadIdx.x == 0) cur = atomicAdd(QSV_DBG(queue), 1);
         __syncthreads();
         const int i = cur;
         if (i >= n_inst) break;
-        const CbInstDev I = inst[i];
+        const CbInstDev I = *QSV_DBG(inst + i);
         const int n = I.n;
         const uint64_t dim = 1ull << n;
         for (uint64_t j = threadIdx.x; j < dim; j += kFsThreads) psi[j] = make_double2(j == 0 ? 1.0 : 0.0, 0.0);
@@ -852,11 +852,11 @@ __global__ void __launch_bounds__(kFsThreads) k_cb_run(const CbInstDev* __restri
         auto stage = [&](uint32_t s) -> const FsStep& {
             __syncthreads();
             const uint64_t* src = reinterpret_cast<const uint64_t*>(steps + s);
-            for (int w = threadIdx.x; w < static_cast<int>(sizeof(FsStep) / 8); w += kFsThreads) sstep[w] = __ldg(src + w);
+            for (int w = threadIdx.x; w < static_cast<int>(sizeof(FsStep) / 8); w += kFsThreads) sstep[w] = __ldg(QSV_DBG(src + w));
             __syncthreads();
             const FsStep& S = *reinterpret_cast<const FsStep*>(sstep);
             for (uint32_t w = threadIdx.x; w < S.ncoef && w < static_cast<uint32_t>(kFsMaxCoef); w += kFsThreads)
-                scoef[w] = __ldg(coef + S.coef + w);
+                scoef[w] = __ldg(QSV_DBG(coef + (S.coef + w)));
             __syncthreads();
             return S;
         };
@@ -870,8 +870,8 @@ __global__ void __launch_bounds__(kFsThreads) k_cb_run(const CbInstDev* __restri
         for (uint64_t j = threadIdx.x; j < dim; j += kFsThreads) {
             double fr = 0.0, fi = 0.0;
             for (uint32_t t = I.t0; t < I.t1; ++t) {
-                const uint64_t x = __ldg(tx + t), z = __ldg(tz + t);
-                const double2 c = __ldg(tc + t);
+                const uint64_t x = __ldg(QSV_DBG(tx + t)), z = __ldg(QSV_DBG(tz + t));
+                const double2 c = __ldg(QSV_DBG(tc + t));
                 const double2 v = psi[j ^ x];
                 const double sg = (__popcll((j ^ x) & z) & 1) ? -1.0 : 1.0;
                 fr = fma(sg, c.x * v.x - c.y * v.y, fr);
@@ -883,14 +883,14 @@ __global__ void __launch_bounds__(kFsThreads) k_cb_run(const CbInstDev* __restri
             er = fma(p.y, fi, er);
         }
         const double2 e = cb_block_sum2(make_double2(er, 0.0), red);
-        if (threadIdx.x == 0) energy[I.pad] = e.x;   // at the caller's instance index
+        if (threadIdx.x == 0) *QSV_DBG(energy + I.pad) = e.x;   // at the caller's instance index
         if (with_grad) {
             for (uint32_t s = I.r0; s < I.r1; ++s) {
                 const FsStep& S = stage(s);
                 if (S.kind == FS_ADJ) {
                     const int D = 1 << S.k;
                     const double2 ip = cb_adj_inner(psi, phi, n, S, scoef, red);
-                    if (threadIdx.x == 0) slots[I.slot0 + static_cast<uint32_t>(S.cbit)] = ip;
+                    if (threadIdx.x == 0) *QSV_DBG(slots + (I.slot0 + static_cast<uint32_t>(S.cbit))) = ip;
                     const double* d = scoef + 2 * D * D;
                     if (S.k == 0) {
                         for (uint64_t j = threadIdx.x; j < dim; j += kFsThreads) {
@@ -999,7 +999,7 @@ struct CircuitBatch {
     ~CircuitBatch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        if (dev) cudaFree(dev);
+        if (dev) dev_free(dev);
         if (host_coef) cudaFreeHost(host_coef);
         if (host_out) cudaFreeHost(host_out);
         if (e0) cudaEventDestroy(e0);
@@ -1123,7 +1123,7 @@ void cb_finalize(CircuitBatch* b) {
     b->off_energy = b->off_queue + 256;
     b->off_slots = b->off_energy + align(n_inst * 8);
     b->total = b->off_slots + align(std::max<uint32_t>(b->n_slots, 1) * 16);
-    check_cuda(cudaMalloc(&b->dev, b->total), "circuit batch buffers");
+    check_cuda(dev_malloc(&b->dev, b->total), "circuit batch buffers");
     check_cuda(cudaMallocHost(&b->host_coef, b->coef.size() * sizeof(double)), "pinned coefficients");
     check_cuda(cudaMallocHost(&b->host_out, (n_inst + 2 * std::max<uint32_t>(b->n_slots, 1)) * sizeof(double)),
                "pinned results");

@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
     // W (N = 64 rows x K = 64) in the K-major layout, split hi/lo
     for (int e = tid; e < kUR * kUChunks; e += blockDim.x) {
         const int r = e / kUChunks, kc = e % kUChunks;
-        const float4 v = make_float4(W[r * kUR + 4 * kc], W[r * kUR + 4 * kc + 1], W[r * kUR + 4 * kc + 2],
-                                     W[r * kUR + 4 * kc + 3]);
+        const float* wr = QSV_DBG_N(W + (r * kUR + 4 * kc), 16);
+        const float4 v = make_float4(wr[0], wr[1], wr[2], wr[3]);
         split_store(b_hi, b_lo, kmajor_offset(r, 4 * kc), v);
     }
     if (tid == 0) {
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
 #pragma unroll
             for (int x = 0; x < kUD; ++x) {
                 const uint32_t sd = static_cast<uint32_t>(__cvta_generic_to_shared(dst + x * kUM));
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sd), "l"(s + (gb | a.off[x]))
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sd), "l"(QSV_DBG(s + (gb | a.off[x])))
                              : "memory");
             }
         }
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
         if (!ok) s_fail = 1;
         __syncthreads();
         if (s_fail) {
-            if (tid == 0) atomicExch(err, 1);
+            if (tid == 0) atomicExch(QSV_DBG(err), 1);
             break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kUThreads) k_dense5_umma(float2* __restrict__ 
         if (live) {
 #pragma unroll
             for (int x = 0; x < kUD; ++x)
-                __stcs(s + (gb | a.off[x]), make_float2(__uint_as_float(d[x]), __uint_as_float(d[kUD + x])));
+                __stcs(QSV_DBG(s + (gb | a.off[x])), make_float2(__uint_as_float(d[x]), __uint_as_float(d[kUD + x])));
         }
         // every warp has read its TMEM lanes before the next tile's first MMA overwrites them
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -275,8 +275,8 @@ __global__ void __launch_bounds__(kUThreads, 1) k_dense5_umma2(float2* __restric
 
     for (int e = tid; e < kUR * kUChunks; e += blockDim.x) {
         const int r = e / kUChunks, kc = e % kUChunks;
-        const float4 v = make_float4(W[r * kUR + 4 * kc], W[r * kUR + 4 * kc + 1], W[r * kUR + 4 * kc + 2],
-                                     W[r * kUR + 4 * kc + 3]);
+        const float* wr = QSV_DBG_N(W + (r * kUR + 4 * kc), 16);
+        const float4 v = make_float4(wr[0], wr[1], wr[2], wr[3]);
         split_store(b_hi, b_lo, kmajor_offset(r, 4 * kc), v);
     }
     if (tid == 0) {
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kUThreads, 1) k_dense5_umma2(float2* __restric
 #pragma unroll
             for (int x = 0; x < kUD; ++x) {
                 const uint32_t sd = static_cast<uint32_t>(__cvta_generic_to_shared(raw + x * kUM + tid));
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sd), "l"(s + (gb | a.off[x]))
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sd), "l"(QSV_DBG_N(s + (gb | a.off[x]), 16))
                              : "memory");
             }
         }
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kUThreads, 1) k_dense5_umma2(float2* __restric
         if (!ok) s_fail = 1;
         __syncthreads();
         if (s_fail) {
-            if (tid == 0) atomicExch(err, 1);
+            if (tid == 0) atomicExch(QSV_DBG(err), 1);
             break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(kUThreads, 1) k_dense5_umma2(float2* __restric
         if (live) {
 #pragma unroll
             for (int x = 0; x < kUD; ++x)
-                __stcs(reinterpret_cast<float4*>(s + (gb | a.off[x])),
+                __stcs(reinterpret_cast<float4*>(QSV_DBG_N(s + (gb | a.off[x]), 16)),
                        make_float4(__uint_as_float(d0[x]), __uint_as_float(d0[kUD + x]), __uint_as_float(d1[x]),
                                    __uint_as_float(d1[kUD + x])));
         }

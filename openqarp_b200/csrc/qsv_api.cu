@@ -18,6 +18,116 @@
 #include "kernels.h"
 #include "lower.h"
 
+#ifdef QSV_DEBUG_BOUNDS
+#include <cstdio>
+#include <map>
+#include <mutex>
+
+namespace qsv {
+namespace dbg {
+namespace {
+struct Unit {
+    const char* file;
+    SyncFn sync;
+    PollFn poll;
+};
+std::vector<Unit>& units() {
+    static std::vector<Unit> u;
+    return u;
+}
+std::mutex& mu() {
+    static std::mutex m;
+    return m;
+}
+// per device: base address -> (bytes, references); a caller buffer handed to an entry point
+// can also be a buffer the library holds (a handle's register passed to qsv_transition_static)
+struct Live {
+    size_t bytes = 0;
+    int refs = 0;
+};
+std::map<int, std::map<uintptr_t, Live>>& live() {
+    static std::map<int, std::map<uintptr_t, Live>> l;
+    return l;
+}
+void sync_device(int dev) {
+    static Ranges r;   // 8 KiB: kept off the stack
+    r.count = 0;
+    for (const auto& [base, b] : live()[dev]) {
+        if (r.count == kMaxRanges) throw std::runtime_error("debug bounds: more live buffers than the range table holds");
+        r.lo[r.count] = base;
+        r.hi[r.count] = base + b.bytes;
+        ++r.count;
+    }
+    for (const Unit& u : units()) u.sync(r);
+}
+}  // namespace
+
+bool register_unit(const char* file, SyncFn sync, PollFn poll) {
+    units().push_back({file, sync, poll});
+    return true;
+}
+
+void track(const void* p, size_t bytes) {
+    if (!p || !bytes) return;
+    std::lock_guard<std::mutex> lock(mu());
+    int dev = 0;
+    cudaGetDevice(&dev);
+    // no kernel may read the table while it changes
+    cudaDeviceSynchronize();
+    Live& b = live()[dev][reinterpret_cast<uintptr_t>(p)];
+    b.bytes = std::max(b.bytes, bytes);
+    ++b.refs;
+    sync_device(dev);
+}
+
+void untrack(const void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(mu());
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceSynchronize();
+    auto& m = live()[dev];
+    auto it = m.find(reinterpret_cast<uintptr_t>(p));
+    if (it == m.end()) return;
+    if (--it->second.refs == 0) {
+        m.erase(it);
+        sync_device(dev);
+    }
+}
+
+void after_call() {
+    std::lock_guard<std::mutex> lock(mu());
+    int cur = 0;
+    cudaGetDevice(&cur);
+    std::string msg;
+    for (const auto& [dev, bufs] : live()) {
+        if (bufs.empty()) continue;
+        cudaSetDevice(dev);
+        cudaDeviceSynchronize();
+        for (const Unit& u : units()) {
+            Fault f{};
+            u.poll(&f);
+            if (f.count && msg.empty()) {
+                char b[256];
+                std::snprintf(b, sizeof b,
+                              "debug bounds: %llu access(es) outside every live buffer on device %d; first at "
+                              "0x%llx (%llu bytes), %s:%llu",
+                              f.count, dev, f.addr, f.bytes, u.file, f.line);
+                msg = b;
+            }
+        }
+    }
+    cudaSetDevice(cur);
+    if (!msg.empty()) throw std::runtime_error(msg);
+}
+
+}  // namespace dbg
+}  // namespace qsv
+#define QSV_DBG_AFTER_CALL() ::qsv::dbg::after_call()
+#else
+#define QSV_DBG_AFTER_CALL() ((void)0)
+#endif
+
 namespace qsv {
 namespace {
 
@@ -79,6 +189,7 @@ int guarded(F&& f) {
     try {
         g_err.clear();
         f();
+        QSV_DBG_AFTER_CALL();
         return QSV_OK;
     } catch (const capability_error& e) {
         return fail(QSV_ECAPABILITY, e.what());
@@ -108,10 +219,10 @@ float2* S64(Handle* h) { return static_cast<float2*>(h->state); }
 void* aux_state(Handle* h) {
     const size_t bytes = h->dim() * h->amp_bytes();
     if (h->aux && h->aux_cap >= bytes) return h->aux;
-    if (h->aux) cudaFree(h->aux);
+    if (h->aux) dev_free(h->aux);
     h->aux = nullptr;
     h->aux_cap = 0;
-    if (cudaMalloc(&h->aux, bytes) != cudaSuccess) {
+    if (dev_malloc(&h->aux, bytes) != cudaSuccess) {
         h->aux = nullptr;
         throw std::bad_alloc();
     }
@@ -318,7 +429,7 @@ int qsv_create(int n_qubits, int dtype, int device, void** out) {
             check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
             check_cuda(cudaEventCreate(&h->e0), "event");
             check_cuda(cudaEventCreate(&h->e1), "event");
-            if (cudaMalloc(&h->state, h->dim() * h->amp_bytes()) != cudaSuccess) {
+            if (dev_malloc(&h->state, h->dim() * h->amp_bytes()) != cudaSuccess) {
                 h->state = nullptr;
                 cudaGetLastError();
                 throw std::bad_alloc();
@@ -330,7 +441,7 @@ int qsv_create(int n_qubits, int dtype, int device, void** out) {
                                        h->amp_bytes(), cudaMemcpyHostToDevice, h->stream), "init");
             check_cuda(cudaStreamSynchronize(h->stream), "init");
         } catch (...) {
-            if (h->state) cudaFree(h->state);
+            if (h->state) dev_free(h->state);
             if (h->stream) cudaStreamDestroy(h->stream);
             delete h;
             throw;
@@ -346,9 +457,9 @@ int qsv_destroy(void* hp) {
         cudaSetDevice(h->device);
         if (h->stream) cudaStreamSynchronize(h->stream);
         h->ws.release();
-        if (h->state) cudaFree(h->state);
-        if (h->aux) cudaFree(h->aux);
-        for (void* b : h->ckpt) cudaFree(b);
+        if (h->state) dev_free(h->state);
+        if (h->aux) dev_free(h->aux);
+        for (void* b : h->ckpt) dev_free(b);
         if (h->e0) cudaEventDestroy(h->e0);
         if (h->e1) cudaEventDestroy(h->e1);
         if (h->stream) cudaStreamDestroy(h->stream);
@@ -571,6 +682,53 @@ int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int dtype, int max_
         *n_passes = static_cast<int32_t>(passes.size());
         *n_kernels = static_cast<int32_t>(k);
         *cubin_bytes = k ? jit_compile_for_test(src, cc_major, cc_minor).size() : 0;
+    });
+}
+
+#ifdef QSV_DEBUG_BOUNDS
+namespace qsv {
+namespace {
+// the self-test's probe: one checked read of buf[idx] into buf[0]
+__global__ void k_dbg_probe(double2* buf, uint64_t idx) {
+    *QSV_DBG(buf) = *QSV_DBG(buf + idx);
+}
+
+// 1 when the probe of buf[idx] (1 KiB of the 4 KiB buffer known to the checks) was flagged
+int32_t dbg_probe(uint64_t idx) {
+    void* raw = nullptr;
+    check_cuda(cudaMalloc(&raw, 4096), "self-test buffer");
+    double2* buf = static_cast<double2*>(raw);
+    dbg::track(buf, 1024);
+    k_dbg_probe<<<1, 1>>>(buf, idx);
+    cudaError_t e = cudaGetLastError();
+    int32_t caught = 0;
+    try {
+        dbg::after_call();
+    } catch (const std::runtime_error&) {
+        caught = 1;
+    }
+    dbg::untrack(buf);
+    cudaFree(raw);
+    check_cuda(e, "self-test probe");
+    return caught;
+}
+}  // namespace
+}  // namespace qsv
+#endif
+
+int qsv_debug_bounds_selftest(int device, int32_t* caught_in, int32_t* caught_out) {
+    return guarded([&] {
+        if (!caught_in || !caught_out) throw std::invalid_argument("null output");
+#ifdef QSV_DEBUG_BOUNDS
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        // every read lies inside the 4 KiB allocation: element 1 inside the known kilobyte,
+        // element 128 (2 KiB in) outside it
+        *caught_in = dbg_probe(1);
+        *caught_out = dbg_probe(128);
+#else
+        (void)device;
+        throw capability_error("the release build has no bounds checks: load libqsv_debug.so");
+#endif
     });
 }
 
@@ -955,7 +1113,7 @@ void adjoint_forward(Handle* h, const std::vector<Cmd>& cs, Checkpoints& ck) {
     const size_t bytes = h->dim() * h->amp_bytes();
     const size_t S = K ? (cs.size() + K - 1) / K : 1;
     if (h->ckpt_bytes != bytes) {   // kept buffers of another register size cannot be reused
-        for (void* b : h->ckpt) cudaFree(b);
+        for (void* b : h->ckpt) dev_free(b);
         h->ckpt.clear();
         h->ckpt_bytes = bytes;
     }
@@ -970,7 +1128,7 @@ void adjoint_forward(Handle* h, const std::vector<Cmd>& cs, Checkpoints& ck) {
     ck.K = K;
     while (h->ckpt.size() < S - 1) {
         void* b = nullptr;
-        if (cudaMalloc(&b, bytes) != cudaSuccess) {
+        if (dev_malloc(&b, bytes) != cudaSuccess) {
             (void)cudaGetLastError();
             throw std::bad_alloc();
         }

@@ -91,3 +91,5 @@ inline unsigned grid_for(uint64_t work, int per_thread = 1, unsigned cap = 1u <<
 }
 
 }  // namespace qsv
+
+#include "debug_bounds.cuh"

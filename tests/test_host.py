@@ -215,3 +215,17 @@ def test_jit_tile_kernels_compile_without_a_gpu(dtype):
         _lib.check(_lib.lib.qsv_jit_check(_lib.u8ptr(buf), len(buf), n, dtype, 1, 12, 10, 0, ctypes.byref(p),
                                           ctypes.byref(k), ctypes.byref(b)))
         assert k.value == p.value > 0 and b.value > 0
+
+
+def test_debug_build_exports_every_declared_symbol():
+    """The bounds-checked debug build (libqsv_debug.so) is the same C-ABI; the release build
+    refuses its self-test with QSV_ECAPABILITY."""
+    import ctypes
+    path = os.path.join(ROOT, "openqarp_b200", "libqsv_debug.so")
+    if not os.path.exists(path):
+        pytest.skip("debug build not built (make -C openqarp_b200/csrc DEBUG_BOUNDS=1)")
+    dbg = ctypes.CDLL(path)
+    for name in declared_symbols():
+        assert hasattr(dbg, name), name
+    a, b = ctypes.c_int32(), ctypes.c_int32()
+    assert _lib.lib.qsv_debug_bounds_selftest(0, ctypes.byref(a), ctypes.byref(b)) == _lib.QSV_ECAPABILITY
