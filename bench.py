@@ -280,15 +280,16 @@ def adjoint_vs_param_shift(device, shift_sample=12):
                                                                   max_weight=4, coeff_std=0.1)
     sim = B200Simulator(device=device)
     masks = observable.to_masks(obs, ADJ_N)
-    stream = ir.pack(cmds, vals, names)
-    reg = sim.register(ADJ_N)
-    reg.reset()
-    reg.adjoint(stream, len(names), masks)       # warm-up
+    # through the plugin call (autotuned forward plan, then the adjoint sweep); the first call
+    # tunes and compiles
+    sim.energy_and_gradient(cmds, ADJ_N, obs, vals, names)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    reg.reset()
-    energy, grad = reg.adjoint(stream, len(names), masks)
+    energy, grad = sim.energy_and_gradient(cmds, ADJ_N, obs, vals, names)
     t_adj = time.perf_counter() - t0
+    grad = np.asarray(grad)
+    forward_plan = dict(sim.last_plan)
+    reg = sim.register(ADJ_N)
     # parameter shift: 2 energy evaluations per parameter occurrence, timed on a sample
     concrete = [Command(c.gate, c.qubits, tuple(p.evaluate(vals) for p in c.params)) for c in cmds]
     param_idx = [i for i, c in enumerate(cmds) if c.is_parametric()]
@@ -317,17 +318,15 @@ def adjoint_vs_param_shift(device, shift_sample=12):
                                                        for i in sample]])))
     sim.close()
     # the same adjoint in complex64 bulk mode (FP64 accumulations, checkpointed psi)
-    from openqarp_b200 import Register
-    r64 = Register(ADJ_N, "complex64", device)
-    r64.reset()
-    r64.adjoint(stream, len(names), masks)
+    s64 = B200Simulator(device=device, dtype="complex64")
+    s64.energy_and_gradient(cmds, ADJ_N, obs, vals, names)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    r64.reset()
-    e64, g64 = r64.adjoint(stream, len(names), masks)
+    e64, g64 = s64.energy_and_gradient(cmds, ADJ_N, obs, vals, names)
     t_adj64 = time.perf_counter() - t0
-    r64.close()
+    s64.close()
     return {"n_qubits": ADJ_N, "params": len(names), "terms": len(obs), "energy": energy,
+            "call": "B200Simulator.energy_and_gradient", "forward_plan": forward_plan,
             "complex64": {"adjoint_s": t_adj64, "adjoint_grads_per_s": 1.0 / t_adj64,
                           "max_abs_grad_diff_vs_complex128": float(np.max(np.abs(np.asarray(g64) - grad))),
                           "energy_diff_vs_complex128": abs(e64 - energy)},

@@ -288,7 +288,7 @@ void apply_cmds(Handle* h, std::vector<Cmd> cmds, bool fuse) {
                                                                : default_tile_qubits(h->n, static_cast<int>(h->amp_bytes()));
         // the compiled passes generate their own addressing and need only line-sized runs
         const int low = h->executor == 3 ? coalesced_low_qubits(static_cast<int>(h->amp_bytes())) : kTileLowQubits;
-        const std::vector<TilePass> passes = plan_tiles(ops, h->n, m, low);
+        const std::vector<TilePass> passes = plan_tiles(ops, h->n, m, low, h->executor == 3 ? kJitPlanSeeds : 0);
         auto stream_op = [h](const Op& o) { launch(h, o, h->state); };
         const bool rt = h->executor == 1 || h->executor == 3;
         const bool jit = h->executor == 3;
@@ -668,7 +668,7 @@ int qsv_jit_check(const uint8_t* cmds, size_t nbytes, int n, int dtype, int max_
             for (Op& o : lower(c, n)) ops.push_back(std::move(o));
         if (dtype != QSV_C128 && dtype != QSV_C64) throw std::invalid_argument("dtype must be QSV_C128 or QSV_C64");
         const std::vector<TilePass> passes =
-            plan_tiles(ops, n, kRtQubits, coalesced_low_qubits(dtype == QSV_C128 ? 16 : 8));
+            plan_tiles(ops, n, kRtQubits, coalesced_low_qubits(dtype == QSV_C128 ? 16 : 8), kJitPlanSeeds);
         std::vector<const TilePass*> ptrs;
         for (const TilePass& p : passes) ptrs.push_back(&p);
         size_t k = 0;

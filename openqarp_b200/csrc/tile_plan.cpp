@@ -52,10 +52,45 @@ uint64_t op_support_mask(const Op& op) {
     }
 }
 
-std::vector<TilePass> plan_tiles(const std::vector<Op>& ops_in, int n, int m, int c) {
-    if (m > kTileMaxQubits) throw std::invalid_argument("tile wider than the shared-memory limit");
-    m = std::min(m, n);
-    c = std::min(c, m);
+namespace {
+
+// One greedy pass over the remaining ops (in order): an op joins the pass when it shares no
+// qubit with an op left behind earlier (so it commutes with everything it overtakes) and its
+// mixing qubits still fit the tile, which starts as `start`.  Returns the tile and marks the
+// ops taken; the score counts the ops taken, a non-diagonal op 4x a diagonal one.
+struct Greedy {
+    uint64_t tile = 0;
+    std::vector<char> take;
+    int score = 0;
+};
+
+Greedy greedy_pass(const std::vector<uint64_t>& sup, const std::vector<uint64_t>& mix, const std::vector<char>& fit,
+                   int m, uint64_t start) {
+    Greedy g;
+    g.tile = start;
+    g.take.assign(sup.size(), 0);
+    int width = __builtin_popcountll(start);
+    uint64_t blocked = 0;
+    for (size_t i = 0; i < sup.size(); ++i) {
+        if (sup[i] & blocked) {
+            blocked |= sup[i];
+            continue;
+        }
+        const uint64_t need = mix[i] & ~g.tile;
+        const int extra = __builtin_popcountll(need);
+        if (fit[i] && width + extra <= m) {
+            g.tile |= need;
+            width += extra;
+            g.take[i] = 1;
+            g.score += mix[i] ? 4 : 1;
+        } else {
+            blocked |= sup[i];
+        }
+    }
+    return g;
+}
+
+std::vector<TilePass> plan_tiles_once(const std::vector<Op>& ops_in, int n, int m, int c, int seeds) {
     std::vector<Op> remaining;
     for (const Op& o : ops_in)
         if (o.kind != OP_NOP) remaining.push_back(o);
@@ -68,6 +103,8 @@ std::vector<TilePass> plan_tiles(const std::vector<Op>& ops_in, int n, int m, in
         if (o.ctrl != 0) return false;         // controlled dense: a stream pass
         return __builtin_popcountll(op_mixing_mask(o) & ~low) + c <= m;
     };
+    std::vector<uint64_t> sup, mix;
+    std::vector<char> fit;
     while (!remaining.empty()) {
         if (!fits(remaining.front())) {
             TilePass single;   // empty tile_qubits: one stream pass
@@ -76,32 +113,38 @@ std::vector<TilePass> plan_tiles(const std::vector<Op>& ops_in, int n, int m, in
             remaining.erase(remaining.begin());
             continue;
         }
-        uint64_t tile = low;
-        int width = c;
+        const size_t nr = remaining.size();
+        sup.resize(nr);
+        mix.resize(nr);
+        fit.resize(nr);
+        for (size_t i = 0; i < nr; ++i) {
+            sup[i] = op_support_mask(remaining[i]);
+            mix[i] = op_mixing_mask(remaining[i]);
+            fit[i] = fits(remaining[i]) ? 1 : 0;
+        }
+        Greedy best = greedy_pass(sup, mix, fit, m, low);
+        // seeded variants: the tile starts with the qubits of one of the first `seeds` ops at
+        // the front of the circuit (ready, non-diagonal); the pass that takes most work wins
         uint64_t blocked = 0;
+        int tried = 0;
+        for (size_t i = 0; i < nr && tried < seeds; ++i) {
+            if (sup[i] & blocked) {
+                blocked |= sup[i];
+                continue;
+            }
+            blocked |= sup[i];
+            if (!mix[i] || !fit[i]) continue;
+            ++tried;
+            Greedy g = greedy_pass(sup, mix, fit, m, low | mix[i]);
+            if (g.score > best.score) best = std::move(g);
+        }
+        uint64_t tile = best.tile;
+        int width = __builtin_popcountll(tile);
         TilePass pass;
         pass.low = c;
         std::vector<Op> deferred;
-        deferred.reserve(remaining.size());
-        for (Op& o : remaining) {
-            const uint64_t support = op_support_mask(o);
-            const uint64_t mix = op_mixing_mask(o);
-            if (support & blocked) {
-                deferred.push_back(std::move(o));
-                blocked |= support;
-                continue;
-            }
-            const uint64_t need = mix & ~tile;
-            const int extra = __builtin_popcountll(need);
-            if (fits(o) && width + extra <= m) {
-                tile |= need;
-                width += extra;
-                pass.ops.push_back(std::move(o));
-            } else {
-                deferred.push_back(std::move(o));
-                blocked |= support;
-            }
-        }
+        deferred.reserve(nr);
+        for (size_t i = 0; i < nr; ++i) (best.take[i] ? pass.ops : deferred).push_back(std::move(remaining[i]));
         // fill the tile up to m qubits with the lowest unused qubits (wider contiguous runs)
         for (int q = 0; q < n && width < m; ++q)
             if (!((tile >> q) & 1)) {
@@ -114,6 +157,20 @@ std::vector<TilePass> plan_tiles(const std::vector<Op>& ops_in, int n, int m, in
         remaining.swap(deferred);
     }
     return passes;
+}
+
+}  // namespace
+
+std::vector<TilePass> plan_tiles(const std::vector<Op>& ops_in, int n, int m, int c, int seeds) {
+    if (m > kTileMaxQubits) throw std::invalid_argument("tile wider than the shared-memory limit");
+    m = std::min(m, n);
+    c = std::min(c, m);
+    std::vector<TilePass> plain = plan_tiles_once(ops_in, n, m, c, 0);
+    if (seeds <= 0) return plain;
+    // a per-pass choice is not a plan-wide optimum: keep the seeded plan only when it has
+    // fewer passes
+    std::vector<TilePass> seeded = plan_tiles_once(ops_in, n, m, c, seeds);
+    return seeded.size() < plain.size() ? seeded : plain;
 }
 
 }  // namespace qsv

@@ -749,7 +749,13 @@ class B200Simulator:
         masks = to_masks(observable, n_qubits, where="run_gradient")
         stream = pack(commands, dict(params), list(param_order))
         reg = self.register(n_qubits)
-        self._seed(reg, n_qubits, initial_state, "run_gradient")
+
+        def seed():
+            self._seed(reg, n_qubits, initial_state, "run_gradient")
+        # the forward sweep runs the circuit's autotuned plan (the reverse sweep is tile passes
+        # over both registers whatever the plan)
+        self._plan_for(reg, commands, stream.buf, seed)
+        seed()
         energy, grad = reg.adjoint(stream, len(param_order), masks)
         if self._c64:
             from .precision import Complex64Report, h_norm1, plan_bound
