@@ -307,7 +307,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
 // the gate, accumulate <phi| G |psi> over the tile (FP64) and apply D (the gate's dagger) to both.
 // coef holds D then G, each 2^K x 2^K.  A thread owns the same groups in both parts, so the step
 // needs no barrier of its own; the caller reduces the returned per-thread partial.
-template <typename T, int K>
+// GC / DC: the generator's / the dagger's structure, known on the host (op.pad0): 0 general,
+// 1 diagonal, 2 (GC) off-diagonal or (DC) real.  A rotation's generator is a Pauli matrix and
+// its dagger a real rotation or a diagonal phase, so most parametric steps skip half of the
+// general complex arithmetic.
+template <typename T, int K, int GC = 0, int DC = 0>
 __device__ __forceinline__ double2 tile_adj(vec2_t<T>* a, vec2_t<T>* f, int m, const TileOpDev& op,
                                             const cplx<T>* coef) {
     constexpr int D = 1 << K;
@@ -354,6 +358,8 @@ __device__ __forceinline__ double2 tile_adj(vec2_t<T>* a, vec2_t<T>* f, int m, c
             double gr = 0, gi = 0;
 #pragma unroll
             for (int x = 0; x < D; ++x) {
+                if constexpr (GC == 1) { if (x != y) continue; }
+                if constexpr (GC == 2) { if (x == y) continue; }
                 const double cr = static_cast<double>(Gm[y * D + x].re), ci = static_cast<double>(Gm[y * D + x].im);
                 const double xr = static_cast<double>(ps[x].x), xi = static_cast<double>(ps[x].y);
                 gr = fma(cr, xr, gr); gr = fma(-ci, xi, gr);
@@ -365,12 +371,28 @@ __device__ __forceinline__ double2 tile_adj(vec2_t<T>* a, vec2_t<T>* f, int m, c
         }
 #pragma unroll
         for (int y = 0; y < D; ++y) {
-            vec2_t<T> o1 = cmul<T>(Dm[y * D], ps[0]);
-            vec2_t<T> o2 = cmul<T>(Dm[y * D], ph[0]);
+            vec2_t<T> o1, o2;
+            if constexpr (DC == 1) {
+                o1 = cmul<T>(Dm[y * D + y], ps[y]);
+                o2 = cmul<T>(Dm[y * D + y], ph[y]);
+            } else if constexpr (DC == 2) {
+                T r = Dm[y * D].re;
+                o1 = mk<T>(r * ps[0].x, r * ps[0].y);
+                o2 = mk<T>(r * ph[0].x, r * ph[0].y);
 #pragma unroll
-            for (int x = 1; x < D; ++x) {
-                o1 = cfma<T>(Dm[y * D + x], ps[x], o1);
-                o2 = cfma<T>(Dm[y * D + x], ph[x], o2);
+                for (int x = 1; x < D; ++x) {
+                    r = Dm[y * D + x].re;
+                    o1 = mk<T>(fma(r, ps[x].x, o1.x), fma(r, ps[x].y, o1.y));
+                    o2 = mk<T>(fma(r, ph[x].x, o2.x), fma(r, ph[x].y, o2.y));
+                }
+            } else {
+                o1 = cmul<T>(Dm[y * D], ps[0]);
+                o2 = cmul<T>(Dm[y * D], ph[0]);
+#pragma unroll
+                for (int x = 1; x < D; ++x) {
+                    o1 = cfma<T>(Dm[y * D + x], ps[x], o1);
+                    o2 = cfma<T>(Dm[y * D + x], ph[x], o2);
+                }
             }
             a[b0 | loff[y]] = o1;
             f[b0 | loff[y]] = o2;
@@ -473,7 +495,19 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_tile(vec2_t<T>* __restri
                 double2 v;
                 switch (op.k) {
                     case 0: v = tile_adj<T, 0>(cur, cur + M, m, op, oc); break;
-                    case 1: v = tile_adj<T, 1>(cur, cur + M, m, op, oc); break;
+                    case 1:
+                        switch (op.pad0) {   // generator class | dagger class << 2
+                            case 0x1: v = tile_adj<T, 1, 1, 0>(cur, cur + M, m, op, oc); break;
+                            case 0x2: v = tile_adj<T, 1, 2, 0>(cur, cur + M, m, op, oc); break;
+                            case 0x4: v = tile_adj<T, 1, 0, 1>(cur, cur + M, m, op, oc); break;
+                            case 0x5: v = tile_adj<T, 1, 1, 1>(cur, cur + M, m, op, oc); break;
+                            case 0x6: v = tile_adj<T, 1, 2, 1>(cur, cur + M, m, op, oc); break;
+                            case 0x8: v = tile_adj<T, 1, 0, 2>(cur, cur + M, m, op, oc); break;
+                            case 0x9: v = tile_adj<T, 1, 1, 2>(cur, cur + M, m, op, oc); break;
+                            case 0xA: v = tile_adj<T, 1, 2, 2>(cur, cur + M, m, op, oc); break;
+                            default: v = tile_adj<T, 1>(cur, cur + M, m, op, oc); break;
+                        }
+                        break;
                     default: v = tile_adj<T, 2>(cur, cur + M, m, op, oc); break;
                 }
                 v = warp_sum2(v);
@@ -788,6 +822,20 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
                     }
                     d.slot = pd.n_adj++;
                     d.gslot = static_cast<uint32_t>(o.slot);
+                    if (o.k == 1) {
+                        // structure of the stored (storage-precision) matrices, for tile_adj's
+                        // specialised forms
+                        auto zero = [](c128 v) {
+                            return static_cast<T>(v.real()) == T(0) && static_cast<T>(v.imag()) == T(0);
+                        };
+                        auto real = [](c128 v) { return static_cast<T>(v.imag()) == T(0); };
+                        const std::vector<c128>& G = o.g;
+                        const std::vector<c128>& Dg = o.m;
+                        const int gc = (zero(G[1]) && zero(G[2])) ? 1 : (zero(G[0]) && zero(G[3])) ? 2 : 0;
+                        const int dc = (zero(Dg[1]) && zero(Dg[2])) ? 1
+                                       : (real(Dg[0]) && real(Dg[1]) && real(Dg[2]) && real(Dg[3])) ? 2 : 0;
+                        d.pad0 = static_cast<uint8_t>(gc | (dc << 2));
+                    }
                     break;
                 }
                 case OP_DENSE:
