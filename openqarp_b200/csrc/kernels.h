@@ -187,6 +187,9 @@ struct PauliTerms {
     std::vector<int32_t> gstart;     // per group: first term (size groups + 1)
     std::vector<uint64_t> z;         // per term: Z mask
     std::vector<double> c;           // per term: coefficient * i^{nY} (re, im)
+    // per group, 9 term offsets: within a group the terms are ordered by their Z bits 5..7
+    // (the run bits of the <H> kernels), class k = those bits, terms [gclass[9g+k], gclass[9g+k+1])
+    std::vector<int32_t> gclass;
 };
 PauliTerms prepare_terms(const uint64_t* xmask, const uint64_t* zmask, const double* coeff,
                          size_t n_terms, int n_qubits);
