@@ -32,7 +32,8 @@ Also reported on the same line:
   * plain_12q_latency: the CPU-runnable 12-qubit configuration (HEA, 64-term <H>, 4000 shots)
     as microseconds per statevector / expectation / run call, beside the reference's calls;
   * circuit_batch: 1024 VQE-shaped circuits of 6..12 qubits, each with its own parameters and
-    observable, <H> and adjoint gradients of all of them in one graph-captured launch;
+    observable, <H> and adjoint gradients of all of them in one graph-captured launch (and 256
+    of 13..16 qubits, whose registers live in L2-resident scratch);
   * trajectories: feed-forward circuits (a mid-circuit measurement and a conditioned gate per
     layer) at 16 qubits (batched executor) and 10 qubits (shared-memory executor) sampled shot
     by shot on the device, noiseless and noisy, against the reference's CPU run() on a bounded
@@ -640,6 +641,8 @@ def b200_arm(args, rank, world, local_rank):
         if single and not args.skip_qaoa:
             from bench_workloads import circuit_batch_rows
             cbatch = circuit_batch_rows(device=device)
+            # members of 13..16 qubits keep their registers in the CTA's L2-resident scratch slot
+            cbatch["wide_13_16"] = circuit_batch_rows(device=device, count=256, sample=8, widths=(13, 16))
         heis = None
         if single and not args.skip_heisenberg:
             from bench_workloads import heisenberg_bulk

@@ -280,9 +280,10 @@ def config1_latency(device: int = 0, n: int = 12, layers: int = 10, n_terms: int
 
 # ---------------------------------------------------------------- general circuit batches
 
-def circuit_batch_rows(device: int = 0, count: int = 1024, seed: int = 1234, sample: int = 16) -> dict:
+def circuit_batch_rows(device: int = 0, count: int = 1024, seed: int = 1234, sample: int = 16,
+                       widths=(6, 12)) -> dict:
     """Many small VQE-shaped circuits in one persistent graph-captured launch: ``count``
-    hardware-efficient ansaetze of 6..12 qubits (1..4 layers), each with its own random
+    hardware-efficient ansaetze of ``widths`` qubits (1..4 layers), each with its own random
     parameters and its own observable (TFIM chain + random weight <= 3 terms), <H> and the
     adjoint gradient of every instance.  Compared with the same instances one at a time through
     B200Simulator.energy_and_gradient and through the reference's run_gradient on the host
@@ -293,7 +294,7 @@ def circuit_batch_rows(device: int = 0, count: int = 1024, seed: int = 1234, sam
     rng = np.random.default_rng(seed)
     insts = []
     for _ in range(count):
-        n = int(rng.integers(6, 13))
+        n = int(rng.integers(widths[0], widths[1] + 1))
         layers = int(rng.integers(1, 5))
         cmds, vals, names = circuits.hea(n, layers, seed=int(rng.integers(1 << 30)))
         obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, int(rng.integers(4, 32)),
@@ -323,7 +324,7 @@ def circuit_batch_rows(device: int = 0, count: int = 1024, seed: int = 1234, sam
     dt = time.perf_counter() - t0
     sim.close()
     scale = sum(cost) / sum(cost[int(j)] for j in pick)
-    out = {"instances": count, "widths": "6..12", "layers": "1..4", "ms_per_batch": ms,
+    out = {"instances": count, "widths": f"{widths[0]}..{widths[1]}", "layers": "1..4", "ms_per_batch": ms,
            "instances_per_s": count / (ms * 1e-3),
            "gradients": "adjoint, every parameter of every instance",
            "graph": "one CUDA graph: coefficients H2D, queue reset, persistent kernel, results D2H",

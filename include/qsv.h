@@ -328,10 +328,11 @@ QSV_API int qsv_qaoa_run(void* q, const double* params, int with_gradient, doubl
 QSV_API int qsv_qaoa_destroy(void* q);
 
 /* ---- circuit batches ---------------------------------------------------------------- *
- * Many circuits of uneven width (1..12 qubits, complex128), each with its own observable and
+ * Many circuits of uneven width (1..16 qubits, complex128), each with its own observable and
  * parameter values, evaluated in one persistent launch captured in a CUDA graph: a CTA takes
  * the next instance from a queue (costliest first) and keeps its |psi> and |phi> = H|psi> in
- * shared memory for the forward gates, <H>, and the adjoint reverse sweep.  Replaces the
+ * shared memory (up to 12 qubits) or in its own slot of an L2-resident scratch buffer (13..16
+ * qubits) for the forward gates, <H>, and the adjoint reverse sweep.  Replaces the
  * serial per-circuit loop of QarpSimulator::batch_expectation (reference:
  * qarp_simulator.cpp:971-984) and of the engine sweep (src/qarp/engines/_qarp_engine.py:
  * 450-503), with the adjoint of run_gradient_core (qarp_simulator.cpp:1519-1605) per instance.
@@ -342,7 +343,7 @@ QSV_API int qsv_qaoa_destroy(void* q);
  * inside the graph.  qsv_cbatch_run: energies[i] <- <H> of instance i; with_gradient batches
  * also fill grads, the instances' gradients back to back (n_params each); device_ms (may be
  * NULL) <- device time of the graph.  The first run builds the graph; instances are added
- * before it.  Registers wider than 12 qubits are refused with QSV_ECAPABILITY. */
+ * before it.  Registers wider than 16 qubits are refused with QSV_ECAPABILITY. */
 QSV_API int qsv_cbatch_create(int device, int with_gradient, void** out);
 QSV_API int qsv_cbatch_add(void* b, int n_qubits, const uint8_t* cmds, size_t nbytes, const int32_t* dep_ptr,
                            const int32_t* dep_param, const double* dep_alpha, int n_params,

@@ -1,6 +1,6 @@
 """Batched circuits: many instances of uneven width, one persistent graph-captured launch.
 
-``CircuitBatch`` wraps qsv_cbatch_* (include/qsv.h): arbitrary circuits of 1..12 qubits, each
+``CircuitBatch`` wraps qsv_cbatch_* (include/qsv.h): arbitrary circuits of 1..16 qubits, each
 with its own observable and parameter values, evaluated together — forward gates, <H> and,
 optionally, the adjoint gradient of every instance — in one CUDA graph; ``set`` swaps in new
 parameter values of an instance and the next ``run`` replays the graph.
@@ -149,7 +149,7 @@ def run_sharded(instances, params, rank: int, world: int, device: int, runner=No
 
 
 class CircuitBatch:
-    """Many circuits (1..12 qubits each, complex128) evaluated in one persistent launch.
+    """Many circuits (1..16 qubits each, complex128) evaluated in one persistent launch.
 
     ``add(commands, n_qubits, observable, values, param_order)`` appends an instance: its
     commands (symbolic parameters are substituted from ``values``), its Pauli-sum observable,
@@ -158,7 +158,7 @@ class CircuitBatch:
     ``with_gradient``, one gradient array per instance (in its ``param_order``).
     ``set(index, values)`` replaces an instance's parameter values; the structure stays."""
 
-    MAX_QUBITS = 12
+    MAX_QUBITS = 16   # registers of up to 12 qubits in shared memory, wider ones in L2-resident scratch
 
     def __init__(self, device: int = 0, with_gradient: bool = True):
         self.device = int(device)

@@ -753,7 +753,8 @@ template bool run_trajectories_fused<float>(const TrPlan&, int, const float2*, u
 
 namespace {
 
-constexpr int kCbMaxQubits = 12;
+constexpr int kCbMaxQubits = 12;   // both registers in shared memory
+constexpr int kCbMaxWide = 16;     // wider members: the CTA's pair in a global scratch slot (L2)
 
 struct CbInstDev {
     int32_t n, pad;
@@ -831,10 +832,10 @@ __global__ void __launch_bounds__(kFsThreads) k_cb_run(const CbInstDev* __restri
                                                       const uint64_t* __restrict__ tx, const uint64_t* __restrict__ tz,
                                                       const double2* __restrict__ tc, int with_grad,
                                                       int* __restrict__ queue, double* __restrict__ energy,
-                                                      double2* __restrict__ slots) {
+                                                      double2* __restrict__ slots, double2* __restrict__ wide,
+                                                      int wide_qubits) {
     extern __shared__ __align__(16) unsigned char cb_smem[];
-    double2* psi = reinterpret_cast<double2*>(cb_smem);
-    double2* phi = psi + (1 << kCbMaxQubits);
+    double2* const sm_psi = reinterpret_cast<double2*>(cb_smem);
     __shared__ uint64_t sstep[sizeof(FsStep) / 8];
     __shared__ __align__(16) double scoef[kFsMaxCoef];
     __shared__ double red[2 * kFsThreads / 32];
@@ -847,6 +848,17 @@ __global__ void __launch_bounds__(kFsThreads) k_cb_run(const CbInstDev* __restri
         const CbInstDev I = *QSV_DBG(inst + i);
         const int n = I.n;
         const uint64_t dim = 1ull << n;
+        // registers of up to kCbMaxQubits qubits in shared memory, wider ones in this CTA's
+        // scratch slot (2 x 2^wide_qubits amplitudes; the host sized it for the widest member)
+        double2* psi = sm_psi;
+        if (n > kCbMaxQubits) {
+            psi = wide + (static_cast<uint64_t>(blockIdx.x) << (wide_qubits + 1));
+            if (!QSV_DBG_RANGE_OK(psi, 32ull << wide_qubits)) {   // the debug build's check of the slot
+                __syncthreads();
+                continue;
+            }
+        }
+        double2* phi = psi + (n > kCbMaxQubits ? (1ull << wide_qubits) : (1ull << kCbMaxQubits));
         for (uint64_t j = threadIdx.x; j < dim; j += kFsThreads) psi[j] = make_double2(j == 0 ? 1.0 : 0.0, 0.0);
         // one step into shared memory: its record and its coefficients
         auto stage = [&](uint32_t s) -> const FsStep& {
@@ -988,6 +1000,8 @@ struct CircuitBatch {
     bool grad = false;
     // device side, built by finalize
     unsigned char* dev = nullptr;
+    double2* wide = nullptr;           // members above 12 qubits: one register pair per CTA
+    int wide_qubits = 0;
     double* host_coef = nullptr;       // pinned: the graph's source of coefficients
     double* host_out = nullptr;        // pinned: energies then slots
     size_t off_inst = 0, off_steps = 0, off_coef = 0, off_tx = 0, off_tz = 0, off_tc = 0, off_queue = 0,
@@ -1000,6 +1014,7 @@ struct CircuitBatch {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (dev) dev_free(dev);
+        if (wide) dev_free(wide);
         if (host_coef) cudaFreeHost(host_coef);
         if (host_out) cudaFreeHost(host_out);
         if (e0) cudaEventDestroy(e0);
@@ -1019,8 +1034,8 @@ int cbatch_add(void* bp, const std::vector<Cmd>& cmds, int n, const int32_t* dep
                const double* dep_alpha, int n_params, const PauliTerms& terms) {
     CircuitBatch* b = static_cast<CircuitBatch*>(bp);
     if (b->exec) throw std::invalid_argument("circuit batch: instances are added before the first run");
-    if (n < 1 || n > kCbMaxQubits)
-        throw capability_error("circuit batch: registers of 1.." + std::to_string(kCbMaxQubits) + " qubits");
+    if (n < 1 || n > kCbMaxWide)
+        throw capability_error("circuit batch: registers of 1.." + std::to_string(kCbMaxWide) + " qubits");
     CbInstHost h;
     h.n = n;
     h.n_params = b->grad ? n_params : 0;
@@ -1143,6 +1158,13 @@ void cb_finalize(CircuitBatch* b) {
     check_cuda(cudaFuncSetAttribute(k_cb_run, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                "batch smem");
     const unsigned grid = static_cast<unsigned>(std::min<size_t>(n_inst, static_cast<size_t>(sms)));
+    b->wide_qubits = 0;
+    for (const CbInstHost& h : b->inst)
+        if (h.n > kCbMaxQubits) b->wide_qubits = std::max(b->wide_qubits, h.n);
+    if (b->wide_qubits) {
+        const size_t bytes = static_cast<size_t>(grid) * (size_t{32} << b->wide_qubits);
+        check_cuda(dev_malloc(&b->wide, bytes), "circuit batch wide registers");
+    }
     // one graph: coefficients up, queue reset, the persistent kernel, results down
     check_cuda(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "batch capture");
     check_cuda(cudaMemcpyAsync(b->dev + b->off_coef, b->host_coef, b->coef.size() * sizeof(double),
@@ -1153,7 +1175,8 @@ void cb_finalize(CircuitBatch* b) {
         reinterpret_cast<const FsStep*>(b->dev + b->off_steps), reinterpret_cast<const double*>(b->dev + b->off_coef),
         reinterpret_cast<const uint64_t*>(b->dev + b->off_tx), reinterpret_cast<const uint64_t*>(b->dev + b->off_tz),
         reinterpret_cast<const double2*>(b->dev + b->off_tc), b->grad ? 1 : 0, reinterpret_cast<int*>(b->dev + b->off_queue),
-        reinterpret_cast<double*>(b->dev + b->off_energy), reinterpret_cast<double2*>(b->dev + b->off_slots));
+        reinterpret_cast<double*>(b->dev + b->off_energy), reinterpret_cast<double2*>(b->dev + b->off_slots),
+        b->wide, b->wide_qubits);
     check_cuda(cudaMemcpyAsync(b->host_out, b->dev + b->off_energy, n_inst * sizeof(double), cudaMemcpyDeviceToHost,
                                b->stream), "batch energies");
     if (b->n_slots)

@@ -696,12 +696,12 @@ class B200Simulator:
 
     def batch_expectation(self, commands, n_qubits: int, observable, param_sets) -> list:
         """<H> for every parameter set (QarpSimulator::batch_expectation,
-        qarp_simulator.cpp:971-984).  Registers of up to 12 qubits in complex128 run every set
+        qarp_simulator.cpp:971-984).  Registers of up to 16 qubits in complex128 run every set
         in one persistent launch (batch.CircuitBatch); wider ones set by set."""
         commands = list(commands)
         self._refuse_noise(_NOISY_STATEVECTOR)
         param_sets = list(param_sets)
-        if not self._c64 and 1 <= n_qubits <= 12 and len(param_sets) > 1:
+        if not self._c64 and 1 <= n_qubits <= 16 and len(param_sets) > 1:
             from .batch import CircuitBatch
             b = CircuitBatch(self.device, with_gradient=False)
             try:

@@ -104,7 +104,7 @@ def batches():
     """A circuit batch (HEA + QAOA members, gradients) and a batched QAOA launch."""
     from openqarp_b200.batch import CircuitBatch, QaoaBatch, QaoaInstance
     members = []
-    for i, n in enumerate((4, 7, 10, 12)):
+    for i, n in enumerate((4, 7, 10, 12, 14)):
         cmds, vals, names = circuits.hea(n, 2, seed=20 + i)
         obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, 6, seed=30 + i, max_weight=3)
         members.append((cmds, n, obs, vals, names))

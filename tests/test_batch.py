@@ -204,9 +204,9 @@ def test_circuit_batch_refuses_wide_registers_and_routes_batch_expectation(resta
     from openqarp_b200.errors import CapabilityError
     b = CircuitBatch(with_gradient=False)
     try:
-        cmds, vals, names = circuits.hea(13, 1, seed=1)
-        with pytest.raises(CapabilityError, match="1..12 qubits"):
-            b.add(cmds, 13, circuits.tfim_chain(13), vals)
+        cmds, vals, names = circuits.hea(17, 1, seed=1)
+        with pytest.raises(CapabilityError, match="1..16 qubits"):
+            b.add(cmds, 17, circuits.tfim_chain(17), vals)
     finally:
         b.close()
     n = 10
@@ -226,3 +226,29 @@ def test_circuit_batch_refuses_wide_registers_and_routes_batch_expectation(resta
         want.append(restatement.transition(psi, psi, n, masks).real)
     np.testing.assert_allclose(got[:8], want, rtol=0, atol=1e-10)
     assert len(got) == 64
+
+
+@pytest.mark.gpu
+def test_circuit_batch_wide_members_against_oracle(restatement):
+    """Members of 13..16 qubits (registers in the CTA's global scratch slot) mixed with narrow
+    ones in one launch: energies and gradients equal the CPU oracle's adjoint at 1e-10, twice."""
+    from openqarp_b200.batch import CircuitBatch
+    rng = np.random.default_rng(21)
+    insts = []
+    for n in (6, 13, 16, 12, 14, 9, 15):
+        cmds, vals, names = circuits.hea(n, 2, seed=int(rng.integers(1 << 30)))
+        obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, 12, seed=int(rng.integers(1 << 30)),
+                                                                 max_weight=3)
+        insts.append((cmds, n, obs, vals, names))
+    b = CircuitBatch(with_gradient=True)
+    try:
+        for inst in insts:
+            b.add(*inst)
+        for _ in range(2):
+            energies, grads, _ = b.run()
+            for j, (cmds, n, obs, vals, names) in enumerate(insts):
+                e, g = restatement.adjoint(ir.pack(cmds, vals, names), n, len(names), observable.to_masks(obs, n))
+                assert abs(energies[j] - e) < 1e-10, (n, energies[j], e)
+                np.testing.assert_allclose(grads[j], g, rtol=0, atol=1e-10, err_msg=f"n={n}")
+    finally:
+        b.close()
