@@ -388,8 +388,9 @@ QSV_API int qsv_device_info(int device, char* name, size_t cap, int* cc_major, i
  * buffers the library holds (and, during qsv_transition_static, the caller's two registers); an
  * access outside all of them is sent to a sink buffer instead and counted, and the entry point
  * that launched it returns QSV_ERUNTIME with the address and source line in qsv_last_error().
- * Every entry point of the debug build synchronises the device.  The compiled tile passes check
- * their amplitude indices against the register instead.
+ * Every entry point of the debug build synchronises the device, and its bookkeeping allocates on
+ * the host (qsv_transition_static included).  The compiled tile passes check their amplitude
+ * indices against the register instead.
  * qsv_debug_bounds_selftest: on `device`, a one-thread kernel reads one amplitude inside a 1 KiB
  * range the checks know and one 2 KiB past it (inside the 4 KiB buffer the self-test allocated,
  * so no read can leave device memory even if a check were wrong); *caught_in and *caught_out
