@@ -711,3 +711,32 @@ def test_28q_round_trip_and_norm():
     idx = reg.sample(np.array([0.5, 0.999999]))
     assert list(idx) == [0, 0]
     reg.close()
+
+
+@pytest.mark.parametrize("dtype,tol", [("complex128", AMP_TOL), ("complex64", 2e-5)])
+def test_compiled_passes_random_circuits_against_oracle(dtype, tol, restatement):
+    """The compiled tile passes (executor 3) on random circuits of every unitary gate kind at 17
+    qubits (five qubits outside each 12-qubit tile, chains of passes handing deferred phases on,
+    seeded tile planning), fusion widths 1..3, against the CPU oracle."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from gen_golden import all_gates_circuit
+    n = 17
+    for seed in (31, 32, 33):
+        rng = np.random.default_rng(seed)
+        cmds = circuits.brickwork(n, 3, seed=seed)
+        for part in range(3):
+            cmds += all_gates_circuit(n, 100 * seed + part)
+            cmds += circuits.brickwork(n, 2, seed=seed + 7 * part)
+            qs = tuple(int(q) for q in rng.permutation(n)[:4])
+            cmds.append(custom(qs, random_unitary(4, rng)))
+        buf = ir.pack(cmds).buf
+        want = restatement.statevector(buf, n)
+        for k in (1, 2, 3):
+            reg = Register(n, dtype)
+            reg.configure(k, 0, 3, 12)
+            reg.apply(buf)
+            got = reg.get_state()
+            reg.close()
+            err = float(np.max(np.abs(got - want)))
+            assert err < tol, f"seed {seed} k={k}: {err}"
