@@ -1,6 +1,6 @@
 """GPU parity: the CUDA engine (through the C-ABI) against the oracle and the reference's
-golden vectors.  Tolerances: amplitudes 1e-12 and <H> 1e-10 in complex128 (the north-star
-bar); sampled indices bit-exact given the same uniforms except at ties; complex64 bulk
+golden vectors.  Tolerances: amplitudes 1e-12 and <H> 1e-10 in complex128 (the parity bar
+of the hot path); sampled indices bit-exact given the same uniforms except at ties; complex64 bulk
 mode within single-precision error bounds stated per test."""
 import json
 import os
