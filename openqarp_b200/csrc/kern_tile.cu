@@ -577,7 +577,8 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
     std::vector<cplx<T>> cdev;
     for (size_t i = 0; i < passes.size(); ++i) {
         const TilePass& p = passes[i];
-        if (p.tile_qubits.empty() || rt_idx[i] >= 0) continue;
+        // shared-memory passes only: the launch loop below numbers exactly these
+        if (p.tile_qubits.empty() || rt_idx[i] >= 0 || (!jp.idx.empty() && jp.idx[i] >= 0)) continue;
         TilePassDev pd{};
         pd.m = static_cast<int32_t>(p.tile_qubits.size());
         for (size_t j = 0; j < p.tile_qubits.size(); ++j) pd.tq[j] = static_cast<uint8_t>(p.tile_qubits[j]);
@@ -669,12 +670,19 @@ void run_tiled(const std::vector<TilePass>& passes, vec2_t<T>* s, int n, cudaStr
     if (!pdev.empty()) std::memcpy(host.data() + a_p, pdev.data(), pdev.size() * sizeof(TilePassDev));
     if (!odev.empty()) std::memcpy(host.data() + a_o, odev.data(), odev.size() * sizeof(TileOpDev));
     if (!cdev.empty()) std::memcpy(host.data() + a_c, cdev.data(), cdev.size() * sizeof(cplx<T>));
-    check_cuda(cudaStreamSynchronize(st), "tile descriptor reuse");
-    uint8_t* dev = static_cast<uint8_t*>(ws.tiles(total));
-    check_cuda(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, st), "tile descriptors");
-    const TilePassDev* d_p = reinterpret_cast<const TilePassDev*>(dev + a_p);
-    const TileOpDev* d_o = reinterpret_cast<const TileOpDev*>(dev + a_o);
-    const cplx<T>* d_c = reinterpret_cast<const cplx<T>*>(dev + a_c);
+    // the descriptor buffer's previous user must be done before it is overwritten: only when
+    // shared-memory passes run (compiled and register-tile passes need no host wait here)
+    const TilePassDev* d_p = nullptr;
+    const TileOpDev* d_o = nullptr;
+    const cplx<T>* d_c = nullptr;
+    if (!pdev.empty()) {
+        check_cuda(cudaStreamSynchronize(st), "tile descriptor reuse");
+        uint8_t* dev = static_cast<uint8_t*>(ws.tiles(total));
+        check_cuda(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, st), "tile descriptors");
+        d_p = reinterpret_cast<const TilePassDev*>(dev + a_p);
+        d_o = reinterpret_cast<const TileOpDev*>(dev + a_o);
+        d_c = reinterpret_cast<const cplx<T>*>(dev + a_c);
+    }
     int sms = 0, device = 0;
     check_cuda(cudaGetDevice(&device), "device");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
