@@ -39,16 +39,17 @@ uint64_t op_support_mask(const Op& op);
 // seeds > 0: also plan with each pass's tile started from the qubits of one of the first
 // `seeds` ops at the circuit's front (the pass taking most work wins), and keep that plan when
 // it has fewer passes (the compiled tile passes use 32; a 28-qubit brickwork then takes 15
-// passes instead of 16)
+// passes instead of 16 in complex128 and 19 instead of 21 in complex64)
 std::vector<TilePass> plan_tiles(const std::vector<Op>& ops, int n, int m, int c = kTileLowQubits, int seeds = 0);
 constexpr int kJitPlanSeeds = 32;
 
-// Contiguous low qubits in the tiles of the compiled register-tile passes: runs of eight
-// amplitudes (128 bytes complex128, 64 bytes complex64), so loads and stores move whole
-// 32-byte sectors while every other tile qubit is free for the circuit.  On a 28-qubit
-// brickwork 12-qubit tiles then take 15 passes instead of the 25 that five mandatory low
-// qubits leave (complex64 with four low qubits took 19 passes and ran 3 % slower).
-inline int coalesced_low_qubits(int /*amp_bytes*/) { return 3; }
+// Contiguous low qubits in the tiles of the compiled register-tile passes: one 128-byte line per
+// run (8 complex128 or 16 complex64 amplitudes), so loads and stores stay whole-line while every
+// other tile qubit is free for the circuit.  On a 28-qubit brickwork 12-qubit tiles then take 15
+// passes (complex128; 19 in complex64) instead of the 25 that five mandatory low qubits leave.
+// Complex64 with three low qubits (64-byte runs) took 15 passes and ran its brickwork 3 % faster,
+// but its 31-qubit Heisenberg chain, nearer the HBM bound, 7 % slower.
+inline int coalesced_low_qubits(int amp_bytes) { return amp_bytes == 16 ? 3 : 4; }
 
 // ---------------------------------------------------------------- register-resident tiles
 // The register-tile kernel (kern_tile_rt.cu) holds a 2^12-amplitude tile in the registers of
