@@ -9,7 +9,7 @@ and fusion width the engine's autotuner chooses (openqarp_b200/autotune.py).  Th
 Metric, "gate GB/s": the workload's fixed gate work per step — the reference's own fused plan
 for the circuit (fusion width 3: 140 full-register passes) x 2 x 2^28 x 16 B — divided by the
 device time of one step.  It is an effective rate (work fixed by the workload, like tokens/s),
-not a count of the engine's own traffic: the engine's plan moves fewer bytes (16 compiled tile
+not a count of the engine's own traffic: the engine's plan moves fewer bytes (15 compiled tile
 passes), so it can exceed the HBM peak.  The engine's own HBM traffic is reported beside it
 (`hbm_gbs`, `hbm_frac_of_peak`).
 

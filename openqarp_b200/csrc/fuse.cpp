@@ -234,6 +234,7 @@ class BlockFuser {
         for (size_t r = 0; r < d; ++r)
             for (size_t j = 0; j < d; ++j) f.u[r * d + j] = cols[j * d + r];
         f.n_gates = b.src_gates;
+        f.fixed = std::all_of(b.gates.begin(), b.gates.end(), [&](size_t gi) { return in_[gi].fixed; });
         out_.push_back(std::move(f));
     }
 
@@ -316,6 +317,7 @@ std::vector<Cmd> fuse_single_qubit(const std::vector<Cmd>& in) {
                 f.q = {q};
                 f.u.assign(r.m, r.m + 4);
                 f.n_gates = r.src;
+                f.fixed = std::all_of(r.gates.begin(), r.gates.end(), [&](size_t gi) { return in[gi].fixed; });
                 out.push_back(std::move(f));
             }
         }

@@ -225,6 +225,11 @@ struct Gen {
     bool has[kRtQubits] = {};
     // a factor owed by every amplitude of the tile: the bit-0 phases of normalised tables
     c128 cglob{1.0, 0.0};
+    // rotations of fixed gates (no parameter: their values do not change between parameter
+    // sets): `forms` hashes which of the two forms each takes; with `spec` the source carries
+    // only that form instead of a branch on the coefficient
+    bool spec = false;
+    uint64_t forms = 1469598103934665603ull;
     int normalised = 0;   // normalised tables since cglob was last applied
     double flops = 0;   // FP64 operations per thread per tile (FMA = 2, MUL = 1)
 
@@ -443,7 +448,11 @@ struct Gen {
             has[b] = true;
             mark(0xB1u, static_cast<uint64_t>(p));
             flops += 8.0 * (kJitAmps / 2);
+            const bool fixed = gates[i]->op->fixed;
+            if (fixed) forms = (forms ^ (cos_form ? 0xC05u : 0x51Du)) * 1099511628211ull;
             if (!emit) continue;
+            // 0: branch on the coefficient, 1: cosine form only, 2: sine form only
+            const int only = (spec && fixed) ? (cos_form ? 1 : 2) : 0;
             const int B = 1 << p;
             std::ostringstream a, bb;
             if (f32) {
@@ -457,8 +466,10 @@ struct Gen {
                     bb << "    { const R2 y0 = " << x0 << "; " << x0 << " = __ffma2_rn(t2, y0, make_float2(-" << x1
                        << ".x, -" << x1 << ".y)); " << x1 << " = __ffma2_rn(t2, " << x1 << ", y0); }\n";
                 }
-                o << "  { const R t = " << cr(at) << "; const R2 t2 = make_float2(t, t), nt2 = make_float2(-t, -t);\n"
-                  << "  if (" << ci(at) << " != 0) {\n" << bb.str() << "  } else {\n" << a.str() << "  } }\n";
+                o << "  { const R t = " << cr(at) << "; const R2 t2 = make_float2(t, t), nt2 = make_float2(-t, -t);\n";
+                if (only == 1) o << a.str() << "  }\n";
+                else if (only == 2) o << bb.str() << "  }\n";
+                else o << "  if (" << ci(at) << " != 0) {\n" << bb.str() << "  } else {\n" << a.str() << "  } }\n";
                 continue;
             }
             for (int g = 0; g < kJitAmps; ++g) {
@@ -472,8 +483,10 @@ struct Gen {
                    << x0r << " = FMA(t, y0r, -" << x1r << "); " << x0i << " = FMA(t, y0i, -" << x1i << "); "
                    << x1r << " = FMA(t, " << x1r << ", y0r); " << x1i << " = FMA(t, " << x1i << ", y0i); }\n";
             }
-            o << "  { const R t = " << cr(at) << ";\n  if (" << ci(at) << " != 0) {\n" << bb.str()
-              << "  } else {\n" << a.str() << "  } }\n";
+            o << "  { const R t = " << cr(at) << ";\n";
+            if (only == 1) o << a.str() << "  }\n";
+            else if (only == 2) o << bb.str() << "  }\n";
+            else o << "  if (" << ci(at) << " != 0) {\n" << bb.str() << "  } else {\n" << a.str() << "  } }\n";
         }
     }
 
@@ -968,10 +981,12 @@ std::string pass_source(const TilePass& pass, const RtPlan& plan, int n, int idx
 // Source (with emit) or only the signature and coefficients (without) of one pass.
 bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emit, bool f32, std::string* src,
               std::vector<double>* coef, uint64_t* sig_hash, double* flops_per_amp = nullptr,
-              const Carry* cin = nullptr, bool final = true, Carry* cout = nullptr) {
+              const Carry* cin = nullptr, bool final = true, Carry* cout = nullptr, bool spec = false,
+              uint64_t* forms = nullptr) {
     Gen g;
     g.emit = emit;
     g.f32 = f32;
+    g.spec = spec;
     g.mark(f32 ? 0xF32u : 0xF64u);
     RtLayout last{};
     if (!walk_pass(pass, plan, n, &g, &last, cin, final, cout)) return false;
@@ -982,6 +997,7 @@ bool gen_pass(const TilePass& pass, const RtPlan& plan, int n, int idx, bool emi
             h *= 1099511628211ull;
         }
     *sig_hash = h;
+    if (forms) *forms = g.forms;
     if (flops_per_amp) *flops_per_amp = g.flops / kJitAmps;
     if (emit) *src = pass_source(pass, plan, n, idx, g.o.str(), g.coef.size(), last, f32);
     coef->swap(g.coef);
@@ -1066,6 +1082,7 @@ struct PassWalk {
     bool has_cin = false;
     Carry cin;
     bool final = true;
+    uint64_t forms = 0;   // the fixed gates' rotation forms (Gen::forms)
 };
 
 std::vector<PassWalk> walk_all(const std::vector<const TilePass*>& passes, std::vector<RtPlan>& plans, int n,
@@ -1078,7 +1095,8 @@ std::vector<PassWalk> walk_all(const std::vector<const TilePass*>& passes, std::
         if (!plan_rt(*passes[i], &plans[i], f32 ? 8 : 16)) continue;
         std::string unused;
         PassWalk& w = alone[i];
-        w.ok = gen_pass(*passes[i], plans[i], n, 0, false, f32, &unused, &w.coef, &w.sig, &w.flops_per_amp);
+        w.ok = gen_pass(*passes[i], plans[i], n, 0, false, f32, &unused, &w.coef, &w.sig, &w.flops_per_amp,
+                        nullptr, true, nullptr, false, &w.forms);
     }
     std::vector<PassWalk> chained(np);
     Carry cur;
@@ -1095,7 +1113,7 @@ std::vector<PassWalk> walk_all(const std::vector<const TilePass*>& passes, std::
         Carry next;
         std::string unused;
         w.ok = gen_pass(*passes[i], plans[i], n, 0, false, f32, &unused, &w.coef, &w.sig, &w.flops_per_amp,
-                        w.has_cin ? &w.cin : nullptr, w.final, w.final ? nullptr : &next);
+                        w.has_cin ? &w.cin : nullptr, w.final, w.final ? nullptr : &next, false, &w.forms);
         if (!w.ok) return alone;
         cur = std::move(next);
         in_chain = !w.final;
@@ -1104,6 +1122,27 @@ std::vector<PassWalk> walk_all(const std::vector<const TilePass*>& passes, std::
 }
 
 std::mutex g_jit_mu;
+
+// Compile-time rotation forms: a pass structure is compiled with its fixed gates' forms when it
+// is first seen; if the same structure later comes with other forms (fixed matrices that do
+// change between calls), it takes the branching kernel from then on, so a stream of new
+// matrices cannot force a compilation per call.  Guarded by g_jit_mu.
+std::map<uint64_t, uint64_t> g_first_forms;
+std::map<uint64_t, bool> g_unstable_forms;
+const uint64_t kNoForms = 1469598103934665603ull;
+
+bool specialise_forms(uint64_t sig, uint64_t forms) {
+    if (forms == kNoForms) return false;   // no fixed rotation in the pass
+    if (g_unstable_forms.count(sig)) return false;
+    auto it = g_first_forms.find(sig);
+    if (it == g_first_forms.end()) {
+        g_first_forms[sig] = forms;
+        return true;
+    }
+    if (it->second == forms) return true;
+    g_unstable_forms[sig] = true;
+    return false;
+}
 
 #ifdef QSV_DEBUG_BOUNDS
 // the compiled passes' fault words (count, first index), one per device, polled with the other
@@ -1191,6 +1230,15 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
     }
     if (sigs.empty()) return out;
     std::lock_guard<std::mutex> lock(g_jit_mu);
+    // passes whose fixed rotations are compiled with their forms get their own kernel key
+    std::vector<char> spec(sigs.size(), 0);
+    for (size_t k = 0; k < sigs.size(); ++k) {
+        const uint64_t forms = walks[pass_of[k]].forms;
+        if (specialise_forms(sigs[k], forms)) {
+            spec[k] = 1;
+            sigs[k] ^= (forms * 0x9E3779B97F4A7C15ull) ^ 0x5BEC0000ull;
+        }
+    }
     std::vector<size_t> missing;
     for (size_t k = 0; k < sigs.size(); ++k)
         if (!g_kernels.count({sigs[k], ctx})) missing.push_back(k);
@@ -1208,7 +1256,7 @@ JitPlan jit_prepare(const std::vector<const TilePass*>& passes, int n, int devic
             uint64_t sig = 0;
             Carry next;
             gen_pass(*passes[i], plans[i], n, 0, true, f32, &srcs[j], &coef, &sig, nullptr,
-                     w.has_cin ? &w.cin : nullptr, w.final, w.final ? nullptr : &next);
+                     w.has_cin ? &w.cin : nullptr, w.final, w.final ? nullptr : &next, spec[missing[j]] != 0);
             srcs[j] = std::string(kPrelude) + kPreludeDebug + srcs[j] + tag;
             char name[40];
             std::snprintf(name, sizeof name, "%016llx.cubin", static_cast<unsigned long long>(fnv1a(srcs[j])));
@@ -1286,7 +1334,7 @@ std::string jit_source_for_test(const std::vector<const TilePass*>& passes, int 
         uint64_t sig = 0;
         Carry out;
         if (!gen_pass(*passes[i], plans[i], n, next, true, f32, &ps, &coef, &sig, nullptr, w.has_cin ? &w.cin : nullptr,
-                      w.final, w.final ? nullptr : &out))
+                      w.final, w.final ? nullptr : &out, w.forms != kNoForms))
             continue;
         if (next > 0) {
             // one program holds every pass: the type definitions come once, with the first

@@ -134,6 +134,7 @@ std::vector<Cmd> decode(const uint8_t* buf, size_t nbytes) {
         c.p.resize(np);
         if (np) std::memcpy(c.p.data(), buf + o, 8 * np);
         o += 8 * np;
+        c.fixed = np == 0;
         if (c.gate == CUSTOM) {
             if (nq == 0 || nq > QSV_MAX_BLOCK_QUBITS)
                 throw std::runtime_error("Custom gate must carry a unitary and 1..8 qubit targets");
@@ -187,7 +188,15 @@ bool needs_trajectory(const Cmd& c) {
 
 // ---------------------------------------------------------------- lowering
 
+static std::vector<Op> lower_impl(const Cmd& c, int n);
+
 std::vector<Op> lower(const Cmd& c, int n) {
+    std::vector<Op> ops = lower_impl(c, n);
+    for (Op& o : ops) o.fixed = c.fixed;
+    return ops;
+}
+
+static std::vector<Op> lower_impl(const Cmd& c, int n) {
     const int g = c.gate;
     // register bounds: a csim kernel would silently write out of bounds; here it is an error
     for (size_t b = 0; b < c.q.size(); ++b) {

@@ -43,6 +43,9 @@ struct Cmd {
     std::vector<uint64_t> table;   // Permutation: |x> -> |table[x]>
     int flags = 0;           // bit 0: classical condition
     int n_gates = 1;         // source gates folded into this command (fusion statistics)
+    bool fixed = false;      // no parameter (Custom, H, CX, ...): its values stay the same from
+                             // one parameter set to the next; a fused block is fixed when all
+                             // its gates are
 };
 
 std::vector<Cmd> decode(const uint8_t* buf, size_t nbytes);
@@ -105,6 +108,7 @@ struct Op {
     std::vector<c128> g;           // OP_ADJ: generator matrix (2^k x 2^k)
     int slot = -1;                 // OP_ADJ: inner-product slot
     int n_gates = 1;
+    bool fixed = false;            // from a fixed command (Cmd::fixed)
 };
 
 // Lower one concrete command to device ops (empty for no-ops).

@@ -740,3 +740,22 @@ def test_compiled_passes_random_circuits_against_oracle(dtype, tol, restatement)
             reg.close()
             err = float(np.max(np.abs(got - want)))
             assert err < tol, f"seed {seed} k={k}: {err}"
+
+
+@pytest.mark.parametrize("dtype,tol", [("complex128", AMP_TOL), ("complex64", 2e-5)])
+def test_compiled_passes_fixed_matrices_change(dtype, tol, restatement):
+    """Compiled passes build a pass's fixed one-qubit rotations in their compile-time form the
+    first time its structure is seen, and fall back to the branching kernel once the same
+    structure comes with other matrices: circuits of one structure and three sets of Haar gates,
+    applied in the order A, B, A, C, against the CPU oracle."""
+    n = 16
+    bufs = {s: ir.pack(circuits.brickwork(n, 6, seed=s)).buf for s in (71, 72, 73)}
+    for s in (71, 72, 71, 73):
+        want = restatement.statevector(bufs[s], n)
+        reg = Register(n, dtype)
+        reg.configure(1, 0, 3, 12)
+        reg.apply(bufs[s])
+        got = reg.get_state()
+        reg.close()
+        err = float(np.max(np.abs(got - want)))
+        assert err < tol, f"seed {s}: {err}"
