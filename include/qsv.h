@@ -290,7 +290,8 @@ QSV_API int qsv_run_trajectories(void* h, const uint8_t* cmds, size_t nbytes, ui
  * dep_param[dep_ptr[i] .. dep_ptr[i+1]) with coefficients dep_alpha (d angle / d param).
  * grad has n_params entries; energy (may be NULL) receives <H>.  Replaces
  * QarpSimulator::run_gradient / run_gradient_core (qarp_simulator.cpp:1519-1605).
- * The register holds psi_final on return. */
+ * The reverse sweep un-computes psi in place: on return the register holds psi0 again, up to
+ * rounding and a unit global phase (prepare it again before reading it). */
 QSV_API int qsv_adjoint(void* h, const uint8_t* cmds, size_t nbytes,
                 const int32_t* dep_ptr, const int32_t* dep_param, const double* dep_alpha,
                 int n_params,

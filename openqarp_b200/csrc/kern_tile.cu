@@ -311,9 +311,91 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
 // 1 diagonal, 2 (GC) off-diagonal or (DC) real.  A rotation's generator is a Pauli matrix and
 // its dagger a real rotation or a diagonal phase, so most parametric steps skip half of the
 // general complex arithmetic.
+// One-qubit form: the step accumulates the sums S_yx = sum over the thread's groups of
+// conj(phi_y) psi_x for the generator's nonzero entries only (two or four complex sums, four
+// FMAs per pair and sum) and applies G to them once at the end, <phi|G|psi> = sum G_yx S_yx.
+// A diagonal dagger diag(d0, d1) is applied as diag(1, d1/d0): the factor d0 left out of both
+// states (adj_dropped_phase) is folded into later steps' inner products on the host, which
+// also resets psi's share of it when psi restarts from a checkpoint.
+template <typename T, int GC, int DC>
+__device__ __forceinline__ double2 tile_adj1(vec2_t<T>* a, vec2_t<T>* f, int m, const TileOpDev& op,
+                                             const cplx<T>* coef) {
+    const uint32_t p = op.lpos[0], bit = 1u << p;
+    cplx<T> Dm[4];
+    double Gr[4], Gi[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        Dm[e] = coef[e];
+        Gr[e] = static_cast<double>(coef[4 + e].re);
+        Gi[e] = static_cast<double>(coef[4 + e].im);
+    }
+    cplx<T> r1{};
+    if constexpr (DC == 1) {
+        const double d0r = static_cast<double>(Dm[0].re), d0i = static_cast<double>(Dm[0].im);
+        const double d1r = static_cast<double>(Dm[3].re), d1i = static_cast<double>(Dm[3].im);
+        const double inv = 1.0 / (d0r * d0r + d0i * d0i);
+        r1.re = static_cast<T>((d1r * d0r + d1i * d0i) * inv);
+        r1.im = static_cast<T>((d1i * d0r - d1r * d0i) * inv);
+    }
+    // S[e] for e = y * 2 + x
+    double sr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0};
+    const uint32_t groups = 1u << (m - 1);
+    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
+        const uint32_t l0 = ins_zero32(g, p), l1 = l0 | bit;
+        const vec2_t<T> ps0 = a[l0], ps1 = a[l1], ph0 = f[l0], ph1 = f[l1];
+        const vec2_t<T> ps[2] = {ps0, ps1}, ph[2] = {ph0, ph1};
+#pragma unroll
+        for (int y = 0; y < 2; ++y)
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {
+                if constexpr (GC == 1) { if (x != y) continue; }
+                if constexpr (GC == 2) { if (x == y) continue; }
+                const int e = y * 2 + x;
+                const double fr = static_cast<double>(ph[y].x), fi = static_cast<double>(ph[y].y);
+                const double xr = static_cast<double>(ps[x].x), xi = static_cast<double>(ps[x].y);
+                sr[e] = fma(fr, xr, sr[e]); sr[e] = fma(fi, xi, sr[e]);
+                si[e] = fma(fr, xi, si[e]); si[e] = fma(-fi, xr, si[e]);
+            }
+        vec2_t<T> o0, o1, q0, q1;
+        if constexpr (DC == 1) {
+            o0 = ps0; q0 = ph0;
+            o1 = cmul<T>(r1, ps1);
+            q1 = cmul<T>(r1, ph1);
+        } else if constexpr (DC == 2) {
+            const T r00 = Dm[0].re, r01 = Dm[1].re, r10 = Dm[2].re, r11 = Dm[3].re;
+            o0 = mk<T>(fma(r01, ps1.x, r00 * ps0.x), fma(r01, ps1.y, r00 * ps0.y));
+            o1 = mk<T>(fma(r11, ps1.x, r10 * ps0.x), fma(r11, ps1.y, r10 * ps0.y));
+            q0 = mk<T>(fma(r01, ph1.x, r00 * ph0.x), fma(r01, ph1.y, r00 * ph0.y));
+            q1 = mk<T>(fma(r11, ph1.x, r10 * ph0.x), fma(r11, ph1.y, r10 * ph0.y));
+        } else {
+            o0 = cfma<T>(Dm[1], ps1, cmul<T>(Dm[0], ps0));
+            o1 = cfma<T>(Dm[3], ps1, cmul<T>(Dm[2], ps0));
+            q0 = cfma<T>(Dm[1], ph1, cmul<T>(Dm[0], ph0));
+            q1 = cfma<T>(Dm[3], ph1, cmul<T>(Dm[2], ph0));
+        }
+        if constexpr (DC == 1) {
+            a[l1] = o1;
+            f[l1] = q1;
+        } else {
+            a[l0] = o0; a[l1] = o1;
+            f[l0] = q0; f[l1] = q1;
+        }
+    }
+    double ar = 0, ai = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        if constexpr (GC == 1) { if (e == 1 || e == 2) continue; }
+        if constexpr (GC == 2) { if (e == 0 || e == 3) continue; }
+        ar = fma(Gr[e], sr[e], ar); ar = fma(-Gi[e], si[e], ar);
+        ai = fma(Gr[e], si[e], ai); ai = fma(Gi[e], sr[e], ai);
+    }
+    return make_double2(ar, ai);
+}
+
 template <typename T, int K, int GC = 0, int DC = 0>
 __device__ __forceinline__ double2 tile_adj(vec2_t<T>* a, vec2_t<T>* f, int m, const TileOpDev& op,
                                             const cplx<T>* coef) {
+    if constexpr (K == 1) return tile_adj1<T, GC, DC>(a, f, m, op, coef);
     constexpr int D = 1 << K;
     uint32_t loff[D];
     uint8_t sp[K > 0 ? K : 1];
@@ -833,15 +915,8 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
                     if (o.k == 1) {
                         // structure of the stored (storage-precision) matrices, for tile_adj's
                         // specialised forms
-                        auto zero = [](c128 v) {
-                            return static_cast<T>(v.real()) == T(0) && static_cast<T>(v.imag()) == T(0);
-                        };
-                        auto real = [](c128 v) { return static_cast<T>(v.imag()) == T(0); };
-                        const std::vector<c128>& G = o.g;
-                        const std::vector<c128>& Dg = o.m;
-                        const int gc = (zero(G[1]) && zero(G[2])) ? 1 : (zero(G[0]) && zero(G[3])) ? 2 : 0;
-                        const int dc = (zero(Dg[1]) && zero(Dg[2])) ? 1
-                                       : (real(Dg[0]) && real(Dg[1]) && real(Dg[2]) && real(Dg[3])) ? 2 : 0;
+                        const int gc = adj_generator_class<T>(o.g);
+                        const int dc = adj_dagger_class<T>(o.m);
                         d.pad0 = static_cast<uint8_t>(gc | (dc << 2));
                     }
                     break;

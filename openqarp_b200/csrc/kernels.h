@@ -24,6 +24,30 @@ inline void check_cuda(cudaError_t e, const char* what) {
         throw cuda_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Structure of a one-qubit reverse step's 2 x 2 matrices as stored in precision T, which selects
+// the adjoint tile pass's specialised forms: 0 general, 1 diagonal, 2 off-diagonal (generator)
+// or real (dagger).
+template <typename T>
+inline bool stored_zero(c128 v) {
+    return static_cast<T>(v.real()) == T(0) && static_cast<T>(v.imag()) == T(0);
+}
+template <typename T>
+inline int adj_generator_class(const std::vector<c128>& G) {
+    return (stored_zero<T>(G[1]) && stored_zero<T>(G[2])) ? 1 : (stored_zero<T>(G[0]) && stored_zero<T>(G[3])) ? 2 : 0;
+}
+template <typename T>
+inline int adj_dagger_class(const std::vector<c128>& D) {
+    auto real = [](c128 v) { return static_cast<T>(v.imag()) == T(0); };
+    if (stored_zero<T>(D[1]) && stored_zero<T>(D[2])) return 1;
+    return (real(D[0]) && real(D[1]) && real(D[2]) && real(D[3])) ? 2 : 0;
+}
+// A diagonal dagger diag(d0, d1) runs as diag(1, d1 / d0) on both states; the factor left out
+// of them, d0 as stored, which the host folds into later steps' inner products.
+template <typename T>
+inline c128 adj_dropped_phase(const std::vector<c128>& D) {
+    return c128(static_cast<double>(static_cast<T>(D[0].real())), static_cast<double>(static_cast<T>(D[0].imag())));
+}
+
 // Device time of a handle's passes, by pass class: when enabled, every pass launch is
 // bracketed by a pair of CUDA events recorded on the handle's stream; collect() waits for
 // them and folds the durations into per-class totals.  Labels are string literals.

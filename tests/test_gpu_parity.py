@@ -654,6 +654,29 @@ def test_tiled_adjoint_complex64_with_checkpoints(restatement):
         assert np.max(np.abs(np.asarray(g) - g_or)) < 1e-4, k
 
 
+def test_tiled_adjoint_complex128_with_checkpoints(restatement):
+    """The tiled sweep leaves the diagonal daggers' first entries out of both states and folds
+    them into later inner products; restarts of psi from checkpoints (every 25 or 60 commands)
+    reset psi's share.  Gradients against the oracle with and without checkpoints."""
+    from openqarp_b200 import Register
+    n = 14
+    cmds, vals, names = _generator_circuit(n, 17, reps=3)
+    h_cmds, h_vals, h_names = circuits.hea(n, 3, seed=32)
+    cmds, names = cmds + h_cmds, names + h_names
+    vals.update(h_vals)
+    obs = circuits.tfim_chain(n) + circuits.random_pauli_sum(n, 12, seed=4, max_weight=3, coeff_std=0.3)
+    stream = ir.pack(cmds, vals, names)
+    m = observable.to_masks(obs, n)
+    _, g_or = restatement.adjoint(stream, n, len(names), m)
+    for k in (0, 25, 60):
+        reg = Register(n)
+        reg.set_checkpoint_interval(k)
+        reg.reset()
+        _, g = reg.adjoint(stream, len(names), m)
+        reg.close()
+        assert np.max(np.abs(np.asarray(g) - g_or)) < 1e-9, k
+
+
 def test_tiled_adjoint_phi_overlap(restatement, sim):
     n = 14
     cmds, vals, names = circuits.hea(n, 2, seed=7)
