@@ -307,16 +307,16 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_pass(vec2_t<T>* __rest
 // the gate, accumulate <phi| G |psi> over the tile (FP64) and apply D (the gate's dagger) to both.
 // coef holds D then G, each 2^K x 2^K.  A thread owns the same groups in both parts, so the step
 // needs no barrier of its own; the caller reduces the returned per-thread partial.
-// GC / DC: the generator's / the dagger's structure, known on the host (op.pad0): 0 general,
-// 1 diagonal, 2 (GC) off-diagonal or (DC) real.  A rotation's generator is a Pauli matrix and
-// its dagger a real rotation or a diagonal phase, so most parametric steps skip half of the
-// general complex arithmetic.
+// GC / DC: the generator's / the dagger's structure, known on the host (op.pad0,
+// adj_generator_class / adj_dagger_class): 0 general, 1 diagonal (DC: diag(1, d)), 2 (GC)
+// off-diagonal or (DC) real.  A rotation's generator is a Pauli matrix and its dagger a real
+// rotation or a diagonal phase, so most parametric steps skip half of the general complex
+// arithmetic.
 // One-qubit form: the step accumulates the sums S_yx = sum over the thread's groups of
 // conj(phi_y) psi_x for the generator's nonzero entries only (two or four complex sums, four
 // FMAs per pair and sum) and applies G to them once at the end, <phi|G|psi> = sum G_yx S_yx.
-// A diagonal dagger diag(d0, d1) is applied as diag(1, d1/d0): the factor d0 left out of both
-// states (adj_dropped_phase) is folded into later steps' inner products on the host, which
-// also resets psi's share of it when psi restarts from a checkpoint.
+// A diagonal dagger arrives as diag(1, d) (DC 1: the host takes the first entry out and folds
+// it into later inner products) and multiplies the |1> half alone.
 template <typename T, int GC, int DC>
 __device__ __forceinline__ double2 tile_adj1(vec2_t<T>* a, vec2_t<T>* f, int m, const TileOpDev& op,
                                              const cplx<T>* coef) {
@@ -329,14 +329,7 @@ __device__ __forceinline__ double2 tile_adj1(vec2_t<T>* a, vec2_t<T>* f, int m, 
         Gr[e] = static_cast<double>(coef[4 + e].re);
         Gi[e] = static_cast<double>(coef[4 + e].im);
     }
-    cplx<T> r1{};
-    if constexpr (DC == 1) {
-        const double d0r = static_cast<double>(Dm[0].re), d0i = static_cast<double>(Dm[0].im);
-        const double d1r = static_cast<double>(Dm[3].re), d1i = static_cast<double>(Dm[3].im);
-        const double inv = 1.0 / (d0r * d0r + d0i * d0i);
-        r1.re = static_cast<T>((d1r * d0r + d1i * d0i) * inv);
-        r1.im = static_cast<T>((d1i * d0r - d1r * d0i) * inv);
-    }
+    const cplx<T> r1 = Dm[3];   // DC == 1: diag(1, r1)
     // S[e] for e = y * 2 + x
     double sr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0};
     const uint32_t groups = 1u << (m - 1);
@@ -819,7 +812,8 @@ unsigned adjoint_tile_grid(int n, int m) {
 template <typename T>
 void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* phi, int n, int m,
                        double* d_partials, unsigned nb, cudaStream_t st, Workspace& ws,
-                       const std::function<void(const Op&)>& stream_op, uint64_t* launches) {
+                       const std::function<void(const Op&)>& stream_op, uint64_t* launches,
+                       std::vector<int>* slot_order) {
     if (ops.empty()) return;
     if (m < kTileMinQubits || m > n) throw std::logic_error("adjoint tile width outside the kernel's range");
     const std::vector<TilePass> planned = plan_tiles(ops, n, m);
@@ -912,6 +906,7 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
                     }
                     d.slot = pd.n_adj++;
                     d.gslot = static_cast<uint32_t>(o.slot);
+                    if (slot_order) slot_order->push_back(o.slot);   // the order the steps run in
                     if (o.k == 1) {
                         // structure of the stored (storage-precision) matrices, for tile_adj's
                         // specialised forms
@@ -1012,9 +1007,11 @@ void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* ph
 }
 
 template void run_adjoint_tiled<double>(const std::vector<Op>&, double2*, double2*, int, int, double*, unsigned,
-                                        cudaStream_t, Workspace&, const std::function<void(const Op&)>&, uint64_t*);
+                                        cudaStream_t, Workspace&, const std::function<void(const Op&)>&, uint64_t*,
+                                        std::vector<int>*);
 template void run_adjoint_tiled<float>(const std::vector<Op>&, float2*, float2*, int, int, double*, unsigned,
-                                       cudaStream_t, Workspace&, const std::function<void(const Op&)>&, uint64_t*);
+                                       cudaStream_t, Workspace&, const std::function<void(const Op&)>&, uint64_t*,
+                                       std::vector<int>*);
 
 template void run_tiled<double>(const std::vector<TilePass>&, double2*, int, cudaStream_t, Workspace&,
                                 const std::function<void(const Op&)>&, bool, bool);

@@ -25,11 +25,16 @@ inline void check_cuda(cudaError_t e, const char* what) {
 }
 
 // Structure of a one-qubit reverse step's 2 x 2 matrices as stored in precision T, which selects
-// the adjoint tile pass's specialised forms: 0 general, 1 diagonal, 2 off-diagonal (generator)
-// or real (dagger).
+// the adjoint tile pass's specialised forms.  Generator: 0 general, 1 diagonal, 2 off-diagonal.
+// Dagger: 0 general, 1 diag(1, d) (the host writes diagonal daggers so and folds the factor
+// taken out into later inner products), 2 real.
 template <typename T>
 inline bool stored_zero(c128 v) {
     return static_cast<T>(v.real()) == T(0) && static_cast<T>(v.imag()) == T(0);
+}
+template <typename T>
+inline bool stored_is(c128 v, double x) {
+    return static_cast<T>(v.real()) == static_cast<T>(x) && static_cast<T>(v.imag()) == T(0);
 }
 template <typename T>
 inline int adj_generator_class(const std::vector<c128>& G) {
@@ -38,14 +43,8 @@ inline int adj_generator_class(const std::vector<c128>& G) {
 template <typename T>
 inline int adj_dagger_class(const std::vector<c128>& D) {
     auto real = [](c128 v) { return static_cast<T>(v.imag()) == T(0); };
-    if (stored_zero<T>(D[1]) && stored_zero<T>(D[2])) return 1;
+    if (stored_zero<T>(D[1]) && stored_zero<T>(D[2])) return stored_is<T>(D[0], 1.0) ? 1 : 0;
     return (real(D[0]) && real(D[1]) && real(D[2]) && real(D[3])) ? 2 : 0;
-}
-// A diagonal dagger diag(d0, d1) runs as diag(1, d1 / d0) on both states; the factor left out
-// of them, d0 as stored, which the host folds into later steps' inner products.
-template <typename T>
-inline c128 adj_dropped_phase(const std::vector<c128>& D) {
-    return c128(static_cast<double>(static_cast<T>(D[0].real())), static_cast<double>(static_cast<T>(D[0].imag())));
 }
 
 // Device time of a handle's passes, by pass class: when enabled, every pass launch is
@@ -176,12 +175,14 @@ std::vector<char> jit_compile_for_test(const std::string& src, int cc_major, int
 // lowered daggers of non-parametric commands and OP_ADJ steps), planned into passes of m tile
 // qubits over both states; every OP_ADJ step writes partials[slot * nb + b] (double2) for the
 // nb = adjoint_tile_grid(n, m) CTAs.  Ops no tile holds go to `stream_op`, which applies them to
-// both states.
+// both states.  The planner may run steps on disjoint qubits out of stream order; `slot_order`
+// (when given) receives the OP_ADJ steps' slots in the order they run.
 unsigned adjoint_tile_grid(int n, int m);
 template <typename T>
 void run_adjoint_tiled(const std::vector<Op>& ops, vec2_t<T>* psi, vec2_t<T>* phi, int n, int m,
                        double* d_partials, unsigned nb, cudaStream_t st, Workspace& ws,
-                       const std::function<void(const Op&)>& stream_op, uint64_t* launches);
+                       const std::function<void(const Op&)>& stream_op, uint64_t* launches,
+                       std::vector<int>* slot_order = nullptr);
 
 // ---------------------------------------------------------------- register tiles (kern_tile_rt.cu)
 struct RtUpload {

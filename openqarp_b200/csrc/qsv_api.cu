@@ -1176,11 +1176,27 @@ constexpr int adjoint_tile_qubits() {
     return sizeof(T) == sizeof(double) ? 12 : 13;
 }
 
+// Writes a one-qubit reverse step's diagonal dagger diag(d0, d1) (2 x 2, row-major) as
+// diag(1, d1/d0), which the adjoint tile pass applies to the |1> half alone, and returns the
+// factor d0 taken out (D = d0 D'); other matrices stay as they are (returns 1).  Works on the
+// entries as stored in precision T.  (Scaling real rotations to unit entries the same way was
+// measured no faster on the 24-qubit HEA gradient and is not done.)
+template <typename T>
+c128 scale_dagger(std::vector<c128>& D) {
+    auto st = [](c128 v) {
+        return c128(static_cast<double>(static_cast<T>(v.real())), static_cast<double>(static_cast<T>(v.imag())));
+    };
+    const c128 a = st(D[0]), b = st(D[1]), c = st(D[2]), d = st(D[3]);
+    if (b != 0.0 || c != 0.0 || a == 0.0) return 1.0;
+    D = {1.0, 0.0, 0.0, d / a};
+    return a;
+}
+
 template <typename T>
 void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps, vec2_t<T>* psi,
                    vec2_t<T>* phi, double* grad, const Checkpoints& ck) {
     const int n = h->n;
-    struct Slot { size_t cmd; c128 pref; c128 corr = 1.0; };
+    struct Slot { size_t cmd; c128 pref; c128 corr = 1.0; c128 f = 1.0; };
     std::vector<Slot> slots;
     size_t n_param_steps = 0;
     for (size_t i = 0; i < cmds.size(); ++i)
@@ -1220,9 +1236,12 @@ void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps
     double* partials = static_cast<double*>(
         h->ws.scratch((n_param_steps * nb + n_param_steps + 1) * 2 * sizeof(double)));
     if (tiled) {
-        // phases the tile passes leave out of psi and phi (diagonal one-qubit daggers): the
-        // stored states are psi = p_psi * psi', phi = p_phi * phi', so a step's inner product is
-        // conj(p_phi) p_psi <phi'|G|psi'>
+        // factors the tile passes leave out of psi and phi (diagonal one-qubit daggers written
+        // by scale_dagger, f per step): the true states are p_psi psi' and p_phi phi' for the
+        // stored psi', phi', so a step's inner product is conj(p_phi) p_psi <phi'|G|psi'>, with
+        // p_psi and p_phi the products of f over the steps that ran before it, in the order the
+        // tile passes run them (the planner reorders steps on disjoint qubits).  psi restarts
+        // from a checkpoint unscaled.
         c128 p_psi = 1.0, p_phi = 1.0;
         std::vector<Op> segment;
         auto stream_op = [&](const Op& o) {
@@ -1231,7 +1250,15 @@ void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps
         };
         auto flush = [&]() {
             uint64_t launches = 0;
-            run_adjoint_tiled<T>(segment, psi, phi, n, mt, partials, nb, h->stream, h->ws, stream_op, &launches);
+            std::vector<int> order;
+            run_adjoint_tiled<T>(segment, psi, phi, n, mt, partials, nb, h->stream, h->ws, stream_op, &launches,
+                                 &order);
+            for (int sl : order) {
+                Slot& s = slots.at(static_cast<size_t>(sl));
+                s.corr = std::conj(p_phi) * p_psi;
+                p_psi *= s.f;
+                p_phi *= s.f;
+            }
             h->stats.launches += launches;
             h->stats.passes += launches;
             h->stats.hbm_bytes += launches * 4ull * h->dim() * h->amp_bytes();
@@ -1250,12 +1277,8 @@ void adjoint_sweep(Handle* h, const std::vector<Cmd>& cmds, const DepTable& deps
                 o.m = std::move(st.D);
                 o.g = std::move(st.G);
                 o.slot = static_cast<int>(slots.size());
-                slots.push_back({idx, pref, std::conj(p_phi) * p_psi});
-                if (o.k == 1 && adj_dagger_class<T>(o.m) == 1) {
-                    const c128 d0 = adj_dropped_phase<T>(o.m);
-                    p_psi *= d0;
-                    p_phi *= d0;
-                }
+                const c128 f = o.k == 1 ? scale_dagger<T>(o.m) : c128(1.0);
+                slots.push_back({idx, pref, 1.0, f});
                 segment.push_back(std::move(o));
             } else {
                 for (Op& o : lower(dagger(c), n)) segment.push_back(std::move(o));
