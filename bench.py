@@ -85,7 +85,9 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks, power and clock-event reasons sampled during the timed region: through NVML
+    every 20 ms where the nvidia-ml-py bindings load (read-only queries), else nvidia-smi
+    every 200 ms.  Samples use nvidia-smi's field order."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -97,7 +99,37 @@ class ClockSampler:
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        except Exception:  # noqa: BLE001
+            return None, None
+
     def _run(self):
+        nv, h = self._nvml()
+        if nv is not None:
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            try:
+                while not self._stop.is_set():
+                    try:
+                        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                        pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append([str(self.device), str(sm), str(mx), f"{pw:.1f}", hex(r)]
+                                            + ["Active" if r & b else "Not Active" for b in bits])
+                    except Exception:  # noqa: BLE001
+                        pass
+                    self._stop.wait(0.02)
+            finally:
+                try:
+                    nv.nvmlShutdown()
+                except Exception:  # noqa: BLE001
+                    pass
+            return
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
