@@ -43,13 +43,18 @@ uint64_t op_support_mask(const Op& op);
 std::vector<TilePass> plan_tiles(const std::vector<Op>& ops, int n, int m, int c = kTileLowQubits, int seeds = 0);
 constexpr int kJitPlanSeeds = 32;
 
-// Contiguous low qubits in the tiles of the compiled register-tile passes: one 128-byte line per
-// run (8 complex128 or 16 complex64 amplitudes), so loads and stores stay whole-line while every
-// other tile qubit is free for the circuit.  On a 28-qubit brickwork 12-qubit tiles then take 15
-// passes (complex128; 19 in complex64) instead of the 25 that five mandatory low qubits leave.
-// Complex64 with three low qubits (64-byte runs) took 15 passes and ran its brickwork 3 % faster,
-// but its 31-qubit Heisenberg chain, nearer the HBM bound, 7 % slower.
-inline int coalesced_low_qubits(int amp_bytes) { return amp_bytes == 16 ? 3 : 4; }
+// Contiguous low qubits in the tiles of the compiled register-tile passes: qubits 0..2 in both
+// storage types, one 128-byte line per run in complex128 (8 amplitudes) and 64 bytes in
+// complex64, so loads and stores stay whole-sector while every other tile qubit is free for
+// the circuit.  On a 28-qubit brickwork 12-qubit tiles then take 15 passes instead of the 25
+// that five mandatory low qubits leave.  Complex64 with four low qubits (128-byte runs) takes
+// 19 passes: its brickwork 24.5 against 23.9 ms, its 31-qubit Heisenberg chain 80.3 against
+// 79.4 ms a step (same box).  (Before the passes compiled fixed gates' rotation forms, the
+// chain ran 7 % faster with four.)
+inline int coalesced_low_qubits(int amp_bytes) {
+    (void)amp_bytes;
+    return 3;
+}
 
 // ---------------------------------------------------------------- register-resident tiles
 // The register-tile kernel (kern_tile_rt.cu) holds a 2^12-amplitude tile in the registers of
