@@ -648,6 +648,13 @@ def b200_arm(args, rank, world, local_rank):
             cpu = {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind,
                    "sample": f"the whole depth-{DEPTH} circuit once at {N_QUBITS} qubits ({cpasses} fused "
                              f"passes, k=3), {dt:.1f} s"}
+            # the same simulator on one host thread, on the circuit's first two layers
+            from openqarp_b200 import circuits, ir
+            head = ir.pack(circuits.brickwork(N_QUBITS, 2, seed=SEED)).buf
+            gbs1, dt1, cpasses1, _, kind1 = cpu_baseline_sample(head, N_QUBITS, threads=1)
+            cpu["single_thread"] = {"value": gbs1, "unit": "GB/s", "cores": 1, "kind": kind1,
+                                    "sample": f"the circuit's first 2 layers at {N_QUBITS} qubits "
+                                              f"({cpasses1} fused passes, k=3), {dt1:.1f} s"}
         scale30 = None
         if single and not args.skip_scale:
             scale30 = scale_row(device, 30)
