@@ -25,7 +25,7 @@ Also reported on the same line:
   * adjoint: 24-qubit HEA (8 layers, 384 parameters) with TFIM + 500 random weight<=4
     terms, gradients/s of the adjoint sweep vs the parameter-shift rule on the same GPU;
   * cpu_baseline: the reference's own CPU simulator (oracle/_ref) on the host cores, the whole
-    circuit once;
+    circuit once, and (single_thread) on one host thread over the circuit's first layer;
   * structured_and_readouts: a phase-estimation-shaped structured program (controlled powers
     + inverse QFT) at 28 and 22 qubits with the reference's CPU program_statevector at 22, the
     exact Born readout and the PauliAveraging parity counts on the device;
